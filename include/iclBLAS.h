@@ -1,0 +1,187 @@
+/*
+ * iclBLAS C API -- B200 (sm_100a) implementation.
+ *
+ * Call-compatible drop-in for the hot-path subset of Intel clGPU's
+ * include/iclBLAS/iclBLAS.h: the same type names, enum values, function names
+ * and parameter order, so code written against the reference header compiles
+ * and links against libiclblas_b200.so unchanged.  Every prototype below cites
+ * the reference declaration it replaces (include/iclBLAS/iclBLAS.h:<line>).
+ *
+ * Semantics kept from the reference:
+ *   - column-major storage, element (i,j) of a matrix at A[j*lda + i];
+ *   - scalars (alpha, beta) are host pointers read at call time;
+ *   - array arguments may be HOST pointers (as in the reference: the call
+ *     copies them to the device, runs, copies outputs back and returns when
+ *     the results are in host memory) or DEVICE pointers (extension: the call
+ *     is enqueued on the handle's stream and returns without waiting);
+ *   - result arguments of reductions (dot/nrm2/asum/iamax) follow the same
+ *     rule: a host pointer is written before return, a device pointer is
+ *     written by the device in stream order;
+ *   - iclblasIsamax / iclblasIcamax return a 0-based index;
+ *   - the error and early-return rules of libs/blas/shlib/iclBLAS_S.cpp,
+ *     iclBLAS_C.cpp and iclBLASImpl.hpp (validation order n, m, k, x, incx,
+ *     y, incy, A, lda, B, ldb, C, ldc; negative increments NOT_SUPPORTED).
+ *
+ * A handle owns one CUDA stream; it is not thread-safe, separate handles are
+ * independent (the reference has the same contract: one queue per handle).
+ */
+#ifndef ICLBLAS_B200_H
+#define ICLBLAS_B200_H
+
+#if defined(__GNUC__)
+#   define ICLBLAS_API __attribute__((visibility("default")))
+#else
+#   define ICLBLAS_API
+#endif
+
+#if defined(__GNUC__) || defined(__clang__)
+#   define ICLBLAS_ALWAYS_INLINE static inline __attribute__((always_inline))
+#else
+#   define ICLBLAS_ALWAYS_INLINE static inline
+#endif
+
+/* Complex single: two packed floats, {re, im}.  Same layout as the
+ * reference's oclComplex_t (iclBLAS.h:71-86), float2 and cuFloatComplex. */
+#ifdef __cplusplus
+#   include <complex>
+    typedef std::complex<float> oclComplex_t;
+    inline float Creal(const oclComplex_t& a)       { return a.real(); }
+    inline float Cimag(const oclComplex_t& a)       { return a.imag(); }
+    inline void  Csetreal(oclComplex_t* a, float r) { a->real(r); }
+    inline void  Csetimag(oclComplex_t* a, float i) { a->imag(i); }
+#else
+    typedef struct _oclComplex_t { float val[2]; } oclComplex_t;
+    ICLBLAS_ALWAYS_INLINE float Creal(struct _oclComplex_t a)              { return a.val[0]; }
+    ICLBLAS_ALWAYS_INLINE float Cimag(struct _oclComplex_t a)              { return a.val[1]; }
+    ICLBLAS_ALWAYS_INLINE void  Csetreal(struct _oclComplex_t* a, float r) { a->val[0] = r; }
+    ICLBLAS_ALWAYS_INLINE void  Csetimag(struct _oclComplex_t* a, float i) { a->val[1] = i; }
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes: values of iclBLAS.h:104-117 (ERROR follows LICENSE_ERROR). */
+typedef enum {
+    ICLBLAS_STATUS_SUCCESS          = 0,
+    ICLBLAS_STATUS_NOT_INITIALIZED  = 1,
+    ICLBLAS_STATUS_ALLOC_FAILED     = 3,
+    ICLBLAS_STATUS_INVALID_VALUE    = 7,
+    ICLBLAS_STATUS_ARCH_MISMATCH    = 8,
+    ICLBLAS_STATUS_MAPPING_ERROR    = 11,
+    ICLBLAS_STATUS_EXECUTION_FAILED = 13,
+    ICLBLAS_STATUS_INTERNAL_ERROR   = 14,
+    ICLBLAS_STATUS_NOT_SUPPORTED    = 15,
+    ICLBLAS_STATUS_LICENSE_ERROR    = 16,
+    ICLBLAS_STATUS_ERROR            = 17
+} iclblasStatus_t;
+
+/* Opaque library context (iclBLAS.h:123). */
+typedef struct iclblasContext* iclblasHandle_t;
+
+/* Enumerations: values of iclBLAS.h:128-158. */
+typedef enum { ICLBLAS_OP_N = 0, ICLBLAS_OP_T = 1, ICLBLAS_OP_C = 2 } iclblasOperation_t;
+typedef enum { ICLBLAS_FILL_MODE_UPPER = 0, ICLBLAS_FILL_MODE_LOWER = 1 } iclblasFillMode_t;
+typedef enum { ICLBLAS_DIAG_NON_UNIT = 0, ICLBLAS_DIAG_UNIT = 1 } iclblasDiagType_t;
+typedef enum { ICLBLAS_SIDE_LEFT = 0, ICLBLAS_SIDE_RIGHT = 1 } iclblasSideMode_t;
+
+/* ---- utilities ---- */
+/* replaces iclBLAS.h:172 */
+ICLBLAS_API iclblasStatus_t iclblasCreate(iclblasHandle_t* handle);
+/* replaces iclBLAS.h:179 */
+ICLBLAS_API iclblasStatus_t iclblasDestroy(iclblasHandle_t handle);
+
+/* ---- level 1, single ---- */
+/* replaces iclBLAS.h:219 */
+ICLBLAS_API iclblasStatus_t iclblasSscal(iclblasHandle_t handle, int n, const float* alpha, float* x, int incx);
+/* replaces iclBLAS.h:237 */
+ICLBLAS_API iclblasStatus_t iclblasSaxpy(iclblasHandle_t handle, int n, const float* alpha, float* x, int incx, float* y, int incy);
+/* replaces iclBLAS.h:250 */
+ICLBLAS_API iclblasStatus_t iclblasSnrm2(iclblasHandle_t handle, int n, float* x, int incx, float* result);
+/* replaces iclBLAS.h:275 (0-based index) */
+ICLBLAS_API iclblasStatus_t iclblasIsamax(iclblasHandle_t handle, int n, float* x, int incx, int* result);
+/* replaces iclBLAS.h:345 */
+ICLBLAS_API iclblasStatus_t iclblasSasum(iclblasHandle_t handle, int n, float* x, int incx, float* result);
+/* replaces iclBLAS.h:371 */
+ICLBLAS_API iclblasStatus_t iclblasSdot(iclblasHandle_t handle, int n, float* x, int incx, float* y, int incy, float* result);
+
+/* ---- level 1, complex ---- */
+/* replaces iclBLAS.h:411 */
+ICLBLAS_API iclblasStatus_t iclblasCscal(iclblasHandle_t handle, int n, const oclComplex_t* alpha, oclComplex_t* x, int incx);
+/* replaces iclBLAS.h:427 */
+ICLBLAS_API iclblasStatus_t iclblasCsscal(iclblasHandle_t handle, int n, const float* alpha, oclComplex_t* x, int incx);
+/* replaces iclBLAS.h:462 */
+ICLBLAS_API iclblasStatus_t iclblasCdotu(iclblasHandle_t handle, int n, oclComplex_t* x, int incx, oclComplex_t* y, int incy, oclComplex_t* result);
+/* replaces iclBLAS.h:475 */
+ICLBLAS_API iclblasStatus_t iclblasScnrm2(iclblasHandle_t handle, int n, oclComplex_t* x, int incx, float* result);
+/* replaces iclBLAS.h:488 (0-based index) */
+ICLBLAS_API iclblasStatus_t iclblasIcamax(iclblasHandle_t handle, int n, oclComplex_t* x, int incx, int* result);
+/* replaces iclBLAS.h:519 */
+ICLBLAS_API iclblasStatus_t iclblasCaxpy(iclblasHandle_t handle, int n, const oclComplex_t* alpha, oclComplex_t* x, int incx, oclComplex_t* y, int incy);
+/* replaces iclBLAS.h:549 */
+ICLBLAS_API iclblasStatus_t iclblasCdotc(iclblasHandle_t handle, int n, oclComplex_t* x, int incx, oclComplex_t* y, int incy, oclComplex_t* result);
+/* replaces iclBLAS.h:590 */
+ICLBLAS_API iclblasStatus_t iclblasScasum(iclblasHandle_t handle, int n, oclComplex_t* x, int incx, float* result);
+
+/* ---- level 2 ---- */
+/* replaces iclBLAS.h:630 */
+ICLBLAS_API iclblasStatus_t iclblasStrsv(iclblasHandle_t handle, iclblasFillMode_t uplo, iclblasOperation_t trans, iclblasDiagType_t diag,
+                                         int n, float* A, int lda, float* x, int incx);
+/* replaces iclBLAS.h:1049 */
+ICLBLAS_API iclblasStatus_t iclblasSgemv(iclblasHandle_t handle, iclblasOperation_t trans, int m, int n, const float* alpha,
+                                         float* A, int lda, float* x, int incx, const float* beta, float* y, int incy);
+/* replaces iclBLAS.h:1164 */
+ICLBLAS_API iclblasStatus_t iclblasCgemv(iclblasHandle_t handle, iclblasOperation_t trans, int m, int n, const oclComplex_t* alpha,
+                                         oclComplex_t* A, int lda, oclComplex_t* x, int incx, const oclComplex_t* beta,
+                                         oclComplex_t* y, int incy);
+/* replaces iclBLAS.h:1463 */
+ICLBLAS_API iclblasStatus_t iclblasCtrsv(iclblasHandle_t handle, iclblasFillMode_t uplo, iclblasOperation_t trans, iclblasDiagType_t diag,
+                                         int n, oclComplex_t* A, int lda, oclComplex_t* x, int incx);
+
+/* ---- level 3 ---- */
+/* replaces iclBLAS.h:1685 */
+ICLBLAS_API iclblasStatus_t iclblasSgemm(iclblasHandle_t handle, iclblasOperation_t transa, iclblasOperation_t transb, int m, int n, int k,
+                                         const float* alpha, float* A, int lda, float* B, int ldb, const float* beta, float* C, int ldc);
+/* replaces iclBLAS.h:1719 */
+ICLBLAS_API iclblasStatus_t iclblasStrsm(iclblasHandle_t handle, iclblasSideMode_t side, iclblasFillMode_t uplo, iclblasOperation_t trans,
+                                         iclblasDiagType_t diag, int m, int n, const float* alpha, float* A, int lda, float* B, int ldb);
+/* replaces iclBLAS.h:1799 */
+ICLBLAS_API iclblasStatus_t iclblasCgemm(iclblasHandle_t handle, iclblasOperation_t transa, iclblasOperation_t transb, int m, int n, int k,
+                                         const oclComplex_t* alpha, oclComplex_t* A, int lda, oclComplex_t* B, int ldb,
+                                         const oclComplex_t* beta, oclComplex_t* C, int ldc);
+/* replaces iclBLAS.h:1925 */
+ICLBLAS_API iclblasStatus_t iclblasCtrsm(iclblasHandle_t handle, iclblasSideMode_t side, iclblasFillMode_t uplo, iclblasOperation_t trans,
+                                         iclblasDiagType_t diag, int m, int n, const oclComplex_t* alpha, oclComplex_t* A, int lda,
+                                         oclComplex_t* B, int ldb);
+
+/* ======================================================================== */
+/* Extensions (new symbols; no reference counterpart).                      */
+/* ======================================================================== */
+
+/* Arithmetic used by S/C GEMM and by the trailing updates of S/C TRSM.
+ *   PLAIN_FP32: FP32 FFMA on the CUDA cores (the drop-in default);
+ *   TF32:       one TF32 product on the tensor cores, FP32 accumulate;
+ *   BF16X3:     FP32 operands split into three BF16 terms, the three leading
+ *               cross products on the tensor cores, FP32 accumulate;
+ *   BF16X6:     as BF16X3 with all six products of split order <= 2. */
+typedef enum {
+    ICLBLAS_MATH_PLAIN_FP32 = 0,
+    ICLBLAS_MATH_TF32       = 1,
+    ICLBLAS_MATH_BF16X3     = 2,
+    ICLBLAS_MATH_BF16X6     = 3
+} iclblasMathMode_t;
+
+/* Stream of the handle (a cudaStream_t passed as void*; NULL = the handle's
+ * own stream).  Device-pointer calls are enqueued on it. */
+ICLBLAS_API iclblasStatus_t iclblasSetStream(iclblasHandle_t handle, void* stream);
+ICLBLAS_API iclblasStatus_t iclblasGetStream(iclblasHandle_t handle, void** stream);
+ICLBLAS_API iclblasStatus_t iclblasSetMathMode(iclblasHandle_t handle, iclblasMathMode_t mode);
+ICLBLAS_API iclblasStatus_t iclblasGetMathMode(iclblasHandle_t handle, iclblasMathMode_t* mode);
+/* Wait for all work enqueued on the handle's stream; reports a device-side
+ * error flag (a bounded wait that ran out) as EXECUTION_FAILED. */
+ICLBLAS_API iclblasStatus_t iclblasSynchronize(iclblasHandle_t handle);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ICLBLAS_B200_H */

@@ -1,0 +1,557 @@
+/*
+ * CPU oracle for the iclBLAS hot path -- TEST INFRASTRUCTURE ONLY.
+ *
+ * Plain-C restatement of the reference's CPU algorithms.  Only the test
+ * suite, the smoke check and the CPU-baseline leg of the benchmark use it,
+ * as the checker; the GPU library never calls it.  Every function cites the
+ * reference file:line it restates (paths relative to the clGPU tree).
+ *
+ * Pinning: tests/golden/ holds the reference's own C-API known-answer suite
+ * compiled against oracle_capi.c (this oracle behind the iclBLAS C API), and
+ * the reference's CPU templates compiled from their own sources into
+ * oracle/_ref/ (oracle/Makefile) are compared with these functions on seeded
+ * random inputs by tests/test_oracle.py.
+ */
+#include "oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef struct { double re, im; } cd;
+
+static inline cd cd_make(double re, double im) { cd r = { re, im }; return r; }
+static inline cd cd_of(orc_c32 a) { return cd_make(a.re, a.im); }
+static inline cd cd_add(cd a, cd b) { return cd_make(a.re + b.re, a.im + b.im); }
+static inline cd cd_sub(cd a, cd b) { return cd_make(a.re - b.re, a.im - b.im); }
+static inline cd cd_mul(cd a, cd b) { return cd_make(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re); }
+static inline cd cd_conj(cd a) { return cd_make(a.re, -a.im); }
+static inline cd cd_div(cd a, cd b)
+{
+    double d = b.re * b.re + b.im * b.im;
+    return cd_make((a.re * b.re + a.im * b.im) / d, (a.im * b.re - a.re * b.im) / d);
+}
+static inline orc_c32 c32_of(cd a) { orc_c32 r = { (float)a.re, (float)a.im }; return r; }
+
+/* ------------------------------------------------------------------------ */
+/* Level 1                                                                  */
+/* ------------------------------------------------------------------------ */
+
+/* y += alpha*x in double, rounded once.
+ * Restates cpu_axpy (tests/blas_funcs/test_axpy.hpp:22-46). */
+void orc_saxpy(int n, float alpha, const float* x, int incx, float* y, int incy)
+{
+    double a = alpha;
+    for (int i = 0; i < n; ++i) {
+        double r = (double)y[(long)i * incy] + a * (double)x[(long)i * incx];
+        y[(long)i * incy] = (float)r;
+    }
+}
+
+/* x *= alpha.  Restates cpu_scal (tests/blas_funcs/test_scal.hpp:27-39). */
+void orc_sscal(int n, float alpha, float* x, int incx)
+{
+    double a = alpha;
+    for (int i = 0; i < n; ++i)
+        x[(long)i * incx] = (float)((double)x[(long)i * incx] * a);
+}
+
+/* sum x*y in double.  Restates cpu_dot (tests/blas_funcs/test_dot.hpp:22-51). */
+float orc_sdot(int n, const float* x, int incx, const float* y, int incy)
+{
+    double acc = 0.0;
+    for (int i = 0; i < n; ++i)
+        acc += (double)x[(long)i * incx] * (double)y[(long)i * incy];
+    return (float)acc;
+}
+
+/* Scaled two-norm (LAPACK-style scale/ssq update) in double.
+ * Restates cpu_nrm2 (tests/blas_funcs/test_nrm2.hpp:23-57). */
+float orc_snrm2(int n, const float* x, int incx)
+{
+    double scale = 0.0, ssq = 1.0;
+    for (int i = 0; i < n; ++i) {
+        double ax = fabs((double)x[(long)i * incx]);
+        if (ax != 0.0) {
+            if (scale < ax) {
+                double r = scale / ax;
+                ssq = 1.0 + r * r * ssq;
+                scale = ax;
+            } else {
+                double r = ax / scale;
+                ssq += r * r;
+            }
+        }
+    }
+    return (float)(scale * sqrt(ssq));
+}
+
+/* sum |x| in double.  Restates cpu_asum (tests/blas_funcs/test_asum.hpp:23-33). */
+float orc_sasum(int n, const float* x, int incx)
+{
+    double acc = 0.0;
+    for (int i = 0; i < n; ++i)
+        acc += fabs((double)x[(long)i * incx]);
+    return (float)acc;
+}
+
+/* 0-based index of the first maximal |x|, strict '>' scan starting from x[0].
+ * Restates amax_reference_impl (tests/blas_reference/blas_reference.cpp:46-64)
+ * with the -1 of cpu_amax<float> (tests/blas_funcs/test_amax.hpp:45-53).
+ * A NaN in x[0] pins the answer to 0; later NaNs are never selected. */
+int orc_isamax(int n, const float* x, int incx)
+{
+    if (n < 1 || incx < 1) return 0;
+    float best = fabsf(x[0]);
+    int idx = 0;
+    for (int i = 1; i < n; ++i) {
+        float v = fabsf(x[(long)i * incx]);
+        if (v > best) { best = v; idx = i; }
+    }
+    return idx;
+}
+
+/* y += alpha*x, complex, in double.  Restates cpu_axpy for complex<float>
+ * (tests/blas_funcs/test_axpy.hpp:22-46, acc = complex<double>). */
+void orc_caxpy(int n, orc_c32 alpha, const orc_c32* x, int incx, orc_c32* y, int incy)
+{
+    cd a = cd_of(alpha);
+    for (int i = 0; i < n; ++i) {
+        cd r = cd_add(cd_of(y[(long)i * incy]), cd_mul(a, cd_of(x[(long)i * incx])));
+        y[(long)i * incy] = c32_of(r);
+    }
+}
+
+/* x *= alpha, complex.  Restates cpu_scal (tests/blas_funcs/test_scal.hpp:27-39);
+ * Csscal is this with alpha = (a, 0) (libs/blas/shlib/iclBLAS_C.cpp:78-84). */
+void orc_cscal(int n, orc_c32 alpha, orc_c32* x, int incx)
+{
+    cd a = cd_of(alpha);
+    for (int i = 0; i < n; ++i)
+        x[(long)i * incx] = c32_of(cd_mul(cd_of(x[(long)i * incx]), a));
+}
+
+/* sum conj?(x)*y in complex<double>.  Restates cpu_dot<complex, conj>
+ * (tests/blas_funcs/test_dot.hpp:22-51); conj_x selects cdotc. */
+orc_c32 orc_cdot(int n, const orc_c32* x, int incx, const orc_c32* y, int incy, int conj_x)
+{
+    cd acc = cd_make(0.0, 0.0);
+    for (int i = 0; i < n; ++i) {
+        cd xv = cd_of(x[(long)i * incx]);
+        if (conj_x) xv = cd_conj(xv);
+        acc = cd_add(acc, cd_mul(xv, cd_of(y[(long)i * incy])));
+    }
+    return c32_of(acc);
+}
+
+/* Scaled two-norm over real and imaginary parts (every component is one
+ * term of the scale/ssq update), in double.  cpu_nrm2 takes abs() of a
+ * complex<double> (tests/blas_funcs/test_nrm2.hpp:23-57), i.e. the modulus
+ * per element; sqrt(sum |x_i|^2) is the same quantity. */
+float orc_scnrm2(int n, const orc_c32* x, int incx)
+{
+    double scale = 0.0, ssq = 1.0;
+    for (int i = 0; i < n; ++i) {
+        cd v = cd_of(x[(long)i * incx]);
+        double ax = hypot(v.re, v.im);
+        if (ax != 0.0) {
+            if (scale < ax) {
+                double r = scale / ax;
+                ssq = 1.0 + r * r * ssq;
+                scale = ax;
+            } else {
+                double r = ax / scale;
+                ssq += r * r;
+            }
+        }
+    }
+    return (float)(scale * sqrt(ssq));
+}
+
+/* sum |re|+|im| in double.  Restates cpu_asum with blas_abs of a complex
+ * (tests/blas_funcs/test_asum.hpp:23-33, test_helpers.hpp:241-246). */
+float orc_scasum(int n, const orc_c32* x, int incx)
+{
+    double acc = 0.0;
+    for (int i = 0; i < n; ++i) {
+        cd v = cd_of(x[(long)i * incx]);
+        acc += fabs(v.re) + fabs(v.im);
+    }
+    return (float)acc;
+}
+
+/* 0-based first index of max |re|+|im| in float.  Restates cpu_amax<complex>
+ * (tests/blas_funcs/test_amax.hpp:24-42) with scabs1 (core/src/ocl/complex.h.cl:54). */
+int orc_icamax(int n, const orc_c32* x, int incx)
+{
+    if (n < 1 || incx < 1) return 0;
+    float best = fabsf(x[0].re) + fabsf(x[0].im);
+    int idx = 0;
+    for (int i = 1; i < n; ++i) {
+        const orc_c32 v = x[(long)i * incx];
+        float a = fabsf(v.re) + fabsf(v.im);
+        if (a > best) { best = a; idx = i; }
+    }
+    return idx;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Level 2                                                                  */
+/* ------------------------------------------------------------------------ */
+
+/* y = alpha*op(A)*x + beta*y, double accumulation; beta == 0 means y is
+ * written without being read.  Restates Sgemv_naive
+ * (libs/blas/funcs/Sgemv/Sgemv_naive.cl:22-59; the beta != 0 test at :34,54). */
+void orc_sgemv(int trans, int m, int n, float alpha, const float* A, int lda,
+               const float* x, int incx, float beta, float* y, int incy)
+{
+    int rows = (trans == 0) ? m : n;
+    int cols = (trans == 0) ? n : m;
+    for (int r = 0; r < rows; ++r) {
+        double acc = 0.0;
+        for (int c = 0; c < cols; ++c) {
+            double a = (trans == 0) ? A[(long)c * lda + r] : A[(long)r * lda + c];
+            acc += a * (double)x[(long)c * incx];
+        }
+        double out = (double)alpha * acc;
+        if (beta != 0.0f) out += (double)beta * (double)y[(long)r * incy];
+        y[(long)r * incy] = (float)out;
+    }
+}
+
+/* Complex GEMV, op in {N, T, C}.  Restates Cgemv_naive
+ * (libs/blas/funcs/Cgemv/Cgemv_naive.cl:16-50), accumulated in double.  The
+ * reference kernel always reads y (:27,37,47); here, as for SGEMV, beta == 0
+ * means y is not read (identical for finite y). */
+void orc_cgemv(int trans, int m, int n, orc_c32 alpha, const orc_c32* A, int lda,
+               const orc_c32* x, int incx, orc_c32 beta, orc_c32* y, int incy)
+{
+    int rows = (trans == 0) ? m : n;
+    int cols = (trans == 0) ? n : m;
+    cd a = cd_of(alpha), b = cd_of(beta);
+    int beta_zero = (beta.re == 0.0f && beta.im == 0.0f);
+    for (int r = 0; r < rows; ++r) {
+        cd acc = cd_make(0, 0);
+        for (int c = 0; c < cols; ++c) {
+            cd e = (trans == 0) ? cd_of(A[(long)c * lda + r]) : cd_of(A[(long)r * lda + c]);
+            if (trans == 2) e = cd_conj(e);
+            acc = cd_add(acc, cd_mul(e, cd_of(x[(long)c * incx])));
+        }
+        cd out = cd_mul(a, acc);
+        if (!beta_zero) out = cd_add(out, cd_mul(b, cd_of(y[(long)r * incy])));
+        y[(long)r * incy] = c32_of(out);
+    }
+}
+
+/* Element (i,j) of op(A) for a triangular solve.  op: 0 = N, 1 = T, 2 = C
+ * (conjugate transpose), 3 = conjugate without transpose (used by the
+ * right-side complex solve). */
+static inline cd tri_elem_c(const orc_c32* A, int lda, int i, int j, int op)
+{
+    switch (op) {
+    case 0: return cd_of(A[(long)j * lda + i]);
+    case 1: return cd_of(A[(long)i * lda + j]);
+    case 2: return cd_conj(cd_of(A[(long)i * lda + j]));
+    default: return cd_conj(cd_of(A[(long)j * lda + i]));
+    }
+}
+
+/* Is op(A) lower triangular? */
+static inline int op_lower(int uplo, int op)
+{
+    int lower = (uplo == 1);
+    return (op == 0 || op == 3) ? lower : !lower;
+}
+
+/* In-place solve op(A) z = z (complex double). */
+static void tri_solve_cd(int uplo, int op, int diag, int n, const orc_c32* A, int lda, cd* z)
+{
+    if (op_lower(uplo, op)) {
+        for (int i = 0; i < n; ++i) {
+            cd s = z[i];
+            for (int j = 0; j < i; ++j) s = cd_sub(s, cd_mul(tri_elem_c(A, lda, i, j, op), z[j]));
+            z[i] = diag == 0 ? cd_div(s, tri_elem_c(A, lda, i, i, op)) : s;
+        }
+    } else {
+        for (int i = n - 1; i >= 0; --i) {
+            cd s = z[i];
+            for (int j = i + 1; j < n; ++j) s = cd_sub(s, cd_mul(tri_elem_c(A, lda, i, j, op), z[j]));
+            z[i] = diag == 0 ? cd_div(s, tri_elem_c(A, lda, i, i, op)) : s;
+        }
+    }
+}
+
+static inline double tri_elem_d(const double* A, int lda, int i, int j, int op)
+{
+    return (op == 0 || op == 3) ? A[(long)j * lda + i] : A[(long)i * lda + j];
+}
+
+/* In-place solve op(A) z = z (real double). */
+static void tri_solve_d(int uplo, int op, int diag, int n, const double* A, int lda, double* z)
+{
+    if (op_lower(uplo, op)) {
+        for (int i = 0; i < n; ++i) {
+            double s = z[i];
+            for (int j = 0; j < i; ++j) s -= tri_elem_d(A, lda, i, j, op) * z[j];
+            z[i] = diag == 0 ? s / tri_elem_d(A, lda, i, i, op) : s;
+        }
+    } else {
+        for (int i = n - 1; i >= 0; --i) {
+            double s = z[i];
+            for (int j = i + 1; j < n; ++j) s -= tri_elem_d(A, lda, i, j, op) * z[j];
+            z[i] = diag == 0 ? s / tri_elem_d(A, lda, i, i, op) : s;
+        }
+    }
+}
+
+/* Column-oriented left solve of op(A) Z = Z for `nrhs` columns of a
+ * column-major double matrix; forward/back substitution by columns of op(A)
+ * so that the op == N inner loop runs down contiguous columns of A. */
+static void tri_solve_cols_d(int uplo, int op, int diag, int n, const double* A, int lda,
+                             double* Z, long ldz, int nrhs)
+{
+    int lower = op_lower(uplo, op);
+    for (int c = 0; c < nrhs; ++c) {
+        double* z = Z + (long)c * ldz;
+        if (op == 0 || op == 3) {
+            if (lower) {
+                for (int i = 0; i < n; ++i) {
+                    if (diag == 0) z[i] /= A[(long)i * lda + i];
+                    double xi = z[i];
+                    const double* col = A + (long)i * lda;
+                    for (int k = i + 1; k < n; ++k) z[k] -= col[k] * xi;
+                }
+            } else {
+                for (int i = n - 1; i >= 0; --i) {
+                    if (diag == 0) z[i] /= A[(long)i * lda + i];
+                    double xi = z[i];
+                    const double* col = A + (long)i * lda;
+                    for (int k = 0; k < i; ++k) z[k] -= col[k] * xi;
+                }
+            }
+        } else {
+            tri_solve_d(uplo, op, diag, n, A, lda, z);
+        }
+    }
+}
+
+/* In-place solve op(A) z = z with float A and a double right-hand side,
+ * op 0 = N, 1 = T.  Every case walks a contiguous column of A: the two
+ * no-transpose cases as column updates (axpy form), the two transposed cases
+ * as dot products with a column. */
+static void tri_solve_fa(int uplo, int op, int diag, int n, const float* A, int lda, double* z)
+{
+    int lower = (uplo == 1);
+    if (op == 0 && lower) {
+        for (int i = 0; i < n; ++i) {
+            const float* col = A + (long)i * lda;
+            if (diag == 0) z[i] /= col[i];
+            double xi = z[i];
+            for (int k = i + 1; k < n; ++k) z[k] -= (double)col[k] * xi;
+        }
+    } else if (op == 0) {
+        for (int i = n - 1; i >= 0; --i) {
+            const float* col = A + (long)i * lda;
+            if (diag == 0) z[i] /= col[i];
+            double xi = z[i];
+            for (int k = 0; k < i; ++k) z[k] -= (double)col[k] * xi;
+        }
+    } else if (lower) {
+        for (int i = n - 1; i >= 0; --i) {
+            const float* col = A + (long)i * lda;
+            double s = z[i];
+            for (int j = i + 1; j < n; ++j) s -= (double)col[j] * z[j];
+            z[i] = diag == 0 ? s / col[i] : s;
+        }
+    } else {
+        for (int i = 0; i < n; ++i) {
+            const float* col = A + (long)i * lda;
+            double s = z[i];
+            for (int j = 0; j < i; ++j) s -= (double)col[j] * z[j];
+            z[i] = diag == 0 ? s / col[i] : s;
+        }
+    }
+}
+
+/* Strsv: solve op(A) x = b in place, double accumulation.  Restates
+ * Strsv_naive (libs/blas/funcs/Strsv/Strsv_naive.cl:20-73); op C is op T for
+ * real data. */
+void orc_strsv(int uplo, int trans, int diag, int n, const float* A, int lda, float* x, int incx)
+{
+    double* z = (double*)malloc(sizeof(double) * (size_t)n);
+    for (int i = 0; i < n; ++i) z[i] = x[(long)i * incx];
+    tri_solve_fa(uplo, trans == 0 ? 0 : 1, diag, n, A, lda, z);
+    for (int i = 0; i < n; ++i) x[(long)i * incx] = (float)z[i];
+    free(z);
+}
+
+/* Ctrsv with op in {N, T, C}.  Restates Ctrsv_naive
+ * (libs/blas/funcs/Ctrsv/Ctrsv_naive.cl:20-96). */
+void orc_ctrsv(int uplo, int trans, int diag, int n, const orc_c32* A, int lda, orc_c32* x, int incx)
+{
+    cd* z = (cd*)malloc(sizeof(cd) * (size_t)n);
+    for (int i = 0; i < n; ++i) z[i] = cd_of(x[(long)i * incx]);
+    tri_solve_cd(uplo, trans, diag, n, A, lda, z);
+    for (int i = 0; i < n; ++i) x[(long)i * incx] = c32_of(z[i]);
+    free(z);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Level 3                                                                  */
+/* ------------------------------------------------------------------------ */
+
+/* C = alpha*op(A)*op(B) + beta*C.  The accumulator is FP32 and each output
+ * sums its k terms in increasing k with fused multiply-adds; the update is
+ * fma(alpha, acc, beta*C), or alpha*acc without reading C when beta == 0.
+ * Restates the reference's selected SGEMM kernels: the per-element FMA loop
+ * of Sgemm_ntransAB (libs/blas/funcs/Sgemm/Sgemm_ntransAB.cl:16-40) and the
+ * subgroup kernel's epilogue (libs/blas/funcs/gemm_n3_template.h.cl:493-511).
+ * The reference's own 64^3 known-answer test compares against an FP32 loop
+ * in this order (tests/iclBLAS/test_Sgemm.cpp:256-270) and fails a double
+ * accumulator at 4 ulp, which is why this oracle is FP32; the double
+ * accumulating cpu_gemm (tests/blas_funcs/test_gemm.hpp:124-201) agrees with
+ * it exactly on the quarter-integer inputs its own tests use. */
+void orc_sgemm(int transa, int transb, int m, int n, int k, float alpha,
+               const float* A, int lda, const float* B, int ldb, float beta, float* C, int ldc)
+{
+    for (int j = 0; j < n; ++j) {
+        for (int i = 0; i < m; ++i) {
+            float acc = 0.0f;
+            for (int p = 0; p < k; ++p) {
+                float a = transa == 0 ? A[(long)p * lda + i] : A[(long)i * lda + p];
+                float b = transb == 0 ? B[(long)j * ldb + p] : B[(long)p * ldb + j];
+                acc = fmaf(a, b, acc);
+            }
+            float* c = &C[(long)j * ldc + i];
+            if (beta == 0.0f) *c = alpha * acc;
+            else *c = fmaf(alpha, acc, beta * *c);
+        }
+    }
+}
+
+/* Complex GEMM, op in {N, T, C} per operand.  Restates cpu_gemm for
+ * complex<float> (tests/blas_funcs/test_gemm.hpp:60-201, conj helper :38-57). */
+void orc_cgemm(int transa, int transb, int m, int n, int k, orc_c32 alpha,
+               const orc_c32* A, int lda, const orc_c32* B, int ldb, orc_c32 beta, orc_c32* C, int ldc)
+{
+    cd al = cd_of(alpha), be = cd_of(beta);
+    int beta_zero = (beta.re == 0.0f && beta.im == 0.0f);
+    for (int j = 0; j < n; ++j) {
+        for (int i = 0; i < m; ++i) {
+            cd acc = cd_make(0, 0);
+            for (int p = 0; p < k; ++p) {
+                cd a = transa == 0 ? cd_of(A[(long)p * lda + i]) : cd_of(A[(long)i * lda + p]);
+                cd b = transb == 0 ? cd_of(B[(long)j * ldb + p]) : cd_of(B[(long)p * ldb + j]);
+                if (transa == 2) a = cd_conj(a);
+                if (transb == 2) b = cd_conj(b);
+                acc = cd_add(acc, cd_mul(a, b));
+            }
+            orc_c32* c = &C[(long)j * ldc + i];
+            cd out = cd_mul(acc, al);
+            if (!beta_zero) out = cd_add(out, cd_mul(cd_of(*c), be));
+            *c = c32_of(out);
+        }
+    }
+}
+
+/* Strsm: op(A) X = alpha B (left) or X op(A) = alpha B (right); X overwrites
+ * B.  Restates Strsm_naive (libs/blas/funcs/Strsm/Strsm_naive.cl:18-126): the
+ * solve runs on the unscaled B and alpha multiplies each solved entry on the
+ * store (:35).  Arithmetic in double. */
+void orc_strsm(int side, int uplo, int trans, int diag, int m, int n, float alpha,
+               const float* A, int lda, float* B, int ldb)
+{
+    int op = (trans == 0) ? 0 : 1;
+    if (side == 0) {
+        double* z = (double*)malloc(sizeof(double) * (size_t)m);
+        for (int j = 0; j < n; ++j) {
+            for (int i = 0; i < m; ++i) z[i] = B[(long)j * ldb + i];
+            tri_solve_fa(uplo, op, diag, m, A, lda, z);
+            for (int i = 0; i < m; ++i) B[(long)j * ldb + i] = (float)(z[i] * (double)alpha);
+        }
+        free(z);
+    } else {
+        /* X op(A) = B  <=>  op(A)^T X^T = B^T: each row of B is solved with
+         * the transposed operator. */
+        double* z = (double*)malloc(sizeof(double) * (size_t)n);
+        for (int i = 0; i < m; ++i) {
+            for (int j = 0; j < n; ++j) z[j] = B[(long)j * ldb + i];
+            tri_solve_fa(uplo, 1 - op, diag, n, A, lda, z);
+            for (int j = 0; j < n; ++j) B[(long)j * ldb + i] = (float)(z[j] * (double)alpha);
+        }
+        free(z);
+    }
+}
+
+/* Ctrsm with op in {N, T, C}.  Restates Ctrsm_naive
+ * (libs/blas/funcs/Ctrsm/Ctrsm_naive.cl:18-183): division by conj(diag) for
+ * op C (:33), alpha applied on the store (:43).  Arithmetic in complex double. */
+void orc_ctrsm(int side, int uplo, int trans, int diag, int m, int n, orc_c32 alpha,
+               const orc_c32* A, int lda, orc_c32* B, int ldb)
+{
+    cd al = cd_of(alpha);
+    if (side == 0) {
+        cd* z = (cd*)malloc(sizeof(cd) * (size_t)m);
+        for (int j = 0; j < n; ++j) {
+            for (int i = 0; i < m; ++i) z[i] = cd_of(B[(long)j * ldb + i]);
+            tri_solve_cd(uplo, trans, diag, m, A, lda, z);
+            for (int i = 0; i < m; ++i) B[(long)j * ldb + i] = c32_of(cd_mul(z[i], al));
+        }
+        free(z);
+    } else {
+        /* X op(A) = B  <=>  op(A)^T X^T = B^T: solve each row of B with the
+         * transposed operator (N -> T, T -> N, C -> conj without transpose). */
+        int op = (trans == 0) ? 1 : (trans == 1) ? 0 : 3;
+        cd* z = (cd*)malloc(sizeof(cd) * (size_t)n);
+        for (int i = 0; i < m; ++i) {
+            for (int j = 0; j < n; ++j) z[j] = cd_of(B[(long)j * ldb + i]);
+            tri_solve_cd(uplo, op, diag, n, A, lda, z);
+            for (int j = 0; j < n; ++j) B[(long)j * ldb + i] = c32_of(cd_mul(z[j], al));
+        }
+        free(z);
+    }
+}
+
+/* FP64 GEMM, same semantics as orc_sgemm; loops ordered j, p, i so the
+ * inner loop walks a column of C and (for op(A) = N) a column of A. */
+void orc_dgemm(int transa, int transb, int m, int n, int k, double alpha,
+               const double* A, int lda, const double* B, int ldb, double beta, double* C, int ldc)
+{
+    double* acc = (double*)malloc(sizeof(double) * (size_t)m);
+    for (int j = 0; j < n; ++j) {
+        memset(acc, 0, sizeof(double) * (size_t)m);
+        for (int p = 0; p < k; ++p) {
+            double b = transb == 0 ? B[(long)j * ldb + p] : B[(long)p * ldb + j];
+            if (transa == 0) {
+                const double* col = A + (long)p * lda;
+                for (int i = 0; i < m; ++i) acc[i] += col[i] * b;
+            } else {
+                for (int i = 0; i < m; ++i) acc[i] += A[(long)i * lda + p] * b;
+            }
+        }
+        double* c = C + (long)j * ldc;
+        for (int i = 0; i < m; ++i) c[i] = (beta == 0.0) ? acc[i] * alpha : acc[i] * alpha + c[i] * beta;
+    }
+    free(acc);
+}
+
+/* FP64 TRSM, same semantics as orc_strsm (alpha applied after the solve). */
+void orc_dtrsm(int side, int uplo, int trans, int diag, int m, int n, double alpha,
+               const double* A, int lda, double* B, int ldb)
+{
+    int op = (trans == 0) ? 0 : 1;
+    if (side == 0) {
+        tri_solve_cols_d(uplo, op, diag, m, A, lda, B, ldb, n);
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < m; ++i) B[(long)j * ldb + i] *= alpha;
+    } else {
+        int rop = (op == 0) ? 1 : 0;
+        double* z = (double*)malloc(sizeof(double) * (size_t)n);
+        for (int i = 0; i < m; ++i) {
+            for (int j = 0; j < n; ++j) z[j] = B[(long)j * ldb + i];
+            tri_solve_d(uplo, rop, diag, n, A, lda, z);
+            for (int j = 0; j < n; ++j) B[(long)j * ldb + i] = z[j] * alpha;
+        }
+        free(z);
+    }
+}

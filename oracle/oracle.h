@@ -1,0 +1,72 @@
+/*
+ * CPU oracle for the iclBLAS hot path (test infrastructure only).
+ *
+ * This header declares a plain-C restatement of the reference's CPU
+ * algorithms for the S/C gemm, gemv, trsv, trsm, dot, nrm2, asum, iamax,
+ * axpy and scal routines.  It is the checker the GPU library is compared
+ * against; nothing in the shipped library links it.  Each function names the
+ * reference source it restates (paths are relative to the clGPU tree).
+ *
+ * Conventions (same as the reference): column-major storage, element (i,j)
+ * at j*ld+i (libs/blas/funcs/iclblas_common.h.cl:47); positive strides only;
+ * complex numbers are two packed floats {re, im}.
+ *
+ * Arithmetic: like the reference test oracles (tests/blas_funcs/test_*.hpp,
+ * accumulator_type<float> = double, tests/blas_funcs/test_helpers.hpp:216-232)
+ * every accumulation runs in double and is rounded to float once at the end,
+ * except SGEMM, which follows the reference kernels' FP32 FMA order.
+ */
+#ifndef ICLB_ORACLE_H
+#define ICLB_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct { float re, im; } orc_c32;
+
+/* ---- level 1, single ---- */
+void  orc_saxpy(int n, float alpha, const float* x, int incx, float* y, int incy);
+void  orc_sscal(int n, float alpha, float* x, int incx);
+float orc_sdot(int n, const float* x, int incx, const float* y, int incy);
+float orc_snrm2(int n, const float* x, int incx);
+float orc_sasum(int n, const float* x, int incx);
+int   orc_isamax(int n, const float* x, int incx);
+
+/* ---- level 1, complex ---- */
+void    orc_caxpy(int n, orc_c32 alpha, const orc_c32* x, int incx, orc_c32* y, int incy);
+void    orc_cscal(int n, orc_c32 alpha, orc_c32* x, int incx);
+orc_c32 orc_cdot(int n, const orc_c32* x, int incx, const orc_c32* y, int incy, int conj_x);
+float   orc_scnrm2(int n, const orc_c32* x, int incx);
+float   orc_scasum(int n, const orc_c32* x, int incx);
+int     orc_icamax(int n, const orc_c32* x, int incx);
+
+/* ---- level 2 ---- */
+void orc_sgemv(int trans, int m, int n, float alpha, const float* A, int lda,
+               const float* x, int incx, float beta, float* y, int incy);
+void orc_cgemv(int trans, int m, int n, orc_c32 alpha, const orc_c32* A, int lda,
+               const orc_c32* x, int incx, orc_c32 beta, orc_c32* y, int incy);
+void orc_strsv(int uplo, int trans, int diag, int n, const float* A, int lda, float* x, int incx);
+void orc_ctrsv(int uplo, int trans, int diag, int n, const orc_c32* A, int lda, orc_c32* x, int incx);
+
+/* ---- level 3 ---- */
+void orc_sgemm(int transa, int transb, int m, int n, int k, float alpha,
+               const float* A, int lda, const float* B, int ldb, float beta, float* C, int ldc);
+void orc_cgemm(int transa, int transb, int m, int n, int k, orc_c32 alpha,
+               const orc_c32* A, int lda, const orc_c32* B, int ldb, orc_c32 beta, orc_c32* C, int ldc);
+void orc_strsm(int side, int uplo, int trans, int diag, int m, int n, float alpha,
+               const float* A, int lda, float* B, int ldb);
+void orc_ctrsm(int side, int uplo, int trans, int diag, int m, int n, orc_c32 alpha,
+               const orc_c32* A, int lda, orc_c32* B, int ldb);
+
+/* FP64 variants used as the error reference for the precision study
+ * (double in, double out; same semantics as the float versions). */
+void orc_dgemm(int transa, int transb, int m, int n, int k, double alpha,
+               const double* A, int lda, const double* B, int ldb, double beta, double* C, int ldc);
+void orc_dtrsm(int side, int uplo, int trans, int diag, int m, int n, double alpha,
+               const double* A, int lda, double* B, int ldb);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

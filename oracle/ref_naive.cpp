@@ -1,0 +1,97 @@
+// The reference's serial OpenCL kernels compiled as C++ -- TEST INFRASTRUCTURE.
+//
+// Each kernel is #included from its .cl file in the clGPU tree (built by
+// oracle/Makefile into oracle/_ref/) behind clshim.hpp and exported with an
+// extern "C" wrapper.  They give CPU results of the reference's own GEMV,
+// TRSV, TRSM and CGEMM algorithms, which its tests have no template for.
+#include "clshim.hpp"
+
+namespace ref_sgemv {
+#include "Sgemv/Sgemv_naive.cl"
+}
+#undef MAT_ACCESS
+#undef ICLBLAS_OP_N
+#undef ICLBLAS_OP_T
+#undef ICLBLAS_OP_C
+namespace ref_cgemv {
+#include "Cgemv/Cgemv_naive.cl"
+}
+namespace ref_strsv {
+#include "Strsv/Strsv_naive.cl"
+}
+namespace ref_ctrsv {
+#include "Ctrsv/Ctrsv_naive.cl"
+}
+namespace ref_strsm {
+#include "Strsm/Strsm_naive.cl"
+}
+#undef ACCESS
+namespace ref_ctrsm {
+#include "Ctrsm/Ctrsm_naive.cl"
+}
+#undef ACCESS
+namespace ref_sgemm {
+#include "Sgemm/Sgemm_naive.cl"
+}
+namespace ref_cgemm {
+#include "Cgemm/Cgemm_naive.cl"
+}
+
+static complex_t c2(const float* p) { return complex_t(p[0], p[1]); }
+
+extern "C" {
+
+// Sgemv_naive: one work-item runs the whole product (Sgemv_naive.cpp launch of 1)
+void ref_naive_sgemv(int trans, int m, int n, float alpha, float* A, int lda, float* x, int incx, float beta,
+                     float* y, int incy)
+{
+    ref_sgemv::Sgemv_naive(trans, m, n, alpha, A, lda, x, incx, beta, y, incy);
+}
+
+// Cgemv_naive: one work-item per output element (Cgemv_naive.cpp:66)
+void ref_naive_cgemv(int trans, int m, int n, const float* alpha, float* A, int lda, float* x, int incx,
+                     const float* beta, float* y, int incy)
+{
+    size_t gws = (trans == 0) ? (size_t)m : (size_t)n;
+    clshim::run_ndrange(gws, [&] {
+        ref_cgemv::Cgemv_naive(trans, m, n, c2(alpha), (complex_t*)A, lda, (complex_t*)x, incx, c2(beta),
+                               (complex_t*)y, incy);
+    });
+}
+
+void ref_naive_strsv(int uplo, int trans, int diag, int n, const float* A, int lda, float* x, int incx)
+{
+    ref_strsv::Strsv_naive(uplo, trans, diag, n, A, lda, x, incx);
+}
+
+void ref_naive_ctrsv(int uplo, int trans, int diag, int n, float* A, int lda, float* x, int incx)
+{
+    ref_ctrsv::Ctrsv_naive(uplo, trans, diag, n, (complex_t*)A, lda, (complex_t*)x, incx);
+}
+
+void ref_naive_strsm(int side, int uplo, int trans, int diag, int m, int n, float alpha, float* A, int lda,
+                     float* B, int ldb)
+{
+    ref_strsm::Strsm_naive(side, uplo, trans, diag, m, n, alpha, A, lda, B, ldb);
+}
+
+void ref_naive_ctrsm(int side, int uplo, int trans, int diag, int m, int n, const float* alpha, float* A, int lda,
+                     float* B, int ldb)
+{
+    ref_ctrsm::Ctrsm_naive(side, uplo, trans, diag, m, n, c2(alpha), (complex_t*)A, lda, (complex_t*)B, ldb);
+}
+
+void ref_naive_sgemm(int ta, int tb, int m, int n, int k, float alpha, float* A, int lda, float* B, int ldb,
+                     float beta, float* C, int ldc)
+{
+    ref_sgemm::Sgemm_naive(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+}
+
+void ref_naive_cgemm(int ta, int tb, int m, int n, int k, const float* alpha, float* A, int lda, float* B, int ldb,
+                     const float* beta, float* C, int ldc)
+{
+    ref_cgemm::Cgemm_naive(ta, tb, m, n, k, c2(alpha), (complex_t*)A, lda, (complex_t*)B, ldb, c2(beta),
+                           (complex_t*)C, ldc);
+}
+
+}  // extern "C"
