@@ -1,0 +1,446 @@
+"""Benchmark of the iclBLAS hot path on B200.
+
+Default workload (one "step"): the bandwidth-bound level-1/2 sweep of the
+reference's bandwidth config: SAXPY, SDOT, SNRM2, SASUM, ISAMAX at n = 2^28
+(fp32, stride 1, U(-1,1), seed 1), SGEMV 16384x16384 (N and T) and CGEMV
+8192x8192 (N and C).  Metric: aggregate achieved HBM GB/s = algorithmic bytes
+of the sweep / time.  Every input (>= 512 MiB) is larger than L2 (126 MB), so
+no L2 flush is needed between steps.
+
+  value   device-resident operands, timed with CUDA events on the stream the
+          kernels run on;
+  e2e     the same sweep through the C ABI with HOST (pinned) operands: every
+          call copies its inputs in and its outputs back, as the reference's
+          API does;
+  roofline  dominant kernel's algorithmic bytes / its mean event-timed
+          duration, against the measured HBM copy bandwidth;
+  cpu_baseline  the reference's own CPU code for the same routines
+          (oracle/_ref, built from the reference's sources) on a bounded
+          sample, 1 thread.
+
+`--impl reference` times the reference's CPU implementation with every host
+thread on a bounded sample of the same workload.  Multi-GPU (torchrun): each
+rank runs an independent replica (BLAS calls do not shard), weak scaling.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+N1 = 1 << 28
+GEMV_N = 16384
+CGEMV_N = 8192
+
+
+def sweep_bytes(n1=N1, gn=GEMV_N, cn=CGEMV_N):
+    """Algorithmic bytes per call of the sweep (beta != 0 GEMV reads y)."""
+    return {
+        "saxpy": 12 * n1,
+        "sdot": 8 * n1,
+        "snrm2": 4 * n1,
+        "sasum": 4 * n1,
+        "isamax": 4 * n1,
+        "sgemv_n": 4 * (gn * gn + gn + 2 * gn),
+        "sgemv_t": 4 * (gn * gn + gn + 2 * gn),
+        "cgemv_n": 8 * (cn * cn + cn + 2 * cn),
+        "cgemv_c": 8 * (cn * cn + cn + 2 * cn),
+    }
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic():
+    """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        try:
+            return json.load(open(p))
+        except Exception:
+            return {}
+    return {}
+
+
+class Clocks:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.f = None
+
+    def __enter__(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", delete=False, suffix=".csv")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.gpu)], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None or self.f is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [c.strip() for c in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- GPU sweep
+class Sweep:
+    """Operands of the sweep on one GPU and the calls that make one step."""
+
+    def __init__(self, torch, dev, B, host: bool):
+        self.B = B
+        g = torch.Generator(device="cpu").manual_seed(1)
+
+        def mk(shape, dtype=torch.float32):
+            t = torch.rand(shape, generator=g, dtype=torch.float32) * 2 - 1
+            if dtype == torch.complex64:
+                t = torch.complex(t, torch.rand(shape, generator=g, dtype=torch.float32) * 2 - 1)
+            if host:
+                return t.pin_memory()
+            return t.to(dev)
+
+        n = N1
+        self.n = n
+        self.x = mk((n,))
+        self.y = mk((n,))
+        self.A = mk((GEMV_N * GEMV_N,))
+        self.gx = mk((GEMV_N,))
+        self.gy = mk((GEMV_N,))
+        self.CA = mk((CGEMV_N * CGEMV_N,), torch.complex64)
+        self.cx = mk((CGEMV_N,), torch.complex64)
+        self.cy = mk((CGEMV_N,), torch.complex64)
+        if host:
+            self.r = torch.zeros(1, dtype=torch.float32).pin_memory()
+            self.ri = torch.zeros(1, dtype=torch.int32).pin_memory()
+        else:
+            self.r = torch.zeros(1, dtype=torch.float32, device=dev)
+            self.ri = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.host = host
+
+    def calls(self, h):
+        """(name, thunk) for each call of one step, in order."""
+        B, n = self.B, self.n
+        gn, cn = GEMV_N, CGEMV_N
+        return [
+            ("saxpy", lambda: B.iclblasSaxpy(h, n, 0.5, self.x, 1, self.y, 1)),
+            ("sdot", lambda: B.iclblasSdot(h, n, self.x, 1, self.y, 1, self.r)),
+            ("snrm2", lambda: B.iclblasSnrm2(h, n, self.x, 1, self.r)),
+            ("sasum", lambda: B.iclblasSasum(h, n, self.x, 1, self.r)),
+            ("isamax", lambda: B.iclblasIsamax(h, n, self.x, 1, self.ri)),
+            ("sgemv_n", lambda: B.iclblasSgemv(h, 0, gn, gn, 1.0, self.A, gn, self.gx, 1, 0.5, self.gy, 1)),
+            ("sgemv_t", lambda: B.iclblasSgemv(h, 1, gn, gn, 1.0, self.A, gn, self.gx, 1, 0.5, self.gy, 1)),
+            ("cgemv_n", lambda: B.iclblasCgemv(h, 0, cn, cn, 1 + 1j, self.CA, cn, self.cx, 1, 0.5, self.cy, 1)),
+            ("cgemv_c", lambda: B.iclblasCgemv(h, 2, cn, cn, 1 + 1j, self.CA, cn, self.cx, 1, 0.5, self.cy, 1)),
+        ]
+
+    def io_bytes(self):
+        """Host<->device bytes per step of the host-operand (e2e) sweep."""
+        n, gn, cn = self.n, GEMV_N, CGEMV_N
+        h2d = 4 * (2 * n + 2 * n + n + n + n) + 2 * 4 * (gn * gn + 2 * gn) + 2 * 8 * (cn * cn + 2 * cn)
+        d2h = 4 * n + 4 + 4 + 4 + 4 + 2 * 4 * gn + 2 * 8 * cn
+        return h2d, d2h
+
+
+LAUNCHES_PER_STEP = 9  # one kernel per call (n = 2^28 is a multiple of 4: no tail launch)
+
+
+def run_ours(args, rank, world, torch):
+    from clgpu_b200 import iclblas as B
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(device=dev)
+    bytes_per = sweep_bytes()
+    step_bytes = sum(bytes_per.values())
+
+    with B.Handle() as h:
+        h.set_stream(stream)
+        sw = Sweep(torch, dev, B, host=False)
+        torch.cuda.synchronize()
+        calls = sw.calls(h)
+        with torch.cuda.stream(stream):
+            for _ in range(args.warmup):
+                for name, f in calls:
+                    B.check(f(), name)
+            torch.cuda.synchronize()
+            ev = {name: [] for name, _ in calls}
+            marks = []
+            if world > 1:
+                torch.distributed.barrier()
+            torch.cuda.synchronize()
+            start = torch.cuda.Event(enable_timing=True)
+            end = torch.cuda.Event(enable_timing=True)
+            with Clocks(dev.index) as clk:
+                start.record(stream)
+                for _ in range(args.steps):
+                    for name, f in calls:
+                        e0 = torch.cuda.Event(enable_timing=True)
+                        e1 = torch.cuda.Event(enable_timing=True)
+                        e0.record(stream)
+                        B.check(f(), name)
+                        e1.record(stream)
+                        ev[name].append((e0, e1))
+                end.record(stream)
+                torch.cuda.synchronize()
+            clocks = clk.summary()
+        total_ms = start.elapsed_time(end)
+        per_call_ms = {name: float(np.mean([a.elapsed_time(b) for a, b in ev[name]])) for name in ev}
+        del marks
+        t_max = total_ms
+        if world > 1:
+            t = torch.tensor([total_ms], device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            t_max = float(t.item())
+        value = world * step_bytes * args.steps / (t_max / 1e3) / 1e9
+
+        # dominant kernel: largest share of the step
+        dom = max(per_call_ms, key=per_call_ms.get)
+        peak, peak_kind = load_peaks()
+        achieved = bytes_per[dom] / (per_call_ms[dom] / 1e3) / 1e9
+        traffic = load_traffic().get(dom)
+
+        # e2e: host (pinned) operands through the same C ABI calls
+        del sw
+        torch.cuda.empty_cache()
+        swh = Sweep(torch, dev, B, host=True)
+        callsh = swh.calls(h)
+        for _ in range(1):
+            for name, f in callsh:
+                B.check(f(), name)
+        e2e_steps = max(1, min(args.steps, 3))
+        torch.cuda.synchronize()
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        for _ in range(e2e_steps):
+            for name, f in callsh:
+                B.check(f(), name)
+        s1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = s0.elapsed_time(s1)
+        if world > 1:
+            t = torch.tensor([e2e_ms], device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        h2d, d2h = swh.io_bytes()
+        e2e_value = world * step_bytes * e2e_steps / (e2e_ms / 1e3) / 1e9
+        del swh
+
+    out = {
+        "metric": "level-1/2 sweep aggregate HBM bandwidth (SAXPY/SDOT/SNRM2/SASUM/ISAMAX n=2^28, "
+                  "SGEMV 16384^2 N+T, CGEMV 8192^2 N+C)",
+        "value": round(value, 2),
+        "unit": "GB/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(t_max / args.steps, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "fp32",
+        "data": "synthetic U(-1,1), seed 1",
+        "config": {"workload": "bandwidth sweep: level-1 n=2^28 x5, SGEMV 16384^2 N,T, CGEMV 8192^2 N,C",
+                   "bytes_per_step": step_bytes, "l2": "inputs larger than L2 (>=512 MiB each), no flush",
+                   "parallelism": f"replicas x{world}"},
+        "per_call_ms": {k: round(v, 4) for k, v in per_call_ms.items()},
+        "per_call_gbs": {k: round(bytes_per[k] / (per_call_ms[k] / 1e3) / 1e9, 1) for k in per_call_ms},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
+                     "peak_source": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                     "traffic": traffic, "algorithmic_bytes": bytes_per[dom]},
+        "e2e": {"value": round(e2e_value, 2), "unit": "GB/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "steps": e2e_steps, "ms_per_step": round(e2e_ms / e2e_steps, 3)},
+        "gpu_launches": LAUNCHES_PER_STEP * args.steps,
+        "clocks": clocks,
+    }
+    return out
+
+
+# ---------------------------------------------------------------- CPU (reference code)
+SAMPLE_N1 = 1 << 24
+SAMPLE_GN = 4096
+SAMPLE_CN = 2048
+
+
+def cpu_sweep(threads: int, reps: int = 3):
+    """Times the reference's own CPU code (oracle/_ref/libiclref.so; the
+    oracle port if the reference was not built) on a bounded sample of the
+    sweep: level-1 at n = 2^24, SGEMV 4096^2, CGEMV 2048^2.  With threads > 1
+    every routine is split into independent chunks run concurrently (ctypes
+    releases the GIL)."""
+    import ctypes as C
+    import oracle_lib as O
+    R = O.ref()
+    kind = "reference" if R is not None else "port"
+    rng = np.random.default_rng(1)
+    n, gn, cn = SAMPLE_N1, SAMPLE_GN, SAMPLE_CN
+    x = rng.uniform(-1, 1, n).astype(np.float32)
+    y = rng.uniform(-1, 1, n).astype(np.float32)
+    A = rng.uniform(-1, 1, gn * gn).astype(np.float32)
+    gx = rng.uniform(-1, 1, gn).astype(np.float32)
+    gy = rng.uniform(-1, 1, gn).astype(np.float32)
+    CA = O.colmajor(cn, cn, cn, rng, np.complex64)
+    cx = O.colmajor(cn, 1, cn, rng, np.complex64)
+    cy = O.colmajor(cn, 1, cn, rng, np.complex64)
+    al = O.cbox(1 + 1j)
+    be = O.cbox(0.5)
+    P = lambda a, off=0: C.c_void_p(a.ctypes.data + off * a.itemsize)  # noqa: E731
+
+    def chunks(total, parts):
+        b = np.linspace(0, total, parts + 1).astype(int)
+        return [(int(b[i]), int(b[i + 1] - b[i])) for i in range(parts) if b[i + 1] > b[i]]
+
+    def par(fn, total):
+        cs = chunks(total, threads)
+        if threads == 1:
+            for o, c in cs:
+                fn(o, c)
+            return
+        ts = [threading.Thread(target=fn, args=(o, c)) for o, c in cs]
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+
+    if R is not None:
+        ops = [
+            ("saxpy", lambda o, c: R.ref_cpu_saxpy(c, 0.5, P(x, o), 1, P(y, o), 1), n),
+            ("sdot", lambda o, c: R.ref_cpu_sdot(c, P(x, o), 1, P(y, o), 1), n),
+            ("snrm2", lambda o, c: R.ref_cpu_snrm2(c, P(x, o), 1), n),
+            ("sasum", lambda o, c: R.ref_cpu_sasum(c, P(x, o), 1), n),
+            ("isamax", lambda o, c: R.ref_cpu_isamax(c, P(x, o), 1), n),
+            # rows of y for op N, columns (outputs) for op T
+            ("sgemv_n", lambda o, c: R.ref_naive_sgemv(0, c, gn, 1.0, P(A, o), gn, P(gx), 1, 0.5, P(gy, o), 1), gn),
+            ("sgemv_t", lambda o, c: R.ref_naive_sgemv(1, gn, c, 1.0, P(A, o * gn), gn, P(gx), 1, 0.5, P(gy, o), 1), gn),
+            ("cgemv_n", lambda o, c: R.ref_naive_cgemv(0, c, cn, P(al), P(CA, o), cn, P(cx), 1, P(be), P(cy, o), 1), cn),
+            ("cgemv_c", lambda o, c: R.ref_naive_cgemv(2, cn, c, P(al), P(CA, o * cn), cn, P(cx), 1, P(be), P(cy, o), 1), cn),
+        ]
+    else:
+        Lo = O.orc()
+        c32a, c32b = O.c32(1 + 1j), O.c32(0.5)
+        ops = [
+            ("saxpy", lambda o, c: Lo.orc_saxpy(c, 0.5, P(x, o), 1, P(y, o), 1), n),
+            ("sdot", lambda o, c: Lo.orc_sdot(c, P(x, o), 1, P(y, o), 1), n),
+            ("snrm2", lambda o, c: Lo.orc_snrm2(c, P(x, o), 1), n),
+            ("sasum", lambda o, c: Lo.orc_sasum(c, P(x, o), 1), n),
+            ("isamax", lambda o, c: Lo.orc_isamax(c, P(x, o), 1), n),
+            ("sgemv_n", lambda o, c: Lo.orc_sgemv(0, c, gn, 1.0, P(A, o), gn, P(gx), 1, 0.5, P(gy, o), 1), gn),
+            ("sgemv_t", lambda o, c: Lo.orc_sgemv(1, gn, c, 1.0, P(A, o * gn), gn, P(gx), 1, 0.5, P(gy, o), 1), gn),
+            ("cgemv_n", lambda o, c: Lo.orc_cgemv(0, c, cn, c32a, P(CA, o), cn, P(cx), 1, c32b, P(cy, o), 1), cn),
+            ("cgemv_c", lambda o, c: Lo.orc_cgemv(2, cn, c, c32a, P(CA, o * cn), cn, P(cx), 1, c32b, P(cy, o), 1), cn),
+        ]
+    bytes_per = sweep_bytes(n, gn, cn)
+    total_bytes = sum(bytes_per.values())
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        for name, fn, total in ops:
+            par(fn, total)
+        times.append(time.perf_counter() - t0)
+    t = float(np.median(times))
+    return {
+        "value": round(total_bytes / t / 1e9, 3), "unit": "GB/s", "cores": threads, "kind": kind,
+        "sample": f"sweep at level-1 n=2^24, SGEMV {gn}^2 N+T, CGEMV {cn}^2 N+C; median of {reps}; "
+                  f"{'reference CPU templates + serial kernels (oracle/_ref)' if kind == 'reference' else 'oracle port'}",
+        "seconds_per_step": round(t, 3),
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        threads = os.cpu_count() or 1
+        for _ in range(max(0, min(args.warmup, 1))):
+            cpu_sweep(threads, reps=1)
+        res = cpu_sweep(threads, reps=max(1, args.steps))
+        line = {
+            "metric": "level-1/2 sweep aggregate HBM bandwidth (SAXPY/SDOT/SNRM2/SASUM/ISAMAX n=2^28, "
+                      "SGEMV 16384^2 N+T, CGEMV 8192^2 N+C)",
+            "value": res["value"], "unit": "GB/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(res["seconds_per_step"] * 1e3, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+            "data": "synthetic U(-1,1), seed 1",
+            "config": {"workload": "bandwidth sweep: level-1 n=2^28 x5, SGEMV 16384^2 N,T, CGEMV 8192^2 N,C",
+                       "sample": res["sample"]},
+            "impl": "reference",
+            "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": res["value"], "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line))
+        return
+
+    import torch
+    if world > 1:
+        torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    out = run_ours(args, rank, world, torch)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = {k: v for k, v in cpu_sweep(1, reps=3).items() if k != "seconds_per_step"}
+    if rank == 0:
+        print(json.dumps(out))
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

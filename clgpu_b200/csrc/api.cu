@@ -1,0 +1,767 @@
+// C-ABI layer of the B200 iclBLAS library.
+//
+// Replaces the reference's C API implementation (libs/blas/shlib/iclBLAS.cpp,
+// iclBLAS_S.cpp, iclBLAS_C.cpp, iclBLASImpl.hpp) and the OpenCL engine under
+// it (core/src/ocl/*): a handle owns a CUDA stream and a device workspace,
+// each routine validates its arguments with the reference's rules, moves
+// host-resident operands to the device (the reference wraps host arrays in
+// OpenCL buffers per call, core/src/ocl/ocl_buffer.cpp:27-58, and reads the
+// outputs back before returning, ocl_kernel.cpp:86-92), and launches the
+// routine's sm_100a kernels directly (no scored implementation selection, no
+// JIT).  Exceptions never cross the ABI, in every build type.
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <stdexcept>
+
+#include "internal.h"
+
+using iclb::cfloat;
+
+namespace {
+
+iclblasStatus_t map_cuda(cudaError_t e)
+{
+    if (e == cudaSuccess) return ICLBLAS_STATUS_SUCCESS;
+    if (e == cudaErrorMemoryAllocation) return ICLBLAS_STATUS_ALLOC_FAILED;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return ICLBLAS_STATUS_NOT_INITIALIZED;
+    if (e == cudaErrorNoKernelImageForDevice || e == cudaErrorInvalidDeviceFunction) return ICLBLAS_STATUS_ARCH_MISMATCH;
+    return ICLBLAS_STATUS_EXECUTION_FAILED;
+}
+
+bool handle_ok(iclblasHandle_t h) { return h != nullptr && h->tag == iclb::kHandleTag; }
+
+// Argument checks in the reference's order (libs/blas/shlib/iclBLASImpl.hpp:
+// validate_params :218-233, then the handle :236-245).  Only the fields
+// flagged in `present` exist for a routine.
+enum : unsigned {
+    P_N = 1u << 0, P_M = 1u << 1, P_K = 1u << 2, P_X = 1u << 3, P_INCX = 1u << 4, P_Y = 1u << 5,
+    P_INCY = 1u << 6, P_A = 1u << 7, P_LDA = 1u << 8, P_B = 1u << 9, P_LDB = 1u << 10, P_C = 1u << 11,
+    P_LDC = 1u << 12
+};
+struct Params {
+    unsigned present = 0;
+    int n = 0, m = 0, k = 0, incx = 0, incy = 0, lda = 0, ldb = 0, ldc = 0;
+    const void *x = nullptr, *y = nullptr, *A = nullptr, *B = nullptr, *C = nullptr;
+};
+// Returns -1 to end the call successfully without work, 0 to run, or a status.
+int validate(const Params& p, iclblasHandle_t h)
+{
+    const unsigned f = p.present;
+    if (f & P_N) { if (p.n < 0) return ICLBLAS_STATUS_INVALID_VALUE; if (p.n == 0) return -1; }
+    if (f & P_M) { if (p.m < 0) return ICLBLAS_STATUS_INVALID_VALUE; if (p.m == 0) return -1; }
+    if ((f & P_K) && p.k < 0) return ICLBLAS_STATUS_INVALID_VALUE;
+    if ((f & P_X) && !p.x) return ICLBLAS_STATUS_INVALID_VALUE;
+    if (f & P_INCX) { if (p.incx == 0) return ICLBLAS_STATUS_INVALID_VALUE; if (p.incx < 0) return ICLBLAS_STATUS_NOT_SUPPORTED; }
+    if ((f & P_Y) && !p.y) return ICLBLAS_STATUS_INVALID_VALUE;
+    if (f & P_INCY) { if (p.incy == 0) return ICLBLAS_STATUS_INVALID_VALUE; if (p.incy < 0) return ICLBLAS_STATUS_NOT_SUPPORTED; }
+    if ((f & P_A) && !p.A) return ICLBLAS_STATUS_INVALID_VALUE;
+    if ((f & P_LDA) && p.lda <= 0) return ICLBLAS_STATUS_INVALID_VALUE;
+    if ((f & P_B) && !p.B) return ICLBLAS_STATUS_INVALID_VALUE;
+    if ((f & P_LDB) && p.ldb <= 0) return ICLBLAS_STATUS_INVALID_VALUE;
+    if ((f & P_C) && !p.C) return ICLBLAS_STATUS_INVALID_VALUE;
+    if ((f & P_LDC) && p.ldc <= 0) return ICLBLAS_STATUS_INVALID_VALUE;
+    if (!handle_ok(h)) return ICLBLAS_STATUS_INVALID_VALUE;
+    return 0;
+}
+
+#define VALIDATE(p, h)                                                          \
+    do {                                                                        \
+        int v_ = validate((p), (h));                                            \
+        if (v_ < 0) return ICLBLAS_STATUS_SUCCESS;                              \
+        if (v_ > 0) return (iclblasStatus_t)v_;                                 \
+    } while (0)
+
+// Can the device dereference `p` directly?
+bool is_device_ptr(const void* p)
+{
+    cudaPointerAttributes a;
+    cudaError_t e = cudaPointerGetAttributes(&a, p);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+size_t vec_extent(int n, int inc) { return n > 0 ? (size_t)(n - 1) * (size_t)inc + 1 : 0; }
+size_t mat_extent(int rows, int cols, int ld)
+{
+    return (rows > 0 && cols > 0) ? (size_t)(cols - 1) * (size_t)ld + (size_t)rows : 0;
+}
+
+// Moves host-resident operands through a device staging area.  Device
+// operands pass through untouched.  When anything was staged, finish()
+// copies outputs back and waits, which gives host callers the reference's
+// blocking semantics; all-device calls stay asynchronous.
+class Stager {
+public:
+    explicit Stager(iclblasHandle_t h) : h_(h) {}
+
+    int add(const void* p, size_t bytes, bool out)
+    {
+        Op& o = ops_[n_];
+        o.user = const_cast<void*>(p);
+        o.bytes = bytes;
+        o.out = out;
+        o.staged = !is_device_ptr(p);
+        o.dev = o.staged ? nullptr : o.user;
+        return n_++;
+    }
+
+    cudaError_t stage_in()
+    {
+        size_t total = 0;
+        for (int i = 0; i < n_; ++i)
+            if (ops_[i].staged) total += (ops_[i].bytes + 255) & ~(size_t)255;
+        if (total == 0) return cudaSuccess;
+        if (total > h_->stage_bytes) {
+            if (h_->stage) cudaFree(h_->stage);
+            h_->stage = nullptr;
+            h_->stage_bytes = 0;
+            cudaError_t e = cudaMalloc(&h_->stage, total);
+            if (e != cudaSuccess) return e;
+            h_->stage_bytes = total;
+        }
+        char* base = (char*)h_->stage;
+        size_t off = 0;
+        for (int i = 0; i < n_; ++i) {
+            Op& o = ops_[i];
+            if (!o.staged) continue;
+            o.dev = base + off;
+            off += (o.bytes + 255) & ~(size_t)255;
+            cudaError_t e = cudaMemcpyAsync(o.dev, o.user, o.bytes, cudaMemcpyHostToDevice, h_->stream);
+            if (e != cudaSuccess) return e;
+            any_staged_ = true;
+        }
+        return cudaSuccess;
+    }
+
+    template <class T>
+    T* dev(int i) const { return (T*)ops_[i].dev; }
+
+    // True when the call blocks (some operand lives in host memory).
+    bool blocking() const { return any_staged_; }
+
+    cudaError_t finish()
+    {
+        if (!any_staged_) return cudaGetLastError();
+        for (int i = 0; i < n_; ++i) {
+            const Op& o = ops_[i];
+            if (o.staged && o.out) {
+                cudaError_t e = cudaMemcpyAsync(o.user, o.dev, o.bytes, cudaMemcpyDeviceToHost, h_->stream);
+                if (e != cudaSuccess) return e;
+            }
+        }
+        return cudaStreamSynchronize(h_->stream);
+    }
+
+private:
+    struct Op {
+        void* user;
+        void* dev;
+        size_t bytes;
+        bool out, staged;
+    };
+    iclblasHandle_t h_;
+    Op ops_[6];
+    int n_ = 0;
+    bool any_staged_ = false;
+};
+
+// Reads a device status word after a blocking call (kernels with bounded
+// waits record a timeout there instead of trapping).
+iclblasStatus_t check_device_status(iclblasHandle_t h)
+{
+    int st = 0;
+    cudaError_t e = cudaMemcpyAsync(&st, h->ws.dev_status, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return map_cuda(e);
+    if (st != iclb::kDevOk) {
+        cudaMemsetAsync(h->ws.dev_status, 0, sizeof(int), h->stream);
+        return ICLBLAS_STATUS_EXECUTION_FAILED;
+    }
+    return ICLBLAS_STATUS_SUCCESS;
+}
+
+// Writes a zero result for the early-return rules that run before handle
+// validation (iclBLAS_S.cpp Snrm2/Sasum/Isamax, iclBLAS_C.cpp Cdotu/Cdotc/
+// Scnrm2/Icamax); a device result is cleared in stream order.
+void zero_result(iclblasHandle_t h, void* result, size_t bytes)
+{
+    if (!result) return;
+    if (is_device_ptr(result)) {
+        if (handle_ok(h)) cudaMemsetAsync(result, 0, bytes, h->stream);
+        else cudaMemset(result, 0, bytes);
+    } else {
+        std::memset(result, 0, bytes);
+    }
+}
+
+template <class F>
+iclblasStatus_t guarded(F&& f)
+{
+    try {
+        return f();
+    } catch (const std::bad_alloc&) {
+        return ICLBLAS_STATUS_ALLOC_FAILED;
+    } catch (const std::invalid_argument&) {
+        return ICLBLAS_STATUS_INVALID_VALUE;
+    } catch (...) {
+        return ICLBLAS_STATUS_ERROR;
+    }
+}
+
+cfloat cf(const oclComplex_t* p)
+{
+    const float* f = reinterpret_cast<const float*>(p);
+    return cfloat{f[0], f[1]};
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------
+// workspace
+// ------------------------------------------------------------------------
+void* iclb::scratch(iclblasHandle_t h, size_t bytes)
+{
+    bytes = (bytes + 255) & ~(size_t)255;
+    if (bytes <= h->ws.scratch_bytes) return h->ws.scratch;
+    // The stream may still be using the old buffer: cudaFree synchronises.
+    if (h->ws.scratch) cudaFree(h->ws.scratch);
+    h->ws.scratch = nullptr;
+    h->ws.scratch_bytes = 0;
+    size_t want = bytes < ((size_t)1 << 20) ? ((size_t)1 << 20) : bytes;
+    if (cudaMalloc(&h->ws.scratch, want) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    h->ws.scratch_bytes = want;
+    return h->ws.scratch;
+}
+
+// ------------------------------------------------------------------------
+// utilities (iclBLAS.cpp:42-59)
+// ------------------------------------------------------------------------
+extern "C" iclblasStatus_t iclblasCreate(iclblasHandle_t* handle)
+{
+    if (!handle) return ICLBLAS_STATUS_INVALID_VALUE;
+    return guarded([&]() -> iclblasStatus_t {
+        iclblasContext* c = new iclblasContext();
+        cudaError_t e = cudaGetDevice(&c->device);
+        int sms = 0;
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaMalloc(&c->ws.counters, sizeof(unsigned) * iclb::kCounterWords);
+        if (e == cudaSuccess) e = cudaMalloc(&c->ws.dev_status, sizeof(int));
+        if (e == cudaSuccess) e = cudaMemsetAsync(c->ws.counters, 0, sizeof(unsigned) * iclb::kCounterWords, c->own_stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(c->ws.dev_status, 0, sizeof(int), c->own_stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->own_stream);
+        if (e != cudaSuccess) {
+            if (c->ws.counters) cudaFree(c->ws.counters);
+            if (c->ws.dev_status) cudaFree(c->ws.dev_status);
+            if (c->own_stream) cudaStreamDestroy(c->own_stream);
+            delete c;
+            cudaGetLastError();
+            return map_cuda(e);
+        }
+        c->sm_count = sms > 0 ? sms : 148;
+        c->stream = c->own_stream;
+        c->tag = iclb::kHandleTag;
+        *handle = c;
+        return ICLBLAS_STATUS_SUCCESS;
+    });
+}
+
+extern "C" iclblasStatus_t iclblasDestroy(iclblasHandle_t handle)
+{
+    // The reference throws out of this extern "C" function on a bad handle
+    // (iclBLAS.cpp:54-59 with iclBLAS.cpp:35-39); here it is a status.
+    if (!handle_ok(handle)) return ICLBLAS_STATUS_INVALID_VALUE;
+    return guarded([&]() -> iclblasStatus_t {
+        cudaStreamSynchronize(handle->stream);
+        if (handle->stage) cudaFree(handle->stage);
+        if (handle->ws.scratch) cudaFree(handle->ws.scratch);
+        cudaFree(handle->ws.counters);
+        cudaFree(handle->ws.dev_status);
+        cudaStreamDestroy(handle->own_stream);
+        handle->tag = 0;
+        delete handle;
+        return ICLBLAS_STATUS_SUCCESS;
+    });
+}
+
+extern "C" iclblasStatus_t iclblasSetStream(iclblasHandle_t h, void* stream)
+{
+    if (!handle_ok(h)) return ICLBLAS_STATUS_INVALID_VALUE;
+    h->stream = (cudaStream_t)stream;  // NULL: the legacy default stream
+    return ICLBLAS_STATUS_SUCCESS;
+}
+
+extern "C" iclblasStatus_t iclblasGetStream(iclblasHandle_t h, void** stream)
+{
+    if (!handle_ok(h) || !stream) return ICLBLAS_STATUS_INVALID_VALUE;
+    *stream = (void*)h->stream;
+    return ICLBLAS_STATUS_SUCCESS;
+}
+
+extern "C" iclblasStatus_t iclblasSetMathMode(iclblasHandle_t h, iclblasMathMode_t mode)
+{
+    if (!handle_ok(h)) return ICLBLAS_STATUS_INVALID_VALUE;
+    if (mode < ICLBLAS_MATH_PLAIN_FP32 || mode > ICLBLAS_MATH_BF16X6) return ICLBLAS_STATUS_INVALID_VALUE;
+    h->math = mode;
+    return ICLBLAS_STATUS_SUCCESS;
+}
+
+extern "C" iclblasStatus_t iclblasGetMathMode(iclblasHandle_t h, iclblasMathMode_t* mode)
+{
+    if (!handle_ok(h) || !mode) return ICLBLAS_STATUS_INVALID_VALUE;
+    *mode = h->math;
+    return ICLBLAS_STATUS_SUCCESS;
+}
+
+extern "C" iclblasStatus_t iclblasSynchronize(iclblasHandle_t h)
+{
+    if (!handle_ok(h)) return ICLBLAS_STATUS_INVALID_VALUE;
+    return guarded([&]() -> iclblasStatus_t {
+        cudaError_t e = cudaStreamSynchronize(h->stream);
+        if (e != cudaSuccess) return map_cuda(e);
+        return check_device_status(h);
+    });
+}
+
+// ------------------------------------------------------------------------
+// level 1, single (iclBLAS_S.cpp:50-211)
+// ------------------------------------------------------------------------
+extern "C" iclblasStatus_t iclblasSscal(iclblasHandle_t h, int n, const float* alpha, float* x, int incx)
+{
+    return guarded([&]() -> iclblasStatus_t {
+        Params p; p.present = P_N | P_X | P_INCX; p.n = n; p.x = x; p.incx = incx;
+        VALIDATE(p, h);
+        if (!alpha) return ICLBLAS_STATUS_INVALID_VALUE;
+        Stager st(h);
+        int ix = st.add(x, vec_extent(n, incx) * sizeof(float), true);
+        cudaError_t e = st.stage_in();
+        if (e == cudaSuccess) e = iclb::sscal(h, n, *alpha, st.dev<float>(ix), incx);
+        if (e == cudaSuccess) e = st.finish();
+        return map_cuda(e);
+    });
+}
+
+extern "C" iclblasStatus_t iclblasSaxpy(iclblasHandle_t h, int n, const float* alpha, float* x, int incx, float* y, int incy)
+{
+    if (n <= 0 || (alpha && *alpha == 0.f)) return ICLBLAS_STATUS_SUCCESS;
+    return guarded([&]() -> iclblasStatus_t {
+        Params p; p.present = P_N | P_X | P_INCX | P_Y | P_INCY;
+        p.n = n; p.x = x; p.incx = incx; p.y = y; p.incy = incy;
+        VALIDATE(p, h);
+        if (!alpha) return ICLBLAS_STATUS_INVALID_VALUE;
+        Stager st(h);
+        int ix = st.add(x, vec_extent(n, incx) * sizeof(float), false);
+        int iy = st.add(y, vec_extent(n, incy) * sizeof(float), true);
+        cudaError_t e = st.stage_in();
+        if (e == cudaSuccess) e = iclb::saxpy(h, n, *alpha, st.dev<float>(ix), incx, st.dev<float>(iy), incy);
+        if (e == cudaSuccess) e = st.finish();
+        return map_cuda(e);
+    });
+}
+
+namespace {
+iclblasStatus_t sreduce_call(iclblasHandle_t h, iclb::Red op, int n, float* x, int incx, float* y, int incy,
+                             float* result)
+{
+    return guarded([&]() -> iclblasStatus_t {
+        Params p;
+        p.present = P_N | P_X | P_INCX;
+        p.n = n; p.x = x; p.incx = incx;
+        if (op == iclb::Red::Dot) { p.present |= P_Y | P_INCY; p.y = y; p.incy = incy; }
+        VALIDATE(p, h);
+        if (!result) return ICLBLAS_STATUS_INVALID_VALUE;
+        Stager st(h);
+        int ix = st.add(x, vec_extent(n, incx) * sizeof(float), false);
+        int iy = (op == iclb::Red::Dot) ? st.add(y, vec_extent(n, incy) * sizeof(float), false) : -1;
+        int ir = st.add(result, sizeof(float), true);
+        cudaError_t e = st.stage_in();
+        if (e == cudaSuccess)
+            e = iclb::sreduce(h, op, n, st.dev<float>(ix), incx, iy >= 0 ? st.dev<float>(iy) : nullptr, incy,
+                              st.dev<float>(ir));
+        if (e == cudaSuccess) e = st.finish();
+        return map_cuda(e);
+    });
+}
+}  // namespace
+
+extern "C" iclblasStatus_t iclblasSnrm2(iclblasHandle_t h, int n, float* x, int incx, float* result)
+{
+    if (n <= 0 || incx <= 0) { zero_result(h, result, sizeof(float)); return ICLBLAS_STATUS_SUCCESS; }
+    return sreduce_call(h, iclb::Red::Nrm2, n, x, incx, nullptr, 0, result);
+}
+
+extern "C" iclblasStatus_t iclblasSasum(iclblasHandle_t h, int n, float* x, int incx, float* result)
+{
+    if (n <= 0 || incx <= 0) { zero_result(h, result, sizeof(float)); return ICLBLAS_STATUS_SUCCESS; }
+    return sreduce_call(h, iclb::Red::Asum, n, x, incx, nullptr, 0, result);
+}
+
+extern "C" iclblasStatus_t iclblasSdot(iclblasHandle_t h, int n, float* x, int incx, float* y, int incy, float* result)
+{
+    if (n <= 0) return ICLBLAS_STATUS_SUCCESS;  // result untouched (iclBLAS_S.cpp:204-205)
+    return sreduce_call(h, iclb::Red::Dot, n, x, incx, y, incy, result);
+}
+
+extern "C" iclblasStatus_t iclblasIsamax(iclblasHandle_t h, int n, float* x, int incx, int* result)
+{
+    if (n <= 0 || incx <= 0) { zero_result(h, result, sizeof(int)); return ICLBLAS_STATUS_SUCCESS; }
+    return guarded([&]() -> iclblasStatus_t {
+        Params p; p.present = P_N | P_X | P_INCX; p.n = n; p.x = x; p.incx = incx;
+        VALIDATE(p, h);
+        if (!result) return ICLBLAS_STATUS_INVALID_VALUE;
+        Stager st(h);
+        int ix = st.add(x, vec_extent(n, incx) * sizeof(float), false);
+        int ir = st.add(result, sizeof(int), true);
+        cudaError_t e = st.stage_in();
+        if (e == cudaSuccess) e = iclb::isamax(h, n, st.dev<float>(ix), incx, st.dev<int>(ir));
+        if (e == cudaSuccess) e = st.finish();
+        return map_cuda(e);
+    });
+}
+
+// ------------------------------------------------------------------------
+// level 1, complex (iclBLAS_C.cpp:69-307)
+// ------------------------------------------------------------------------
+namespace {
+iclblasStatus_t cscal_call(iclblasHandle_t h, int n, cfloat alpha, oclComplex_t* x, int incx)
+{
+    return guarded([&]() -> iclblasStatus_t {
+        Params p; p.present = P_N | P_X | P_INCX; p.n = n; p.x = x; p.incx = incx;
+        VALIDATE(p, h);
+        Stager st(h);
+        int ix = st.add(x, vec_extent(n, incx) * sizeof(cfloat), true);
+        cudaError_t e = st.stage_in();
+        if (e == cudaSuccess) e = iclb::cscal(h, n, alpha, st.dev<cfloat>(ix), incx);
+        if (e == cudaSuccess) e = st.finish();
+        return map_cuda(e);
+    });
+}
+}  // namespace
+
+extern "C" iclblasStatus_t iclblasCscal(iclblasHandle_t h, int n, const oclComplex_t* alpha, oclComplex_t* x, int incx)
+{
+    if (!alpha) return ICLBLAS_STATUS_INVALID_VALUE;
+    return cscal_call(h, n, cf(alpha), x, incx);
+}
+
+extern "C" iclblasStatus_t iclblasCsscal(iclblasHandle_t h, int n, const float* alpha, oclComplex_t* x, int incx)
+{
+    // Cscal with alpha = (a, 0) (iclBLAS_C.cpp:78-84)
+    if (!alpha) return ICLBLAS_STATUS_INVALID_VALUE;
+    return cscal_call(h, n, cfloat{*alpha, 0.f}, x, incx);
+}
+
+extern "C" iclblasStatus_t iclblasCaxpy(iclblasHandle_t h, int n, const oclComplex_t* alpha, oclComplex_t* x, int incx,
+                                        oclComplex_t* y, int incy)
+{
+    if (!alpha) return ICLBLAS_STATUS_INVALID_VALUE;
+    cfloat a = cf(alpha);
+    if (n <= 0 || (a.re == 0.f && a.im == 0.f)) return ICLBLAS_STATUS_SUCCESS;
+    return guarded([&]() -> iclblasStatus_t {
+        Params p; p.present = P_N | P_X | P_INCX | P_Y | P_INCY;
+        p.n = n; p.x = x; p.incx = incx; p.y = y; p.incy = incy;
+        VALIDATE(p, h);
+        Stager st(h);
+        int ix = st.add(x, vec_extent(n, incx) * sizeof(cfloat), false);
+        int iy = st.add(y, vec_extent(n, incy) * sizeof(cfloat), true);
+        cudaError_t e = st.stage_in();
+        if (e == cudaSuccess) e = iclb::caxpy(h, n, a, st.dev<cfloat>(ix), incx, st.dev<cfloat>(iy), incy);
+        if (e == cudaSuccess) e = st.finish();
+        return map_cuda(e);
+    });
+}
+
+namespace {
+iclblasStatus_t cdot_call(iclblasHandle_t h, bool conj, int n, oclComplex_t* x, int incx, oclComplex_t* y, int incy,
+                          oclComplex_t* result)
+{
+    if (n <= 0) { zero_result(h, result, sizeof(cfloat)); return ICLBLAS_STATUS_SUCCESS; }
+    return guarded([&]() -> iclblasStatus_t {
+        Params p; p.present = P_N | P_X | P_INCX | P_Y | P_INCY;
+        p.n = n; p.x = x; p.incx = incx; p.y = y; p.incy = incy;
+        VALIDATE(p, h);
+        if (!result) return ICLBLAS_STATUS_INVALID_VALUE;
+        Stager st(h);
+        int ix = st.add(x, vec_extent(n, incx) * sizeof(cfloat), false);
+        int iy = st.add(y, vec_extent(n, incy) * sizeof(cfloat), false);
+        int ir = st.add(result, sizeof(cfloat), true);
+        cudaError_t e = st.stage_in();
+        if (e == cudaSuccess)
+            e = iclb::cdot(h, conj, n, st.dev<cfloat>(ix), incx, st.dev<cfloat>(iy), incy, st.dev<cfloat>(ir));
+        if (e == cudaSuccess) e = st.finish();
+        return map_cuda(e);
+    });
+}
+
+iclblasStatus_t creduce_call(iclblasHandle_t h, iclb::Red op, int n, oclComplex_t* x, int incx, float* result)
+{
+    return guarded([&]() -> iclblasStatus_t {
+        Params p; p.present = P_N | P_X | P_INCX; p.n = n; p.x = x; p.incx = incx;
+        VALIDATE(p, h);
+        if (!result) return ICLBLAS_STATUS_INVALID_VALUE;
+        Stager st(h);
+        int ix = st.add(x, vec_extent(n, incx) * sizeof(cfloat), false);
+        int ir = st.add(result, sizeof(float), true);
+        cudaError_t e = st.stage_in();
+        if (e == cudaSuccess) e = iclb::creduce_real(h, op, n, st.dev<cfloat>(ix), incx, st.dev<float>(ir));
+        if (e == cudaSuccess) e = st.finish();
+        return map_cuda(e);
+    });
+}
+}  // namespace
+
+extern "C" iclblasStatus_t iclblasCdotu(iclblasHandle_t h, int n, oclComplex_t* x, int incx, oclComplex_t* y, int incy,
+                                        oclComplex_t* result)
+{
+    return cdot_call(h, false, n, x, incx, y, incy, result);
+}
+
+extern "C" iclblasStatus_t iclblasCdotc(iclblasHandle_t h, int n, oclComplex_t* x, int incx, oclComplex_t* y, int incy,
+                                        oclComplex_t* result)
+{
+    return cdot_call(h, true, n, x, incx, y, incy, result);
+}
+
+extern "C" iclblasStatus_t iclblasScnrm2(iclblasHandle_t h, int n, oclComplex_t* x, int incx, float* result)
+{
+    if (n <= 0 || incx <= 0) { zero_result(h, result, sizeof(float)); return ICLBLAS_STATUS_SUCCESS; }
+    return creduce_call(h, iclb::Red::Nrm2, n, x, incx, result);
+}
+
+extern "C" iclblasStatus_t iclblasScasum(iclblasHandle_t h, int n, oclComplex_t* x, int incx, float* result)
+{
+    // No early return in the reference (iclBLAS_C.cpp:112-118): n == 0
+    // succeeds without writing result.
+    return creduce_call(h, iclb::Red::Asum, n, x, incx, result);
+}
+
+extern "C" iclblasStatus_t iclblasIcamax(iclblasHandle_t h, int n, oclComplex_t* x, int incx, int* result)
+{
+    if (n <= 0 || incx <= 0) { zero_result(h, result, sizeof(int)); return ICLBLAS_STATUS_SUCCESS; }
+    return guarded([&]() -> iclblasStatus_t {
+        Params p; p.present = P_N | P_X | P_INCX; p.n = n; p.x = x; p.incx = incx;
+        VALIDATE(p, h);
+        if (!result) return ICLBLAS_STATUS_INVALID_VALUE;
+        Stager st(h);
+        int ix = st.add(x, vec_extent(n, incx) * sizeof(cfloat), false);
+        int ir = st.add(result, sizeof(int), true);
+        cudaError_t e = st.stage_in();
+        if (e == cudaSuccess) e = iclb::icamax(h, n, st.dev<cfloat>(ix), incx, st.dev<int>(ir));
+        if (e == cudaSuccess) e = st.finish();
+        return map_cuda(e);
+    });
+}
+
+// ------------------------------------------------------------------------
+// level 2
+// ------------------------------------------------------------------------
+extern "C" iclblasStatus_t iclblasSgemv(iclblasHandle_t h, iclblasOperation_t trans, int m, int n, const float* alpha,
+                                        float* A, int lda, float* x, int incx, const float* beta, float* y, int incy)
+{
+    if (!alpha || !beta) return ICLBLAS_STATUS_INVALID_VALUE;
+    // iclBLAS_S.cpp:450-455
+    if (m == 0 || n == 0 || (*alpha == 0.f && *beta == 1.f)) return ICLBLAS_STATUS_SUCCESS;
+    if (m < 0 || n < 0 || incx == 0 || incy == 0) return ICLBLAS_STATUS_INVALID_VALUE;
+    return guarded([&]() -> iclblasStatus_t {
+        Params p; p.present = P_N | P_M | P_A | P_LDA | P_X | P_INCX | P_Y | P_INCY;
+        p.n = n; p.m = m; p.A = A; p.lda = lda; p.x = x; p.incx = incx; p.y = y; p.incy = incy;
+        VALIDATE(p, h);
+        if (trans < ICLBLAS_OP_N || trans > ICLBLAS_OP_C) return ICLBLAS_STATUS_INVALID_VALUE;
+        const int xl = trans == ICLBLAS_OP_N ? n : m, yl = trans == ICLBLAS_OP_N ? m : n;
+        Stager st(h);
+        int ia = st.add(A, mat_extent(m, n, lda) * sizeof(float), false);
+        int ix = st.add(x, vec_extent(xl, incx) * sizeof(float), false);
+        int iy = st.add(y, vec_extent(yl, incy) * sizeof(float), true);
+        cudaError_t e = st.stage_in();
+        if (e == cudaSuccess)
+            e = iclb::sgemv(h, trans, m, n, *alpha, st.dev<float>(ia), lda, st.dev<float>(ix), incx, *beta,
+                            st.dev<float>(iy), incy);
+        if (e == cudaSuccess) e = st.finish();
+        return map_cuda(e);
+    });
+}
+
+extern "C" iclblasStatus_t iclblasCgemv(iclblasHandle_t h, iclblasOperation_t trans, int m, int n,
+                                        const oclComplex_t* alpha, oclComplex_t* A, int lda, oclComplex_t* x, int incx,
+                                        const oclComplex_t* beta, oclComplex_t* y, int incy)
+{
+    if (!alpha || !beta) return ICLBLAS_STATUS_INVALID_VALUE;
+    const cfloat a = cf(alpha), b = cf(beta);
+    // iclBLAS_C.cpp:236-243
+    if (m == 0 || n == 0 || (a.re == 0.f && a.im == 0.f && b.re == 1.f && b.im == 0.f)) return ICLBLAS_STATUS_SUCCESS;
+    if (m < 0 || n < 0 || incx == 0 || incy == 0) return ICLBLAS_STATUS_INVALID_VALUE;
+    return guarded([&]() -> iclblasStatus_t {
+        Params p; p.present = P_N | P_M | P_A | P_LDA | P_X | P_INCX | P_Y | P_INCY;
+        p.n = n; p.m = m; p.A = A; p.lda = lda; p.x = x; p.incx = incx; p.y = y; p.incy = incy;
+        VALIDATE(p, h);
+        if (trans < ICLBLAS_OP_N || trans > ICLBLAS_OP_C) return ICLBLAS_STATUS_INVALID_VALUE;
+        const int xl = trans == ICLBLAS_OP_N ? n : m, yl = trans == ICLBLAS_OP_N ? m : n;
+        Stager st(h);
+        int ia = st.add(A, mat_extent(m, n, lda) * sizeof(cfloat), false);
+        int ix = st.add(x, vec_extent(xl, incx) * sizeof(cfloat), false);
+        int iy = st.add(y, vec_extent(yl, incy) * sizeof(cfloat), true);
+        cudaError_t e = st.stage_in();
+        if (e == cudaSuccess)
+            e = iclb::cgemv(h, trans, m, n, a, st.dev<cfloat>(ia), lda, st.dev<cfloat>(ix), incx, b,
+                            st.dev<cfloat>(iy), incy);
+        if (e == cudaSuccess) e = st.finish();
+        return map_cuda(e);
+    });
+}
+
+extern "C" iclblasStatus_t iclblasStrsv(iclblasHandle_t h, iclblasFillMode_t uplo, iclblasOperation_t trans,
+                                        iclblasDiagType_t diag, int n, float* A, int lda, float* x, int incx)
+{
+    // iclBLAS_S.cpp:223-226
+    if (n == 0) return ICLBLAS_STATUS_SUCCESS;
+    if (n < 0 || incx == 0) return ICLBLAS_STATUS_INVALID_VALUE;
+    return guarded([&]() -> iclblasStatus_t {
+        Params p; p.present = P_N | P_A | P_LDA | P_X | P_INCX;
+        p.n = n; p.A = A; p.lda = lda; p.x = x; p.incx = incx;
+        VALIDATE(p, h);
+        if (trans < ICLBLAS_OP_N || trans > ICLBLAS_OP_C) return ICLBLAS_STATUS_INVALID_VALUE;
+        Stager st(h);
+        int ia = st.add(A, mat_extent(n, n, lda) * sizeof(float), false);
+        int ix = st.add(x, vec_extent(n, incx) * sizeof(float), true);
+        cudaError_t e = st.stage_in();
+        if (e == cudaSuccess) e = iclb::strsv(h, uplo, trans, diag, n, st.dev<float>(ia), lda, st.dev<float>(ix), incx);
+        if (e == cudaSuccess) e = st.finish();
+        if (e != cudaSuccess) return map_cuda(e);
+        // device-pointer calls stay asynchronous: iclblasSynchronize reports
+        return st.blocking() ? check_device_status(h) : ICLBLAS_STATUS_SUCCESS;
+    });
+}
+
+extern "C" iclblasStatus_t iclblasCtrsv(iclblasHandle_t h, iclblasFillMode_t uplo, iclblasOperation_t trans,
+                                        iclblasDiagType_t diag, int n, oclComplex_t* A, int lda, oclComplex_t* x,
+                                        int incx)
+{
+    if (n == 0) return ICLBLAS_STATUS_SUCCESS;
+    if (n < 0 || incx == 0) return ICLBLAS_STATUS_INVALID_VALUE;
+    return guarded([&]() -> iclblasStatus_t {
+        Params p; p.present = P_N | P_A | P_LDA | P_X | P_INCX;
+        p.n = n; p.A = A; p.lda = lda; p.x = x; p.incx = incx;
+        VALIDATE(p, h);
+        if (trans < ICLBLAS_OP_N || trans > ICLBLAS_OP_C) return ICLBLAS_STATUS_INVALID_VALUE;
+        Stager st(h);
+        int ia = st.add(A, mat_extent(n, n, lda) * sizeof(cfloat), false);
+        int ix = st.add(x, vec_extent(n, incx) * sizeof(cfloat), true);
+        cudaError_t e = st.stage_in();
+        if (e == cudaSuccess)
+            e = iclb::ctrsv(h, uplo, trans, diag, n, st.dev<cfloat>(ia), lda, st.dev<cfloat>(ix), incx);
+        if (e == cudaSuccess) e = st.finish();
+        if (e != cudaSuccess) return map_cuda(e);
+        return st.blocking() ? check_device_status(h) : ICLBLAS_STATUS_SUCCESS;
+    });
+}
+
+// ------------------------------------------------------------------------
+// level 3
+// ------------------------------------------------------------------------
+extern "C" iclblasStatus_t iclblasSgemm(iclblasHandle_t h, iclblasOperation_t transa, iclblasOperation_t transb, int m,
+                                        int n, int k, const float* alpha, float* A, int lda, float* B, int ldb,
+                                        const float* beta, float* C, int ldc)
+{
+    if (m < 0 || n < 0 || k < 0) return ICLBLAS_STATUS_INVALID_VALUE;  // iclBLAS_S.cpp:465-466
+    return guarded([&]() -> iclblasStatus_t {
+        Params p; p.present = P_N | P_M | P_K | P_A | P_LDA | P_B | P_LDB | P_C | P_LDC;
+        p.n = n; p.m = m; p.k = k; p.A = A; p.lda = lda; p.B = B; p.ldb = ldb; p.C = C; p.ldc = ldc;
+        VALIDATE(p, h);
+        if (!alpha || !beta) return ICLBLAS_STATUS_INVALID_VALUE;
+        if (transa < ICLBLAS_OP_N || transa > ICLBLAS_OP_C || transb < ICLBLAS_OP_N || transb > ICLBLAS_OP_C)
+            return ICLBLAS_STATUS_INVALID_VALUE;
+        const int ar = transa == ICLBLAS_OP_N ? m : k, ac = transa == ICLBLAS_OP_N ? k : m;
+        const int br = transb == ICLBLAS_OP_N ? k : n, bc = transb == ICLBLAS_OP_N ? n : k;
+        Stager st(h);
+        int ia = st.add(A, mat_extent(ar, ac, lda) * sizeof(float), false);
+        int ib = st.add(B, mat_extent(br, bc, ldb) * sizeof(float), false);
+        int ic = st.add(C, mat_extent(m, n, ldc) * sizeof(float), true);
+        cudaError_t e = st.stage_in();
+        if (e == cudaSuccess)
+            e = iclb::sgemm(h, transa, transb, m, n, k, *alpha, st.dev<float>(ia), lda, st.dev<float>(ib), ldb, *beta,
+                            st.dev<float>(ic), ldc);
+        if (e == cudaSuccess) e = st.finish();
+        return map_cuda(e);
+    });
+}
+
+extern "C" iclblasStatus_t iclblasCgemm(iclblasHandle_t h, iclblasOperation_t transa, iclblasOperation_t transb, int m,
+                                        int n, int k, const oclComplex_t* alpha, oclComplex_t* A, int lda,
+                                        oclComplex_t* B, int ldb, const oclComplex_t* beta, oclComplex_t* C, int ldc)
+{
+    if (m < 0 || n < 0 || k < 0) return ICLBLAS_STATUS_INVALID_VALUE;  // iclBLAS_C.cpp:462-463
+    return guarded([&]() -> iclblasStatus_t {
+        Params p; p.present = P_N | P_M | P_K | P_A | P_LDA | P_B | P_LDB | P_C | P_LDC;
+        p.n = n; p.m = m; p.k = k; p.A = A; p.lda = lda; p.B = B; p.ldb = ldb; p.C = C; p.ldc = ldc;
+        VALIDATE(p, h);
+        if (!alpha || !beta) return ICLBLAS_STATUS_INVALID_VALUE;
+        if (transa < ICLBLAS_OP_N || transa > ICLBLAS_OP_C || transb < ICLBLAS_OP_N || transb > ICLBLAS_OP_C)
+            return ICLBLAS_STATUS_INVALID_VALUE;
+        const int ar = transa == ICLBLAS_OP_N ? m : k, ac = transa == ICLBLAS_OP_N ? k : m;
+        const int br = transb == ICLBLAS_OP_N ? k : n, bc = transb == ICLBLAS_OP_N ? n : k;
+        Stager st(h);
+        int ia = st.add(A, mat_extent(ar, ac, lda) * sizeof(cfloat), false);
+        int ib = st.add(B, mat_extent(br, bc, ldb) * sizeof(cfloat), false);
+        int ic = st.add(C, mat_extent(m, n, ldc) * sizeof(cfloat), true);
+        cudaError_t e = st.stage_in();
+        if (e == cudaSuccess)
+            e = iclb::cgemm(h, transa, transb, m, n, k, cf(alpha), st.dev<cfloat>(ia), lda, st.dev<cfloat>(ib), ldb,
+                            cf(beta), st.dev<cfloat>(ic), ldc);
+        if (e == cudaSuccess) e = st.finish();
+        return map_cuda(e);
+    });
+}
+
+extern "C" iclblasStatus_t iclblasStrsm(iclblasHandle_t h, iclblasSideMode_t side, iclblasFillMode_t uplo,
+                                        iclblasOperation_t trans, iclblasDiagType_t diag, int m, int n,
+                                        const float* alpha, float* A, int lda, float* B, int ldb)
+{
+    if (m == 0 || n == 0) return ICLBLAS_STATUS_SUCCESS;  // iclBLAS_S.cpp:477-478
+    return guarded([&]() -> iclblasStatus_t {
+        Params p; p.present = P_N | P_M | P_A | P_LDA | P_B | P_LDB;
+        p.n = n; p.m = m; p.A = A; p.lda = lda; p.B = B; p.ldb = ldb;
+        VALIDATE(p, h);
+        if (!alpha) return ICLBLAS_STATUS_INVALID_VALUE;
+        if (trans < ICLBLAS_OP_N || trans > ICLBLAS_OP_C) return ICLBLAS_STATUS_INVALID_VALUE;
+        const int na = side == ICLBLAS_SIDE_LEFT ? m : n;
+        Stager st(h);
+        int ia = st.add(A, mat_extent(na, na, lda) * sizeof(float), false);
+        int ib = st.add(B, mat_extent(m, n, ldb) * sizeof(float), true);
+        cudaError_t e = st.stage_in();
+        if (e == cudaSuccess)
+            e = iclb::strsm(h, side, uplo, trans, diag, m, n, *alpha, st.dev<float>(ia), lda, st.dev<float>(ib), ldb);
+        if (e == cudaSuccess) e = st.finish();
+        return map_cuda(e);
+    });
+}
+
+extern "C" iclblasStatus_t iclblasCtrsm(iclblasHandle_t h, iclblasSideMode_t side, iclblasFillMode_t uplo,
+                                        iclblasOperation_t trans, iclblasDiagType_t diag, int m, int n,
+                                        const oclComplex_t* alpha, oclComplex_t* A, int lda, oclComplex_t* B, int ldb)
+{
+    if (m == 0 || n == 0) return ICLBLAS_STATUS_SUCCESS;  // iclBLAS_C.cpp:527-528
+    return guarded([&]() -> iclblasStatus_t {
+        Params p; p.present = P_N | P_M | P_A | P_LDA | P_B | P_LDB;
+        p.n = n; p.m = m; p.A = A; p.lda = lda; p.B = B; p.ldb = ldb;
+        VALIDATE(p, h);
+        if (!alpha) return ICLBLAS_STATUS_INVALID_VALUE;
+        if (trans < ICLBLAS_OP_N || trans > ICLBLAS_OP_C) return ICLBLAS_STATUS_INVALID_VALUE;
+        const int na = side == ICLBLAS_SIDE_LEFT ? m : n;
+        Stager st(h);
+        int ia = st.add(A, mat_extent(na, na, lda) * sizeof(cfloat), false);
+        int ib = st.add(B, mat_extent(m, n, ldb) * sizeof(cfloat), true);
+        cudaError_t e = st.stage_in();
+        if (e == cudaSuccess)
+            e = iclb::ctrsm(h, side, uplo, trans, diag, m, n, cf(alpha), st.dev<cfloat>(ia), lda, st.dev<cfloat>(ib),
+                            ldb);
+        if (e == cudaSuccess) e = st.finish();
+        return map_cuda(e);
+    });
+}

@@ -1,0 +1,30 @@
+// GEMM dispatch by the handle's math mode.
+//
+// The reference picks among seven SGEMM implementations by summed accept()
+// scores (libs/blas/functions_base.hpp:164-223); here the routine maps
+// directly: PLAIN_FP32 runs the CUDA-core FFMA kernel (bit-identical to the
+// reference's FP32 FMA order), the tensor-core modes run the tcgen05 kernel.
+#include "common.cuh"
+
+namespace iclb {
+
+cudaError_t sgemm_simt(iclblasHandle_t h, int ta, int tb, int m, int n, int k, float alpha, const float* A, int lda,
+                       const float* B, int ldb, float beta, float* C, int ldc);
+cudaError_t cgemm_simt(iclblasHandle_t h, int ta, int tb, int m, int n, int k, cfloat alpha, const cfloat* A, int lda,
+                       const cfloat* B, int ldb, cfloat beta, cfloat* C, int ldc);
+
+cudaError_t sgemm(iclblasHandle_t h, int ta, int tb, int m, int n, int k, float alpha, const float* A, int lda,
+                  const float* B, int ldb, float beta, float* C, int ldc)
+{
+    if (m == 0 || n == 0) return cudaSuccess;
+    return sgemm_simt(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+}
+
+cudaError_t cgemm(iclblasHandle_t h, int ta, int tb, int m, int n, int k, cfloat alpha, const cfloat* A, int lda,
+                  const cfloat* B, int ldb, cfloat beta, cfloat* C, int ldc)
+{
+    if (m == 0 || n == 0) return cudaSuccess;
+    return cgemm_simt(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+}
+
+}  // namespace iclb

@@ -1,0 +1,99 @@
+// Internal declarations of the B200 iclBLAS library: the handle, device
+// workspace management, error plumbing and the kernel launchers that the
+// C-ABI layer (api.cu) dispatches to.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+
+#include "../../include/iclBLAS.h"
+
+namespace iclb {
+
+// Complex single as two packed floats; layout-identical to oclComplex_t.
+struct cfloat {
+    float re, im;
+};
+
+constexpr uint32_t kHandleTag = 0xB1A5B200u;
+
+// Device-side status word bits (written by kernels, read by the host).
+enum DeviceStatus : int {
+    kDevOk = 0,
+    kDevWaitTimeout = 1,   // a bounded spin-wait ran out
+};
+
+// Per-handle device workspace.  Grows on demand; never shrinks until the
+// handle is destroyed.  `counters` is a small zero-initialised area for
+// last-block-done tickets and flags; kernels that use a counter leave it at
+// zero (or, for epoch flags, monotonically increasing) when they finish.
+struct Workspace {
+    void* scratch = nullptr;   // general scratch (partials, staging)
+    size_t scratch_bytes = 0;
+    unsigned* counters = nullptr;   // kCounterWords words, zeroed at creation
+    int* dev_status = nullptr;      // one int, DeviceStatus bits
+    unsigned epoch = 0;             // host-side epoch for flag-based kernels
+};
+constexpr int kCounterWords = 1 << 16;
+
+}  // namespace iclb
+
+struct iclblasContext {
+    uint32_t tag = 0;
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    iclblasMathMode_t math = ICLBLAS_MATH_PLAIN_FP32;
+    iclb::Workspace ws;
+    // Device staging for host-pointer arguments (grows on demand).
+    void* stage = nullptr;
+    size_t stage_bytes = 0;
+    // Pinned host bounce buffer for reduction results.
+    void* pinned = nullptr;
+};
+
+namespace iclb {
+
+// Returns scratch of at least `bytes` (256-byte aligned) or nullptr.
+void* scratch(iclblasHandle_t h, size_t bytes);
+
+// ---------------------------------------------------------------- level 1
+// All pointers are device pointers; n > 0, inc > 0.  Reduction results are
+// written to device memory `result` in stream order.
+cudaError_t saxpy(iclblasHandle_t h, int n, float alpha, const float* x, int incx, float* y, int incy);
+cudaError_t sscal(iclblasHandle_t h, int n, float alpha, float* x, int incx);
+cudaError_t caxpy(iclblasHandle_t h, int n, cfloat alpha, const cfloat* x, int incx, cfloat* y, int incy);
+cudaError_t cscal(iclblasHandle_t h, int n, cfloat alpha, cfloat* x, int incx);
+
+enum class Red { Dot, Asum, Nrm2 };
+cudaError_t sreduce(iclblasHandle_t h, Red op, int n, const float* x, int incx, const float* y, int incy,
+                    float* result);
+cudaError_t creduce_real(iclblasHandle_t h, Red op, int n, const cfloat* x, int incx, float* result);
+cudaError_t cdot(iclblasHandle_t h, bool conj, int n, const cfloat* x, int incx, const cfloat* y, int incy,
+                 cfloat* result);
+cudaError_t isamax(iclblasHandle_t h, int n, const float* x, int incx, int* result);
+cudaError_t icamax(iclblasHandle_t h, int n, const cfloat* x, int incx, int* result);
+
+// ---------------------------------------------------------------- level 2
+cudaError_t sgemv(iclblasHandle_t h, int trans, int m, int n, float alpha, const float* A, int lda,
+                  const float* x, int incx, float beta, float* y, int incy);
+cudaError_t cgemv(iclblasHandle_t h, int trans, int m, int n, cfloat alpha, const cfloat* A, int lda,
+                  const cfloat* x, int incx, cfloat beta, cfloat* y, int incy);
+cudaError_t strsv(iclblasHandle_t h, int uplo, int trans, int diag, int n, const float* A, int lda, float* x,
+                  int incx);
+cudaError_t ctrsv(iclblasHandle_t h, int uplo, int trans, int diag, int n, const cfloat* A, int lda, cfloat* x,
+                  int incx);
+
+// ---------------------------------------------------------------- level 3
+cudaError_t sgemm(iclblasHandle_t h, int transa, int transb, int m, int n, int k, float alpha, const float* A,
+                  int lda, const float* B, int ldb, float beta, float* C, int ldc);
+cudaError_t cgemm(iclblasHandle_t h, int transa, int transb, int m, int n, int k, cfloat alpha, const cfloat* A,
+                  int lda, const cfloat* B, int ldb, cfloat beta, cfloat* C, int ldc);
+cudaError_t strsm(iclblasHandle_t h, int side, int uplo, int trans, int diag, int m, int n, float alpha,
+                  const float* A, int lda, float* B, int ldb);
+cudaError_t ctrsm(iclblasHandle_t h, int side, int uplo, int trans, int diag, int m, int n, cfloat alpha,
+                  const cfloat* A, int lda, cfloat* B, int ldb);
+
+}  // namespace iclb

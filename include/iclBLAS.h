@@ -171,8 +171,9 @@ typedef enum {
     ICLBLAS_MATH_BF16X6     = 3
 } iclblasMathMode_t;
 
-/* Stream of the handle (a cudaStream_t passed as void*; NULL = the handle's
- * own stream).  Device-pointer calls are enqueued on it. */
+/* Stream of the handle (a cudaStream_t passed as void*; NULL = the legacy
+ * default stream).  A new handle uses a stream of its own.  Device-pointer
+ * calls are enqueued on the handle's stream. */
 ICLBLAS_API iclblasStatus_t iclblasSetStream(iclblasHandle_t handle, void* stream);
 ICLBLAS_API iclblasStatus_t iclblasGetStream(iclblasHandle_t handle, void** stream);
 ICLBLAS_API iclblasStatus_t iclblasSetMathMode(iclblasHandle_t handle, iclblasMathMode_t mode);
