@@ -7,11 +7,15 @@
 // recursive on the triangular operand M = op(A):
 //     left, M lower:   X1 = M11 \ (s*B1);  B2 = s*B2 - M21*X1;  X2 = M22 \ B2
 // (and the mirrored orders for upper / right side), so almost all flops run in
-// large GEMMs with k = half the remaining size.  The scale s = alpha enters
-// the first update as its beta and the leaf solve as a factor, which applies
-// alpha exactly once to every entry.  Leaves of <= 64 rows are solved in
+// large GEMMs with k = half the remaining size.  As in the reference
+// (Strsm_naive.cl:35, Ctrsm_naive.cl:43) the solve runs on the unscaled B and
+// alpha multiplies the solution afterwards (one pass over B when alpha != 1);
+// scaling B first rounds differently and misses the reference's 4-ulp
+// known-answer checks after cancellation.  Leaves of <= 64 rows are solved in
 // shared memory, one RHS per thread.  GEMMs use the handle's math mode (the
 // plain FP32 default is the CUDA-core kernel).
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace iclb {
@@ -193,6 +197,21 @@ struct Solver {
     }
 };
 
+// B[:, :] *= alpha for an m x n column-major block.
+template <class T>
+__global__ void scale_kernel(int m, int n, T alpha, T* __restrict__ B, long ldb)
+{
+    const long total = (long)m * n;
+    for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+        const long j = e / m, i = e % m;
+        T* p = B + j * ldb + i;
+        *p = mulv(*p, alpha);
+    }
+}
+
+__host__ bool is_one(float a) { return a == 1.f; }
+__host__ bool is_one(cfloat a) { return a.re == 1.f && a.im == 0.f; }
+
 template <class T>
 cudaError_t trsm_impl(iclblasHandle_t h, int side, int uplo, int trans, int diag, int m, int n, T alpha, const T* A,
                       int lda, T* B, int ldb)
@@ -209,7 +228,12 @@ cudaError_t trsm_impl(iclblasHandle_t h, int side, int uplo, int trans, int diag
     s.B = B;
     s.ldb = ldb;
     s.nrhs = s.left ? n : m;
-    return s.solve(0, s.left ? m : n, alpha);
+    cudaError_t e = s.solve(0, s.left ? m : n, Gemm<T>::one());
+    if (e != cudaSuccess || is_one(alpha)) return e;
+    const long total = (long)m * n;
+    const int grid = (int)std::min<long>((total + 255) / 256, (long)h->sm_count * 8);
+    scale_kernel<T><<<grid, 256, 0, h->stream>>>(m, n, alpha, B, ldb);
+    return cudaGetLastError();
 }
 
 }  // namespace

@@ -72,7 +72,7 @@ def tri(n, lda, lower, rng, dtype=np.float32):
     """Triangle with |diag| in [1, 2] and off-diagonal N(0,1)/sqrt(n) (the
     STRSM/STRSV config's construction); the other triangle holds junk."""
     A = O.colmajor(n, n, lda, rng, dtype)
-    M = A.reshape(n, lda).T
+    M = A.reshape(n, lda).T[:n]  # view: M[i, j] = A[j*lda + i]
     d = rng.uniform(1, 2, n)
     if np.dtype(dtype) == np.complex64:
         d = d * np.exp(1j * rng.uniform(0, 2 * np.pi, n))

@@ -104,7 +104,7 @@ def test_cgemm(handle, ta, tb, mnk):
 
 def tri(n, lda, lower, rng, dtype=np.float32):
     A = O.colmajor(n, n, lda, rng, dtype)
-    M = A.reshape(n, lda).T
+    M = A.reshape(n, lda).T[:n]  # view: M[i, j] = A[j*lda + i]
     d = rng.uniform(1, 2, n)
     if np.dtype(dtype) == np.complex64:
         d = d * np.exp(1j * rng.uniform(0, 2 * np.pi, n))
