@@ -79,9 +79,10 @@ def load_traffic():
 
 
 class Clocks:
-    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+    """Samples nvidia-smi clocks and throttle reasons; summary() keeps the
+    samples whose timestamps fall inside the timed window."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -89,16 +90,31 @@ class Clocks:
         self.gpu = gpu
         self.proc = None
         self.f = None
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         try:
             self.f = tempfile.NamedTemporaryFile("w+", delete=False, suffix=".csv")
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200",
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "100",
                  "-i", str(self.gpu)], stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
         return self
+
+    def started(self) -> bool:
+        """True once the sampler has written a line (or cannot run at all)."""
+        if self.proc is None or self.proc.poll() is not None:
+            return True
+        self.f.flush()
+        return os.path.getsize(self.f.name) > 0
+
+    def mark_start(self):
+        self.t0 = time.time()
+
+    def mark_end(self):
+        self.t1 = time.time()
+        time.sleep(0.25)  # let the sampler flush a line past the window
 
     def __exit__(self, *exc):
         if self.proc is not None:
@@ -110,34 +126,44 @@ class Clocks:
 
     def summary(self):
         if self.proc is None or self.f is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        import datetime as dt
         self.f.flush()
         rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
         os.unlink(self.f.name)
-        sm, smax, reasons = [], None, set()
+        sm, smax, reasons, power = [], None, set(), []
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for r in rows:
             r = [c.strip() for c in r]
-            if len(r) < 9:
+            if len(r) < 10:
                 continue
             try:
-                sm.append(float(r[1]))
-                smax = float(r[2])
+                ts = dt.datetime.strptime(r[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                clk, cmax = float(r[2]), float(r[3])
             except ValueError:
                 continue
-            for nm, v in zip(names, r[5:9]):
+            if self.t0 is not None and not (self.t0 - 0.15 <= ts <= self.t1 + 0.15):
+                continue
+            sm.append(clk)
+            smax = cmax
+            try:
+                power.append(float(r[4]))
+            except ValueError:
+                pass
+            for nm, v in zip(names, r[6:10]):
                 if v.lower() == "active":
                     reasons.add(nm)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "power_w_max": max(power) if power else None}
 
 
 # ---------------------------------------------------------------- GPU sweep
 class Sweep:
     """Operands of the sweep on one GPU and the calls that make one step."""
 
-    def __init__(self, torch, dev, B, host: bool):
+    def __init__(self, torch, dev, B, host: bool, n1: int = N1, only=None):
         self.B = B
+        self.only = only
         g = torch.Generator(device="cpu").manual_seed(1)
 
         def mk(shape, dtype=torch.float32):
@@ -148,16 +174,22 @@ class Sweep:
                 return t.pin_memory()
             return t.to(dev)
 
-        n = N1
+        def want(*names):
+            return not only or any(nm in only for nm in names)
+
+        n = n1
         self.n = n
-        self.x = mk((n,))
-        self.y = mk((n,))
-        self.A = mk((GEMV_N * GEMV_N,))
-        self.gx = mk((GEMV_N,))
-        self.gy = mk((GEMV_N,))
-        self.CA = mk((CGEMV_N * CGEMV_N,), torch.complex64)
-        self.cx = mk((CGEMV_N,), torch.complex64)
-        self.cy = mk((CGEMV_N,), torch.complex64)
+        l1 = want("saxpy", "sdot", "snrm2", "sasum", "isamax")
+        self.x = mk((n,)) if l1 else None
+        self.y = mk((n,)) if want("saxpy", "sdot") else None
+        sg = want("sgemv_n", "sgemv_t")
+        self.A = mk((GEMV_N * GEMV_N,)) if sg else None
+        self.gx = mk((GEMV_N,)) if sg else None
+        self.gy = mk((GEMV_N,)) if sg else None
+        cg = want("cgemv_n", "cgemv_c")
+        self.CA = mk((CGEMV_N * CGEMV_N,), torch.complex64) if cg else None
+        self.cx = mk((CGEMV_N,), torch.complex64) if cg else None
+        self.cy = mk((CGEMV_N,), torch.complex64) if cg else None
         if host:
             self.r = torch.zeros(1, dtype=torch.float32).pin_memory()
             self.ri = torch.zeros(1, dtype=torch.int32).pin_memory()
@@ -170,7 +202,7 @@ class Sweep:
         """(name, thunk) for each call of one step, in order."""
         B, n = self.B, self.n
         gn, cn = GEMV_N, CGEMV_N
-        return [
+        allc = [
             ("saxpy", lambda: B.iclblasSaxpy(h, n, 0.5, self.x, 1, self.y, 1)),
             ("sdot", lambda: B.iclblasSdot(h, n, self.x, 1, self.y, 1, self.r)),
             ("snrm2", lambda: B.iclblasSnrm2(h, n, self.x, 1, self.r)),
@@ -181,6 +213,7 @@ class Sweep:
             ("cgemv_n", lambda: B.iclblasCgemv(h, 0, cn, cn, 1 + 1j, self.CA, cn, self.cx, 1, 0.5, self.cy, 1)),
             ("cgemv_c", lambda: B.iclblasCgemv(h, 2, cn, cn, 1 + 1j, self.CA, cn, self.cx, 1, 0.5, self.cy, 1)),
         ]
+        return [c for c in allc if not self.only or c[0] in self.only]
 
     def io_bytes(self):
         """Host<->device bytes per step of the host-operand (e2e) sweep."""
@@ -190,50 +223,54 @@ class Sweep:
         return h2d, d2h
 
 
-LAUNCHES_PER_STEP = 9  # one kernel per call (n = 2^28 is a multiple of 4: no tail launch)
-
-
 def run_ours(args, rank, world, torch):
     from clgpu_b200 import iclblas as B
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
     stream = torch.cuda.Stream(device=dev)
-    bytes_per = sweep_bytes()
-    step_bytes = sum(bytes_per.values())
+    only = set(args.only.split(",")) if args.only else None
+    bytes_all = sweep_bytes(args.n1)
 
     with B.Handle() as h:
         h.set_stream(stream)
-        sw = Sweep(torch, dev, B, host=False)
+        sw = Sweep(torch, dev, B, host=False, n1=args.n1, only=only)
         torch.cuda.synchronize()
         calls = sw.calls(h)
-        with torch.cuda.stream(stream):
+        bytes_per = {name: bytes_all[name] for name, _ in calls}
+        step_bytes = sum(bytes_per.values())
+        with torch.cuda.stream(stream), Clocks(dev.index) as clk:
             for _ in range(args.warmup):
                 for name, f in calls:
                     B.check(f(), name)
+            # keep the GPU busy until the clock sampler is running
+            t_wait = time.time()
+            while not clk.started() and time.time() - t_wait < 5.0:
+                for name, f in calls:
+                    B.check(f(), name)
+                torch.cuda.synchronize()
             torch.cuda.synchronize()
             ev = {name: [] for name, _ in calls}
-            marks = []
             if world > 1:
                 torch.distributed.barrier()
             torch.cuda.synchronize()
             start = torch.cuda.Event(enable_timing=True)
             end = torch.cuda.Event(enable_timing=True)
-            with Clocks(dev.index) as clk:
-                start.record(stream)
-                for _ in range(args.steps):
-                    for name, f in calls:
-                        e0 = torch.cuda.Event(enable_timing=True)
-                        e1 = torch.cuda.Event(enable_timing=True)
-                        e0.record(stream)
-                        B.check(f(), name)
-                        e1.record(stream)
-                        ev[name].append((e0, e1))
-                end.record(stream)
-                torch.cuda.synchronize()
-            clocks = clk.summary()
+            clk.mark_start()
+            start.record(stream)
+            for _ in range(args.steps):
+                for name, f in calls:
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    B.check(f(), name)
+                    e1.record(stream)
+                    ev[name].append((e0, e1))
+            end.record(stream)
+            torch.cuda.synchronize()
+            clk.mark_end()
+        clocks = clk.summary()
         total_ms = start.elapsed_time(end)
         per_call_ms = {name: float(np.mean([a.elapsed_time(b) for a, b in ev[name]])) for name in ev}
-        del marks
         t_max = total_ms
         if world > 1:
             t = torch.tensor([total_ms], device=dev)
@@ -241,38 +278,48 @@ def run_ours(args, rank, world, torch):
             t_max = float(t.item())
         value = world * step_bytes * args.steps / (t_max / 1e3) / 1e9
 
-        # dominant kernel: largest share of the step
+        # dominant kernel: the call with the largest share of the step
         dom = max(per_call_ms, key=per_call_ms.get)
         peak, peak_kind = load_peaks()
         achieved = bytes_per[dom] / (per_call_ms[dom] / 1e3) / 1e9
-        traffic = load_traffic().get(dom)
+        tr = load_traffic().get(dom)
+        traffic = None
+        if tr:
+            # scale the captured launch's DRAM bytes to this launch's size
+            traffic = int(tr["dram_bytes"] * bytes_per[dom] / tr["algorithmic_bytes"])
 
-        # e2e: host (pinned) operands through the same C ABI calls
-        del sw
-        torch.cuda.empty_cache()
-        swh = Sweep(torch, dev, B, host=True)
-        callsh = swh.calls(h)
-        for _ in range(1):
+        e2e = None
+        if not args.no_e2e:
+            # host (pinned) operands through the same C ABI calls
+            del sw
+            torch.cuda.empty_cache()
+            swh = Sweep(torch, dev, B, host=True, n1=args.n1, only=only)
+            callsh = swh.calls(h)
             for name, f in callsh:
                 B.check(f(), name)
-        e2e_steps = max(1, min(args.steps, 3))
-        torch.cuda.synchronize()
-        s0 = torch.cuda.Event(enable_timing=True)
-        s1 = torch.cuda.Event(enable_timing=True)
-        s0.record(stream)
-        for _ in range(e2e_steps):
-            for name, f in callsh:
-                B.check(f(), name)
-        s1.record(stream)
-        torch.cuda.synchronize()
-        e2e_ms = s0.elapsed_time(s1)
-        if world > 1:
-            t = torch.tensor([e2e_ms], device=dev)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            e2e_ms = float(t.item())
-        h2d, d2h = swh.io_bytes()
-        e2e_value = world * step_bytes * e2e_steps / (e2e_ms / 1e3) / 1e9
-        del swh
+            e2e_steps = max(1, min(args.steps, 3))
+            torch.cuda.synchronize()
+            if world > 1:
+                torch.distributed.barrier()
+            s0 = torch.cuda.Event(enable_timing=True)
+            s1 = torch.cuda.Event(enable_timing=True)
+            s0.record(stream)
+            for _ in range(e2e_steps):
+                for name, f in callsh:
+                    B.check(f(), name)
+            s1.record(stream)
+            torch.cuda.synchronize()
+            e2e_ms = s0.elapsed_time(s1)
+            if world > 1:
+                t = torch.tensor([e2e_ms], device=dev)
+                torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+                e2e_ms = float(t.item())
+            h2d, d2h = swh.io_bytes()
+            e2e = {"value": round(world * step_bytes * e2e_steps / (e2e_ms / 1e3) / 1e9, 2), "unit": "GB/s",
+                   "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": e2e_steps,
+                   "ms_per_step": round(e2e_ms / e2e_steps, 3),
+                   "path": "C ABI with pinned host operands; copies in/out inside every call"}
+            del swh
 
     out = {
         "metric": "level-1/2 sweep aggregate HBM bandwidth (SAXPY/SDOT/SNRM2/SASUM/ISAMAX n=2^28, "
@@ -288,7 +335,8 @@ def run_ours(args, rank, world, torch):
         "vs_baseline": None,
         "dtype": "fp32",
         "data": "synthetic U(-1,1), seed 1",
-        "config": {"workload": "bandwidth sweep: level-1 n=2^28 x5, SGEMV 16384^2 N,T, CGEMV 8192^2 N,C",
+        "config": {"workload": "bandwidth sweep: level-1 n=%d x5, SGEMV 16384^2 N,T, CGEMV 8192^2 N,C" % args.n1
+                   if not only else "subset %s, level-1 n=%d" % (sorted(only), args.n1),
                    "bytes_per_step": step_bytes, "l2": "inputs larger than L2 (>=512 MiB each), no flush",
                    "parallelism": f"replicas x{world}"},
         "per_call_ms": {k: round(v, 4) for k, v in per_call_ms.items()},
@@ -296,9 +344,8 @@ def run_ours(args, rank, world, torch):
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
                      "peak_source": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
                      "traffic": traffic, "algorithmic_bytes": bytes_per[dom]},
-        "e2e": {"value": round(e2e_value, 2), "unit": "GB/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "steps": e2e_steps, "ms_per_step": round(e2e_ms / e2e_steps, 3)},
-        "gpu_launches": LAUNCHES_PER_STEP * args.steps,
+        "e2e": e2e,
+        "gpu_launches": len(calls) * args.steps,
         "clocks": clocks,
     }
     return out
@@ -397,10 +444,13 @@ def cpu_sweep(threads: int, reps: int = 3):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-operand (C ABI) leg")
+    ap.add_argument("--only", default="", help="comma-separated subset of the sweep's calls")
+    ap.add_argument("--n1", type=int, default=N1, help="level-1 vector length (default 2^28)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -433,7 +483,7 @@ def main():
     if world > 1:
         torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     out = run_ours(args, rank, world, torch)
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.only:
         out["cpu_baseline"] = {k: v for k, v in cpu_sweep(1, reps=3).items() if k != "seconds_per_step"}
     if rank == 0:
         print(json.dumps(out))
