@@ -69,7 +69,7 @@ def load_peaks():
 
 def load_traffic():
     """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "traffic.json")
+    p = os.path.join(ROOT, "profiles", "sweep_kernels_dram_traffic.json")
     if os.path.exists(p):
         try:
             return json.load(open(p))

@@ -75,7 +75,7 @@ iclblasStatus_t iclblasDestroy(iclblasHandle_t handle)
     return ICLBLAS_STATUS_SUCCESS;
 }
 
-/* ---- level 1, single (iclBLAS_S.cpp:50-211) ---- */
+/* ---- level 1, single (iclBLAS_S.cpp:66-228) ---- */
 iclblasStatus_t iclblasSscal(iclblasHandle_t h, int n, const float* alpha, float* x, int incx)
 {
     vparams p = { P_N | P_X | P_INCX, .n = n, .x = x, .incx = incx };

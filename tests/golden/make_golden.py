@@ -1,0 +1,213 @@
+"""Generates tests/golden/reference_cpu_vectors.npz from the reference's own CPU code.
+
+Inputs are seeded here; outputs come from oracle/_ref/libiclref.so, i.e. the
+reference's CPU templates (tests/blas_funcs/*.hpp: cpu_gemm, cpu_dot,
+cpu_nrm2, cpu_asum, cpu_axpy, cpu_scal, cpu_amax; tests/blas_reference/
+blas_reference.cpp: Isamax_reference, Caxpy_reference) and its serial OpenCL
+kernels compiled as C++ (Sgemv/Cgemv/Strsv/Ctrsv/Strsm/Ctrsm/Sgemm/Cgemm
+_naive.cl), all built from the reference's sources by oracle/Makefile.
+
+Each case is stored under a key prefix "<case>/" with its inputs, scalar
+parameters and the reference output.  The fixture is committed; run this
+script (with the reference tree built into oracle/_ref) to regenerate it.
+
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(HERE))
+import oracle_lib as O  # noqa: E402
+
+OUT = os.path.join(HERE, "reference_cpu_vectors.npz")
+
+
+def P(a):
+    return a.ctypes.data
+
+
+def tri(n, lda, lower, rng, dtype=np.float32):
+    A = O.colmajor(n, n, lda, rng, dtype)
+    M = A.reshape(n, lda).T[:n]
+    d = rng.uniform(1, 2, n)
+    if np.dtype(dtype) == np.complex64:
+        d = d * np.exp(1j * rng.uniform(0, 2 * np.pi, n))
+    off = (rng.standard_normal((n, n)) / np.sqrt(n)).astype(np.float32)
+    mask = np.tril(np.ones((n, n), bool), -1) if lower else np.triu(np.ones((n, n), bool), 1)
+    M[mask] = off[mask]
+    M[np.arange(n), np.arange(n)] = d
+    return A
+
+
+def main():
+    R = O.ref()
+    if R is None:
+        raise SystemExit("oracle/_ref/libiclref.so is missing: build the oracle with the reference tree present")
+    rng = np.random.default_rng(20261203)
+    d = {}
+
+    # ---- level 1, real
+    for n, inc in ((1000, 1), (513, 3)):
+        k = f"l1s_{n}_{inc}/"
+        x = rng.uniform(-1, 1, n * inc).astype(np.float32)
+        y = rng.uniform(-1, 1, n * inc).astype(np.float32)
+        d[k + "x"], d[k + "y"] = x, y
+        d[k + "n"], d[k + "inc"] = np.int32(n), np.int32(inc)
+        d[k + "sdot"] = np.float32(R.ref_cpu_sdot(n, P(x), inc, P(y), inc))
+        d[k + "snrm2"] = np.float32(R.ref_cpu_snrm2(n, P(x), inc))
+        d[k + "sasum"] = np.float32(R.ref_cpu_sasum(n, P(x), inc))
+        d[k + "isamax"] = np.int32(R.ref_cpu_isamax(n, P(x), inc))
+        y2 = y.copy()
+        R.ref_cpu_saxpy(n, 0.75, P(x), inc, P(y2), inc)
+        d[k + "saxpy_alpha"], d[k + "saxpy"] = np.float32(0.75), y2
+        x2 = x.copy()
+        R.ref_cpu_sscal(n, -1.5, P(x2), inc)
+        d[k + "sscal_alpha"], d[k + "sscal"] = np.float32(-1.5), x2
+    # ties and NaN for iamax
+    for i, x in enumerate((np.array([1, -5, 3, 5, -5, 2], np.float32),
+                           np.array([np.nan, 1, 7, 2, 9], np.float32),
+                           np.array([1, np.nan, 7, 2, 7], np.float32))):
+        k = f"iamax_edge_{i}/"
+        d[k + "x"] = x
+        d[k + "isamax"] = np.int32(R.ref_cpu_isamax(len(x), P(x), 1))
+
+    # ---- level 1, complex
+    for n, inc in ((777, 1), (301, 2)):
+        k = f"l1c_{n}_{inc}/"
+        x = O.colmajor(n * inc, 1, n * inc, rng, np.complex64)
+        y = O.colmajor(n * inc, 1, n * inc, rng, np.complex64)
+        d[k + "x"], d[k + "y"] = x, y
+        d[k + "n"], d[k + "inc"] = np.int32(n), np.int32(inc)
+        for conj, nm in ((0, "cdotu"), (1, "cdotc")):
+            out = np.zeros(2, np.float32)
+            R.ref_cpu_cdot(n, P(x), inc, P(y), inc, conj, P(out))
+            d[k + nm] = np.complex64(complex(out[0], out[1]))
+        d[k + "scnrm2"] = np.float32(R.ref_cpu_scnrm2(n, P(x), inc))
+        d[k + "scasum"] = np.float32(R.ref_cpu_scasum(n, P(x), inc))
+        d[k + "icamax"] = np.int32(R.ref_cpu_icamax(n, P(x), inc))
+        a = np.complex64(0.5 - 0.25j)
+        ab = O.cbox(a)
+        x2 = x.copy()
+        R.ref_cpu_cscal(n, P(ab), P(x2), inc)
+        d[k + "cscal_alpha"], d[k + "cscal"] = a, x2
+        y2 = y.copy()
+        xc = x.copy()
+        R.ref_caxpy_reference(n, P(ab), P(xc), inc, P(y2), inc)
+        d[k + "caxpy_alpha"], d[k + "caxpy"] = a, y2
+
+    # ---- SGEMM: quarter-integer values (exact) through cpu_gemm, all op pairs
+    m, n, kk = 24, 20, 28
+    for ta in (0, 1, 2):
+        for tb in (0, 1, 2):
+            for beta in (0.0, 0.5):
+                k = f"sgemm_q_{ta}{tb}_{int(beta * 10)}/"
+                ar, ac = (m, kk) if ta == 0 else (kk, m)
+                br, bc = (kk, n) if tb == 0 else (n, kk)
+                lda, ldb, ldc = ar + 1, br + 3, m + 2
+                A = O.quarter_ints(lda * ac, rng)
+                Bm = O.quarter_ints(ldb * bc, rng)
+                Cm = O.quarter_ints(ldc * n, rng)
+                d[k + "A"], d[k + "B"], d[k + "C"] = A, Bm, Cm.copy()
+                d[k + "dims"] = np.array([ta, tb, m, n, kk, lda, ldb, ldc], np.int32)
+                d[k + "ab"] = np.array([1.5, beta], np.float32)
+                R.ref_cpu_sgemm(ta, tb, m, n, kk, 1.5, P(A), lda, P(Bm), ldb, beta, P(Cm), ldc)
+                d[k + "out"] = Cm
+    # ---- CGEMM: random values through cpu_gemm<complex> (double accumulator)
+    m, n, kk = 14, 12, 16
+    for ta in (0, 1, 2):
+        for tb in (0, 1, 2):
+            k = f"cgemm_{ta}{tb}/"
+            ar, ac = (m, kk) if ta == 0 else (kk, m)
+            br, bc = (kk, n) if tb == 0 else (n, kk)
+            A = O.colmajor(ar, ac, ar, rng, np.complex64)
+            Bm = O.colmajor(br, bc, br, rng, np.complex64)
+            Cm = O.colmajor(m, n, m, rng, np.complex64)
+            al, be = np.complex64(1.5 - 0.5j), np.complex64(0.25 + 1j)
+            alb, beb = O.cbox(al), O.cbox(be)
+            d[k + "A"], d[k + "B"], d[k + "C"] = A, Bm, Cm.copy()
+            d[k + "dims"] = np.array([ta, tb, m, n, kk, ar, br, m], np.int32)
+            d[k + "ab"] = np.array([al, be], np.complex64)
+            R.ref_cpu_cgemm(ta, tb, m, n, kk, P(alb), P(A), ar, P(Bm), br, P(beb), P(Cm), m)
+            d[k + "out"] = Cm
+
+    # ---- GEMV through the serial kernels
+    m, n, lda = 40, 27, 43
+    for trans in (0, 1, 2):
+        k = f"sgemv_{trans}/"
+        A = O.colmajor(m, n, lda, rng)
+        xl, yl = (n, m) if trans == 0 else (m, n)
+        x = rng.uniform(-1, 1, xl * 2).astype(np.float32)
+        y = rng.uniform(-1, 1, yl * 3).astype(np.float32)
+        d[k + "A"], d[k + "x"], d[k + "y"] = A, x, y.copy()
+        d[k + "dims"] = np.array([trans, m, n, lda, 2, 3], np.int32)
+        d[k + "ab"] = np.array([0.75, -0.5], np.float32)
+        R.ref_naive_sgemv(trans, m, n, 0.75, P(A), lda, P(x), 2, -0.5, P(y), 3)
+        d[k + "out"] = y
+        k = f"cgemv_{trans}/"
+        A = O.colmajor(m, n, lda, rng, np.complex64)
+        x = O.colmajor(xl, 1, xl, rng, np.complex64)
+        y = O.colmajor(yl, 1, yl, rng, np.complex64)
+        al, be = np.complex64(0.5 + 1j), np.complex64(1 - 0.5j)
+        alb, beb = O.cbox(al), O.cbox(be)
+        d[k + "A"], d[k + "x"], d[k + "y"] = A, x, y.copy()
+        d[k + "dims"] = np.array([trans, m, n, lda, 1, 1], np.int32)
+        d[k + "ab"] = np.array([al, be], np.complex64)
+        R.ref_naive_cgemv(trans, m, n, P(alb), P(A), lda, P(x), 1, P(beb), P(y), 1)
+        d[k + "out"] = y
+
+    # ---- TRSV / TRSM through the serial kernels
+    n, lda = 37, 39
+    for uplo in (0, 1):
+        for trans in (0, 1, 2):
+            for diag in (0, 1):
+                k = f"strsv_{uplo}{trans}{diag}/"
+                A = tri(n, lda, uplo == 1, rng)
+                x = rng.uniform(-1, 1, n * 2).astype(np.float32)
+                d[k + "A"], d[k + "x"] = A, x.copy()
+                d[k + "dims"] = np.array([uplo, trans, diag, n, lda, 2], np.int32)
+                R.ref_naive_strsv(uplo, trans, diag, n, P(A), lda, P(x), 2)
+                d[k + "out"] = x
+                k = f"ctrsv_{uplo}{trans}{diag}/"
+                A = tri(n, lda, uplo == 1, rng, np.complex64)
+                x = O.colmajor(n, 1, n, rng, np.complex64)
+                d[k + "A"], d[k + "x"] = A, x.copy()
+                d[k + "dims"] = np.array([uplo, trans, diag, n, lda, 1], np.int32)
+                R.ref_naive_ctrsv(uplo, trans, diag, n, P(A), lda, P(x), 1)
+                d[k + "out"] = x
+    m, n = 20, 13
+    for side in (0, 1):
+        for uplo in (0, 1):
+            for trans in (0, 1, 2):
+                for diag in (0, 1):
+                    na = m if side == 0 else n
+                    lda, ldb = na + 2, m + 3
+                    k = f"strsm_{side}{uplo}{trans}{diag}/"
+                    A = tri(na, lda, uplo == 1, rng)
+                    Bm = O.colmajor(m, n, ldb, rng)
+                    d[k + "A"], d[k + "B"] = A, Bm.copy()
+                    d[k + "dims"] = np.array([side, uplo, trans, diag, m, n, lda, ldb], np.int32)
+                    d[k + "alpha"] = np.float32(-0.75)
+                    R.ref_naive_strsm(side, uplo, trans, diag, m, n, -0.75, P(A), lda, P(Bm), ldb)
+                    d[k + "out"] = Bm
+                    k = f"ctrsm_{side}{uplo}{trans}{diag}/"
+                    A = tri(na, lda, uplo == 1, rng, np.complex64)
+                    Bm = O.colmajor(m, n, ldb, rng, np.complex64)
+                    al = np.complex64(0.5 - 1j)
+                    alb = O.cbox(al)
+                    d[k + "A"], d[k + "B"] = A, Bm.copy()
+                    d[k + "dims"] = np.array([side, uplo, trans, diag, m, n, lda, ldb], np.int32)
+                    d[k + "alpha"] = al
+                    R.ref_naive_ctrsm(side, uplo, trans, diag, m, n, P(alb), P(A), lda, P(Bm), ldb)
+                    d[k + "out"] = Bm
+
+    np.savez_compressed(OUT, **d)
+    print(f"wrote {OUT}: {len(d)} arrays, {os.path.getsize(OUT) / 1024:.0f} KiB")
+
+
+if __name__ == "__main__":
+    main()

@@ -56,23 +56,23 @@ def test_validation_order_without_device(libpath):
     assert B.iclblasSscal(None, 4, 2.0, x, 0) == B.INVALID_VALUE      # incx == 0
     assert B.iclblasSscal(None, 4, 2.0, x, -1) == B.NOT_SUPPORTED     # negative stride
     assert B.iclblasSscal(None, 4, 2.0, x, 1) == B.INVALID_VALUE      # bad handle last
-    # Saxpy: alpha == 0 or n <= 0 returns first (iclBLAS_S.cpp:62-63)
+    # Saxpy: alpha == 0 or n <= 0 returns first (iclBLAS_S.cpp:77-78)
     assert B.iclblasSaxpy(None, 4, 0.0, x, 1, y, 1) == B.SUCCESS
     assert B.iclblasSaxpy(None, -3, 1.0, x, 1, y, 1) == B.SUCCESS
     assert B.iclblasSaxpy(None, 4, 1.0, x, 1, y, -2) == B.NOT_SUPPORTED
-    # Sgemm: negative sizes first (iclBLAS_S.cpp:465-466), then validate_params
+    # Sgemm: negative sizes first (iclBLAS_S.cpp:491-492), then validate_params
     assert B.iclblasSgemm(None, 0, 0, -1, 4, 4, 1.0, A, 8, A, 8, 0.0, A, 8) == B.INVALID_VALUE
     assert B.iclblasSgemm(None, 0, 0, 4, 0, 4, 1.0, A, 8, A, 8, 0.0, A, 8) == B.SUCCESS
     assert B.iclblasSgemm(None, 0, 0, 4, 4, 4, 1.0, A, 0, A, 8, 0.0, A, 8) == B.INVALID_VALUE
     assert B.iclblasSgemm(None, 0, 0, 4, 4, 4, 1.0, A, 8, A, 8, 0.0, None, 8) == B.INVALID_VALUE
-    # Sgemv: early success on alpha == 0 and beta == 1 (iclBLAS_S.cpp:452)
+    # Sgemv: early success on alpha == 0 and beta == 1 (iclBLAS_S.cpp:477)
     assert B.iclblasSgemv(None, 0, 4, 4, 0.0, A, 4, x, 1, 1.0, y, 1) == B.SUCCESS
     assert B.iclblasSgemv(None, 0, 4, 4, 1.0, A, 4, x, 0, 1.0, y, 1) == B.INVALID_VALUE
-    # Strsv: n == 0 success, n < 0 / incx == 0 invalid (iclBLAS_S.cpp:224-226)
+    # Strsv: n == 0 success, n < 0 / incx == 0 invalid (iclBLAS_S.cpp:242-244)
     assert B.iclblasStrsv(None, 1, 0, 0, 0, A, 4, x, 1) == B.SUCCESS
     assert B.iclblasStrsv(None, 1, 0, 0, -2, A, 4, x, 1) == B.INVALID_VALUE
     assert B.iclblasStrsv(None, 1, 0, 0, 4, A, 4, x, 0) == B.INVALID_VALUE
-    # Strsm: m == 0 success before anything (iclBLAS_S.cpp:477-478)
+    # Strsm: m == 0 success before anything (iclBLAS_S.cpp:503-504)
     assert B.iclblasStrsm(None, 0, 1, 0, 0, 0, 4, 1.0, A, 4, A, 4) == B.SUCCESS
     assert B.iclblasStrsm(None, 0, 1, 0, 0, 4, 4, 1.0, A, -1, A, 4) == B.INVALID_VALUE
 
@@ -80,7 +80,7 @@ def test_validation_order_without_device(libpath):
 def test_reduction_early_results_without_device(libpath):
     x = np.ones(8, np.float32)
     r = np.array([123.0], np.float32)
-    assert B.iclblasSnrm2(None, 0, x, 1, r) == B.SUCCESS and r[0] == 0.0   # iclBLAS_S.cpp:74-77
+    assert B.iclblasSnrm2(None, 0, x, 1, r) == B.SUCCESS and r[0] == 0.0   # iclBLAS_S.cpp:89-92
     r[0] = 5
     assert B.iclblasSasum(None, 4, x, -1, r) == B.SUCCESS and r[0] == 0.0
     ri = np.array([9], np.int32)

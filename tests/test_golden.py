@@ -1,0 +1,212 @@
+"""Golden vectors produced by the reference's own CPU code (tests/golden/
+reference_cpu_vectors.npz, made by tests/golden/make_golden.py from the
+reference's CPU templates and serial kernels compiled from its sources).
+
+CPU tests pin the oracle to them; GPU tests check the library through its C
+ABI against them directly, so GPU parity does not depend on the oracle.
+Bars: index results and the quarter-integer SGEMM exact; level-1 float
+results within 1 ulp (different summation order of the same FP64 sums);
+GEMV/TRSV/TRSM/CGEMM relative Frobenius error <= 1e-5 (the reference's serial
+kernels round in FP32).
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle_lib as O
+from clgpu_b200 import iclblas as B
+
+G = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_cpu_vectors.npz"))
+CASES = sorted({k.split("/")[0] for k in G.files})
+TOL = 1e-5
+
+
+def g(case, name):
+    return G[f"{case}/{name}"]
+
+
+def cases(prefix):
+    return [c for c in CASES if c.startswith(prefix)]
+
+
+def ulps(a, b):
+    return int(O.ulp_diff(np.float32(a), np.float32(b)).max())
+
+
+def cnear(got, want, scale, k=2):
+    tol = k * 2.0 ** -23 * max(abs(want.real), abs(want.imag)) + 1e-12 * scale
+    return abs(got.real - want.real) <= tol and abs(got.imag - want.imag) <= tol
+
+
+# ------------------------------------------------------------------ oracle
+@pytest.mark.parametrize("case", cases("l1s_"))
+def test_oracle_level1_real(case):
+    x, y, n, inc = g(case, "x"), g(case, "y"), int(g(case, "n")), int(g(case, "inc"))
+    assert O.sdot(n, x, inc, y, inc) == g(case, "sdot")
+    assert O.snrm2(n, x, inc) == g(case, "snrm2")
+    assert O.sasum(n, x, inc) == g(case, "sasum")
+    assert O.isamax(n, x, inc) == g(case, "isamax")
+    y2 = y.copy()
+    O.saxpy(n, float(g(case, "saxpy_alpha")), x, inc, y2, inc)
+    assert np.array_equal(y2, g(case, "saxpy"))
+    x2 = x.copy()
+    O.sscal(n, float(g(case, "sscal_alpha")), x2, inc)
+    assert np.array_equal(x2, g(case, "sscal"))
+
+
+@pytest.mark.parametrize("case", cases("iamax_edge_"))
+def test_oracle_iamax_edges(case):
+    x = g(case, "x")
+    assert O.isamax(len(x), x, 1) == g(case, "isamax")
+
+
+@pytest.mark.parametrize("case", cases("l1c_"))
+def test_oracle_level1_complex(case):
+    x, y, n, inc = g(case, "x"), g(case, "y"), int(g(case, "n")), int(g(case, "inc"))
+    assert O.cdot(n, x, inc, y, inc, False) == complex(g(case, "cdotu"))
+    assert O.cdot(n, x, inc, y, inc, True) == complex(g(case, "cdotc"))
+    assert O.scnrm2(n, x, inc) == g(case, "scnrm2")
+    assert O.scasum(n, x, inc) == g(case, "scasum")
+    assert O.icamax(n, x, inc) == g(case, "icamax")
+    x2 = x.copy()
+    O.cscal(n, complex(g(case, "cscal_alpha")), x2, inc)
+    assert np.array_equal(x2, g(case, "cscal"))
+    y2 = y.copy()
+    O.caxpy(n, complex(g(case, "caxpy_alpha")), x, inc, y2, inc)
+    assert np.max(np.abs(y2 - g(case, "caxpy"))) <= 4e-7 * (1 + np.max(np.abs(y2)))
+
+
+@pytest.mark.parametrize("case", cases("sgemm_q_"))
+def test_oracle_sgemm_quarter(case):
+    ta, tb, m, n, k, lda, ldb, ldc = (int(v) for v in g(case, "dims"))
+    al, be = (float(v) for v in g(case, "ab"))
+    Cm = g(case, "C").copy()
+    O.sgemm(ta, tb, m, n, k, al, g(case, "A"), lda, g(case, "B"), ldb, be, Cm, ldc)
+    assert np.array_equal(Cm, g(case, "out"))
+
+
+@pytest.mark.parametrize("case", cases("cgemm_"))
+def test_oracle_cgemm(case):
+    ta, tb, m, n, k, lda, ldb, ldc = (int(v) for v in g(case, "dims"))
+    al, be = (complex(v) for v in g(case, "ab"))
+    Cm = g(case, "C").copy()
+    O.cgemm(ta, tb, m, n, k, al, g(case, "A"), lda, g(case, "B"), ldb, be, Cm, ldc)
+    assert O.rel_fro(Cm, g(case, "out")) <= 1e-7
+
+
+@pytest.mark.parametrize("case", cases("sgemv_") + cases("cgemv_"))
+def test_oracle_gemv(case):
+    trans, m, n, lda, incx, incy = (int(v) for v in g(case, "dims"))
+    ab = g(case, "ab")
+    y = g(case, "y").copy()
+    if case.startswith("s"):
+        O.sgemv(trans, m, n, float(ab[0]), g(case, "A"), lda, g(case, "x"), incx, float(ab[1]), y, incy)
+    else:
+        O.cgemv(trans, m, n, complex(ab[0]), g(case, "A"), lda, g(case, "x"), incx, complex(ab[1]), y, incy)
+    assert O.rel_fro(y, g(case, "out")) <= 1e-6
+
+
+@pytest.mark.parametrize("case", cases("strsv_") + cases("ctrsv_"))
+def test_oracle_trsv(case):
+    uplo, trans, diag, n, lda, inc = (int(v) for v in g(case, "dims"))
+    x = g(case, "x").copy()
+    (O.strsv if case.startswith("s") else O.ctrsv)(uplo, trans, diag, n, g(case, "A"), lda, x, inc)
+    assert O.rel_fro(x, g(case, "out")) <= TOL
+
+
+@pytest.mark.parametrize("case", cases("strsm_") + cases("ctrsm_"))
+def test_oracle_trsm(case):
+    side, uplo, trans, diag, m, n, lda, ldb = (int(v) for v in g(case, "dims"))
+    Bm = g(case, "B").copy()
+    al = g(case, "alpha")
+    if case.startswith("s"):
+        O.strsm(side, uplo, trans, diag, m, n, float(al), g(case, "A"), lda, Bm, ldb)
+    else:
+        O.ctrsm(side, uplo, trans, diag, m, n, complex(al), g(case, "A"), lda, Bm, ldb)
+    assert O.rel_fro(Bm, g(case, "out")) <= TOL
+
+
+# ------------------------------------------------------------------ GPU library
+@pytest.mark.gpu
+def test_gpu_level1_against_golden(handle):
+    for case in cases("l1s_"):
+        x, y, n, inc = g(case, "x"), g(case, "y"), int(g(case, "n")), int(g(case, "inc"))
+        r = np.zeros(1, np.float32)
+        ri = np.zeros(1, np.int32)
+        assert B.iclblasSdot(handle, n, x, inc, y, inc, r) == B.SUCCESS and ulps(r[0], g(case, "sdot")) <= 1
+        assert B.iclblasSnrm2(handle, n, x, inc, r) == B.SUCCESS and ulps(r[0], g(case, "snrm2")) <= 1
+        assert B.iclblasSasum(handle, n, x, inc, r) == B.SUCCESS and ulps(r[0], g(case, "sasum")) <= 1
+        assert B.iclblasIsamax(handle, n, x, inc, ri) == B.SUCCESS and ri[0] == g(case, "isamax")
+        y2 = y.copy()
+        assert B.iclblasSaxpy(handle, n, float(g(case, "saxpy_alpha")), x, inc, y2, inc) == B.SUCCESS
+        assert O.ulp_diff(y2, g(case, "saxpy")).max() <= 1
+        x2 = x.copy()
+        assert B.iclblasSscal(handle, n, float(g(case, "sscal_alpha")), x2, inc) == B.SUCCESS
+        assert np.array_equal(x2, g(case, "sscal"))
+    for case in cases("iamax_edge_"):
+        x = g(case, "x")
+        ri = np.zeros(1, np.int32)
+        assert B.iclblasIsamax(handle, len(x), x, 1, ri) == B.SUCCESS and ri[0] == g(case, "isamax")
+    for case in cases("l1c_"):
+        x, y, n, inc = g(case, "x"), g(case, "y"), int(g(case, "n")), int(g(case, "inc"))
+        scale = float(np.sum(np.abs(x) * np.abs(y)))
+        r = np.zeros(1, np.complex64)
+        assert B.iclblasCdotu(handle, n, x, inc, y, inc, r) == B.SUCCESS
+        assert cnear(complex(r[0]), complex(g(case, "cdotu")), scale)
+        assert B.iclblasCdotc(handle, n, x, inc, y, inc, r) == B.SUCCESS
+        assert cnear(complex(r[0]), complex(g(case, "cdotc")), scale)
+        rf = np.zeros(1, np.float32)
+        assert B.iclblasScnrm2(handle, n, x, inc, rf) == B.SUCCESS and ulps(rf[0], g(case, "scnrm2")) <= 1
+        assert B.iclblasScasum(handle, n, x, inc, rf) == B.SUCCESS and ulps(rf[0], g(case, "scasum")) <= 1
+        ri = np.zeros(1, np.int32)
+        assert B.iclblasIcamax(handle, n, x, inc, ri) == B.SUCCESS and ri[0] == g(case, "icamax")
+        x2 = x.copy()
+        assert B.iclblasCscal(handle, n, complex(g(case, "cscal_alpha")), x2, inc) == B.SUCCESS
+        assert np.array_equal(x2, g(case, "cscal"))
+        y2 = y.copy()
+        assert B.iclblasCaxpy(handle, n, complex(g(case, "caxpy_alpha")), x, inc, y2, inc) == B.SUCCESS
+        assert np.max(np.abs(y2 - g(case, "caxpy"))) <= 4e-7 * (1 + np.max(np.abs(y2)))
+
+
+@pytest.mark.gpu
+def test_gpu_level3_level2_against_golden(handle):
+    for case in cases("sgemm_q_"):
+        ta, tb, m, n, k, lda, ldb, ldc = (int(v) for v in g(case, "dims"))
+        al, be = (float(v) for v in g(case, "ab"))
+        Cm = g(case, "C").copy()
+        assert B.iclblasSgemm(handle, ta, tb, m, n, k, al, g(case, "A"), lda, g(case, "B"), ldb, be, Cm,
+                              ldc) == B.SUCCESS
+        assert np.array_equal(Cm, g(case, "out")), case
+    for case in cases("cgemm_"):
+        ta, tb, m, n, k, lda, ldb, ldc = (int(v) for v in g(case, "dims"))
+        al, be = (complex(v) for v in g(case, "ab"))
+        Cm = g(case, "C").copy()
+        assert B.iclblasCgemm(handle, ta, tb, m, n, k, al, g(case, "A"), lda, g(case, "B"), ldb, be, Cm,
+                              ldc) == B.SUCCESS
+        assert O.rel_fro(Cm, g(case, "out")) <= TOL, case
+    for case in cases("sgemv_") + cases("cgemv_"):
+        trans, m, n, lda, incx, incy = (int(v) for v in g(case, "dims"))
+        ab = g(case, "ab")
+        y = g(case, "y").copy()
+        f = B.iclblasSgemv if case.startswith("s") else B.iclblasCgemv
+        cv = float if case.startswith("s") else complex
+        assert f(handle, trans, m, n, cv(ab[0]), g(case, "A"), lda, g(case, "x"), incx, cv(ab[1]), y,
+                 incy) == B.SUCCESS
+        assert O.rel_fro(y, g(case, "out")) <= TOL, case
+    for case in cases("strsv_") + cases("ctrsv_"):
+        uplo, trans, diag, n, lda, inc = (int(v) for v in g(case, "dims"))
+        x = g(case, "x").copy()
+        f = B.iclblasStrsv if case.startswith("s") else B.iclblasCtrsv
+        assert f(handle, uplo, trans, diag, n, g(case, "A"), lda, x, inc) == B.SUCCESS
+        assert O.rel_fro(x, g(case, "out")) <= TOL, case
+    for case in cases("strsm_") + cases("ctrsm_"):
+        side, uplo, trans, diag, m, n, lda, ldb = (int(v) for v in g(case, "dims"))
+        Bm = g(case, "B").copy()
+        al = g(case, "alpha")
+        if case.startswith("s"):
+            st = B.iclblasStrsm(handle, side, uplo, trans, diag, m, n, float(al), g(case, "A"), lda, Bm, ldb)
+        else:
+            st = B.iclblasCtrsm(handle, side, uplo, trans, diag, m, n, complex(al), g(case, "A"), lda, Bm, ldb)
+        assert st == B.SUCCESS
+        assert O.rel_fro(Bm, g(case, "out")) <= TOL, case
