@@ -331,7 +331,7 @@ extern "C" iclblasStatus_t iclblasSynchronize(iclblasHandle_t h)
 }
 
 // ------------------------------------------------------------------------
-// level 1, single (iclBLAS_S.cpp:50-211)
+// level 1, single (iclBLAS_S.cpp:66-228)
 // ------------------------------------------------------------------------
 extern "C" iclblasStatus_t iclblasSscal(iclblasHandle_t h, int n, const float* alpha, float* x, int incx)
 {
@@ -405,7 +405,7 @@ extern "C" iclblasStatus_t iclblasSasum(iclblasHandle_t h, int n, float* x, int 
 
 extern "C" iclblasStatus_t iclblasSdot(iclblasHandle_t h, int n, float* x, int incx, float* y, int incy, float* result)
 {
-    if (n <= 0) return ICLBLAS_STATUS_SUCCESS;  // result untouched (iclBLAS_S.cpp:204-205)
+    if (n <= 0) return ICLBLAS_STATUS_SUCCESS;  // result untouched (iclBLAS_S.cpp:221-222)
     return sreduce_call(h, iclb::Red::Dot, n, x, incx, y, incy, result);
 }
 
@@ -566,7 +566,7 @@ extern "C" iclblasStatus_t iclblasSgemv(iclblasHandle_t h, iclblasOperation_t tr
                                         float* A, int lda, float* x, int incx, const float* beta, float* y, int incy)
 {
     if (!alpha || !beta) return ICLBLAS_STATUS_INVALID_VALUE;
-    // iclBLAS_S.cpp:450-455
+    // iclBLAS_S.cpp:477-480
     if (m == 0 || n == 0 || (*alpha == 0.f && *beta == 1.f)) return ICLBLAS_STATUS_SUCCESS;
     if (m < 0 || n < 0 || incx == 0 || incy == 0) return ICLBLAS_STATUS_INVALID_VALUE;
     return guarded([&]() -> iclblasStatus_t {
@@ -619,7 +619,7 @@ extern "C" iclblasStatus_t iclblasCgemv(iclblasHandle_t h, iclblasOperation_t tr
 extern "C" iclblasStatus_t iclblasStrsv(iclblasHandle_t h, iclblasFillMode_t uplo, iclblasOperation_t trans,
                                         iclblasDiagType_t diag, int n, float* A, int lda, float* x, int incx)
 {
-    // iclBLAS_S.cpp:223-226
+    // iclBLAS_S.cpp:242-244
     if (n == 0) return ICLBLAS_STATUS_SUCCESS;
     if (n < 0 || incx == 0) return ICLBLAS_STATUS_INVALID_VALUE;
     return guarded([&]() -> iclblasStatus_t {
@@ -669,7 +669,7 @@ extern "C" iclblasStatus_t iclblasSgemm(iclblasHandle_t h, iclblasOperation_t tr
                                         int n, int k, const float* alpha, float* A, int lda, float* B, int ldb,
                                         const float* beta, float* C, int ldc)
 {
-    if (m < 0 || n < 0 || k < 0) return ICLBLAS_STATUS_INVALID_VALUE;  // iclBLAS_S.cpp:465-466
+    if (m < 0 || n < 0 || k < 0) return ICLBLAS_STATUS_INVALID_VALUE;  // iclBLAS_S.cpp:491-492
     return guarded([&]() -> iclblasStatus_t {
         Params p; p.present = P_N | P_M | P_K | P_A | P_LDA | P_B | P_LDB | P_C | P_LDC;
         p.n = n; p.m = m; p.k = k; p.A = A; p.lda = lda; p.B = B; p.ldb = ldb; p.C = C; p.ldc = ldc;
@@ -723,7 +723,7 @@ extern "C" iclblasStatus_t iclblasStrsm(iclblasHandle_t h, iclblasSideMode_t sid
                                         iclblasOperation_t trans, iclblasDiagType_t diag, int m, int n,
                                         const float* alpha, float* A, int lda, float* B, int ldb)
 {
-    if (m == 0 || n == 0) return ICLBLAS_STATUS_SUCCESS;  // iclBLAS_S.cpp:477-478
+    if (m == 0 || n == 0) return ICLBLAS_STATUS_SUCCESS;  // iclBLAS_S.cpp:503-504
     return guarded([&]() -> iclblasStatus_t {
         Params p; p.present = P_N | P_M | P_A | P_LDA | P_B | P_LDB;
         p.n = n; p.m = m; p.A = A; p.lda = lda; p.B = B; p.ldb = ldb;
