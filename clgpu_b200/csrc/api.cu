@@ -409,6 +409,26 @@ extern "C" iclblasStatus_t iclblasSdot(iclblasHandle_t h, int n, float* x, int i
     return sreduce_call(h, iclb::Red::Dot, n, x, incx, y, incy, result);
 }
 
+// SDOT for callers that cannot allocate device memory (see include/iclBLAS.h).
+// Same validation as iclblasSdot; then every array must be device memory,
+// because staging host data would allocate.  No cudaMalloc/cudaFree, no
+// workspace growth: the kernel's scratch is a fixed array in the library.
+extern "C" iclblasStatus_t iclblasSdotNoAlloc(iclblasHandle_t h, int n, const float* x, int incx, const float* y,
+                                              int incy, float* result)
+{
+    if (n <= 0) return ICLBLAS_STATUS_SUCCESS;  // result untouched, as iclblasSdot
+    return guarded([&]() -> iclblasStatus_t {
+        Params p; p.present = P_N | P_X | P_INCX | P_Y | P_INCY;
+        p.n = n; p.x = x; p.incx = incx; p.y = y; p.incy = incy;
+        VALIDATE(p, h);
+        if (!result) return ICLBLAS_STATUS_INVALID_VALUE;
+        if (!is_device_ptr(x) || !is_device_ptr(y) || !is_device_ptr(result)) return ICLBLAS_STATUS_INVALID_VALUE;
+        cudaError_t e = iclb::sdot_noalloc(h, n, x, incx, y, incy, result);
+        if (e == cudaErrorNotSupported) return ICLBLAS_STATUS_NOT_SUPPORTED;
+        return map_cuda(e);
+    });
+}
+
 extern "C" iclblasStatus_t iclblasIsamax(iclblasHandle_t h, int n, float* x, int incx, int* result)
 {
     if (n <= 0 || incx <= 0) { zero_result(h, result, sizeof(int)); return ICLBLAS_STATUS_SUCCESS; }

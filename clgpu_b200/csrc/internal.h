@@ -74,6 +74,12 @@ cudaError_t creduce_real(iclblasHandle_t h, Red op, int n, const cfloat* x, int 
 cudaError_t cdot(iclblasHandle_t h, bool conj, int n, const cfloat* x, int incx, const cfloat* y, int incy,
                  cfloat* result);
 cudaError_t isamax(iclblasHandle_t h, int n, const float* x, int incx, int* result);
+// SDOT whose scratch is a fixed array in the library image (no allocation);
+// device pointers only.  cudaErrorNotSupported when the launch would need
+// more than kSdotNoAllocMaxBlocks per-block partials.
+constexpr int kSdotNoAllocMaxBlocks = 4096;
+cudaError_t sdot_noalloc(iclblasHandle_t h, int n, const float* x, int incx, const float* y, int incy,
+                         float* result);
 cudaError_t icamax(iclblasHandle_t h, int n, const cfloat* x, int incx, int* result);
 
 // ---------------------------------------------------------------- level 2

@@ -13,6 +13,7 @@
 // 0-based first maximal index (tests/blas_reference/blas_reference.cpp:46-64)
 // exactly, for every n (no float-encoded indices).
 #include <climits>
+#include <mutex>
 
 #include "common.cuh"
 
@@ -487,6 +488,65 @@ cudaError_t sreduce(iclblasHandle_t h, Red op, int n, const float* x, int incx, 
     case Red::Nrm2: if (vec) LAUNCH(Red::Nrm2, true); else LAUNCH(Red::Nrm2, false); break;
     }
 #undef LAUNCH
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- SDOT without allocation
+// Fixed scratch of iclblasSdotNoAlloc: one FP64 partial per thread block and
+// the last-block ticket.  It is part of the library image, so every GPU that
+// loads the library holds it (32 KiB + 256 B) until the process exits.  In
+// host code `g_sdot_noalloc_scratch` names a host-side stand-in, not device
+// memory: host code must use the address from cudaGetSymbolAddress.
+struct SdotNoAllocScratch {
+    double partials[kSdotNoAllocMaxBlocks];
+    unsigned counter;
+};
+static __device__ __align__(256) SdotNoAllocScratch g_sdot_noalloc_scratch;
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+SdotNoAllocScratch* g_noalloc_addr[kMaxDevices] = {};
+
+// Device address of the scratch on `device`, looked up once per device with
+// that device current.
+cudaError_t noalloc_scratch_addr(int device, SdotNoAllocScratch** out)
+{
+    if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[device]) {
+        int cur = -1;
+        cudaError_t e = cudaGetDevice(&cur);
+        if (e != cudaSuccess) return e;
+        if (cur != device && (e = cudaSetDevice(device)) != cudaSuccess) return e;
+        void* ptr = nullptr;
+        e = cudaGetSymbolAddress(&ptr, g_sdot_noalloc_scratch);
+        if (cur != device) cudaSetDevice(cur);
+        if (e != cudaSuccess) return e;
+        g_noalloc_addr[device] = (SdotNoAllocScratch*)ptr;
+    }
+    *out = g_noalloc_addr[device];
+    return cudaSuccess;
+}
+}  // namespace
+
+cudaError_t sdot_noalloc(iclblasHandle_t h, int n, const float* x, int incx, const float* y, int incy, float* result)
+{
+    const bool vec = incx == 1 && aligned16(x) && incy == 1 && aligned16(y);
+    const int grid = l1_grid(h, vec ? ((long)n + 3) / 4 : n);
+    if (grid > kSdotNoAllocMaxBlocks) return cudaErrorNotSupported;
+    SdotNoAllocScratch* sc = nullptr;
+    cudaError_t e = noalloc_scratch_addr(h->device, &sc);
+    if (e != cudaSuccess) return e;
+    // the array keeps the previous call's contents: the ticket must start at 0
+    e = cudaMemsetAsync(&sc->counter, 0, sizeof(unsigned), h->stream);
+    if (e != cudaSuccess) return e;
+    if (vec)
+        sreduce_kernel<Red::Dot, true><<<grid, kThreads, 0, h->stream>>>(n, x, incx, y, incy, sc->partials,
+                                                                          &sc->counter, result);
+    else
+        sreduce_kernel<Red::Dot, false><<<grid, kThreads, 0, h->stream>>>(n, x, incx, y, incy, sc->partials,
+                                                                           &sc->counter, result);
     return cudaGetLastError();
 }
 

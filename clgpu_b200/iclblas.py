@@ -76,6 +76,7 @@ _SIGS = {
     "iclblasIsamax": [_H, _I, _P, _I, _P],
     "iclblasSasum": [_H, _I, _P, _I, _P],
     "iclblasSdot": [_H, _I, _P, _I, _P, _I, _P],
+    "iclblasSdotNoAlloc": [_H, _I, _P, _I, _P, _I, _P],
     "iclblasCscal": [_H, _I, _P, _P, _I],
     "iclblasCsscal": [_H, _I, _P, _P, _I],
     "iclblasCdotu": [_H, _I, _P, _I, _P, _I, _P],
@@ -218,6 +219,11 @@ def iclblasSasum(h, n, x, incx, result):
 
 def iclblasSdot(h, n, x, incx, y, incy, result):
     return _call("iclblasSdot", _h(h), n, ptr(x), incx, ptr(y), incy, ptr(result))
+
+
+def iclblasSdotNoAlloc(h, n, x, incx, y, incy, result):
+    """SDOT with no device allocation; device operands only (see include/iclBLAS.h)."""
+    return _call("iclblasSdotNoAlloc", _h(h), n, ptr(x), incx, ptr(y), incy, ptr(result))
 
 
 def iclblasCscal(h, n, alpha, x, incx):

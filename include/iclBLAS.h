@@ -104,6 +104,31 @@ ICLBLAS_API iclblasStatus_t iclblasIsamax(iclblasHandle_t handle, int n, float* 
 ICLBLAS_API iclblasStatus_t iclblasSasum(iclblasHandle_t handle, int n, float* x, int incx, float* result);
 /* replaces iclBLAS.h:371 */
 ICLBLAS_API iclblasStatus_t iclblasSdot(iclblasHandle_t handle, int n, float* x, int incx, float* y, int incy, float* result);
+/* No counterpart in the reference: SDOT that allocates no device memory.
+ * For callers that cannot call cudaMalloc: code whose device memory is owned
+ * by another allocator (a framework's caching pool that has reserved the free
+ * memory, so a private cudaMalloc would fail), and latency-critical paths
+ * that must not call cudaMalloc/cudaFree because those can synchronize the
+ * device and serialize with other host threads.  iclblasSdot may grow the
+ * handle's workspace with cudaMalloc/cudaFree; this variant instead keeps its
+ * scratch (one FP64 partial per thread block, at most 4096, and a ticket
+ * counter: 32 KiB + 256 B) in a fixed array compiled into the library, which
+ * every GPU that loads the library holds until the process exits.
+ *   - x, y and result must be device pointers (INVALID_VALUE otherwise:
+ *     staging host data would allocate); the call is asynchronous on the
+ *     handle's stream and its result equals iclblasSdot's;
+ *   - a call needing more than 4096 partials -- one per block, with
+ *     min(ceil(n/1024), 8 x SM count) blocks for unit-stride 16-byte-aligned
+ *     operands and min(ceil(n/256), 8 x SM count) otherwise -- returns
+ *     NOT_SUPPORTED;
+ *   - the first call on each device looks up the array's device address
+ *     (cudaGetSymbolAddress); make that first call before any stream capture;
+ *   - all calls share the one array, which keeps the previous call's
+ *     contents (the counter is cleared at the start of each call): calls that
+ *     overlap on the GPU (other streams or handles at the same time) race and
+ *     give wrong results, so serialize them. */
+ICLBLAS_API iclblasStatus_t iclblasSdotNoAlloc(iclblasHandle_t handle, int n, const float* x, int incx, const float* y,
+                                               int incy, float* result);
 
 /* ---- level 1, complex ---- */
 /* replaces iclBLAS.h:411 */
