@@ -351,6 +351,106 @@ def run_ours(args, rank, world, torch):
     return out
 
 
+# ---------------------------------------------------------------- GEMM precision study
+def run_gemm_study(args, torch):
+    """Precision config: SGEMM and CGEMM at M=N=K=n (default 8192), NN and
+    A^T*B, U(-1,1) (seed 2) plus a row-scaled variant (row i of A times
+    10^U(-4,4)); plain FP32 (CUDA cores) vs TF32 vs 3xBF16 vs 6xBF16 on the
+    tensor cores.  Error = ||C - C64||_F / ||C64||_F against an FP64 product of
+    the same FP32 inputs (torch float64 on the GPU, plumbing only); for the
+    row-scaled variant also the largest per-row relative error.  Throughput =
+    algorithmic 2MNK (8MNK complex) flops / CUDA-event time, device operands."""
+    from clgpu_b200 import iclblas as B
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    n = args.gemm_n
+    modes = [(B.MATH_PLAIN_FP32, "fp32_simt"), (B.MATH_TF32, "tf32"), (B.MATH_BF16X3, "3xbf16"),
+             (B.MATH_BF16X6, "6xbf16")]
+    stream = torch.cuda.Stream(device=dev)
+    g = torch.Generator(device=dev).manual_seed(2)
+    results = []
+    peak_bf16 = None
+    pp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pp):
+        peak_bf16 = json.load(open(pp)).get("bf16_tflops")
+    with B.Handle() as h, torch.cuda.stream(stream):
+        h.set_stream(stream)
+        for cplx in (False, True):
+            if cplx and args.skip_cgemm:
+                continue
+            dt = torch.complex64 if cplx else torch.float32
+            fl = (8.0 if cplx else 2.0) * n * n * n
+
+            def rnd(shape):
+                t = torch.rand(shape, generator=g, device=dev) * 2 - 1
+                if cplx:
+                    t = torch.complex(t, torch.rand(shape, generator=g, device=dev) * 2 - 1)
+                return t
+
+            A = rnd((n * n,))
+            Bm = rnd((n * n,))
+            for variant in ("uniform", "row_scaled"):
+                if variant == "row_scaled":
+                    if cplx:
+                        continue
+                    sc = 10.0 ** (torch.rand(n, generator=g, device=dev) * 8 - 4)
+                    # row i of op(A): A is column-major n x n, element (i, j) at j*n + i
+                    As = (A.view(n, n) * sc.view(1, n)).reshape(-1)
+                else:
+                    As = A
+                for ta in (0, 1):
+                    # FP64 reference of op(A) @ B (column-major views)
+                    Am = As.view(n, n).t()             # Am[i, j] = As[j*n + i]
+                    opA = Am if ta == 0 else Am.t()
+                    Bmat = Bm.view(n, n).t()
+                    ref = (opA.to(torch.complex128 if cplx else torch.float64)
+                           @ Bmat.to(torch.complex128 if cplx else torch.float64))
+                    refn = torch.linalg.norm(ref).item()
+                    for mode, name in modes:
+                        if cplx and mode == B.MATH_PLAIN_FP32 and args.quick:
+                            continue
+                        h.set_math_mode(mode)
+                        Cm = torch.empty(n * n, dtype=dt, device=dev)
+                        call = (B.iclblasCgemm if cplx else B.iclblasSgemm)
+                        one = 1.0 + 0j if cplx else 1.0
+                        zero = 0.0
+                        for _ in range(1):
+                            B.check(call(h, ta, 0, n, n, n, one, As, n, Bm, n, zero, Cm, n), name)
+                        torch.cuda.synchronize()
+                        reps = 3
+                        e0 = torch.cuda.Event(enable_timing=True)
+                        e1 = torch.cuda.Event(enable_timing=True)
+                        e0.record(stream)
+                        for _ in range(reps):
+                            B.check(call(h, ta, 0, n, n, n, one, As, n, Bm, n, zero, Cm, n), name)
+                        e1.record(stream)
+                        torch.cuda.synchronize()
+                        ms = e0.elapsed_time(e1) / reps
+                        Cmat = Cm.view(n, n).t().to(ref.dtype)
+                        err = (torch.linalg.norm(Cmat - ref).item()) / refn
+                        row_err = None
+                        if variant == "row_scaled":
+                            rerr = torch.linalg.norm(Cmat - ref, dim=1) / torch.linalg.norm(ref, dim=1)
+                            row_err = rerr.max().item()
+                        r = {"routine": "cgemm" if cplx else "sgemm", "variant": variant,
+                             "op": "NN" if ta == 0 else "TN", "mode": name, "n": n,
+                             "tflops": round(fl / (ms / 1e3) / 1e12, 2), "ms": round(ms, 3),
+                             "rel_fro_err_vs_fp64": err}
+                        if row_err is not None:
+                            r["max_row_rel_err"] = row_err
+                        if mode != B.MATH_PLAIN_FP32 and peak_bf16:
+                            nprod = {B.MATH_TF32: 1, B.MATH_BF16X3: 3, B.MATH_BF16X6: 6}[mode]
+                            exec_tf = nprod * fl / (ms / 1e3) / 1e12
+                            r["tensor_tflops_executed"] = round(exec_tf, 1)
+                            if mode != B.MATH_TF32:
+                                r["frac_of_bf16_peak_executed"] = round(exec_tf / peak_bf16, 3)
+                        print(json.dumps(r), flush=True)
+                        results.append(r)
+                        del Cm
+                    del ref
+    return results
+
+
 # ---------------------------------------------------------------- CPU (reference code)
 SAMPLE_N1 = 1 << 24
 SAMPLE_GN = 4096
@@ -451,6 +551,11 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-operand (C ABI) leg")
     ap.add_argument("--only", default="", help="comma-separated subset of the sweep's calls")
     ap.add_argument("--n1", type=int, default=N1, help="level-1 vector length (default 2^28)")
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "gemm"],
+                    help="sweep: the bandwidth config (default); gemm: the precision config study")
+    ap.add_argument("--gemm-n", type=int, default=8192)
+    ap.add_argument("--skip-cgemm", action="store_true")
+    ap.add_argument("--quick", action="store_true")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -480,6 +585,9 @@ def main():
         return
 
     import torch
+    if args.workload == "gemm":
+        run_gemm_study(args, torch)
+        return
     if world > 1:
         torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     out = run_ours(args, rank, world, torch)

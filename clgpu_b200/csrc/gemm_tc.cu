@@ -1,0 +1,696 @@
+// Tensor-core GEMM for the TF32 / 3xBF16 / 6xBF16 math modes (sm_100a).
+//
+// C = alpha*op(A)*op(B) + beta*C in FP32 (and complex FP32) computed on the
+// 5th-generation tensor cores.  No reference counterpart: the reference's
+// GEMMs are FP32 SIMD kernels; this is the split-precision mode of the
+// north_star.
+//
+// 1. Pre-pass (split kernel): each operand op(X) is rewritten K-major (row r
+//    holds its K values contiguously, zero-padded to a multiple of the
+//    K block) as
+//      TF32:  one FP32 plane rounded to TF32 (cvt.rna.tf32.f32);
+//      BF16:  hi = bf16(x), mid = bf16(x - hi), lo = bf16(x - hi - mid)
+//             (each difference is exact in FP32).
+//    Complex operands are embedded in a real GEMM with the same flop count:
+//    A' = [re A | im A] (M x 2K) and, for each column j of op(B), the rows
+//    2j = [re b_j | -im b_j] and 2j+1 = [im b_j | re b_j] of B'' (2N x 2K), so
+//    C'' = A' B''^T holds re C(:,j) in column 2j and im C(:,j) in 2j+1.
+// 2. Main kernel: persistent, one CTA per SM, CTA tile 128 x 256, 6 warps:
+//      warp 0     TMA producer: 128-byte-swizzled tiles of the split planes
+//                 into a 4-stage shared-memory ring (mbarrier expect-tx);
+//      warp 1     allocates 512 TMEM columns (two 128x256 FP32 accumulators)
+//                 and one thread issues tcgen05.mma (M=128, N=256, K=32 bytes
+//                 per instruction, 4 per stage) and tcgen05.commit;
+//      warps 2-9  epilogue: two warps per 32-lane TMEM quarter, 128 columns
+//                 each.  They drain the accumulator into FP32 registers
+//                 once per chunk of K blocks and store alpha*sum + beta*C
+//                 (coalesced column-major) at the end of the tile.
+//    Each pipeline stage is one (K block, product) pair.  The BF16 modes run
+//    the products of every K block small-first -- 3xBF16: mid*hi, hi*mid,
+//    hi*hi; 6xBF16: lo*hi, hi*lo, mid*mid, mid*hi, hi*mid, hi*hi -- into a
+//    fresh accumulator per chunk of one K block.  The tensor core's FP32
+//    accumulation loses a fraction of an ulp of the running value at every
+//    update; starting each chunk from zero and adding the largest term last
+//    keeps that loss at the chunk's size, and the chunks are summed in FP32
+//    in registers (the two accumulator buffers let the next chunk's MMAs run
+//    while the previous chunk is drained).  TF32 uses one chunk per tile.
+// Every mbarrier wait is bounded; on timeout the kernel records
+// kDevWaitTimeout, waits (bounded) for its own TMA copies, frees TMEM and
+// returns.  No cluster multicast is used.
+#include <cuda.h>
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <mutex>
+#include <type_traits>
+
+#include "common.cuh"
+
+namespace iclb {
+namespace tc {
+namespace {
+
+constexpr int BM = 128;
+constexpr int BN = 256;
+constexpr int STAGES = 4;
+constexpr int ROW_BYTES = 128;                  // one K block per tile row
+constexpr int A_TILE = BM * ROW_BYTES;          // 16 KiB
+constexpr int B_TILE = BN * ROW_BYTES;          // 32 KiB
+constexpr int STAGE_BYTES = A_TILE + B_TILE;    // 48 KiB
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*barriers*/ + 1024 /*alignment*/;
+constexpr int EPI_WARPS = 8;                    // two per TMEM lane quarter
+constexpr int THREADS = 64 + 32 * EPI_WARPS;    // producer, MMA, epilogue
+constexpr int GROUP_M = 16;                     // tile raster: 16 M-tiles per band
+constexpr unsigned long long kWaitNs = 2000000000ull;  // a wait gives up after 2 s
+
+struct Params {
+    int M, N;          // output rows / columns of the (real) GEMM
+    int kblocks;       // K_pad / elements-per-row-block
+    int nprod;         // products per K block (1, 3 or 6)
+    int chunk;         // K blocks per TMEM chunk (drained into registers)
+    int pa[6], pb[6];  // split level of A and B for each product
+    int complex_out;   // columns come in (re, im) pairs
+    float alpha_re, alpha_im, beta_re, beta_im;
+    float* C;
+    long ldc;          // in elements of the output type
+    int* status;
+};
+
+// ---------------------------------------------------------------- PTX helpers
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait: false when 2 s passed or another role gave up.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    while (!mbar_try_wait(bar, parity)) {
+        if (*abort_flag) return false;
+        if (global_ns() - t0 > kWaitNs) {
+            *abort_flag = 1;
+            return false;
+        }
+    }
+    return true;
+}
+
+// Wait without the abort shortcut, bounded by 2 s (drains own async work).
+__device__ __forceinline__ void mbar_drain(uint64_t* bar, uint32_t parity)
+{
+    const unsigned long long t0 = global_ns();
+    while (!mbar_try_wait(bar, parity) && global_ns() - t0 < kWaitNs) {}
+}
+
+__device__ __forceinline__ void tma_load_2d(void* smem_dst, const CUtensorMap* map, int x, int y, uint64_t* bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        ::"r"(smem_u32(smem_dst)), "l"((uint64_t)map), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void tmem_alloc(uint32_t* dst_smem, uint32_t ncols)
+{
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst_smem)),
+                 "r"(ncols));
+}
+__device__ __forceinline__ void tmem_relinquish()
+{
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols)
+{
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols));
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+template <bool TF32>
+__device__ __forceinline__ void umma(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                     uint32_t accumulate)
+{
+    if (TF32) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}"
+            ::"r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+    } else {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+            ::"r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+    }
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+// 32 lanes x 32 consecutive columns of FP32 from TMEM (one column per register).
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v)
+{
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Shared-memory matrix descriptor, K-major, 128-byte swizzle: rows of 128 B,
+// 8-row groups 1024 B apart (SBO), version 1, layout type 2.
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t saddr)
+{
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)1u << 16;           // leading byte offset (unused for swizzled K-major)
+    d |= (uint64_t)(1024u >> 4) << 32; // stride byte offset: next 8-row group
+    d |= (uint64_t)1u << 46;           // descriptor version
+    d |= (uint64_t)2u << 61;           // SWIZZLE_128B
+    return d;
+}
+
+// Instruction descriptor: FP32 accumulator, A/B format (1 = BF16, 2 = TF32),
+// both K-major, N = 256, M = 128.
+__host__ __device__ constexpr uint32_t instr_desc(uint32_t ab_format)
+{
+    return (1u << 4) | (ab_format << 7) | (ab_format << 10) | ((uint32_t)(BN >> 3) << 17) |
+           ((uint32_t)(BM >> 4) << 24);
+}
+
+__device__ __forceinline__ void tile_coords(int t, int tiles_m, int tiles_n, int& tm, int& tn)
+{
+    const int per_band = GROUP_M * tiles_n;
+    const int band = t / per_band;
+    const int first_m = band * GROUP_M;
+    const int rows = min(GROUP_M, tiles_m - first_m);
+    const int in_band = t - band * per_band;
+    tm = first_m + in_band % rows;
+    tn = in_band / rows;
+}
+
+template <bool TF32>
+__global__ void __launch_bounds__(THREADS, 1)
+    gemm_tc_kernel(const __grid_constant__ CUtensorMap mA0, const __grid_constant__ CUtensorMap mA1,
+                   const __grid_constant__ CUtensorMap mA2, const __grid_constant__ CUtensorMap mB0,
+                   const __grid_constant__ CUtensorMap mB1, const __grid_constant__ CUtensorMap mB2, Params p)
+{
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint8_t* tiles = smem;
+    uint64_t* full = (uint64_t*)(smem + STAGES * STAGE_BYTES);
+    uint64_t* empty = full + STAGES;
+    uint64_t* tfull = empty + STAGES;
+    uint64_t* tempty = tfull + 2;
+    uint32_t* tmem_slot = (uint32_t*)(tempty + 2);
+    volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
+
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const int tiles_m = (p.M + BM - 1) / BM, tiles_n = (p.N + BN - 1) / BN;
+    const int ntiles = tiles_m * tiles_n;
+    const int steps = p.kblocks * p.nprod;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(&tfull[a], 1);
+            mbar_init(&tempty[a], EPI_WARPS);  // one arrive per epilogue warp
+        }
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        tmem_alloc(tmem_slot, 512);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+
+    if (warp == 0) {
+        // ---------------------------------------------------------- TMA producer
+        if (lane == 0) {
+            const CUtensorMap* ma[3] = {&mA0, &mA1, &mA2};
+            const CUtensorMap* mb[3] = {&mB0, &mB1, &mB2};
+            int s = 0;
+            uint32_t ph = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+                int tm, tn;
+                tile_coords(t, tiles_m, tiles_n, tm, tn);
+                for (int st = 0; st < steps && ok; ++st) {
+                    const int kb = st / p.nprod, pr = st % p.nprod;
+                    if (!mbar_wait(&empty[s], ph ^ 1, abort_flag)) { ok = false; break; }
+                    uint8_t* sa = tiles + s * STAGE_BYTES;
+                    uint8_t* sb = sa + A_TILE;
+                    mbar_expect_tx(&full[s], STAGE_BYTES);
+                    const int kx = kb * (TF32 ? 32 : 64);
+                    tma_load_2d(sa, ma[p.pa[pr]], kx, tm * BM, &full[s]);
+                    tma_load_2d(sb, mb[p.pb[pr]], kx, tn * BN, &full[s]);
+                    if (++s == STAGES) { s = 0; ph ^= 1; }
+                }
+            }
+            if (!ok) {
+                // wait (bounded) for the copies this thread issued, then leave
+                for (int i = 0; i < STAGES; ++i) mbar_drain(&full[(s + i) % STAGES], ph);
+            }
+        }
+    } else if (warp == 1) {
+        // ---------------------------------------------------------- MMA issuer
+        if (lane == 0) {
+            const uint32_t idesc = instr_desc(TF32 ? 2u : 1u);
+            int s = 0;
+            uint32_t ph = 0;
+            int acc = 0;
+            uint32_t acc_ph = 0;
+            bool ok = true;
+            const int chunk_steps = p.chunk * p.nprod;
+            for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+                for (int c0 = 0; c0 < steps && ok; c0 += chunk_steps) {
+                    if (!mbar_wait(&tempty[acc], acc_ph ^ 1, abort_flag)) { ok = false; break; }
+                    tc_fence_after();
+                    const uint32_t d = tmem_base + (uint32_t)(acc * BN);
+                    const int c1 = min(steps, c0 + chunk_steps);
+                    for (int st = c0; st < c1; ++st) {
+                        if (!mbar_wait(&full[s], ph, abort_flag)) { ok = false; break; }
+                        tc_fence_after();
+                        const uint32_t sa = smem_u32(tiles + s * STAGE_BYTES);
+                        const uint32_t sb = sa + A_TILE;
+                        const uint64_t da = smem_desc_sw128(sa), db = smem_desc_sw128(sb);
+#pragma unroll
+                        for (int kk = 0; kk < 4; ++kk)  // 4 x 32 bytes of K per stage
+                            umma<TF32>(d, da + (uint64_t)(2 * kk), db + (uint64_t)(2 * kk), idesc,
+                                       (st > c0 || kk > 0) ? 1u : 0u);
+                        umma_commit(&empty[s]);
+                        if (++s == STAGES) { s = 0; ph ^= 1; }
+                    }
+                    // chunk done (or aborted): the epilogue may read this accumulator
+                    umma_commit(&tfull[acc]);
+                    if (!ok) {
+                        mbar_drain(&tfull[acc], acc_ph);  // every issued MMA done before TMEM is freed
+                        break;
+                    }
+                    if (++acc == 2) { acc = 0; acc_ph ^= 1; }
+                }
+            }
+        }
+    } else {
+        // ---------------------------------------------------------- epilogue
+        const int ew = warp - 2;
+        const int q = warp & 3;             // TMEM lane quarter this warp may access
+        const int half = ew / 4;            // columns [half*128, half*128+128) of the tile
+        const int nchunks = (p.kblocks + p.chunk - 1) / p.chunk;
+        int acc = 0;
+        uint32_t acc_ph = 0;
+        bool ok = true;
+        for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+            int tm, tn;
+            tile_coords(t, tiles_m, tiles_n, tm, tn);
+            float sum[128];
+#pragma unroll
+            for (int j = 0; j < 128; ++j) sum[j] = 0.f;
+            for (int c = 0; c < nchunks; ++c) {
+                int w = 1;
+                if (lane == 0) w = mbar_wait(&tfull[acc], acc_ph, abort_flag) ? 1 : 0;
+                ok = __shfl_sync(0xffffffffu, w, 0) != 0;
+                if (!ok) break;
+                tc_fence_after();
+                const uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN + half * 128);
+#pragma unroll
+                for (int g = 0; g < 4; ++g) {
+                    float v[32];
+                    tmem_ld32(taddr + (uint32_t)(g * 32), v);
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) sum[g * 32 + j] += v[j];
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&tempty[acc]);
+                if (++acc == 2) { acc = 0; acc_ph ^= 1; }
+            }
+            if (!ok) break;
+            const int row = tm * BM + q * 32 + lane;
+            const int col0 = tn * BN + half * 128;
+            const bool beta_zero = p.beta_re == 0.f && p.beta_im == 0.f;
+            if (row < p.M) {
+                if (!p.complex_out) {
+#pragma unroll
+                    for (int j = 0; j < 128; ++j) {
+                        const int col = col0 + j;
+                        if (col < p.N) {
+                            float* cp = p.C + (long)col * p.ldc + row;
+                            *cp = beta_zero ? __fmul_rn(p.alpha_re, sum[j])
+                                            : fmaf(p.alpha_re, sum[j], __fmul_rn(p.beta_re, *cp));
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 128; j += 2) {
+                        if (col0 + j < p.N) {
+                            float2* cp = (float2*)p.C + (long)((col0 + j) >> 1) * p.ldc + row;
+                            const float re = sum[j], im = sum[j + 1];
+                            float2 r;
+                            r.x = fmaf(p.alpha_re, re, -p.alpha_im * im);
+                            r.y = fmaf(p.alpha_re, im, p.alpha_im * re);
+                            if (!beta_zero) {
+                                const float2 cv = *cp;
+                                r.x += fmaf(p.beta_re, cv.x, -p.beta_im * cv.y);
+                                r.y += fmaf(p.beta_re, cv.y, p.beta_im * cv.x);
+                            }
+                            *cp = r;
+                        }
+                    }
+                }
+            }
+        }
+    }
+
+    __syncthreads();
+    if (threadIdx.x == 0 && *abort_flag) atomicOr(p.status, (int)kDevWaitTimeout);
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tmem_base, 512);
+    }
+}
+
+// ---------------------------------------------------------------- split pre-pass
+// Logical operand L (R x K): L[r][k] = S[r*rs + k*ks] (conj if requested).
+// Output planes are K-major with row pitch kpad elements.
+// Real:    plane[l][r*kpad + k]            (k >= K: zero)
+// Complex A: plane[l][r*kpad + k] = re, [r*kpad + K + k] = im       (kpad >= 2K)
+// Complex B: plane[l][(2r)*kpad + k] = re, [(2r)*kpad + K + k] = -im,
+//            plane[l][(2r+1)*kpad + k] = im, [(2r+1)*kpad + K + k] = re
+enum SplitMode { kReal = 0, kCplxA = 1, kCplxB = 2 };
+
+__device__ __forceinline__ void split3(float x, __nv_bfloat16& hi, __nv_bfloat16& mid, __nv_bfloat16& lo)
+{
+    hi = __float2bfloat16_rn(x);
+    const float r1 = x - __bfloat162float(hi);
+    mid = __float2bfloat16_rn(r1);
+    const float r2 = r1 - __bfloat162float(mid);
+    lo = __float2bfloat16_rn(r2);
+}
+
+__device__ __forceinline__ float to_tf32(float x)
+{
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
+struct SplitOut {
+    void* plane[3];
+    int nlev;  // planes to write (TF32: 1 FP32 plane)
+    int tf32;
+    long kpad;
+};
+
+__device__ __forceinline__ void put(const SplitOut& o, long idx, float x)
+{
+    if (o.tf32) {
+        ((float*)o.plane[0])[idx] = to_tf32(x);
+        return;
+    }
+    __nv_bfloat16 h, m, l;
+    split3(x, h, m, l);
+    ((__nv_bfloat16*)o.plane[0])[idx] = h;
+    if (o.nlev > 1) ((__nv_bfloat16*)o.plane[1])[idx] = m;
+    if (o.nlev > 2) ((__nv_bfloat16*)o.plane[2])[idx] = l;
+}
+
+// 32 x 32 tile of L per block (blockDim 32 x 8), transposed through shared
+// memory when the source is contiguous along r, so that both the reads of S
+// and the K-contiguous writes are coalesced.
+template <class T>
+__global__ void __launch_bounds__(256) split_kernel(int R, int K, const T* __restrict__ S, long rs, long ks, int conj,
+                                                    int mode, SplitOut o)
+{
+    __shared__ T tile[32][33];
+    const int k0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    // load tile[rr][kk] = L[r0+rr][k0+kk]
+    if (rs == 1) {  // contiguous along r
+        for (int kk = ty; kk < 32; kk += 8) {
+            const int r = r0 + tx, k = k0 + kk;
+            T v{};
+            if (r < R && k < K) v = S[(long)r + (long)k * ks];
+            tile[tx][kk] = v;
+        }
+    } else {
+        for (int rr = ty; rr < 32; rr += 8) {
+            const int r = r0 + rr, k = k0 + tx;
+            T v{};
+            if (r < R && k < K) v = S[(long)r * rs + (long)k];
+            tile[rr][tx] = v;
+        }
+    }
+    __syncthreads();
+    for (int rr = ty; rr < 32; rr += 8) {
+        const int r = r0 + rr, k = k0 + tx;
+        if (r >= R) continue;
+        const T v = tile[rr][tx];
+        if constexpr (sizeof(T) == sizeof(float)) {
+            // real: K is padded to a multiple of the block by the grid; k >= K writes zeros
+            if (k < o.kpad) put(o, (long)r * o.kpad + k, k < K ? (float)*(const float*)&v : 0.f);
+        } else {
+            const float re = ((const float*)&v)[0];
+            const float im = (conj ? -1.f : 1.f) * ((const float*)&v)[1];
+            if (k >= K) continue;
+            if (mode == kCplxA) {
+                put(o, (long)r * o.kpad + k, re);
+                put(o, (long)r * o.kpad + K + k, im);
+            } else {
+                put(o, (long)(2 * r) * o.kpad + k, re);
+                put(o, (long)(2 * r) * o.kpad + K + k, -im);
+                put(o, (long)(2 * r + 1) * o.kpad + k, im);
+                put(o, (long)(2 * r + 1) * o.kpad + K + k, re);
+            }
+        }
+    }
+}
+
+// zero the K padding columns [kfrom, kpad) of every row (complex layouts)
+__global__ void zero_pad_kernel(long rows, long kfrom, SplitOut o)
+{
+    const long w = o.kpad - kfrom;
+    const long total = rows * w;
+    for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+        const long r = e / w, k = kfrom + e % w;
+        const long idx = r * o.kpad + k;
+        if (o.tf32) ((float*)o.plane[0])[idx] = 0.f;
+        else
+            for (int l = 0; l < o.nlev; ++l) ((__nv_bfloat16*)o.plane[l])[idx] = __float2bfloat16_rn(0.f);
+    }
+}
+
+// ---------------------------------------------------------------- host side
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn()
+{
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+    });
+    return fn;
+}
+
+bool make_map(CUtensorMap* m, void* base, bool tf32, long rows, long kpad, int box_rows)
+{
+    EncodeTiledFn f = encode_fn();
+    if (!f) return false;
+    const int esize = tf32 ? 4 : 2;
+    cuuint64_t dims[2] = {(cuuint64_t)kpad, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)(kpad * esize)};
+    cuuint32_t box[2] = {(cuuint32_t)(ROW_BYTES / esize), (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = f(m, tf32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims,
+                   strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+struct ModeInfo {
+    bool tf32;
+    int nlev;
+    int nprod;
+    int pa[6], pb[6];
+};
+
+ModeInfo mode_info(iclblasMathMode_t mode)
+{
+    ModeInfo mi{};
+    if (mode == ICLBLAS_MATH_TF32) {
+        mi.tf32 = true;
+        mi.nlev = 1;
+        mi.nprod = 1;
+        mi.pa[0] = mi.pb[0] = 0;
+    } else if (mode == ICLBLAS_MATH_BF16X3) {
+        mi.nlev = 2;
+        mi.nprod = 3;  // mid*hi, hi*mid, hi*hi: smallest first (levels: 0 hi, 1 mid)
+        const int a[3] = {1, 0, 0}, b[3] = {0, 1, 0};
+        for (int i = 0; i < 3; ++i) { mi.pa[i] = a[i]; mi.pb[i] = b[i]; }
+    } else {
+        mi.nlev = 3;
+        mi.nprod = 6;  // lo*hi, hi*lo, mid*mid, mid*hi, hi*mid, hi*hi: smallest first
+        const int a[6] = {2, 0, 1, 1, 0, 0}, b[6] = {0, 2, 1, 0, 1, 0};
+        for (int i = 0; i < 6; ++i) { mi.pa[i] = a[i]; mi.pb[i] = b[i]; }
+    }
+    return mi;
+}
+
+template <class T>
+cudaError_t run_split(iclblasHandle_t h, const T* S, int R, int K, long rs, long ks, int conj, int mode,
+                      const SplitOut& o, long out_rows)
+{
+    const int kgrid = std::is_same<T, float>::value ? (int)(o.kpad / 32) : ceil_div(K, 32);
+    dim3 grid(kgrid, ceil_div(R, 32));
+    split_kernel<T><<<grid, dim3(32, 8), 0, h->stream>>>(R, K, S, rs, ks, conj, mode, o);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if (!std::is_same<T, float>::value && o.kpad > 2L * K) {
+        const long total = out_rows * (o.kpad - 2L * K);
+        const int g = (int)std::min<long>((total + 255) / 256, (long)h->sm_count * 8);
+        zero_pad_kernel<<<g, 256, 0, h->stream>>>(out_rows, 2L * K, o);
+        e = cudaGetLastError();
+    }
+    return e;
+}
+
+}  // namespace
+
+// Real or complex GEMM on the tensor cores.  `cplx` selects complex operands
+// (T = cfloat); the real GEMM then has M rows, 2N columns and 2K depth.
+template <class T>
+cudaError_t gemm_tc(iclblasHandle_t h, int ta, int tb, int m, int n, int k, T alpha, const T* A, int lda,
+                    const T* B, int ldb, T beta, T* C, int ldc)
+{
+    constexpr bool cplx = sizeof(T) == sizeof(cfloat);
+    const ModeInfo mi = mode_info(h->math);
+    const int esize = mi.tf32 ? 4 : 2;
+    const int kblk = ROW_BYTES / esize;
+    const long kreal = cplx ? 2L * k : (long)k;
+    const long kpad = (kreal + kblk - 1) / kblk * kblk;
+    const long rows_a = m, rows_b = cplx ? 2L * n : (long)n;
+    const size_t plane_a = (size_t)rows_a * kpad * esize, plane_b = (size_t)rows_b * kpad * esize;
+    const size_t align = 1024;
+    const size_t pa_al = (plane_a + align - 1) / align * align, pb_al = (plane_b + align - 1) / align * align;
+    char* ws = (char*)scratch(h, (pa_al + pb_al) * mi.nlev);
+    if (!ws) return cudaErrorMemoryAllocation;
+    SplitOut oa{}, ob{};
+    oa.nlev = ob.nlev = mi.nlev;
+    oa.tf32 = ob.tf32 = mi.tf32 ? 1 : 0;
+    oa.kpad = ob.kpad = kpad;
+    for (int l = 0; l < mi.nlev; ++l) {
+        oa.plane[l] = ws + l * pa_al;
+        ob.plane[l] = ws + mi.nlev * pa_al + l * pb_al;
+    }
+    // A: L[r=m][k] ; op N: S[m + k*lda] ; op T/C: S[k + m*lda]
+    const bool at = ta != ICLBLAS_OP_N, bt = tb != ICLBLAS_OP_N;
+    cudaError_t e = run_split<T>(h, A, m, k, at ? lda : 1, at ? 1 : lda, ta == ICLBLAS_OP_C, kCplxA, oa, rows_a);
+    if (e != cudaSuccess) return e;
+    // B: L[r=n][k] = op(B)[k][n] ; op N: S[k + n*ldb] ; op T/C: S[n + k*ldb]
+    e = run_split<T>(h, B, n, k, bt ? 1 : ldb, bt ? ldb : 1, tb == ICLBLAS_OP_C, kCplxB, ob, rows_b);
+    if (e != cudaSuccess) return e;
+
+    CUtensorMap ma[3], mb[3];
+    for (int l = 0; l < 3; ++l) {
+        const int ll = l < mi.nlev ? l : 0;
+        if (!make_map(&ma[l], oa.plane[ll], mi.tf32, rows_a, kpad, BM)) return cudaErrorInvalidValue;
+        if (!make_map(&mb[l], ob.plane[ll], mi.tf32, rows_b, kpad, BN)) return cudaErrorInvalidValue;
+    }
+    Params p{};
+    p.M = m;
+    p.N = (int)rows_b;
+    p.kblocks = (int)(kpad / kblk);
+    p.nprod = mi.nprod;
+    // BF16 modes drain the accumulator every K block; TF32 accumulates the
+    // whole K in TMEM (its operand rounding dominates its error)
+    p.chunk = mi.tf32 ? p.kblocks : 1;
+    for (int i = 0; i < 6; ++i) { p.pa[i] = mi.pa[i]; p.pb[i] = mi.pb[i]; }
+    p.complex_out = cplx ? 1 : 0;
+    const float* al = (const float*)&alpha;
+    const float* be = (const float*)&beta;
+    p.alpha_re = al[0];
+    p.alpha_im = cplx ? al[1] : 0.f;
+    p.beta_re = be[0];
+    p.beta_im = cplx ? be[1] : 0.f;
+    p.C = (float*)C;
+    p.ldc = ldc;
+    p.status = h->ws.dev_status;
+
+    const int tiles = ceil_div(m, BM) * ceil_div((long)rows_b, BN);
+    const int grid = std::min(tiles, h->sm_count);
+    if (mi.tf32) {
+        e = cudaFuncSetAttribute(gemm_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+        if (e != cudaSuccess) return e;
+        gemm_tc_kernel<true><<<grid, THREADS, SMEM_BYTES, h->stream>>>(ma[0], ma[1], ma[2], mb[0], mb[1], mb[2], p);
+    } else {
+        e = cudaFuncSetAttribute(gemm_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+        if (e != cudaSuccess) return e;
+        gemm_tc_kernel<false><<<grid, THREADS, SMEM_BYTES, h->stream>>>(ma[0], ma[1], ma[2], mb[0], mb[1], mb[2],
+                                                                         p);
+    }
+    return cudaGetLastError();
+}
+
+template cudaError_t gemm_tc<float>(iclblasHandle_t, int, int, int, int, int, float, const float*, int, const float*,
+                                    int, float, float*, int);
+template cudaError_t gemm_tc<cfloat>(iclblasHandle_t, int, int, int, int, int, cfloat, const cfloat*, int,
+                                     const cfloat*, int, cfloat, cfloat*, int);
+
+}  // namespace tc
+}  // namespace iclb

@@ -1,0 +1,102 @@
+"""Tensor-core GEMM modes (TF32, 3xBF16, 6xBF16) on the GPU against the FP64 oracle.
+
+These modes have no reference counterpart; they are pinned to the FP64
+oracle (orc_dgemm, the same arithmetic as the FP32 oracle in double).  Error
+bars (relative Frobenius, U(-1,1) data, K <= 513): TF32 <= 2e-3 (10-bit
+mantissa operands), 3xBF16 <= 3e-5 (three leading split products; the
+dropped terms are ~2^-16 relative), 6xBF16 <= 2e-6 (FP32 level; measured
+2.2e-7 at 8192^3 where the plain FP32 path gives 1.6e-6).
+"""
+import numpy as np
+import pytest
+
+import oracle_lib as O
+from clgpu_b200 import iclblas as B
+
+pytestmark = pytest.mark.gpu
+
+BARS = {B.MATH_TF32: 2e-3, B.MATH_BF16X3: 3e-5, B.MATH_BF16X6: 2e-6}
+
+
+def _shape(op, rows, cols):
+    return (rows, cols) if op == 0 else (cols, rows)
+
+
+def _dref(ta, tb, m, n, k, alpha, A, lda, Bm, ldb, beta, Cm, ldc):
+    Cd = Cm.astype(np.float64)
+    O.dgemm(ta, tb, m, n, k, alpha, A.astype(np.float64), lda, Bm.astype(np.float64), ldb, beta, Cd, ldc)
+    return Cd
+
+
+@pytest.mark.parametrize("mode", [B.MATH_TF32, B.MATH_BF16X3, B.MATH_BF16X6])
+@pytest.mark.parametrize("ta,tb", [(0, 0), (1, 0), (0, 1), (1, 1)])
+@pytest.mark.parametrize("mnk", [(1, 1, 1), (100, 7, 33), (129, 257, 64), (300, 300, 513), (256, 512, 256)])
+def test_sgemm_tensor_core_modes(handle, mode, ta, tb, mnk):
+    m, n, k = mnk
+    rng = np.random.default_rng(m * 7 + n * 3 + k + 100 * ta + 10 * tb + mode)
+    ar, ac = _shape(ta, m, k)
+    br, bc = _shape(tb, k, n)
+    lda, ldb, ldc = ar + 3, br + 1, m + 2
+    A = O.colmajor(ar, ac, lda, rng)
+    Bm = O.colmajor(br, bc, ldb, rng)
+    Cm = O.colmajor(m, n, ldc, rng)
+    ref = _dref(ta, tb, m, n, k, 1.25, A, lda, Bm, ldb, -0.5, Cm, ldc)
+    handle.set_math_mode(mode)
+    assert B.iclblasSgemm(handle, ta, tb, m, n, k, 1.25, A, lda, Bm, ldb, -0.5, Cm, ldc) == B.SUCCESS
+    err = O.rel_fro(Cm.reshape(n, ldc)[:, :m], ref.reshape(n, ldc)[:, :m])
+    assert err <= BARS[mode], err
+    # padding rows of C untouched
+    assert np.array_equal(Cm.reshape(n, ldc)[:, m:], ref.reshape(n, ldc)[:, m:].astype(np.float32))
+
+
+@pytest.mark.parametrize("mode", [B.MATH_TF32, B.MATH_BF16X3, B.MATH_BF16X6])
+def test_sgemm_tensor_core_beta0_ignores_c(handle, mode):
+    m, n, k = 200, 300, 96
+    rng = np.random.default_rng(5)
+    A = O.colmajor(m, k, m, rng)
+    Bm = O.colmajor(k, n, k, rng)
+    Cm = np.full(m * n, np.nan, np.float32)
+    ref = _dref(0, 0, m, n, k, 2.0, A, m, Bm, k, 0.0, np.zeros(m * n, np.float32), m)
+    handle.set_math_mode(mode)
+    assert B.iclblasSgemm(handle, 0, 0, m, n, k, 2.0, A, m, Bm, k, 0.0, Cm, m) == B.SUCCESS
+    assert np.all(np.isfinite(Cm))
+    assert O.rel_fro(Cm, ref) <= BARS[mode]
+
+
+@pytest.mark.parametrize("mode", [B.MATH_TF32, B.MATH_BF16X3, B.MATH_BF16X6])
+@pytest.mark.parametrize("ta,tb", [(0, 0), (2, 0), (1, 2)])
+def test_cgemm_tensor_core_modes(handle, mode, ta, tb):
+    m, n, k = 150, 130, 77
+    rng = np.random.default_rng(ta * 3 + tb + mode)
+    ar, ac = _shape(ta, m, k)
+    br, bc = _shape(tb, k, n)
+    A = O.colmajor(ar, ac, ar, rng, np.complex64)
+    Bm = O.colmajor(br, bc, br, rng, np.complex64)
+    Cm = O.colmajor(m, n, m + 1, rng, np.complex64)
+    al, be = 0.75 - 0.5j, 0.25 + 0.5j
+    # FP64 reference with numpy (complex128) on the same op semantics
+    Ad = A.astype(np.complex128).reshape(ac, ar).T
+    Bd = Bm.astype(np.complex128).reshape(bc, br).T
+    opA = Ad if ta == 0 else (Ad.T if ta == 1 else Ad.conj().T)
+    opB = Bd if tb == 0 else (Bd.T if tb == 1 else Bd.conj().T)
+    Cd = Cm.astype(np.complex128).reshape(n, m + 1).T[:m]
+    ref = al * (opA @ opB) + be * Cd
+    handle.set_math_mode(mode)
+    assert B.iclblasCgemm(handle, ta, tb, m, n, k, al, A, ar, Bm, br, be, Cm, m + 1) == B.SUCCESS
+    got = Cm.reshape(n, m + 1).T[:m]
+    assert O.rel_fro(got, ref) <= BARS[mode]
+
+
+def test_plain_mode_unchanged_after_tc(handle):
+    """Switching back to PLAIN_FP32 restores the bit-exact CUDA-core path."""
+    m, n, k = 64, 48, 40
+    rng = np.random.default_rng(8)
+    A = O.colmajor(m, k, m, rng)
+    Bm = O.colmajor(k, n, k, rng)
+    Cm = O.colmajor(m, n, m, rng)
+    C_ref = Cm.copy()
+    O.sgemm(0, 0, m, n, k, 1.0, A, m, Bm, k, 1.0, C_ref, m)
+    handle.set_math_mode(B.MATH_BF16X3)
+    handle.set_math_mode(B.MATH_PLAIN_FP32)
+    assert B.iclblasSgemm(handle, 0, 0, m, n, k, 1.0, A, m, Bm, k, 1.0, Cm, m) == B.SUCCESS
+    assert np.array_equal(Cm, C_ref)
