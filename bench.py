@@ -451,6 +451,112 @@ def run_gemm_study(args, torch):
     return results
 
 
+# ---------------------------------------------------------------- TRSM / TRSV study
+def run_trsm_study(args, torch):
+    """Triangular-solve config: STRSM left/lower/N/non-unit M=8192, NRHS=4096
+    (L: diagonal U(1,2), strictly lower N(0,1)/sqrt(M); B U(-1,1); seed 3),
+    CTRSM upper/conj-trans M=4096, NRHS=2048, and STRSV n=16384 with the same
+    L.  TFLOP/s use the algorithmic M^2*N (4*M^2*N complex) flops; STRSV is
+    reported in GB/s of the triangle + vector (4n(n+1)/2 + 8n bytes).  Error:
+    relative Frobenius error of X against an FP64 solve of the same FP32
+    inputs (torch.linalg.solve_triangular in float64, plumbing only)."""
+    from clgpu_b200 import iclblas as B
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(device=dev)
+    g = torch.Generator(device=dev).manual_seed(3)
+    modes = [(B.MATH_PLAIN_FP32, "fp32_simt"), (B.MATH_TF32, "tf32"), (B.MATH_BF16X3, "3xbf16"),
+             (B.MATH_BF16X6, "6xbf16")]
+    out = []
+
+    def make_tri(n, lower, cplx):
+        L = torch.randn(n, n, generator=g, device=dev) / (n ** 0.5)
+        L = torch.tril(L, -1) if lower else torch.triu(L, 1)
+        d = torch.rand(n, generator=g, device=dev) + 1.0
+        if cplx:
+            Li = torch.randn(n, n, generator=g, device=dev) / (n ** 0.5)
+            Li = torch.tril(Li, -1) if lower else torch.triu(Li, 1)
+            ph = torch.rand(n, generator=g, device=dev) * 6.283185307
+            L = torch.complex(L, Li) + torch.diag(torch.polar(d, ph))
+        else:
+            L = L + torch.diag(d)
+        return L  # row-major [i, j] = L(i, j); column-major storage is L.t().contiguous()
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    with B.Handle() as h, torch.cuda.stream(stream):
+        h.set_stream(stream)
+        for name_r, cplx, m, nrhs, lower, trans in (("strsm", False, args.trsm_m, args.trsm_n, True, 0),
+                                                    ("ctrsm", True, 4096, 2048, False, 2)):
+            L = make_tri(m, lower, cplx)
+            Acm = L.t().contiguous().reshape(-1)          # column-major storage of L
+            dt = torch.complex64 if cplx else torch.float32
+            B0 = torch.rand(nrhs, m, generator=g, device=dev) * 2 - 1
+            if cplx:
+                B0 = torch.complex(B0, torch.rand(nrhs, m, generator=g, device=dev) * 2 - 1)
+            B0 = B0.reshape(-1)                            # column-major m x nrhs
+            Bmat = B0.view(nrhs, m).t()
+            op = L if trans == 0 else (L.t() if trans == 1 else L.conj().t())
+            X64 = torch.linalg.solve_triangular(op.to(torch.complex128 if cplx else torch.float64),
+                                                Bmat.to(torch.complex128 if cplx else torch.float64),
+                                                upper=(not lower) if trans == 0 else lower)
+            x64n = torch.linalg.norm(X64).item()
+            fl = (4.0 if cplx else 1.0) * m * m * nrhs
+            for mode, mname in modes:
+                h.set_math_mode(mode)
+                Bw = B0.clone()
+                call = B.iclblasCtrsm if cplx else B.iclblasStrsm
+                one = (1.0 + 0j) if cplx else 1.0
+
+                def run():
+                    Bw.copy_(B0)
+                    B.check(call(h, 0, 1 if lower else 0, trans, 0, m, nrhs, one, Acm, m, Bw, m), mname)
+                ms = timed(run, 2)
+                X = Bw.view(nrhs, m).t().to(X64.dtype)  # result of the last timed call
+                # subtract the time of the copy that restores B before each call
+                Bt = torch.empty_like(B0)
+                ms = max(ms - timed(lambda: Bt.copy_(B0), 3), 1e-6)
+                err = torch.linalg.norm(X - X64).item() / x64n
+                r = {"routine": name_r, "m": m, "nrhs": nrhs, "mode": mname, "tflops": round(fl / (ms / 1e3) / 1e12, 2),
+                     "ms": round(ms, 3), "rel_fro_err_vs_fp64": err}
+                print(json.dumps(r), flush=True)
+                out.append(r)
+            del L, Acm, B0, X64
+        # STRSV n = 16384, lower / N / non-unit, same L construction
+        n = args.trsv_n
+        L = make_tri(n, True, False)
+        Acm = L.t().contiguous().reshape(-1)
+        x0 = torch.rand(n, generator=g, device=dev) * 2 - 1
+        x64 = torch.linalg.solve_triangular(L.double(), x0.double().view(n, 1), upper=False).view(-1)
+        xw = x0.clone()
+
+        def run_v():
+            xw.copy_(x0)
+            B.check(B.iclblasStrsv(h, 1, 0, 0, n, Acm, n, xw, 1), "strsv")
+        h.set_math_mode(B.MATH_PLAIN_FP32)
+        ms = timed(run_v, 5)
+        assert h.synchronize() == B.SUCCESS
+        err = (torch.linalg.norm(xw.double() - x64) / torch.linalg.norm(x64)).item()
+        xt = torch.empty_like(x0)
+        ms -= timed(lambda: xt.copy_(x0), 5)
+        gb = (4.0 * n * (n + 1) / 2 + 8.0 * n) / 1e9
+        r = {"routine": "strsv", "n": n, "gbs": round(gb / (ms / 1e3), 1), "ms": round(ms, 4),
+             "rel_fro_err_vs_fp64": err}
+        print(json.dumps(r), flush=True)
+        out.append(r)
+    return out
+
+
 # ---------------------------------------------------------------- CPU (reference code)
 SAMPLE_N1 = 1 << 24
 SAMPLE_GN = 4096
@@ -551,8 +657,12 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-operand (C ABI) leg")
     ap.add_argument("--only", default="", help="comma-separated subset of the sweep's calls")
     ap.add_argument("--n1", type=int, default=N1, help="level-1 vector length (default 2^28)")
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "gemm"],
-                    help="sweep: the bandwidth config (default); gemm: the precision config study")
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "gemm", "trsm"],
+                    help="sweep: the bandwidth config (default); gemm / trsm: the precision and "
+                         "triangular-solve config studies")
+    ap.add_argument("--trsm-m", type=int, default=8192)
+    ap.add_argument("--trsm-n", type=int, default=4096)
+    ap.add_argument("--trsv-n", type=int, default=16384)
     ap.add_argument("--gemm-n", type=int, default=8192)
     ap.add_argument("--skip-cgemm", action="store_true")
     ap.add_argument("--quick", action="store_true")
@@ -587,6 +697,9 @@ def main():
     import torch
     if args.workload == "gemm":
         run_gemm_study(args, torch)
+        return
+    if args.workload == "trsm":
+        run_trsm_study(args, torch)
         return
     if world > 1:
         torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))

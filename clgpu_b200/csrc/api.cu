@@ -240,6 +240,21 @@ void* iclb::scratch(iclblasHandle_t h, size_t bytes)
     return h->ws.scratch;
 }
 
+void* iclb::solver_scratch(iclblasHandle_t h, size_t bytes)
+{
+    bytes = (bytes + 255) & ~(size_t)255;
+    if (bytes <= h->ws.solver_bytes) return h->ws.solver;
+    if (h->ws.solver) cudaFree(h->ws.solver);
+    h->ws.solver = nullptr;
+    h->ws.solver_bytes = 0;
+    if (cudaMalloc(&h->ws.solver, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    h->ws.solver_bytes = bytes;
+    return h->ws.solver;
+}
+
 // ------------------------------------------------------------------------
 // utilities (iclBLAS.cpp:42-59)
 // ------------------------------------------------------------------------
@@ -282,6 +297,7 @@ extern "C" iclblasStatus_t iclblasDestroy(iclblasHandle_t handle)
         cudaStreamSynchronize(handle->stream);
         if (handle->stage) cudaFree(handle->stage);
         if (handle->ws.scratch) cudaFree(handle->ws.scratch);
+        if (handle->ws.solver) cudaFree(handle->ws.solver);
         cudaFree(handle->ws.counters);
         cudaFree(handle->ws.dev_status);
         cudaStreamDestroy(handle->own_stream);

@@ -29,8 +29,10 @@ enum DeviceStatus : int {
 // last-block-done tickets and flags; kernels that use a counter leave it at
 // zero (or, for epoch flags, monotonically increasing) when they finish.
 struct Workspace {
-    void* scratch = nullptr;   // general scratch (partials, staging)
+    void* scratch = nullptr;   // general scratch (partials, GEMM operand planes)
     size_t scratch_bytes = 0;
+    void* solver = nullptr;    // solver workspace (TRSM diagonal inverses), kept
+    size_t solver_bytes = 0;   // apart so the GEMMs inside a solve can grow `scratch`
     unsigned* counters = nullptr;   // kCounterWords words, zeroed at creation
     int* dev_status = nullptr;      // one int, DeviceStatus bits
     unsigned epoch = 0;             // host-side epoch for flag-based kernels
@@ -58,6 +60,8 @@ namespace iclb {
 
 // Returns scratch of at least `bytes` (256-byte aligned) or nullptr.
 void* scratch(iclblasHandle_t h, size_t bytes);
+// Same for the solver workspace.
+void* solver_scratch(iclblasHandle_t h, size_t bytes);
 
 // ---------------------------------------------------------------- level 1
 // All pointers are device pointers; n > 0, inc > 0.  Reduction results are

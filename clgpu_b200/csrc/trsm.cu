@@ -62,68 +62,176 @@ __device__ __forceinline__ cfloat divv(cfloat a, cfloat d)
     return cfloat{fmaf(a.re, d.re, a.im * d.im) / q, fmaf(a.im, d.re, -a.re * d.im) / q};
 }
 
-// Leaf solve of an nm x nm triangle.  `op` is how M's elements are read from
-// A: M(i,j) = A[a0 + i + j*lda] (op 0), A[a0 + j + i*lda] (op 1),
-// conj of the latter (op 2).  Left side: RHS j is column j of B (rows
-// 0..nm-1), solved with M.  Right side: RHS i is row i of B, solved with M^T
-// (x^T M = b^T).  One thread per RHS; M and the RHS block live in shared memory.
-template <class T, int LEAF = Leaf<T>::value>
-__global__ void __launch_bounds__(LEAF) trsm_leaf_kernel(int left, int m_lower, int op, int unit, int nm, int nrhs,
-                                                         T scale, const T* __restrict__ A, long lda,
-                                                         T* __restrict__ B, long ldb)
+// ------------------------------------------------------------------ FP64 leaves
+template <class T>
+struct Wide;
+template <>
+struct Wide<float> {
+    using type = double;
+};
+template <>
+struct Wide<cfloat> {
+    using type = double2;
+};
+
+__device__ __forceinline__ double wz(double) { return 0.0; }
+__device__ __forceinline__ double2 wz(double2) { return make_double2(0.0, 0.0); }
+__device__ __forceinline__ double widen(float a) { return (double)a; }
+__device__ __forceinline__ double2 widen(cfloat a) { return make_double2(a.re, a.im); }
+__device__ __forceinline__ float narrow(double a, float) { return (float)a; }
+__device__ __forceinline__ cfloat narrow(double2 a, cfloat) { return cfloat{(float)a.x, (float)a.y}; }
+__device__ __forceinline__ double wone(double) { return 1.0; }
+__device__ __forceinline__ double2 wone(double2) { return make_double2(1.0, 0.0); }
+__device__ __forceinline__ void wfma(double& acc, double a, double b) { acc = fma(a, b, acc); }
+__device__ __forceinline__ void wfma(double2& acc, double2 a, double2 b)
 {
-    __shared__ T Ms[LEAF][LEAF + 1];
-    __shared__ T Xs[LEAF][LEAF + 1];  // Xs[e][t]: element e of RHS t
-    const int t = threadIdx.x;
-    const int rhs0 = blockIdx.x * LEAF;
-    // M into shared memory, coalesced along A's columns
-    for (int idx = t; idx < LEAF * LEAF; idx += LEAF) {
-        const int r = idx % LEAF, c = idx / LEAF;  // A-local (r, c)
-        T v = zero_v(T());
-        if (r < nm && c < nm) v = A[(long)c * lda + r];
-        // M(i,j) from A-local (r,c): op 0 -> (r,c); op 1/2 -> (c,r)
-        if (op == 0) Ms[r][c] = v;
-        else Ms[c][r] = (op == 2) ? conj_v(v) : v;
+    acc.x = fma(a.x, b.x, fma(-a.y, b.y, acc.x));
+    acc.y = fma(a.x, b.y, fma(a.y, b.x, acc.y));
+}
+__device__ __forceinline__ void wfms(double& acc, double a, double b) { acc = fma(-a, b, acc); }
+__device__ __forceinline__ void wfms(double2& acc, double2 a, double2 b)
+{
+    acc.x = fma(-a.x, b.x, fma(a.y, b.y, acc.x));
+    acc.y = fma(-a.x, b.y, fma(-a.y, b.x, acc.y));
+}
+__device__ __forceinline__ double wdiv(double a, double d) { return a / d; }
+__device__ __forceinline__ double2 wdiv(double2 a, double2 d)
+{
+    const double q = d.x * d.x + d.y * d.y;
+    return make_double2((a.x * d.x + a.y * d.y) / q, (a.y * d.x - a.x * d.y) / q);
+}
+
+// Inverse in FP64 of every NB x NB diagonal block of M = op(A) (the last
+// block may be partial).  M(i,j) = A[i + j*lda] (op 0) or A[j + i*lda]
+// (op 1; op 2 conjugates).  Block b is written column-major to
+// inv[b*NB*NB ...], zero outside the block.  Thread j forms column j of the
+// inverse by substitution on e_j.
+template <class T, int NB>
+__global__ void __launch_bounds__(NB) trsm_inv_diag_kernel(int n, int op, int m_lower, int unit,
+                                                           const T* __restrict__ A, long lda,
+                                                           typename Wide<T>::type* __restrict__ inv)
+{
+    using W = typename Wide<T>::type;
+    extern __shared__ uint8_t smem_raw[];
+    W(*M)[NB + 1] = (W(*)[NB + 1])smem_raw;
+    W(*Y)[NB + 1] = M + NB;
+    const int b = blockIdx.x, o = b * NB, nb = min(NB, n - o);
+    for (int idx = threadIdx.x; idx < NB * NB; idx += NB) {
+        const int r = idx % NB, c = idx / NB;  // A-local (r, c): coalesced down A's columns
+        W v = wz(W());
+        if (r < nb && c < nb) {
+            T a = A[(long)(o + c) * lda + (o + r)];
+            if (op == 2) a = conj_v(a);
+            v = widen(a);
+        }
+        if (op == 0) M[r][c] = v;
+        else M[c][r] = v;
     }
-    // RHS block, scaled
-    for (int idx = t; idx < LEAF * LEAF; idx += LEAF) {
-        const int a = idx % LEAF, b = idx / LEAF;  // contiguous index first
-        T v = zero_v(T());
-        if (left) {  // element a of RHS column rhs0+b
-            if (a < nm && rhs0 + b < nrhs) v = mulv(B[(long)(rhs0 + b) * ldb + a], scale);
-            Xs[a][b] = v;
-        } else {  // element b of RHS row rhs0+a
-            if (b < nm && rhs0 + a < nrhs) v = mulv(B[(long)b * ldb + rhs0 + a], scale);
-            Xs[b][a] = v;
+    __syncthreads();
+    const int j = threadIdx.x;
+    if (m_lower) {
+        for (int i = 0; i < NB; ++i) {
+            W y = wz(W());
+            if (i >= j && i < nb && j < nb) {
+                y = (i == j) ? wone(W()) : wz(W());
+                for (int k = j; k < i; ++k) wfms(y, M[i][k], Y[k][j]);
+                if (!unit) y = wdiv(y, M[i][i]);
+            }
+            Y[i][j] = y;
+        }
+    } else {
+        for (int i = NB - 1; i >= 0; --i) {
+            W y = wz(W());
+            if (i <= j && i < nb && j < nb) {
+                y = (i == j) ? wone(W()) : wz(W());
+                for (int k = i + 1; k <= j; ++k) wfms(y, M[i][k], Y[k][j]);
+                if (!unit) y = wdiv(y, M[i][i]);
+            }
+            Y[i][j] = y;
         }
     }
     __syncthreads();
-    // Effective triangle: left uses M, right uses M^T (lower <-> upper).
-    const bool lower = left ? m_lower : !m_lower;
-    if (rhs0 + t < nrhs) {
-        if (lower) {
-            for (int k = 0; k < nm; ++k) {
-                T xk = Xs[k][t];
-                if (!unit) xk = divv(xk, left ? Ms[k][k] : Ms[k][k]);
-                Xs[k][t] = xk;
-                for (int r = k + 1; r < nm; ++r) msub(Xs[r][t], left ? Ms[r][k] : Ms[k][r], xk);
-            }
-        } else {
-            for (int k = nm - 1; k >= 0; --k) {
-                T xk = Xs[k][t];
-                if (!unit) xk = divv(xk, Ms[k][k]);
-                Xs[k][t] = xk;
-                for (int r = 0; r < k; ++r) msub(Xs[r][t], left ? Ms[r][k] : Ms[k][r], xk);
-            }
-        }
+    W* out = inv + (long)b * NB * NB;
+    for (int idx = threadIdx.x; idx < NB * NB; idx += NB) out[idx] = Y[idx % NB][idx / NB];
+}
+
+// Leaf of a left solve: B[0:nb, r] = inv * B[0:nb, r] for the RHS columns of
+// this block (64 per CTA), in FP64.  Thread t owns row t % NB of the block
+// and RHS columns t / NB + G*q (G = 256 / NB groups).
+template <class T, int NB>
+__global__ void __launch_bounds__(256) trsm_apply_left_kernel(int nb, int nrhs, const typename Wide<T>::type* inv,
+                                                              T* __restrict__ B, long ldb)
+{
+    using W = typename Wide<T>::type;
+    constexpr int R = 64;        // RHS per CTA
+    constexpr int G = 256 / NB;  // RHS groups
+    constexpr int Q = R / G;     // RHS per thread
+    extern __shared__ uint8_t smem_raw[];
+    W(*Iv)[NB + 1] = (W(*)[NB + 1])smem_raw;
+    W(*Bv)[R + 1] = (W(*)[R + 1])(smem_raw + sizeof(W) * NB * (NB + 1));
+    const int r0 = blockIdx.x * R;
+    for (int idx = threadIdx.x; idx < NB * NB; idx += 256) Iv[idx % NB][idx / NB] = inv[idx];
+    for (int idx = threadIdx.x; idx < NB * R; idx += 256) {
+        const int k = idx % NB, r = idx / NB;
+        W v = wz(W());
+        if (k < nb && r0 + r < nrhs) v = widen(B[(long)(r0 + r) * ldb + k]);
+        Bv[k][r] = v;
     }
     __syncthreads();
-    for (int idx = t; idx < LEAF * LEAF; idx += LEAF) {
-        const int a = idx % LEAF, b = idx / LEAF;
-        if (left) {
-            if (a < nm && rhs0 + b < nrhs) B[(long)(rhs0 + b) * ldb + a] = Xs[a][b];
-        } else {
-            if (b < nm && rhs0 + a < nrhs) B[(long)b * ldb + rhs0 + a] = Xs[b][a];
+    const int i = threadIdx.x % NB, g = threadIdx.x / NB;
+    W acc[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) acc[q] = wz(W());
+    for (int k = 0; k < nb; ++k) {
+        const W a = Iv[i][k];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) wfma(acc[q], a, Bv[k][g + G * q]);
+    }
+    if (i < nb) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const int r = r0 + g + G * q;
+            if (r < nrhs) B[(long)r * ldb + i] = narrow(acc[q], T());
+        }
+    }
+}
+
+// Leaf of a right solve: B[r, 0:nb] = B[r, 0:nb] * inv for the rows of this
+// block (64 per CTA), in FP64.  Thread t owns row t % 64 and columns
+// t / 64 + 4*q.
+template <class T, int NB>
+__global__ void __launch_bounds__(256) trsm_apply_right_kernel(int nb, int nrows, const typename Wide<T>::type* inv,
+                                                               T* __restrict__ B, long ldb)
+{
+    using W = typename Wide<T>::type;
+    constexpr int R = 64;  // rows per CTA
+    constexpr int Q = NB / 4;
+    extern __shared__ uint8_t smem_raw[];
+    W(*Iv)[NB + 1] = (W(*)[NB + 1])smem_raw;
+    W(*Bv)[NB + 1] = (W(*)[NB + 1])(smem_raw + sizeof(W) * NB * (NB + 1));
+    const int r0 = blockIdx.x * R;
+    for (int idx = threadIdx.x; idx < NB * NB; idx += 256) Iv[idx % NB][idx / NB] = inv[idx];
+    for (int idx = threadIdx.x; idx < R * NB; idx += 256) {
+        const int r = idx % R, k = idx / R;
+        W v = wz(W());
+        if (k < nb && r0 + r < nrows) v = widen(B[(long)k * ldb + r0 + r]);
+        Bv[r][k] = v;
+    }
+    __syncthreads();
+    const int r = threadIdx.x % R, g = threadIdx.x / R;
+    W acc[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) acc[q] = wz(W());
+    for (int k = 0; k < nb; ++k) {
+        const W bv = Bv[r][k];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) wfma(acc[q], bv, Iv[k][g + 4 * q]);
+    }
+    if (r0 + r < nrows) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const int c = g + 4 * q;
+            if (c < nb) B[(long)c * ldb + r0 + r] = narrow(acc[q], T());
         }
     }
 }
@@ -165,14 +273,23 @@ struct Solver {
     // Pointer and GEMM op of block M[r0.., c0..] of M = op(A).
     const T* mblk(int r0, int c0) const { return op == 0 ? A + r0 + (long)c0 * lda : A + c0 + (long)r0 * lda; }
 
+    const typename Wide<T>::type* inv = nullptr;  // FP64 inverses of M's diagonal blocks
+
     // Solve the diagonal range [o, o+sz) of M against the matching part of B.
     cudaError_t solve(int o, int sz, T scale)
     {
         if (sz <= LEAF) {
-            const T* a0 = A + o + (long)o * lda;
-            T* b0 = left ? B + o : B + (long)o * ldb;
-            trsm_leaf_kernel<T><<<ceil_div(nrhs, LEAF), LEAF, 0, h->stream>>>(left, m_lower, op, unit, sz, nrhs,
-                                                                                scale, a0, lda, b0, ldb);
+            using W = typename Wide<T>::type;
+            const W* ib = inv + (long)(o / LEAF) * LEAF * LEAF;
+            if (left) {
+                const size_t sm = sizeof(W) * (LEAF * (LEAF + 1) + LEAF * 65);
+                trsm_apply_left_kernel<T, LEAF><<<ceil_div(nrhs, 64), 256, sm, h->stream>>>(sz, nrhs, ib, B + o, ldb);
+            } else {
+                const size_t sm = sizeof(W) * (LEAF * (LEAF + 1) + 64 * (LEAF + 1));
+                trsm_apply_right_kernel<T, LEAF><<<ceil_div(nrhs, 64), 256, sm, h->stream>>>(
+                    sz, nrhs, ib, B + (long)o * ldb, ldb);
+            }
+            (void)scale;
             return cudaGetLastError();
         }
         int h1 = (sz / 2 + LEAF - 1) / LEAF * LEAF;  // first half, a multiple of the leaf
@@ -228,7 +345,29 @@ cudaError_t trsm_impl(iclblasHandle_t h, int side, int uplo, int trans, int diag
     s.B = B;
     s.ldb = ldb;
     s.nrhs = s.left ? n : m;
-    cudaError_t e = s.solve(0, s.left ? m : n, Gemm<T>::one());
+    // FP64 inverses of all diagonal blocks of op(A), one launch
+    using W = typename Wide<T>::type;
+    constexpr int NB = Solver<T>::LEAF;
+    const int na = s.left ? m : n;
+    const int nblk = ceil_div(na, NB);
+    W* inv = (W*)solver_scratch(h, sizeof(W) * (size_t)nblk * NB * NB);
+    if (!inv) return cudaErrorMemoryAllocation;
+    const size_t sm_inv = sizeof(W) * 2 * NB * (NB + 1);
+    cudaError_t e = cudaFuncSetAttribute(trsm_inv_diag_kernel<T, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sm_inv);
+    if (e != cudaSuccess) return e;
+    const size_t sm_app = sizeof(W) * (NB * (NB + 1) + NB * 65);
+    const size_t sm_app_r = sizeof(W) * (NB * (NB + 1) + 64 * (NB + 1));
+    if ((e = cudaFuncSetAttribute(trsm_apply_left_kernel<T, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sm_app)) != cudaSuccess)
+        return e;
+    if ((e = cudaFuncSetAttribute(trsm_apply_right_kernel<T, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sm_app_r)) != cudaSuccess)
+        return e;
+    trsm_inv_diag_kernel<T, NB><<<nblk, NB, sm_inv, h->stream>>>(na, s.op, s.m_lower, s.unit, A, lda, inv);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    s.inv = inv;
+    e = s.solve(0, na, Gemm<T>::one());
     if (e != cudaSuccess || is_one(alpha)) return e;
     const long total = (long)m * n;
     const int grid = (int)std::min<long>((total + 255) / 256, (long)h->sm_count * 8);
