@@ -94,6 +94,8 @@ __device__ __forceinline__ void wfms(double2& acc, double2 a, double2 b)
     acc.x = fma(-a.x, b.x, fma(a.y, b.y, acc.x));
     acc.y = fma(-a.x, b.y, fma(-a.y, b.x, acc.y));
 }
+__device__ __forceinline__ void wneg(double& a) { a = -a; }
+__device__ __forceinline__ void wneg(double2& a) { a.x = -a.x; a.y = -a.y; }
 __device__ __forceinline__ double wdiv(double a, double d) { return a / d; }
 __device__ __forceinline__ double2 wdiv(double2 a, double2 d)
 {
@@ -101,13 +103,14 @@ __device__ __forceinline__ double2 wdiv(double2 a, double2 d)
     return make_double2((a.x * d.x + a.y * d.y) / q, (a.y * d.x - a.x * d.y) / q);
 }
 
-// Inverse in FP64 of every NB x NB diagonal block of M = op(A) (the last
-// block may be partial).  M(i,j) = A[i + j*lda] (op 0) or A[j + i*lda]
-// (op 1; op 2 conjugates).  Block b is written column-major to
-// inv[b*NB*NB ...], zero outside the block.  Thread j forms column j of the
-// inverse by substitution on e_j.
+// Inverse in FP64 of every NB x NB diagonal block of M = op(A) over the
+// padded range [0, nbig*BIG): M(i,j) = A[i + j*lda] (op 0) or A[j + i*lda]
+// (op 1; op 2 conjugates); rows and columns at or beyond n are the identity.
+// Block b is written into its big block's column-major BIG x BIG inverse
+// (inv + (b*NB / BIG) * BIG*BIG, at local offset (b*NB) % BIG).  Thread j
+// forms column j of the inverse by substitution on e_j.
 template <class T, int NB>
-__global__ void __launch_bounds__(NB) trsm_inv_diag_kernel(int n, int op, int m_lower, int unit,
+__global__ void __launch_bounds__(NB) trsm_inv_diag_kernel(int n, int op, int m_lower, int unit, int big,
                                                            const T* __restrict__ A, long lda,
                                                            typename Wide<T>::type* __restrict__ inv)
 {
@@ -115,10 +118,10 @@ __global__ void __launch_bounds__(NB) trsm_inv_diag_kernel(int n, int op, int m_
     extern __shared__ uint8_t smem_raw[];
     W(*M)[NB + 1] = (W(*)[NB + 1])smem_raw;
     W(*Y)[NB + 1] = M + NB;
-    const int b = blockIdx.x, o = b * NB, nb = min(NB, n - o);
+    const int b = blockIdx.x, o = b * NB, nb = max(0, min(NB, n - o));
     for (int idx = threadIdx.x; idx < NB * NB; idx += NB) {
         const int r = idx % NB, c = idx / NB;  // A-local (r, c): coalesced down A's columns
-        W v = wz(W());
+        W v = (r == c && r >= nb) ? wone(W()) : wz(W());
         if (r < nb && c < nb) {
             T a = A[(long)(o + c) * lda + (o + r)];
             if (op == 2) a = conj_v(a);
@@ -129,111 +132,132 @@ __global__ void __launch_bounds__(NB) trsm_inv_diag_kernel(int n, int op, int m_
     }
     __syncthreads();
     const int j = threadIdx.x;
+    const bool unit_j = unit || j >= nb;  // padding rows have a unit diagonal
     if (m_lower) {
         for (int i = 0; i < NB; ++i) {
             W y = wz(W());
-            if (i >= j && i < nb && j < nb) {
+            if (i >= j) {
                 y = (i == j) ? wone(W()) : wz(W());
                 for (int k = j; k < i; ++k) wfms(y, M[i][k], Y[k][j]);
-                if (!unit) y = wdiv(y, M[i][i]);
+                if (!(unit || i >= nb)) y = wdiv(y, M[i][i]);
             }
             Y[i][j] = y;
         }
     } else {
         for (int i = NB - 1; i >= 0; --i) {
             W y = wz(W());
-            if (i <= j && i < nb && j < nb) {
+            if (i <= j) {
                 y = (i == j) ? wone(W()) : wz(W());
                 for (int k = i + 1; k <= j; ++k) wfms(y, M[i][k], Y[k][j]);
-                if (!unit) y = wdiv(y, M[i][i]);
+                if (!(unit || i >= nb)) y = wdiv(y, M[i][i]);
             }
             Y[i][j] = y;
         }
     }
+    (void)unit_j;
     __syncthreads();
-    W* out = inv + (long)b * NB * NB;
-    for (int idx = threadIdx.x; idx < NB * NB; idx += NB) out[idx] = Y[idx % NB][idx / NB];
+    const int bb = o / big, lo = o % big;
+    W* out = inv + (long)bb * big * big + (long)lo * big + lo;
+    for (int idx = threadIdx.x; idx < NB * NB; idx += NB) out[(long)(idx / NB) * big + idx % NB] = Y[idx % NB][idx / NB];
 }
 
-// Leaf of a left solve: B[0:nb, r] = inv * B[0:nb, r] for the RHS columns of
-// this block (64 per CTA), in FP64.  Thread t owns row t % NB of the block
-// and RHS columns t / NB + G*q (G = 256 / NB groups).
-template <class T, int NB>
-__global__ void __launch_bounds__(256) trsm_apply_left_kernel(int nb, int nrhs, const typename Wide<T>::type* inv,
-                                                              T* __restrict__ B, long ldb)
+// One doubling step of the block inverses: for every 2s x 2s diagonal block
+// (offset o in big block bb) whose two s x s diagonal inverses are known,
+//   lower M = [[P, 0], [C, Q]]:  inv = [[P^-1, 0], [-Q^-1 C P^-1, Q^-1]]
+//   upper M = [[P, C], [0, Q]]:  inv = [[P^-1, -P^-1 C Q^-1], [0, Q^-1]]
+// STEP 0 forms T = C * P^-1 (lower) or T = C * Q^-1 (upper) with C read from
+// A through op; STEP 1 forms the off-diagonal block -Q^-1 T (lower) or
+// -P^-1 T (upper) into the inverse.  FP64, TS x TS tiles, 256 threads, each
+// thread (TS/16) x (TS/16) outputs; blockIdx.z enumerates the 2s blocks.
+template <class T, int TS, int STEP>
+__global__ void __launch_bounds__(256) trsm_inv_double_kernel(int n, int op, int m_lower, int s, int big,
+                                                              const T* __restrict__ A, long lda,
+                                                              typename Wide<T>::type* __restrict__ inv,
+                                                              typename Wide<T>::type* __restrict__ tmp)
 {
     using W = typename Wide<T>::type;
-    constexpr int R = 64;        // RHS per CTA
-    constexpr int G = 256 / NB;  // RHS groups
-    constexpr int Q = R / G;     // RHS per thread
-    extern __shared__ uint8_t smem_raw[];
-    W(*Iv)[NB + 1] = (W(*)[NB + 1])smem_raw;
-    W(*Bv)[R + 1] = (W(*)[R + 1])(smem_raw + sizeof(W) * NB * (NB + 1));
-    const int r0 = blockIdx.x * R;
-    for (int idx = threadIdx.x; idx < NB * NB; idx += 256) Iv[idx % NB][idx / NB] = inv[idx];
-    for (int idx = threadIdx.x; idx < NB * R; idx += 256) {
-        const int k = idx % NB, r = idx / NB;
-        W v = wz(W());
-        if (k < nb && r0 + r < nrhs) v = widen(B[(long)(r0 + r) * ldb + k]);
-        Bv[k][r] = v;
-    }
-    __syncthreads();
-    const int i = threadIdx.x % NB, g = threadIdx.x / NB;
-    W acc[Q];
+    constexpr int KC = 16;
+    constexpr int PT = TS / 16;  // outputs per thread per dimension
+    __shared__ W Xs[TS][KC + 1];
+    __shared__ W Ys[KC][TS + 1];
+    const int pairs = big / (2 * s);
+    const int z = blockIdx.z, bb = z / pairs, o = (z % pairs) * 2 * s;
+    const int gbase = bb * big;  // global row/col of the big block
+    W* invb = inv + (long)bb * big * big;
+    W* tz = tmp + (long)z * s * s;
+    const int i0 = blockIdx.y * TS, j0 = blockIdx.x * TS;  // output tile (rows, cols) in s x s
+    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    // X (s x s) and Y (s x s) sources; output location
+    //  STEP 0 lower: X = C = M[o+s.., o..],  Y = P^-1 = inv[o.., o..],     out = tmp
+    //  STEP 0 upper: X = C = M[o.., o+s..],  Y = Q^-1 = inv[o+s.., o+s..], out = tmp
+    //  STEP 1 lower: X = Q^-1 = inv[o+s.., o+s..], Y = tmp, out = inv[o+s.., o..] (negated)
+    //  STEP 1 upper: X = P^-1 = inv[o.., o..],     Y = tmp, out = inv[o.., o+s..] (negated)
+    const int xr = (STEP == 0) ? (m_lower ? o + s : o) : (m_lower ? o + s : o);
+    const int xc = (STEP == 0) ? (m_lower ? o : o + s) : (m_lower ? o + s : o);
+    const int yo = m_lower ? o : o + s;  // STEP 0 diagonal inverse offset
+    W acc[PT][PT];
 #pragma unroll
-    for (int q = 0; q < Q; ++q) acc[q] = wz(W());
-    for (int k = 0; k < nb; ++k) {
-        const W a = Iv[i][k];
+    for (int a = 0; a < PT; ++a)
 #pragma unroll
-        for (int q = 0; q < Q; ++q) wfma(acc[q], a, Bv[k][g + G * q]);
-    }
-    if (i < nb) {
-#pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            const int r = r0 + g + G * q;
-            if (r < nrhs) B[(long)r * ldb + i] = narrow(acc[q], T());
+        for (int c = 0; c < PT; ++c) acc[a][c] = wz(W());
+    for (int k0 = 0; k0 < s; k0 += KC) {
+        for (int idx = threadIdx.x; idx < TS * KC; idx += 256) {
+            const int r = idx % TS, k = idx / TS;
+            W v;
+            if (STEP == 0) {
+                const int gi = gbase + xr + i0 + r, gj = gbase + xc + k0 + k;  // M(gi, gj)
+                v = wz(W());
+                if (gi < n && gj < n) {
+                    T a = (op == 0) ? A[(long)gj * lda + gi] : A[(long)gi * lda + gj];
+                    if (op == 2) a = conj_v(a);
+                    v = widen(a);
+                }
+            } else {
+                v = invb[(long)(xc + k0 + k) * big + xr + i0 + r];
+            }
+            Xs[r][k] = v;
         }
+        for (int idx = threadIdx.x; idx < KC * TS; idx += 256) {
+            const int k = idx % KC, c = idx / KC;
+            Ys[k][c] = (STEP == 0) ? invb[(long)(yo + j0 + c) * big + yo + k0 + k] : tz[(long)(j0 + c) * s + k0 + k];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < KC; ++k) {
+            W xv[PT], yv[PT];
+#pragma unroll
+            for (int a = 0; a < PT; ++a) xv[a] = Xs[ty + 16 * a][k];
+#pragma unroll
+            for (int c = 0; c < PT; ++c) yv[c] = Ys[k][tx + 16 * c];
+#pragma unroll
+            for (int a = 0; a < PT; ++a)
+#pragma unroll
+                for (int c = 0; c < PT; ++c) wfma(acc[a][c], xv[a], yv[c]);
+        }
+        __syncthreads();
     }
+#pragma unroll
+    for (int a = 0; a < PT; ++a)
+#pragma unroll
+        for (int c = 0; c < PT; ++c) {
+            const int i = i0 + ty + 16 * a, j = j0 + tx + 16 * c;
+            if (STEP == 0) {
+                tz[(long)j * s + i] = acc[a][c];
+            } else {
+                W v = acc[a][c];
+                wneg(v);
+                const int orow = m_lower ? o + s : o, ocol = m_lower ? o : o + s;
+                invb[(long)(ocol + j) * big + orow + i] = v;
+            }
+        }
 }
 
-// Leaf of a right solve: B[r, 0:nb] = B[r, 0:nb] * inv for the rows of this
-// block (64 per CTA), in FP64.  Thread t owns row t % 64 and columns
-// t / 64 + 4*q.
-template <class T, int NB>
-__global__ void __launch_bounds__(256) trsm_apply_right_kernel(int nb, int nrows, const typename Wide<T>::type* inv,
-                                                               T* __restrict__ B, long ldb)
+// FP64 inverse blocks rounded to the working precision (for the GEMM apply).
+template <class T>
+__global__ void narrow_kernel(long count, const typename Wide<T>::type* __restrict__ src, T* __restrict__ dst)
 {
-    using W = typename Wide<T>::type;
-    constexpr int R = 64;  // rows per CTA
-    constexpr int Q = NB / 4;
-    extern __shared__ uint8_t smem_raw[];
-    W(*Iv)[NB + 1] = (W(*)[NB + 1])smem_raw;
-    W(*Bv)[NB + 1] = (W(*)[NB + 1])(smem_raw + sizeof(W) * NB * (NB + 1));
-    const int r0 = blockIdx.x * R;
-    for (int idx = threadIdx.x; idx < NB * NB; idx += 256) Iv[idx % NB][idx / NB] = inv[idx];
-    for (int idx = threadIdx.x; idx < R * NB; idx += 256) {
-        const int r = idx % R, k = idx / R;
-        W v = wz(W());
-        if (k < nb && r0 + r < nrows) v = widen(B[(long)k * ldb + r0 + r]);
-        Bv[r][k] = v;
-    }
-    __syncthreads();
-    const int r = threadIdx.x % R, g = threadIdx.x / R;
-    W acc[Q];
-#pragma unroll
-    for (int q = 0; q < Q; ++q) acc[q] = wz(W());
-    for (int k = 0; k < nb; ++k) {
-        const W bv = Bv[r][k];
-#pragma unroll
-        for (int q = 0; q < Q; ++q) wfma(acc[q], bv, Iv[k][g + 4 * q]);
-    }
-    if (r0 + r < nrows) {
-#pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            const int c = g + 4 * q;
-            if (c < nb) B[(long)c * ldb + r0 + r] = narrow(acc[q], T());
-        }
-    }
+    for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < count; e += (long)gridDim.x * blockDim.x)
+        dst[e] = narrow(src[e], T());
 }
 
 template <class T>
@@ -246,6 +270,7 @@ struct Gemm<float> {
         return sgemm(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
     }
     static float one() { return 1.f; }
+    static float zero() { return 0.f; }
     static float minus_one() { return -1.f; }
 };
 template <>
@@ -256,12 +281,13 @@ struct Gemm<cfloat> {
         return cgemm(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
     }
     static cfloat one() { return cfloat{1.f, 0.f}; }
+    static cfloat zero() { return cfloat{0.f, 0.f}; }
     static cfloat minus_one() { return cfloat{-1.f, 0.f}; }
 };
 
 template <class T>
 struct Solver {
-    static constexpr int LEAF = Leaf<T>::value;
+    static constexpr int NB = Leaf<T>::value;  // base inverse block
     iclblasHandle_t h;
     int left, op, unit, m_lower;
     const T* A;
@@ -269,48 +295,53 @@ struct Solver {
     T* B;
     long ldb;
     int nrhs;  // RHS count (n for left, m for right)
+    int big;   // leaf size (a power-of-two multiple of NB)
+    const T* inv = nullptr;  // inverses of the BIG diagonal blocks (FP64-formed, rounded)
+    T* tmp = nullptr;        // leaf staging: big x nrhs (left) or nrhs x big (right)
 
     // Pointer and GEMM op of block M[r0.., c0..] of M = op(A).
     const T* mblk(int r0, int c0) const { return op == 0 ? A + r0 + (long)c0 * lda : A + c0 + (long)r0 * lda; }
 
-    const typename Wide<T>::type* inv = nullptr;  // FP64 inverses of M's diagonal blocks
-
     // Solve the diagonal range [o, o+sz) of M against the matching part of B.
-    cudaError_t solve(int o, int sz, T scale)
+    cudaError_t solve(int o, int sz)
     {
-        if (sz <= LEAF) {
-            using W = typename Wide<T>::type;
-            const W* ib = inv + (long)(o / LEAF) * LEAF * LEAF;
+        if (sz <= big) {
+            // leaf: X = inv(M_oo) * B_o (left) or B_o * inv(M_oo) (right), by GEMM
+            const T* ib = inv + (long)(o / big) * big * big;
+            cudaError_t e;
             if (left) {
-                const size_t sm = sizeof(W) * (LEAF * (LEAF + 1) + LEAF * 65);
-                trsm_apply_left_kernel<T, LEAF><<<ceil_div(nrhs, 64), 256, sm, h->stream>>>(sz, nrhs, ib, B + o, ldb);
-            } else {
-                const size_t sm = sizeof(W) * (LEAF * (LEAF + 1) + 64 * (LEAF + 1));
-                trsm_apply_right_kernel<T, LEAF><<<ceil_div(nrhs, 64), 256, sm, h->stream>>>(
-                    sz, nrhs, ib, B + (long)o * ldb, ldb);
+                e = cudaMemcpy2DAsync(tmp, sizeof(T) * sz, B + o, sizeof(T) * ldb, sizeof(T) * sz, nrhs,
+                                      cudaMemcpyDeviceToDevice, h->stream);
+                if (e != cudaSuccess) return e;
+                return Gemm<T>::run(h, ICLBLAS_OP_N, ICLBLAS_OP_N, sz, nrhs, sz, Gemm<T>::one(), ib, big, tmp, sz,
+                                    Gemm<T>::zero(), B + o, ldb);
             }
-            (void)scale;
-            return cudaGetLastError();
+            e = cudaMemcpy2DAsync(tmp, sizeof(T) * nrhs, B + (long)o * ldb, sizeof(T) * ldb, sizeof(T) * nrhs, sz,
+                                  cudaMemcpyDeviceToDevice, h->stream);
+            if (e != cudaSuccess) return e;
+            return Gemm<T>::run(h, ICLBLAS_OP_N, ICLBLAS_OP_N, nrhs, sz, sz, Gemm<T>::one(), tmp, nrhs, ib, big,
+                                Gemm<T>::zero(), B + (long)o * ldb, ldb);
         }
-        int h1 = (sz / 2 + LEAF - 1) / LEAF * LEAF;  // first half, a multiple of the leaf
+        const int nleaf = (sz + big - 1) / big;
+        const int h1 = (nleaf / 2) * big;  // first half: a whole number of leaves
         const int o1 = o, s1 = h1, o2 = o + h1, s2 = sz - h1;
         // Forward (first half first) when: left & M lower, or right & M upper.
         const bool forward = left ? m_lower : !m_lower;
         const int fo = forward ? o1 : o2, fs = forward ? s1 : s2;  // solved first
         const int so = forward ? o2 : o1, ss = forward ? s2 : s1;  // updated, solved second
-        cudaError_t e = solve(fo, fs, scale);
+        cudaError_t e = solve(fo, fs);
         if (e != cudaSuccess) return e;
         if (left) {
-            // B[so] = scale*B[so] - M[so, fo] * X[fo]
+            // B[so] = B[so] - M[so, fo] * X[fo]
             e = Gemm<T>::run(h, op, ICLBLAS_OP_N, ss, nrhs, fs, Gemm<T>::minus_one(), mblk(so, fo), lda, B + fo, ldb,
-                             scale, B + so, ldb);
+                             Gemm<T>::one(), B + so, ldb);
         } else {
-            // B[:, so] = scale*B[:, so] - X[:, fo] * M[fo, so]
+            // B[:, so] = B[:, so] - X[:, fo] * M[fo, so]
             e = Gemm<T>::run(h, ICLBLAS_OP_N, op, nrhs, ss, fs, Gemm<T>::minus_one(), B + (long)fo * ldb, ldb,
-                             mblk(fo, so), lda, scale, B + (long)so * ldb, ldb);
+                             mblk(fo, so), lda, Gemm<T>::one(), B + (long)so * ldb, ldb);
         }
         if (e != cudaSuccess) return e;
-        return solve(so, ss, Gemm<T>::one());
+        return solve(so, ss);
     }
 };
 
@@ -345,29 +376,52 @@ cudaError_t trsm_impl(iclblasHandle_t h, int side, int uplo, int trans, int diag
     s.B = B;
     s.ldb = ldb;
     s.nrhs = s.left ? n : m;
-    // FP64 inverses of all diagonal blocks of op(A), one launch
     using W = typename Wide<T>::type;
-    constexpr int NB = Solver<T>::LEAF;
+    constexpr int NB = Solver<T>::NB;
+    constexpr int BIG_MAX = sizeof(T) == sizeof(float) ? 512 : 256;
     const int na = s.left ? m : n;
-    const int nblk = ceil_div(na, NB);
-    W* inv = (W*)solver_scratch(h, sizeof(W) * (size_t)nblk * NB * NB);
-    if (!inv) return cudaErrorMemoryAllocation;
-    const size_t sm_inv = sizeof(W) * 2 * NB * (NB + 1);
-    cudaError_t e = cudaFuncSetAttribute(trsm_inv_diag_kernel<T, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)sm_inv);
+    int big = NB;
+    while (big < BIG_MAX && big < na) big *= 2;
+    s.big = big;
+    const int nbig = ceil_div(na, big);
+    const int nsmall = nbig * (big / NB);
+    // workspace: FP64 inverses, doubling temporaries, rounded inverses, leaf staging
+    const size_t inv_w = (size_t)nbig * big * big;
+    const size_t tmp_w = (size_t)nbig * (big / 2) * (big / 2);
+    const size_t leaf_t = (size_t)big * s.nrhs;
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    const size_t bytes = al(sizeof(W) * inv_w) + al(sizeof(W) * tmp_w) + al(sizeof(T) * inv_w) + al(sizeof(T) * leaf_t);
+    char* ws = (char*)solver_scratch(h, bytes);
+    if (!ws) return cudaErrorMemoryAllocation;
+    W* invd = (W*)ws;
+    W* dtmp = (W*)(ws + al(sizeof(W) * inv_w));
+    T* inv32 = (T*)(ws + al(sizeof(W) * inv_w) + al(sizeof(W) * tmp_w));
+    s.tmp = (T*)(ws + al(sizeof(W) * inv_w) + al(sizeof(W) * tmp_w) + al(sizeof(T) * inv_w));
+    cudaError_t e = cudaMemsetAsync(invd, 0, sizeof(W) * inv_w, h->stream);
     if (e != cudaSuccess) return e;
-    const size_t sm_app = sizeof(W) * (NB * (NB + 1) + NB * 65);
-    const size_t sm_app_r = sizeof(W) * (NB * (NB + 1) + 64 * (NB + 1));
-    if ((e = cudaFuncSetAttribute(trsm_apply_left_kernel<T, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)sm_app)) != cudaSuccess)
+    const size_t sm_inv = sizeof(W) * 2 * NB * (NB + 1);
+    if ((e = cudaFuncSetAttribute(trsm_inv_diag_kernel<T, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sm_inv)) != cudaSuccess)
         return e;
-    if ((e = cudaFuncSetAttribute(trsm_apply_right_kernel<T, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)sm_app_r)) != cudaSuccess)
-        return e;
-    trsm_inv_diag_kernel<T, NB><<<nblk, NB, sm_inv, h->stream>>>(na, s.op, s.m_lower, s.unit, A, lda, inv);
+    trsm_inv_diag_kernel<T, NB><<<nsmall, NB, sm_inv, h->stream>>>(na, s.op, s.m_lower, s.unit, big, A, lda, invd);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    s.inv = inv;
-    e = s.solve(0, na, Gemm<T>::one());
+    constexpr int TS = NB;  // doubling tile: 64 real, 32 complex
+    for (int sz = NB; sz < big; sz *= 2) {
+        dim3 grid(sz / TS, sz / TS, nbig * (big / (2 * sz)));
+        trsm_inv_double_kernel<T, TS, 0><<<grid, 256, 0, h->stream>>>(na, s.op, s.m_lower, sz, big, A, lda, invd,
+                                                                       dtmp);
+        trsm_inv_double_kernel<T, TS, 1><<<grid, 256, 0, h->stream>>>(na, s.op, s.m_lower, sz, big, A, lda, invd,
+                                                                       dtmp);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    {
+        const long cnt = (long)inv_w;
+        const int g = (int)std::min<long>((cnt + 255) / 256, (long)h->sm_count * 8);
+        narrow_kernel<T><<<g, 256, 0, h->stream>>>(cnt, invd, inv32);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    s.inv = inv32;
+    e = s.solve(0, na);
     if (e != cudaSuccess || is_one(alpha)) return e;
     const long total = (long)m * n;
     const int grid = (int)std::min<long>((total + 255) / 256, (long)h->sm_count * 8);
