@@ -801,3 +801,73 @@ extern "C" iclblasStatus_t iclblasCtrsm(iclblasHandle_t h, iclblasSideMode_t sid
         return map_cuda(e);
     });
 }
+
+// ------------------------------------------------------------------------
+// adjoints (extension)
+// ------------------------------------------------------------------------
+extern "C" iclblasStatus_t iclblasStrsm_backward(iclblasHandle_t h, iclblasSideMode_t side, iclblasFillMode_t uplo,
+                                                 iclblasOperation_t trans, iclblasDiagType_t diag, int m, int n,
+                                                 const float* alpha, const float* A, int lda, const float* X, int ldx,
+                                                 float* G, int ldg, float* dA, int ldda)
+{
+    if (m == 0 || n == 0) return ICLBLAS_STATUS_SUCCESS;
+    return guarded([&]() -> iclblasStatus_t {
+        Params p; p.present = P_N | P_M | P_A | P_LDA | P_B | P_LDB;
+        p.n = n; p.m = m; p.A = A; p.lda = lda; p.B = G; p.ldb = ldg;
+        VALIDATE(p, h);
+        if (!alpha || !X || ldx <= 0 || (dA && ldda <= 0)) return ICLBLAS_STATUS_INVALID_VALUE;
+        if (trans < ICLBLAS_OP_N || trans > ICLBLAS_OP_C) return ICLBLAS_STATUS_INVALID_VALUE;
+        const int na = side == ICLBLAS_SIDE_LEFT ? m : n;
+        Stager st(h);
+        int ia = st.add(A, mat_extent(na, na, lda) * sizeof(float), false);
+        int ix = st.add(X, mat_extent(m, n, ldx) * sizeof(float), false);
+        int ig = st.add(G, mat_extent(m, n, ldg) * sizeof(float), true);
+        int id = dA ? st.add(dA, mat_extent(na, na, ldda) * sizeof(float), true) : -1;
+        cudaError_t e = st.stage_in();
+        if (e == cudaSuccess)
+            e = iclb::strsm_backward(h, side, uplo, trans, diag, m, n, *alpha, st.dev<float>(ia), lda,
+                                     st.dev<float>(ix), ldx, st.dev<float>(ig), ldg,
+                                     id >= 0 ? st.dev<float>(id) : nullptr, ldda);
+        if (e == cudaSuccess) e = st.finish();
+        return map_cuda(e);
+    });
+}
+
+extern "C" iclblasStatus_t iclblasSgemm_backward(iclblasHandle_t h, iclblasOperation_t transa,
+                                                 iclblasOperation_t transb, int m, int n, int k, const float* alpha,
+                                                 const float* A, int lda, const float* B, int ldb, const float* beta,
+                                                 const float* G, int ldg, float* dA, int ldda, float* dB, int lddb,
+                                                 float* dC, int lddc)
+{
+    if (m < 0 || n < 0 || k < 0) return ICLBLAS_STATUS_INVALID_VALUE;
+    return guarded([&]() -> iclblasStatus_t {
+        Params p; p.present = P_N | P_M | P_K | P_A | P_LDA | P_B | P_LDB | P_C | P_LDC;
+        p.n = n; p.m = m; p.k = k; p.A = A; p.lda = lda; p.B = B; p.ldb = ldb; p.C = G; p.ldc = ldg;
+        VALIDATE(p, h);
+        if (!alpha || !beta || (dA && ldda <= 0) || (dB && lddb <= 0) || (dC && lddc <= 0))
+            return ICLBLAS_STATUS_INVALID_VALUE;
+        if (transa < ICLBLAS_OP_N || transa > ICLBLAS_OP_C || transb < ICLBLAS_OP_N || transb > ICLBLAS_OP_C)
+            return ICLBLAS_STATUS_INVALID_VALUE;
+        const int ar = transa == ICLBLAS_OP_N ? m : k, ac = transa == ICLBLAS_OP_N ? k : m;
+        const int br = transb == ICLBLAS_OP_N ? k : n, bc = transb == ICLBLAS_OP_N ? n : k;
+        Stager st(h);
+        int ia = st.add(A, mat_extent(ar, ac, lda) * sizeof(float), false);
+        int ib = st.add(B, mat_extent(br, bc, ldb) * sizeof(float), false);
+        int ig = st.add(G, mat_extent(m, n, ldg) * sizeof(float), false);
+        int ida = dA ? st.add(dA, mat_extent(ar, ac, ldda) * sizeof(float), true) : -1;
+        int idb = dB ? st.add(dB, mat_extent(br, bc, lddb) * sizeof(float), true) : -1;
+        int idc = dC ? st.add(dC, mat_extent(m, n, lddc) * sizeof(float), true) : -1;
+        cudaError_t e = st.stage_in();
+        if (e == cudaSuccess && k > 0)
+            e = iclb::sgemm_backward(h, transa, transb, m, n, k, *alpha, st.dev<float>(ia), lda, st.dev<float>(ib),
+                                     ldb, *beta, st.dev<float>(ig), ldg, ida >= 0 ? st.dev<float>(ida) : nullptr,
+                                     ldda, idb >= 0 ? st.dev<float>(idb) : nullptr, lddb,
+                                     idc >= 0 ? st.dev<float>(idc) : nullptr, lddc);
+        else if (e == cudaSuccess && idc >= 0)
+            e = iclb::sgemm_backward(h, transa, transb, m, n, 0, *alpha, st.dev<float>(ia), lda, st.dev<float>(ib),
+                                     ldb, *beta, st.dev<float>(ig), ldg, nullptr, ldda, nullptr, lddb,
+                                     st.dev<float>(idc), lddc);
+        if (e == cudaSuccess) e = st.finish();
+        return map_cuda(e);
+    });
+}

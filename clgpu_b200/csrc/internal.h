@@ -39,6 +39,13 @@ struct Workspace {
 };
 constexpr int kCounterWords = 1 << 16;
 
+// ---------------------------------------------------------------- adjoints
+cudaError_t strsm_backward(iclblasHandle_t h, int side, int uplo, int trans, int diag, int m, int n, float alpha,
+                           const float* A, int lda, const float* X, int ldx, float* G, int ldg, float* dA, int ldda);
+cudaError_t sgemm_backward(iclblasHandle_t h, int ta, int tb, int m, int n, int k, float alpha, const float* A, int lda,
+                           const float* B, int ldb, float beta, const float* G, int ldg, float* dA, int ldda,
+                           float* dB, int lddb, float* dC, int lddc);
+
 }  // namespace iclb
 
 struct iclblasContext {
@@ -105,5 +112,12 @@ cudaError_t strsm(iclblasHandle_t h, int side, int uplo, int trans, int diag, in
                   const float* A, int lda, float* B, int ldb);
 cudaError_t ctrsm(iclblasHandle_t h, int side, int uplo, int trans, int diag, int m, int n, cfloat alpha,
                   const cfloat* A, int lda, cfloat* B, int ldb);
+
+// ---------------------------------------------------------------- adjoints
+cudaError_t strsm_backward(iclblasHandle_t h, int side, int uplo, int trans, int diag, int m, int n, float alpha,
+                           const float* A, int lda, const float* X, int ldx, float* G, int ldg, float* dA, int ldda);
+cudaError_t sgemm_backward(iclblasHandle_t h, int ta, int tb, int m, int n, int k, float alpha, const float* A, int lda,
+                           const float* B, int ldb, float beta, const float* G, int ldg, float* dA, int ldda,
+                           float* dB, int lddb, float* dC, int lddc);
 
 }  // namespace iclb

@@ -93,6 +93,8 @@ _SIGS = {
     "iclblasCgemm": [_H, _I, _I, _I, _I, _I, _P, _P, _I, _P, _I, _P, _P, _I],
     "iclblasStrsm": [_H, _I, _I, _I, _I, _I, _I, _P, _P, _I, _P, _I],
     "iclblasCtrsm": [_H, _I, _I, _I, _I, _I, _I, _P, _P, _I, _P, _I],
+    "iclblasStrsm_backward": [_H, _I, _I, _I, _I, _I, _I, _P, _P, _I, _P, _I, _P, _I, _P, _I],
+    "iclblasSgemm_backward": [_H, _I, _I, _I, _I, _I, _P, _P, _I, _P, _I, _P, _P, _I, _P, _I, _P, _I, _P, _I],
 }
 
 _lib = None
@@ -294,6 +296,17 @@ def iclblasStrsm(h, side, uplo, trans, diag, m, n, alpha, A, lda, B, ldb):
 def iclblasCtrsm(h, side, uplo, trans, diag, m, n, alpha, A, lda, B, ldb):
     return _call("iclblasCtrsm", _h(h), side, uplo, trans, diag, m, n, C.byref(_cscalar(alpha)), ptr(A), lda, ptr(B),
                  ldb)
+
+
+def iclblasStrsm_backward(h, side, uplo, trans, diag, m, n, alpha, A, lda, X, ldx, G, ldg, dA, ldda):
+    return _call("iclblasStrsm_backward", _h(h), side, uplo, trans, diag, m, n, C.byref(_fscalar(alpha)), ptr(A), lda,
+                 ptr(X), ldx, ptr(G), ldg, ptr(dA), ldda)
+
+
+def iclblasSgemm_backward(h, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, G, ldg, dA, ldda, dB, lddb, dC,
+                          lddc):
+    return _call("iclblasSgemm_backward", _h(h), transa, transb, m, n, k, C.byref(_fscalar(alpha)), ptr(A), lda,
+                 ptr(B), ldb, C.byref(_fscalar(beta)), ptr(G), ldg, ptr(dA), ldda, ptr(dB), lddb, ptr(dC), lddc)
 
 
 def check(status: int, fn: str = "iclblas call") -> None:

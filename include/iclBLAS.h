@@ -207,6 +207,26 @@ ICLBLAS_API iclblasStatus_t iclblasGetMathMode(iclblasHandle_t handle, iclblasMa
  * error flag (a bounded wait that ran out) as EXECUTION_FAILED. */
 ICLBLAS_API iclblasStatus_t iclblasSynchronize(iclblasHandle_t handle);
 
+/* Adjoints (reverse-mode derivatives), no reference counterpart.
+ * iclblasStrsm_backward: given the TRSM inputs A, the solution X (= the B that
+ * iclblasStrsm returned) and G = dL/dX, overwrites G with dL/dB and writes
+ * dL/dA into dA on the stored triangle of A (zero elsewhere; zero diagonal for
+ * a unit diagonal).  dA may be NULL.  Left side: W = op(A)^-T G, dB = alpha W,
+ * d op(A) = -W X^T; right side: W = G op(A)^-T, dB = alpha W,
+ * d op(A) = -X^T W. */
+ICLBLAS_API iclblasStatus_t iclblasStrsm_backward(iclblasHandle_t handle, iclblasSideMode_t side, iclblasFillMode_t uplo,
+                                                  iclblasOperation_t trans, iclblasDiagType_t diag, int m, int n,
+                                                  const float* alpha, const float* A, int lda, const float* X, int ldx,
+                                                  float* G, int ldg, float* dA, int ldda);
+/* iclblasSgemm_backward: for C = alpha*op(A)*op(B) + beta*C_in and G = dL/dC,
+ * writes dL/dA (shape of A), dL/dB (shape of B) and dL/dC_in = beta*G; any of
+ * dA, dB, dC may be NULL. */
+ICLBLAS_API iclblasStatus_t iclblasSgemm_backward(iclblasHandle_t handle, iclblasOperation_t transa,
+                                                  iclblasOperation_t transb, int m, int n, int k, const float* alpha,
+                                                  const float* A, int lda, const float* B, int ldb, const float* beta,
+                                                  const float* G, int ldg, float* dA, int ldda, float* dB, int lddb,
+                                                  float* dC, int lddc);
+
 #ifdef __cplusplus
 }
 #endif
