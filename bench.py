@@ -557,6 +557,136 @@ def run_trsm_study(args, torch):
     return out
 
 
+def run_batched_study(args, torch):
+    """Batched uneven TRSM + adjoint config: 512 instances, n ~ UniformInt[32,1024],
+    nrhs ~ UniformInt[1,256], L built as in the STRSM config (diagonal U(1,2),
+    strictly lower N(0,1)/sqrt(n)), B and upstream gradients N(0,1), seed 4.
+    One step = the forward solve X = L^-1 B (one persistent launch) plus the
+    adjoint (dB = L^-T G, one persistent launch; dA = -tril(dB X^T), one
+    persistent launch), replayed as one CUDA graph.  Algorithmic flops per
+    step: 3 * sum(n^2 * nrhs) (forward n^2 r, adjoint solve n^2 r, the kept
+    triangle of dB X^T n^2 r).  Compared with the plain form: the same work as
+    per-instance iclblasStrsm + iclblasStrsm_backward calls (PLAIN_FP32).
+    Errors: relative Frobenius error of X, dB and dA against FP64 torch
+    (solve_triangular and its formulae in float64, plumbing only), worst
+    instance."""
+    import numpy as np
+    from clgpu_b200 import iclblas as B
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(device=dev)
+    rng = np.random.default_rng(4)
+    g = torch.Generator(device=dev).manual_seed(4)
+    batch = args.batch
+    ns = rng.integers(32, 1025, batch)
+    rs = rng.integers(1, 257, batch)
+    Ls, As, B0, G0 = [], [], [], []
+    for n, r in zip(ns, rs):
+        n, r = int(n), int(r)
+        L = torch.tril(torch.randn(n, n, generator=g, device=dev) / n ** 0.5, -1)
+        L = L + torch.diag(torch.rand(n, generator=g, device=dev) + 1.0)
+        Ls.append(L)
+        As.append(L.t().contiguous().reshape(-1))             # column-major storage
+        B0.append(torch.randn(r, n, generator=g, device=dev).reshape(-1))
+        G0.append(torch.randn(r, n, generator=g, device=dev).reshape(-1))
+    flops = 3.0 * float(np.sum(ns.astype(np.float64) ** 2 * rs))
+    X = [b.clone() for b in B0]
+    Gw = [b.clone() for b in G0]
+    dA = [torch.empty(int(n) * int(n), device=dev) for n in ns]
+    P = lambda ts: torch.tensor([t.data_ptr() for t in ts], dtype=torch.int64, device=dev)  # noqa: E731
+    pA, pX, pG, pdA = P(As), P(X), P(Gw), P(dA)
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    def restore():
+        for x, b in zip(X, B0):
+            x.copy_(b)
+        for gw, g0 in zip(Gw, G0):
+            gw.copy_(g0)
+
+    def errors():
+        worst = [0.0, 0.0, 0.0]
+        for i in range(batch):
+            n, r = int(ns[i]), int(rs[i])
+            L64 = Ls[i].double()
+            Bm = B0[i].view(r, n).t().double()
+            Gm = G0[i].view(r, n).t().double()
+            X64 = torch.linalg.solve_triangular(L64, Bm, upper=False)
+            W64 = torch.linalg.solve_triangular(L64.t(), Gm, upper=True)
+            dA64 = torch.tril(-W64 @ X64.t())
+            got = (X[i].view(r, n).t().double(), Gw[i].view(r, n).t().double(), dA[i].view(n, n).t().double())
+            for j, (a, b) in enumerate(zip(got, (X64, W64, dA64))):
+                worst[j] = max(worst[j], (torch.linalg.norm(a - b) / torch.linalg.norm(b)).item())
+        return worst
+
+    out = []
+    with B.Handle() as h, torch.cuda.stream(stream):
+        h.set_stream(stream)
+        plan = B.BatchPlan(h, "trsm", side=0, uplo=1, trans=0, diag=0, m=[int(v) for v in ns],
+                           n=[int(v) for v in rs], lda=[int(v) for v in ns], ldb=[int(v) for v in ns])
+        _, width, ctas = plan.info()
+
+        def step():
+            B.check(B.iclblasStrsmBatchedUneven(h, plan, 1.0, pA, pX), "batched trsm")
+            B.check(B.iclblasStrsmBatchedUnevenBackward(h, plan, 1.0, pA, pX, pG, pdA), "batched adjoint")
+
+        # the restore copies are captured too; their own graph's time is subtracted
+        restore()
+        torch.cuda.synchronize()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=stream):
+            restore()
+            step()
+        rgraph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(rgraph, stream=stream):
+            restore()
+        for _ in range(args.warmup):
+            graph.replay()
+        reps = max(args.steps, 3)
+        ms_all = timed(graph.replay, reps)
+        ms_copy = timed(rgraph.replay, reps)
+        ms = max(ms_all - ms_copy, 1e-6)
+        graph.replay()
+        torch.cuda.synchronize()
+        ex, eg, ea = errors()
+        r = {"routine": "batched strsm fwd+adjoint", "batch": batch, "form": "persistent launches in a CUDA graph",
+             "tile_width": width, "ctas_per_sm": ctas, "tflops": round(flops / (ms / 1e3) / 1e12, 3),
+             "ms": round(ms, 3), "err_X": ex, "err_dB": eg, "err_dA": ea}
+        print(json.dumps(r), flush=True)
+        out.append(r)
+
+        # plain form: per-instance calls (PLAIN_FP32)
+        h.set_math_mode(B.MATH_PLAIN_FP32)
+
+        def loop_step():
+            restore()
+            for i in range(batch):
+                n, rr = int(ns[i]), int(rs[i])
+                B.check(B.iclblasStrsm(h, 0, 1, 0, 0, n, rr, 1.0, As[i], n, X[i], n), "strsm")
+                B.check(B.iclblasStrsm_backward(h, 0, 1, 0, 0, n, rr, 1.0, As[i], n, X[i], n, Gw[i], n, dA[i], n),
+                        "strsm_backward")
+        ms_loop = max(timed(loop_step, 3) - ms_copy, 1e-6)
+        ex, eg, ea = errors()
+        r = {"routine": "batched strsm fwd+adjoint", "batch": batch, "form": "per-instance calls, plain FP32",
+             "tflops": round(flops / (ms_loop / 1e3) / 1e12, 3), "ms": round(ms_loop, 3), "err_X": ex, "err_dB": eg,
+             "err_dA": ea}
+        print(json.dumps(r), flush=True)
+        out.append(r)
+        del graph, rgraph
+        plan.destroy()
+    return out
+
+
 # ---------------------------------------------------------------- CPU (reference code)
 SAMPLE_N1 = 1 << 24
 SAMPLE_GN = 4096
@@ -657,15 +787,16 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-operand (C ABI) leg")
     ap.add_argument("--only", default="", help="comma-separated subset of the sweep's calls")
     ap.add_argument("--n1", type=int, default=N1, help="level-1 vector length (default 2^28)")
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "gemm", "trsm"],
-                    help="sweep: the bandwidth config (default); gemm / trsm: the precision and "
-                         "triangular-solve config studies")
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "gemm", "trsm", "batched"],
+                    help="sweep: the bandwidth config (default); gemm / trsm / batched: the precision, "
+                         "triangular-solve and batched-solve config studies")
     ap.add_argument("--trsm-m", type=int, default=8192)
     ap.add_argument("--trsm-n", type=int, default=4096)
     ap.add_argument("--trsv-n", type=int, default=16384)
     ap.add_argument("--gemm-n", type=int, default=8192)
     ap.add_argument("--skip-cgemm", action="store_true")
     ap.add_argument("--quick", action="store_true")
+    ap.add_argument("--batch", type=int, default=512)
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -700,6 +831,9 @@ def main():
         return
     if args.workload == "trsm":
         run_trsm_study(args, torch)
+        return
+    if args.workload == "batched":
+        run_batched_study(args, torch)
         return
     if world > 1:
         torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))

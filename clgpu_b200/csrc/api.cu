@@ -871,3 +871,118 @@ extern "C" iclblasStatus_t iclblasSgemm_backward(iclblasHandle_t h, iclblasOpera
         return map_cuda(e);
     });
 }
+
+// ------------------------------------------------------------------------
+// uneven batched TRSM / GEMM (extension)
+// ------------------------------------------------------------------------
+namespace {
+
+bool plan_ok(iclblasBatchPlan_t p, int kind) { return p != nullptr && p->tag == kBatchPlanTag && p->kind == kind; }
+
+bool op_ok(int t) { return t >= ICLBLAS_OP_N && t <= ICLBLAS_OP_C; }
+
+// Arrays of per-instance pointers must be device memory (the kernels read them).
+bool ptr_array_ok(const void* p) { return p != nullptr && is_device_ptr(p); }
+
+}  // namespace
+
+extern "C" iclblasStatus_t iclblasStrsmBatchedPlanCreate(iclblasHandle_t h, iclblasSideMode_t side,
+                                                         iclblasFillMode_t uplo, iclblasOperation_t trans,
+                                                         iclblasDiagType_t diag, int batch, const int* m, const int* n,
+                                                         const int* lda, const int* ldb, iclblasBatchPlan_t* plan)
+{
+    return guarded([&]() -> iclblasStatus_t {
+        if (!plan) return ICLBLAS_STATUS_INVALID_VALUE;
+        *plan = nullptr;
+        if (!handle_ok(h) || batch < 0) return ICLBLAS_STATUS_INVALID_VALUE;
+        if (batch > 0 && (!m || !n || !lda || !ldb)) return ICLBLAS_STATUS_INVALID_VALUE;
+        if ((side != ICLBLAS_SIDE_LEFT && side != ICLBLAS_SIDE_RIGHT) ||
+            (uplo != ICLBLAS_FILL_MODE_UPPER && uplo != ICLBLAS_FILL_MODE_LOWER) || !op_ok(trans) ||
+            (diag != ICLBLAS_DIAG_NON_UNIT && diag != ICLBLAS_DIAG_UNIT))
+            return ICLBLAS_STATUS_INVALID_VALUE;
+        if (side != ICLBLAS_SIDE_LEFT) return ICLBLAS_STATUS_NOT_SUPPORTED;
+        for (int i = 0; i < batch; ++i) {
+            const int lo = m[i] > 1 ? m[i] : 1;
+            if (m[i] < 0 || n[i] < 0 || lda[i] < lo || ldb[i] < lo) return ICLBLAS_STATUS_INVALID_VALUE;
+        }
+        return map_cuda(iclb::batch_plan_create_trsm(h, side, uplo, trans, diag, batch, m, n, lda, ldb, plan));
+    });
+}
+
+extern "C" iclblasStatus_t iclblasSgemmBatchedPlanCreate(iclblasHandle_t h, iclblasOperation_t transa,
+                                                         iclblasOperation_t transb, int batch, const int* m,
+                                                         const int* n, const int* k, const int* lda, const int* ldb,
+                                                         const int* ldc, iclblasBatchPlan_t* plan)
+{
+    return guarded([&]() -> iclblasStatus_t {
+        if (!plan) return ICLBLAS_STATUS_INVALID_VALUE;
+        *plan = nullptr;
+        if (!handle_ok(h) || batch < 0 || !op_ok(transa) || !op_ok(transb)) return ICLBLAS_STATUS_INVALID_VALUE;
+        if (batch > 0 && (!m || !n || !k || !lda || !ldb || !ldc)) return ICLBLAS_STATUS_INVALID_VALUE;
+        for (int i = 0; i < batch; ++i) {
+            if (m[i] < 0 || n[i] < 0 || k[i] < 0) return ICLBLAS_STATUS_INVALID_VALUE;
+            const int ar = transa == ICLBLAS_OP_N ? m[i] : k[i];
+            const int br = transb == ICLBLAS_OP_N ? k[i] : n[i];
+            if (lda[i] < (ar > 1 ? ar : 1) || ldb[i] < (br > 1 ? br : 1) || ldc[i] < (m[i] > 1 ? m[i] : 1))
+                return ICLBLAS_STATUS_INVALID_VALUE;
+        }
+        return map_cuda(iclb::batch_plan_create_gemm(h, transa, transb, batch, m, n, k, lda, ldb, ldc, plan));
+    });
+}
+
+extern "C" iclblasStatus_t iclblasBatchPlanDestroy(iclblasBatchPlan_t plan)
+{
+    return guarded([&]() -> iclblasStatus_t {
+        if (!plan || plan->tag != kBatchPlanTag) return ICLBLAS_STATUS_INVALID_VALUE;
+        iclb::batch_plan_free(plan);
+        return ICLBLAS_STATUS_SUCCESS;
+    });
+}
+
+extern "C" iclblasStatus_t iclblasBatchPlanGetInfo(iclblasBatchPlan_t plan, double* flops, int* tile_width,
+                                                   int* ctas_per_sm)
+{
+    if (!plan || plan->tag != kBatchPlanTag) return ICLBLAS_STATUS_INVALID_VALUE;
+    if (flops) *flops = plan->flops;
+    if (tile_width) *tile_width = plan->main.rc;
+    if (ctas_per_sm) *ctas_per_sm = plan->main.ctas_per_sm;
+    return ICLBLAS_STATUS_SUCCESS;
+}
+
+extern "C" iclblasStatus_t iclblasStrsmBatchedUneven(iclblasHandle_t h, iclblasBatchPlan_t plan, const float* alpha,
+                                                     const float* const* A, float* const* B)
+{
+    return guarded([&]() -> iclblasStatus_t {
+        if (!handle_ok(h) || !plan_ok(plan, 0) || !alpha) return ICLBLAS_STATUS_INVALID_VALUE;
+        if (plan->batch == 0) return ICLBLAS_STATUS_SUCCESS;
+        if (plan->device != h->device || !ptr_array_ok(A) || !ptr_array_ok(B)) return ICLBLAS_STATUS_INVALID_VALUE;
+        return map_cuda(iclb::batch_trsm(h, plan, *alpha, A, B));
+    });
+}
+
+extern "C" iclblasStatus_t iclblasSgemmBatchedUneven(iclblasHandle_t h, iclblasBatchPlan_t plan, const float* alpha,
+                                                     const float* const* A, const float* const* B, const float* beta,
+                                                     float* const* C)
+{
+    return guarded([&]() -> iclblasStatus_t {
+        if (!handle_ok(h) || !plan_ok(plan, 1) || !alpha || !beta) return ICLBLAS_STATUS_INVALID_VALUE;
+        if (plan->batch == 0) return ICLBLAS_STATUS_SUCCESS;
+        if (plan->device != h->device || !ptr_array_ok(A) || !ptr_array_ok(B) || !ptr_array_ok(C))
+            return ICLBLAS_STATUS_INVALID_VALUE;
+        return map_cuda(iclb::batch_gemm(h, plan, *alpha, A, B, *beta, C));
+    });
+}
+
+extern "C" iclblasStatus_t iclblasStrsmBatchedUnevenBackward(iclblasHandle_t h, iclblasBatchPlan_t plan,
+                                                             const float* alpha, const float* const* A,
+                                                             const float* const* X, float* const* G, float* const* dA)
+{
+    return guarded([&]() -> iclblasStatus_t {
+        if (!handle_ok(h) || !plan_ok(plan, 0) || !alpha) return ICLBLAS_STATUS_INVALID_VALUE;
+        if (plan->batch == 0) return ICLBLAS_STATUS_SUCCESS;
+        if (plan->device != h->device || !ptr_array_ok(A) || !ptr_array_ok(X) || !ptr_array_ok(G) ||
+            (dA && !ptr_array_ok(dA)))
+            return ICLBLAS_STATUS_INVALID_VALUE;
+        return map_cuda(iclb::batch_trsm_backward(h, plan, *alpha, A, X, G, dA));
+    });
+}

@@ -1,0 +1,737 @@
+// Uneven batched TRSM and GEMM in one persistent launch each, plus the
+// batched TRSM adjoint.  No reference counterpart: the reference has no
+// batched routines; these extend its TRSM and GEMM to many independent
+// instances of different sizes.
+//
+// A plan holds, in device memory, each instance's sizes and a work list of
+// (instance, tile) items sorted by decreasing cost (longest first, which
+// balances the uneven sizes).  A launch runs (SM count x CTAs per SM)
+// persistent CTAs that take items from an atomic queue until it is empty.
+//   TRSM item: one instance, RC right-hand sides.  Left-looking blocked solve
+//     over 64-row blocks of M = op(A) in solve order: the block's RHS rows
+//     (scaled by alpha on load) minus M[blk, earlier] * X[earlier] (a 64 x RC
+//     register-tiled product per earlier block, operands staged in shared
+//     memory), then substitution on the 64 x 64 diagonal block in shared
+//     memory, store.  Left side only.
+//   GEMM item: one 64 x RC tile of one instance's C.
+// The queue head is cleared with cudaMemsetAsync before each launch, so a
+// call is a memset node plus a kernel node and can be captured in a CUDA
+// graph (the plan, its work lists and its tuning are built before).
+// The tile width RC in {32, 64} and the CTAs per SM in {1, 2, 4} are chosen
+// by timing the candidates on synthetic operands of the plan's shapes when
+// the plan is created; the choice is cached per (kind, shapes, GPU) in memory
+// and, when ICLBLAS_TUNE_CACHE names a file, on disk (one "key rc ctas" line
+// each).  All arithmetic is FP32 FMA on the CUDA cores, whatever the handle's
+// math mode.
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+namespace iclb {
+
+namespace {
+
+constexpr int TB = 64;  // row block / tile height
+
+// ---------------------------------------------------------------- TRSM kernel
+template <int RC>
+__global__ void __launch_bounds__(256) batched_trsm_kernel(int nitems, const int2* __restrict__ items,
+                                                           const int* __restrict__ dims, int lower_op, int op,
+                                                           int unit, float alpha, const float* const* __restrict__ Aptr,
+                                                           float* const* __restrict__ Bptr, unsigned* counter)
+{
+    constexpr int CPT = RC / 16;   // columns per thread in the update
+    constexpr int G = 256 / RC;    // row groups in the substitution
+    __shared__ float Ms[TB][TB + 1];
+    __shared__ float Xs[TB][RC + 1];
+    __shared__ int item_sh;
+    const int t = threadIdx.x, tx = t % 16, ty = t / 16;
+    for (;;) {
+        __syncthreads();
+        if (t == 0) item_sh = (int)atomicAdd(counter, 1u);
+        __syncthreads();
+        const int it = item_sh;
+        if (it >= nitems) break;
+        const int2 w = items[it];
+        const int* d = dims + 4 * w.x;
+        const int m = d[0], nrhs = d[1];
+        const long lda = d[2], ldb = d[3];
+        const float* A = Aptr[w.x];
+        float* B = Bptr[w.x];
+        const int c0 = w.y * RC, nc = min(RC, nrhs - c0);
+        const int nb = (m + TB - 1) / TB;
+        for (int p = 0; p < nb; ++p) {
+            const int kb = lower_op ? p : nb - 1 - p;
+            const int r0 = kb * TB, nr = min(TB, m - r0);
+            float acc[4][CPT];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < CPT; ++j) {
+                    const int r = ty * 4 + i, c = tx * CPT + j;
+                    acc[i][j] = (r < nr && c < nc) ? alpha * B[(long)(c0 + c) * ldb + r0 + r] : 0.f;
+                }
+            for (int q = 0; q < p; ++q) {
+                const int jb = lower_op ? q : nb - 1 - q;
+                const int j0 = jb * TB, nj = min(TB, m - j0);
+                __syncthreads();
+                for (int idx = t; idx < TB * TB; idx += 256) {
+                    int r, cc;
+                    if (op == 0) { r = idx % TB; cc = idx / TB; } else { cc = idx % TB; r = idx / TB; }
+                    float v = 0.f;
+                    if (r < nr && cc < nj)
+                        v = op == 0 ? A[(long)(j0 + cc) * lda + r0 + r] : A[(long)(r0 + r) * lda + j0 + cc];
+                    Ms[r][cc] = v;
+                }
+                for (int idx = t; idx < TB * RC; idx += 256) {
+                    const int r = idx % TB, c = idx / TB;
+                    Xs[r][c] = (r < nj && c < nc) ? B[(long)(c0 + c) * ldb + j0 + r] : 0.f;
+                }
+                __syncthreads();
+#pragma unroll 8
+                for (int k = 0; k < TB; ++k) {
+                    float a[4], b[CPT];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) a[i] = Ms[ty * 4 + i][k];
+#pragma unroll
+                    for (int j = 0; j < CPT; ++j) b[j] = Xs[k][tx * CPT + j];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+#pragma unroll
+                        for (int j = 0; j < CPT; ++j) acc[i][j] = fmaf(-a[i], b[j], acc[i][j]);
+                }
+            }
+            // diagonal block: RHS rows into shared memory, substitution
+            __syncthreads();
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < CPT; ++j) Xs[ty * 4 + i][tx * CPT + j] = acc[i][j];
+            for (int idx = t; idx < TB * TB; idx += 256) {
+                int r, cc;
+                if (op == 0) { r = idx % TB; cc = idx / TB; } else { cc = idx % TB; r = idx / TB; }
+                float v = 0.f;
+                if (r < nr && cc < nr)
+                    v = op == 0 ? A[(long)(r0 + cc) * lda + r0 + r] : A[(long)(r0 + r) * lda + r0 + cc];
+                Ms[r][cc] = v;
+            }
+            __syncthreads();
+            const int c = t % RC, rg = t / RC;
+            if (lower_op) {
+                for (int k = 0; k < nr; ++k) {
+                    if (rg == k % G && !unit) Xs[k][c] = Xs[k][c] / Ms[k][k];
+                    __syncthreads();
+                    const float xk = Xs[k][c];
+                    for (int r = rg; r < nr; r += G)
+                        if (r > k) Xs[r][c] = fmaf(-Ms[r][k], xk, Xs[r][c]);
+                    __syncthreads();
+                }
+            } else {
+                for (int k = nr - 1; k >= 0; --k) {
+                    if (rg == k % G && !unit) Xs[k][c] = Xs[k][c] / Ms[k][k];
+                    __syncthreads();
+                    const float xk = Xs[k][c];
+                    for (int r = rg; r < k; r += G) Xs[r][c] = fmaf(-Ms[r][k], xk, Xs[r][c]);
+                    __syncthreads();
+                }
+            }
+            for (int idx = t; idx < TB * RC; idx += 256) {
+                const int r = idx % TB, cc = idx / TB;
+                if (r < nr && cc < nc) B[(long)(c0 + cc) * ldb + r0 + r] = Xs[r][cc];
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- GEMM kernel
+// MODE 0: C = alpha*op(A)*op(B) + beta*C, each element's products summed in
+// k order by FP32 FMA from zero, then fmaf(alpha, acc, beta*C) (alpha*acc
+// when beta == 0), the order of the single-instance plain SGEMM.
+// MODE 1 (adjoint of TRSM): C is an m x m block kept on the triangle
+// `tri_lower` (strict when `tri_strict`), zero elsewhere.
+template <int RC, int MODE>
+__global__ void __launch_bounds__(256) batched_gemm_kernel(int nitems, const int2* __restrict__ items,
+                                                           const int* __restrict__ dims, int ta, int tb, float alpha,
+                                                           float beta, const float* const* __restrict__ Aptr,
+                                                           const float* const* __restrict__ Bptr,
+                                                           float* const* __restrict__ Cptr, unsigned* counter,
+                                                           int tri_lower, int tri_strict)
+{
+    constexpr int CPT = RC / 16;
+    __shared__ float As[TB][TB + 1];
+    __shared__ float Bs[TB][RC + 1];
+    __shared__ int item_sh;
+    const int t = threadIdx.x, tx = t % 16, ty = t / 16;
+    for (;;) {
+        __syncthreads();
+        if (t == 0) item_sh = (int)atomicAdd(counter, 1u);
+        __syncthreads();
+        const int it = item_sh;
+        if (it >= nitems) break;
+        const int2 w = items[it];
+        const int* d = dims + 6 * w.x;
+        const int m = d[0], n = d[1], k = d[2];
+        const long lda = d[3], ldb = d[4], ldc = d[5];
+        const float* A = Aptr[w.x];
+        const float* Bm = Bptr[w.x];
+        float* C = Cptr[w.x];
+        const int tiles_m = (m + TB - 1) / TB;
+        const int tm = w.y % tiles_m, tn = w.y / tiles_m;
+        const int i0 = tm * TB, j0 = tn * RC;
+        // adjoint tiles entirely off the kept triangle are only zeroed
+        bool skip = false;
+        if (MODE == 1) skip = tri_lower ? (j0 > i0 + TB - 1) : (i0 > j0 + RC - 1);
+        float acc[4][CPT];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < CPT; ++j) acc[i][j] = 0.f;
+        for (int k0 = 0; k0 < k && !skip; k0 += TB) {
+            __syncthreads();
+            for (int idx = t; idx < TB * TB; idx += 256) {
+                int r, kk;
+                if (ta == 0) { r = idx % TB; kk = idx / TB; } else { kk = idx % TB; r = idx / TB; }
+                float v = 0.f;
+                if (i0 + r < m && k0 + kk < k)
+                    v = ta == 0 ? A[(long)(k0 + kk) * lda + i0 + r] : A[(long)(i0 + r) * lda + k0 + kk];
+                As[r][kk] = v;
+            }
+            for (int idx = t; idx < TB * RC; idx += 256) {
+                int kk, c;
+                if (tb == 0) { kk = idx % TB; c = idx / TB; } else { c = idx % RC; kk = idx / RC; }
+                float v = 0.f;
+                if (k0 + kk < k && j0 + c < n)
+                    v = tb == 0 ? Bm[(long)(j0 + c) * ldb + k0 + kk] : Bm[(long)(k0 + kk) * ldb + j0 + c];
+                Bs[kk][c] = v;
+            }
+            __syncthreads();
+#pragma unroll 8
+            for (int kk = 0; kk < TB; ++kk) {
+                float a[4], b[CPT];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) a[i] = As[ty * 4 + i][kk];
+#pragma unroll
+                for (int j = 0; j < CPT; ++j) b[j] = Bs[kk][tx * CPT + j];
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int j = 0; j < CPT; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < CPT; ++j) {
+                const int r = i0 + ty * 4 + i, c = j0 + tx * CPT + j;
+                if (r >= m || c >= n) continue;
+                float* cp = C + (long)c * ldc + r;
+                if (MODE == 1) {
+                    const bool keep = tri_lower ? (r > c || (r == c && !tri_strict))
+                                                : (r < c || (r == c && !tri_strict));
+                    *cp = keep ? alpha * acc[i][j] : 0.f;
+                } else {
+                    *cp = beta == 0.f ? alpha * acc[i][j] : fmaf(alpha, acc[i][j], __fmul_rn(beta, *cp));
+                }
+            }
+    }
+}
+
+// Synthetic operand fill for tuning.
+__global__ void tune_fill_kernel(long count, float* __restrict__ p, float v)
+{
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (long)gridDim.x * blockDim.x) p[i] = v;
+}
+
+__global__ void tune_ptrs_kernel(int batch, const float** __restrict__ a, const float* pa, const float** __restrict__ b,
+                                 const float* pb, const float** __restrict__ c, const float* pc)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < batch; i += gridDim.x * blockDim.x) {
+        a[i] = pa;
+        b[i] = pb;
+        c[i] = pc;
+    }
+}
+
+// ---------------------------------------------------------------- host: work lists
+struct Item {
+    double cost;
+    int2 w;
+};
+
+void sort_items(std::vector<Item>& v)
+{
+    std::stable_sort(v.begin(), v.end(), [](const Item& a, const Item& b) { return a.cost > b.cost; });
+}
+
+// TRSM: one item per (instance, RC-wide column block); cost m^2 * columns.
+std::vector<int2> trsm_items(int batch, const std::vector<int>& dims, int rc)
+{
+    std::vector<Item> v;
+    for (int i = 0; i < batch; ++i) {
+        const int m = dims[4 * i], n = dims[4 * i + 1];
+        if (m == 0 || n == 0) continue;
+        for (int c = 0; c * rc < n; ++c) {
+            const int nc = std::min(rc, n - c * rc);
+            v.push_back({(double)m * m * nc + (double)m * rc, make_int2(i, c)});
+        }
+    }
+    sort_items(v);
+    std::vector<int2> out(v.size());
+    for (size_t i = 0; i < v.size(); ++i) out[i] = v[i].w;
+    return out;
+}
+
+// GEMM: one item per 64 x RC tile of C; cost k (tiles off the kept triangle
+// of the adjoint product cost a store only).
+std::vector<int2> gemm_items(int batch, const std::vector<int>& dims, int rc, bool masked, bool tri_lower)
+{
+    std::vector<Item> v;
+    for (int i = 0; i < batch; ++i) {
+        const int m = dims[6 * i], n = dims[6 * i + 1], k = dims[6 * i + 2];
+        if (m == 0 || n == 0) continue;
+        const int tm = (m + TB - 1) / TB, tn = (n + rc - 1) / rc;
+        for (int b = 0; b < tm * tn; ++b) {
+            const int i0 = (b % tm) * TB, j0 = (b / tm) * rc;
+            const bool skip = masked && (tri_lower ? (j0 > i0 + TB - 1) : (i0 > j0 + rc - 1));
+            v.push_back({skip ? 1.0 : (double)k * TB * rc + TB * rc, make_int2(i, b)});
+        }
+    }
+    sort_items(v);
+    std::vector<int2> out(v.size());
+    for (size_t i = 0; i < v.size(); ++i) out[i] = v[i].w;
+    return out;
+}
+
+cudaError_t upload_items(const std::vector<int2>& items, BatchList& l)
+{
+    if (l.items) cudaFree(l.items);
+    l.items = nullptr;
+    l.nitems = (int)items.size();
+    if (items.empty()) return cudaSuccess;
+    cudaError_t e = cudaMalloc(&l.items, items.size() * sizeof(int2));
+    if (e != cudaSuccess) return e;
+    return cudaMemcpy(l.items, items.data(), items.size() * sizeof(int2), cudaMemcpyHostToDevice);
+}
+
+cudaError_t upload_dims(const std::vector<int>& dims, BatchList& l)
+{
+    if (dims.empty()) return cudaSuccess;
+    cudaError_t e = cudaMalloc(&l.dims, dims.size() * sizeof(int));
+    if (e != cudaSuccess) return e;
+    return cudaMemcpy(l.dims, dims.data(), dims.size() * sizeof(int), cudaMemcpyHostToDevice);
+}
+
+int grid_of(iclblasHandle_t h, const BatchList& l)
+{
+    return std::max(1, std::min(l.nitems, h->sm_count * l.ctas_per_sm));
+}
+
+// ---------------------------------------------------------------- host: launches
+cudaError_t launch_trsm(iclblasHandle_t h, const BatchList& l, unsigned* counter, int lower_op, int op, int unit,
+                        float alpha, const float* const* A, float* const* B)
+{
+    if (l.nitems == 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned), h->stream);
+    if (e != cudaSuccess) return e;
+    const int grid = grid_of(h, l);
+    if (l.rc == 32)
+        batched_trsm_kernel<32><<<grid, 256, 0, h->stream>>>(l.nitems, l.items, l.dims, lower_op, op, unit, alpha, A, B,
+                                                             counter);
+    else
+        batched_trsm_kernel<64><<<grid, 256, 0, h->stream>>>(l.nitems, l.items, l.dims, lower_op, op, unit, alpha, A, B,
+                                                             counter);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gemm(iclblasHandle_t h, const BatchList& l, unsigned* counter, bool masked, int ta, int tb,
+                        float alpha, float beta, const float* const* A, const float* const* B, float* const* C,
+                        int tri_lower, int tri_strict)
+{
+    if (l.nitems == 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned), h->stream);
+    if (e != cudaSuccess) return e;
+    const int grid = grid_of(h, l);
+    if (masked) {
+        if (l.rc == 32)
+            batched_gemm_kernel<32, 1><<<grid, 256, 0, h->stream>>>(l.nitems, l.items, l.dims, ta, tb, alpha, beta, A,
+                                                                    B, C, counter, tri_lower, tri_strict);
+        else
+            batched_gemm_kernel<64, 1><<<grid, 256, 0, h->stream>>>(l.nitems, l.items, l.dims, ta, tb, alpha, beta, A,
+                                                                    B, C, counter, tri_lower, tri_strict);
+    } else {
+        if (l.rc == 32)
+            batched_gemm_kernel<32, 0><<<grid, 256, 0, h->stream>>>(l.nitems, l.items, l.dims, ta, tb, alpha, beta, A,
+                                                                    B, C, counter, 0, 0);
+        else
+            batched_gemm_kernel<64, 0><<<grid, 256, 0, h->stream>>>(l.nitems, l.items, l.dims, ta, tb, alpha, beta, A,
+                                                                    B, C, counter, 0, 0);
+    }
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- host: tuning cache
+struct Choice {
+    int rc, ctas;
+};
+std::mutex g_tune_mu;
+std::map<std::string, Choice> g_tune;
+bool g_tune_loaded = false;
+
+const char* tune_path()
+{
+    const char* p = std::getenv("ICLBLAS_TUNE_CACHE");
+    return (p && *p) ? p : nullptr;
+}
+
+void load_tune_file_locked()
+{
+    if (g_tune_loaded) return;
+    g_tune_loaded = true;
+    const char* path = tune_path();
+    if (!path) return;
+    std::ifstream f(path);
+    std::string key;
+    int rc, ctas;
+    while (f >> key >> rc >> ctas)
+        if ((rc == 32 || rc == 64) && (ctas == 1 || ctas == 2 || ctas == 4)) g_tune[key] = Choice{rc, ctas};
+}
+
+bool lookup_tune(const std::string& key, Choice& c)
+{
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    load_tune_file_locked();
+    auto it = g_tune.find(key);
+    if (it == g_tune.end()) return false;
+    c = it->second;
+    return true;
+}
+
+void store_tune(const std::string& key, Choice c)
+{
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    g_tune[key] = c;
+    if (const char* path = tune_path()) {
+        std::ofstream f(path, std::ios::app);
+        f << key << ' ' << c.rc << ' ' << c.ctas << '\n';
+    }
+}
+
+// Key: kind, flags, instance count, FNV-1a hash of the sizes, GPU name and SM count.
+std::string tune_key(iclblasHandle_t h, const char* kind, const std::vector<int>& flags, int batch,
+                     const std::vector<int>& dims)
+{
+    uint64_t x = 1469598103934665603ull;
+    for (int v : dims)
+        for (int b = 0; b < 4; ++b) {
+            x ^= (uint64_t)((v >> (8 * b)) & 0xff);
+            x *= 1099511628211ull;
+        }
+    cudaDeviceProp prop;
+    std::string name = "gpu";
+    if (cudaGetDeviceProperties(&prop, h->device) == cudaSuccess) name = prop.name;
+    for (char& ch : name)
+        if (ch == ' ' || ch == '\t') ch = '_';
+    char buf[64];
+    std::snprintf(buf, sizeof(buf), "%016llx", (unsigned long long)x);
+    std::string key = std::string(kind);
+    for (int f : flags) key += "." + std::to_string(f);
+    key += "|b" + std::to_string(batch) + "|" + buf + "|" + name + "|sm" + std::to_string(h->sm_count);
+    return key;
+}
+
+// Device buffers for timing candidates: every instance points at the same
+// operands (sized for the largest instance).  TRSM: A all ones, B zero, so
+// every solve writes zeros and concurrent instances store identical values.
+// GEMM: A, B, C zero.
+struct TuneBuffers {
+    float *a = nullptr, *b = nullptr, *c = nullptr;
+    const float** ptrs = nullptr;   // 3 x batch pointers
+    unsigned* counter = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    ~TuneBuffers()
+    {
+        if (a) cudaFree(a);
+        if (b) cudaFree(b);
+        if (c) cudaFree(c);
+        if (ptrs) cudaFree(ptrs);
+        if (counter) cudaFree(counter);
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+    }
+    cudaError_t init(iclblasHandle_t h, int batch, long na, long nb, long nc, float fill_a)
+    {
+        cudaError_t e;
+        if ((e = cudaMalloc(&a, std::max(na, 1L) * sizeof(float))) != cudaSuccess) return e;
+        if ((e = cudaMalloc(&b, std::max(nb, 1L) * sizeof(float))) != cudaSuccess) return e;
+        if ((e = cudaMalloc(&c, std::max(nc, 1L) * sizeof(float))) != cudaSuccess) return e;
+        if ((e = cudaMalloc(&ptrs, 3 * (size_t)batch * sizeof(float*))) != cudaSuccess) return e;
+        if ((e = cudaMalloc(&counter, sizeof(unsigned))) != cudaSuccess) return e;
+        if ((e = cudaEventCreate(&e0)) != cudaSuccess) return e;
+        if ((e = cudaEventCreate(&e1)) != cudaSuccess) return e;
+        tune_fill_kernel<<<h->sm_count * 4, 256, 0, h->stream>>>(std::max(na, 1L), a, fill_a);
+        tune_fill_kernel<<<h->sm_count * 4, 256, 0, h->stream>>>(std::max(nb, 1L), b, 0.f);
+        tune_fill_kernel<<<h->sm_count * 4, 256, 0, h->stream>>>(std::max(nc, 1L), c, 0.f);
+        tune_ptrs_kernel<<<(batch + 255) / 256, 256, 0, h->stream>>>(batch, ptrs, a, ptrs + batch, b,
+                                                                      ptrs + 2 * batch, c);
+        return cudaGetLastError();
+    }
+};
+
+// Times `run` (one launch of the list) once untimed and 3 times timed; ms per launch.
+template <class F>
+cudaError_t time_launch(iclblasHandle_t h, TuneBuffers& tb, F&& run, float& ms)
+{
+    cudaError_t e = run();
+    if (e != cudaSuccess) return e;
+    if ((e = cudaEventRecord(tb.e0, h->stream)) != cudaSuccess) return e;
+    for (int r = 0; r < 3; ++r)
+        if ((e = run()) != cudaSuccess) return e;
+    if ((e = cudaEventRecord(tb.e1, h->stream)) != cudaSuccess) return e;
+    if ((e = cudaEventSynchronize(tb.e1)) != cudaSuccess) return e;
+    if ((e = cudaEventElapsedTime(&ms, tb.e0, tb.e1)) != cudaSuccess) return e;
+    ms /= 3.f;
+    return cudaSuccess;
+}
+
+const int kRcs[] = {32, 64};
+const int kCtas[] = {1, 2, 4};
+
+// Chooses (rc, ctas) for a TRSM list and fills l.items for the choice.
+cudaError_t tune_trsm(iclblasHandle_t h, int batch, const std::vector<int>& dims, int lower_op, int op, int unit,
+                      BatchList& l)
+{
+    if (trsm_items(batch, dims, 64).empty()) return upload_items({}, l);   // nothing to solve
+    const std::string key = tune_key(h, "trsm", {lower_op, op, unit}, batch, dims);
+    Choice best{64, 1};
+    if (!lookup_tune(key, best)) {
+        long na = 0, nb = 0;
+        for (int i = 0; i < batch; ++i) {
+            na = std::max(na, (long)dims[4 * i + 2] * dims[4 * i]);
+            nb = std::max(nb, (long)dims[4 * i + 3] * dims[4 * i + 1]);
+        }
+        TuneBuffers tb;
+        cudaError_t e = tb.init(h, batch, na, nb, 1, 1.f);
+        if (e != cudaSuccess) return e;
+        float best_ms = 3.4e38f;
+        for (int rc : kRcs) {
+            BatchList cand;
+            cand.dims = l.dims;
+            cand.rc = rc;
+            if ((e = upload_items(trsm_items(batch, dims, rc), cand)) != cudaSuccess) return e;
+            for (int ctas : kCtas) {
+                cand.ctas_per_sm = ctas;
+                float ms = 0;
+                e = time_launch(h, tb, [&]() {
+                    return launch_trsm(h, cand, tb.counter, lower_op, op, unit, 1.f, tb.ptrs,
+                                       const_cast<float* const*>(tb.ptrs + batch));
+                }, ms);
+                if (e != cudaSuccess) break;
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best = Choice{rc, ctas};
+                }
+            }
+            if (cand.items) cudaFree(cand.items);
+            if (e != cudaSuccess) return e;
+        }
+        store_tune(key, best);
+    }
+    l.rc = best.rc;
+    l.ctas_per_sm = best.ctas;
+    return upload_items(trsm_items(batch, dims, best.rc), l);
+}
+
+cudaError_t tune_gemm(iclblasHandle_t h, int batch, const std::vector<int>& dims, int ta, int tb_, bool masked,
+                      int tri_lower, int tri_strict, BatchList& l)
+{
+    if (gemm_items(batch, dims, 64, masked, tri_lower).empty()) return upload_items({}, l);
+    const std::string key = tune_key(h, masked ? "gemm_adj" : "gemm", {ta, tb_, tri_lower, tri_strict}, batch, dims);
+    Choice best{64, 1};
+    if (!lookup_tune(key, best)) {
+        long na = 0, nb = 0, nc = 0;
+        for (int i = 0; i < batch; ++i) {
+            const int m = dims[6 * i], n = dims[6 * i + 1], k = dims[6 * i + 2];
+            na = std::max(na, (long)dims[6 * i + 3] * (ta ? m : k));
+            nb = std::max(nb, (long)dims[6 * i + 4] * (tb_ ? k : n));
+            nc = std::max(nc, (long)dims[6 * i + 5] * n);
+        }
+        TuneBuffers tb;
+        cudaError_t e = tb.init(h, batch, na, nb, nc, 0.f);
+        if (e != cudaSuccess) return e;
+        float best_ms = 3.4e38f;
+        for (int rc : kRcs) {
+            BatchList cand;
+            cand.dims = l.dims;
+            cand.rc = rc;
+            if ((e = upload_items(gemm_items(batch, dims, rc, masked, tri_lower), cand)) != cudaSuccess) return e;
+            for (int ctas : kCtas) {
+                cand.ctas_per_sm = ctas;
+                float ms = 0;
+                e = time_launch(h, tb, [&]() {
+                    return launch_gemm(h, cand, tb.counter, masked, ta, tb_, 1.f, 0.f, tb.ptrs, tb.ptrs + batch,
+                                       const_cast<float* const*>(tb.ptrs + 2 * batch), tri_lower, tri_strict);
+                }, ms);
+                if (e != cudaSuccess) break;
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best = Choice{rc, ctas};
+                }
+            }
+            if (cand.items) cudaFree(cand.items);
+            if (e != cudaSuccess) return e;
+        }
+        store_tune(key, best);
+    }
+    l.rc = best.rc;
+    l.ctas_per_sm = best.ctas;
+    return upload_items(gemm_items(batch, dims, best.rc, masked, tri_lower), l);
+}
+
+bool lower_op_of(int uplo, int trans)
+{
+    return (uplo == ICLBLAS_FILL_MODE_LOWER) != (trans != ICLBLAS_OP_N);
+}
+
+}  // namespace
+
+cudaError_t batch_list_free(BatchList& l)
+{
+    if (l.dims) cudaFree(l.dims);
+    if (l.items) cudaFree(l.items);
+    l.dims = nullptr;
+    l.items = nullptr;
+    l.nitems = 0;
+    return cudaSuccess;
+}
+
+void batch_plan_free(iclblasBatchPlan* p)
+{
+    if (!p) return;
+    batch_list_free(p->main);
+    batch_list_free(p->adj);
+    if (p->counter) cudaFree(p->counter);
+    p->tag = 0;
+    delete p;
+}
+
+cudaError_t batch_plan_create_trsm(iclblasHandle_t h, int side, int uplo, int trans, int diag, int batch,
+                                   const int* m, const int* n, const int* lda, const int* ldb,
+                                   iclblasBatchPlan** out)
+{
+    auto* p = new iclblasBatchPlan();
+    p->kind = 0;
+    p->side = side;
+    p->uplo = uplo;
+    p->trans = trans;
+    p->diag = diag;
+    p->batch = batch;
+    p->device = h->device;
+    std::vector<int> dims(4 * (size_t)batch), adims(6 * (size_t)batch);
+    for (int i = 0; i < batch; ++i) {
+        dims[4 * i] = m[i];
+        dims[4 * i + 1] = n[i];
+        dims[4 * i + 2] = lda[i];
+        dims[4 * i + 3] = ldb[i];
+        // adjoint product: dA (m x m, ld lda) from G and X (m x n, ld ldb), inner n
+        adims[6 * i] = m[i];
+        adims[6 * i + 1] = m[i];
+        adims[6 * i + 2] = n[i];
+        adims[6 * i + 3] = ldb[i];
+        adims[6 * i + 4] = ldb[i];
+        adims[6 * i + 5] = lda[i];
+        p->flops += (double)m[i] * m[i] * n[i];
+    }
+    const int op = trans != ICLBLAS_OP_N;
+    const int unit = diag == ICLBLAS_DIAG_UNIT;
+    cudaError_t e = cudaMalloc(&p->counter, sizeof(unsigned));
+    if (e == cudaSuccess) e = upload_dims(dims, p->main);
+    if (e == cudaSuccess) e = upload_dims(adims, p->adj);
+    if (e == cudaSuccess) e = tune_trsm(h, batch, dims, lower_op_of(uplo, trans), op, unit, p->main);
+    if (e == cudaSuccess)
+        e = tune_gemm(h, batch, adims, ICLBLAS_OP_N, ICLBLAS_OP_T, true, uplo == ICLBLAS_FILL_MODE_LOWER, unit,
+                      p->adj);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) {
+        batch_plan_free(p);
+        return e;
+    }
+    p->tag = kBatchPlanTag;
+    *out = p;
+    return cudaSuccess;
+}
+
+cudaError_t batch_plan_create_gemm(iclblasHandle_t h, int transa, int transb, int batch, const int* m, const int* n,
+                                   const int* k, const int* lda, const int* ldb, const int* ldc,
+                                   iclblasBatchPlan** out)
+{
+    auto* p = new iclblasBatchPlan();
+    p->kind = 1;
+    p->transa = transa;
+    p->transb = transb;
+    p->batch = batch;
+    p->device = h->device;
+    std::vector<int> dims(6 * (size_t)batch);
+    for (int i = 0; i < batch; ++i) {
+        dims[6 * i] = m[i];
+        dims[6 * i + 1] = n[i];
+        dims[6 * i + 2] = k[i];
+        dims[6 * i + 3] = lda[i];
+        dims[6 * i + 4] = ldb[i];
+        dims[6 * i + 5] = ldc[i];
+        p->flops += 2.0 * m[i] * n[i] * k[i];
+    }
+    const int ta = transa != ICLBLAS_OP_N, tb = transb != ICLBLAS_OP_N;
+    cudaError_t e = cudaMalloc(&p->counter, sizeof(unsigned));
+    if (e == cudaSuccess) e = upload_dims(dims, p->main);
+    if (e == cudaSuccess) e = tune_gemm(h, batch, dims, ta, tb, false, 0, 0, p->main);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) {
+        batch_plan_free(p);
+        return e;
+    }
+    p->tag = kBatchPlanTag;
+    *out = p;
+    return cudaSuccess;
+}
+
+cudaError_t batch_trsm(iclblasHandle_t h, const iclblasBatchPlan* p, float alpha, const float* const* A,
+                       float* const* B)
+{
+    return launch_trsm(h, p->main, p->counter, lower_op_of(p->uplo, p->trans), p->trans != ICLBLAS_OP_N,
+                       p->diag == ICLBLAS_DIAG_UNIT, alpha, A, B);
+}
+
+cudaError_t batch_gemm(iclblasHandle_t h, const iclblasBatchPlan* p, float alpha, const float* const* A,
+                       const float* const* B, float beta, float* const* C)
+{
+    return launch_gemm(h, p->main, p->counter, false, p->transa != ICLBLAS_OP_N, p->transb != ICLBLAS_OP_N, alpha,
+                       beta, A, B, C, 0, 0);
+}
+
+// Adjoint of X = alpha * op(A)^-1 B for every instance.  G (= dL/dX) becomes
+// dB = alpha * op(A)^-T G (the TRSM launch with the transposed operator,
+// alpha applied on load); then dA = -W X^T (op N) or -X W^T (op T/C) with
+// W = dB / alpha, kept on the stored triangle (the masked GEMM launch, its
+// alpha -1/alpha; alpha == 0 gives X == 0 and so dA == 0).
+cudaError_t batch_trsm_backward(iclblasHandle_t h, const iclblasBatchPlan* p, float alpha, const float* const* A,
+                                const float* const* X, float* const* G, float* const* dA)
+{
+    const int op = p->trans != ICLBLAS_OP_N;
+    const int unit = p->diag == ICLBLAS_DIAG_UNIT;
+    cudaError_t e = launch_trsm(h, p->main, p->counter, !lower_op_of(p->uplo, p->trans), !op, unit, alpha, A, G);
+    if (e != cudaSuccess || !dA) return e;
+    const float s = alpha != 0.f ? -1.f / alpha : 0.f;
+    const float* const* Gc = const_cast<const float* const*>(G);
+    return launch_gemm(h, p->adj, p->counter, true, 0, 1, s, 0.f, op ? X : Gc, op ? Gc : X, dA,
+                       p->uplo == ICLBLAS_FILL_MODE_LOWER, unit);
+}
+
+}  // namespace iclb

@@ -120,4 +120,47 @@ cudaError_t sgemm_backward(iclblasHandle_t h, int ta, int tb, int m, int n, int 
                            const float* B, int ldb, float beta, const float* G, int ldg, float* dA, int ldda,
                            float* dB, int lddb, float* dC, int lddc);
 
+// ---------------------------------------------------------------- batched
+// A plan for uneven batched TRSM (left side) or GEMM: per-instance sizes and
+// a cost-sorted work list in device memory, plus the tuned launch shape.
+struct BatchList {
+    int* dims = nullptr;     // per instance: TRSM (m, n, lda, ldb); GEMM (m, n, k, lda, ldb, ldc)
+    int2* items = nullptr;   // (instance, tile) work items, most expensive first
+    int nitems = 0;
+    int rc = 64;             // tile width (right-hand sides / C columns per item)
+    int ctas_per_sm = 1;
+};
+cudaError_t batch_list_free(BatchList& l);
+
+}  // namespace iclb
+
+constexpr uint32_t kBatchPlanTag = 0xBA7C4001u;
+struct iclblasBatchPlan {
+    uint32_t tag = 0;
+    int kind = 0;   // 0 = TRSM, 1 = GEMM
+    int side = 0, uplo = 0, trans = 0, diag = 0;
+    int transa = 0, transb = 0;
+    int batch = 0;
+    int device = 0;
+    double flops = 0;
+    iclb::BatchList main;   // the TRSM (forward and the adjoint's solve) or the GEMM
+    iclb::BatchList adj;    // TRSM plans: the masked dA product of the adjoint
+    unsigned* counter = nullptr;   // work-queue head, cleared before each launch
+};
+
+namespace iclb {
+cudaError_t batch_plan_create_trsm(iclblasHandle_t h, int side, int uplo, int trans, int diag, int batch,
+                                   const int* m, const int* n, const int* lda, const int* ldb,
+                                   iclblasBatchPlan** out);
+cudaError_t batch_plan_create_gemm(iclblasHandle_t h, int transa, int transb, int batch, const int* m, const int* n,
+                                   const int* k, const int* lda, const int* ldb, const int* ldc,
+                                   iclblasBatchPlan** out);
+void batch_plan_free(iclblasBatchPlan* p);
+cudaError_t batch_trsm(iclblasHandle_t h, const iclblasBatchPlan* p, float alpha, const float* const* A,
+                       float* const* B);
+cudaError_t batch_gemm(iclblasHandle_t h, const iclblasBatchPlan* p, float alpha, const float* const* A,
+                       const float* const* B, float beta, float* const* C);
+cudaError_t batch_trsm_backward(iclblasHandle_t h, const iclblasBatchPlan* p, float alpha, const float* const* A,
+                                const float* const* X, float* const* G, float* const* dA);
+
 }  // namespace iclb

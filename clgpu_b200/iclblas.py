@@ -95,6 +95,13 @@ _SIGS = {
     "iclblasCtrsm": [_H, _I, _I, _I, _I, _I, _I, _P, _P, _I, _P, _I],
     "iclblasStrsm_backward": [_H, _I, _I, _I, _I, _I, _I, _P, _P, _I, _P, _I, _P, _I, _P, _I],
     "iclblasSgemm_backward": [_H, _I, _I, _I, _I, _I, _P, _P, _I, _P, _I, _P, _P, _I, _P, _I, _P, _I, _P, _I],
+    "iclblasStrsmBatchedPlanCreate": [_H, _I, _I, _I, _I, _I, _P, _P, _P, _P, C.POINTER(_P)],
+    "iclblasSgemmBatchedPlanCreate": [_H, _I, _I, _I, _P, _P, _P, _P, _P, _P, C.POINTER(_P)],
+    "iclblasBatchPlanDestroy": [_P],
+    "iclblasBatchPlanGetInfo": [_P, C.POINTER(C.c_double), C.POINTER(_I), C.POINTER(_I)],
+    "iclblasStrsmBatchedUneven": [_H, _P, _P, _P, _P],
+    "iclblasSgemmBatchedUneven": [_H, _P, _P, _P, _P, _P, _P],
+    "iclblasStrsmBatchedUnevenBackward": [_H, _P, _P, _P, _P, _P, _P],
 }
 
 _lib = None
@@ -312,3 +319,51 @@ def iclblasSgemm_backward(h, transa, transb, m, n, k, alpha, A, lda, B, ldb, bet
 def check(status: int, fn: str = "iclblas call") -> None:
     if status != SUCCESS:
         raise IclblasError(fn, status)
+
+
+class BatchPlan:
+    """An iclblasBatchPlan_t built from per-instance sizes (int sequences).
+
+    ``BatchPlan(h, "trsm", side=, uplo=, trans=, diag=, m=, n=, lda=, ldb=)`` or
+    ``BatchPlan(h, "gemm", transa=, transb=, m=, n=, k=, lda=, ldb=, ldc=)``."""
+
+    def __init__(self, h, kind, **kw):
+        self.value = _P()
+        arr = lambda v: np.ascontiguousarray(np.asarray(v, dtype=np.int32))  # noqa: E731
+        d = {k: arr(v) for k, v in kw.items() if isinstance(v, (list, tuple, np.ndarray))}
+        if kind == "trsm":
+            st = _call("iclblasStrsmBatchedPlanCreate", _h(h), kw["side"], kw["uplo"], kw["trans"], kw["diag"],
+                       len(d["m"]), ptr(d["m"]), ptr(d["n"]), ptr(d["lda"]), ptr(d["ldb"]), C.byref(self.value))
+        elif kind == "gemm":
+            st = _call("iclblasSgemmBatchedPlanCreate", _h(h), kw["transa"], kw["transb"], len(d["m"]), ptr(d["m"]),
+                       ptr(d["n"]), ptr(d["k"]), ptr(d["lda"]), ptr(d["ldb"]), ptr(d["ldc"]), C.byref(self.value))
+        else:
+            raise ValueError(kind)
+        if st != SUCCESS:
+            raise IclblasError("iclblas*BatchedPlanCreate", st)
+
+    def info(self):
+        """(algorithmic flops per call, tile width, CTAs per SM)."""
+        f, w, c = C.c_double(), C.c_int(), C.c_int()
+        check(_call("iclblasBatchPlanGetInfo", self.value, C.byref(f), C.byref(w), C.byref(c)))
+        return f.value, w.value, c.value
+
+    def destroy(self):
+        if self.value:
+            _call("iclblasBatchPlanDestroy", self.value)
+            self.value = _P()
+
+
+def iclblasStrsmBatchedUneven(h, plan, alpha, A, B):
+    """A, B: device arrays of per-instance device pointers (e.g. int64 CUDA tensors)."""
+    return _call("iclblasStrsmBatchedUneven", _h(h), plan.value, C.byref(_fscalar(alpha)), ptr(A), ptr(B))
+
+
+def iclblasSgemmBatchedUneven(h, plan, alpha, A, B, beta, Cm):
+    return _call("iclblasSgemmBatchedUneven", _h(h), plan.value, C.byref(_fscalar(alpha)), ptr(A), ptr(B),
+                 C.byref(_fscalar(beta)), ptr(Cm))
+
+
+def iclblasStrsmBatchedUnevenBackward(h, plan, alpha, A, X, G, dA):
+    return _call("iclblasStrsmBatchedUnevenBackward", _h(h), plan.value, C.byref(_fscalar(alpha)), ptr(A), ptr(X),
+                 ptr(G), ptr(dA))

@@ -227,6 +227,51 @@ ICLBLAS_API iclblasStatus_t iclblasSgemm_backward(iclblasHandle_t handle, iclbla
                                                   const float* G, int ldg, float* dA, int ldda, float* dB, int lddb,
                                                   float* dC, int lddc);
 
+/* Uneven batched TRSM and GEMM, no reference counterpart.  A plan is built
+ * once for a list of instance sizes (host arrays of `batch` ints); each call
+ * then runs every instance in one persistent launch (a memset of the plan's
+ * work-queue head plus one kernel on the handle's stream), which can be
+ * captured in a CUDA graph.  Plan creation is synchronous, allocates device
+ * memory and times the launch-shape candidates on synthetic operands (the
+ * choice is cached per shapes and GPU, and in the file named by the
+ * environment variable ICLBLAS_TUNE_CACHE when set); do not create a plan
+ * during stream capture.  The calls take device arrays of `batch` device
+ * pointers, one per instance; a plan serves one stream at a time.  All
+ * arithmetic is FP32 FMA on the CUDA cores, whatever the math mode.
+ * TRSM: left side only (a right-side plan is NOT_SUPPORTED); instance i
+ * solves op(A_i) X_i = alpha B_i with A_i m_i x m_i (leading dimension
+ * lda_i >= max(1, m_i)) and B_i m_i x n_i (ldb_i >= max(1, m_i)).
+ * GEMM: C_i = alpha op(A_i) op(B_i) + beta C_i, leading dimensions at least
+ * the stored row counts; each element is bit-identical to iclblasSgemm in
+ * PLAIN_FP32 mode. */
+typedef struct iclblasBatchPlan* iclblasBatchPlan_t;
+ICLBLAS_API iclblasStatus_t iclblasStrsmBatchedPlanCreate(iclblasHandle_t handle, iclblasSideMode_t side,
+                                                          iclblasFillMode_t uplo, iclblasOperation_t trans,
+                                                          iclblasDiagType_t diag, int batch, const int* m,
+                                                          const int* n, const int* lda, const int* ldb,
+                                                          iclblasBatchPlan_t* plan);
+ICLBLAS_API iclblasStatus_t iclblasSgemmBatchedPlanCreate(iclblasHandle_t handle, iclblasOperation_t transa,
+                                                          iclblasOperation_t transb, int batch, const int* m,
+                                                          const int* n, const int* k, const int* lda, const int* ldb,
+                                                          const int* ldc, iclblasBatchPlan_t* plan);
+ICLBLAS_API iclblasStatus_t iclblasBatchPlanDestroy(iclblasBatchPlan_t plan);
+/* Algorithmic flops of one call (TRSM sum m^2 n, GEMM sum 2mnk) and the
+ * tuned launch shape (tile width, CTAs per SM); any output may be NULL. */
+ICLBLAS_API iclblasStatus_t iclblasBatchPlanGetInfo(iclblasBatchPlan_t plan, double* flops, int* tile_width,
+                                                    int* ctas_per_sm);
+ICLBLAS_API iclblasStatus_t iclblasStrsmBatchedUneven(iclblasHandle_t handle, iclblasBatchPlan_t plan,
+                                                      const float* alpha, const float* const* A, float* const* B);
+ICLBLAS_API iclblasStatus_t iclblasSgemmBatchedUneven(iclblasHandle_t handle, iclblasBatchPlan_t plan,
+                                                      const float* alpha, const float* const* A,
+                                                      const float* const* B, const float* beta, float* const* C);
+/* Batched iclblasStrsm_backward for a TRSM plan: X_i and G_i use ldb_i, dA_i
+ * uses lda_i; G_i is overwritten with dL/dB_i, dA_i receives dL/dA_i on the
+ * stored triangle (zero elsewhere).  dA may be NULL (then only dB). */
+ICLBLAS_API iclblasStatus_t iclblasStrsmBatchedUnevenBackward(iclblasHandle_t handle, iclblasBatchPlan_t plan,
+                                                              const float* alpha, const float* const* A,
+                                                              const float* const* X, float* const* G,
+                                                              float* const* dA);
+
 #ifdef __cplusplus
 }
 #endif
