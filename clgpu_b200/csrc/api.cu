@@ -298,6 +298,7 @@ extern "C" iclblasStatus_t iclblasDestroy(iclblasHandle_t handle)
         if (handle->stage) cudaFree(handle->stage);
         if (handle->ws.scratch) cudaFree(handle->ws.scratch);
         if (handle->ws.solver) cudaFree(handle->ws.solver);
+        if (handle->ws.pub) cudaFree(handle->ws.pub);
         cudaFree(handle->ws.counters);
         cudaFree(handle->ws.dev_status);
         cudaStreamDestroy(handle->own_stream);

@@ -36,6 +36,8 @@ struct Workspace {
     unsigned* counters = nullptr;   // kCounterWords words, zeroed at creation
     int* dev_status = nullptr;      // one int, DeviceStatus bits
     unsigned epoch = 0;             // host-side epoch for flag-based kernels
+    unsigned long long* pub = nullptr;   // TRSV: published solution entries (value, epoch), zeroed when grown
+    size_t pub_elems = 0;
 };
 constexpr int kCounterWords = 1 << 16;
 

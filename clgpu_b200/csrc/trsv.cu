@@ -20,6 +20,7 @@
 // polls that word, returns; the host reports EXECUTION_FAILED.  Reads of
 // other CTAs' results go through L2 (ld.cg) so no stale L1 line is used.
 #include "common.cuh"
+#include "tma.cuh"
 
 namespace iclb {
 namespace {
@@ -215,6 +216,273 @@ __global__ void __launch_bounds__(kThreads) trsv_kernel(int n, int lower_op, int
     if (threadIdx.x == 0) st_release(flags + s, epoch);
 }
 
+// ---------------------------------------------------------------- STRSV, TMA path
+// Float TRSV when A is 16-byte aligned with lda a multiple of 4 and >= n
+// (the usual case).  Same ticket-ordered one-launch structure as above, with
+// three changes that shorten the chain of dependent block solves:
+//   - tiles arrive by TMA (one 64 x 64 box per cp.async.bulk.tensor) into a
+//     4-stage shared-memory ring, so up to 64 KiB per CTA are in flight while
+//     the CTA waits for earlier blocks, and two CTAs fit on an SM;
+//   - the first box is the diagonal block: the CTA inverts it in FP64 before
+//     it needs it (while earlier blocks are still being solved), so its own
+//     step of the chain is a 64 x 64 FP64 matrix-vector product instead of
+//     64 dependent substitution steps;
+//   - each solved entry is published as one 64-bit word (value, call epoch):
+//     a consumer polls the entries it needs directly, with no separate flag.
+//     The epoch lives in device memory: each CTA reads the last launch's
+//     epoch at its start and uses the next one; the CTA that solves the last
+//     block stores it back once everything is published (every other CTA has
+//     read it by then), so replays of a captured launch get fresh epochs.
+// Entries of x are FP32 results of FP64 products with the FP64 inverse of the
+// FP32 diagonal block applied to the FP32 right-hand side of the block.
+constexpr int FS = 4;
+constexpr int TILE_ELEMS = NB * NB;
+constexpr unsigned long long kTrsvWaitNs = 2000000000ull;  // a wait gives up after 2 s
+
+struct FastSmem {
+    float stage[FS][TILE_ELEMS];
+    double inv[NB][NB + 1];
+    double ys[NB];
+    double partd[4][NB];
+    float xs[NB];
+    float part[4][NB];
+    uint64_t full[FS];
+    unsigned s, epoch;
+};
+
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p)
+{
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v)
+{
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__global__ void __launch_bounds__(kThreads, 2)
+    strsv_tma_kernel(const __grid_constant__ CUtensorMap amap, int n, int lower_op, int op, int unit, float* x,
+                     long incx, unsigned long long* pub, unsigned* ticket, unsigned* epoch_word, int* status)
+{
+    extern __shared__ unsigned char smem_raw[];
+    FastSmem& S = *reinterpret_cast<FastSmem*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    const int t = threadIdx.x;
+    const int nb = (n + NB - 1) / NB;
+    if (t == 0) {
+        unsigned e = *(volatile unsigned*)epoch_word + 1u;
+        S.epoch = e == 0u ? 1u : e;
+        S.s = atomicAdd(ticket, 1u);
+        for (int i = 0; i < FS; ++i) tma::mbar_init(&S.full[i], 1);
+        tma::mbar_init_fence();
+    }
+    __syncthreads();
+    const int s = (int)S.s;
+    const unsigned epoch = S.epoch;
+    if (s == nb - 1 && t == 0) *ticket = 0u;  // every ticket of this launch is taken
+    auto blk = [&](int p) { return lower_op ? p : nb - 1 - p; };
+    const int kb = blk(s), r0 = kb * NB, nr = min(NB, n - r0);
+    // load i = 0 is the diagonal block, load i >= 1 the tile of solve-order block i - 1
+    int issued = 0;  // (thread 0)
+    auto issue = [&](int i) {
+        issued = i + 1;
+        const int cb = i == 0 ? kb : blk(i - 1);
+        uint64_t* bar = &S.full[i % FS];
+        tma::mbar_expect_tx(bar, TILE_ELEMS * 4);
+        if (op == 0) tma::load_2d(S.stage[i % FS], &amap, r0, cb * NB, bar);   // A[r0.., cb*NB..]
+        else tma::load_2d(S.stage[i % FS], &amap, cb * NB, r0, bar);           // A[cb*NB.., r0..]
+    };
+    if (t == 0)
+        for (int i = 0; i < min(FS, s + 1); ++i) issue(i);
+    const float b = t < nr ? x[(long)(r0 + t) * incx] : 0.f;
+
+    // ---- diagonal block: FP64 inverse, one column per thread (t < 64)
+    // on a failed wait: record it, let this CTA's copies still in flight land
+    // (each wait bounded), then leave
+    auto bail = [&](int consumed) {
+        if (t == 0) {
+            atomicOr(status, (int)kDevWaitTimeout);
+            for (int j = consumed; j < issued; ++j)
+                tma::mbar_wait_bounded(&S.full[j % FS], (j / FS) & 1, kTrsvWaitNs);
+        }
+    };
+    int bad = tma::mbar_wait_bounded(&S.full[0], 0, kTrsvWaitNs) ? 0 : 1;
+    if (__syncthreads_or(bad)) {
+        bail(0);
+        return;
+    }
+    if (t < NB) {
+        const float* D = S.stage[0];
+        const int j = t;
+        for (int i = 0; i < NB; ++i) S.inv[i][j] = 0.0;
+        // D(r, c) = op(A)(r0 + r, r0 + c): op N stores column-major, op T row-major
+        auto d = [&](int r, int c) -> double { return (double)(op == 0 ? D[c * NB + r] : D[r * NB + c]); };
+        if (j < nr) {
+            if (lower_op) {
+                for (int i = 0; i < nr; ++i) {
+                    // every thread walks the same (i, k): D reads are broadcasts
+                    double s0 = 0.0, s1 = 0.0;
+                    int k = 0;
+                    for (; k + 1 < i; k += 2) {
+                        s0 = fma(d(i, k), S.inv[k][j], s0);
+                        s1 = fma(d(i, k + 1), S.inv[k + 1][j], s1);
+                    }
+                    if (k < i) s0 = fma(d(i, k), S.inv[k][j], s0);
+                    const double dii = unit ? 1.0 : d(i, i);
+                    double v = 0.0;
+                    if (i == j) v = 1.0 / dii;
+                    else if (i > j) v = -(s0 + s1) / dii;
+                    S.inv[i][j] = v;
+                }
+            } else {
+                for (int i = nr - 1; i >= 0; --i) {
+                    double s0 = 0.0, s1 = 0.0;
+                    int k = i + 1;
+                    for (; k + 1 < nr; k += 2) {
+                        s0 = fma(d(i, k), S.inv[k][j], s0);
+                        s1 = fma(d(i, k + 1), S.inv[k + 1][j], s1);
+                    }
+                    if (k < nr) s0 = fma(d(i, k), S.inv[k][j], s0);
+                    const double dii = unit ? 1.0 : d(i, i);
+                    double v = 0.0;
+                    if (i == j) v = 1.0 / dii;
+                    else if (i < j) v = -(s0 + s1) / dii;
+                    S.inv[i][j] = v;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if (t == 0 && FS <= s) issue(FS);
+
+    // ---- off-diagonal tiles in solve order
+    const int lane = t & 31, warp = t >> 5;
+    const int rN = t % NB, gN = t / NB;      // op N: row, group of 16 columns
+    float accN = 0.f;
+    float accT[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) accT[i] = 0.f;
+    for (int i = 1; i <= s; ++i) {
+        const int c0 = blk(i - 1) * NB, nc = min(NB, n - c0);
+        bad = tma::mbar_wait_bounded(&S.full[i % FS], (i / FS) & 1, kTrsvWaitNs) ? 0 : 1;
+        if (t < NB) {
+            float v = 0.f;
+            if (t < nc) {
+                const unsigned long long* src = pub + c0 + t;
+                unsigned long long w = ld_relaxed_u64(src);
+                if ((unsigned)(w >> 32) != epoch) {
+                    const unsigned long long t0 = tma::global_ns();
+                    for (;;) {
+                        __nanosleep(32);
+                        w = ld_relaxed_u64(src);
+                        if ((unsigned)(w >> 32) == epoch) break;
+                        if (ld_volatile(status) != kDevOk) { bad = 1; break; }
+                        if (tma::global_ns() - t0 > kTrsvWaitNs) {
+                            atomicOr(status, (int)kDevWaitTimeout);
+                            bad = 1;
+                            break;
+                        }
+                    }
+                }
+                v = __uint_as_float((unsigned)w);
+            }
+            S.xs[t] = v;
+        }
+        if (__syncthreads_or(bad)) {
+            bail(i);
+            return;
+        }
+        const float* T = S.stage[i % FS];
+        if (op == 0) {
+#pragma unroll
+            for (int jj = 0; jj < 16; ++jj) {
+                const int c = gN * 16 + jj;
+                accN = fmaf(-T[c * NB + rN], S.xs[c], accN);
+            }
+        } else {
+            const float x0 = S.xs[lane], x1 = S.xs[lane + 32];
+#pragma unroll
+            for (int ii = 0; ii < 8; ++ii) {
+                const int r = warp * 8 + ii;
+                accT[ii] = fmaf(-T[r * NB + lane], x0, accT[ii]);
+                accT[ii] = fmaf(-T[r * NB + lane + 32], x1, accT[ii]);
+            }
+        }
+        __syncthreads();
+        if (t == 0 && i + FS <= s) issue(i + FS);
+    }
+
+    // ---- row sums, right-hand side, x = inv * y in FP64, publish
+    if (op == 0) {
+        S.part[gN][rN] = accN;
+    } else {
+#pragma unroll
+        for (int ii = 0; ii < 8; ++ii) {
+            const float v = warp_sum(accT[ii]);
+            if (lane == 0) S.part[0][warp * 8 + ii] = v;
+        }
+    }
+    __syncthreads();
+    if (t < NB) {
+        const float sum = op == 0 ? (S.part[0][t] + S.part[1][t]) + (S.part[2][t] + S.part[3][t]) : S.part[0][t];
+        S.ys[t] = t < nr ? (double)(b + sum) : 0.0;
+    }
+    __syncthreads();
+    {
+        double acc = 0.0;
+#pragma unroll
+        for (int jj = 0; jj < 16; ++jj) {
+            const int c = gN * 16 + jj;
+            acc = fma(S.inv[rN][c], S.ys[c], acc);
+        }
+        S.partd[gN][rN] = acc;
+    }
+    __syncthreads();
+    if (t < nr) {
+        const float xf = (float)((S.partd[0][t] + S.partd[1][t]) + (S.partd[2][t] + S.partd[3][t]));
+        x[(long)(r0 + t) * incx] = xf;
+        st_relaxed_u64(pub + r0 + t, ((unsigned long long)epoch << 32) | __float_as_uint(xf));
+    }
+    if (s == nb - 1) {
+        __syncthreads();
+        if (t == 0) *(volatile unsigned*)epoch_word = epoch;
+    }
+}
+
+cudaError_t strsv_tma(iclblasHandle_t h, int uplo, int trans, int diag, int n, const float* A, int lda, float* x,
+                      int incx, bool& used)
+{
+    used = false;
+    CUtensorMap map;
+    if (lda < n || !tma::map_f32_colmajor(&map, A, n, n, lda, NB, NB)) return cudaSuccess;
+    if ((size_t)n > h->ws.pub_elems) {
+        if (h->ws.pub) cudaFree(h->ws.pub);
+        h->ws.pub = nullptr;
+        h->ws.pub_elems = 0;
+        cudaError_t e = cudaMalloc(&h->ws.pub, (size_t)n * sizeof(unsigned long long));
+        if (e != cudaSuccess) return e;
+        e = cudaMemsetAsync(h->ws.pub, 0, (size_t)n * sizeof(unsigned long long), h->stream);
+        if (e != cudaSuccess) return e;
+        h->ws.pub_elems = n;
+    }
+    static int smem_set = 0;
+    const int smem = (int)sizeof(FastSmem) + 1024;
+    if (!smem_set) {
+        cudaError_t e = cudaFuncSetAttribute(strsv_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+        smem_set = 1;
+    }
+    const int op = trans == ICLBLAS_OP_N ? 0 : 1;
+    const bool lower = uplo == ICLBLAS_FILL_MODE_LOWER;
+    const int lower_op = (op == 0) ? lower : !lower;
+    const int nb = (n + NB - 1) / NB;
+    strsv_tma_kernel<<<nb, kThreads, smem, h->stream>>>(map, n, lower_op, op, diag == ICLBLAS_DIAG_UNIT, x, incx,
+                                                        h->ws.pub, h->ws.counters,
+                                                        h->ws.counters + kCounterWords - 1, h->ws.dev_status);
+    used = true;
+    return cudaGetLastError();
+}
+
 template <class T>
 cudaError_t trsv_impl(iclblasHandle_t h, int uplo, int trans, int diag, int n, const T* A, int lda, T* x, int incx)
 {
@@ -237,6 +505,9 @@ cudaError_t trsv_impl(iclblasHandle_t h, int uplo, int trans, int diag, int n, c
 
 cudaError_t strsv(iclblasHandle_t h, int uplo, int trans, int diag, int n, const float* A, int lda, float* x, int incx)
 {
+    bool used = false;
+    cudaError_t e = strsv_tma(h, uplo, trans, diag, n, A, lda, x, incx, used);
+    if (e != cudaSuccess || used) return e;
     return trsv_impl<float>(h, uplo, trans == ICLBLAS_OP_C ? ICLBLAS_OP_T : trans, diag, n, A, lda, x, incx);
 }
 

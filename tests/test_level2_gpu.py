@@ -142,3 +142,53 @@ def test_trsv_device_pointers(handle, cuda):
     assert B.iclblasStrsv(handle, 0, 1, 0, n, Ad, n, xd, 1) == B.SUCCESS
     assert handle.synchronize() == B.SUCCESS
     assert O.rel_fro(xd.cpu().numpy(), x_ref) <= TOL
+
+
+@pytest.mark.parametrize("n", [64, 130, 2048, 3001])
+@pytest.mark.parametrize("uplo,trans", [(0, 0), (1, 0), (0, 1), (1, 2)])
+def test_strsv_tma_path_padded_lda(handle, n, uplo, trans):
+    """lda a multiple of 4 above n (the TMA-staged path), stride 2, three
+    calls in a row on one handle (each call a new epoch)."""
+    rng = np.random.default_rng(n + 7 * uplo + trans)
+    lda = (n + 4 + 3) // 4 * 4
+    for diag in (0, 1, 0):
+        A = tri(n, lda, uplo == 1, rng)
+        x = rng.uniform(-1, 1, 2 * n).astype(np.float32)
+        x_ref = x.copy()
+        O.strsv(uplo, trans, diag, n, A, lda, x_ref, 2)
+        assert B.iclblasStrsv(handle, uplo, trans, diag, n, A, lda, x, 2) == B.SUCCESS
+        assert O.rel_fro(x, x_ref) <= TOL
+        assert np.array_equal(x[1::2], x_ref[1::2])   # entries between the strided ones untouched
+
+
+def test_strsv_replayed_in_cuda_graph(handle, cuda):
+    """A captured STRSV replayed several times gives the eager result each time
+    (the publication epoch advances on the device, not at capture)."""
+    import torch
+    n = 5000
+    rng = np.random.default_rng(21)
+    A = tri(n, n, True, rng)
+    x0 = rng.uniform(-1, 1, n).astype(np.float32)
+    x_ref = x0.copy()
+    O.strsv(1, 0, 0, n, A, n, x_ref, 1)
+    Ad = torch.from_numpy(A).to(cuda)
+    x0d = torch.from_numpy(x0).to(cuda)
+    xw = x0d.clone()
+    # first call outside capture (sizes the handle's buffers)
+    handle.set_stream(torch.cuda.current_stream())
+    assert B.iclblasStrsv(handle, 1, 0, 0, n, Ad, n, xw, 1) == B.SUCCESS
+    torch.cuda.synchronize()
+    s = torch.cuda.Stream()
+    handle.set_stream(s)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        xw.copy_(x0d)
+        st = B.iclblasStrsv(handle, 1, 0, 0, n, Ad, n, xw, 1)
+    assert st == B.SUCCESS
+    for _ in range(3):
+        xw.fill_(7.0)
+        g.replay()
+        torch.cuda.synchronize()
+        assert O.rel_fro(xw.cpu().numpy(), x_ref) <= TOL
+    handle.set_stream(torch.cuda.current_stream())
+    del g
