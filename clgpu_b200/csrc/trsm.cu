@@ -11,9 +11,11 @@
 // (Strsm_naive.cl:35, Ctrsm_naive.cl:43) the solve runs on the unscaled B and
 // alpha multiplies the solution afterwards (one pass over B when alpha != 1);
 // scaling B first rounds differently and misses the reference's 4-ulp
-// known-answer checks after cancellation.  Leaves of <= 64 rows are solved in
-// shared memory, one RHS per thread.  GEMMs use the handle's math mode (the
-// plain FP32 default is the CUDA-core kernel).
+// known-answer checks after cancellation.  Leaves are 512 rows (256 complex):
+// their inverses are formed on the GPU in FP64 (64 x 64 diagonal blocks by
+// substitution, then doubling steps up to the leaf size), rounded to the
+// working type, and applied as GEMMs.  Every GEMM uses the handle's math mode
+// (the plain FP32 default is the CUDA-core kernel).
 #include <algorithm>
 
 #include "common.cuh"
