@@ -465,8 +465,8 @@ def run_trsm_study(args, torch):
     torch.cuda.set_device(dev)
     stream = torch.cuda.Stream(device=dev)
     g = torch.Generator(device=dev).manual_seed(3)
-    modes = [(B.MATH_PLAIN_FP32, "fp32_simt"), (B.MATH_TF32, "tf32"), (B.MATH_BF16X3, "3xbf16"),
-             (B.MATH_BF16X6, "6xbf16")]
+    modes = [(B.MATH_PLAIN_FP32, "fp32_simt", 0), (B.MATH_TF32, "tf32", 0), (B.MATH_BF16X3, "3xbf16", 0),
+             (B.MATH_BF16X6, "6xbf16", 0), (B.MATH_BF16X3, "3xbf16+refine1", 1), (B.MATH_TF32, "tf32+refine2", 2)]
     out = []
 
     def make_tri(n, lower, cplx):
@@ -512,8 +512,9 @@ def run_trsm_study(args, torch):
                                                 upper=(not lower) if trans == 0 else lower)
             x64n = torch.linalg.norm(X64).item()
             fl = (4.0 if cplx else 1.0) * m * m * nrhs
-            for mode, mname in modes:
+            for mode, mname, steps in modes:
                 h.set_math_mode(mode)
+                h.set_trsm_refinement(steps)
                 Bw = B0.clone()
                 call = B.iclblasCtrsm if cplx else B.iclblasStrsm
                 one = (1.0 + 0j) if cplx else 1.0
@@ -531,6 +532,7 @@ def run_trsm_study(args, torch):
                      "ms": round(ms, 3), "rel_fro_err_vs_fp64": err}
                 print(json.dumps(r), flush=True)
                 out.append(r)
+            h.set_trsm_refinement(0)
             del L, Acm, B0, X64
         # STRSV n = 16384, lower / N / non-unit, same L construction
         n = args.trsv_n

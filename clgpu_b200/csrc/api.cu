@@ -337,6 +337,20 @@ extern "C" iclblasStatus_t iclblasGetMathMode(iclblasHandle_t h, iclblasMathMode
     return ICLBLAS_STATUS_SUCCESS;
 }
 
+extern "C" iclblasStatus_t iclblasSetTrsmRefinement(iclblasHandle_t h, int steps)
+{
+    if (!handle_ok(h) || steps < 0 || steps > 2) return ICLBLAS_STATUS_INVALID_VALUE;
+    h->trsm_refine = steps;
+    return ICLBLAS_STATUS_SUCCESS;
+}
+
+extern "C" iclblasStatus_t iclblasGetTrsmRefinement(iclblasHandle_t h, int* steps)
+{
+    if (!handle_ok(h) || !steps) return ICLBLAS_STATUS_INVALID_VALUE;
+    *steps = h->trsm_refine;
+    return ICLBLAS_STATUS_SUCCESS;
+}
+
 extern "C" iclblasStatus_t iclblasSynchronize(iclblasHandle_t h)
 {
     if (!handle_ok(h)) return ICLBLAS_STATUS_INVALID_VALUE;

@@ -57,6 +57,7 @@ struct iclblasContext {
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
     iclblasMathMode_t math = ICLBLAS_MATH_PLAIN_FP32;
+    int trsm_refine = 0;   // TRSM residual-refinement steps (0..2)
     iclb::Workspace ws;
     // Device staging for host-pointer arguments (grows on demand).
     void* stage = nullptr;

@@ -44,6 +44,10 @@ __device__ __forceinline__ float zero_v(float) { return 0.f; }
 __device__ __forceinline__ cfloat zero_v(cfloat) { return cfloat{0.f, 0.f}; }
 __device__ __forceinline__ float conj_v(float v) { return v; }
 __device__ __forceinline__ cfloat conj_v(cfloat v) { return cfloat{v.re, -v.im}; }
+__device__ __forceinline__ float one_v(float) { return 1.f; }
+__device__ __forceinline__ cfloat one_v(cfloat) { return cfloat{1.f, 0.f}; }
+__device__ __forceinline__ float addv(float a, float b) { return a + b; }
+__device__ __forceinline__ cfloat addv(cfloat a, cfloat b) { return cfloat{a.re + b.re, a.im + b.im}; }
 __device__ __forceinline__ float mulv(float a, float b) { return a * b; }
 __device__ __forceinline__ cfloat mulv(cfloat a, cfloat b)
 {
@@ -262,6 +266,45 @@ __global__ void narrow_kernel(long count, const typename Wide<T>::type* __restri
         dst[e] = narrow(src[e], T());
 }
 
+// Copy of every leaf's diagonal block of M = op(A) (op 2 conjugates) with
+// the other triangle zeroed (and the diagonal 1 for a unit diagonal), leaf
+// bb at out + bb*big*big, column-major with leading dimension big; rows and
+// columns at or beyond n are zero.  Used for the refinement residual.
+template <class T>
+__global__ void leaf_tri_kernel(int n, int op, int m_lower, int unit, int big, int nbig, const T* __restrict__ A,
+                                long lda, T* __restrict__ out)
+{
+    const long per = (long)big * big, total = per * nbig;
+    for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+        const long bb = e / per, rem = e % per;
+        const int c = (int)(rem / big), r = (int)(rem % big);
+        const long i = bb * big + r, j = bb * big + c;
+        T v = zero_v(T());
+        if (i < n && j < n && (r == c || (m_lower ? r > c : r < c))) {
+            if (r == c && unit) v = one_v(T());
+            else if (op == 0) v = A[i + j * lda];
+            else {
+                v = A[j + i * lda];
+                if (op == 2) v = conj_v(v);
+            }
+        }
+        out[e] = v;
+    }
+}
+
+// X = alpha * (X + D) for m x n column-major blocks.
+template <class T>
+__global__ void add_scale_kernel(int m, int n, T alpha, T* __restrict__ X, long ldx, const T* __restrict__ D,
+                                 long ldd)
+{
+    const long total = (long)m * n;
+    for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+        const long j = e / m, i = e % m;
+        T* p = X + j * ldx + i;
+        *p = mulv(addv(*p, D[j * ldd + i]), alpha);
+    }
+}
+
 template <class T>
 struct Gemm;
 template <>
@@ -300,6 +343,7 @@ struct Solver {
     int big;   // leaf size (a power-of-two multiple of NB)
     const T* inv = nullptr;  // inverses of the BIG diagonal blocks (FP64-formed, rounded)
     T* tmp = nullptr;        // leaf staging: big x nrhs (left) or nrhs x big (right)
+    const T* mtri = nullptr; // masked leaf diagonal blocks (refinement only)
 
     // Pointer and GEMM op of block M[r0.., c0..] of M = op(A).
     const T* mblk(int r0, int c0) const { return op == 0 ? A + r0 + (long)c0 * lda : A + c0 + (long)r0 * lda; }
@@ -344,6 +388,35 @@ struct Solver {
         }
         if (e != cudaSuccess) return e;
         return solve(so, ss);
+    }
+
+    // R -= M X over the diagonal range [o, o+sz) (left: rows of R and X;
+    // right: columns), with the same recursive split as solve(): leaves use
+    // the masked diagonal blocks, the off-diagonal blocks are GEMMs on A.
+    cudaError_t residual(int o, int sz, const T* X, long ldx, T* R, long ldr)
+    {
+        if (sz <= big) {
+            const T* mt = mtri + (long)(o / big) * big * big;
+            if (left)
+                return Gemm<T>::run(h, ICLBLAS_OP_N, ICLBLAS_OP_N, sz, nrhs, sz, Gemm<T>::minus_one(), mt, big, X + o,
+                                    (int)ldx, Gemm<T>::one(), R + o, (int)ldr);
+            return Gemm<T>::run(h, ICLBLAS_OP_N, ICLBLAS_OP_N, nrhs, sz, sz, Gemm<T>::minus_one(), X + (long)o * ldx,
+                                (int)ldx, mt, big, Gemm<T>::one(), R + (long)o * ldr, (int)ldr);
+        }
+        const int nleaf = (sz + big - 1) / big;
+        const int h1 = (nleaf / 2) * big;
+        const int o1 = o, s1 = h1, o2 = o + h1, s2 = sz - h1;
+        const bool forward = left ? m_lower : !m_lower;
+        const int fo = forward ? o1 : o2, fs = forward ? s1 : s2;
+        const int so = forward ? o2 : o1, ss = forward ? s2 : s1;
+        cudaError_t e = residual(fo, fs, X, ldx, R, ldr);
+        if (e == cudaSuccess) e = residual(so, ss, X, ldx, R, ldr);
+        if (e != cudaSuccess) return e;
+        if (left)
+            return Gemm<T>::run(h, op, ICLBLAS_OP_N, ss, nrhs, fs, Gemm<T>::minus_one(), mblk(so, fo), lda, X + fo,
+                                (int)ldx, Gemm<T>::one(), R + so, (int)ldr);
+        return Gemm<T>::run(h, ICLBLAS_OP_N, op, nrhs, ss, fs, Gemm<T>::minus_one(), X + (long)fo * ldx, (int)ldx,
+                            mblk(fo, so), lda, Gemm<T>::one(), R + (long)so * ldr, (int)ldr);
     }
 };
 
@@ -392,13 +465,21 @@ cudaError_t trsm_impl(iclblasHandle_t h, int side, int uplo, int trans, int diag
     const size_t tmp_w = (size_t)nbig * (big / 2) * (big / 2);
     const size_t leaf_t = (size_t)big * s.nrhs;
     auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
-    const size_t bytes = al(sizeof(W) * inv_w) + al(sizeof(W) * tmp_w) + al(sizeof(T) * inv_w) + al(sizeof(T) * leaf_t);
+    // refinement: masked leaf blocks, a copy of B, the residual / correction
+    const int steps = h->trsm_refine;
+    const size_t mn = (size_t)m * n;
+    const size_t bytes = al(sizeof(W) * inv_w) + al(sizeof(W) * tmp_w) + al(sizeof(T) * inv_w) +
+                         al(sizeof(T) * leaf_t) +
+                         (steps > 0 ? al(sizeof(T) * inv_w) + 2 * al(sizeof(T) * mn) : 0);
     char* ws = (char*)solver_scratch(h, bytes);
     if (!ws) return cudaErrorMemoryAllocation;
     W* invd = (W*)ws;
     W* dtmp = (W*)(ws + al(sizeof(W) * inv_w));
     T* inv32 = (T*)(ws + al(sizeof(W) * inv_w) + al(sizeof(W) * tmp_w));
     s.tmp = (T*)(ws + al(sizeof(W) * inv_w) + al(sizeof(W) * tmp_w) + al(sizeof(T) * inv_w));
+    T* mtri = (T*)((char*)s.tmp + al(sizeof(T) * leaf_t));
+    T* b0 = (T*)((char*)mtri + al(sizeof(T) * inv_w));
+    T* res = (T*)((char*)b0 + al(sizeof(T) * mn));
     cudaError_t e = cudaMemsetAsync(invd, 0, sizeof(W) * inv_w, h->stream);
     if (e != cudaSuccess) return e;
     const size_t sm_inv = sizeof(W) * 2 * NB * (NB + 1);
@@ -423,8 +504,41 @@ cudaError_t trsm_impl(iclblasHandle_t h, int side, int uplo, int trans, int diag
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     s.inv = inv32;
+    if (steps > 0) {
+        e = cudaMemcpy2DAsync(b0, sizeof(T) * m, B, sizeof(T) * ldb, sizeof(T) * m, n, cudaMemcpyDeviceToDevice,
+                              h->stream);
+        if (e != cudaSuccess) return e;
+        const long cnt = (long)inv_w;
+        const int g = (int)std::min<long>((cnt + 255) / 256, (long)h->sm_count * 8);
+        leaf_tri_kernel<T><<<g, 256, 0, h->stream>>>(na, s.op, s.m_lower, s.unit, big, nbig, A, lda, mtri);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        s.mtri = mtri;
+    }
     e = s.solve(0, na);
-    if (e != cudaSuccess || is_one(alpha)) return e;
+    if (e != cudaSuccess) return e;
+    for (int it = 0; it < steps; ++it) {
+        // R = B0 - M X with FP32-accurate products (6xBF16 on the tensor cores,
+        // or the CUDA-core kernel in PLAIN_FP32 mode), then M D = R in the
+        // handle's mode with the same inverses, X = X + D (alpha on the last)
+        e = cudaMemcpy2DAsync(res, sizeof(T) * m, b0, sizeof(T) * m, sizeof(T) * m, n, cudaMemcpyDeviceToDevice,
+                              h->stream);
+        if (e != cudaSuccess) return e;
+        const iclblasMathMode_t mode = h->math;
+        if (mode != ICLBLAS_MATH_PLAIN_FP32) h->math = ICLBLAS_MATH_BF16X6;
+        e = s.residual(0, na, B, ldb, res, m);
+        h->math = mode;
+        if (e != cudaSuccess) return e;
+        Solver<T> c = s;
+        c.B = res;
+        c.ldb = m;
+        if ((e = c.solve(0, na)) != cudaSuccess) return e;
+        const long total = (long)m * n;
+        const int grid = (int)std::min<long>((total + 255) / 256, (long)h->sm_count * 8);
+        const T sc = it == steps - 1 ? alpha : Gemm<T>::one();
+        add_scale_kernel<T><<<grid, 256, 0, h->stream>>>(m, n, sc, B, ldb, res, m);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    if (steps > 0 || is_one(alpha)) return cudaSuccess;
     const long total = (long)m * n;
     const int grid = (int)std::min<long>((total + 255) / 256, (long)h->sm_count * 8);
     scale_kernel<T><<<grid, 256, 0, h->stream>>>(m, n, alpha, B, ldb);

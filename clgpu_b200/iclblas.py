@@ -70,6 +70,8 @@ _SIGS = {
     "iclblasSetMathMode": [_H, _I],
     "iclblasGetMathMode": [_H, C.POINTER(_I)],
     "iclblasSynchronize": [_H],
+    "iclblasSetTrsmRefinement": [_H, _I],
+    "iclblasGetTrsmRefinement": [_H, C.POINTER(_I)],
     "iclblasSscal": [_H, _I, _P, _P, _I],
     "iclblasSaxpy": [_H, _I, _P, _P, _I, _P, _I],
     "iclblasSnrm2": [_H, _I, _P, _I, _P],
@@ -178,6 +180,11 @@ class Handle:
         st = _call("iclblasSetMathMode", self.value, mode)
         if st != SUCCESS:
             raise IclblasError("iclblasSetMathMode", st)
+
+    def set_trsm_refinement(self, steps: int) -> None:
+        st = _call("iclblasSetTrsmRefinement", self.value, steps)
+        if st != SUCCESS:
+            raise IclblasError("iclblasSetTrsmRefinement", st)
 
     def synchronize(self) -> int:
         return _call("iclblasSynchronize", self.value)

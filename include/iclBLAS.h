@@ -203,6 +203,15 @@ ICLBLAS_API iclblasStatus_t iclblasSetStream(iclblasHandle_t handle, void* strea
 ICLBLAS_API iclblasStatus_t iclblasGetStream(iclblasHandle_t handle, void** stream);
 ICLBLAS_API iclblasStatus_t iclblasSetMathMode(iclblasHandle_t handle, iclblasMathMode_t mode);
 ICLBLAS_API iclblasStatus_t iclblasGetMathMode(iclblasHandle_t handle, iclblasMathMode_t* mode);
+/* TRSM residual refinement, no reference counterpart.  With steps = 1 or 2
+ * (0, the default, turns it off), S/C TRSM follows its solve X by `steps`
+ * rounds of: R = B - op(A) X with FP32-accurate products (6xBF16 on the tensor
+ * cores in the tensor-core modes, FP32 on the CUDA cores in PLAIN_FP32),
+ * D = solve(R) in the handle's math mode with the same FP64-formed diagonal
+ * inverses, X = X + D.  Each round costs about one extra solve plus one
+ * triangle product and needs workspace for two copies of B. */
+ICLBLAS_API iclblasStatus_t iclblasSetTrsmRefinement(iclblasHandle_t handle, int steps);
+ICLBLAS_API iclblasStatus_t iclblasGetTrsmRefinement(iclblasHandle_t handle, int* steps);
 /* Wait for all work enqueued on the handle's stream; reports a device-side
  * error flag (a bounded wait that ran out) as EXECUTION_FAILED. */
 ICLBLAS_API iclblasStatus_t iclblasSynchronize(iclblasHandle_t handle);
