@@ -378,32 +378,52 @@ __global__ void __launch_bounds__(THREADS, 1)
             const int row = tm * BM + q * 32 + lane;
             const int col0 = tn * BN + half * 128;
             const bool beta_zero = p.beta_re == 0.f && p.beta_im == 0.f;
+            // C is read in groups of 8 columns before any of them is stored,
+            // so the loads overlap (columns of C never alias for ldc >= M)
             if (row < p.M) {
                 if (!p.complex_out) {
 #pragma unroll
-                    for (int j = 0; j < 128; ++j) {
-                        const int col = col0 + j;
-                        if (col < p.N) {
-                            float* cp = p.C + (long)col * p.ldc + row;
-                            *cp = beta_zero ? __fmul_rn(p.alpha_re, sum[j])
-                                            : fmaf(p.alpha_re, sum[j], __fmul_rn(p.beta_re, *cp));
+                    for (int j0 = 0; j0 < 128; j0 += 8) {
+                        float cv[8];
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) {
+                            const int col = col0 + j0 + j;
+                            cv[j] = (!beta_zero && col < p.N) ? p.C[(long)col * p.ldc + row] : 0.f;
+                        }
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) {
+                            const int col = col0 + j0 + j;
+                            if (col < p.N)
+                                p.C[(long)col * p.ldc + row] =
+                                    beta_zero ? __fmul_rn(p.alpha_re, sum[j0 + j])
+                                              : fmaf(p.alpha_re, sum[j0 + j], __fmul_rn(p.beta_re, cv[j]));
                         }
                     }
                 } else {
+                    float2* const C2 = (float2*)p.C;
 #pragma unroll
-                    for (int j = 0; j < 128; j += 2) {
-                        if (col0 + j < p.N) {
-                            float2* cp = (float2*)p.C + (long)((col0 + j) >> 1) * p.ldc + row;
-                            const float re = sum[j], im = sum[j + 1];
-                            float2 r;
-                            r.x = fmaf(p.alpha_re, re, -p.alpha_im * im);
-                            r.y = fmaf(p.alpha_re, im, p.alpha_im * re);
-                            if (!beta_zero) {
-                                const float2 cv = *cp;
-                                r.x += fmaf(p.beta_re, cv.x, -p.beta_im * cv.y);
-                                r.y += fmaf(p.beta_re, cv.y, p.beta_im * cv.x);
+                    for (int j0 = 0; j0 < 128; j0 += 8) {
+                        float2 cv[4];
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) {
+                            const int col = col0 + j0 + 2 * j;
+                            cv[j] = (!beta_zero && col < p.N) ? C2[(long)(col >> 1) * p.ldc + row]
+                                                              : make_float2(0.f, 0.f);
+                        }
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) {
+                            const int col = col0 + j0 + 2 * j;
+                            if (col < p.N) {
+                                const float re = sum[j0 + 2 * j], im = sum[j0 + 2 * j + 1];
+                                float2 r;
+                                r.x = fmaf(p.alpha_re, re, -p.alpha_im * im);
+                                r.y = fmaf(p.alpha_re, im, p.alpha_im * re);
+                                if (!beta_zero) {
+                                    r.x += fmaf(p.beta_re, cv[j].x, -p.beta_im * cv[j].y);
+                                    r.y += fmaf(p.beta_re, cv[j].y, p.beta_im * cv[j].x);
+                                }
+                                C2[(long)(col >> 1) * p.ldc + row] = r;
                             }
-                            *cp = r;
                         }
                     }
                 }
