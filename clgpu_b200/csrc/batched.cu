@@ -41,17 +41,86 @@ namespace {
 
 constexpr int TB = 64;  // row block / tile height
 
+// ---------------------------------------------------------------- diagonal inverses
+// Inverse of every 64 x 64 diagonal block of every instance's M = op(A),
+// formed in FP64 (thread j solves D y = e_j by substitution; rows and columns
+// beyond the instance's size are the identity) and stored in FP32,
+// column-major, 4096 floats per block at inv + inv_off[instance] + 4096*block.
+// One CTA of 64 threads per (instance, block) item.
+__global__ void __launch_bounds__(TB) batched_inv_kernel(const int2* __restrict__ inv_items,
+                                                         const int* __restrict__ dims,
+                                                         const long* __restrict__ inv_off, int lower_op, int op,
+                                                         int unit, const float* const* __restrict__ Aptr,
+                                                         float* __restrict__ inv)
+{
+    extern __shared__ double ysm[];
+    double(*Y)[TB + 1] = (double(*)[TB + 1])ysm;
+    float(*D)[TB + 1] = (float(*)[TB + 1])(ysm + TB * (TB + 1));
+    const int2 w = inv_items[blockIdx.x];
+    const int* d = dims + 4 * w.x;
+    const int m = d[0];
+    const long lda = d[2];
+    const float* A = Aptr[w.x];
+    const int r0 = w.y * TB, nr = min(TB, m - r0);
+    for (int idx = threadIdx.x; idx < TB * TB; idx += TB) {
+        const int r = idx % TB, c = idx / TB;  // A-local (r, c): coalesced down A's columns
+        float v = 0.f;
+        if (r < nr && c < nr) v = A[(long)(r0 + c) * lda + r0 + r];
+        if (op == 0) D[r][c] = v;
+        else D[c][r] = v;
+    }
+    __syncthreads();
+    const int j = threadIdx.x;
+    if (lower_op) {
+        for (int i = 0; i < TB; ++i) {
+            double y = 0.0;
+            if (i >= j) {
+                y = (i == j) ? 1.0 : 0.0;
+                for (int k = j; k < i; ++k) y = fma(-(double)D[i][k], Y[k][j], y);
+                if (!unit && i < nr) y /= (double)D[i][i];
+            }
+            Y[i][j] = y;
+        }
+    } else {
+        for (int i = TB - 1; i >= 0; --i) {
+            double y = 0.0;
+            if (i <= j) {
+                y = (i == j) ? 1.0 : 0.0;
+                for (int k = i + 1; k <= j; ++k) y = fma(-(double)D[i][k], Y[k][j], y);
+                if (!unit && i < nr) y /= (double)D[i][i];
+            }
+            Y[i][j] = y;
+        }
+    }
+    __syncthreads();
+    float* out = inv + inv_off[w.x] + (long)w.y * TB * TB;
+    for (int idx = threadIdx.x; idx < TB * TB; idx += TB) out[idx] = (float)Y[idx % TB][idx / TB];
+}
+
 // ---------------------------------------------------------------- TRSM kernel
+// Persistent; each item is one instance and RC right-hand sides.  For each
+// 64-row block of M = op(A) in solve order:
+//   Y = alpha * B[block] - sum over earlier blocks q of M[block, q] X[q]
+//       (K slices of 16 staged in shared memory, double-buffered through
+//        registers; 4 x RC/16 outputs per thread from float4 reads)
+//   X[block] = inv(M[block, block]) Y        (the precomputed FP32 inverse,
+//        read transposed when `inv_t`: the adjoint's transposed operator)
+constexpr int KC = 16;
+
 template <int RC>
 __global__ void __launch_bounds__(256) batched_trsm_kernel(int nitems, const int2* __restrict__ items,
-                                                           const int* __restrict__ dims, int lower_op, int op,
-                                                           int unit, float alpha, const float* const* __restrict__ Aptr,
+                                                           const int* __restrict__ dims,
+                                                           const long* __restrict__ inv_off,
+                                                           const float* __restrict__ inv, int lower_op, int op,
+                                                           int inv_t, float alpha,
+                                                           const float* const* __restrict__ Aptr,
                                                            float* const* __restrict__ Bptr, unsigned* counter)
 {
-    constexpr int CPT = RC / 16;   // columns per thread in the update
-    constexpr int G = 256 / RC;    // row groups in the substitution
-    __shared__ float Ms[TB][TB + 1];
-    __shared__ float Xs[TB][RC + 1];
+    constexpr int CPT = RC / 16;        // columns per thread
+    constexpr int XPT = KC * RC / 256;  // X slice elements per thread
+    __shared__ __align__(16) float Ms[2][KC][TB + 4];
+    __shared__ __align__(16) float Xs[2][KC][RC + 4];
+    __shared__ __align__(16) float Ys[TB][RC + 4];
     __shared__ int item_sh;
     const int t = threadIdx.x, tx = t % 16, ty = t / 16;
     for (;;) {
@@ -66,86 +135,140 @@ __global__ void __launch_bounds__(256) batched_trsm_kernel(int nitems, const int
         const long lda = d[2], ldb = d[3];
         const float* A = Aptr[w.x];
         float* B = Bptr[w.x];
+        const float* IV = inv + inv_off[w.x];
         const int c0 = w.y * RC, nc = min(RC, nrhs - c0);
         const int nb = (m + TB - 1) / TB;
         for (int p = 0; p < nb; ++p) {
             const int kb = lower_op ? p : nb - 1 - p;
             const int r0 = kb * TB, nr = min(TB, m - r0);
+            __syncthreads();
+            for (int idx = t; idx < TB * RC; idx += 256) {
+                const int r = idx % TB, c = idx / TB;
+                Ys[r][c] = (r < nr && c < nc) ? alpha * B[(long)(c0 + c) * ldb + r0 + r] : 0.f;
+            }
+            __syncthreads();
             float acc[4][CPT];
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
-                for (int j = 0; j < CPT; ++j) {
-                    const int r = ty * 4 + i, c = tx * CPT + j;
-                    acc[i][j] = (r < nr && c < nc) ? alpha * B[(long)(c0 + c) * ldb + r0 + r] : 0.f;
-                }
-            for (int q = 0; q < p; ++q) {
-                const int jb = lower_op ? q : nb - 1 - q;
-                const int j0 = jb * TB, nj = min(TB, m - j0);
-                __syncthreads();
-                for (int idx = t; idx < TB * TB; idx += 256) {
-                    int r, cc;
-                    if (op == 0) { r = idx % TB; cc = idx / TB; } else { cc = idx % TB; r = idx / TB; }
+                for (int j = 0; j < CPT; ++j) acc[i][j] = Ys[ty * 4 + i][tx * CPT + j];
+
+            // ---- update by the earlier blocks: K = 64 p in slices of 16
+            const int nslices = p * (TB / KC);
+            float ra[4], rx[XPT];
+            auto load = [&](int sl) {
+                const int q = sl / (TB / KC), kk0 = (sl % (TB / KC)) * KC;
+                const int j0 = (lower_op ? q : nb - 1 - q) * TB;
+                const int nk = min(TB, m - j0) - kk0;  // valid k in this slice: k < nk
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int e = t + 256 * u;
+                    int r, k;
+                    if (op == 0) { r = e % TB; k = e / TB; } else { k = e % KC; r = e / KC; }
                     float v = 0.f;
-                    if (r < nr && cc < nj)
-                        v = op == 0 ? A[(long)(j0 + cc) * lda + r0 + r] : A[(long)(r0 + r) * lda + j0 + cc];
-                    Ms[r][cc] = v;
+                    if (r < nr && k < nk)
+                        v = op == 0 ? A[(long)(j0 + kk0 + k) * lda + r0 + r] : A[(long)(r0 + r) * lda + j0 + kk0 + k];
+                    ra[u] = v;
                 }
-                for (int idx = t; idx < TB * RC; idx += 256) {
-                    const int r = idx % TB, c = idx / TB;
-                    Xs[r][c] = (r < nj && c < nc) ? B[(long)(c0 + c) * ldb + j0 + r] : 0.f;
+#pragma unroll
+                for (int u = 0; u < XPT; ++u) {
+                    const int e = t + 256 * u, k = e % KC, c = e / KC;
+                    rx[u] = (c < nc && k < nk) ? B[(long)(c0 + c) * ldb + j0 + kk0 + k] : 0.f;
                 }
+            };
+            auto store = [&](int buf) {
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int e = t + 256 * u;
+                    int r, k;
+                    if (op == 0) { r = e % TB; k = e / TB; } else { k = e % KC; r = e / KC; }
+                    Ms[buf][k][r] = ra[u];
+                }
+#pragma unroll
+                for (int u = 0; u < XPT; ++u) {
+                    const int e = t + 256 * u;
+                    Xs[buf][e % KC][e / KC] = rx[u];
+                }
+            };
+            if (nslices > 0) {
+                load(0);
+                store(0);
                 __syncthreads();
-#pragma unroll 8
-                for (int k = 0; k < TB; ++k) {
-                    float a[4], b[CPT];
+                for (int sl = 0; sl < nslices; ++sl) {
+                    const int buf = sl & 1;
+                    if (sl + 1 < nslices) load(sl + 1);
 #pragma unroll
-                    for (int i = 0; i < 4; ++i) a[i] = Ms[ty * 4 + i][k];
+                    for (int k = 0; k < KC; ++k) {
+                        const float4 a = *reinterpret_cast<const float4*>(&Ms[buf][k][ty * 4]);
+                        float b[CPT];
+                        if (CPT == 4) {
+                            const float4 bv = *reinterpret_cast<const float4*>(&Xs[buf][k][tx * 4]);
+                            b[0] = bv.x; b[1] = bv.y; b[2] = bv.z; b[3] = bv.w;
+                        } else {
+                            const float2 bv = *reinterpret_cast<const float2*>(&Xs[buf][k][tx * CPT]);
+                            b[0] = bv.x; b[1] = bv.y;
+                        }
+                        const float av[4] = {a.x, a.y, a.z, a.w};
 #pragma unroll
-                    for (int j = 0; j < CPT; ++j) b[j] = Xs[k][tx * CPT + j];
+                        for (int i = 0; i < 4; ++i)
 #pragma unroll
-                    for (int i = 0; i < 4; ++i)
-#pragma unroll
-                        for (int j = 0; j < CPT; ++j) acc[i][j] = fmaf(-a[i], b[j], acc[i][j]);
+                            for (int j = 0; j < CPT; ++j) acc[i][j] = fmaf(-av[i], b[j], acc[i][j]);
+                    }
+                    if (sl + 1 < nslices) store(buf ^ 1);
+                    __syncthreads();
                 }
             }
-            // diagonal block: RHS rows into shared memory, substitution
+
+            // ---- X = inv(M[block, block]) Y
             __syncthreads();
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
-                for (int j = 0; j < CPT; ++j) Xs[ty * 4 + i][tx * CPT + j] = acc[i][j];
-            for (int idx = t; idx < TB * TB; idx += 256) {
-                int r, cc;
-                if (op == 0) { r = idx % TB; cc = idx / TB; } else { cc = idx % TB; r = idx / TB; }
-                float v = 0.f;
-                if (r < nr && cc < nr)
-                    v = op == 0 ? A[(long)(r0 + cc) * lda + r0 + r] : A[(long)(r0 + r) * lda + r0 + cc];
-                Ms[r][cc] = v;
+                for (int j = 0; j < CPT; ++j) Ys[ty * 4 + i][tx * CPT + j] = acc[i][j];
+            float out[4][CPT];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < CPT; ++j) out[i][j] = 0.f;
+            const float* IB = IV + (long)kb * TB * TB;
+            for (int kk0 = 0; kk0 < TB; kk0 += KC) {
+                __syncthreads();
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int e = t + 256 * u;
+                    int r, k;
+                    if (!inv_t) { r = e % TB; k = e / TB; } else { k = e % KC; r = e / KC; }
+                    // inv(r, kk0 + k): column-major block, or its transpose
+                    Ms[0][k][r] = inv_t ? IB[(long)r * TB + kk0 + k] : IB[(long)(kk0 + k) * TB + r];
+                }
+                __syncthreads();
+#pragma unroll
+                for (int k = 0; k < KC; ++k) {
+                    const float4 a = *reinterpret_cast<const float4*>(&Ms[0][k][ty * 4]);
+                    float b[CPT];
+                    if (CPT == 4) {
+                        const float4 bv = *reinterpret_cast<const float4*>(&Ys[kk0 + k][tx * 4]);
+                        b[0] = bv.x; b[1] = bv.y; b[2] = bv.z; b[3] = bv.w;
+                    } else {
+                        const float2 bv = *reinterpret_cast<const float2*>(&Ys[kk0 + k][tx * CPT]);
+                        b[0] = bv.x; b[1] = bv.y;
+                    }
+                    const float av[4] = {a.x, a.y, a.z, a.w};
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+#pragma unroll
+                        for (int j = 0; j < CPT; ++j) out[i][j] = fmaf(av[i], b[j], out[i][j]);
+                }
             }
             __syncthreads();
-            const int c = t % RC, rg = t / RC;
-            if (lower_op) {
-                for (int k = 0; k < nr; ++k) {
-                    if (rg == k % G && !unit) Xs[k][c] = Xs[k][c] / Ms[k][k];
-                    __syncthreads();
-                    const float xk = Xs[k][c];
-                    for (int r = rg; r < nr; r += G)
-                        if (r > k) Xs[r][c] = fmaf(-Ms[r][k], xk, Xs[r][c]);
-                    __syncthreads();
-                }
-            } else {
-                for (int k = nr - 1; k >= 0; --k) {
-                    if (rg == k % G && !unit) Xs[k][c] = Xs[k][c] / Ms[k][k];
-                    __syncthreads();
-                    const float xk = Xs[k][c];
-                    for (int r = rg; r < k; r += G) Xs[r][c] = fmaf(-Ms[r][k], xk, Xs[r][c]);
-                    __syncthreads();
-                }
-            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < CPT; ++j) Ys[ty * 4 + i][tx * CPT + j] = out[i][j];
+            __syncthreads();
             for (int idx = t; idx < TB * RC; idx += 256) {
                 const int r = idx % TB, cc = idx / TB;
-                if (r < nr && cc < nc) B[(long)(c0 + cc) * ldb + r0 + r] = Xs[r][cc];
+                if (r < nr && cc < nc) B[(long)(c0 + cc) * ldb + r0 + r] = Ys[r][cc];
             }
         }
     }
@@ -335,19 +458,39 @@ int grid_of(iclblasHandle_t h, const BatchList& l)
 }
 
 // ---------------------------------------------------------------- host: launches
-cudaError_t launch_trsm(iclblasHandle_t h, const BatchList& l, unsigned* counter, int lower_op, int op, int unit,
-                        float alpha, const float* const* A, float* const* B)
+constexpr int kInvSmem = TB * (TB + 1) * (int)(sizeof(double) + sizeof(float));
+
+// The pass forming the diagonal-block inverses of M = op(A).
+cudaError_t launch_inv(iclblasHandle_t h, const int2* inv_items, int n_inv, const int* dims, const long* inv_off,
+                       int lower_op, int op, int unit, const float* const* A, float* inv)
+{
+    if (n_inv == 0) return cudaSuccess;
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(batched_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             kInvSmem);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    batched_inv_kernel<<<n_inv, TB, kInvSmem, h->stream>>>(inv_items, dims, inv_off, lower_op, op, unit, A, inv);
+    return cudaGetLastError();
+}
+
+// The solve, given the inverses (read transposed when inv_t).
+cudaError_t launch_trsm(iclblasHandle_t h, const BatchList& l, unsigned* counter, const long* inv_off,
+                        const float* inv, int lower_op, int op, int inv_t, float alpha, const float* const* A,
+                        float* const* B)
 {
     if (l.nitems == 0) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned), h->stream);
     if (e != cudaSuccess) return e;
     const int grid = grid_of(h, l);
     if (l.rc == 32)
-        batched_trsm_kernel<32><<<grid, 256, 0, h->stream>>>(l.nitems, l.items, l.dims, lower_op, op, unit, alpha, A, B,
-                                                             counter);
+        batched_trsm_kernel<32><<<grid, 256, 0, h->stream>>>(l.nitems, l.items, l.dims, inv_off, inv, lower_op, op,
+                                                             inv_t, alpha, A, B, counter);
     else
-        batched_trsm_kernel<64><<<grid, 256, 0, h->stream>>>(l.nitems, l.items, l.dims, lower_op, op, unit, alpha, A, B,
-                                                             counter);
+        batched_trsm_kernel<64><<<grid, 256, 0, h->stream>>>(l.nitems, l.items, l.dims, inv_off, inv, lower_op, op,
+                                                             inv_t, alpha, A, B, counter);
     return cudaGetLastError();
 }
 
@@ -454,10 +597,12 @@ std::string tune_key(iclblasHandle_t h, const char* kind, const std::vector<int>
 struct TuneBuffers {
     float *a = nullptr, *b = nullptr, *c = nullptr;
     const float** ptrs = nullptr;   // 3 x batch pointers
+    long* zoff = nullptr;           // batch zero offsets (every instance's inverses at c)
     unsigned* counter = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     ~TuneBuffers()
     {
+        if (zoff) cudaFree(zoff);
         if (a) cudaFree(a);
         if (b) cudaFree(b);
         if (c) cudaFree(c);
@@ -474,6 +619,8 @@ struct TuneBuffers {
         if ((e = cudaMalloc(&c, std::max(nc, 1L) * sizeof(float))) != cudaSuccess) return e;
         if ((e = cudaMalloc(&ptrs, 3 * (size_t)batch * sizeof(float*))) != cudaSuccess) return e;
         if ((e = cudaMalloc(&counter, sizeof(unsigned))) != cudaSuccess) return e;
+        if ((e = cudaMalloc(&zoff, (size_t)batch * sizeof(long))) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(zoff, 0, (size_t)batch * sizeof(long), h->stream)) != cudaSuccess) return e;
         if ((e = cudaEventCreate(&e0)) != cudaSuccess) return e;
         if ((e = cudaEventCreate(&e1)) != cudaSuccess) return e;
         tune_fill_kernel<<<h->sm_count * 4, 256, 0, h->stream>>>(std::max(na, 1L), a, fill_a);
@@ -509,16 +656,19 @@ cudaError_t tune_trsm(iclblasHandle_t h, int batch, const std::vector<int>& dims
                       BatchList& l)
 {
     if (trsm_items(batch, dims, 64).empty()) return upload_items({}, l);   // nothing to solve
-    const std::string key = tune_key(h, "trsm", {lower_op, op, unit}, batch, dims);
+    // the key names the kernel generation so that cached choices for an older
+    // kernel are not reused
+    const std::string key = tune_key(h, "trsm2", {lower_op, op, unit}, batch, dims);
     Choice best{64, 1};
     if (!lookup_tune(key, best)) {
-        long na = 0, nb = 0;
+        long na = 0, nb = 0, ni = 0;
         for (int i = 0; i < batch; ++i) {
             na = std::max(na, (long)dims[4 * i + 2] * dims[4 * i]);
             nb = std::max(nb, (long)dims[4 * i + 3] * dims[4 * i + 1]);
+            ni = std::max(ni, (long)((dims[4 * i] + TB - 1) / TB) * TB * TB);
         }
-        TuneBuffers tb;
-        cudaError_t e = tb.init(h, batch, na, nb, 1, 1.f);
+        TuneBuffers tb;  // inverses: zeros at c for every instance
+        cudaError_t e = tb.init(h, batch, na, nb, ni, 1.f);
         if (e != cudaSuccess) return e;
         float best_ms = 3.4e38f;
         for (int rc : kRcs) {
@@ -530,7 +680,7 @@ cudaError_t tune_trsm(iclblasHandle_t h, int batch, const std::vector<int>& dims
                 cand.ctas_per_sm = ctas;
                 float ms = 0;
                 e = time_launch(h, tb, [&]() {
-                    return launch_trsm(h, cand, tb.counter, lower_op, op, unit, 1.f, tb.ptrs,
+                    return launch_trsm(h, cand, tb.counter, tb.zoff, tb.c, lower_op, op, 0, 1.f, tb.ptrs,
                                        const_cast<float* const*>(tb.ptrs + batch));
                 }, ms);
                 if (e != cudaSuccess) break;
@@ -618,6 +768,9 @@ void batch_plan_free(iclblasBatchPlan* p)
     batch_list_free(p->main);
     batch_list_free(p->adj);
     if (p->counter) cudaFree(p->counter);
+    if (p->inv) cudaFree(p->inv);
+    if (p->inv_off) cudaFree(p->inv_off);
+    if (p->inv_items) cudaFree(p->inv_items);
     p->tag = 0;
     delete p;
 }
@@ -651,7 +804,26 @@ cudaError_t batch_plan_create_trsm(iclblasHandle_t h, int side, int uplo, int tr
     }
     const int op = trans != ICLBLAS_OP_N;
     const int unit = diag == ICLBLAS_DIAG_UNIT;
+    // diagonal-block inverses: 64 x 64 FP32 per block of each instance
+    std::vector<long> inv_off(batch > 0 ? batch : 1, 0);
+    std::vector<int2> inv_items;
+    long inv_total = 0;
+    for (int i = 0; i < batch; ++i) {
+        inv_off[i] = inv_total;
+        const int nblk = (m[i] + TB - 1) / TB;
+        if (n[i] > 0)
+            for (int b = 0; b < nblk; ++b) inv_items.push_back(make_int2(i, b));
+        inv_total += (long)nblk * TB * TB;
+    }
+    p->n_inv = (int)inv_items.size();
     cudaError_t e = cudaMalloc(&p->counter, sizeof(unsigned));
+    if (e == cudaSuccess && batch > 0) e = cudaMalloc(&p->inv_off, (size_t)batch * sizeof(long));
+    if (e == cudaSuccess && batch > 0)
+        e = cudaMemcpy(p->inv_off, inv_off.data(), (size_t)batch * sizeof(long), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && inv_total > 0) e = cudaMalloc(&p->inv, (size_t)inv_total * sizeof(float));
+    if (e == cudaSuccess && p->n_inv > 0) e = cudaMalloc(&p->inv_items, inv_items.size() * sizeof(int2));
+    if (e == cudaSuccess && p->n_inv > 0)
+        e = cudaMemcpy(p->inv_items, inv_items.data(), inv_items.size() * sizeof(int2), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = upload_dims(dims, p->main);
     if (e == cudaSuccess) e = upload_dims(adims, p->adj);
     if (e == cudaSuccess) e = tune_trsm(h, batch, dims, lower_op_of(uplo, trans), op, unit, p->main);
@@ -705,8 +877,11 @@ cudaError_t batch_plan_create_gemm(iclblasHandle_t h, int transa, int transb, in
 cudaError_t batch_trsm(iclblasHandle_t h, const iclblasBatchPlan* p, float alpha, const float* const* A,
                        float* const* B)
 {
-    return launch_trsm(h, p->main, p->counter, lower_op_of(p->uplo, p->trans), p->trans != ICLBLAS_OP_N,
-                       p->diag == ICLBLAS_DIAG_UNIT, alpha, A, B);
+    const int lower_op = lower_op_of(p->uplo, p->trans), op = p->trans != ICLBLAS_OP_N;
+    cudaError_t e = launch_inv(h, p->inv_items, p->n_inv, p->main.dims, p->inv_off, lower_op, op,
+                               p->diag == ICLBLAS_DIAG_UNIT, A, p->inv);
+    if (e != cudaSuccess) return e;
+    return launch_trsm(h, p->main, p->counter, p->inv_off, p->inv, lower_op, op, 0, alpha, A, B);
 }
 
 cudaError_t batch_gemm(iclblasHandle_t h, const iclblasBatchPlan* p, float alpha, const float* const* A,
@@ -726,7 +901,10 @@ cudaError_t batch_trsm_backward(iclblasHandle_t h, const iclblasBatchPlan* p, fl
 {
     const int op = p->trans != ICLBLAS_OP_N;
     const int unit = p->diag == ICLBLAS_DIAG_UNIT;
-    cudaError_t e = launch_trsm(h, p->main, p->counter, !lower_op_of(p->uplo, p->trans), !op, unit, alpha, A, G);
+    const int lower_op = lower_op_of(p->uplo, p->trans);
+    // inverses of the diagonal blocks of op(A); the transposed solve reads them transposed
+    cudaError_t e = launch_inv(h, p->inv_items, p->n_inv, p->main.dims, p->inv_off, lower_op, op, unit, A, p->inv);
+    if (e == cudaSuccess) e = launch_trsm(h, p->main, p->counter, p->inv_off, p->inv, !lower_op, !op, 1, alpha, A, G);
     if (e != cudaSuccess || !dA) return e;
     const float s = alpha != 0.f ? -1.f / alpha : 0.f;
     const float* const* Gc = const_cast<const float* const*>(G);

@@ -149,6 +149,13 @@ struct iclblasBatchPlan {
     iclb::BatchList main;   // the TRSM (forward and the adjoint's solve) or the GEMM
     iclb::BatchList adj;    // TRSM plans: the masked dA product of the adjoint
     unsigned* counter = nullptr;   // work-queue head, cleared before each launch
+    // TRSM plans: FP32 inverses of every 64 x 64 diagonal block of every
+    // instance (formed by each call), their per-instance offsets and the
+    // (instance, block) list of the pass that forms them
+    float* inv = nullptr;
+    long* inv_off = nullptr;
+    int2* inv_items = nullptr;
+    int n_inv = 0;
 };
 
 namespace iclb {
