@@ -280,6 +280,8 @@ __global__ void __launch_bounds__(256) batched_trsm_kernel(int nitems, const int
 // when beta == 0), the order of the single-instance plain SGEMM.
 // MODE 1 (adjoint of TRSM): C is an m x m block kept on the triangle
 // `tri_lower` (strict when `tri_strict`), zero elsewhere.
+// Each item is one 64 x RC tile; K slices of 16 are double-buffered through
+// registers into shared memory (k-major), 4 x RC/16 outputs per thread.
 template <int RC, int MODE>
 __global__ void __launch_bounds__(256) batched_gemm_kernel(int nitems, const int2* __restrict__ items,
                                                            const int* __restrict__ dims, int ta, int tb, float alpha,
@@ -289,8 +291,9 @@ __global__ void __launch_bounds__(256) batched_gemm_kernel(int nitems, const int
                                                            int tri_lower, int tri_strict)
 {
     constexpr int CPT = RC / 16;
-    __shared__ float As[TB][TB + 1];
-    __shared__ float Bs[TB][RC + 1];
+    constexpr int BPT = KC * RC / 256;  // B slice elements per thread
+    __shared__ __align__(16) float As[2][KC][TB + 4];
+    __shared__ __align__(16) float Bs[2][KC][RC + 4];
     __shared__ int item_sh;
     const int t = threadIdx.x, tx = t % 16, ty = t / 16;
     for (;;) {
@@ -317,36 +320,73 @@ __global__ void __launch_bounds__(256) batched_gemm_kernel(int nitems, const int
         for (int i = 0; i < 4; ++i)
 #pragma unroll
             for (int j = 0; j < CPT; ++j) acc[i][j] = 0.f;
-        for (int k0 = 0; k0 < k && !skip; k0 += TB) {
-            __syncthreads();
-            for (int idx = t; idx < TB * TB; idx += 256) {
+        const int nslices = skip ? 0 : (k + KC - 1) / KC;
+        float ra[4], rb[BPT];
+        auto load = [&](int sl) {
+            const int k0 = sl * KC;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int e = t + 256 * u;
                 int r, kk;
-                if (ta == 0) { r = idx % TB; kk = idx / TB; } else { kk = idx % TB; r = idx / TB; }
+                if (ta == 0) { r = e % TB; kk = e / TB; } else { kk = e % KC; r = e / KC; }
                 float v = 0.f;
                 if (i0 + r < m && k0 + kk < k)
                     v = ta == 0 ? A[(long)(k0 + kk) * lda + i0 + r] : A[(long)(i0 + r) * lda + k0 + kk];
-                As[r][kk] = v;
+                ra[u] = v;
             }
-            for (int idx = t; idx < TB * RC; idx += 256) {
+#pragma unroll
+            for (int u = 0; u < BPT; ++u) {
+                const int e = t + 256 * u;
                 int kk, c;
-                if (tb == 0) { kk = idx % TB; c = idx / TB; } else { c = idx % RC; kk = idx / RC; }
+                if (tb == 0) { kk = e % KC; c = e / KC; } else { c = e % RC; kk = e / RC; }
                 float v = 0.f;
                 if (k0 + kk < k && j0 + c < n)
                     v = tb == 0 ? Bm[(long)(j0 + c) * ldb + k0 + kk] : Bm[(long)(k0 + kk) * ldb + j0 + c];
-                Bs[kk][c] = v;
+                rb[u] = v;
             }
+        };
+        auto store = [&](int buf) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int e = t + 256 * u;
+                int r, kk;
+                if (ta == 0) { r = e % TB; kk = e / TB; } else { kk = e % KC; r = e / KC; }
+                As[buf][kk][r] = ra[u];
+            }
+#pragma unroll
+            for (int u = 0; u < BPT; ++u) {
+                const int e = t + 256 * u;
+                int kk, c;
+                if (tb == 0) { kk = e % KC; c = e / KC; } else { c = e % RC; kk = e / RC; }
+                Bs[buf][kk][c] = rb[u];
+            }
+        };
+        if (nslices > 0) {
+            load(0);
+            store(0);
             __syncthreads();
-#pragma unroll 8
-            for (int kk = 0; kk < TB; ++kk) {
-                float a[4], b[CPT];
+            for (int sl = 0; sl < nslices; ++sl) {
+                const int buf = sl & 1;
+                if (sl + 1 < nslices) load(sl + 1);
 #pragma unroll
-                for (int i = 0; i < 4; ++i) a[i] = As[ty * 4 + i][kk];
+                for (int kk = 0; kk < KC; ++kk) {
+                    const float4 a = *reinterpret_cast<const float4*>(&As[buf][kk][ty * 4]);
+                    float b[CPT];
+                    if (CPT == 4) {
+                        const float4 bv = *reinterpret_cast<const float4*>(&Bs[buf][kk][tx * 4]);
+                        b[0] = bv.x; b[1] = bv.y; b[2] = bv.z; b[3] = bv.w;
+                    } else {
+                        const float2 bv = *reinterpret_cast<const float2*>(&Bs[buf][kk][tx * CPT]);
+                        b[0] = bv.x; b[1] = bv.y;
+                    }
+                    const float av[4] = {a.x, a.y, a.z, a.w};
 #pragma unroll
-                for (int j = 0; j < CPT; ++j) b[j] = Bs[kk][tx * CPT + j];
+                    for (int i = 0; i < 4; ++i)
 #pragma unroll
-                for (int i = 0; i < 4; ++i)
-#pragma unroll
-                    for (int j = 0; j < CPT; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+                        for (int j = 0; j < CPT; ++j) acc[i][j] = fmaf(av[i], b[j], acc[i][j]);
+                }
+                if (sl + 1 < nslices) store(buf ^ 1);
+                __syncthreads();
             }
         }
 #pragma unroll
@@ -703,7 +743,7 @@ cudaError_t tune_gemm(iclblasHandle_t h, int batch, const std::vector<int>& dims
                       int tri_lower, int tri_strict, BatchList& l)
 {
     if (gemm_items(batch, dims, 64, masked, tri_lower).empty()) return upload_items({}, l);
-    const std::string key = tune_key(h, masked ? "gemm_adj" : "gemm", {ta, tb_, tri_lower, tri_strict}, batch, dims);
+    const std::string key = tune_key(h, masked ? "gemm_adj2" : "gemm2", {ta, tb_, tri_lower, tri_strict}, batch, dims);
     Choice best{64, 1};
     if (!lookup_tune(key, best)) {
         long na = 0, nb = 0, nc = 0;
