@@ -223,6 +223,21 @@ class Sweep:
         return h2d, d2h
 
 
+def max_over_ranks(torch, value, device, world):
+    """The largest per-rank value over all ranks: a replicated job's time is
+    its slowest rank's.  One all-reduce (MAX) when world > 1."""
+    if world <= 1:
+        return float(value)
+    t = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_gbs(world, bytes_per_step, steps, ms):
+    """Whole-job bandwidth: every rank moved bytes_per_step per step in ms."""
+    return world * bytes_per_step * steps / (ms / 1e3) / 1e9
+
+
 def run_ours(args, rank, world, torch):
     from clgpu_b200 import iclblas as B
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
@@ -271,12 +286,8 @@ def run_ours(args, rank, world, torch):
         clocks = clk.summary()
         total_ms = start.elapsed_time(end)
         per_call_ms = {name: float(np.mean([a.elapsed_time(b) for a, b in ev[name]])) for name in ev}
-        t_max = total_ms
-        if world > 1:
-            t = torch.tensor([total_ms], device=dev)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            t_max = float(t.item())
-        value = world * step_bytes * args.steps / (t_max / 1e3) / 1e9
+        t_max = max_over_ranks(torch, total_ms, dev, world)
+        value = aggregate_gbs(world, step_bytes, args.steps, t_max)
 
         # dominant kernel: the call with the largest share of the step
         dom = max(per_call_ms, key=per_call_ms.get)
@@ -309,13 +320,9 @@ def run_ours(args, rank, world, torch):
                     B.check(f(), name)
             s1.record(stream)
             torch.cuda.synchronize()
-            e2e_ms = s0.elapsed_time(s1)
-            if world > 1:
-                t = torch.tensor([e2e_ms], device=dev)
-                torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-                e2e_ms = float(t.item())
+            e2e_ms = max_over_ranks(torch, s0.elapsed_time(s1), dev, world)
             h2d, d2h = swh.io_bytes()
-            e2e = {"value": round(world * step_bytes * e2e_steps / (e2e_ms / 1e3) / 1e9, 2), "unit": "GB/s",
+            e2e = {"value": round(aggregate_gbs(world, step_bytes, e2e_steps, e2e_ms), 2), "unit": "GB/s",
                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": e2e_steps,
                    "ms_per_step": round(e2e_ms / e2e_steps, 3),
                    "path": "C ABI with pinned host operands; copies in/out inside every call"}
