@@ -219,32 +219,36 @@ __global__ void __launch_bounds__(kThreads) trsv_kernel(int n, int lower_op, int
 // ---------------------------------------------------------------- STRSV, TMA path
 // Float TRSV when A is 16-byte aligned with lda a multiple of 4 and >= n
 // (the usual case).  Same ticket-ordered one-launch structure as above, with
-// three changes that shorten the chain of dependent block solves:
+// changes that shorten the chain of dependent block solves:
 //   - tiles arrive by TMA (one 64 x 64 box per cp.async.bulk.tensor) into a
 //     4-stage shared-memory ring, so up to 64 KiB per CTA are in flight while
 //     the CTA waits for earlier blocks, and two CTAs fit on an SM;
-//   - the first box is the diagonal block: the CTA inverts it in FP64 before
-//     it needs it (while earlier blocks are still being solved), so its own
-//     step of the chain is a 64 x 64 FP64 matrix-vector product instead of
-//     64 dependent substitution steps;
+//   - the first box is the diagonal block D, inverted in FP64 (then kept in
+//     FP32) before the CTA needs it; the second box is the tile T next to D
+//     (the block solved just before this one), turned into W = inv(D) T
+//     while earlier blocks are still being solved; then the remaining tiles
+//     in solve order.  Once all but the last earlier block are known, the CTA
+//     forms z = inv(D) (b - sum of those tiles' products), so its own step of
+//     the chain, when the last block x_prev is published, is
+//     x = z - W x_prev: one 64 x 64 product and a publication;
 //   - each solved entry is published as one 64-bit word (value, call epoch):
 //     a consumer polls the entries it needs directly, with no separate flag.
 //     The epoch lives in device memory: each CTA reads the last launch's
 //     epoch at its start and uses the next one; the CTA that solves the last
 //     block stores it back once everything is published (every other CTA has
 //     read it by then), so replays of a captured launch get fresh epochs.
-// Entries of x are FP32 results of FP64 products with the FP64 inverse of the
-// FP32 diagonal block applied to the FP32 right-hand side of the block.
 constexpr int FS = 4;
 constexpr int TILE_ELEMS = NB * NB;
 constexpr unsigned long long kTrsvWaitNs = 2000000000ull;  // a wait gives up after 2 s
 
 struct FastSmem {
     float stage[FS][TILE_ELEMS];
-    double inv[NB][NB + 1];
-    double ys[NB];
-    double partd[4][NB];
+    // FP64 inverse while it is formed; then the same bytes hold the FP32
+    // inverse and W (two [NB][NB + 1] float arrays)
+    double R[NB][NB + 1];
     float xs[NB];
+    float ys[NB];
+    float zs[NB];
     float part[4][NB];
     uint64_t full[FS];
     unsigned s, epoch;
@@ -267,6 +271,8 @@ __global__ void __launch_bounds__(kThreads, 2)
 {
     extern __shared__ unsigned char smem_raw[];
     FastSmem& S = *reinterpret_cast<FastSmem*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    float(*IV)[NB + 1] = reinterpret_cast<float(*)[NB + 1]>(&S.R[0][0]);
+    float(*W)[NB + 1] = IV + NB;
     const int t = threadIdx.x;
     const int nb = (n + NB - 1) / NB;
     if (t == 0) {
@@ -282,21 +288,22 @@ __global__ void __launch_bounds__(kThreads, 2)
     if (s == nb - 1 && t == 0) *ticket = 0u;  // every ticket of this launch is taken
     auto blk = [&](int p) { return lower_op ? p : nb - 1 - p; };
     const int kb = blk(s), r0 = kb * NB, nr = min(NB, n - r0);
-    // load i = 0 is the diagonal block, load i >= 1 the tile of solve-order block i - 1
+    // loads: 0 the diagonal block, 1 the tile of block s-1 (s >= 1), then the
+    // tiles of blocks 0 .. s-2 in solve order
+    const int nloads = s + 1;
+    auto load_block = [&](int i) { return i == 0 ? kb : (i == 1 ? blk(s - 1) : blk(i - 2)); };
     int issued = 0;  // (thread 0)
     auto issue = [&](int i) {
         issued = i + 1;
-        const int cb = i == 0 ? kb : blk(i - 1);
+        const int cb = load_block(i);
         uint64_t* bar = &S.full[i % FS];
         tma::mbar_expect_tx(bar, TILE_ELEMS * 4);
         if (op == 0) tma::load_2d(S.stage[i % FS], &amap, r0, cb * NB, bar);   // A[r0.., cb*NB..]
         else tma::load_2d(S.stage[i % FS], &amap, cb * NB, r0, bar);           // A[cb*NB.., r0..]
     };
     if (t == 0)
-        for (int i = 0; i < min(FS, s + 1); ++i) issue(i);
+        for (int i = 0; i < min(FS, nloads); ++i) issue(i);
     const float b = t < nr ? x[(long)(r0 + t) * incx] : 0.f;
-
-    // ---- diagonal block: FP64 inverse, one column per thread (t < 64)
     // on a failed wait: record it, let this CTA's copies still in flight land
     // (each wait bounded), then leave
     auto bail = [&](int consumed) {
@@ -306,65 +313,9 @@ __global__ void __launch_bounds__(kThreads, 2)
                 tma::mbar_wait_bounded(&S.full[j % FS], (j / FS) & 1, kTrsvWaitNs);
         }
     };
-    int bad = tma::mbar_wait_bounded(&S.full[0], 0, kTrsvWaitNs) ? 0 : 1;
-    if (__syncthreads_or(bad)) {
-        bail(0);
-        return;
-    }
-    if (t < NB) {
-        const float* D = S.stage[0];
-        const int j = t;
-        for (int i = 0; i < NB; ++i) S.inv[i][j] = 0.0;
-        // D(r, c) = op(A)(r0 + r, r0 + c): op N stores column-major, op T row-major
-        auto d = [&](int r, int c) -> double { return (double)(op == 0 ? D[c * NB + r] : D[r * NB + c]); };
-        if (j < nr) {
-            if (lower_op) {
-                for (int i = 0; i < nr; ++i) {
-                    // every thread walks the same (i, k): D reads are broadcasts
-                    double s0 = 0.0, s1 = 0.0;
-                    int k = 0;
-                    for (; k + 1 < i; k += 2) {
-                        s0 = fma(d(i, k), S.inv[k][j], s0);
-                        s1 = fma(d(i, k + 1), S.inv[k + 1][j], s1);
-                    }
-                    if (k < i) s0 = fma(d(i, k), S.inv[k][j], s0);
-                    const double dii = unit ? 1.0 : d(i, i);
-                    double v = 0.0;
-                    if (i == j) v = 1.0 / dii;
-                    else if (i > j) v = -(s0 + s1) / dii;
-                    S.inv[i][j] = v;
-                }
-            } else {
-                for (int i = nr - 1; i >= 0; --i) {
-                    double s0 = 0.0, s1 = 0.0;
-                    int k = i + 1;
-                    for (; k + 1 < nr; k += 2) {
-                        s0 = fma(d(i, k), S.inv[k][j], s0);
-                        s1 = fma(d(i, k + 1), S.inv[k + 1][j], s1);
-                    }
-                    if (k < nr) s0 = fma(d(i, k), S.inv[k][j], s0);
-                    const double dii = unit ? 1.0 : d(i, i);
-                    double v = 0.0;
-                    if (i == j) v = 1.0 / dii;
-                    else if (i < j) v = -(s0 + s1) / dii;
-                    S.inv[i][j] = v;
-                }
-            }
-        }
-    }
-    __syncthreads();
-    if (t == 0 && FS <= s) issue(FS);
-
-    // ---- off-diagonal tiles in solve order
-    const int lane = t & 31, warp = t >> 5;
-    const int rN = t % NB, gN = t / NB;      // op N: row, group of 16 columns
-    float accN = 0.f;
-    float accT[8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i) accT[i] = 0.f;
-    for (int i = 1; i <= s; ++i) {
-        const int c0 = blk(i - 1) * NB, nc = min(NB, n - c0);
-        bad = tma::mbar_wait_bounded(&S.full[i % FS], (i / FS) & 1, kTrsvWaitNs) ? 0 : 1;
+    // waits for the published entries of the block at c0 (threads t < 64 poll)
+    auto fetch_x = [&](int c0, int nc) -> int {
+        int bad = 0;
         if (t < NB) {
             float v = 0.f;
             if (t < nc) {
@@ -373,7 +324,6 @@ __global__ void __launch_bounds__(kThreads, 2)
                 if ((unsigned)(w >> 32) != epoch) {
                     const unsigned long long t0 = tma::global_ns();
                     for (;;) {
-                        __nanosleep(32);
                         w = ld_relaxed_u64(src);
                         if ((unsigned)(w >> 32) == epoch) break;
                         if (ld_volatile(status) != kDevOk) { bad = 1; break; }
@@ -388,6 +338,108 @@ __global__ void __launch_bounds__(kThreads, 2)
             }
             S.xs[t] = v;
         }
+        return bad;
+    };
+    const int rN = t % NB, gN = t / NB;      // row, group of 16 columns
+    // element (r, c) of the op(A) tile in a stage
+    auto tile = [&](const float* T, int r, int c) { return op == 0 ? T[c * NB + r] : T[r * NB + c]; };
+
+    // ---- diagonal block: FP64 inverse (one column per thread, t < 64), then FP32
+    int bad = tma::mbar_wait_bounded(&S.full[0], 0, kTrsvWaitNs) ? 0 : 1;
+    if (__syncthreads_or(bad)) {
+        bail(0);
+        return;
+    }
+    if (t < NB) {
+        const float* D = S.stage[0];
+        const int j = t;
+        for (int i = 0; i < NB; ++i) S.R[i][j] = 0.0;
+        auto d = [&](int r, int c) -> double { return (double)tile(D, r, c); };
+        if (j < nr) {
+            if (lower_op) {
+                for (int i = 0; i < nr; ++i) {
+                    // every thread walks the same (i, k): D reads are broadcasts
+                    double s0 = 0.0, s1 = 0.0;
+                    int k = 0;
+                    for (; k + 1 < i; k += 2) {
+                        s0 = fma(d(i, k), S.R[k][j], s0);
+                        s1 = fma(d(i, k + 1), S.R[k + 1][j], s1);
+                    }
+                    if (k < i) s0 = fma(d(i, k), S.R[k][j], s0);
+                    const double dii = unit ? 1.0 : d(i, i);
+                    double v = 0.0;
+                    if (i == j) v = 1.0 / dii;
+                    else if (i > j) v = -(s0 + s1) / dii;
+                    S.R[i][j] = v;
+                }
+            } else {
+                for (int i = nr - 1; i >= 0; --i) {
+                    double s0 = 0.0, s1 = 0.0;
+                    int k = i + 1;
+                    for (; k + 1 < nr; k += 2) {
+                        s0 = fma(d(i, k), S.R[k][j], s0);
+                        s1 = fma(d(i, k + 1), S.R[k + 1][j], s1);
+                    }
+                    if (k < nr) s0 = fma(d(i, k), S.R[k][j], s0);
+                    const double dii = unit ? 1.0 : d(i, i);
+                    double v = 0.0;
+                    if (i == j) v = 1.0 / dii;
+                    else if (i < j) v = -(s0 + s1) / dii;
+                    S.R[i][j] = v;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    {
+        float v[TILE_ELEMS / kThreads];
+#pragma unroll
+        for (int u = 0; u < TILE_ELEMS / kThreads; ++u) {
+            const int idx = t + kThreads * u;
+            v[u] = (float)S.R[idx % NB][idx / NB];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < TILE_ELEMS / kThreads; ++u) {
+            const int idx = t + kThreads * u;
+            IV[idx % NB][idx / NB] = v[u];
+        }
+    }
+    __syncthreads();
+    if (t == 0 && FS < nloads) issue(FS);
+
+    // ---- W = inv(D) T for the tile of block s-1
+    if (s >= 1) {
+        bad = tma::mbar_wait_bounded(&S.full[1], 0, kTrsvWaitNs) ? 0 : 1;
+        if (__syncthreads_or(bad)) {
+            bail(1);
+            return;
+        }
+        const float* T = S.stage[1];
+        float acc[16];
+#pragma unroll
+        for (int jj = 0; jj < 16; ++jj) acc[jj] = 0.f;
+        for (int k = 0; k < NB; ++k) {
+            const float a = IV[rN][k];
+#pragma unroll
+            for (int jj = 0; jj < 16; ++jj) acc[jj] = fmaf(a, tile(T, k, gN * 16 + jj), acc[jj]);
+        }
+#pragma unroll
+        for (int jj = 0; jj < 16; ++jj) W[rN][gN * 16 + jj] = acc[jj];
+        __syncthreads();
+        if (t == 0 && FS + 1 < nloads) issue(FS + 1);
+    }
+
+    // ---- the other earlier blocks, in solve order
+    const int lane = t & 31, warp = t >> 5;
+    float accN = 0.f;
+    float accT[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) accT[i] = 0.f;
+    for (int i = 2; i <= s; ++i) {
+        const int c0 = blk(i - 2) * NB, nc = min(NB, n - c0);
+        bad = tma::mbar_wait_bounded(&S.full[i % FS], (i / FS) & 1, kTrsvWaitNs) ? 0 : 1;
+        bad |= fetch_x(c0, nc);
         if (__syncthreads_or(bad)) {
             bail(i);
             return;
@@ -409,10 +461,10 @@ __global__ void __launch_bounds__(kThreads, 2)
             }
         }
         __syncthreads();
-        if (t == 0 && i + FS <= s) issue(i + FS);
+        if (t == 0 && i + FS < nloads) issue(i + FS);
     }
 
-    // ---- row sums, right-hand side, x = inv * y in FP64, publish
+    // ---- z = inv(D) (b - row sums)
     if (op == 0) {
         S.part[gN][rN] = accN;
     } else {
@@ -425,21 +477,35 @@ __global__ void __launch_bounds__(kThreads, 2)
     __syncthreads();
     if (t < NB) {
         const float sum = op == 0 ? (S.part[0][t] + S.part[1][t]) + (S.part[2][t] + S.part[3][t]) : S.part[0][t];
-        S.ys[t] = t < nr ? (double)(b + sum) : 0.0;
+        S.ys[t] = t < nr ? b + sum : 0.f;
     }
     __syncthreads();
     {
-        double acc = 0.0;
+        float acc = 0.f;
 #pragma unroll
-        for (int jj = 0; jj < 16; ++jj) {
-            const int c = gN * 16 + jj;
-            acc = fma(S.inv[rN][c], S.ys[c], acc);
-        }
-        S.partd[gN][rN] = acc;
+        for (int jj = 0; jj < 16; ++jj) acc = fmaf(IV[rN][gN * 16 + jj], S.ys[gN * 16 + jj], acc);
+        S.part[gN][rN] = acc;
     }
     __syncthreads();
+    if (t < NB) S.zs[t] = (S.part[0][t] + S.part[1][t]) + (S.part[2][t] + S.part[3][t]);
+
+    // ---- this block's step of the chain: x = z - W x_prev
+    if (s >= 1) {
+        const int c0 = blk(s - 1) * NB, nc = min(NB, n - c0);
+        bad = fetch_x(c0, nc);
+        if (__syncthreads_or(bad)) {
+            bail(nloads);
+            return;
+        }
+        float acc = 0.f;
+#pragma unroll
+        for (int jj = 0; jj < 16; ++jj) acc = fmaf(W[rN][gN * 16 + jj], S.xs[gN * 16 + jj], acc);
+        S.part[gN][rN] = acc;
+        __syncthreads();
+        if (t < nr) S.zs[t] -= (S.part[0][t] + S.part[1][t]) + (S.part[2][t] + S.part[3][t]);
+    }
     if (t < nr) {
-        const float xf = (float)((S.partd[0][t] + S.partd[1][t]) + (S.partd[2][t] + S.partd[3][t]));
+        const float xf = S.zs[t];
         x[(long)(r0 + t) * incx] = xf;
         st_relaxed_u64(pub + r0 + t, ((unsigned long long)epoch << 32) | __float_as_uint(xf));
     }
