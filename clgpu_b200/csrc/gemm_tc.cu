@@ -484,9 +484,53 @@ __device__ __forceinline__ void put(const SplitOut& o, long idx, float x)
     if (o.nlev > 2) ((__nv_bfloat16*)o.plane[2])[idx] = l;
 }
 
-// 32 x 32 tile of L per block (blockDim 32 x 8), transposed through shared
-// memory when the source is contiguous along r, so that both the reads of S
-// and the K-contiguous writes are coalesced.
+// Real operands: 32 rows x 64 K per block (256 threads).  Reads are coalesced
+// along the source's contiguous dimension (through shared memory); each
+// thread then writes two consecutive K values: one bfloat162 per plane, or a
+// float2 for TF32 (128- or 256-byte rows per warp).
+__global__ void __launch_bounds__(256) split_real_kernel(int R, int K, const float* __restrict__ S, long rs, long ks,
+                                                         SplitOut o)
+{
+    __shared__ float tile[32][65];
+    const int k0 = blockIdx.x * 64, r0 = blockIdx.y * 32, t = threadIdx.x;
+    if (rs == 1) {  // contiguous along r
+        for (int idx = t; idx < 32 * 64; idx += 256) {
+            const int rr = idx % 32, kk = idx / 32;
+            const int r = r0 + rr, k = k0 + kk;
+            tile[rr][kk] = (r < R && k < K) ? S[(long)r + (long)k * ks] : 0.f;
+        }
+    } else {        // contiguous along k (ks == 1)
+        for (int idx = t; idx < 32 * 64; idx += 256) {
+            const int kk = idx % 64, rr = idx / 64;
+            const int r = r0 + rr, k = k0 + kk;
+            tile[rr][kk] = (r < R && k < K) ? S[(long)r * rs + k] : 0.f;
+        }
+    }
+    __syncthreads();
+    for (int idx = t; idx < 32 * 32; idx += 256) {
+        const int kp = idx % 32, rr = idx / 32;
+        const int r = r0 + rr, k = k0 + 2 * kp;
+        if (r >= R || k >= o.kpad) continue;
+        const float a = tile[rr][2 * kp], b = tile[rr][2 * kp + 1];
+        const long off = (long)r * o.kpad + k;  // even: 4- and 8-byte aligned pairs
+        if (o.tf32) {
+            *reinterpret_cast<float2*>((float*)o.plane[0] + off) = make_float2(to_tf32(a), to_tf32(b));
+        } else {
+            __nv_bfloat16 ha, ma, la, hb, mb, lb;
+            split3(a, ha, ma, la);
+            split3(b, hb, mb, lb);
+            *reinterpret_cast<__nv_bfloat162*>((__nv_bfloat16*)o.plane[0] + off) = __halves2bfloat162(ha, hb);
+            if (o.nlev > 1)
+                *reinterpret_cast<__nv_bfloat162*>((__nv_bfloat16*)o.plane[1] + off) = __halves2bfloat162(ma, mb);
+            if (o.nlev > 2)
+                *reinterpret_cast<__nv_bfloat162*>((__nv_bfloat16*)o.plane[2] + off) = __halves2bfloat162(la, lb);
+        }
+    }
+}
+
+// Complex operands: 32 x 32 tile of L per block (blockDim 32 x 8), transposed
+// through shared memory when the source is contiguous along r, so that both
+// the reads of S and the K-contiguous writes are coalesced.
 template <class T>
 __global__ void __launch_bounds__(256) split_kernel(int R, int K, const T* __restrict__ S, long rs, long ks, int conj,
                                                     int mode, SplitOut o)
@@ -616,8 +660,12 @@ template <class T>
 cudaError_t run_split(iclblasHandle_t h, const T* S, int R, int K, long rs, long ks, int conj, int mode,
                       const SplitOut& o, long out_rows)
 {
-    const int kgrid = std::is_same<T, float>::value ? (int)(o.kpad / 32) : ceil_div(K, 32);
-    dim3 grid(kgrid, ceil_div(R, 32));
+    if (std::is_same<T, float>::value) {
+        dim3 grid((unsigned)ceil_div(o.kpad, 64L), (unsigned)ceil_div(R, 32));
+        split_real_kernel<<<grid, 256, 0, h->stream>>>(R, K, (const float*)S, rs, ks, o);
+        return cudaGetLastError();
+    }
+    dim3 grid(ceil_div(K, 32), ceil_div(R, 32));
     split_kernel<T><<<grid, dim3(32, 8), 0, h->stream>>>(R, K, S, rs, ks, conj, mode, o);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;

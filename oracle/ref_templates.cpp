@@ -26,6 +26,15 @@ void ref_cpu_sgemm(int ta, int tb, int m, int n, int k, float alpha, const float
     cpu_gemm<float>((iclblasOperation_t)ta, (iclblasOperation_t)tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
 }
 
+// cpu_gemm in double with a double accumulator: ties the FP64 products used
+// as the error reference of the precision studies to the reference's GEMM.
+void ref_cpu_dgemm(int ta, int tb, int m, int n, int k, double alpha, const double* A, int lda,
+                   const double* B, int ldb, double beta, double* C, int ldc)
+{
+    cpu_gemm<double, double>((iclblasOperation_t)ta, (iclblasOperation_t)tb, m, n, k, alpha, A, lda, B, ldb, beta, C,
+                             ldc);
+}
+
 void ref_cpu_cgemm(int ta, int tb, int m, int n, int k, const float* alpha, const float* A, int lda,
                    const float* B, int ldb, const float* beta, float* C, int ldc)
 {

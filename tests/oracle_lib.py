@@ -82,6 +82,7 @@ def ref() -> C.CDLL | None:
         sig = {
             "ref_cpu_sgemm": ([i, i, i, i, i, f, p, i, p, i, f, p, i], None),
             "ref_cpu_cgemm": ([i, i, i, i, i, p, p, i, p, i, p, p, i], None),
+            "ref_cpu_dgemm": ([i, i, i, i, i, C.c_double, p, i, p, i, C.c_double, p, i], None),
             "ref_cpu_sdot": ([i, p, i, p, i], f),
             "ref_cpu_cdot": ([i, p, i, p, i, i, p], None),
             "ref_cpu_snrm2": ([i, p, i], f),
