@@ -51,13 +51,21 @@ namespace tc {
 namespace {
 
 constexpr int BM = 128;
-constexpr int BN = 256;
-constexpr int STAGES = 4;
 constexpr int ROW_BYTES = 128;                  // one K block per tile row
 constexpr int A_TILE = BM * ROW_BYTES;          // 16 KiB
-constexpr int B_TILE = BN * ROW_BYTES;          // 32 KiB
-constexpr int STAGE_BYTES = A_TILE + B_TILE;    // 48 KiB
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*barriers*/ + 1024 /*alignment*/;
+constexpr int RING_BYTES = 192 * 1024;          // the stage ring
+constexpr int SMEM_BYTES = RING_BYTES + 1024 /*barriers*/ + 1024 /*alignment*/;
+// Output tile 128 x BN: 256 columns, or 128 when the 256-wide tiles would
+// leave a quarter or more of the SMs idle (more, smaller tiles).
+template <int BN_>
+struct Tile {
+    static constexpr int BN = BN_;
+    static constexpr int B_TILE = BN * ROW_BYTES;             // 32 or 16 KiB
+    static constexpr int STAGE_BYTES = A_TILE + B_TILE;       // 48 or 32 KiB
+    static constexpr int STAGES = RING_BYTES / STAGE_BYTES;   // 4 or 6
+    static constexpr int TMEM_COLS = 2 * BN;                  // two accumulators
+    static constexpr int EPI_COLS = BN / 2;                   // columns per epilogue warp
+};
 constexpr int EPI_WARPS = 8;                    // two per TMEM lane quarter
 constexpr int THREADS = 64 + 32 * EPI_WARPS;    // producer, MMA, epilogue
 constexpr int GROUP_M = 16;                     // tile raster: 16 M-tiles per band
@@ -214,9 +222,9 @@ __device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t saddr)
 
 // Instruction descriptor: FP32 accumulator, A/B format (1 = BF16, 2 = TF32),
 // both K-major, N = 256, M = 128.
-__host__ __device__ constexpr uint32_t instr_desc(uint32_t ab_format)
+__host__ __device__ constexpr uint32_t instr_desc(uint32_t ab_format, int bn)
 {
-    return (1u << 4) | (ab_format << 7) | (ab_format << 10) | ((uint32_t)(BN >> 3) << 17) |
+    return (1u << 4) | (ab_format << 7) | (ab_format << 10) | ((uint32_t)(bn >> 3) << 17) |
            ((uint32_t)(BM >> 4) << 24);
 }
 
@@ -231,7 +239,7 @@ __device__ __forceinline__ void tile_coords(int t, int tiles_m, int tiles_n, int
     tn = in_band / rows;
 }
 
-template <bool TF32>
+template <bool TF32, int BN_>
 __global__ void __launch_bounds__(THREADS, 1)
     gemm_tc_kernel(const __grid_constant__ CUtensorMap mA0, const __grid_constant__ CUtensorMap mA1,
                    const __grid_constant__ CUtensorMap mA2, const __grid_constant__ CUtensorMap mB0,
@@ -240,6 +248,8 @@ __global__ void __launch_bounds__(THREADS, 1)
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     uint8_t* tiles = smem;
+    using TC = Tile<BN_>;
+    constexpr int BN = TC::BN, STAGES = TC::STAGES, STAGE_BYTES = TC::STAGE_BYTES, EPI_COLS = TC::EPI_COLS;
     uint64_t* full = (uint64_t*)(smem + STAGES * STAGE_BYTES);
     uint64_t* empty = full + STAGES;
     uint64_t* tfull = empty + STAGES;
@@ -265,7 +275,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 1) {
-        tmem_alloc(tmem_slot, 512);
+        tmem_alloc(tmem_slot, TC::TMEM_COLS);
         tmem_relinquish();
     }
     tc_fence_before();
@@ -304,7 +314,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     } else if (warp == 1) {
         // ---------------------------------------------------------- MMA issuer
         if (lane == 0) {
-            const uint32_t idesc = instr_desc(TF32 ? 2u : 1u);
+            const uint32_t idesc = instr_desc(TF32 ? 2u : 1u, BN);
             int s = 0;
             uint32_t ph = 0;
             int acc = 0;
@@ -344,7 +354,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         // ---------------------------------------------------------- epilogue
         const int ew = warp - 2;
         const int q = warp & 3;             // TMEM lane quarter this warp may access
-        const int half = ew / 4;            // columns [half*128, half*128+128) of the tile
+        const int half = ew / 4;            // columns [half*EPI_COLS, (half+1)*EPI_COLS) of the tile
         const int nchunks = (p.kblocks + p.chunk - 1) / p.chunk;
         int acc = 0;
         uint32_t acc_ph = 0;
@@ -352,18 +362,19 @@ __global__ void __launch_bounds__(THREADS, 1)
         for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
             int tm, tn;
             tile_coords(t, tiles_m, tiles_n, tm, tn);
-            float sum[128];
+            float sum[EPI_COLS];
 #pragma unroll
-            for (int j = 0; j < 128; ++j) sum[j] = 0.f;
+            for (int j = 0; j < EPI_COLS; ++j) sum[j] = 0.f;
             for (int c = 0; c < nchunks; ++c) {
                 int w = 1;
                 if (lane == 0) w = mbar_wait(&tfull[acc], acc_ph, abort_flag) ? 1 : 0;
                 ok = __shfl_sync(0xffffffffu, w, 0) != 0;
                 if (!ok) break;
                 tc_fence_after();
-                const uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN + half * 128);
+                const uint32_t taddr =
+                    tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN + half * EPI_COLS);
 #pragma unroll
-                for (int g = 0; g < 4; ++g) {
+                for (int g = 0; g < EPI_COLS / 32; ++g) {
                     float v[32];
                     tmem_ld32(taddr + (uint32_t)(g * 32), v);
 #pragma unroll
@@ -376,14 +387,14 @@ __global__ void __launch_bounds__(THREADS, 1)
             }
             if (!ok) break;
             const int row = tm * BM + q * 32 + lane;
-            const int col0 = tn * BN + half * 128;
+            const int col0 = tn * BN + half * EPI_COLS;
             const bool beta_zero = p.beta_re == 0.f && p.beta_im == 0.f;
             // C is read in groups of 8 columns before any of them is stored,
             // so the loads overlap (columns of C never alias for ldc >= M)
             if (row < p.M) {
                 if (!p.complex_out) {
 #pragma unroll
-                    for (int j0 = 0; j0 < 128; j0 += 8) {
+                    for (int j0 = 0; j0 < EPI_COLS; j0 += 8) {
                         float cv[8];
 #pragma unroll
                         for (int j = 0; j < 8; ++j) {
@@ -402,7 +413,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                 } else {
                     float2* const C2 = (float2*)p.C;
 #pragma unroll
-                    for (int j0 = 0; j0 < 128; j0 += 8) {
+                    for (int j0 = 0; j0 < EPI_COLS; j0 += 8) {
                         float2 cv[4];
 #pragma unroll
                         for (int j = 0; j < 4; ++j) {
@@ -435,7 +446,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     if (threadIdx.x == 0 && *abort_flag) atomicOr(p.status, (int)kDevWaitTimeout);
     if (warp == 1) {
         tc_fence_after();
-        tmem_dealloc(tmem_base, 512);
+        tmem_dealloc(tmem_base, TC::TMEM_COLS);
     }
 }
 
@@ -714,11 +725,14 @@ cudaError_t gemm_tc(iclblasHandle_t h, int ta, int tb, int m, int n, int k, T al
     e = run_split<T>(h, B, n, k, bt ? 1 : ldb, bt ? ldb : 1, tb == ICLBLAS_OP_C, kCplxB, ob, rows_b);
     if (e != cudaSuccess) return e;
 
+    // 128-wide tiles when 256-wide ones would leave a quarter of the SMs idle
+    const int tiles256 = ceil_div(m, BM) * ceil_div((long)rows_b, 256);
+    const int bn = tiles256 * 4 < h->sm_count * 3 ? 128 : 256;
     CUtensorMap ma[3], mb[3];
     for (int l = 0; l < 3; ++l) {
         const int ll = l < mi.nlev ? l : 0;
         if (!make_map(&ma[l], oa.plane[ll], mi.tf32, rows_a, kpad, BM)) return cudaErrorInvalidValue;
-        if (!make_map(&mb[l], ob.plane[ll], mi.tf32, rows_b, kpad, BN)) return cudaErrorInvalidValue;
+        if (!make_map(&mb[l], ob.plane[ll], mi.tf32, rows_b, kpad, bn)) return cudaErrorInvalidValue;
     }
     Params p{};
     p.M = m;
@@ -742,19 +756,16 @@ cudaError_t gemm_tc(iclblasHandle_t h, int ta, int tb, int m, int n, int k, T al
     p.ldc = ldc;
     p.status = h->ws.dev_status;
 
-    const int tiles = ceil_div(m, BM) * ceil_div((long)rows_b, BN);
+    const int tiles = ceil_div(m, BM) * ceil_div((long)rows_b, bn);
     const int grid = std::min(tiles, h->sm_count);
-    if (mi.tf32) {
-        e = cudaFuncSetAttribute(gemm_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-        if (e != cudaSuccess) return e;
-        gemm_tc_kernel<true><<<grid, THREADS, SMEM_BYTES, h->stream>>>(ma[0], ma[1], ma[2], mb[0], mb[1], mb[2], p);
-    } else {
-        e = cudaFuncSetAttribute(gemm_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-        if (e != cudaSuccess) return e;
-        gemm_tc_kernel<false><<<grid, THREADS, SMEM_BYTES, h->stream>>>(ma[0], ma[1], ma[2], mb[0], mb[1], mb[2],
-                                                                         p);
-    }
-    return cudaGetLastError();
+    auto run = [&](auto kernel) -> cudaError_t {
+        cudaError_t r = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+        if (r != cudaSuccess) return r;
+        kernel<<<grid, THREADS, SMEM_BYTES, h->stream>>>(ma[0], ma[1], ma[2], mb[0], mb[1], mb[2], p);
+        return cudaGetLastError();
+    };
+    if (mi.tf32) return bn == 128 ? run(gemm_tc_kernel<true, 128>) : run(gemm_tc_kernel<true, 256>);
+    return bn == 128 ? run(gemm_tc_kernel<false, 128>) : run(gemm_tc_kernel<false, 256>);
 }
 
 template cudaError_t gemm_tc<float>(iclblasHandle_t, int, int, int, int, int, float, const float*, int, const float*,

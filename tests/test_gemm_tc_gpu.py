@@ -100,3 +100,32 @@ def test_plain_mode_unchanged_after_tc(handle):
     handle.set_math_mode(B.MATH_PLAIN_FP32)
     assert B.iclblasSgemm(handle, 0, 0, m, n, k, 1.0, A, m, Bm, k, 1.0, Cm, m) == B.SUCCESS
     assert np.array_equal(Cm, C_ref)
+
+
+@pytest.mark.parametrize("mode", [B.MATH_TF32, B.MATH_BF16X3, B.MATH_BF16X6])
+def test_sgemm_tensor_core_256_wide_tiles(handle, mode):
+    """Large enough for 256-column tiles (the sizes above run 128-column ones)."""
+    m, n, k = 1536, 2560, 100
+    rng = np.random.default_rng(500 + mode)
+    A = O.colmajor(k, m, k + 4, rng)          # op T
+    Bm = O.colmajor(k, n, k, rng)
+    Cm = O.colmajor(m, n, m, rng)
+    ref = _dref(1, 0, m, n, k, 0.75, A, k + 4, Bm, k, -1.25, Cm, m)
+    handle.set_math_mode(mode)
+    assert B.iclblasSgemm(handle, 1, 0, m, n, k, 0.75, A, k + 4, Bm, k, -1.25, Cm, m) == B.SUCCESS
+    assert O.rel_fro(Cm, ref) <= BARS[mode]
+
+
+def test_cgemm_tensor_core_256_wide_tiles(handle):
+    m, n, k = 1280, 1600, 40
+    rng = np.random.default_rng(77)
+    A = O.colmajor(m, k, m, rng, np.complex64)
+    Bm = O.colmajor(n, k, n, rng, np.complex64)   # op C
+    Cm = O.colmajor(m, n, m, rng, np.complex64)
+    al, be = 0.5 + 0.25j, -0.75j
+    Ad = A.astype(np.complex128).reshape(k, m).T
+    Bd = Bm.astype(np.complex128).reshape(k, n).T
+    ref = al * (Ad @ Bd.conj().T) + be * Cm.astype(np.complex128).reshape(n, m).T
+    handle.set_math_mode(B.MATH_BF16X6)
+    assert B.iclblasCgemm(handle, 0, 2, m, n, k, al, A, m, Bm, n, be, Cm, m) == B.SUCCESS
+    assert O.rel_fro(Cm.reshape(n, m).T, ref) <= BARS[B.MATH_BF16X6]
