@@ -43,58 +43,96 @@ constexpr int TB = 64;  // row block / tile height
 
 // ---------------------------------------------------------------- diagonal inverses
 // Inverse of every 64 x 64 diagonal block of every instance's M = op(A),
-// formed in FP64 (thread j solves D y = e_j by substitution; rows and columns
-// beyond the instance's size are the identity) and stored in FP32,
-// column-major, 4096 floats per block at inv + inv_off[instance] + 4096*block.
-// One CTA of 64 threads per (instance, block) item.
-__global__ void __launch_bounds__(TB) batched_inv_kernel(const int2* __restrict__ inv_items,
-                                                         const int* __restrict__ dims,
-                                                         const long* __restrict__ inv_off, int lower_op, int op,
-                                                         int unit, const float* const* __restrict__ Aptr,
-                                                         float* __restrict__ inv)
+// formed in FP64 and stored in FP32, column-major, 4096 floats per block at
+// inv + inv_off[instance] + 4096*block; rows and columns beyond the
+// instance's size are the identity.  One CTA of 256 threads per (instance,
+// block) item, blocked so that no long dependent chain remains:
+//   1. the four 16 x 16 diagonal sub-blocks by substitution (64 threads, one
+//      column each);
+//   2. doubling to 32 and then to 64: for M = [[P, 0], [C, Q]] (lower)
+//      inv = [[P^-1, 0], [-Q^-1 C P^-1, Q^-1]], and for M = [[P, C], [0, Q]]
+//      (upper) the off-diagonal block is -P^-1 C Q^-1; each step is two small
+//      products spread over all threads.
+constexpr int kInvThreads = 256;
+
+__global__ void __launch_bounds__(kInvThreads) batched_inv_kernel(const int2* __restrict__ inv_items,
+                                                                  const int* __restrict__ dims,
+                                                                  const long* __restrict__ inv_off, int lower_op,
+                                                                  int op, int unit,
+                                                                  const float* const* __restrict__ Aptr,
+                                                                  float* __restrict__ inv)
 {
     extern __shared__ double ysm[];
-    double(*Y)[TB + 1] = (double(*)[TB + 1])ysm;
-    float(*D)[TB + 1] = (float(*)[TB + 1])(ysm + TB * (TB + 1));
+    double(*Y)[TB + 1] = (double(*)[TB + 1])ysm;              // the inverse being built
+    double(*Tm)[TB / 2 + 1] = (double(*)[TB / 2 + 1])(ysm + TB * (TB + 1));  // doubling temporary
+    float(*D)[TB + 1] = (float(*)[TB + 1])(ysm + TB * (TB + 1) + (TB / 2) * (TB / 2 + 1));
+    const int t = threadIdx.x;
     const int2 w = inv_items[blockIdx.x];
     const int* d = dims + 4 * w.x;
     const int m = d[0];
     const long lda = d[2];
     const float* A = Aptr[w.x];
     const int r0 = w.y * TB, nr = min(TB, m - r0);
-    for (int idx = threadIdx.x; idx < TB * TB; idx += TB) {
+    for (int idx = t; idx < TB * TB; idx += kInvThreads) {
         const int r = idx % TB, c = idx / TB;  // A-local (r, c): coalesced down A's columns
-        float v = 0.f;
-        if (r < nr && c < nr) v = A[(long)(r0 + c) * lda + r0 + r];
+        float v = (r == c && (r >= nr || unit)) ? 1.f : 0.f;
+        if (r < nr && c < nr && !(r == c && unit)) v = A[(long)(r0 + c) * lda + r0 + r];
         if (op == 0) D[r][c] = v;
         else D[c][r] = v;
     }
+    for (int idx = t; idx < TB * TB; idx += kInvThreads) Y[idx % TB][idx / TB] = 0.0;
     __syncthreads();
-    const int j = threadIdx.x;
-    if (lower_op) {
-        for (int i = 0; i < TB; ++i) {
-            double y = 0.0;
-            if (i >= j) {
-                y = (i == j) ? 1.0 : 0.0;
-                for (int k = j; k < i; ++k) y = fma(-(double)D[i][k], Y[k][j], y);
-                if (!unit && i < nr) y /= (double)D[i][i];
+    // 1. 16 x 16 diagonal sub-blocks, one column per thread
+    if (t < TB) {
+        const int b = (t / 16) * 16, j = t % 16;
+        if (lower_op) {
+            for (int i = 0; i < 16; ++i) {
+                double y = (i == j) ? 1.0 : 0.0;
+                for (int k = j; k < i; ++k) y = fma(-(double)D[b + i][b + k], Y[b + k][b + j], y);
+                Y[b + i][b + j] = (i >= j) ? y / (double)D[b + i][b + i] : 0.0;
             }
-            Y[i][j] = y;
-        }
-    } else {
-        for (int i = TB - 1; i >= 0; --i) {
-            double y = 0.0;
-            if (i <= j) {
-                y = (i == j) ? 1.0 : 0.0;
-                for (int k = i + 1; k <= j; ++k) y = fma(-(double)D[i][k], Y[k][j], y);
-                if (!unit && i < nr) y /= (double)D[i][i];
+        } else {
+            for (int i = 15; i >= 0; --i) {
+                double y = (i == j) ? 1.0 : 0.0;
+                for (int k = i + 1; k <= j; ++k) y = fma(-(double)D[b + i][b + k], Y[b + k][b + j], y);
+                Y[b + i][b + j] = (i <= j) ? y / (double)D[b + i][b + i] : 0.0;
             }
-            Y[i][j] = y;
         }
     }
     __syncthreads();
+    // 2. doubling: blocks of size h combine into 2h
+    for (int h = 16; h < TB; h *= 2) {
+        const int npairs = TB / (2 * h), nout = npairs * h * h;
+        // T = C P^-1 (lower) or C Q^-1 (upper), C the off-diagonal block of D
+        for (int idx = t; idx < nout; idx += kInvThreads) {
+            const int pr = idx / (h * h), e = idx % (h * h), r = e % h, c = e / h;
+            const int o = pr * 2 * h;
+            double acc = 0.0;
+            if (lower_op) {
+                for (int k = 0; k < h; ++k) acc = fma((double)D[o + h + r][o + k], Y[o + k][o + c], acc);
+            } else {
+                for (int k = 0; k < h; ++k) acc = fma((double)D[o + r][o + h + k], Y[o + h + k][o + h + c], acc);
+            }
+            Tm[pr * h + r][c] = acc;
+        }
+        __syncthreads();
+        // off-diagonal block of the inverse: -Q^-1 T (lower) or -P^-1 T (upper)
+        for (int idx = t; idx < nout; idx += kInvThreads) {
+            const int pr = idx / (h * h), e = idx % (h * h), r = e % h, c = e / h;
+            const int o = pr * 2 * h;
+            double acc = 0.0;
+            if (lower_op) {
+                for (int k = 0; k < h; ++k) acc = fma(Y[o + h + r][o + h + k], Tm[pr * h + k][c], acc);
+                Y[o + h + r][o + c] = -acc;
+            } else {
+                for (int k = 0; k < h; ++k) acc = fma(Y[o + r][o + k], Tm[pr * h + k][c], acc);
+                Y[o + r][o + h + c] = -acc;
+            }
+        }
+        __syncthreads();
+    }
     float* out = inv + inv_off[w.x] + (long)w.y * TB * TB;
-    for (int idx = threadIdx.x; idx < TB * TB; idx += TB) out[idx] = (float)Y[idx % TB][idx / TB];
+    for (int idx = t; idx < TB * TB; idx += kInvThreads) out[idx] = (float)Y[idx % TB][idx / TB];
 }
 
 // ---------------------------------------------------------------- TRSM kernel
@@ -498,7 +536,8 @@ int grid_of(iclblasHandle_t h, const BatchList& l)
 }
 
 // ---------------------------------------------------------------- host: launches
-constexpr int kInvSmem = TB * (TB + 1) * (int)(sizeof(double) + sizeof(float));
+constexpr int kInvSmem = TB * (TB + 1) * (int)(sizeof(double) + sizeof(float)) +
+                         (TB / 2) * (TB / 2 + 1) * (int)sizeof(double);
 
 // The pass forming the diagonal-block inverses of M = op(A).
 cudaError_t launch_inv(iclblasHandle_t h, const int2* inv_items, int n_inv, const int* dims, const long* inv_off,
@@ -512,7 +551,8 @@ cudaError_t launch_inv(iclblasHandle_t h, const int2* inv_items, int n_inv, cons
         if (e != cudaSuccess) return e;
         attr = true;
     }
-    batched_inv_kernel<<<n_inv, TB, kInvSmem, h->stream>>>(inv_items, dims, inv_off, lower_op, op, unit, A, inv);
+    batched_inv_kernel<<<n_inv, kInvThreads, kInvSmem, h->stream>>>(inv_items, dims, inv_off, lower_op, op, unit, A,
+                                                                    inv);
     return cudaGetLastError();
 }
 
