@@ -206,9 +206,13 @@ __global__ void __launch_bounds__(256) trsm_inv_double_kernel(int n, int op, int
     for (int a = 0; a < PT; ++a)
 #pragma unroll
         for (int c = 0; c < PT; ++c) acc[a][c] = wz(W());
-    for (int k0 = 0; k0 < s; k0 += KC) {
-        for (int idx = threadIdx.x; idx < TS * KC; idx += 256) {
-            const int r = idx % TS, k = idx / TS;
+    // K slices of KC, the next slice's operands prefetched into registers
+    constexpr int XPT = TS * KC / 256, YPT = KC * TS / 256;
+    W rx[XPT], ry[YPT];
+    auto load = [&](int k0) {
+#pragma unroll
+        for (int u = 0; u < XPT; ++u) {
+            const int idx = threadIdx.x + 256 * u, r = idx % TS, k = idx / TS;
             W v;
             if (STEP == 0) {
                 const int gi = gbase + xr + i0 + r, gj = gbase + xc + k0 + k;  // M(gi, gj)
@@ -221,13 +225,32 @@ __global__ void __launch_bounds__(256) trsm_inv_double_kernel(int n, int op, int
             } else {
                 v = invb[(long)(xc + k0 + k) * big + xr + i0 + r];
             }
-            Xs[r][k] = v;
+            rx[u] = v;
         }
-        for (int idx = threadIdx.x; idx < KC * TS; idx += 256) {
-            const int k = idx % KC, c = idx / KC;
-            Ys[k][c] = (STEP == 0) ? invb[(long)(yo + j0 + c) * big + yo + k0 + k] : tz[(long)(j0 + c) * s + k0 + k];
+#pragma unroll
+        for (int u = 0; u < YPT; ++u) {
+            const int idx = threadIdx.x + 256 * u, k = idx % KC, c = idx / KC;
+            ry[u] = (STEP == 0) ? invb[(long)(yo + j0 + c) * big + yo + k0 + k] : tz[(long)(j0 + c) * s + k0 + k];
         }
+    };
+    auto store = [&]() {
+#pragma unroll
+        for (int u = 0; u < XPT; ++u) {
+            const int idx = threadIdx.x + 256 * u;
+            Xs[idx % TS][idx / TS] = rx[u];
+        }
+#pragma unroll
+        for (int u = 0; u < YPT; ++u) {
+            const int idx = threadIdx.x + 256 * u;
+            Ys[idx % KC][idx / KC] = ry[u];
+        }
+    };
+    load(0);
+    for (int k0 = 0; k0 < s; k0 += KC) {
         __syncthreads();
+        store();
+        __syncthreads();
+        if (k0 + KC < s) load(k0 + KC);
 #pragma unroll
         for (int k = 0; k < KC; ++k) {
             W xv[PT], yv[PT];
@@ -240,7 +263,6 @@ __global__ void __launch_bounds__(256) trsm_inv_double_kernel(int n, int op, int
 #pragma unroll
                 for (int c = 0; c < PT; ++c) wfma(acc[a][c], xv[a], yv[c]);
         }
-        __syncthreads();
     }
 #pragma unroll
     for (int a = 0; a < PT; ++a)
