@@ -32,6 +32,9 @@ __device__ __forceinline__ void mac(cfloat& acc, cfloat a, cfloat b)
     acc.im = fmaf(a.im, b.re, acc.im);
 }
 
+__host__ __device__ __forceinline__ bool is_zero(float v) { return v == 0.f; }
+__host__ __device__ __forceinline__ bool is_zero(cfloat v) { return v.re == 0.f && v.im == 0.f; }
+
 __device__ __forceinline__ float epilogue(float alpha, float acc, float beta, const float* c)
 {
     return beta == 0.f ? __fmul_rn(alpha, acc) : fmaf(alpha, acc, __fmul_rn(beta, *c));
@@ -51,6 +54,28 @@ __device__ __forceinline__ cfloat epilogue(cfloat alpha, cfloat acc, cfloat beta
     return r;
 }
 
+// N consecutive elements from shared memory in 16- or 8-byte vector loads
+// (the caller guarantees the alignment).
+template <class T, int N>
+__device__ __forceinline__ void lds_vec(T* dst, const T* src)
+{
+    constexpr int bytes = N * (int)sizeof(T);
+    if constexpr (bytes == 16) {
+        union { float4 v; T t[N]; } u;
+        u.v = *reinterpret_cast<const float4*>(src);
+#pragma unroll
+        for (int i = 0; i < N; ++i) dst[i] = u.t[i];
+    } else if constexpr (bytes == 8) {
+        union { float2 v; T t[N]; } u;
+        u.v = *reinterpret_cast<const float2*>(src);
+#pragma unroll
+        for (int i = 0; i < N; ++i) dst[i] = u.t[i];
+    } else {
+#pragma unroll
+        for (int i = 0; i < N; ++i) dst[i] = src[i];
+    }
+}
+
 // Threads: (BM/TM) x (BN/TN).  Each thread owns TM x TN outputs split in two
 // halves along each dimension (rows ty*TM/2 + {0..TM/2-1} and
 // BM/2 + ty*TM/2 + ...) so its shared-memory reads are conflict-free vectors.
@@ -68,8 +93,10 @@ __global__ void __launch_bounds__(Cfg<T, BM, BN, BK, TM, TN>::NT)
 {
     using CF = Cfg<T, BM, BN, BK, TM, TN>;
     constexpr int NT = CF::NT, TX = CF::TX;
-    __shared__ T As[2][BK][BM];
-    __shared__ T Bs[2][BK][BN];
+    // rows padded by 4 elements: the k-contiguous operand's stores (consecutive
+    // kk in a warp) fall in different banks, and fragment reads stay aligned
+    __shared__ __align__(16) T As[2][BK][BM + 4];
+    __shared__ __align__(16) T Bs[2][BK][BN + 4];
 
     const int tid = threadIdx.x;
     const int tx = tid % TX, ty = tid / TX;
@@ -148,16 +175,10 @@ __global__ void __launch_bounds__(Cfg<T, BM, BN, BK, TM, TN>::NT)
 #pragma unroll
         for (int kk = 0; kk < BK; ++kk) {
             T a[TM], b[TN];
-#pragma unroll
-            for (int i = 0; i < TM / 2; ++i) {
-                a[i] = As[buf][kk][ty * (TM / 2) + i];
-                a[TM / 2 + i] = As[buf][kk][BM / 2 + ty * (TM / 2) + i];
-            }
-#pragma unroll
-            for (int j = 0; j < TN / 2; ++j) {
-                b[j] = Bs[buf][kk][tx * (TN / 2) + j];
-                b[TN / 2 + j] = Bs[buf][kk][BN / 2 + tx * (TN / 2) + j];
-            }
+            lds_vec<T, TM / 2>(a, &As[buf][kk][ty * (TM / 2)]);
+            lds_vec<T, TM / 2>(a + TM / 2, &As[buf][kk][BM / 2 + ty * (TM / 2)]);
+            lds_vec<T, TN / 2>(b, &Bs[buf][kk][tx * (TN / 2)]);
+            lds_vec<T, TN / 2>(b + TN / 2, &Bs[buf][kk][BN / 2 + tx * (TN / 2)]);
 #pragma unroll
             for (int i = 0; i < TM; ++i)
 #pragma unroll
@@ -170,16 +191,24 @@ __global__ void __launch_bounds__(Cfg<T, BM, BN, BK, TM, TN>::NT)
         __syncthreads();
     }
 
+    // the row's C values are all loaded before any is stored, so the loads
+    // overlap (C is read only when beta != 0)
+    const bool read_c = !is_zero(beta);
 #pragma unroll
     for (int i = 0; i < TM; ++i) {
         const int gi = m0 + (i < TM / 2 ? ty * (TM / 2) + i : BM / 2 + ty * (TM / 2) + (i - TM / 2));
         if (gi >= m) continue;
+        T cv[TN];
+#pragma unroll
+        for (int j = 0; j < TN; ++j) {
+            const int gj = n0 + (j < TN / 2 ? tx * (TN / 2) + j : BN / 2 + tx * (TN / 2) + (j - TN / 2));
+            cv[j] = (read_c && gj < n) ? C[(long)gj * ldc + gi] : zero_v(T());
+        }
 #pragma unroll
         for (int j = 0; j < TN; ++j) {
             const int gj = n0 + (j < TN / 2 ? tx * (TN / 2) + j : BN / 2 + tx * (TN / 2) + (j - TN / 2));
             if (gj >= n) continue;
-            T* cp = C + (long)gj * ldc + gi;
-            *cp = epilogue(alpha, acc[i][j], beta, cp);
+            C[(long)gj * ldc + gi] = epilogue(alpha, acc[i][j], beta, &cv[j]);
         }
     }
 }
