@@ -231,7 +231,7 @@ cudaError_t sgemm_simt(iclblasHandle_t h, int ta, int tb, int m, int n, int k, f
 {
     const long big_tiles = (long)ceil_div(m, 128) * ceil_div(n, 128);
     if (big_tiles >= h->sm_count)
-        return launch<float, 128, 128, 8, 8, 8>(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+        return launch<float, 128, 128, 16, 8, 8>(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
     return launch<float, 64, 64, 8, 4, 4>(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
 }
 
