@@ -9,6 +9,7 @@
 // outputs back before returning, ocl_kernel.cpp:86-92), and launches the
 // routine's sm_100a kernels directly (no scored implementation selection, no
 // JIT).  Exceptions never cross the ABI, in every build type.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -109,7 +110,8 @@ public:
         return n_++;
     }
 
-    cudaError_t stage_in()
+    // Device addresses for the staged operands (grows the staging buffer).
+    cudaError_t reserve()
     {
         size_t total = 0;
         for (int i = 0; i < n_; ++i)
@@ -130,7 +132,18 @@ public:
             if (!o.staged) continue;
             o.dev = base + off;
             off += (o.bytes + 255) & ~(size_t)255;
-            cudaError_t e = cudaMemcpyAsync(o.dev, o.user, o.bytes, cudaMemcpyHostToDevice, h_->stream);
+        }
+        return cudaSuccess;
+    }
+
+    cudaError_t stage_in()
+    {
+        cudaError_t e = reserve();
+        if (e != cudaSuccess) return e;
+        for (int i = 0; i < n_; ++i) {
+            Op& o = ops_[i];
+            if (!o.staged) continue;
+            e = cudaMemcpyAsync(o.dev, o.user, o.bytes, cudaMemcpyHostToDevice, h_->stream);
             if (e != cudaSuccess) return e;
             any_staged_ = true;
         }
@@ -139,6 +152,65 @@ public:
 
     template <class T>
     T* dev(int i) const { return (T*)ops_[i].dev; }
+
+    // Elementwise calls (every operand i covers elements [0, n) with stride
+    // incs[i], element size esize): when some operand lives in host memory and
+    // the call is large, run it in chunks so that each chunk's outputs are
+    // copied back on the handle's second stream while the next chunk's inputs
+    // are copied in (H2D and D2H use separate copy engines).  `launch(c0, c1)`
+    // runs the kernel on elements [c0, c1) through dev().  Results are those
+    // of the unchunked call (elementwise arithmetic).  Returns false in `used`
+    // when the call is small or all-device (then run it the usual way).
+    template <class F>
+    cudaError_t run_chunked(long n, const int* incs, size_t esize, F&& launch, bool& used)
+    {
+        used = false;
+        bool any = false;
+        size_t total = 0;
+        for (int i = 0; i < n_; ++i) {
+            any |= ops_[i].staged;
+            total += ops_[i].bytes;
+        }
+        constexpr long kChunk = 1L << 24;  // elements per chunk
+        if (!any || total < ((size_t)64 << 20) || n < 2 * kChunk) return cudaSuccess;
+        const long nchunks = std::min<long>((n + kChunk - 1) / kChunk, iclblasContext::kMaxChunks);
+        const long per = ((n + nchunks - 1) / nchunks + 3) & ~3L;  // multiple of 4: keeps 16-byte alignment
+        cudaError_t e = reserve();
+        if (e != cudaSuccess) return e;
+        if (!h_->aux_stream) {
+            if ((e = cudaStreamCreateWithFlags(&h_->aux_stream, cudaStreamNonBlocking)) != cudaSuccess) return e;
+        }
+        for (int c = 0; c < iclblasContext::kMaxChunks; ++c)
+            if (!h_->chunk_ev[c] &&
+                (e = cudaEventCreateWithFlags(&h_->chunk_ev[c], cudaEventDisableTiming)) != cudaSuccess)
+                return e;
+        used = true;
+        int c = 0;
+        for (long c0 = 0; c0 < n; c0 += per, ++c) {
+            const long c1 = std::min(n, c0 + per);
+            for (int i = 0; i < n_; ++i) {
+                Op& o = ops_[i];
+                if (!o.staged) continue;
+                const size_t b0 = (size_t)c0 * incs[i] * esize, b1 = ((size_t)(c1 - 1) * incs[i] + 1) * esize;
+                e = cudaMemcpyAsync((char*)o.dev + b0, (const char*)o.user + b0, b1 - b0, cudaMemcpyHostToDevice,
+                                    h_->stream);
+                if (e != cudaSuccess) return e;
+            }
+            if ((e = launch(c0, c1)) != cudaSuccess) return e;
+            if ((e = cudaEventRecord(h_->chunk_ev[c], h_->stream)) != cudaSuccess) return e;
+            if ((e = cudaStreamWaitEvent(h_->aux_stream, h_->chunk_ev[c], 0)) != cudaSuccess) return e;
+            for (int i = 0; i < n_; ++i) {
+                Op& o = ops_[i];
+                if (!o.staged || !o.out) continue;
+                const size_t b0 = (size_t)c0 * incs[i] * esize, b1 = ((size_t)(c1 - 1) * incs[i] + 1) * esize;
+                e = cudaMemcpyAsync((char*)o.user + b0, (const char*)o.dev + b0, b1 - b0, cudaMemcpyDeviceToHost,
+                                    h_->aux_stream);
+                if (e != cudaSuccess) return e;
+            }
+        }
+        if ((e = cudaStreamSynchronize(h_->aux_stream)) != cudaSuccess) return e;
+        return cudaStreamSynchronize(h_->stream);
+    }
 
     // True when the call blocks (some operand lives in host memory).
     bool blocking() const { return any_staged_; }
@@ -299,6 +371,12 @@ extern "C" iclblasStatus_t iclblasDestroy(iclblasHandle_t handle)
         if (handle->ws.scratch) cudaFree(handle->ws.scratch);
         if (handle->ws.solver) cudaFree(handle->ws.solver);
         if (handle->ws.pub) cudaFree(handle->ws.pub);
+        if (handle->aux_stream) {
+            cudaStreamSynchronize(handle->aux_stream);
+            cudaStreamDestroy(handle->aux_stream);
+        }
+        for (int c = 0; c < iclblasContext::kMaxChunks; ++c)
+            if (handle->chunk_ev[c]) cudaEventDestroy(handle->chunk_ev[c]);
         cudaFree(handle->ws.counters);
         cudaFree(handle->ws.dev_status);
         cudaStreamDestroy(handle->own_stream);
@@ -372,7 +450,13 @@ extern "C" iclblasStatus_t iclblasSscal(iclblasHandle_t h, int n, const float* a
         if (!alpha) return ICLBLAS_STATUS_INVALID_VALUE;
         Stager st(h);
         int ix = st.add(x, vec_extent(n, incx) * sizeof(float), true);
-        cudaError_t e = st.stage_in();
+        const int incs[1] = {incx};
+        bool chunked = false;
+        cudaError_t e = st.run_chunked(n, incs, sizeof(float), [&](long c0, long c1) {
+            return iclb::sscal(h, (int)(c1 - c0), *alpha, st.dev<float>(ix) + c0 * incx, incx);
+        }, chunked);
+        if (chunked || e != cudaSuccess) return map_cuda(e);
+        e = st.stage_in();
         if (e == cudaSuccess) e = iclb::sscal(h, n, *alpha, st.dev<float>(ix), incx);
         if (e == cudaSuccess) e = st.finish();
         return map_cuda(e);
@@ -390,7 +474,14 @@ extern "C" iclblasStatus_t iclblasSaxpy(iclblasHandle_t h, int n, const float* a
         Stager st(h);
         int ix = st.add(x, vec_extent(n, incx) * sizeof(float), false);
         int iy = st.add(y, vec_extent(n, incy) * sizeof(float), true);
-        cudaError_t e = st.stage_in();
+        const int incs[2] = {incx, incy};
+        bool chunked = false;
+        cudaError_t e = st.run_chunked(n, incs, sizeof(float), [&](long c0, long c1) {
+            return iclb::saxpy(h, (int)(c1 - c0), *alpha, st.dev<float>(ix) + c0 * incx, incx,
+                               st.dev<float>(iy) + c0 * incy, incy);
+        }, chunked);
+        if (chunked || e != cudaSuccess) return map_cuda(e);
+        e = st.stage_in();
         if (e == cudaSuccess) e = iclb::saxpy(h, n, *alpha, st.dev<float>(ix), incx, st.dev<float>(iy), incy);
         if (e == cudaSuccess) e = st.finish();
         return map_cuda(e);
@@ -488,7 +579,13 @@ iclblasStatus_t cscal_call(iclblasHandle_t h, int n, cfloat alpha, oclComplex_t*
         VALIDATE(p, h);
         Stager st(h);
         int ix = st.add(x, vec_extent(n, incx) * sizeof(cfloat), true);
-        cudaError_t e = st.stage_in();
+        const int incs[1] = {incx};
+        bool chunked = false;
+        cudaError_t e = st.run_chunked(n, incs, sizeof(cfloat), [&](long c0, long c1) {
+            return iclb::cscal(h, (int)(c1 - c0), alpha, st.dev<cfloat>(ix) + c0 * incx, incx);
+        }, chunked);
+        if (chunked || e != cudaSuccess) return map_cuda(e);
+        e = st.stage_in();
         if (e == cudaSuccess) e = iclb::cscal(h, n, alpha, st.dev<cfloat>(ix), incx);
         if (e == cudaSuccess) e = st.finish();
         return map_cuda(e);
@@ -522,7 +619,14 @@ extern "C" iclblasStatus_t iclblasCaxpy(iclblasHandle_t h, int n, const oclCompl
         Stager st(h);
         int ix = st.add(x, vec_extent(n, incx) * sizeof(cfloat), false);
         int iy = st.add(y, vec_extent(n, incy) * sizeof(cfloat), true);
-        cudaError_t e = st.stage_in();
+        const int incs[2] = {incx, incy};
+        bool chunked = false;
+        cudaError_t e = st.run_chunked(n, incs, sizeof(cfloat), [&](long c0, long c1) {
+            return iclb::caxpy(h, (int)(c1 - c0), a, st.dev<cfloat>(ix) + c0 * incx, incx,
+                               st.dev<cfloat>(iy) + c0 * incy, incy);
+        }, chunked);
+        if (chunked || e != cudaSuccess) return map_cuda(e);
+        e = st.stage_in();
         if (e == cudaSuccess) e = iclb::caxpy(h, n, a, st.dev<cfloat>(ix), incx, st.dev<cfloat>(iy), incy);
         if (e == cudaSuccess) e = st.finish();
         return map_cuda(e);

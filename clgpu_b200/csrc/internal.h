@@ -64,6 +64,11 @@ struct iclblasContext {
     size_t stage_bytes = 0;
     // Pinned host bounce buffer for reduction results.
     void* pinned = nullptr;
+    // Second stream and per-chunk events for pipelined host-operand calls
+    // (created on first use).
+    cudaStream_t aux_stream = nullptr;
+    static constexpr int kMaxChunks = 32;
+    cudaEvent_t chunk_ev[kMaxChunks] = {};
 };
 
 namespace iclb {
