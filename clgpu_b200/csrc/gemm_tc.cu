@@ -450,6 +450,310 @@ __global__ void __launch_bounds__(THREADS, 1)
     }
 }
 
+// ---------------------------------------------------------------- 2-SM variant
+// The same GEMM on CTA pairs (cluster of 2, tcgen05 cta_group::2): the pair
+// computes a 256 x 256 output tile; each CTA holds its own 128 rows of the A
+// tile and one half (128 rows) of the B tile in shared memory, so B is
+// fetched once per pair instead of once per CTA.  The even CTA (the leader)
+// issues the MMAs (M = 256, N = 256), which read A and B from both CTAs'
+// shared memory at the same offsets and accumulate each CTA's 128 rows into
+// its own TMEM.  Both CTAs issue their own TMA loads, completing on the
+// leader's stage barrier, on which only the leader arrives (expecting both
+// CTAs' bytes); the leader's MMA commits are multicast to both CTAs' "stage
+// free" and "accumulator ready" barriers; both CTAs' epilogue warps report a
+// drained accumulator to the leader.  No load uses cluster multicast.
+namespace two_sm {
+constexpr int BN = 256;                     // pair tile columns; each CTA stores 128 rows of B
+constexpr int B_HALF = 128 * ROW_BYTES;     // 16 KiB
+constexpr int STAGE_BYTES = A_TILE + B_HALF;  // 32 KiB
+constexpr int STAGES = RING_BYTES / STAGE_BYTES;  // 6
+
+__device__ __forceinline__ uint32_t cta_rank()
+{
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+// shared::cluster address of the same variable in CTA `rank` of the cluster
+__device__ __forceinline__ uint32_t map_rank(const void* p, uint32_t rank)
+{
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(p)), "r"(rank));
+    return r;
+}
+__device__ __forceinline__ void cluster_sync()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tma_load_2d_pair(void* smem_dst, const CUtensorMap* map, int x, int y,
+                                                 uint32_t bar_cluster)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%2, %3}], [%4];"
+        ::"r"(smem_u32(smem_dst)), "l"((uint64_t)map), "r"(x), "r"(y), "r"(bar_cluster)
+        : "memory");
+}
+template <bool TF32>
+__device__ __forceinline__ void umma_pair(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate)
+{
+    if (TF32) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::2.kind::tf32 [%0], %1, %2, %3, p;\n\t}"
+            ::"r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+    } else {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+            ::"r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+    }
+}
+// arrive on the barrier at this offset in both CTAs of the pair when the
+// leader's MMAs issued so far have completed
+__device__ __forceinline__ void commit_both(uint64_t* bar)
+{
+    asm volatile(
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;"
+        ::"r"(smem_u32(bar)), "h"((uint16_t)0x3)
+        : "memory");
+}
+__device__ __forceinline__ void arrive_remote(uint32_t bar_cluster)
+{
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(bar_cluster) : "memory");
+}
+__device__ __forceinline__ void alloc_pair(uint32_t* dst, uint32_t ncols)
+{
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst)), "r"(ncols));
+}
+__device__ __forceinline__ void relinquish_pair()
+{
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+}
+__device__ __forceinline__ void dealloc_pair(uint32_t taddr, uint32_t ncols)
+{
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols));
+}
+}  // namespace two_sm
+
+template <bool TF32>
+__global__ void __launch_bounds__(THREADS, 1)
+    gemm_tc2_kernel(const __grid_constant__ CUtensorMap mA0, const __grid_constant__ CUtensorMap mA1,
+                    const __grid_constant__ CUtensorMap mA2, const __grid_constant__ CUtensorMap mB0,
+                    const __grid_constant__ CUtensorMap mB1, const __grid_constant__ CUtensorMap mB2, Params p)
+{
+    using namespace two_sm;
+    constexpr int EPI_COLS = BN / 2;  // columns per epilogue warp
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint8_t* tiles = smem;
+    uint64_t* full = (uint64_t*)(smem + RING_BYTES);
+    uint64_t* empty = full + STAGES;
+    uint64_t* tfull = empty + STAGES;
+    uint64_t* tempty = tfull + 2;
+    uint32_t* tmem_slot = (uint32_t*)(tempty + 2);
+    volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
+
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const uint32_t rank = cta_rank();
+    const bool leader = rank == 0;
+    const int pair = blockIdx.x / 2, npairs = gridDim.x / 2;
+    const int tiles_m = (p.M + 2 * BM - 1) / (2 * BM), tiles_n = (p.N + BN - 1) / BN;
+    const int ntiles = tiles_m * tiles_n;
+    const int steps = p.kblocks * p.nprod;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full[s], 1);    // the leader's producer (bytes of both CTAs)
+            mbar_init(&empty[s], 1);   // the leader's MMA commit
+        }
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(&tfull[a], 1);
+            mbar_init(&tempty[a], 2 * EPI_WARPS);  // every epilogue warp of both CTAs
+        }
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        alloc_pair(tmem_slot, 512);
+        relinquish_pair();
+    }
+    tc_fence_before();
+    cluster_sync();  // both CTAs' barriers and TMEM are set up
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+
+    if (warp == 0) {
+        // ---------------------------------------------------------- TMA producer (both CTAs)
+        if (lane == 0) {
+            const CUtensorMap* ma[3] = {&mA0, &mA1, &mA2};
+            const CUtensorMap* mb[3] = {&mB0, &mB1, &mB2};
+            int s = 0;
+            uint32_t ph = 0;
+            bool ok = true;
+            for (int t = pair; t < ntiles && ok; t += npairs) {
+                int tm, tn;
+                tile_coords(t, tiles_m, tiles_n, tm, tn);
+                for (int st = 0; st < steps && ok; ++st) {
+                    const int kb = st / p.nprod, pr = st % p.nprod;
+                    if (!mbar_wait(&empty[s], ph ^ 1, abort_flag)) { ok = false; break; }
+                    uint8_t* sa = tiles + s * STAGE_BYTES;
+                    uint8_t* sb = sa + A_TILE;
+                    if (leader) mbar_expect_tx(&full[s], 2 * STAGE_BYTES);
+                    const uint32_t bar = map_rank(&full[s], 0);
+                    const int kx = kb * (TF32 ? 32 : 64);
+                    tma_load_2d_pair(sa, ma[p.pa[pr]], kx, tm * 2 * BM + (int)rank * BM, bar);
+                    tma_load_2d_pair(sb, mb[p.pb[pr]], kx, tn * BN + (int)rank * 128, bar);
+                    if (++s == STAGES) { s = 0; ph ^= 1; }
+                }
+            }
+            if (!ok && leader) {
+                // wait (bounded) for the copies in flight to this CTA's barriers, then leave
+                for (int i = 0; i < STAGES; ++i) mbar_drain(&full[(s + i) % STAGES], ph);
+            }
+        }
+    } else if (warp == 1) {
+        // ---------------------------------------------------------- MMA issuer (leader only)
+        if (lane == 0 && leader) {
+            const uint32_t idesc = (1u << 4) | ((TF32 ? 2u : 1u) << 7) | ((TF32 ? 2u : 1u) << 10) |
+                                   ((uint32_t)(BN >> 3) << 17) | ((uint32_t)((2 * BM) >> 4) << 24);
+            int s = 0;
+            uint32_t ph = 0;
+            int acc = 0;
+            uint32_t acc_ph = 0;
+            bool ok = true;
+            const int chunk_steps = p.chunk * p.nprod;
+            for (int t = pair; t < ntiles && ok; t += npairs) {
+                for (int c0 = 0; c0 < steps && ok; c0 += chunk_steps) {
+                    if (!mbar_wait(&tempty[acc], acc_ph ^ 1, abort_flag)) { ok = false; break; }
+                    tc_fence_after();
+                    const uint32_t d = tmem_base + (uint32_t)(acc * BN);
+                    const int c1 = min(steps, c0 + chunk_steps);
+                    for (int st = c0; st < c1; ++st) {
+                        if (!mbar_wait(&full[s], ph, abort_flag)) { ok = false; break; }
+                        tc_fence_after();
+                        const uint32_t sa = smem_u32(tiles + s * STAGE_BYTES);
+                        const uint32_t sb = sa + A_TILE;
+                        const uint64_t da = smem_desc_sw128(sa), db = smem_desc_sw128(sb);
+#pragma unroll
+                        for (int kk = 0; kk < 4; ++kk)
+                            umma_pair<TF32>(d, da + (uint64_t)(2 * kk), db + (uint64_t)(2 * kk), idesc,
+                                            (st > c0 || kk > 0) ? 1u : 0u);
+                        commit_both(&empty[s]);
+                        if (++s == STAGES) { s = 0; ph ^= 1; }
+                    }
+                    commit_both(&tfull[acc]);
+                    if (!ok) {
+                        mbar_drain(&tfull[acc], acc_ph);  // every issued MMA done
+                        break;
+                    }
+                    if (++acc == 2) { acc = 0; acc_ph ^= 1; }
+                }
+            }
+        }
+    } else {
+        // ---------------------------------------------------------- epilogue (both CTAs)
+        const int ew = warp - 2;
+        const int q = warp & 3;
+        const int half = ew / 4;
+        const int nchunks = (p.kblocks + p.chunk - 1) / p.chunk;
+        const uint32_t tempty_leader[2] = {map_rank(&tempty[0], 0), map_rank(&tempty[1], 0)};
+        int acc = 0;
+        uint32_t acc_ph = 0;
+        bool ok = true;
+        for (int t = pair; t < ntiles && ok; t += npairs) {
+            int tm, tn;
+            tile_coords(t, tiles_m, tiles_n, tm, tn);
+            float sum[EPI_COLS];
+#pragma unroll
+            for (int j = 0; j < EPI_COLS; ++j) sum[j] = 0.f;
+            for (int c = 0; c < nchunks; ++c) {
+                int w = 1;
+                if (lane == 0) w = mbar_wait(&tfull[acc], acc_ph, abort_flag) ? 1 : 0;
+                ok = __shfl_sync(0xffffffffu, w, 0) != 0;
+                if (!ok) break;
+                tc_fence_after();
+                const uint32_t taddr =
+                    tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN + half * EPI_COLS);
+#pragma unroll
+                for (int g = 0; g < EPI_COLS / 32; ++g) {
+                    float v[32];
+                    tmem_ld32(taddr + (uint32_t)(g * 32), v);
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) sum[g * 32 + j] += v[j];
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) arrive_remote(tempty_leader[acc]);
+                if (++acc == 2) { acc = 0; acc_ph ^= 1; }
+            }
+            if (!ok) break;
+            const int row = tm * 2 * BM + (int)rank * BM + q * 32 + lane;
+            const int col0 = tn * BN + half * EPI_COLS;
+            const bool beta_zero = p.beta_re == 0.f && p.beta_im == 0.f;
+            if (row < p.M) {
+                if (!p.complex_out) {
+#pragma unroll
+                    for (int j0 = 0; j0 < EPI_COLS; j0 += 8) {
+                        float cv[8];
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) {
+                            const int col = col0 + j0 + j;
+                            cv[j] = (!beta_zero && col < p.N) ? p.C[(long)col * p.ldc + row] : 0.f;
+                        }
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) {
+                            const int col = col0 + j0 + j;
+                            if (col < p.N)
+                                p.C[(long)col * p.ldc + row] =
+                                    beta_zero ? __fmul_rn(p.alpha_re, sum[j0 + j])
+                                              : fmaf(p.alpha_re, sum[j0 + j], __fmul_rn(p.beta_re, cv[j]));
+                        }
+                    }
+                } else {
+                    float2* const C2 = (float2*)p.C;
+#pragma unroll
+                    for (int j0 = 0; j0 < EPI_COLS; j0 += 8) {
+                        float2 cv[4];
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) {
+                            const int col = col0 + j0 + 2 * j;
+                            cv[j] = (!beta_zero && col < p.N) ? C2[(long)(col >> 1) * p.ldc + row]
+                                                              : make_float2(0.f, 0.f);
+                        }
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) {
+                            const int col = col0 + j0 + 2 * j;
+                            if (col < p.N) {
+                                const float re = sum[j0 + 2 * j], im = sum[j0 + 2 * j + 1];
+                                float2 r;
+                                r.x = fmaf(p.alpha_re, re, -p.alpha_im * im);
+                                r.y = fmaf(p.alpha_re, im, p.alpha_im * re);
+                                if (!beta_zero) {
+                                    r.x += fmaf(p.beta_re, cv[j].x, -p.beta_im * cv[j].y);
+                                    r.y += fmaf(p.beta_re, cv[j].y, p.beta_im * cv[j].x);
+                                }
+                                C2[(long)(col >> 1) * p.ldc + row] = r;
+                            }
+                        }
+                    }
+                }
+            }
+        }
+    }
+
+    __syncthreads();
+    if (threadIdx.x == 0 && *abort_flag) atomicOr(p.status, (int)kDevWaitTimeout);
+    // the leader's MMAs write both CTAs' TMEM: free it only when both are done
+    tc_fence_before();
+    cluster_sync();
+    tc_fence_after();
+    if (warp == 1) dealloc_pair(tmem_base, 512);
+}
+
 // ---------------------------------------------------------------- split pre-pass
 // Logical operand L (R x K): L[r][k] = S[r*rs + k*ks] (conj if requested).
 // Output planes are K-major with row pitch kpad elements.
@@ -725,9 +1029,13 @@ cudaError_t gemm_tc(iclblasHandle_t h, int ta, int tb, int m, int n, int k, T al
     e = run_split<T>(h, B, n, k, bt ? 1 : ldb, bt ? ldb : 1, tb == ICLBLAS_OP_C, kCplxB, ob, rows_b);
     if (e != cudaSuccess) return e;
 
-    // 128-wide tiles when 256-wide ones would leave a quarter of the SMs idle
+    // CTA pairs (256 x 256 tiles) when there are enough pair tiles to fill the
+    // GPU; else single CTAs, with 128-wide tiles when 256-wide ones would leave
+    // a quarter of the SMs idle
+    const int pair_tiles = ceil_div(m, 2 * BM) * ceil_div((long)rows_b, 256);
+    const bool pairs = pair_tiles * 2 >= h->sm_count;
     const int tiles256 = ceil_div(m, BM) * ceil_div((long)rows_b, 256);
-    const int bn = tiles256 * 4 < h->sm_count * 3 ? 128 : 256;
+    const int bn = pairs ? 128 : (tiles256 * 4 < h->sm_count * 3 ? 128 : 256);  // B box rows
     CUtensorMap ma[3], mb[3];
     for (int l = 0; l < 3; ++l) {
         const int ll = l < mi.nlev ? l : 0;
@@ -756,6 +1064,35 @@ cudaError_t gemm_tc(iclblasHandle_t h, int ta, int tb, int m, int n, int k, T al
     p.ldc = ldc;
     p.status = h->ws.dev_status;
 
+    if (pairs) {
+        auto run2 = [&](auto kernel) -> cudaError_t {
+            cudaError_t r = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+            if (r != cudaSuccess) return r;
+            cudaLaunchConfig_t cfg = {};
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = 2;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.blockDim = dim3(THREADS);
+            cfg.dynamicSmemBytes = SMEM_BYTES;
+            cfg.stream = h->stream;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            // as many pairs as can be resident at once (persistent), at most one per tile
+            int max_clusters = 0;
+            cfg.gridDim = dim3(2 * std::max(1, h->sm_count / 2));
+            if (cudaOccupancyMaxActiveClusters(&max_clusters, kernel, &cfg) != cudaSuccess || max_clusters < 1) {
+                cudaGetLastError();
+                max_clusters = std::max(1, h->sm_count / 2);
+            }
+            cfg.gridDim = dim3(2 * std::min(pair_tiles, max_clusters));
+            r = cudaLaunchKernelEx(&cfg, kernel, ma[0], ma[1], ma[2], mb[0], mb[1], mb[2], p);
+            if (r != cudaSuccess) return r;
+            return cudaGetLastError();
+        };
+        return mi.tf32 ? run2(gemm_tc2_kernel<true>) : run2(gemm_tc2_kernel<false>);
+    }
     const int tiles = ceil_div(m, BM) * ceil_div((long)rows_b, bn);
     const int grid = std::min(tiles, h->sm_count);
     auto run = [&](auto kernel) -> cudaError_t {

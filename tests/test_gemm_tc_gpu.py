@@ -129,3 +129,35 @@ def test_cgemm_tensor_core_256_wide_tiles(handle):
     handle.set_math_mode(B.MATH_BF16X6)
     assert B.iclblasCgemm(handle, 0, 2, m, n, k, al, A, m, Bm, n, be, Cm, m) == B.SUCCESS
     assert O.rel_fro(Cm.reshape(n, m).T, ref) <= BARS[B.MATH_BF16X6]
+
+
+@pytest.mark.parametrize("mode", [B.MATH_TF32, B.MATH_BF16X3, B.MATH_BF16X6])
+@pytest.mark.parametrize("ta,tb", [(0, 0), (1, 1)])
+def test_sgemm_tensor_core_cta_pairs(handle, mode, ta, tb):
+    """Enough 256 x 256 tiles for the CTA-pair (2-SM) kernel; ragged edges."""
+    m, n, k = 2560 + 37, 2048 + 5, 200
+    rng = np.random.default_rng(900 + mode + 10 * ta)
+    ar, ac = _shape(ta, m, k)
+    br, bc = _shape(tb, k, n)
+    A = O.colmajor(ar, ac, ar + 1, rng)
+    Bm = O.colmajor(br, bc, br, rng)
+    Cm = O.colmajor(m, n, m, rng)
+    ref = _dref(ta, tb, m, n, k, 1.5, A, ar + 1, Bm, br, 0.5, Cm, m)
+    handle.set_math_mode(mode)
+    assert B.iclblasSgemm(handle, ta, tb, m, n, k, 1.5, A, ar + 1, Bm, br, 0.5, Cm, m) == B.SUCCESS
+    assert O.rel_fro(Cm, ref) <= BARS[mode]
+
+
+def test_cgemm_tensor_core_cta_pairs(handle):
+    m, n, k = 2560, 1100, 60
+    rng = np.random.default_rng(78)
+    A = O.colmajor(m, k, m, rng, np.complex64)
+    Bm = O.colmajor(k, n, k, rng, np.complex64)
+    Cm = O.colmajor(m, n, m, rng, np.complex64)
+    al, be = 1.0 - 0.5j, 0.25 + 0.25j
+    Ad = A.astype(np.complex128).reshape(k, m).T
+    Bd = Bm.astype(np.complex128).reshape(n, k).T
+    ref = al * (Ad @ Bd) + be * Cm.astype(np.complex128).reshape(n, m).T
+    handle.set_math_mode(B.MATH_BF16X3)
+    assert B.iclblasCgemm(handle, 0, 0, m, n, k, al, A, m, Bm, k, be, Cm, m) == B.SUCCESS
+    assert O.rel_fro(Cm.reshape(n, m).T, ref) <= BARS[B.MATH_BF16X3]
