@@ -36,7 +36,7 @@
 //    while the previous chunk is drained).  TF32 uses one chunk per tile.
 // Every mbarrier wait is bounded; on timeout the kernel records
 // kDevWaitTimeout, waits (bounded) for its own TMA copies, frees TMEM and
-// returns.  No cluster multicast is used.
+// returns.  Every TMA load targets the issuing CTA's own shared memory.
 #include <cuda.h>
 #include <cuda_bf16.h>
 
@@ -457,11 +457,11 @@ __global__ void __launch_bounds__(THREADS, 1)
 // fetched once per pair instead of once per CTA.  The even CTA (the leader)
 // issues the MMAs (M = 256, N = 256), which read A and B from both CTAs'
 // shared memory at the same offsets and accumulate each CTA's 128 rows into
-// its own TMEM.  Both CTAs issue their own TMA loads, completing on the
-// leader's stage barrier, on which only the leader arrives (expecting both
-// CTAs' bytes); the leader's MMA commits are multicast to both CTAs' "stage
-// free" and "accumulator ready" barriers; both CTAs' epilogue warps report a
-// drained accumulator to the leader.  No load uses cluster multicast.
+// its own TMEM.  Both CTAs issue their own TMA loads (each into its own
+// shared memory), completing on the leader's stage barrier, on which only the
+// leader arrives (expecting both CTAs' bytes); the leader's MMA commits arrive
+// on both CTAs' "stage free" and "accumulator ready" barriers; both CTAs'
+// epilogue warps report a drained accumulator to the leader.
 namespace two_sm {
 constexpr int BN = 256;                     // pair tile columns; each CTA stores 128 rows of B
 constexpr int B_HALF = 128 * ROW_BYTES;     // 16 KiB
@@ -513,13 +513,16 @@ __device__ __forceinline__ void umma_pair(uint32_t d_tmem, uint64_t adesc, uint6
     }
 }
 // arrive on the barrier at this offset in both CTAs of the pair when the
-// leader's MMAs issued so far have completed
+// leader's MMAs issued so far have completed (one commit per CTA's barrier)
+__device__ __forceinline__ void commit_to(uint32_t bar_cluster)
+{
+    asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar_cluster)
+                 : "memory");
+}
 __device__ __forceinline__ void commit_both(uint64_t* bar)
 {
-    asm volatile(
-        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;"
-        ::"r"(smem_u32(bar)), "h"((uint16_t)0x3)
-        : "memory");
+    commit_to(map_rank(bar, 0));
+    commit_to(map_rank(bar, 1));
 }
 __device__ __forceinline__ void arrive_remote(uint32_t bar_cluster)
 {

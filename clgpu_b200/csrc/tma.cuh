@@ -50,7 +50,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
         if (global_ns() - t0 > limit_ns) return false;
     return true;
 }
-// 2D tiled load (no multicast) into this CTA's shared memory; completion is
+// 2D tiled load into this CTA's own shared memory; completion is
 // counted in bytes on `bar`.
 __device__ __forceinline__ void load_2d(void* smem_dst, const CUtensorMap* map, int x, int y, uint64_t* bar)
 {
