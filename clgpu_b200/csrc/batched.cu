@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(kInvThreads) batched_inv_kernel(const int2* __
 constexpr int KC = 16;
 
 template <int RC>
-__global__ void __launch_bounds__(256) batched_trsm_kernel(int nitems, const int2* __restrict__ items,
+__global__ void __launch_bounds__(256, 4) batched_trsm_kernel(int nitems, const int2* __restrict__ items,
                                                            const int* __restrict__ dims,
                                                            const long* __restrict__ inv_off,
                                                            const float* __restrict__ inv, int lower_op, int op,
@@ -321,7 +321,7 @@ __global__ void __launch_bounds__(256) batched_trsm_kernel(int nitems, const int
 // Each item is one 64 x RC tile; K slices of 16 are double-buffered through
 // registers into shared memory (k-major), 4 x RC/16 outputs per thread.
 template <int RC, int MODE>
-__global__ void __launch_bounds__(256) batched_gemm_kernel(int nitems, const int2* __restrict__ items,
+__global__ void __launch_bounds__(256, 4) batched_gemm_kernel(int nitems, const int2* __restrict__ items,
                                                            const int* __restrict__ dims, int ta, int tb, float alpha,
                                                            float beta, const float* const* __restrict__ Aptr,
                                                            const float* const* __restrict__ Bptr,
