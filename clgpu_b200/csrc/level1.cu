@@ -151,7 +151,7 @@ __global__ void __launch_bounds__(kThreads) sreduce_kernel(long n, const float* 
     __shared__ double sh[32];
     const long stride = (long)gridDim.x * blockDim.x;
     const long tid = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    double acc = 0.0;
+    double acc = 0.0, acc2 = 0.0;
     if (VEC) {
         const float4* x4 = (const float4*)x;
         const float4* y4 = (const float4*)y;
@@ -164,14 +164,17 @@ __global__ void __launch_bounds__(kThreads) sreduce_kernel(long n, const float* 
                 a[u] = ld_stream4(x4 + i + u * stride);
                 b[u] = OP == Red::Dot ? ld_stream4(y4 + i + u * stride) : a[u];
             }
+            // two partial sums (x,y and z,w components) shorten the dependent
+            // FP64 chain; they are combined in a fixed order below
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 acc += rterm<OP>(a[u].x, b[u].x);
+                acc2 += rterm<OP>(a[u].z, b[u].z);
                 acc += rterm<OP>(a[u].y, b[u].y);
-                acc += rterm<OP>(a[u].z, b[u].z);
-                acc += rterm<OP>(a[u].w, b[u].w);
+                acc2 += rterm<OP>(a[u].w, b[u].w);
             }
         }
+        acc += acc2;
         for (; i < n4; i += stride) {
             float4 a = ld_stream4(x4 + i);
             float4 b = OP == Red::Dot ? ld_stream4(y4 + i) : a;
