@@ -166,7 +166,12 @@ __global__ void __launch_bounds__(kTThreads) gemv_t_kernel(int m, int n, T alpha
     const T* Ac = A + col * lda;
     T acc = zero_of(T());
     if (VEC) {
-        // r0 is a multiple of 32*R: every load is one aligned 128-bit vector
+        // r0 is a multiple of 32*R: every load is one aligned 128-bit vector.
+        // Real data: two partial sums (even and odd vectors of the unrolled
+        // step) halve the dependent FMA chain and are added in a fixed order
+        // after it (complex data keeps one: its four-FMA updates already
+        // interleave, and a second sum measured slower).
+        T acc2 = zero_of(T());
         int r = r0 + lane * R;
         for (; r + 3 * 32 * R + R <= r1; r += 4 * 32 * R) {
             float4 v[4], xv[4];
@@ -180,9 +185,10 @@ __global__ void __launch_bounds__(kTThreads) gemv_t_kernel(int m, int n, T alpha
                 const T* e = (const T*)&v[u];
                 const T* xe = (const T*)&xv[u];
 #pragma unroll
-                for (int k = 0; k < R; ++k) madd<CONJ>(acc, e[k], xe[k]);
+                for (int k = 0; k < R; ++k) madd<CONJ>((sizeof(T) == sizeof(float) && (u & 1)) ? acc2 : acc, e[k], xe[k]);
             }
         }
+        acc = add(acc, acc2);
         for (; r + R <= r1; r += 32 * R) {
             float4 v = ld_stream4((const float4*)(Ac + r));
             float4 xv = __ldg((const float4*)(x + r));
