@@ -1019,10 +1019,11 @@ extern "C" iclblasStatus_t iclblasStrsmBatchedPlanCreate(iclblasHandle_t h, iclb
             (uplo != ICLBLAS_FILL_MODE_UPPER && uplo != ICLBLAS_FILL_MODE_LOWER) || !op_ok(trans) ||
             (diag != ICLBLAS_DIAG_NON_UNIT && diag != ICLBLAS_DIAG_UNIT))
             return ICLBLAS_STATUS_INVALID_VALUE;
-        if (side != ICLBLAS_SIDE_LEFT) return ICLBLAS_STATUS_NOT_SUPPORTED;
+        const bool right = side == ICLBLAS_SIDE_RIGHT;
         for (int i = 0; i < batch; ++i) {
-            const int lo = m[i] > 1 ? m[i] : 1;
-            if (m[i] < 0 || n[i] < 0 || lda[i] < lo || ldb[i] < lo) return ICLBLAS_STATUS_INVALID_VALUE;
+            if (m[i] < 0 || n[i] < 0) return ICLBLAS_STATUS_INVALID_VALUE;
+            const int na = right ? n[i] : m[i];   // order of A
+            if (lda[i] < (na > 1 ? na : 1) || ldb[i] < (m[i] > 1 ? m[i] : 1)) return ICLBLAS_STATUS_INVALID_VALUE;
         }
         return map_cuda(iclb::batch_plan_create_trsm(h, side, uplo, trans, diag, batch, m, n, lda, ldb, plan));
     });

@@ -143,9 +143,12 @@ __global__ void __launch_bounds__(kInvThreads) batched_inv_kernel(const int2* __
 //        registers; 4 x RC/16 outputs per thread from float4 reads)
 //   X[block] = inv(M[block, block]) Y        (the precomputed FP32 inverse,
 //        read transposed when `inv_t`: the adjoint's transposed operator)
+// BT: the right-hand sides are the rows of B (element (row, rhs) at
+// B[row * ldb + rhs]): the right-side solve X op(A) = alpha B run as
+// op(A)^T X^T = alpha B^T.  Loads and stores then run along the rows.
 constexpr int KC = 16;
 
-template <int RC>
+template <int RC, bool BT>
 __global__ void __launch_bounds__(256, 4) batched_trsm_kernel(int nitems, const int2* __restrict__ items,
                                                            const int* __restrict__ dims,
                                                            const long* __restrict__ inv_off,
@@ -181,8 +184,9 @@ __global__ void __launch_bounds__(256, 4) batched_trsm_kernel(int nitems, const 
             const int r0 = kb * TB, nr = min(TB, m - r0);
             __syncthreads();
             for (int idx = t; idx < TB * RC; idx += 256) {
-                const int r = idx % TB, c = idx / TB;
-                Ys[r][c] = (r < nr && c < nc) ? alpha * B[(long)(c0 + c) * ldb + r0 + r] : 0.f;
+                const int r = BT ? idx / RC : idx % TB, c = BT ? idx % RC : idx / TB;
+                const long bi = BT ? (long)(r0 + r) * ldb + c0 + c : (long)(c0 + c) * ldb + r0 + r;
+                Ys[r][c] = (r < nr && c < nc) ? alpha * B[bi] : 0.f;
             }
             __syncthreads();
             float acc[4][CPT];
@@ -210,8 +214,10 @@ __global__ void __launch_bounds__(256, 4) batched_trsm_kernel(int nitems, const 
                 }
 #pragma unroll
                 for (int u = 0; u < XPT; ++u) {
-                    const int e = t + 256 * u, k = e % KC, c = e / KC;
-                    rx[u] = (c < nc && k < nk) ? B[(long)(c0 + c) * ldb + j0 + kk0 + k] : 0.f;
+                    const int e = t + 256 * u;
+                    const int k = BT ? e / RC : e % KC, c = BT ? e % RC : e / KC;
+                    const long bi = BT ? (long)(j0 + kk0 + k) * ldb + c0 + c : (long)(c0 + c) * ldb + j0 + kk0 + k;
+                    rx[u] = (c < nc && k < nk) ? B[bi] : 0.f;
                 }
             };
             auto store = [&](int buf) {
@@ -225,7 +231,8 @@ __global__ void __launch_bounds__(256, 4) batched_trsm_kernel(int nitems, const 
 #pragma unroll
                 for (int u = 0; u < XPT; ++u) {
                     const int e = t + 256 * u;
-                    Xs[buf][e % KC][e / KC] = rx[u];
+                    if (BT) Xs[buf][e / RC][e % RC] = rx[u];
+                    else Xs[buf][e % KC][e / KC] = rx[u];
                 }
             };
             if (nslices > 0) {
@@ -305,8 +312,9 @@ __global__ void __launch_bounds__(256, 4) batched_trsm_kernel(int nitems, const 
                 for (int j = 0; j < CPT; ++j) Ys[ty * 4 + i][tx * CPT + j] = out[i][j];
             __syncthreads();
             for (int idx = t; idx < TB * RC; idx += 256) {
-                const int r = idx % TB, cc = idx / TB;
-                if (r < nr && cc < nc) B[(long)(c0 + cc) * ldb + r0 + r] = Ys[r][cc];
+                const int r = BT ? idx / RC : idx % TB, cc = BT ? idx % RC : idx / TB;
+                const long bi = BT ? (long)(r0 + r) * ldb + c0 + cc : (long)(c0 + cc) * ldb + r0 + r;
+                if (r < nr && cc < nc) B[bi] = Ys[r][cc];
             }
         }
     }
@@ -558,19 +566,19 @@ cudaError_t launch_inv(iclblasHandle_t h, const int2* inv_items, int n_inv, cons
 
 // The solve, given the inverses (read transposed when inv_t).
 cudaError_t launch_trsm(iclblasHandle_t h, const BatchList& l, unsigned* counter, const long* inv_off,
-                        const float* inv, int lower_op, int op, int inv_t, float alpha, const float* const* A,
-                        float* const* B)
+                        const float* inv, int lower_op, int op, int inv_t, bool bt, float alpha,
+                        const float* const* A, float* const* B)
 {
     if (l.nitems == 0) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned), h->stream);
     if (e != cudaSuccess) return e;
     const int grid = grid_of(h, l);
-    if (l.rc == 32)
-        batched_trsm_kernel<32><<<grid, 256, 0, h->stream>>>(l.nitems, l.items, l.dims, inv_off, inv, lower_op, op,
-                                                             inv_t, alpha, A, B, counter);
-    else
-        batched_trsm_kernel<64><<<grid, 256, 0, h->stream>>>(l.nitems, l.items, l.dims, inv_off, inv, lower_op, op,
-                                                             inv_t, alpha, A, B, counter);
+    auto go = [&](auto kernel) {
+        kernel<<<grid, 256, 0, h->stream>>>(l.nitems, l.items, l.dims, inv_off, inv, lower_op, op, inv_t, alpha, A, B,
+                                            counter);
+    };
+    if (l.rc == 32) bt ? go(batched_trsm_kernel<32, true>) : go(batched_trsm_kernel<32, false>);
+    else bt ? go(batched_trsm_kernel<64, true>) : go(batched_trsm_kernel<64, false>);
     return cudaGetLastError();
 }
 
@@ -733,18 +741,18 @@ const int kCtas[] = {1, 2, 4};
 
 // Chooses (rc, ctas) for a TRSM list and fills l.items for the choice.
 cudaError_t tune_trsm(iclblasHandle_t h, int batch, const std::vector<int>& dims, int lower_op, int op, int unit,
-                      BatchList& l)
+                      bool bt, BatchList& l)
 {
     if (trsm_items(batch, dims, 64).empty()) return upload_items({}, l);   // nothing to solve
     // the key names the kernel generation so that cached choices for an older
     // kernel are not reused
-    const std::string key = tune_key(h, "trsm2", {lower_op, op, unit}, batch, dims);
+    const std::string key = tune_key(h, "trsm2", {lower_op, op, unit, bt ? 1 : 0}, batch, dims);
     Choice best{64, 1};
     if (!lookup_tune(key, best)) {
         long na = 0, nb = 0, ni = 0;
         for (int i = 0; i < batch; ++i) {
             na = std::max(na, (long)dims[4 * i + 2] * dims[4 * i]);
-            nb = std::max(nb, (long)dims[4 * i + 3] * dims[4 * i + 1]);
+            nb = std::max(nb, (long)dims[4 * i + 3] * dims[4 * i + (bt ? 0 : 1)]);
             ni = std::max(ni, (long)((dims[4 * i] + TB - 1) / TB) * TB * TB);
         }
         TuneBuffers tb;  // inverses: zeros at c for every instance
@@ -760,7 +768,7 @@ cudaError_t tune_trsm(iclblasHandle_t h, int batch, const std::vector<int>& dims
                 cand.ctas_per_sm = ctas;
                 float ms = 0;
                 e = time_launch(h, tb, [&]() {
-                    return launch_trsm(h, cand, tb.counter, tb.zoff, tb.c, lower_op, op, 0, 1.f, tb.ptrs,
+                    return launch_trsm(h, cand, tb.counter, tb.zoff, tb.c, lower_op, op, 0, bt, 1.f, tb.ptrs,
                                        const_cast<float* const*>(tb.ptrs + batch));
                 }, ms);
                 if (e != cudaSuccess) break;
@@ -867,20 +875,24 @@ cudaError_t batch_plan_create_trsm(iclblasHandle_t h, int side, int uplo, int tr
     p->diag = diag;
     p->batch = batch;
     p->device = h->device;
+    // Solve dimension `na` (the triangle) and right-hand-side count `nr` per
+    // instance: left side (m, n); right side (n, m), run on B's rows.
+    const bool right = side == ICLBLAS_SIDE_RIGHT;
     std::vector<int> dims(4 * (size_t)batch), adims(6 * (size_t)batch);
     for (int i = 0; i < batch; ++i) {
-        dims[4 * i] = m[i];
-        dims[4 * i + 1] = n[i];
+        const int na = right ? n[i] : m[i], nr = right ? m[i] : n[i];
+        dims[4 * i] = na;
+        dims[4 * i + 1] = nr;
         dims[4 * i + 2] = lda[i];
         dims[4 * i + 3] = ldb[i];
-        // adjoint product: dA (m x m, ld lda) from G and X (m x n, ld ldb), inner n
-        adims[6 * i] = m[i];
-        adims[6 * i + 1] = m[i];
-        adims[6 * i + 2] = n[i];
+        // adjoint product: dA (na x na, ld lda) from G and X (ld ldb), inner nr
+        adims[6 * i] = na;
+        adims[6 * i + 1] = na;
+        adims[6 * i + 2] = nr;
         adims[6 * i + 3] = ldb[i];
         adims[6 * i + 4] = ldb[i];
         adims[6 * i + 5] = lda[i];
-        p->flops += (double)m[i] * m[i] * n[i];
+        p->flops += (double)na * na * nr;
     }
     const int op = trans != ICLBLAS_OP_N;
     const int unit = diag == ICLBLAS_DIAG_UNIT;
@@ -890,8 +902,8 @@ cudaError_t batch_plan_create_trsm(iclblasHandle_t h, int side, int uplo, int tr
     long inv_total = 0;
     for (int i = 0; i < batch; ++i) {
         inv_off[i] = inv_total;
-        const int nblk = (m[i] + TB - 1) / TB;
-        if (n[i] > 0)
+        const int nblk = (dims[4 * i] + TB - 1) / TB;
+        if (dims[4 * i + 1] > 0)
             for (int b = 0; b < nblk; ++b) inv_items.push_back(make_int2(i, b));
         inv_total += (long)nblk * TB * TB;
     }
@@ -906,9 +918,13 @@ cudaError_t batch_plan_create_trsm(iclblasHandle_t h, int side, int uplo, int tr
         e = cudaMemcpy(p->inv_items, inv_items.data(), inv_items.size() * sizeof(int2), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = upload_dims(dims, p->main);
     if (e == cudaSuccess) e = upload_dims(adims, p->adj);
-    if (e == cudaSuccess) e = tune_trsm(h, batch, dims, lower_op_of(uplo, trans), op, unit, p->main);
+    // the right side solves op(A)^T X^T = alpha B^T: flipped operator, B's rows
+    const int s_lower = right ? !lower_op_of(uplo, trans) : lower_op_of(uplo, trans);
+    const int s_op = right ? !op : op;
+    if (e == cudaSuccess) e = tune_trsm(h, batch, dims, s_lower, s_op, unit, right, p->main);
+    // dA: left -(1/alpha) dB X^T (op N) or X dB^T; right -(1/alpha) X^T dB (op N) or dB^T X
     if (e == cudaSuccess)
-        e = tune_gemm(h, batch, adims, ICLBLAS_OP_N, ICLBLAS_OP_T, true, uplo == ICLBLAS_FILL_MODE_LOWER, unit,
+        e = tune_gemm(h, batch, adims, right ? 1 : 0, right ? 0 : 1, true, uplo == ICLBLAS_FILL_MODE_LOWER, unit,
                       p->adj);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) {
@@ -957,11 +973,14 @@ cudaError_t batch_plan_create_gemm(iclblasHandle_t h, int transa, int transb, in
 cudaError_t batch_trsm(iclblasHandle_t h, const iclblasBatchPlan* p, float alpha, const float* const* A,
                        float* const* B)
 {
-    const int lower_op = lower_op_of(p->uplo, p->trans), op = p->trans != ICLBLAS_OP_N;
+    // left: M = op(A) on B's columns; right: M = op(A)^T on B's rows
+    const bool right = p->side == ICLBLAS_SIDE_RIGHT;
+    const int lower_op = lower_op_of(p->uplo, p->trans) ^ (right ? 1 : 0);
+    const int op = (p->trans != ICLBLAS_OP_N) ^ (right ? 1 : 0);
     cudaError_t e = launch_inv(h, p->inv_items, p->n_inv, p->main.dims, p->inv_off, lower_op, op,
                                p->diag == ICLBLAS_DIAG_UNIT, A, p->inv);
     if (e != cudaSuccess) return e;
-    return launch_trsm(h, p->main, p->counter, p->inv_off, p->inv, lower_op, op, 0, alpha, A, B);
+    return launch_trsm(h, p->main, p->counter, p->inv_off, p->inv, lower_op, op, 0, right, alpha, A, B);
 }
 
 cudaError_t batch_gemm(iclblasHandle_t h, const iclblasBatchPlan* p, float alpha, const float* const* A,
@@ -979,16 +998,23 @@ cudaError_t batch_gemm(iclblasHandle_t h, const iclblasBatchPlan* p, float alpha
 cudaError_t batch_trsm_backward(iclblasHandle_t h, const iclblasBatchPlan* p, float alpha, const float* const* A,
                                 const float* const* X, float* const* G, float* const* dA)
 {
+    const bool right = p->side == ICLBLAS_SIDE_RIGHT;
     const int op = p->trans != ICLBLAS_OP_N;
     const int unit = p->diag == ICLBLAS_DIAG_UNIT;
-    const int lower_op = lower_op_of(p->uplo, p->trans);
-    // inverses of the diagonal blocks of op(A); the transposed solve reads them transposed
-    cudaError_t e = launch_inv(h, p->inv_items, p->n_inv, p->main.dims, p->inv_off, lower_op, op, unit, A, p->inv);
-    if (e == cudaSuccess) e = launch_trsm(h, p->main, p->counter, p->inv_off, p->inv, !lower_op, !op, 1, alpha, A, G);
+    // the forward's operator (right side: op(A)^T on B's rows) and its inverses;
+    // the adjoint solves with the transposed operator, reading them transposed
+    const int f_lower = lower_op_of(p->uplo, p->trans) ^ (right ? 1 : 0);
+    const int f_op = op ^ (right ? 1 : 0);
+    cudaError_t e = launch_inv(h, p->inv_items, p->n_inv, p->main.dims, p->inv_off, f_lower, f_op, unit, A, p->inv);
+    if (e == cudaSuccess)
+        e = launch_trsm(h, p->main, p->counter, p->inv_off, p->inv, !f_lower, !f_op, 1, right, alpha, A, G);
     if (e != cudaSuccess || !dA) return e;
     const float s = alpha != 0.f ? -1.f / alpha : 0.f;
     const float* const* Gc = const_cast<const float* const*>(G);
-    return launch_gemm(h, p->adj, p->counter, true, 0, 1, s, 0.f, op ? X : Gc, op ? Gc : X, dA,
+    // left: dM = -W X^T; right: dM = -X^T W; dA = dM (op N) or dM^T (op T/C)
+    const float* const* P = right ? (op ? Gc : X) : (op ? X : Gc);
+    const float* const* Q = right ? (op ? X : Gc) : (op ? Gc : X);
+    return launch_gemm(h, p->adj, p->counter, true, right ? 1 : 0, right ? 0 : 1, s, 0.f, P, Q, dA,
                        p->uplo == ICLBLAS_FILL_MODE_LOWER, unit);
 }
 

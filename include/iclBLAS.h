@@ -247,9 +247,9 @@ ICLBLAS_API iclblasStatus_t iclblasSgemm_backward(iclblasHandle_t handle, iclbla
  * during stream capture.  The calls take device arrays of `batch` device
  * pointers, one per instance; a plan serves one stream at a time.  All
  * arithmetic is FP32 FMA on the CUDA cores, whatever the math mode.
- * TRSM: left side only (a right-side plan is NOT_SUPPORTED); instance i
- * solves op(A_i) X_i = alpha B_i with A_i m_i x m_i (leading dimension
- * lda_i >= max(1, m_i)) and B_i m_i x n_i (ldb_i >= max(1, m_i)).
+ * TRSM: instance i solves op(A_i) X_i = alpha B_i (left side, A_i m_i x m_i,
+ * lda_i >= max(1, m_i)) or X_i op(A_i) = alpha B_i (right side, A_i n_i x n_i,
+ * lda_i >= max(1, n_i)); B_i is m_i x n_i with ldb_i >= max(1, m_i).
  * GEMM: C_i = alpha op(A_i) op(B_i) + beta C_i, leading dimensions at least
  * the stored row counts; each element is bit-identical to iclblasSgemm in
  * PLAIN_FP32 mode. */

@@ -203,10 +203,73 @@ def test_batched_trsm_under_cuda_graph(handle, cuda):
     plan.destroy()
 
 
+@pytest.mark.parametrize("uplo,trans,diag", [(1, 0, 0), (0, 0, 1), (1, 1, 0), (0, 2, 0)])
+def test_batched_trsm_right_side_matches_oracle(handle, cuda, uplo, trans, diag):
+    """X op(A) = alpha B, run on B's rows."""
+    handle.set_stream(torch.cuda.current_stream())
+    rng = np.random.default_rng(40 + uplo + 2 * trans + 4 * diag)
+    batch = 23
+    ms = rng.integers(1, 120, batch)      # rows of B (right-hand sides)
+    ns = rng.integers(1, 260, batch)      # order of A
+    ms[0], ns[0] = 64, 128
+    ldbs = ms + rng.integers(0, 5, batch)
+    As = [tri_np(int(n), uplo == 1, rng) for n in ns]
+    Bs = [rng.standard_normal(int(lb) * int(n)).astype(np.float32) for lb, n in zip(ldbs, ns)]
+    plan = B.BatchPlan(handle, "trsm", side=1, uplo=uplo, trans=trans, diag=diag, m=list(ms), n=list(ns),
+                       lda=list(ns), ldb=list(ldbs))
+    flops, _, _ = plan.info()
+    assert abs(flops - float(np.sum(ns.astype(float) ** 2 * ms))) < 1
+    dA = [torch.from_numpy(a).to(cuda) for a in As]
+    dB = [torch.from_numpy(b).to(cuda) for b in Bs]
+    assert B.iclblasStrsmBatchedUneven(handle, plan, 0.75, ptrs(dA, cuda), ptrs(dB, cuda)) == B.SUCCESS
+    torch.cuda.synchronize()
+    for i in range(batch):
+        ref = Bs[i].copy()
+        O.strsm(1, uplo, trans, diag, int(ms[i]), int(ns[i]), 0.75, As[i], int(ns[i]), ref, int(ldbs[i]))
+        got = dB[i].cpu().numpy()
+        assert O.rel_fro(got, ref) <= 1e-5, i
+        assert np.array_equal(got.reshape(int(ns[i]), int(ldbs[i]))[:, ms[i]:],
+                              ref.reshape(int(ns[i]), int(ldbs[i]))[:, ms[i]:])   # padding rows untouched
+    plan.destroy()
+
+
+@pytest.mark.parametrize("uplo,trans,diag,alpha", [(1, 0, 0, 1.0), (0, 1, 0, -0.5), (1, 2, 1, 2.0)])
+def test_batched_trsm_right_backward_matches_single(handle, cuda, uplo, trans, diag, alpha):
+    handle.set_stream(torch.cuda.current_stream())
+    rng = np.random.default_rng(60 + uplo + trans)
+    batch = 13
+    ms = rng.integers(1, 90, batch)
+    ns = rng.integers(1, 200, batch)
+    As = [torch.from_numpy(tri_np(int(n), uplo == 1, rng)).to(cuda) for n in ns]
+    Bs = [torch.from_numpy(rng.standard_normal(int(m) * int(n)).astype(np.float32)).to(cuda) for m, n in zip(ms, ns)]
+    Gs = [torch.from_numpy(rng.standard_normal(int(m) * int(n)).astype(np.float32)).to(cuda) for m, n in zip(ms, ns)]
+    plan = B.BatchPlan(handle, "trsm", side=1, uplo=uplo, trans=trans, diag=diag, m=list(ms), n=list(ns),
+                       lda=list(ns), ldb=list(ms))
+    Xs = [b.clone() for b in Bs]
+    assert B.iclblasStrsmBatchedUneven(handle, plan, alpha, ptrs(As, cuda), ptrs(Xs, cuda)) == B.SUCCESS
+    Gb = [g.clone() for g in Gs]
+    dAb = [torch.full((int(n) * int(n),), 3.0, device=cuda) for n in ns]
+    assert B.iclblasStrsmBatchedUnevenBackward(handle, plan, alpha, ptrs(As, cuda), ptrs(Xs, cuda), ptrs(Gb, cuda),
+                                               ptrs(dAb, cuda)) == B.SUCCESS
+    for i in range(batch):
+        m, n = int(ms[i]), int(ns[i])
+        x1 = Bs[i].clone()
+        assert B.iclblasStrsm(handle, 1, uplo, trans, diag, m, n, alpha, As[i], n, x1, m) == B.SUCCESS
+        g1 = Gs[i].clone()
+        dA1 = torch.zeros(n * n, device=cuda)
+        assert B.iclblasStrsm_backward(handle, 1, uplo, trans, diag, m, n, alpha, As[i], n, x1, m, g1, m, dA1,
+                                       n) == B.SUCCESS
+        torch.cuda.synchronize()
+        assert rel(Xs[i], x1) <= 1e-5, i
+        assert rel(Gb[i], g1) <= 1e-5, i
+        assert rel(dAb[i], dA1) <= 1e-5, i
+    plan.destroy()
+
+
 def test_batched_rejects_bad_arguments(handle, cuda):
-    with pytest.raises(B.IclblasError) as ei:
-        B.BatchPlan(handle, "trsm", side=1, uplo=1, trans=0, diag=0, m=[4], n=[4], lda=[4], ldb=[4])
-    assert ei.value.status == B.NOT_SUPPORTED
+    with pytest.raises(B.IclblasError) as ei:   # right side: lda below the order of A (n)
+        B.BatchPlan(handle, "trsm", side=1, uplo=1, trans=0, diag=0, m=[4], n=[9], lda=[8], ldb=[4])
+    assert ei.value.status == B.INVALID_VALUE
     with pytest.raises(B.IclblasError) as ei:
         B.BatchPlan(handle, "trsm", side=0, uplo=1, trans=0, diag=0, m=[8], n=[4], lda=[7], ldb=[8])
     assert ei.value.status == B.INVALID_VALUE
