@@ -566,6 +566,73 @@ def run_trsm_study(args, torch):
     return out
 
 
+def level1x_bytes(n):
+    """Algorithmic bytes per call of the copy / swap / rotation / iamin study
+    (every element of each vector read and, where written, written once)."""
+    return {
+        "scopy": 8 * n, "sswap": 16 * n, "srot": 16 * n, "srotm": 16 * n, "isamin": 4 * n,
+        "ccopy": 16 * n, "cswap": 32 * n, "csrot": 32 * n, "crot": 32 * n, "icamin": 8 * n,
+    }
+
+
+def run_level1x_study(args, torch):
+    """Copy, swap, rot, rotm and iamin (S and C) at n = --n1 (default 2^28,
+    fp32 U(-1,1), seed 2; complex n/2 so every vector is the same 1 GiB):
+    per-routine achieved HBM GB/s with device operands, CUDA events on the
+    launching stream, inputs far larger than L2.  One JSON line per routine."""
+    from clgpu_b200 import iclblas as B
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(device=dev)
+    g = torch.Generator(device=dev).manual_seed(2)
+    n = args.n1
+    nc = n // 2
+    x = torch.rand(n, generator=g, device=dev) * 2 - 1
+    y = torch.rand(n, generator=g, device=dev) * 2 - 1
+    xc, yc = x.view(torch.complex64), y.view(torch.complex64)
+    param = torch.tensor([-1.0, 0.6, -0.8, 0.8, 0.6], device=dev)
+    ri = torch.zeros(1, dtype=torch.int32, device=dev)
+    peak, peak_kind = load_peaks()
+    n_of = {k: (nc if k.startswith("c") or k == "icamin" else n) for k in level1x_bytes(n)}
+    nbytes = {k: level1x_bytes(n_of[k])[k] for k in n_of}
+    calls = [
+        ("scopy", lambda h: B.iclblasScopy(h, n, x, 1, y, 1)),
+        ("sswap", lambda h: B.iclblasSswap(h, n, x, 1, y, 1)),
+        ("srot", lambda h: B.iclblasSrot(h, n, x, 1, y, 1, 0.6, 0.8)),
+        ("srotm", lambda h: B.iclblasSrotm(h, n, x, 1, y, 1, param)),
+        ("isamin", lambda h: B.iclblasIsamin(h, n, x, 1, ri)),
+        ("ccopy", lambda h: B.iclblasCcopy(h, nc, xc, 1, yc, 1)),
+        ("cswap", lambda h: B.iclblasCswap(h, nc, xc, 1, yc, 1)),
+        ("csrot", lambda h: B.iclblasCsrot(h, nc, xc, 1, yc, 1, 0.6, 0.8)),
+        ("crot", lambda h: B.iclblasCrot(h, nc, xc, 1, yc, 1, 0.6, 0.48 + 0.64j)),
+        ("icamin", lambda h: B.iclblasIcamin(h, nc, xc, 1, ri)),
+    ]
+    only = set(args.only.split(",")) if args.only else None
+    with B.Handle() as h, torch.cuda.stream(stream):
+        h.set_stream(stream)
+        for name, f in calls:
+            if only and name not in only:
+                continue
+            for _ in range(max(3, args.warmup)):
+                B.check(f(h), name)
+            reps = max(3, min(args.steps, 50))
+            evs = []
+            torch.cuda.synchronize()
+            for _ in range(reps):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                B.check(f(h), name)
+                e1.record(stream)
+                evs.append((e0, e1))
+            torch.cuda.synchronize()
+            ms = float(np.median([a.elapsed_time(b) for a, b in evs]))
+            gbs = nbytes[name] / (ms / 1e3) / 1e9
+            print(json.dumps({"routine": name, "n": n_of[name], "ms": round(ms, 4),
+                              "gbs": round(gbs, 1), "frac_of_hbm": round(gbs / peak, 3), "peak_kind": peak_kind,
+                              "algorithmic_bytes": nbytes[name]}), flush=True)
+
+
 def run_batched_study(args, torch):
     """Batched uneven TRSM + adjoint config: 512 instances, n ~ UniformInt[32,1024],
     nrhs ~ UniformInt[1,256], L built as in the STRSM config (diagonal U(1,2),
@@ -796,9 +863,10 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-operand (C ABI) leg")
     ap.add_argument("--only", default="", help="comma-separated subset of the sweep's calls")
     ap.add_argument("--n1", type=int, default=N1, help="level-1 vector length (default 2^28)")
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "gemm", "trsm", "batched"],
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "gemm", "trsm", "batched", "level1x"],
                     help="sweep: the bandwidth config (default); gemm / trsm / batched: the precision, "
-                         "triangular-solve and batched-solve config studies")
+                         "triangular-solve and batched-solve config studies; level1x: copy / swap / "
+                         "rotation / iamin bandwidth study")
     ap.add_argument("--trsm-m", type=int, default=8192)
     ap.add_argument("--trsm-n", type=int, default=4096)
     ap.add_argument("--trsv-n", type=int, default=16384)
@@ -843,6 +911,9 @@ def main():
         return
     if args.workload == "batched":
         run_batched_study(args, torch)
+        return
+    if args.workload == "level1x":
+        run_level1x_study(args, torch)
         return
     if world > 1:
         torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))

@@ -99,12 +99,15 @@ class Stager {
 public:
     explicit Stager(iclblasHandle_t h) : h_(h) {}
 
-    int add(const void* p, size_t bytes, bool out)
+    // `in` = false: an output whose every covered byte the call overwrites
+    // (no host-to-device copy needed).
+    int add(const void* p, size_t bytes, bool out, bool in = true)
     {
         Op& o = ops_[n_];
         o.user = const_cast<void*>(p);
         o.bytes = bytes;
         o.out = out;
+        o.in = in;
         o.staged = !is_device_ptr(p);
         o.dev = o.staged ? nullptr : o.user;
         return n_++;
@@ -143,9 +146,10 @@ public:
         for (int i = 0; i < n_; ++i) {
             Op& o = ops_[i];
             if (!o.staged) continue;
+            any_staged_ = true;
+            if (!o.in) continue;
             e = cudaMemcpyAsync(o.dev, o.user, o.bytes, cudaMemcpyHostToDevice, h_->stream);
             if (e != cudaSuccess) return e;
-            any_staged_ = true;
         }
         return cudaSuccess;
     }
@@ -190,7 +194,7 @@ public:
             const long c1 = std::min(n, c0 + per);
             for (int i = 0; i < n_; ++i) {
                 Op& o = ops_[i];
-                if (!o.staged) continue;
+                if (!o.staged || !o.in) continue;
                 const size_t b0 = (size_t)c0 * incs[i] * esize, b1 = ((size_t)(c1 - 1) * incs[i] + 1) * esize;
                 e = cudaMemcpyAsync((char*)o.dev + b0, (const char*)o.user + b0, b1 - b0, cudaMemcpyHostToDevice,
                                     h_->stream);
@@ -233,7 +237,7 @@ private:
         void* user;
         void* dev;
         size_t bytes;
-        bool out, staged;
+        bool out, in, staged;
     };
     iclblasHandle_t h_;
     Op ops_[6];
@@ -442,6 +446,57 @@ extern "C" iclblasStatus_t iclblasSynchronize(iclblasHandle_t h)
 // ------------------------------------------------------------------------
 // level 1, single (iclBLAS_S.cpp:66-228)
 // ------------------------------------------------------------------------
+namespace {
+// Elementwise two-vector calls (copy, swap, rot, rotm): the reference's
+// n <= 0 no-op, then the usual x/incx/y/incy checks, host operands staged
+// (pipelined in chunks when large).  `kernel(n, x, y)` runs on device
+// pointers.  x_out: x is written; y_in: y is read (or only partly written).
+template <class T, class F>
+iclblasStatus_t pair_call(iclblasHandle_t h, int n, T* x, int incx, bool x_out, T* y, int incy, bool y_in,
+                          F&& kernel)
+{
+    if (n <= 0) return ICLBLAS_STATUS_SUCCESS;
+    return guarded([&]() -> iclblasStatus_t {
+        Params p; p.present = P_N | P_X | P_INCX | P_Y | P_INCY;
+        p.n = n; p.x = x; p.incx = incx; p.y = y; p.incy = incy;
+        VALIDATE(p, h);
+        Stager st(h);
+        int ix = st.add(x, vec_extent(n, incx) * sizeof(T), x_out);
+        int iy = st.add(y, vec_extent(n, incy) * sizeof(T), true, y_in);
+        const int incs[2] = {incx, incy};
+        bool chunked = false;
+        cudaError_t e = st.run_chunked(n, incs, sizeof(T), [&](long c0, long c1) {
+            return kernel((int)(c1 - c0), st.dev<T>(ix) + c0 * incx, st.dev<T>(iy) + c0 * incy);
+        }, chunked);
+        if (chunked || e != cudaSuccess) return map_cuda(e);
+        e = st.stage_in();
+        if (e == cudaSuccess) e = kernel(n, st.dev<T>(ix), st.dev<T>(iy));
+        if (e == cudaSuccess) e = st.finish();
+        return map_cuda(e);
+    });
+}
+
+cudaError_t iamin_dispatch(iclblasHandle_t h, int n, const float* x, int incx, int* r) { return iclb::isamin(h, n, x, incx, r); }
+cudaError_t iamin_dispatch(iclblasHandle_t h, int n, const cfloat* x, int incx, int* r) { return iclb::icamin(h, n, x, incx, r); }
+
+template <class T, class U>
+iclblasStatus_t iamin_call(iclblasHandle_t h, int n, U* x, int incx, int* result)
+{
+    return guarded([&]() -> iclblasStatus_t {
+        Params p; p.present = P_N | P_X | P_INCX; p.n = n; p.x = x; p.incx = incx;
+        VALIDATE(p, h);
+        if (!result) return ICLBLAS_STATUS_INVALID_VALUE;
+        Stager st(h);
+        int ix = st.add(x, vec_extent(n, incx) * sizeof(T), false);
+        int ir = st.add(result, sizeof(int), true, false);
+        cudaError_t e = st.stage_in();
+        if (e == cudaSuccess) e = iamin_dispatch(h, n, st.dev<T>(ix), incx, st.dev<int>(ir));
+        if (e == cudaSuccess) e = st.finish();
+        return map_cuda(e);
+    });
+}
+}  // namespace
+
 extern "C" iclblasStatus_t iclblasSscal(iclblasHandle_t h, int n, const float* alpha, float* x, int incx)
 {
     return guarded([&]() -> iclblasStatus_t {
@@ -563,6 +618,88 @@ extern "C" iclblasStatus_t iclblasIsamax(iclblasHandle_t h, int n, float* x, int
         int ir = st.add(result, sizeof(int), true);
         cudaError_t e = st.stage_in();
         if (e == cudaSuccess) e = iclb::isamax(h, n, st.dev<float>(ix), incx, st.dev<int>(ir));
+        if (e == cudaSuccess) e = st.finish();
+        return map_cuda(e);
+    });
+}
+
+extern "C" iclblasStatus_t iclblasIsamin(iclblasHandle_t h, int n, float* x, int incx, int* result)
+{
+    // iclBLAS_S.cpp:152-164
+    if (n <= 0 || incx <= 0) { zero_result(h, result, sizeof(int)); return ICLBLAS_STATUS_SUCCESS; }
+    return iamin_call<float>(h, n, x, incx, result);
+}
+
+extern "C" iclblasStatus_t iclblasScopy(iclblasHandle_t h, int n, float* x, int incx, float* y, int incy)
+{
+    // y is written without being read where it is contiguous
+    return pair_call<float>(h, n, x, incx, false, y, incy, incy != 1, [&](int nn, float* dx, float* dy) {
+        return iclb::scopy(h, nn, dx, incx, dy, incy);
+    });
+}
+
+extern "C" iclblasStatus_t iclblasSswap(iclblasHandle_t h, int n, float* x, int incx, float* y, int incy)
+{
+    return pair_call<float>(h, n, x, incx, true, y, incy, true, [&](int nn, float* dx, float* dy) {
+        return iclb::sswap(h, nn, dx, incx, dy, incy);
+    });
+}
+
+extern "C" iclblasStatus_t iclblasSrot(iclblasHandle_t h, int n, float* x, int incx, float* y, int incy, float c,
+                                       float s)
+{
+    if (n <= 0 || (c == 1.f && s == 0.f)) return ICLBLAS_STATUS_SUCCESS;  // iclBLAS_S.cpp:182-183
+    return pair_call<float>(h, n, x, incx, true, y, incy, true, [&](int nn, float* dx, float* dy) {
+        return iclb::srot(h, nn, dx, incx, dy, incy, c, s);
+    });
+}
+
+extern "C" iclblasStatus_t iclblasSrotm(iclblasHandle_t h, int n, float* x, int incx, float* y, int incy,
+                                        float* param)
+{
+    if (n <= 0) return ICLBLAS_STATUS_SUCCESS;
+    if (!param) return ICLBLAS_STATUS_INVALID_VALUE;
+    // Host parameters are read here (the reference's early return for the
+    // identity flag -2, iclBLAS_S.cpp:194-195); device parameters are read
+    // by the kernel, which skips every flag outside {-1, 0, 1}.
+    const bool dev_param = is_device_ptr(param);
+    if (!dev_param && param[0] == -2.f) return ICLBLAS_STATUS_SUCCESS;
+    return pair_call<float>(h, n, x, incx, true, y, incy, true, [&](int nn, float* dx, float* dy) {
+        return iclb::srotm(h, nn, dx, incx, dy, incy, dev_param ? nullptr : param, dev_param ? param : nullptr);
+    });
+}
+
+extern "C" iclblasStatus_t iclblasSrotg(iclblasHandle_t h, float* a, float* b, float* c, float* s)
+{
+    return guarded([&]() -> iclblasStatus_t {
+        if (!handle_ok(h) || !a || !b || !c || !s) return ICLBLAS_STATUS_INVALID_VALUE;
+        Stager st(h);
+        int ia = st.add(a, sizeof(float), true), ib = st.add(b, sizeof(float), true);
+        int ic = st.add(c, sizeof(float), true, false), is = st.add(s, sizeof(float), true, false);
+        cudaError_t e = st.stage_in();
+        if (e == cudaSuccess) e = iclb::srotg(h, st.dev<float>(ia), st.dev<float>(ib), st.dev<float>(ic), st.dev<float>(is));
+        if (e == cudaSuccess) e = st.finish();
+        return map_cuda(e);
+    });
+}
+
+extern "C" iclblasStatus_t iclblasSrotmg(iclblasHandle_t h, float* d1, float* d2, float* x1, const float* y1,
+                                         float* param)
+{
+    // The reference's host-side checks (iclBLAS_S.cpp:101-128) run inside
+    // the kernel so that device-resident operands work too.  param is
+    // staged in as well: flags 0, 1 and -2 leave some of its entries as
+    // they were.
+    return guarded([&]() -> iclblasStatus_t {
+        if (!handle_ok(h) || !d1 || !d2 || !x1 || !y1 || !param) return ICLBLAS_STATUS_INVALID_VALUE;
+        Stager st(h);
+        int i1 = st.add(d1, sizeof(float), true), i2 = st.add(d2, sizeof(float), true);
+        int ix = st.add(x1, sizeof(float), true), iy = st.add(y1, sizeof(float), false);
+        int ip = st.add(param, 5 * sizeof(float), true);
+        cudaError_t e = st.stage_in();
+        if (e == cudaSuccess)
+            e = iclb::srotmg(h, st.dev<float>(i1), st.dev<float>(i2), st.dev<float>(ix), st.dev<float>(iy),
+                             st.dev<float>(ip));
         if (e == cudaSuccess) e = st.finish();
         return map_cuda(e);
     });
@@ -709,6 +846,66 @@ extern "C" iclblasStatus_t iclblasIcamax(iclblasHandle_t h, int n, oclComplex_t*
         int ir = st.add(result, sizeof(int), true);
         cudaError_t e = st.stage_in();
         if (e == cudaSuccess) e = iclb::icamax(h, n, st.dev<cfloat>(ix), incx, st.dev<int>(ir));
+        if (e == cudaSuccess) e = st.finish();
+        return map_cuda(e);
+    });
+}
+
+extern "C" iclblasStatus_t iclblasIcamin(iclblasHandle_t h, int n, oclComplex_t* x, int incx, int* result)
+{
+    // iclBLAS_C.cpp:153-165
+    if (n <= 0 || incx <= 0) { zero_result(h, result, sizeof(int)); return ICLBLAS_STATUS_SUCCESS; }
+    return iamin_call<cfloat>(h, n, x, incx, result);
+}
+
+extern "C" iclblasStatus_t iclblasCcopy(iclblasHandle_t h, int n, oclComplex_t* x, int incx, oclComplex_t* y,
+                                        int incy)
+{
+    return pair_call<cfloat>(h, n, (cfloat*)x, incx, false, (cfloat*)y, incy, incy != 1,
+                             [&](int nn, cfloat* dx, cfloat* dy) { return iclb::ccopy(h, nn, dx, incx, dy, incy); });
+}
+
+extern "C" iclblasStatus_t iclblasCswap(iclblasHandle_t h, int n, oclComplex_t* x, int incx, oclComplex_t* y,
+                                        int incy)
+{
+    return pair_call<cfloat>(h, n, (cfloat*)x, incx, true, (cfloat*)y, incy, true,
+                             [&](int nn, cfloat* dx, cfloat* dy) { return iclb::cswap(h, nn, dx, incx, dy, incy); });
+}
+
+extern "C" iclblasStatus_t iclblasCrot(iclblasHandle_t h, int n, oclComplex_t* x, int incx, oclComplex_t* y, int incy,
+                                       const float* c, const oclComplex_t* s)
+{
+    if (n <= 0) return ICLBLAS_STATUS_SUCCESS;
+    if (!c || !s) return ICLBLAS_STATUS_INVALID_VALUE;
+    const float cv = *c;
+    const cfloat sv = cf(s);
+    if (cv == 1.f && sv.re == 0.f && sv.im == 0.f) return ICLBLAS_STATUS_SUCCESS;  // iclBLAS_C.cpp:313-314
+    return pair_call<cfloat>(h, n, (cfloat*)x, incx, true, (cfloat*)y, incy, true,
+                             [&](int nn, cfloat* dx, cfloat* dy) { return iclb::crot(h, nn, dx, incx, dy, incy, cv, sv); });
+}
+
+extern "C" iclblasStatus_t iclblasCsrot(iclblasHandle_t h, int n, oclComplex_t* x, int incx, oclComplex_t* y,
+                                        int incy, const float* c, const float* s)
+{
+    if (n <= 0) return ICLBLAS_STATUS_SUCCESS;
+    if (!c || !s) return ICLBLAS_STATUS_INVALID_VALUE;
+    const float cv = *c, sv = *s;
+    if (cv == 1.f && sv == 0.f) return ICLBLAS_STATUS_SUCCESS;  // iclBLAS_C.cpp:326-327
+    return pair_call<cfloat>(h, n, (cfloat*)x, incx, true, (cfloat*)y, incy, true,
+                             [&](int nn, cfloat* dx, cfloat* dy) { return iclb::csrot(h, nn, dx, incx, dy, incy, cv, sv); });
+}
+
+extern "C" iclblasStatus_t iclblasCrotg(iclblasHandle_t h, oclComplex_t* a, oclComplex_t* b, float* c,
+                                        oclComplex_t* s)
+{
+    return guarded([&]() -> iclblasStatus_t {
+        if (!handle_ok(h) || !a || !b || !c || !s) return ICLBLAS_STATUS_INVALID_VALUE;
+        Stager st(h);
+        int ia = st.add(a, sizeof(cfloat), true), ib = st.add(b, sizeof(cfloat), false);
+        int ic = st.add(c, sizeof(float), true, false), is = st.add(s, sizeof(cfloat), true, false);
+        cudaError_t e = st.stage_in();
+        if (e == cudaSuccess)
+            e = iclb::crotg(h, st.dev<cfloat>(ia), st.dev<cfloat>(ib), st.dev<float>(ic), st.dev<cfloat>(is));
         if (e == cudaSuccess) e = st.finish();
         return map_cuda(e);
     });

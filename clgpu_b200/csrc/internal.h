@@ -100,6 +100,24 @@ constexpr int kSdotNoAllocMaxBlocks = 4096;
 cudaError_t sdot_noalloc(iclblasHandle_t h, int n, const float* x, int incx, const float* y, int incy,
                          float* result);
 cudaError_t icamax(iclblasHandle_t h, int n, const cfloat* x, int incx, int* result);
+cudaError_t isamin(iclblasHandle_t h, int n, const float* x, int incx, int* result);
+cudaError_t icamin(iclblasHandle_t h, int n, const cfloat* x, int incx, int* result);
+
+// copy, swap, plane rotations and their generators (level1_rot.cu)
+cudaError_t scopy(iclblasHandle_t h, int n, const float* x, int incx, float* y, int incy);
+cudaError_t ccopy(iclblasHandle_t h, int n, const cfloat* x, int incx, cfloat* y, int incy);
+cudaError_t sswap(iclblasHandle_t h, int n, float* x, int incx, float* y, int incy);
+cudaError_t cswap(iclblasHandle_t h, int n, cfloat* x, int incx, cfloat* y, int incy);
+cudaError_t srot(iclblasHandle_t h, int n, float* x, int incx, float* y, int incy, float c, float s);
+cudaError_t csrot(iclblasHandle_t h, int n, cfloat* x, int incx, cfloat* y, int incy, float c, float s);
+cudaError_t crot(iclblasHandle_t h, int n, cfloat* x, int incx, cfloat* y, int incy, float c, cfloat s);
+// Exactly one of host_param (read now) and dev_param (read by the kernel) is set.
+cudaError_t srotm(iclblasHandle_t h, int n, float* x, int incx, float* y, int incy, const float* host_param,
+                  const float* dev_param);
+// Generators: every pointer is device memory.
+cudaError_t srotg(iclblasHandle_t h, float* a, float* b, float* c, float* s);
+cudaError_t crotg(iclblasHandle_t h, cfloat* a, cfloat* b, float* c, cfloat* s);
+cudaError_t srotmg(iclblasHandle_t h, float* d1, float* d2, float* x1, const float* y1, float* param);
 
 // ---------------------------------------------------------------- level 2
 cudaError_t sgemv(iclblasHandle_t h, int trans, int m, int n, float alpha, const float* A, int lda,

@@ -1,4 +1,4 @@
-// Level-1 kernels: axpy, scal, dot, nrm2, asum, iamax (single and complex).
+// Level-1 kernels: axpy, scal, dot, nrm2, asum, iamax, iamin (single and complex).
 //
 // All of them stream their vectors once from HBM.  Unit-stride vectors whose
 // base addresses are 16-byte aligned take 128-bit loads/stores; other
@@ -322,12 +322,14 @@ __global__ void __launch_bounds__(kThreads) cdot_kernel(long n, const cfloat* __
 }
 
 // ---------------------------------------------------------------- iamax
-// Candidate (value, index) pairs are ordered by value, then by smaller index;
-// NaN never enters (comparisons with NaN are false), the start value -1 is
-// below every |x|.  The reduction of that total order gives the first index
-// of the maximum over non-NaN elements, which is what the reference's scan
-// (strict '>' from x[0]) returns unless x[0] itself is NaN; that case pins
-// the scan to 0 and is applied at the end.
+// Candidate (value, index) pairs are ordered by key, then by smaller index;
+// NaN never enters (comparisons with NaN are false) and the start key -inf is
+// below every other key.  iamax keys are |x|, iamin keys are -|x|.  The
+// reduction of that total order gives the first index of the extreme key over
+// non-NaN elements, which is what the reference's scans (strict '>' or '<'
+// from x[0]) return unless x[0] itself is NaN; that case pins the scan to 0
+// and is applied at the end, as is an iamin input made only of infinities
+// (no candidate: the scan stays at 0).
 struct Cand {
     float v;
     int i;
@@ -358,7 +360,7 @@ __device__ __forceinline__ Cand block_cand(Cand c, Cand* sh)
     __syncthreads();
     if (lane == 0) sh[wid] = c;
     __syncthreads();
-    Cand r{-1.0f, INT_MAX};
+    Cand r{-INFINITY, INT_MAX};
     if (wid == 0) {
         if (lane < nw) r = sh[lane];
         r = warp_cand(r);
@@ -372,7 +374,13 @@ __device__ __forceinline__ float absval(cfloat v) { return fabsf(v.re) + fabsf(v
 __device__ __forceinline__ bool isnan_v(float v) { return isnan(v); }
 __device__ __forceinline__ bool isnan_v(cfloat v) { return isnan(fabsf(v.re) + fabsf(v.im)); }
 
-template <class T, bool VEC>
+template <bool MIN, class T>
+__device__ __forceinline__ float iakey(T v)
+{
+    return MIN ? -absval(v) : absval(v);
+}
+
+template <class T, bool VEC, bool MIN = false>
 __global__ void __launch_bounds__(kThreads) iamax_kernel(long n, const T* __restrict__ x, long incx,
                                                          Cand* __restrict__ partials, unsigned* counter,
                                                          int* __restrict__ result)
@@ -380,7 +388,7 @@ __global__ void __launch_bounds__(kThreads) iamax_kernel(long n, const T* __rest
     __shared__ Cand sh[32];
     const long stride = (long)gridDim.x * blockDim.x;
     const long tid = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    Cand c{-1.0f, INT_MAX};
+    Cand c{-INFINITY, INT_MAX};
     constexpr int per = (int)(16 / sizeof(T));  // elements per 128-bit load
     if (VEC) {
         const float4* x4 = (const float4*)x;
@@ -395,24 +403,24 @@ __global__ void __launch_bounds__(kThreads) iamax_kernel(long n, const T* __rest
                 const T* e = (const T*)&a[u];
                 const int base = (int)((i + u * stride) * per);
 #pragma unroll
-                for (int k = 0; k < per; ++k) cand_take(c, absval(e[k]), base + k);
+                for (int k = 0; k < per; ++k) cand_take(c, iakey<MIN>(e[k]), base + k);
             }
         }
         for (; i < nv; i += stride) {
             float4 a = ld_stream4(x4 + i);
             const T* e = (const T*)&a;
 #pragma unroll
-            for (int k = 0; k < per; ++k) cand_take(c, absval(e[k]), (int)(i * per + k));
+            for (int k = 0; k < per; ++k) cand_take(c, iakey<MIN>(e[k]), (int)(i * per + k));
         }
         if (tid == 0)
-            for (long j = nv * per; j < n; ++j) cand_take(c, absval(x[j]), (int)j);
+            for (long j = nv * per; j < n; ++j) cand_take(c, iakey<MIN>(x[j]), (int)j);
     } else {
-        for (long i = tid; i < n; i += stride) cand_take(c, absval(x[i * incx]), (int)i);
+        for (long i = tid; i < n; i += stride) cand_take(c, iakey<MIN>(x[i * incx]), (int)i);
     }
     Cand b = block_cand(c, sh);
     if (threadIdx.x == 0) partials[blockIdx.x] = b;
     if (!last_block(counter)) return;
-    Cand r{-1.0f, INT_MAX};
+    Cand r{-INFINITY, INT_MAX};
     for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
         Cand o;
         o.v = ((volatile float*)&partials[i].v)[0];
@@ -585,26 +593,39 @@ cudaError_t cdot(iclblasHandle_t h, bool conj, int n, const cfloat* x, int incx,
     return cudaGetLastError();
 }
 
-cudaError_t isamax(iclblasHandle_t h, int n, const float* x, int incx, int* result)
+namespace {
+template <class T, bool MIN>
+cudaError_t iamax_impl(iclblasHandle_t h, int n, const T* x, int incx, int* result)
 {
     const bool vec = incx == 1 && aligned16(x);
-    const int grid = l1_grid(h, vec ? ((long)n + 3) / 4 : n);
+    const int grid = l1_grid(h, vec ? ((long)n + (16 / sizeof(T)) - 1) / (16 / sizeof(T)) : n);
     Cand* partials = (Cand*)scratch(h, sizeof(Cand) * (size_t)grid);
     if (!partials) return cudaErrorMemoryAllocation;
-    if (vec) iamax_kernel<float, true><<<grid, kThreads, 0, h->stream>>>(n, x, incx, partials, h->ws.counters, result);
-    else iamax_kernel<float, false><<<grid, kThreads, 0, h->stream>>>(n, x, incx, partials, h->ws.counters, result);
+    if (vec)
+        iamax_kernel<T, true, MIN><<<grid, kThreads, 0, h->stream>>>(n, x, incx, partials, h->ws.counters, result);
+    else
+        iamax_kernel<T, false, MIN><<<grid, kThreads, 0, h->stream>>>(n, x, incx, partials, h->ws.counters, result);
     return cudaGetLastError();
 }
+}  // namespace
 
+cudaError_t isamax(iclblasHandle_t h, int n, const float* x, int incx, int* result)
+{
+    return iamax_impl<float, false>(h, n, x, incx, result);
+}
 cudaError_t icamax(iclblasHandle_t h, int n, const cfloat* x, int incx, int* result)
 {
-    const bool vec = incx == 1 && aligned16(x);
-    const int grid = l1_grid(h, vec ? ((long)n + 1) / 2 : n);
-    Cand* partials = (Cand*)scratch(h, sizeof(Cand) * (size_t)grid);
-    if (!partials) return cudaErrorMemoryAllocation;
-    if (vec) iamax_kernel<cfloat, true><<<grid, kThreads, 0, h->stream>>>(n, x, incx, partials, h->ws.counters, result);
-    else iamax_kernel<cfloat, false><<<grid, kThreads, 0, h->stream>>>(n, x, incx, partials, h->ws.counters, result);
-    return cudaGetLastError();
+    return iamax_impl<cfloat, false>(h, n, x, incx, result);
+}
+// first index of the smallest |x| (scabs1 for complex): the reference's
+// Isamin_naive.cl / Icamin_naive.cl scan (strict '<' from x[0])
+cudaError_t isamin(iclblasHandle_t h, int n, const float* x, int incx, int* result)
+{
+    return iamax_impl<float, true>(h, n, x, incx, result);
+}
+cudaError_t icamin(iclblasHandle_t h, int n, const cfloat* x, int incx, int* result)
+{
+    return iamax_impl<cfloat, true>(h, n, x, incx, result);
 }
 
 }  // namespace iclb

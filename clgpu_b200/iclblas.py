@@ -87,6 +87,19 @@ _SIGS = {
     "iclblasIcamax": [_H, _I, _P, _I, _P],
     "iclblasCaxpy": [_H, _I, _P, _P, _I, _P, _I],
     "iclblasScasum": [_H, _I, _P, _I, _P],
+    "iclblasIsamin": [_H, _I, _P, _I, _P],
+    "iclblasScopy": [_H, _I, _P, _I, _P, _I],
+    "iclblasSswap": [_H, _I, _P, _I, _P, _I],
+    "iclblasSrot": [_H, _I, _P, _I, _P, _I, C.c_float, C.c_float],
+    "iclblasSrotm": [_H, _I, _P, _I, _P, _I, _P],
+    "iclblasSrotg": [_H, _P, _P, _P, _P],
+    "iclblasSrotmg": [_H, _P, _P, _P, _P, _P],
+    "iclblasIcamin": [_H, _I, _P, _I, _P],
+    "iclblasCcopy": [_H, _I, _P, _I, _P, _I],
+    "iclblasCswap": [_H, _I, _P, _I, _P, _I],
+    "iclblasCrot": [_H, _I, _P, _I, _P, _I, _P, _P],
+    "iclblasCsrot": [_H, _I, _P, _I, _P, _I, _P, _P],
+    "iclblasCrotg": [_H, _P, _P, _P, _P],
     "iclblasStrsv": [_H, _I, _I, _I, _I, _P, _I, _P, _I],
     "iclblasCtrsv": [_H, _I, _I, _I, _I, _P, _I, _P, _I],
     "iclblasSgemv": [_H, _I, _I, _I, _P, _P, _I, _P, _I, _P, _P, _I],
@@ -272,6 +285,62 @@ def iclblasCaxpy(h, n, alpha, x, incx, y, incy):
 
 def iclblasScasum(h, n, x, incx, result):
     return _call("iclblasScasum", _h(h), n, ptr(x), incx, ptr(result))
+
+
+def iclblasIsamin(h, n, x, incx, result):
+    return _call("iclblasIsamin", _h(h), n, ptr(x), incx, ptr(result))
+
+
+def iclblasScopy(h, n, x, incx, y, incy):
+    return _call("iclblasScopy", _h(h), n, ptr(x), incx, ptr(y), incy)
+
+
+def iclblasSswap(h, n, x, incx, y, incy):
+    return _call("iclblasSswap", _h(h), n, ptr(x), incx, ptr(y), incy)
+
+
+def iclblasSrot(h, n, x, incx, y, incy, c, s):
+    return _call("iclblasSrot", _h(h), n, ptr(x), incx, ptr(y), incy, float(c), float(s))
+
+
+def iclblasSrotm(h, n, x, incx, y, incy, param):
+    """param: 5 floats {flag, p1, p2, p3, p4}, host array or device tensor."""
+    return _call("iclblasSrotm", _h(h), n, ptr(x), incx, ptr(y), incy, ptr(param))
+
+
+def iclblasSrotg(h, a, b, c, s):
+    """a, b, c, s: one-element float arrays (host or device), updated in place."""
+    return _call("iclblasSrotg", _h(h), ptr(a), ptr(b), ptr(c), ptr(s))
+
+
+def iclblasSrotmg(h, d1, d2, x1, y1, param):
+    return _call("iclblasSrotmg", _h(h), ptr(d1), ptr(d2), ptr(x1), ptr(y1), ptr(param))
+
+
+def iclblasIcamin(h, n, x, incx, result):
+    return _call("iclblasIcamin", _h(h), n, ptr(x), incx, ptr(result))
+
+
+def iclblasCcopy(h, n, x, incx, y, incy):
+    return _call("iclblasCcopy", _h(h), n, ptr(x), incx, ptr(y), incy)
+
+
+def iclblasCswap(h, n, x, incx, y, incy):
+    return _call("iclblasCswap", _h(h), n, ptr(x), incx, ptr(y), incy)
+
+
+def iclblasCrot(h, n, x, incx, y, incy, c, s):
+    """c: real scalar, s: complex scalar (both passed by host pointer)."""
+    return _call("iclblasCrot", _h(h), n, ptr(x), incx, ptr(y), incy, C.byref(_fscalar(c)), C.byref(_cscalar(s)))
+
+
+def iclblasCsrot(h, n, x, incx, y, incy, c, s):
+    return _call("iclblasCsrot", _h(h), n, ptr(x), incx, ptr(y), incy, C.byref(_fscalar(c)), C.byref(_fscalar(s)))
+
+
+def iclblasCrotg(h, a, b, c, s):
+    """a, b, s: one-element complex64 arrays; c: one-element float array."""
+    return _call("iclblasCrotg", _h(h), ptr(a), ptr(b), ptr(c), ptr(s))
 
 
 def iclblasStrsv(h, uplo, trans, diag, n, A, lda, x, incx):

@@ -130,6 +130,34 @@ ICLBLAS_API iclblasStatus_t iclblasSdot(iclblasHandle_t handle, int n, float* x,
 ICLBLAS_API iclblasStatus_t iclblasSdotNoAlloc(iclblasHandle_t handle, int n, const float* x, int incx, const float* y,
                                                int incy, float* result);
 
+/* ---- level 1, single: copy, swap, rotations, iamin ----
+ * Vector arguments follow the same host/device rule as above.  Srot's c and
+ * s are passed by value; Srotm's param may be a host pointer (read at call
+ * time; flag -2 returns at once) or a device pointer (read by the kernel,
+ * which leaves x and y unchanged for any flag outside {-1, 0, 1}).  param
+ * uses the reference's layout {flag, p1, p2, p3, p4} with
+ *   flag -1: x' = p1 x + p2 y, y' = p3 x + p4 y
+ *   flag  0: x' = x + p2 y,    y' = p3 x + y
+ *   flag  1: x' = p1 x + y,    y' = p4 y - x
+ * (libs/blas/funcs/Srotm/Srotm_helpers.h.cl).  The generators (Srotg,
+ * Srotmg, Crotg) accept all-host or all-device operands and reproduce the
+ * reference kernels' formulas, including Srotg's zero result when a or b is
+ * 0 and Srotmg's partial writes of param for flags 0, 1 and -2. */
+/* replaces iclBLAS.h:203 */
+ICLBLAS_API iclblasStatus_t iclblasScopy(iclblasHandle_t handle, int n, float* x, int incx, float* y, int incy);
+/* replaces iclBLAS.h:262 */
+ICLBLAS_API iclblasStatus_t iclblasSrotmg(iclblasHandle_t handle, float* d1, float* d2, float* x1, const float* y1, float* params);
+/* replaces iclBLAS.h:288 (0-based index of the first smallest |x_i|) */
+ICLBLAS_API iclblasStatus_t iclblasIsamin(iclblasHandle_t handle, int n, float* x, int incx, int* result);
+/* replaces iclBLAS.h:305 */
+ICLBLAS_API iclblasStatus_t iclblasSswap(iclblasHandle_t handle, int n, float* x, int incx, float* y, int incy);
+/* replaces iclBLAS.h:319 */
+ICLBLAS_API iclblasStatus_t iclblasSrot(iclblasHandle_t handle, int n, float* x, int incx, float* y, int incy, float c, float s);
+/* replaces iclBLAS.h:332 */
+ICLBLAS_API iclblasStatus_t iclblasSrotm(iclblasHandle_t handle, int n, float* x, int incx, float* y, int incy, float* param);
+/* replaces iclBLAS.h:356 */
+ICLBLAS_API iclblasStatus_t iclblasSrotg(iclblasHandle_t handle, float* a, float* b, float* c, float* s);
+
 /* ---- level 1, complex ---- */
 /* replaces iclBLAS.h:411 */
 ICLBLAS_API iclblasStatus_t iclblasCscal(iclblasHandle_t handle, int n, const oclComplex_t* alpha, oclComplex_t* x, int incx);
@@ -147,6 +175,23 @@ ICLBLAS_API iclblasStatus_t iclblasCaxpy(iclblasHandle_t handle, int n, const oc
 ICLBLAS_API iclblasStatus_t iclblasCdotc(iclblasHandle_t handle, int n, oclComplex_t* x, int incx, oclComplex_t* y, int incy, oclComplex_t* result);
 /* replaces iclBLAS.h:590 */
 ICLBLAS_API iclblasStatus_t iclblasScasum(iclblasHandle_t handle, int n, oclComplex_t* x, int incx, float* result);
+
+/* ---- level 1, complex: copy, swap, rotations, iamin ----
+ * Crot and Csrot read c and s through host pointers at call time. */
+/* replaces iclBLAS.h:395 */
+ICLBLAS_API iclblasStatus_t iclblasCcopy(iclblasHandle_t handle, int n, oclComplex_t* x, int incx, oclComplex_t* y, int incy);
+/* replaces iclBLAS.h:444 */
+ICLBLAS_API iclblasStatus_t iclblasCswap(iclblasHandle_t handle, int n, oclComplex_t* x, int incx, oclComplex_t* y, int incy);
+/* replaces iclBLAS.h:501 (0-based index of the first smallest |re| + |im|) */
+ICLBLAS_API iclblasStatus_t iclblasIcamin(iclblasHandle_t handle, int n, oclComplex_t* x, int incx, int* result);
+/* replaces iclBLAS.h:530 */
+ICLBLAS_API iclblasStatus_t iclblasCrotg(iclblasHandle_t handle, oclComplex_t* a, oclComplex_t* b, float* c, oclComplex_t* s);
+/* replaces iclBLAS.h:563 */
+ICLBLAS_API iclblasStatus_t iclblasCrot(iclblasHandle_t handle, int n, oclComplex_t* x, int incx, oclComplex_t* y, int incy,
+                                        const float* c, const oclComplex_t* s);
+/* replaces iclBLAS.h:577 */
+ICLBLAS_API iclblasStatus_t iclblasCsrot(iclblasHandle_t handle, int n, oclComplex_t* x, int incx, oclComplex_t* y, int incy,
+                                         const float* c, const float* s);
 
 /* ---- level 2 ---- */
 /* replaces iclBLAS.h:630 */

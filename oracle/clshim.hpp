@@ -7,7 +7,9 @@
 // OpenCL's scalar broadcast, and the complex helpers that the reference
 // prepends to every program (core/src/ocl/complex.h.cl:28-72).  The helpers
 // are restated here because the OpenCL vector literal "(complex_t)(a, b)" in
-// that file has a different meaning in C++.
+// that file has a different meaning in C++ (a comma expression: it yields
+// (b, b)); kernels that write such a literal themselves are only compared on
+// inputs that do not reach it.
 #pragma once
 #include <cmath>
 #include <cstdint>
@@ -59,6 +61,17 @@ inline complex_t cdiv(complex_t a, complex_t b)
 inline complex_t conjg(complex_t a) { return complex_t(a.x, -a.y); }
 // complex.h.cl:54
 inline float scabs1(complex_t a) { return std::fabs(a.x) + std::fabs(a.y); }
+// complex.h.cl:28 -- modulus with one fused multiply-add
+inline float cabs(complex_t a) { return std::sqrt(std::fma(a.x, a.x, a.y * a.y)); }
+// complex.h.cl:41-47, 62-68 -- scalar broadcasts and negation
+inline complex_t cmulf(complex_t a, float b) { return a * float2(b); }
+inline complex_t cdivf(complex_t a, float b) { return a / float2(b); }
+inline complex_t cneg(complex_t a) { return -a; }
+// OpenCL's componentwise fma on float2; cfmaf broadcasts b (complex.h.cl:66)
+inline float2 fma(float2 a, float2 b, float2 c) { return float2(std::fma(a.x, b.x, c.x), std::fma(a.y, b.y, c.y)); }
+inline complex_t cfmaf(complex_t a, float b, complex_t c) { return fma(a, float2(b), c); }
+// OpenCL sign(): 1, -1, or 0 for zero and NaN
+inline float sign(float v) { return v > 0.f ? 1.f : (v < 0.f ? -1.f : 0.f); }
 
 namespace clshim {
 // Runs a 1-D NDRange of `gws` work-items sequentially.

@@ -196,6 +196,255 @@ int orc_icamax(int n, const orc_c32* x, int incx)
 }
 
 /* ------------------------------------------------------------------------ */
+/* Level 1: iamin, copy, swap, plane rotations and their generators         */
+/* ------------------------------------------------------------------------ */
+/* These restate the reference's OpenCL kernels expression by expression in
+ * FP32 (this file is compiled with -ffp-contract=off: a product is rounded
+ * before it is added unless the kernel writes fma/mad, restated as fmaf). */
+
+/* First index of the smallest |x_i|: Isamin_naive.cl:16-33 (strict '<'
+ * scan from x[0]). */
+int orc_isamin(int n, const float* x, int incx)
+{
+    if (n < 1 || incx < 1) return 0;
+    float best = fabsf(x[0]);
+    int idx = 0;
+    for (int i = 1; i < n; ++i) {
+        float v = fabsf(x[(long)i * incx]);
+        if (v < best) { best = v; idx = i; }
+    }
+    return idx;
+}
+
+/* Icamin_naive.cl:22-44, key scabs1 = |re| + |im|. */
+int orc_icamin(int n, const orc_c32* x, int incx)
+{
+    if (n < 1 || incx < 1) return 0;
+    float best = fabsf(x[0].re) + fabsf(x[0].im);
+    int idx = 0;
+    for (int i = 1; i < n; ++i) {
+        const orc_c32 v = x[(long)i * incx];
+        float a = fabsf(v.re) + fabsf(v.im);
+        if (a < best) { best = a; idx = i; }
+    }
+    return idx;
+}
+
+/* y_i = x_i for elements of esize bytes: copy_interleave_naive.cl:16-23. */
+void orc_copy(int n, const void* x, int incx, void* y, int incy, int esize)
+{
+    for (long i = 0; i < n; ++i)
+        memcpy((char*)y + i * incy * esize, (const char*)x + i * incx * esize, (size_t)esize);
+}
+
+/* x_i <-> y_i: swap_interleave_naive.cl:16-26. */
+void orc_swap(int n, void* x, int incx, void* y, int incy, int esize)
+{
+    char t[16];
+    for (long i = 0; i < n; ++i) {
+        char* a = (char*)x + i * incx * esize;
+        char* b = (char*)y + i * incy * esize;
+        memcpy(t, a, (size_t)esize);
+        memcpy(a, b, (size_t)esize);
+        memcpy(b, t, (size_t)esize);
+    }
+}
+
+/* Srot_naive.cl:16-35: sy = s*y, cy = c*y, x' = fma(c, x, sy),
+ * y' = fma(-s, x, cy). */
+static void rot1(float* x, float* y, float c, float s)
+{
+    const float sy = s * *y, cy = c * *y;
+    const float nx = fmaf(c, *x, sy);
+    *y = fmaf(-s, *x, cy);
+    *x = nx;
+}
+
+void orc_srot(int n, float* x, int incx, float* y, int incy, float c, float s)
+{
+    for (long i = 0; i < n; ++i) rot1(x + i * incx, y + i * incy, c, s);
+}
+
+/* Csrot_naive.cl:16-25: the same map per real component
+ * (cfmaf(x, c, y*s) = fma(x, c, y*s) componentwise). */
+void orc_csrot(int n, orc_c32* x, int incx, orc_c32* y, int incy, float c, float s)
+{
+    for (long i = 0; i < n; ++i) {
+        orc_c32* a = x + i * incx;
+        orc_c32* b = y + i * incy;
+        rot1(&a->re, &b->re, c, s);
+        rot1(&a->im, &b->im, c, s);
+    }
+}
+
+/* cmul with the reference's fma placement (core/src/ocl/complex.h.cl:32-34) */
+static orc_c32 cmul_fma(orc_c32 a, orc_c32 b)
+{
+    orc_c32 r;
+    r.re = fmaf(a.re, b.re, -(a.im * b.im));
+    r.im = fmaf(a.re, b.im, a.im * b.re);
+    return r;
+}
+
+/* Crot_naive.cl:16-25: x' = x c + s y, y' = y c - conj(s) x. */
+void orc_crot(int n, orc_c32* x, int incx, orc_c32* y, int incy, float c, orc_c32 s)
+{
+    const orc_c32 mcs = { -s.re, s.im };
+    for (long i = 0; i < n; ++i) {
+        orc_c32* a = x + i * incx;
+        orc_c32* b = y + i * incy;
+        const orc_c32 sy = cmul_fma(s, *b);
+        const orc_c32 mx = cmul_fma(mcs, *a);
+        orc_c32 nx, ny;
+        nx.re = fmaf(a->re, c, sy.re);
+        nx.im = fmaf(a->im, c, sy.im);
+        ny.re = fmaf(b->re, c, mx.re);
+        ny.im = fmaf(b->im, c, mx.im);
+        *a = nx;
+        *b = ny;
+    }
+}
+
+/* Modified rotation, the reference's parameter layout
+ * (Srotm_naive.cl:18-48 with Srotm_helpers.h.cl:27-41; mad as fmaf):
+ *   flag -1: x' = p1 x + p2 y, y' = p3 x + p4 y
+ *   flag  0: x' = x + p2 y,    y' = p3 x + y
+ *   flag  1: x' = p1 x + y,    y' = p4 y - x
+ * any other flag leaves x and y unchanged. */
+void orc_srotm(int n, float* x, int incx, float* y, int incy, const float* p)
+{
+    const float f = p[0];
+    if (!(f == -1.f || f == 0.f || f == 1.f)) return;
+    for (long i = 0; i < n; ++i) {
+        float* a = x + i * incx;
+        float* b = y + i * incy;
+        const float xv = *a, yv = *b;
+        float nx, ny;
+        if (f == -1.f) { nx = fmaf(p[1], xv, p[2] * yv); ny = fmaf(p[3], xv, p[4] * yv); }
+        else if (f == 0.f) { nx = fmaf(p[2], yv, xv); ny = fmaf(p[3], xv, yv); }
+        else { nx = fmaf(p[1], xv, yv); ny = fmaf(p[4], yv, -xv); }
+        *a = nx;
+        *b = ny;
+    }
+}
+
+/* OpenCL sign(): 1, -1, or 0 for zero and NaN. */
+static float ocl_sign(float v) { return v > 0.f ? 1.f : (v < 0.f ? -1.f : 0.f); }
+
+/* Srotg_naive.cl:16-56, including scale = |a| * |b| (zero when either input
+ * is zero, giving c = 1, s = 0, r = z = 0). */
+void orc_srotg(float* a, float* b, float* c, float* s)
+{
+    const float av = *a, bv = *b;
+    const float fa = fabsf(av), fb = fabsf(bv);
+    const float roe = fa > fb ? av : bv;
+    const float scale = fa * fb;
+    float r, z;
+    if (scale == 0.f) {
+        *c = 1.f; *s = 0.f; r = 0.f; z = 0.f;
+    } else {
+        const float a2 = av / scale, b2 = bv / scale;
+        const float sg = ocl_sign(roe) * scale;
+        r = sg * sqrtf(a2 * a2 + b2 * b2);
+        *c = av / r;
+        *s = bv / r;
+        z = 1.f;
+        if (fa > fb) z = *s;
+        if (fb >= fa && *c != 0.f) z = 1.f / *c;
+    }
+    *a = r;
+    *b = z;
+}
+
+/* |v| as cabs (complex.h.cl:28-30): sqrt(fma(re, re, im*im)). */
+static float cabs_fma(orc_c32 v) { return sqrtf(fmaf(v.re, v.re, v.im * v.im)); }
+
+/* Crotg_naive.cl:16-44. */
+void orc_crotg(orc_c32* a, orc_c32* b, float* c, orc_c32* s)
+{
+    const orc_c32 av = *a, bv = *b;
+    const float fa = cabs_fma(av), fb = cabs_fma(bv);
+    if (fa == 0.f) {
+        *c = 0.f;
+        s->re = 1.f; s->im = 0.f;
+        *a = bv;
+        return;
+    }
+    const float scale = fa + fb;
+    orc_c32 as = { av.re / scale, av.im / scale }, bs = { bv.re / scale, bv.im / scale };
+    const float da = cabs_fma(as), db = cabs_fma(bs);
+    const float norm = scale * sqrtf(da * da + db * db);
+    const orc_c32 alpha = { av.re / fa, av.im / fa };
+    *c = fa / norm;
+    const orc_c32 cb = { bv.re, -bv.im };
+    const orc_c32 t = cmul_fma(cb, alpha);
+    s->re = t.re / norm;
+    s->im = t.im / norm;
+    a->re = alpha.re * norm;
+    a->im = alpha.im * norm;
+}
+
+/* Modified Givens generator: the reference's host-side checks
+ * (libs/blas/shlib/iclBLAS_S.cpp:101-128) then its kernel
+ * (Srotmg_naive.cl:16-143).  The rescaling loops are capped at 16 steps
+ * (finite values need at most 12; the reference's loop never ends for an
+ * infinite d1 or d2). */
+void orc_srotmg(float* d1, float* d2, float* x1, float y1, float* param)
+{
+    float dd1 = *d1, dd2 = *d2, bb1 = *x1;
+    const float bb2 = y1;
+    if (dd1 < 0.f) { param[0] = -1.f; param[1] = param[2] = param[3] = param[4] = 0.f; return; }
+    if (dd2 == 0.f || bb2 == 0.f) { param[0] = -2.f; return; }
+    if (-dd2 * bb2 * bb2 >= dd1 * bb1 * bb1) {
+        param[0] = -1.f; param[1] = param[2] = param[3] = param[4] = 0.f; return;
+    }
+    const float p1 = dd1 * bb1, p2 = dd2 * bb2;
+    const float q1 = p1 * bb1, q2 = p2 * bb2;
+    float h11 = 0.f, h12 = 0.f, h21 = 0.f, h22 = 0.f, flag;
+    if (q1 > fabsf(q2)) {
+        h12 = p2 / p1;
+        h21 = -bb2 / bb1;
+        const float u = 1.f - h12 * h21;
+        flag = 0.f;
+        if (u > 0.f) { dd1 /= u; dd2 /= u; bb1 *= u; }
+    } else {
+        h11 = p1 / p2;
+        h22 = bb1 / bb2;
+        const float u = 1.f + h11 * h22;
+        const float v = dd1 / u;
+        flag = 1.f;
+        dd1 = dd2 / u;
+        dd2 = v;
+        bb1 = bb2 * u;
+    }
+    const float g = 4096.f, gsq = g * g, gmsq = 1.f / gsq;
+    if (dd1 != 0.f && (fabsf(dd1) < gmsq || fabsf(dd1) > gsq)) {
+        if (flag == 0.f) { h11 = 1.f; h22 = 1.f; }
+        else { h12 = 1.f; h21 = -1.f; }
+        flag = -1.f;
+        for (int it = 0; it < 16 && (fabsf(dd1) < gmsq || fabsf(dd1) > gsq); ++it) {
+            if (fabsf(dd1) < gmsq) { dd1 *= gsq; bb1 /= g; h11 /= g; h12 /= g; }
+            else { dd1 /= gsq; bb1 *= g; h11 *= g; h12 *= g; }
+        }
+    }
+    if (dd2 != 0.f && (fabsf(dd2) < gmsq || fabsf(dd2) > gsq)) {
+        if (flag == 0.f) { h11 = 1.f; h22 = 1.f; flag = -1.f; }
+        else if (flag == 1.f) { h12 = 1.f; h21 = -1.f; flag = -1.f; }
+        for (int it = 0; it < 16 && (fabsf(dd2) < gmsq || fabsf(dd2) > gsq); ++it) {
+            if (fabsf(dd2) < gmsq) { dd2 *= gsq; h21 /= g; h22 /= g; }
+            else { dd2 /= gsq; h21 *= g; h22 *= g; }
+        }
+    }
+    param[0] = flag;
+    if (flag == -1.f) { param[1] = h11; param[2] = h21; param[3] = h12; param[4] = h22; }
+    else if (flag == 0.f) { param[2] = h21; param[3] = h12; }
+    else { param[1] = h11; param[4] = h22; }
+    *d1 = dd1;
+    *d2 = dd2;
+    *x1 = bb1;
+}
+
+/* ------------------------------------------------------------------------ */
 /* Level 2                                                                  */
 /* ------------------------------------------------------------------------ */
 

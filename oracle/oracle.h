@@ -3,7 +3,7 @@
  *
  * This header declares a plain-C restatement of the reference's CPU
  * algorithms for the S/C gemm, gemv, trsv, trsm, dot, nrm2, asum, iamax,
- * axpy and scal routines.  It is the checker the GPU library is compared
+ * axpy and scal routines, and for iamin, copy, swap, rot, rotm, rotg, rotmg.  It is the checker the GPU library is compared
  * against; nothing in the shipped library links it.  Each function names the
  * reference source it restates (paths are relative to the clGPU tree).
  *
@@ -14,7 +14,9 @@
  * Arithmetic: like the reference test oracles (tests/blas_funcs/test_*.hpp,
  * accumulator_type<float> = double, tests/blas_funcs/test_helpers.hpp:216-232)
  * every accumulation runs in double and is rounded to float once at the end,
- * except SGEMM, which follows the reference kernels' FP32 FMA order.
+ * except SGEMM, which follows the reference kernels' FP32 FMA order, and the
+ * copy/swap/rotation family, which restates the reference kernels' FP32
+ * expressions (their fma placement included) exactly.
  */
 #ifndef ICLB_ORACLE_H
 #define ICLB_ORACLE_H
@@ -40,6 +42,19 @@ orc_c32 orc_cdot(int n, const orc_c32* x, int incx, const orc_c32* y, int incy, 
 float   orc_scnrm2(int n, const orc_c32* x, int incx);
 float   orc_scasum(int n, const orc_c32* x, int incx);
 int     orc_icamax(int n, const orc_c32* x, int incx);
+
+/* ---- level 1: iamin, copy, swap, plane rotations ---- */
+int   orc_isamin(int n, const float* x, int incx);
+int   orc_icamin(int n, const orc_c32* x, int incx);
+void  orc_copy(int n, const void* x, int incx, void* y, int incy, int esize);
+void  orc_swap(int n, void* x, int incx, void* y, int incy, int esize);
+void  orc_srot(int n, float* x, int incx, float* y, int incy, float c, float s);
+void  orc_csrot(int n, orc_c32* x, int incx, orc_c32* y, int incy, float c, float s);
+void  orc_crot(int n, orc_c32* x, int incx, orc_c32* y, int incy, float c, orc_c32 s);
+void  orc_srotm(int n, float* x, int incx, float* y, int incy, const float* param);
+void  orc_srotg(float* a, float* b, float* c, float* s);
+void  orc_crotg(orc_c32* a, orc_c32* b, float* c, orc_c32* s);
+void  orc_srotmg(float* d1, float* d2, float* x1, float y1, float* param);
 
 /* ---- level 2 ---- */
 void orc_sgemv(int trans, int m, int n, float alpha, const float* A, int lda,

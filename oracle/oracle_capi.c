@@ -298,3 +298,115 @@ iclblasStatus_t iclblasCtrsm(iclblasHandle_t h, iclblasSideMode_t side, iclblasF
     orc_ctrsm(side, uplo, trans, diag, m, n, c32(alpha), (const orc_c32*)A, lda, (orc_c32*)B, ldb);
     return ICLBLAS_STATUS_SUCCESS;
 }
+
+/* ---- level 1: iamin, copy, swap, rotations (iclBLAS_S.cpp:54-62, 101-246;
+ *      iclBLAS_C.cpp:58-95, 151-190, 309-333) ---- */
+iclblasStatus_t iclblasIsamin(iclblasHandle_t h, int n, float* x, int incx, int* result)
+{
+    if (n <= 0 || incx <= 0) { *result = 0; return ICLBLAS_STATUS_SUCCESS; }
+    vparams p = { P_N | P_X | P_INCX, .n = n, .x = x, .incx = incx };
+    CHECK(p, h);
+    *result = orc_isamin(n, x, incx);
+    return ICLBLAS_STATUS_SUCCESS;
+}
+
+iclblasStatus_t iclblasIcamin(iclblasHandle_t h, int n, oclComplex_t* x, int incx, int* result)
+{
+    if (n <= 0 || incx <= 0) { *result = 0; return ICLBLAS_STATUS_SUCCESS; }
+    vparams p = { P_N | P_X | P_INCX, .n = n, .x = x, .incx = incx };
+    CHECK(p, h);
+    *result = orc_icamin(n, (const orc_c32*)x, incx);
+    return ICLBLAS_STATUS_SUCCESS;
+}
+
+static iclblasStatus_t pair_check(iclblasHandle_t h, int n, const void* x, int incx, const void* y, int incy)
+{
+    vparams p = { P_N | P_X | P_INCX | P_Y | P_INCY, .n = n, .x = x, .incx = incx, .y = y, .incy = incy };
+    int v = validate(&p, h);
+    return v == 1 ? ICLBLAS_STATUS_SUCCESS : (iclblasStatus_t)v;
+}
+#define PAIR(h, n, x, incx, y, incy) do { if ((n) <= 0) return ICLBLAS_STATUS_SUCCESS; \
+    iclblasStatus_t s_ = pair_check(h, n, x, incx, y, incy); if (s_) return s_; } while (0)
+
+iclblasStatus_t iclblasScopy(iclblasHandle_t h, int n, float* x, int incx, float* y, int incy)
+{
+    PAIR(h, n, x, incx, y, incy);
+    orc_copy(n, x, incx, y, incy, (int)sizeof(float));
+    return ICLBLAS_STATUS_SUCCESS;
+}
+
+iclblasStatus_t iclblasCcopy(iclblasHandle_t h, int n, oclComplex_t* x, int incx, oclComplex_t* y, int incy)
+{
+    PAIR(h, n, x, incx, y, incy);
+    orc_copy(n, x, incx, y, incy, (int)sizeof(oclComplex_t));
+    return ICLBLAS_STATUS_SUCCESS;
+}
+
+iclblasStatus_t iclblasSswap(iclblasHandle_t h, int n, float* x, int incx, float* y, int incy)
+{
+    PAIR(h, n, x, incx, y, incy);
+    orc_swap(n, x, incx, y, incy, (int)sizeof(float));
+    return ICLBLAS_STATUS_SUCCESS;
+}
+
+iclblasStatus_t iclblasCswap(iclblasHandle_t h, int n, oclComplex_t* x, int incx, oclComplex_t* y, int incy)
+{
+    PAIR(h, n, x, incx, y, incy);
+    orc_swap(n, x, incx, y, incy, (int)sizeof(oclComplex_t));
+    return ICLBLAS_STATUS_SUCCESS;
+}
+
+iclblasStatus_t iclblasSrot(iclblasHandle_t h, int n, float* x, int incx, float* y, int incy, float c, float s)
+{
+    if (c == 1.f && s == 0.f) return ICLBLAS_STATUS_SUCCESS;
+    PAIR(h, n, x, incx, y, incy);
+    orc_srot(n, x, incx, y, incy, c, s);
+    return ICLBLAS_STATUS_SUCCESS;
+}
+
+iclblasStatus_t iclblasSrotm(iclblasHandle_t h, int n, float* x, int incx, float* y, int incy, float* param)
+{
+    if (n <= 0 || param[0] == -2.f) return ICLBLAS_STATUS_SUCCESS;
+    PAIR(h, n, x, incx, y, incy);
+    orc_srotm(n, x, incx, y, incy, param);
+    return ICLBLAS_STATUS_SUCCESS;
+}
+
+iclblasStatus_t iclblasCrot(iclblasHandle_t h, int n, oclComplex_t* x, int incx, oclComplex_t* y, int incy,
+                            const float* c, const oclComplex_t* s)
+{
+    if (n <= 0 || (*c == 1.f && s->val[0] == 0.f && s->val[1] == 0.f)) return ICLBLAS_STATUS_SUCCESS;
+    PAIR(h, n, x, incx, y, incy);
+    orc_crot(n, (orc_c32*)x, incx, (orc_c32*)y, incy, *c, c32(s));
+    return ICLBLAS_STATUS_SUCCESS;
+}
+
+iclblasStatus_t iclblasCsrot(iclblasHandle_t h, int n, oclComplex_t* x, int incx, oclComplex_t* y, int incy,
+                             const float* c, const float* s)
+{
+    if (n <= 0 || (*c == 1.f && *s == 0.f)) return ICLBLAS_STATUS_SUCCESS;
+    PAIR(h, n, x, incx, y, incy);
+    orc_csrot(n, (orc_c32*)x, incx, (orc_c32*)y, incy, *c, *s);
+    return ICLBLAS_STATUS_SUCCESS;
+}
+
+iclblasStatus_t iclblasSrotg(iclblasHandle_t h, float* a, float* b, float* c, float* s)
+{
+    if (!h || h->tag != ORC_TAG || !a || !b || !c || !s) return ICLBLAS_STATUS_INVALID_VALUE;
+    orc_srotg(a, b, c, s);
+    return ICLBLAS_STATUS_SUCCESS;
+}
+
+iclblasStatus_t iclblasCrotg(iclblasHandle_t h, oclComplex_t* a, oclComplex_t* b, float* c, oclComplex_t* s)
+{
+    if (!h || h->tag != ORC_TAG || !a || !b || !c || !s) return ICLBLAS_STATUS_INVALID_VALUE;
+    orc_crotg((orc_c32*)a, (orc_c32*)b, c, (orc_c32*)s);
+    return ICLBLAS_STATUS_SUCCESS;
+}
+
+iclblasStatus_t iclblasSrotmg(iclblasHandle_t h, float* d1, float* d2, float* x1, const float* y1, float* param)
+{
+    if (!h || h->tag != ORC_TAG || !d1 || !d2 || !x1 || !y1 || !param) return ICLBLAS_STATUS_INVALID_VALUE;
+    orc_srotmg(d1, d2, x1, *y1, param);
+    return ICLBLAS_STATUS_SUCCESS;
+}

@@ -3,7 +3,8 @@
 // Each kernel is #included from its .cl file in the clGPU tree (built by
 // oracle/Makefile into oracle/_ref/) behind clshim.hpp and exported with an
 // extern "C" wrapper.  They give CPU results of the reference's own GEMV,
-// TRSV, TRSM and CGEMM algorithms, which its tests have no template for.
+// TRSV, TRSM and CGEMM algorithms, which its tests have no template for, and
+// of its iamin, rotation and rotation-generator kernels.
 #include "clshim.hpp"
 
 namespace ref_sgemv {
@@ -35,6 +36,34 @@ namespace ref_sgemm {
 }
 namespace ref_cgemm {
 #include "Cgemm/Cgemm_naive.cl"
+}
+
+namespace ref_isamin {
+#include "Isamin/Isamin_naive.cl"
+}
+namespace ref_icamin {
+#include "Icamin/Icamin_naive.cl"
+}
+namespace ref_srot {
+#include "Srot/Srot_naive.cl"
+}
+namespace ref_csrot {
+#include "Csrot/Csrot_naive.cl"
+}
+namespace ref_crot {
+#include "Crot/Crot_naive.cl"
+}
+namespace ref_srotm {
+#include "Srotm/Srotm_naive.cl"
+}
+namespace ref_srotg {
+#include "Srotg/Srotg_naive.cl"
+}
+namespace ref_crotg {
+#include "Crotg/Crotg_naive.cl"
+}
+namespace ref_srotmg {
+#include "Srotmg/Srotmg_naive.cl"
 }
 
 static complex_t c2(const float* p) { return complex_t(p[0], p[1]); }
@@ -92,6 +121,63 @@ void ref_naive_cgemm(int ta, int tb, int m, int n, int k, const float* alpha, fl
 {
     ref_cgemm::Cgemm_naive(ta, tb, m, n, k, c2(alpha), (complex_t*)A, lda, (complex_t*)B, ldb, c2(beta),
                            (complex_t*)C, ldc);
+}
+
+// Level-1 kernels: each one is launched with a single work-item
+// (Isamin_naive.cpp, Icamin_naive.cpp, Srot_naive.cpp:45, Crot_naive.cpp:46,
+// Csrot_naive.cpp, Srotm_naive.cpp, Srotg_naive.cpp:44, Crotg_naive.cpp:44,
+// Srotmg_naive.cpp:45).
+int ref_naive_isamin(int n, float* x, int incx)
+{
+    int r = -1;
+    ref_isamin::Isamin_naive(n, x, incx, &r);
+    return r;
+}
+
+int ref_naive_icamin(int n, float* x, int incx)
+{
+    int r = -1;
+    ref_icamin::Icamin_naive(n, (complex_t*)x, incx, &r);
+    return r;
+}
+
+void ref_naive_srot(int n, float* x, int incx, float* y, int incy, float c, float s)
+{
+    ref_srot::Srot_naive((uint)n, x, incx, y, incy, c, s);
+}
+
+void ref_naive_csrot(int n, float* x, int incx, float* y, int incy, float c, float s)
+{
+    ref_csrot::Csrot_naive(n, (complex_t*)x, incx, (complex_t*)y, incy, c, s);
+}
+
+void ref_naive_crot(int n, float* x, int incx, float* y, int incy, float c, const float* s)
+{
+    ref_crot::Crot_naive(n, (complex_t*)x, incx, (complex_t*)y, incy, c, c2(s));
+}
+
+void ref_naive_srotm(int n, float* x, int incx, float* y, int incy, float* param)
+{
+    ref_srotm::Srotm_naive((uint)n, x, (uint)incx, y, (uint)incy, param);
+}
+
+void ref_naive_srotg(float* a, float* b, float* c, float* s)
+{
+    ref_srotg::Srotg_naive(a, b, c, s);
+}
+
+// Compare only for a != 0: the a == 0 branch writes an OpenCL vector literal.
+void ref_naive_crotg(float* a, float* b, float* c, float* s)
+{
+    ref_crotg::Crotg_naive((complex_t*)a, (complex_t*)b, c, (complex_t*)s);
+}
+
+// The kernel alone; the caller applies the host-side checks of
+// iclBLAS_S.cpp:101-128 first.  Inputs whose rescaling loops would not end
+// (an infinite d1 or d2) must not be passed.
+void ref_naive_srotmg(float* d1, float* d2, float* x1, float y1, float* param)
+{
+    ref_srotmg::Srotmg_naive(d1, d2, x1, y1, param);
 }
 
 }  // extern "C"

@@ -5,7 +5,8 @@ reference's CPU templates (tests/blas_funcs/*.hpp: cpu_gemm, cpu_dot,
 cpu_nrm2, cpu_asum, cpu_axpy, cpu_scal, cpu_amax; tests/blas_reference/
 blas_reference.cpp: Isamax_reference, Caxpy_reference) and its serial OpenCL
 kernels compiled as C++ (Sgemv/Cgemv/Strsv/Ctrsv/Strsm/Ctrsm/Sgemm/Cgemm
-_naive.cl), all built from the reference's sources by oracle/Makefile.
+_naive.cl and the level-1 Isamin/Icamin/Srot/Csrot/Crot/Srotm/Srotg/Crotg/
+Srotmg _naive.cl), all built from the reference's sources by oracle/Makefile.
 
 Each case is stored under a key prefix "<case>/" with its inputs, scalar
 parameters and the reference output.  The fixture is committed; run this
@@ -42,6 +43,75 @@ def tri(n, lda, lower, rng, dtype=np.float32):
     M[mask] = off[mask]
     M[np.arange(n), np.arange(n)] = d
     return A
+
+
+def rotmg_passes_host_checks(d1, d2, x1, y1):
+    """The reference's host-side Srotmg checks (libs/blas/shlib/iclBLAS_S.cpp:
+    101-128) all pass, so its kernel runs."""
+    f = np.float32
+    return not (f(d1) < 0 or f(d2) == 0 or f(y1) == 0 or f(f(-f(d2) * f(y1)) * f(y1)) >= f(f(f(d1) * f(x1)) * f(x1)))
+
+
+def rotation_cases(R, d):
+    """iamin, rot, csrot, crot, rotm, rotg, crotg and rotmg through the
+    reference's serial kernels (Isamin/Icamin/Srot/Csrot/Crot/Srotm/Srotg/
+    Crotg/Srotmg _naive.cl); own seed, so the other cases stay unchanged."""
+    rng = np.random.default_rng(20261204)
+    for n, incx, incy in ((1000, 1, 1), (257, 2, 3)):
+        k = f"rot_{n}_{incx}_{incy}/"
+        x = rng.uniform(-4, 4, n * incx).astype(np.float32)
+        y = rng.uniform(-4, 4, n * incy).astype(np.float32)
+        xc = rng.uniform(-4, 4, (n * incx, 2)).astype(np.float32).view(np.complex64).reshape(-1)
+        yc = rng.uniform(-4, 4, (n * incy, 2)).astype(np.float32).view(np.complex64).reshape(-1)
+        d[k + "x"], d[k + "y"], d[k + "xc"], d[k + "yc"] = x, y, xc, yc
+        d[k + "dims"] = np.array([n, incx, incy], np.int32)
+        d[k + "isamin"] = np.int32(R.ref_naive_isamin(n, P(x), incx))
+        d[k + "icamin"] = np.int32(R.ref_naive_icamin(n, P(xc), incx))
+        c, s, sc = np.float32(0.6), np.float32(-0.8), np.complex64(0.25 - 0.5j)
+        d[k + "cs"] = np.array([c, s], np.float32)
+        d[k + "sc"] = sc
+        x1, y1 = x.copy(), y.copy()
+        R.ref_naive_srot(n, P(x1), incx, P(y1), incy, float(c), float(s))
+        d[k + "srot_x"], d[k + "srot_y"] = x1, y1
+        x1, y1 = xc.copy(), yc.copy()
+        R.ref_naive_csrot(n, P(x1), incx, P(y1), incy, float(c), float(s))
+        d[k + "csrot_x"], d[k + "csrot_y"] = x1, y1
+        x1, y1 = xc.copy(), yc.copy()
+        R.ref_naive_crot(n, P(x1), incx, P(y1), incy, float(c), P(O.cbox(sc)))
+        d[k + "crot_x"], d[k + "crot_y"] = x1, y1
+        for flag in (-1, 0, 1):
+            param = np.array([flag, 0.75, -1.5, 2.25, 0.125], np.float32)
+            x1, y1 = x.copy(), y.copy()
+            R.ref_naive_srotm(n, P(x1), incx, P(y1), incy, P(param))
+            d[k + f"srotm{flag}_param"] = param
+            d[k + f"srotm{flag}_x"], d[k + f"srotm{flag}_y"] = x1, y1
+    ab = np.concatenate([rng.uniform(-10, 10, (64, 2)),
+                         [[0, 3], [3, 0], [0, 0], [-2, 2], [1, 1.5], [1e-20, 3e-20], [1e20, -7e19]]]).astype(np.float32)
+    out = np.zeros((len(ab), 4), np.float32)
+    for i, (a, b) in enumerate(ab):
+        v = np.array([a, b, 0, 0], np.float32)
+        R.ref_naive_srotg(P(v[0:]), P(v[1:]), P(v[2:]), P(v[3:]))
+        out[i] = v
+    d["srotg/ab"], d["srotg/out"] = ab, out
+    abc = rng.uniform(-10, 10, (64, 4)).astype(np.float32).view(np.complex64)
+    outc = np.zeros((64, 3), np.complex64)
+    for i, (a, b) in enumerate(abc):
+        v = np.array([a, b, 0], np.complex64)
+        cc = np.zeros(1, np.float32)
+        R.ref_naive_crotg(P(v[0:]), P(v[1:]), P(cc), P(v[2:]))
+        outc[i] = [v[0], cc[0], v[2]]
+    d["crotg/ab"], d["crotg/out"] = abc, outc
+    rows = [r for r in rng.uniform(-2, 10, (200, 4)) if rotmg_passes_host_checks(*r)][:48]
+    rows += [(1.1, -1.0, 3.3, 3.2), (0.0, 1.2, 3.3, 3.2), (1 / 4096 / 4096, 1 / 4096 / 4096, 3.3, 3.2),
+             (1e-12, 2e-12, 1.0, 0.5), (1e9, 3e9, 2.0, 1.0), (5e8, 1e-10, 1.0, 4.0)]
+    rows = np.array(rows, np.float32)
+    outm = np.zeros((len(rows), 8), np.float32)
+    for i, (d1, d2, x1, y1) in enumerate(rows):
+        param = np.full(5, 7, np.float32)
+        v = np.array([d1, d2, x1], np.float32)
+        R.ref_naive_srotmg(P(v[0:]), P(v[1:]), P(v[2:]), float(y1), P(param))
+        outm[i, :3], outm[i, 3:] = v, param
+    d["srotmg/in"], d["srotmg/out"] = rows, outm
 
 
 def main():
@@ -204,6 +274,8 @@ def main():
                     d[k + "alpha"] = al
                     R.ref_naive_ctrsm(side, uplo, trans, diag, m, n, P(alb), P(A), lda, P(Bm), ldb)
                     d[k + "out"] = Bm
+
+    rotation_cases(R, d)
 
     np.savez_compressed(OUT, **d)
     print(f"wrote {OUT}: {len(d)} arrays, {os.path.getsize(OUT) / 1024:.0f} KiB")

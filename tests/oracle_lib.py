@@ -63,6 +63,17 @@ def orc() -> C.CDLL:
             "orc_ctrsm": ([i, i, i, i, i, i, C32, p, i, p, i], None),
             "orc_dgemm": ([i, i, i, i, i, d, p, i, p, i, d, p, i], None),
             "orc_dtrsm": ([i, i, i, i, i, i, d, p, i, p, i], None),
+            "orc_isamin": ([i, p, i], i),
+            "orc_icamin": ([i, p, i], i),
+            "orc_copy": ([i, p, i, p, i, i], None),
+            "orc_swap": ([i, p, i, p, i, i], None),
+            "orc_srot": ([i, p, i, p, i, f, f], None),
+            "orc_csrot": ([i, p, i, p, i, f, f], None),
+            "orc_crot": ([i, p, i, p, i, f, C32], None),
+            "orc_srotm": ([i, p, i, p, i, p], None),
+            "orc_srotg": ([p, p, p, p], None),
+            "orc_crotg": ([p, p, p, p], None),
+            "orc_srotmg": ([p, p, p, f, p], None),
         }
         for name, (a, r) in sig.items():
             fn = getattr(L, name)
@@ -103,6 +114,15 @@ def ref() -> C.CDLL | None:
             "ref_naive_ctrsm": ([i, i, i, i, i, i, p, p, i, p, i], None),
             "ref_naive_sgemm": ([i, i, i, i, i, f, p, i, p, i, f, p, i], None),
             "ref_naive_cgemm": ([i, i, i, i, i, p, p, i, p, i, p, p, i], None),
+            "ref_naive_isamin": ([i, p, i], i),
+            "ref_naive_icamin": ([i, p, i], i),
+            "ref_naive_srot": ([i, p, i, p, i, f, f], None),
+            "ref_naive_csrot": ([i, p, i, p, i, f, f], None),
+            "ref_naive_crot": ([i, p, i, p, i, f, p], None),
+            "ref_naive_srotm": ([i, p, i, p, i, p], None),
+            "ref_naive_srotg": ([p, p, p, p], None),
+            "ref_naive_crotg": ([p, p, p, p], None),
+            "ref_naive_srotmg": ([p, p, p, f, p], None),
         }
         for name, (a, r) in sig.items():
             fn = getattr(L, name)
@@ -211,6 +231,60 @@ def dgemm(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc):
 
 def dtrsm(side, uplo, trans, diag, m, n, alpha, A, lda, B, ldb):
     orc().orc_dtrsm(side, uplo, trans, diag, m, n, alpha, _p(A), lda, _p(B), ldb)
+
+
+def isamin(n, x, incx) -> int:
+    return orc().orc_isamin(n, _p(x), incx)
+
+
+def icamin(n, x, incx) -> int:
+    return orc().orc_icamin(n, _p(x), incx)
+
+
+def copy(n, x, incx, y, incy):
+    orc().orc_copy(n, _p(x), incx, _p(y), incy, x.itemsize)
+
+
+def swap(n, x, incx, y, incy):
+    orc().orc_swap(n, _p(x), incx, _p(y), incy, x.itemsize)
+
+
+def srot(n, x, incx, y, incy, c, s):
+    orc().orc_srot(n, _p(x), incx, _p(y), incy, c, s)
+
+
+def csrot(n, x, incx, y, incy, c, s):
+    orc().orc_csrot(n, _p(x), incx, _p(y), incy, c, s)
+
+
+def crot(n, x, incx, y, incy, c, s):
+    orc().orc_crot(n, _p(x), incx, _p(y), incy, c, c32(s))
+
+
+def srotm(n, x, incx, y, incy, param):
+    orc().orc_srotm(n, _p(x), incx, _p(y), incy, _p(param))
+
+
+def srotg(a, b):
+    """Returns (r, z, c, s) as float32 for inputs a, b."""
+    v = np.array([a, b, 0, 0], dtype=np.float32)
+    orc().orc_srotg(_p(v[0:]), _p(v[1:]), _p(v[2:]), _p(v[3:]))
+    return tuple(v)
+
+
+def crotg(a, b):
+    """Returns (a', c, s) for complex inputs a, b."""
+    v = np.array([a, b, 0], dtype=np.complex64)
+    c = np.zeros(1, dtype=np.float32)
+    orc().orc_crotg(_p(v[0:]), _p(v[1:]), _p(c), _p(v[2:]))
+    return v[0], c[0], v[2]
+
+
+def srotmg(d1, d2, x1, y1, param):
+    """Returns (d1', d2', x1'); param (5 floats) is updated in place."""
+    v = np.array([d1, d2, x1], dtype=np.float32)
+    orc().orc_srotmg(_p(v[0:]), _p(v[1:]), _p(v[2:]), float(np.float32(y1)), _p(param))
+    return tuple(v)
 
 
 # ------------------------------------------------------------ data helpers

@@ -127,7 +127,94 @@ def test_oracle_trsm(case):
     assert O.rel_fro(Bm, g(case, "out")) <= TOL
 
 
+def bits(a):
+    return np.ascontiguousarray(a).view(np.uint32)
+
+
+def same(a, b):
+    """Bit-identical, except that any two NaNs match (the GPU writes a
+    canonical NaN where the CPU propagates its operand's payload)."""
+    fa = np.ascontiguousarray(a).view(np.float32)
+    fb = np.ascontiguousarray(b).view(np.float32)
+    return fa.shape == fb.shape and bool(np.all((bits(fa) == bits(fb)) | (np.isnan(fa) & np.isnan(fb))))
+
+
+@pytest.mark.parametrize("case", cases("rot_"))
+def test_oracle_rotations(case):
+    n, incx, incy = (int(v) for v in g(case, "dims"))
+    x, y, xc, yc = g(case, "x"), g(case, "y"), g(case, "xc"), g(case, "yc")
+    c, s = (float(v) for v in g(case, "cs"))
+    assert O.isamin(n, x, incx) == g(case, "isamin")
+    assert O.icamin(n, xc, incx) == g(case, "icamin")
+    for name, fn, a, b, arg in (("srot", O.srot, x, y, s), ("csrot", O.csrot, xc, yc, s),
+                                ("crot", O.crot, xc, yc, complex(g(case, "sc")))):
+        a1, b1 = a.copy(), b.copy()
+        fn(n, a1, incx, b1, incy, c, arg)
+        assert np.array_equal(bits(a1), bits(g(case, name + "_x"))), name
+        assert np.array_equal(bits(b1), bits(g(case, name + "_y"))), name
+    for flag in (-1, 0, 1):
+        a1, b1 = x.copy(), y.copy()
+        O.srotm(n, a1, incx, b1, incy, g(case, f"srotm{flag}_param"))
+        assert np.array_equal(bits(a1), bits(g(case, f"srotm{flag}_x")))
+        assert np.array_equal(bits(b1), bits(g(case, f"srotm{flag}_y")))
+
+
+def test_oracle_rotation_generators():
+    for (a, b), want in zip(g("srotg", "ab"), g("srotg", "out")):
+        assert np.array_equal(bits(np.array(O.srotg(a, b), np.float32)), bits(want))
+    for (a, b), want in zip(g("crotg", "ab"), g("crotg", "out")):
+        ar, c, s = O.crotg(complex(a), complex(b))
+        assert np.array_equal(bits(np.array([ar, c, s], np.complex64)), bits(want))
+    for row, want in zip(g("srotmg", "in"), g("srotmg", "out")):
+        param = np.full(5, 7, np.float32)
+        v = O.srotmg(*row, param)
+        assert np.array_equal(bits(np.array(v, np.float32)), bits(want[:3]))
+        assert np.array_equal(bits(param), bits(want[3:]))
+
+
 # ------------------------------------------------------------------ GPU library
+@pytest.mark.gpu
+def test_gpu_rotations_against_golden(handle):
+    for case in cases("rot_"):
+        n, incx, incy = (int(v) for v in g(case, "dims"))
+        x, y, xc, yc = g(case, "x"), g(case, "y"), g(case, "xc"), g(case, "yc")
+        c, s = (float(v) for v in g(case, "cs"))
+        ri = np.zeros(1, np.int32)
+        assert B.iclblasIsamin(handle, n, x, incx, ri) == B.SUCCESS and ri[0] == g(case, "isamin")
+        assert B.iclblasIcamin(handle, n, xc, incx, ri) == B.SUCCESS and ri[0] == g(case, "icamin")
+        for name, fn, a, b, arg in (("srot", B.iclblasSrot, x, y, s), ("csrot", B.iclblasCsrot, xc, yc, s),
+                                    ("crot", B.iclblasCrot, xc, yc, complex(g(case, "sc")))):
+            a1, b1 = a.copy(), b.copy()
+            assert fn(handle, n, a1, incx, b1, incy, c, arg) == B.SUCCESS
+            assert same(a1, g(case, name + "_x")), (case, name)
+            assert same(b1, g(case, name + "_y")), (case, name)
+        for flag in (-1, 0, 1):
+            a1, b1 = x.copy(), y.copy()
+            assert B.iclblasSrotm(handle, n, a1, incx, b1, incy, g(case, f"srotm{flag}_param").copy()) == B.SUCCESS
+            assert same(a1, g(case, f"srotm{flag}_x")), (case, flag)
+            assert same(b1, g(case, f"srotm{flag}_y")), (case, flag)
+
+
+@pytest.mark.gpu
+def test_gpu_rotation_generators_against_golden(handle):
+    for (a, b), want in zip(g("srotg", "ab"), g("srotg", "out")):
+        v = np.array([a, b, 0, 0], np.float32)
+        assert B.iclblasSrotg(handle, v[0:], v[1:], v[2:], v[3:]) == B.SUCCESS
+        assert same(v, want), (a, b)
+    for (a, b), want in zip(g("crotg", "ab"), g("crotg", "out")):
+        v = np.array([a, b, 0], np.complex64)
+        cc = np.zeros(1, np.float32)
+        assert B.iclblasCrotg(handle, v[0:], v[1:], cc, v[2:]) == B.SUCCESS
+        assert same(np.array([v[0], cc[0], v[2]], np.complex64), want)
+    for row, want in zip(g("srotmg", "in"), g("srotmg", "out")):
+        v = row[:3].copy()
+        y1 = row[3:4].copy()
+        param = np.full(5, 7, np.float32)
+        assert B.iclblasSrotmg(handle, v[0:], v[1:], v[2:], y1, param) == B.SUCCESS
+        assert same(v, want[:3]) and same(param, want[3:]), row
+
+
+
 @pytest.mark.gpu
 def test_gpu_level1_against_golden(handle):
     for case in cases("l1s_"):
