@@ -22,10 +22,14 @@ namespace {
 
 constexpr int kThreads = 256;
 
-__host__ int l1_grid(iclblasHandle_t h, long units)
+// One thread per unit, at most `per_sm` CTAs per SM (grid-stride beyond).
+// The cap is per kernel, the best of 3/4/6/8 CTAs per SM measured at
+// n = 2^28: 4 for saxpy, 6 for sasum and iamax, 8 for the others (sscal and
+// snrm2 lose 15-25% at 4; sdot is flat).
+__host__ int l1_grid(iclblasHandle_t h, long units, int per_sm = 8)
 {
     long g = (units + kThreads - 1) / kThreads;
-    long cap = (long)h->sm_count * 8;
+    long cap = (long)h->sm_count * per_sm;
     if (g > cap) g = cap;
     return g < 1 ? 1 : (int)g;
 }
@@ -443,7 +447,7 @@ cudaError_t saxpy(iclblasHandle_t h, int n, float alpha, const float* x, int inc
 {
     if (incx == 1 && incy == 1 && aligned16(x) && aligned16(y)) {
         long n4 = n >> 2;
-        if (n4 > 0) saxpy_vec<<<l1_grid(h, n4), kThreads, 0, h->stream>>>(n4, alpha, (const float4*)x, (float4*)y);
+        if (n4 > 0) saxpy_vec<<<l1_grid(h, n4, 4), kThreads, 0, h->stream>>>(n4, alpha, (const float4*)x, (float4*)y);
         long rem = n - n4 * 4;
         if (rem > 0) saxpy_strided<<<1, 32, 0, h->stream>>>(rem, alpha, x + n4 * 4, 1, y + n4 * 4, 1);
     } else {
@@ -487,7 +491,7 @@ cudaError_t sreduce(iclblasHandle_t h, Red op, int n, const float* x, int incx, 
                     float* result)
 {
     const bool vec = incx == 1 && aligned16(x) && (op != Red::Dot || (incy == 1 && aligned16(y)));
-    const int grid = l1_grid(h, vec ? ((long)n + 3) / 4 : n);
+    const int grid = l1_grid(h, vec ? ((long)n + 3) / 4 : n, op == Red::Asum ? 6 : 8);
     double* partials = (double*)scratch(h, sizeof(double) * (size_t)grid);
     if (!partials) return cudaErrorMemoryAllocation;
     unsigned* ctr = h->ws.counters;
@@ -598,7 +602,7 @@ template <class T, bool MIN>
 cudaError_t iamax_impl(iclblasHandle_t h, int n, const T* x, int incx, int* result)
 {
     const bool vec = incx == 1 && aligned16(x);
-    const int grid = l1_grid(h, vec ? ((long)n + (16 / sizeof(T)) - 1) / (16 / sizeof(T)) : n);
+    const int grid = l1_grid(h, vec ? ((long)n + (16 / sizeof(T)) - 1) / (16 / sizeof(T)) : n, 6);
     Cand* partials = (Cand*)scratch(h, sizeof(Cand) * (size_t)grid);
     if (!partials) return cudaErrorMemoryAllocation;
     if (vec)
