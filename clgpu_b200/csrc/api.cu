@@ -1015,6 +1015,123 @@ extern "C" iclblasStatus_t iclblasCtrsv(iclblasHandle_t h, iclblasFillMode_t upl
 }
 
 // ------------------------------------------------------------------------
+// level 2: rank-1 updates and symmetric / Hermitian products
+// ------------------------------------------------------------------------
+extern "C" iclblasStatus_t iclblasSger(iclblasHandle_t h, int m, int n, const float* alpha, float* x, int incx,
+                                       float* y, int incy, float* A, int lda)
+{
+    if (!alpha) return ICLBLAS_STATUS_INVALID_VALUE;
+    // iclBLAS_S.cpp (Sger): m == 0, n == 0 or alpha == 0 return first
+    if (m == 0 || n == 0 || *alpha == 0.f) return ICLBLAS_STATUS_SUCCESS;
+    if (m < 0 || n < 0 || incx == 0 || incy == 0) return ICLBLAS_STATUS_INVALID_VALUE;
+    return guarded([&]() -> iclblasStatus_t {
+        Params p; p.present = P_N | P_M | P_X | P_INCX | P_Y | P_INCY | P_A | P_LDA;
+        p.n = n; p.m = m; p.x = x; p.incx = incx; p.y = y; p.incy = incy; p.A = A; p.lda = lda;
+        VALIDATE(p, h);
+        Stager st(h);
+        int ix = st.add(x, vec_extent(m, incx) * sizeof(float), false);
+        int iy = st.add(y, vec_extent(n, incy) * sizeof(float), false);
+        int ia = st.add(A, mat_extent(m, n, lda) * sizeof(float), true);
+        cudaError_t e = st.stage_in();
+        if (e == cudaSuccess)
+            e = iclb::sger(h, m, n, *alpha, st.dev<float>(ix), incx, st.dev<float>(iy), incy, st.dev<float>(ia), lda);
+        if (e == cudaSuccess) e = st.finish();
+        return map_cuda(e);
+    });
+}
+
+namespace {
+iclblasStatus_t cger_call(iclblasHandle_t h, bool conj, int m, int n, const oclComplex_t* alpha, oclComplex_t* x,
+                          int incx, oclComplex_t* y, int incy, oclComplex_t* A, int lda)
+{
+    if (!alpha) return ICLBLAS_STATUS_INVALID_VALUE;
+    const cfloat a = cf(alpha);
+    // iclBLAS_C.cpp (Cgeru / Cgerc): m == 0, n == 0 or alpha == 0 return first
+    if (m == 0 || n == 0 || (a.re == 0.f && a.im == 0.f)) return ICLBLAS_STATUS_SUCCESS;
+    if (m < 0 || n < 0 || incx == 0) return ICLBLAS_STATUS_INVALID_VALUE;
+    return guarded([&]() -> iclblasStatus_t {
+        Params p; p.present = P_N | P_M | P_X | P_INCX | P_Y | P_INCY | P_A | P_LDA;
+        p.n = n; p.m = m; p.x = x; p.incx = incx; p.y = y; p.incy = incy; p.A = A; p.lda = lda;
+        VALIDATE(p, h);
+        Stager st(h);
+        int ix = st.add(x, vec_extent(m, incx) * sizeof(cfloat), false);
+        int iy = st.add(y, vec_extent(n, incy) * sizeof(cfloat), false);
+        int ia = st.add(A, mat_extent(m, n, lda) * sizeof(cfloat), true);
+        cudaError_t e = st.stage_in();
+        if (e == cudaSuccess)
+            e = iclb::cger(h, conj, m, n, a, st.dev<cfloat>(ix), incx, st.dev<cfloat>(iy), incy, st.dev<cfloat>(ia),
+                           lda);
+        if (e == cudaSuccess) e = st.finish();
+        return map_cuda(e);
+    });
+}
+}  // namespace
+
+extern "C" iclblasStatus_t iclblasCgeru(iclblasHandle_t h, int m, int n, const oclComplex_t* alpha, oclComplex_t* x,
+                                        int incx, oclComplex_t* y, int incy, oclComplex_t* A, int lda)
+{
+    return cger_call(h, false, m, n, alpha, x, incx, y, incy, A, lda);
+}
+
+extern "C" iclblasStatus_t iclblasCgerc(iclblasHandle_t h, int m, int n, const oclComplex_t* alpha, oclComplex_t* x,
+                                        int incx, oclComplex_t* y, int incy, oclComplex_t* A, int lda)
+{
+    return cger_call(h, true, m, n, alpha, x, incx, y, incy, A, lda);
+}
+
+extern "C" iclblasStatus_t iclblasSsymv(iclblasHandle_t h, iclblasFillMode_t uplo, int n, const float* alpha,
+                                        float* A, int lda, float* x, int incx, const float* beta, float* y, int incy)
+{
+    if (!alpha || !beta) return ICLBLAS_STATUS_INVALID_VALUE;
+    // iclBLAS_S.cpp (Ssymv)
+    if (n == 0 || (*alpha == 0.f && *beta == 1.f)) return ICLBLAS_STATUS_SUCCESS;
+    if (n < 0 || incx == 0 || incy == 0) return ICLBLAS_STATUS_INVALID_VALUE;
+    return guarded([&]() -> iclblasStatus_t {
+        Params p; p.present = P_N | P_A | P_LDA | P_X | P_INCX | P_Y | P_INCY;
+        p.n = n; p.A = A; p.lda = lda; p.x = x; p.incx = incx; p.y = y; p.incy = incy;
+        VALIDATE(p, h);
+        if (uplo != ICLBLAS_FILL_MODE_UPPER && uplo != ICLBLAS_FILL_MODE_LOWER) return ICLBLAS_STATUS_INVALID_VALUE;
+        Stager st(h);
+        int ia = st.add(A, mat_extent(n, n, lda) * sizeof(float), false);
+        int ix = st.add(x, vec_extent(n, incx) * sizeof(float), false);
+        int iy = st.add(y, vec_extent(n, incy) * sizeof(float), true);
+        cudaError_t e = st.stage_in();
+        if (e == cudaSuccess)
+            e = iclb::ssymv(h, uplo, n, *alpha, st.dev<float>(ia), lda, st.dev<float>(ix), incx, *beta,
+                            st.dev<float>(iy), incy);
+        if (e == cudaSuccess) e = st.finish();
+        return map_cuda(e);
+    });
+}
+
+extern "C" iclblasStatus_t iclblasChemv(iclblasHandle_t h, iclblasFillMode_t uplo, int n, const oclComplex_t* alpha,
+                                        oclComplex_t* A, int lda, oclComplex_t* x, int incx, const oclComplex_t* beta,
+                                        oclComplex_t* y, int incy)
+{
+    if (!alpha || !beta) return ICLBLAS_STATUS_INVALID_VALUE;
+    const cfloat a = cf(alpha), b = cf(beta);
+    // iclBLAS_C.cpp (Chemv)
+    if (n == 0 || (a.re == 0.f && a.im == 0.f && b.re == 1.f && b.im == 0.f)) return ICLBLAS_STATUS_SUCCESS;
+    if (n < 0 || incx == 0 || incy == 0) return ICLBLAS_STATUS_INVALID_VALUE;
+    return guarded([&]() -> iclblasStatus_t {
+        Params p; p.present = P_N | P_A | P_LDA | P_X | P_INCX | P_Y | P_INCY;
+        p.n = n; p.A = A; p.lda = lda; p.x = x; p.incx = incx; p.y = y; p.incy = incy;
+        VALIDATE(p, h);
+        if (uplo != ICLBLAS_FILL_MODE_UPPER && uplo != ICLBLAS_FILL_MODE_LOWER) return ICLBLAS_STATUS_INVALID_VALUE;
+        Stager st(h);
+        int ia = st.add(A, mat_extent(n, n, lda) * sizeof(cfloat), false);
+        int ix = st.add(x, vec_extent(n, incx) * sizeof(cfloat), false);
+        int iy = st.add(y, vec_extent(n, incy) * sizeof(cfloat), true);
+        cudaError_t e = st.stage_in();
+        if (e == cudaSuccess)
+            e = iclb::chemv(h, uplo, n, a, st.dev<cfloat>(ia), lda, st.dev<cfloat>(ix), incx, b, st.dev<cfloat>(iy),
+                            incy);
+        if (e == cudaSuccess) e = st.finish();
+        return map_cuda(e);
+    });
+}
+
+// ------------------------------------------------------------------------
 // level 3
 // ------------------------------------------------------------------------
 extern "C" iclblasStatus_t iclblasSgemm(iclblasHandle_t h, iclblasOperation_t transa, iclblasOperation_t transb, int m,
@@ -1113,6 +1230,117 @@ extern "C" iclblasStatus_t iclblasCtrsm(iclblasHandle_t h, iclblasSideMode_t sid
         if (e == cudaSuccess)
             e = iclb::ctrsm(h, side, uplo, trans, diag, m, n, cf(alpha), st.dev<cfloat>(ia), lda, st.dev<cfloat>(ib),
                             ldb);
+        if (e == cudaSuccess) e = st.finish();
+        return map_cuda(e);
+    });
+}
+
+// ------------------------------------------------------------------------
+// level 3 on the GEMM engine: syrk, syr2k, symm, trmm
+// ------------------------------------------------------------------------
+extern "C" iclblasStatus_t iclblasSsyrk(iclblasHandle_t h, iclblasFillMode_t uplo, iclblasOperation_t trans, int n,
+                                        int k, const float* alpha, float* A, int lda, const float* beta, float* C,
+                                        int ldc)
+{
+    if (!alpha || !beta) return ICLBLAS_STATUS_INVALID_VALUE;
+    // iclBLAS_S.cpp (Ssyrk): n == 0, k == 0 or (alpha == 0 and beta == 1) return first
+    if (n == 0 || k == 0 || (*alpha == 0.f && *beta == 1.f)) return ICLBLAS_STATUS_SUCCESS;
+    return guarded([&]() -> iclblasStatus_t {
+        Params p; p.present = P_N | P_K | P_A | P_LDA | P_C | P_LDC;
+        p.n = n; p.k = k; p.A = A; p.lda = lda; p.C = C; p.ldc = ldc;
+        VALIDATE(p, h);
+        if (trans < ICLBLAS_OP_N || trans > ICLBLAS_OP_C) return ICLBLAS_STATUS_INVALID_VALUE;
+        if (uplo != ICLBLAS_FILL_MODE_UPPER && uplo != ICLBLAS_FILL_MODE_LOWER) return ICLBLAS_STATUS_INVALID_VALUE;
+        const bool nt = trans == ICLBLAS_OP_N;
+        Stager st(h);
+        int ia = st.add(A, mat_extent(nt ? n : k, nt ? k : n, lda) * sizeof(float), false);
+        int ic = st.add(C, mat_extent(n, n, ldc) * sizeof(float), true);
+        cudaError_t e = st.stage_in();
+        if (e == cudaSuccess)
+            e = iclb::ssyrk(h, uplo, trans, n, k, *alpha, st.dev<float>(ia), lda, *beta, st.dev<float>(ic), ldc);
+        if (e == cudaSuccess) e = st.finish();
+        return map_cuda(e);
+    });
+}
+
+extern "C" iclblasStatus_t iclblasSsyr2k(iclblasHandle_t h, iclblasFillMode_t uplo, iclblasOperation_t trans, int n,
+                                         int k, const float* alpha, float* A, int lda, float* B, int ldb,
+                                         const float* beta, float* C, int ldc)
+{
+    if (!alpha || !beta) return ICLBLAS_STATUS_INVALID_VALUE;
+    // iclBLAS_S.cpp (Ssyr2k)
+    if (n == 0 || k == 0 || (*alpha == 0.f && *beta == 1.f)) return ICLBLAS_STATUS_SUCCESS;
+    return guarded([&]() -> iclblasStatus_t {
+        Params p; p.present = P_N | P_K | P_A | P_LDA | P_B | P_LDB | P_C | P_LDC;
+        p.n = n; p.k = k; p.A = A; p.lda = lda; p.B = B; p.ldb = ldb; p.C = C; p.ldc = ldc;
+        VALIDATE(p, h);
+        if (trans < ICLBLAS_OP_N || trans > ICLBLAS_OP_C) return ICLBLAS_STATUS_INVALID_VALUE;
+        if (uplo != ICLBLAS_FILL_MODE_UPPER && uplo != ICLBLAS_FILL_MODE_LOWER) return ICLBLAS_STATUS_INVALID_VALUE;
+        const bool nt = trans == ICLBLAS_OP_N;
+        Stager st(h);
+        int ia = st.add(A, mat_extent(nt ? n : k, nt ? k : n, lda) * sizeof(float), false);
+        int ib = st.add(B, mat_extent(nt ? n : k, nt ? k : n, ldb) * sizeof(float), false);
+        int ic = st.add(C, mat_extent(n, n, ldc) * sizeof(float), true);
+        cudaError_t e = st.stage_in();
+        if (e == cudaSuccess)
+            e = iclb::ssyr2k(h, uplo, trans, n, k, *alpha, st.dev<float>(ia), lda, st.dev<float>(ib), ldb, *beta,
+                             st.dev<float>(ic), ldc);
+        if (e == cudaSuccess) e = st.finish();
+        return map_cuda(e);
+    });
+}
+
+extern "C" iclblasStatus_t iclblasSsymm(iclblasHandle_t h, iclblasSideMode_t side, iclblasFillMode_t uplo, int m,
+                                        int n, const float* alpha, float* A, int lda, float* B, int ldb,
+                                        const float* beta, float* C, int ldc)
+{
+    if (!alpha || !beta) return ICLBLAS_STATUS_INVALID_VALUE;
+    // iclBLAS_S.cpp (Ssymm)
+    if (n == 0 || m == 0 || (*alpha == 0.f && *beta == 1.f)) return ICLBLAS_STATUS_SUCCESS;
+    return guarded([&]() -> iclblasStatus_t {
+        Params p; p.present = P_N | P_M | P_A | P_LDA | P_B | P_LDB | P_C | P_LDC;
+        p.n = n; p.m = m; p.A = A; p.lda = lda; p.B = B; p.ldb = ldb; p.C = C; p.ldc = ldc;
+        VALIDATE(p, h);
+        if (side != ICLBLAS_SIDE_LEFT && side != ICLBLAS_SIDE_RIGHT) return ICLBLAS_STATUS_INVALID_VALUE;
+        if (uplo != ICLBLAS_FILL_MODE_UPPER && uplo != ICLBLAS_FILL_MODE_LOWER) return ICLBLAS_STATUS_INVALID_VALUE;
+        const int na = side == ICLBLAS_SIDE_LEFT ? m : n;
+        Stager st(h);
+        int ia = st.add(A, mat_extent(na, na, lda) * sizeof(float), false);
+        int ib = st.add(B, mat_extent(m, n, ldb) * sizeof(float), false);
+        int ic = st.add(C, mat_extent(m, n, ldc) * sizeof(float), true);
+        cudaError_t e = st.stage_in();
+        if (e == cudaSuccess)
+            e = iclb::ssymm(h, side, uplo, m, n, *alpha, st.dev<float>(ia), lda, st.dev<float>(ib), ldb, *beta,
+                            st.dev<float>(ic), ldc);
+        if (e == cudaSuccess) e = st.finish();
+        return map_cuda(e);
+    });
+}
+
+extern "C" iclblasStatus_t iclblasStrmm(iclblasHandle_t h, iclblasSideMode_t side, iclblasFillMode_t uplo,
+                                        iclblasOperation_t transa, iclblasDiagType_t diag, int m, int n,
+                                        const float* alpha, float* A, int lda, float* B, int ldb, float* C, int ldc)
+{
+    // iclBLAS_S.cpp (Strmm): no early return; the parameter checks end an
+    // m == 0 or n == 0 call successfully
+    return guarded([&]() -> iclblasStatus_t {
+        Params p; p.present = P_N | P_M | P_A | P_LDA | P_B | P_LDB | P_C | P_LDC;
+        p.n = n; p.m = m; p.A = A; p.lda = lda; p.B = B; p.ldb = ldb; p.C = C; p.ldc = ldc;
+        VALIDATE(p, h);
+        if (!alpha) return ICLBLAS_STATUS_INVALID_VALUE;
+        if (side != ICLBLAS_SIDE_LEFT && side != ICLBLAS_SIDE_RIGHT) return ICLBLAS_STATUS_INVALID_VALUE;
+        if (uplo != ICLBLAS_FILL_MODE_UPPER && uplo != ICLBLAS_FILL_MODE_LOWER) return ICLBLAS_STATUS_INVALID_VALUE;
+        if (transa < ICLBLAS_OP_N || transa > ICLBLAS_OP_C) return ICLBLAS_STATUS_INVALID_VALUE;
+        const int na = side == ICLBLAS_SIDE_LEFT ? m : n;
+        Stager st(h);
+        int ia = st.add(A, mat_extent(na, na, lda) * sizeof(float), false);
+        int ib = st.add(B, mat_extent(m, n, ldb) * sizeof(float), false);
+        // C is written in full; its gaps between columns (ldc > m) are kept
+        int ic = st.add(C, mat_extent(m, n, ldc) * sizeof(float), true, ldc > m);
+        cudaError_t e = st.stage_in();
+        if (e == cudaSuccess)
+            e = iclb::strmm(h, side, uplo, transa, diag, m, n, *alpha, st.dev<float>(ia), lda, st.dev<float>(ib), ldb,
+                            st.dev<float>(ic), ldc);
         if (e == cudaSuccess) e = st.finish();
         return map_cuda(e);
     });

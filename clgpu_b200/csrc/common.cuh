@@ -10,6 +10,14 @@ namespace iclb {
 
 constexpr int kWarp = 32;
 
+// Complex product with the reference's fma placement
+// (core/src/ocl/complex.h.cl:32-34): re = fma(a.re, b.re, -(a.im*b.im)),
+// im = fma(a.re, b.im, a.im*b.re), the inner products rounded on their own.
+__device__ __forceinline__ cfloat cmul_fma(cfloat a, cfloat b)
+{
+    return cfloat{fmaf(a.re, b.re, -__fmul_rn(a.im, b.im)), fmaf(a.re, b.im, __fmul_rn(a.im, b.re))};
+}
+
 __device__ __forceinline__ float4 ld_stream4(const float4* p) { return __ldcs(p); }
 __device__ __forceinline__ float ld_stream(const float* p) { return __ldcs(p); }
 

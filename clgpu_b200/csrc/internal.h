@@ -129,6 +129,16 @@ cudaError_t strsv(iclblasHandle_t h, int uplo, int trans, int diag, int n, const
 cudaError_t ctrsv(iclblasHandle_t h, int uplo, int trans, int diag, int n, const cfloat* A, int lda, cfloat* x,
                   int incx);
 
+// rank-1 updates (ger.cu) and symmetric / Hermitian products (symv.cu)
+cudaError_t sger(iclblasHandle_t h, int m, int n, float alpha, const float* x, int incx, const float* y, int incy,
+                 float* A, int lda);
+cudaError_t cger(iclblasHandle_t h, bool conj, int m, int n, cfloat alpha, const cfloat* x, int incx,
+                 const cfloat* y, int incy, cfloat* A, int lda);
+cudaError_t ssymv(iclblasHandle_t h, int uplo, int n, float alpha, const float* A, int lda, const float* x, int incx,
+                  float beta, float* y, int incy);
+cudaError_t chemv(iclblasHandle_t h, int uplo, int n, cfloat alpha, const cfloat* A, int lda, const cfloat* x,
+                  int incx, cfloat beta, cfloat* y, int incy);
+
 // ---------------------------------------------------------------- level 3
 cudaError_t sgemm(iclblasHandle_t h, int transa, int transb, int m, int n, int k, float alpha, const float* A,
                   int lda, const float* B, int ldb, float beta, float* C, int ldc);
@@ -138,6 +148,16 @@ cudaError_t strsm(iclblasHandle_t h, int side, int uplo, int trans, int diag, in
                   const float* A, int lda, float* B, int ldb);
 cudaError_t ctrsm(iclblasHandle_t h, int side, int uplo, int trans, int diag, int m, int n, cfloat alpha,
                   const cfloat* A, int lda, cfloat* B, int ldb);
+
+// GEMM-shaped level-3 routines (level3_ext.cu)
+cudaError_t ssyrk(iclblasHandle_t h, int uplo, int trans, int n, int k, float alpha, const float* A, int lda,
+                  float beta, float* C, int ldc);
+cudaError_t ssyr2k(iclblasHandle_t h, int uplo, int trans, int n, int k, float alpha, const float* A, int lda,
+                   const float* B, int ldb, float beta, float* C, int ldc);
+cudaError_t ssymm(iclblasHandle_t h, int side, int uplo, int m, int n, float alpha, const float* A, int lda,
+                  const float* B, int ldb, float beta, float* C, int ldc);
+cudaError_t strmm(iclblasHandle_t h, int side, int uplo, int transa, int diag, int m, int n, float alpha,
+                  const float* A, int lda, const float* B, int ldb, float* C, int ldc);
 
 // ---------------------------------------------------------------- adjoints
 cudaError_t strsm_backward(iclblasHandle_t h, int side, int uplo, int trans, int diag, int m, int n, float alpha,

@@ -40,12 +40,7 @@ bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 
 __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
 
-// complex product with the reference's fma placement
-// (core/src/ocl/complex.h.cl:32-34)
-__device__ __forceinline__ cfloat cmul(cfloat a, cfloat b)
-{
-    return cfloat{fmaf(a.re, b.re, -mul(a.im, b.im)), fmaf(a.re, b.im, mul(a.im, b.re))};
-}
+__device__ __forceinline__ cfloat cmul(cfloat a, cfloat b) { return cmul_fma(a, b); }
 
 // ---------------------------------------------------------------- ops
 // Each op maps one (x, y) element pair in registers.  kReadY / kWriteX say

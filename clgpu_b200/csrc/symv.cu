@@ -1,0 +1,275 @@
+// Symmetric / Hermitian matrix-vector products: Ssymv (y = alpha A x + beta y,
+// A symmetric) and Chemv (A Hermitian), one triangle of A stored.
+//
+// HBM-bound on the stored triangle (n(n+1)/2 elements).  Each stored element
+// contributes twice -- A(i,j) x_j to y_i and A(i,j) x_i (conjugated for
+// Chemv) to y_j -- so the triangle is read once and both contributions are
+// formed from registers.  The triangle is cut into TS x TS tiles (TS = 128
+// single, 64 complex: 32 lanes x one 16-byte word of rows); one CTA per
+// stored tile (I, J):
+//   - lane l owns rows [l*per, l*per + per) of the tile, warp w the columns
+//     w, w+8, ...; A is read in 16-byte words down each column;
+//   - row contributions sum in registers across the warp's columns and then
+//     across the 8 warps (shared memory);
+//   - column contributions sum over the word in registers and over the 32
+//     lanes of the column (shuffle tree);
+//   - diagonal tiles read only the stored triangle (elements outside it are
+//     selected away, never multiplied) and count the diagonal once; Chemv
+//     takes the diagonal's real part.
+// Tile (I, J) writes its row partial to Q[J][I*TS..] and its column partial
+// to Q[I][J*TS..] (a diagonal tile writes their sum to Q[I][I*TS..]), so
+// every Q entry is written exactly once and no memset is needed.  A second
+// kernel forms y_i = alpha * sum_t Q[t][i] + beta y_i with the sum in FP64 in
+// fixed order (deterministic).  Q adds 2 * n * ceil(n/TS) * sizeof(T) bytes
+// of traffic: 3 % of the triangle's bytes for single, 6 % for complex.
+//
+// beta == 0: y is written without being read (the BLAS convention; the
+// reference's Chemv_naive.cl:46 always reads it).
+#include <algorithm>
+
+#include "common.cuh"
+
+namespace iclb {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+
+bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
+__device__ __forceinline__ float zero_t(float) { return 0.f; }
+__device__ __forceinline__ cfloat zero_t(cfloat) { return cfloat{0.f, 0.f}; }
+__device__ __forceinline__ float conj_t(float v) { return v; }
+__device__ __forceinline__ cfloat conj_t(cfloat v) { return cfloat{v.re, -v.im}; }
+__device__ __forceinline__ float real_part(float v) { return v; }
+__device__ __forceinline__ cfloat real_part(cfloat v) { return cfloat{v.re, 0.f}; }
+__device__ __forceinline__ void mac(float& acc, float a, float b) { acc = fmaf(a, b, acc); }
+__device__ __forceinline__ void mac(cfloat& acc, cfloat a, cfloat b)
+{
+    acc.re = fmaf(a.re, b.re, acc.re);
+    acc.re = fmaf(-a.im, b.im, acc.re);
+    acc.im = fmaf(a.re, b.im, acc.im);
+    acc.im = fmaf(a.im, b.re, acc.im);
+}
+__device__ __forceinline__ float add_t(float a, float b) { return a + b; }
+__device__ __forceinline__ cfloat add_t(cfloat a, cfloat b) { return cfloat{a.re + b.re, a.im + b.im}; }
+__device__ __forceinline__ float shfl_xor_t(float v, int o) { return __shfl_xor_sync(0xffffffffu, v, o); }
+__device__ __forceinline__ cfloat shfl_xor_t(cfloat v, int o)
+{
+    return cfloat{__shfl_xor_sync(0xffffffffu, v.re, o), __shfl_xor_sync(0xffffffffu, v.im, o)};
+}
+
+template <class T>
+struct Tile {
+    static constexpr int per = (int)(16 / sizeof(T));  // elements per 16-byte word
+    static constexpr int TS = 32 * per;                // tile rows = tile columns
+    static constexpr int PASSES = TS / kWarps;         // columns per warp
+};
+
+// Stored tile number t -> (I, J) with I >= J (row-major over the lower block
+// triangle).  Upper storage uses the transposed pair.
+__device__ __forceinline__ void tile_of(long t, int& I, int& J)
+{
+    long i = (long)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+    while ((i + 1) * (i + 2) / 2 <= t) ++i;
+    while (i * (i + 1) / 2 > t) --i;
+    I = (int)i;
+    J = (int)(t - i * (i + 1) / 2);
+}
+
+template <class T, bool LOWER, bool HERM, bool VEC>
+__global__ void __launch_bounds__(kThreads) symv_tile_kernel(int n, const T* __restrict__ A, long lda,
+                                                             const T* __restrict__ x, long incx, T* __restrict__ Q,
+                                                             long qld)
+{
+    using TL = Tile<T>;
+    constexpr int per = TL::per, TS = TL::TS;
+    __shared__ T xr[TS];              // x over the tile's rows
+    __shared__ T xc[TS];              // x over the tile's columns
+    __shared__ T red[kWarps][TS + 1]; // row partials per warp
+    __shared__ T colp[TS];
+
+    int I, J;
+    tile_of(blockIdx.x, I, J);
+    if (!LOWER) {
+        const int t = I;
+        I = J;
+        J = t;
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const long row0 = (long)I * TS, col0 = (long)J * TS;
+    const bool diag = (I == J);
+    for (int k = threadIdx.x; k < TS; k += kThreads) {
+        xr[k] = (row0 + k < n) ? x[(row0 + k) * incx] : zero_t(T());
+        xc[k] = (col0 + k < n) ? x[(col0 + k) * incx] : zero_t(T());
+    }
+    __syncthreads();
+
+    const long r0 = row0 + (long)lane * per;  // first row of this lane's word
+    T racc[per];
+    T xw[per];
+#pragma unroll
+    for (int k = 0; k < per; ++k) {
+        racc[k] = zero_t(T());
+        xw[k] = xr[lane * per + k];
+    }
+    const bool full_word = r0 + per <= n;
+
+    constexpr int B = 4;  // words in flight per thread
+#pragma unroll 1
+    for (int p0 = 0; p0 < TL::PASSES; p0 += B) {
+        T a[B][per];
+#pragma unroll
+        for (int b = 0; b < B; ++b) {
+            const long c = col0 + w + (long)(p0 + b) * kWarps;
+            if (c < n && r0 < n) {
+                const T* src = A + c * lda + r0;
+                if (VEC && full_word) {
+                    float4 v = ld_stream4((const float4*)src);
+                    const T* e = (const T*)&v;
+#pragma unroll
+                    for (int k = 0; k < per; ++k) a[b][k] = e[k];
+                } else {
+#pragma unroll
+                    for (int k = 0; k < per; ++k) a[b][k] = (r0 + k < n) ? src[k] : zero_t(T());
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < per; ++k) a[b][k] = zero_t(T());
+            }
+        }
+#pragma unroll
+        for (int b = 0; b < B; ++b) {
+            const int cl = w + (p0 + b) * kWarps;  // column within the tile
+            const long c = col0 + cl;
+            const T xcv = xc[cl];
+            T csum = zero_t(T());
+#pragma unroll
+            for (int k = 0; k < per; ++k) {
+                const long r = r0 + k;
+                T v = a[b][k];
+                bool in_row = true, in_col = true;
+                if (diag) {
+                    // stored triangle only; the diagonal counts once (as a row term)
+                    in_row = LOWER ? (r >= c) : (r <= c);
+                    in_col = LOWER ? (r > c) : (r < c);
+                    if (r == c && HERM) v = real_part(v);
+                }
+                if (in_row) mac(racc[k], v, xcv);
+                if (in_col) mac(csum, HERM ? conj_t(v) : v, xw[k]);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) csum = add_t(csum, shfl_xor_t(csum, o));
+            if (lane == 0) colp[cl] = csum;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < per; ++k) red[w][lane * per + k] = racc[k];
+    __syncthreads();
+    for (int k = threadIdx.x; k < TS; k += kThreads) {
+        T s = red[0][k];
+#pragma unroll
+        for (int ww = 1; ww < kWarps; ++ww) s = add_t(s, red[ww][k]);
+        if (diag) {
+            Q[(long)I * qld + row0 + k] = add_t(s, colp[k]);
+        } else {
+            Q[(long)J * qld + row0 + k] = s;         // to y over the tile's rows
+            Q[(long)I * qld + col0 + k] = colp[k];   // to y over the tile's columns
+        }
+    }
+}
+
+__device__ __forceinline__ void acc_d(double& re, double& im, float v)
+{
+    re += (double)v;
+    (void)im;
+}
+__device__ __forceinline__ void acc_d(double& re, double& im, cfloat v)
+{
+    re += (double)v.re;
+    im += (double)v.im;
+}
+
+// y_i = alpha * sum_t Q[t][i] + beta * y_i, the reference's final expressions
+// (Ssymv_naive_lower.cl:34-37, Chemv_naive.cl:45-46) on the FP64 sum rounded
+// to T.
+__global__ void __launch_bounds__(kThreads) symv_finish_kernel(int n, int nb, const float* __restrict__ Q, long qld,
+                                                               float alpha, float beta, float* y, long incy)
+{
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double s = 0.0, unused = 0.0;
+    for (int t = 0; t < nb; ++t) acc_d(s, unused, Q[(long)t * qld + i]);
+    const float r = (float)s;
+    float* yp = y + i * incy;
+    *yp = (beta != 0.f) ? fmaf(alpha, r, __fmul_rn(beta, *yp)) : __fmul_rn(alpha, r);
+}
+
+__global__ void __launch_bounds__(kThreads) hemv_finish_kernel(int n, int nb, const cfloat* __restrict__ Q, long qld,
+                                                               cfloat alpha, cfloat beta, cfloat* y, long incy)
+{
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double re = 0.0, im = 0.0;
+    for (int t = 0; t < nb; ++t) acc_d(re, im, Q[(long)t * qld + i]);
+    const cfloat r = cmul_fma(cfloat{(float)re, (float)im}, alpha);
+    cfloat* yp = y + i * incy;
+    if (beta.re != 0.f || beta.im != 0.f) {
+        const cfloat b = cmul_fma(beta, *yp);
+        *yp = cfloat{__fadd_rn(b.re, r.re), __fadd_rn(b.im, r.im)};
+    } else {
+        *yp = r;
+    }
+}
+
+template <class T, bool HERM>
+cudaError_t symv_tiles(iclblasHandle_t h, bool lower, int n, const T* A, int lda, const T* x, int incx, T* Q,
+                       long qld, int nb)
+{
+    const long tiles = (long)nb * (nb + 1) / 2;
+    const bool vec = aligned16(A) && lda % Tile<T>::per == 0;
+    const unsigned grid = (unsigned)tiles;
+#define SYMV_LAUNCH(L, V) \
+    symv_tile_kernel<T, L, HERM, V><<<grid, kThreads, 0, h->stream>>>(n, A, lda, x, incx, Q, qld)
+    if (lower) {
+        if (vec) SYMV_LAUNCH(true, true); else SYMV_LAUNCH(true, false);
+    } else {
+        if (vec) SYMV_LAUNCH(false, true); else SYMV_LAUNCH(false, false);
+    }
+#undef SYMV_LAUNCH
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t ssymv(iclblasHandle_t h, int uplo, int n, float alpha, const float* A, int lda, const float* x, int incx,
+                  float beta, float* y, int incy)
+{
+    constexpr int TS = Tile<float>::TS;
+    const int nb = (n + TS - 1) / TS;
+    const long qld = (long)nb * TS;
+    float* Q = (float*)scratch(h, sizeof(float) * (size_t)nb * (size_t)qld);
+    if (!Q) return cudaErrorMemoryAllocation;
+    cudaError_t e = symv_tiles<float, false>(h, uplo == ICLBLAS_FILL_MODE_LOWER, n, A, lda, x, incx, Q, qld, nb);
+    if (e != cudaSuccess) return e;
+    symv_finish_kernel<<<(n + kThreads - 1) / kThreads, kThreads, 0, h->stream>>>(n, nb, Q, qld, alpha, beta, y,
+                                                                                  incy);
+    return cudaGetLastError();
+}
+
+cudaError_t chemv(iclblasHandle_t h, int uplo, int n, cfloat alpha, const cfloat* A, int lda, const cfloat* x,
+                  int incx, cfloat beta, cfloat* y, int incy)
+{
+    constexpr int TS = Tile<cfloat>::TS;
+    const int nb = (n + TS - 1) / TS;
+    const long qld = (long)nb * TS;
+    cfloat* Q = (cfloat*)scratch(h, sizeof(cfloat) * (size_t)nb * (size_t)qld);
+    if (!Q) return cudaErrorMemoryAllocation;
+    cudaError_t e = symv_tiles<cfloat, true>(h, uplo == ICLBLAS_FILL_MODE_LOWER, n, A, lda, x, incx, Q, qld, nb);
+    if (e != cudaSuccess) return e;
+    hemv_finish_kernel<<<(n + kThreads - 1) / kThreads, kThreads, 0, h->stream>>>(n, nb, Q, qld, alpha, beta, y,
+                                                                                  incy);
+    return cudaGetLastError();
+}
+
+}  // namespace iclb

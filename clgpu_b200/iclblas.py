@@ -100,6 +100,15 @@ _SIGS = {
     "iclblasCrot": [_H, _I, _P, _I, _P, _I, _P, _P],
     "iclblasCsrot": [_H, _I, _P, _I, _P, _I, _P, _P],
     "iclblasCrotg": [_H, _P, _P, _P, _P],
+    "iclblasSger": [_H, _I, _I, _P, _P, _I, _P, _I, _P, _I],
+    "iclblasCgeru": [_H, _I, _I, _P, _P, _I, _P, _I, _P, _I],
+    "iclblasCgerc": [_H, _I, _I, _P, _P, _I, _P, _I, _P, _I],
+    "iclblasSsymv": [_H, _I, _I, _P, _P, _I, _P, _I, _P, _P, _I],
+    "iclblasChemv": [_H, _I, _I, _P, _P, _I, _P, _I, _P, _P, _I],
+    "iclblasSsyrk": [_H, _I, _I, _I, _I, _P, _P, _I, _P, _P, _I],
+    "iclblasSsyr2k": [_H, _I, _I, _I, _I, _P, _P, _I, _P, _I, _P, _P, _I],
+    "iclblasSsymm": [_H, _I, _I, _I, _I, _P, _P, _I, _P, _I, _P, _P, _I],
+    "iclblasStrmm": [_H, _I, _I, _I, _I, _I, _I, _P, _P, _I, _P, _I, _P, _I],
     "iclblasStrsv": [_H, _I, _I, _I, _I, _P, _I, _P, _I],
     "iclblasCtrsv": [_H, _I, _I, _I, _I, _P, _I, _P, _I],
     "iclblasSgemv": [_H, _I, _I, _I, _P, _P, _I, _P, _I, _P, _P, _I],
@@ -341,6 +350,48 @@ def iclblasCsrot(h, n, x, incx, y, incy, c, s):
 def iclblasCrotg(h, a, b, c, s):
     """a, b, s: one-element complex64 arrays; c: one-element float array."""
     return _call("iclblasCrotg", _h(h), ptr(a), ptr(b), ptr(c), ptr(s))
+
+
+def iclblasSger(h, m, n, alpha, x, incx, y, incy, A, lda):
+    return _call("iclblasSger", _h(h), m, n, C.byref(_fscalar(alpha)), ptr(x), incx, ptr(y), incy, ptr(A), lda)
+
+
+def iclblasCgeru(h, m, n, alpha, x, incx, y, incy, A, lda):
+    return _call("iclblasCgeru", _h(h), m, n, C.byref(_cscalar(alpha)), ptr(x), incx, ptr(y), incy, ptr(A), lda)
+
+
+def iclblasCgerc(h, m, n, alpha, x, incx, y, incy, A, lda):
+    return _call("iclblasCgerc", _h(h), m, n, C.byref(_cscalar(alpha)), ptr(x), incx, ptr(y), incy, ptr(A), lda)
+
+
+def iclblasSsymv(h, uplo, n, alpha, A, lda, x, incx, beta, y, incy):
+    return _call("iclblasSsymv", _h(h), uplo, n, C.byref(_fscalar(alpha)), ptr(A), lda, ptr(x), incx,
+                 C.byref(_fscalar(beta)), ptr(y), incy)
+
+
+def iclblasChemv(h, uplo, n, alpha, A, lda, x, incx, beta, y, incy):
+    return _call("iclblasChemv", _h(h), uplo, n, C.byref(_cscalar(alpha)), ptr(A), lda, ptr(x), incx,
+                 C.byref(_cscalar(beta)), ptr(y), incy)
+
+
+def iclblasSsyrk(h, uplo, trans, n, k, alpha, A, lda, beta, Cm, ldc):
+    return _call("iclblasSsyrk", _h(h), uplo, trans, n, k, C.byref(_fscalar(alpha)), ptr(A), lda,
+                 C.byref(_fscalar(beta)), ptr(Cm), ldc)
+
+
+def iclblasSsyr2k(h, uplo, trans, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc):
+    return _call("iclblasSsyr2k", _h(h), uplo, trans, n, k, C.byref(_fscalar(alpha)), ptr(A), lda, ptr(B), ldb,
+                 C.byref(_fscalar(beta)), ptr(Cm), ldc)
+
+
+def iclblasSsymm(h, side, uplo, m, n, alpha, A, lda, B, ldb, beta, Cm, ldc):
+    return _call("iclblasSsymm", _h(h), side, uplo, m, n, C.byref(_fscalar(alpha)), ptr(A), lda, ptr(B), ldb,
+                 C.byref(_fscalar(beta)), ptr(Cm), ldc)
+
+
+def iclblasStrmm(h, side, uplo, transa, diag, m, n, alpha, A, lda, B, ldb, Cm, ldc):
+    return _call("iclblasStrmm", _h(h), side, uplo, transa, diag, m, n, C.byref(_fscalar(alpha)), ptr(A), lda,
+                 ptr(B), ldb, ptr(Cm), ldc)
 
 
 def iclblasStrsv(h, uplo, trans, diag, n, A, lda, x, incx):

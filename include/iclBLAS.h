@@ -208,6 +208,26 @@ ICLBLAS_API iclblasStatus_t iclblasCgemv(iclblasHandle_t handle, iclblasOperatio
 ICLBLAS_API iclblasStatus_t iclblasCtrsv(iclblasHandle_t handle, iclblasFillMode_t uplo, iclblasOperation_t trans, iclblasDiagType_t diag,
                                          int n, oclComplex_t* A, int lda, oclComplex_t* x, int incx);
 
+/* ---- level 2: rank-1 updates, symmetric / Hermitian products ----
+ * Ssymv / Chemv read only the uplo triangle of A (Chemv takes the real part
+ * of its diagonal); beta == 0 writes y without reading it. */
+/* replaces iclBLAS.h:727 */
+ICLBLAS_API iclblasStatus_t iclblasSger(iclblasHandle_t handle, int m, int n, const float* alpha, float* x, int incx, float* y, int incy,
+                                        float* A, int lda);
+/* replaces iclBLAS.h:1018 */
+ICLBLAS_API iclblasStatus_t iclblasSsymv(iclblasHandle_t handle, iclblasFillMode_t uplo, int n, const float* alpha, float* A, int lda,
+                                         float* x, int incx, const float* beta, float* y, int incy);
+/* replaces iclBLAS.h:1112 */
+ICLBLAS_API iclblasStatus_t iclblasCgeru(iclblasHandle_t handle, int m, int n, const oclComplex_t* alpha, oclComplex_t* x, int incx,
+                                         oclComplex_t* y, int incy, oclComplex_t* A, int lda);
+/* replaces iclBLAS.h:1133 */
+ICLBLAS_API iclblasStatus_t iclblasCgerc(iclblasHandle_t handle, int m, int n, const oclComplex_t* alpha, oclComplex_t* x, int incx,
+                                         oclComplex_t* y, int incy, oclComplex_t* A, int lda);
+/* replaces iclBLAS.h:1205 */
+ICLBLAS_API iclblasStatus_t iclblasChemv(iclblasHandle_t handle, iclblasFillMode_t uplo, int n, const oclComplex_t* alpha,
+                                         oclComplex_t* A, int lda, oclComplex_t* x, int incx, const oclComplex_t* beta,
+                                         oclComplex_t* y, int incy);
+
 /* ---- level 3 ---- */
 /* replaces iclBLAS.h:1685 */
 ICLBLAS_API iclblasStatus_t iclblasSgemm(iclblasHandle_t handle, iclblasOperation_t transa, iclblasOperation_t transb, int m, int n, int k,
@@ -223,6 +243,26 @@ ICLBLAS_API iclblasStatus_t iclblasCgemm(iclblasHandle_t handle, iclblasOperatio
 ICLBLAS_API iclblasStatus_t iclblasCtrsm(iclblasHandle_t handle, iclblasSideMode_t side, iclblasFillMode_t uplo, iclblasOperation_t trans,
                                          iclblasDiagType_t diag, int m, int n, const oclComplex_t* alpha, oclComplex_t* A, int lda,
                                          oclComplex_t* B, int ldb);
+
+/* ---- level 3 on the GEMM engine (the handle's math mode applies) ----
+ * Ssyrk / Ssyr2k update only the uplo triangle of C; Ssymm reads only the
+ * uplo triangle of A.  beta == 0 writes C without reading it.  Strmm computes
+ * the documented C = alpha op(A) B (left) or alpha B op(A) (right) with A
+ * triangular (uplo, diag) into a separate C, which may be B itself: an
+ * overlapping C gets the product of the original B. */
+/* replaces iclBLAS.h:1579 */
+ICLBLAS_API iclblasStatus_t iclblasSsymm(iclblasHandle_t handle, iclblasSideMode_t side, iclblasFillMode_t uplo, int m, int n,
+                                         const float* alpha, float* A, int lda, float* B, int ldb, const float* beta, float* C, int ldc);
+/* replaces iclBLAS.h:1608 */
+ICLBLAS_API iclblasStatus_t iclblasSsyrk(iclblasHandle_t handle, iclblasFillMode_t uplo, iclblasOperation_t trans, int n, int k,
+                                         const float* alpha, float* A, int lda, const float* beta, float* C, int ldc);
+/* replaces iclBLAS.h:1645 */
+ICLBLAS_API iclblasStatus_t iclblasSsyr2k(iclblasHandle_t handle, iclblasFillMode_t uplo, iclblasOperation_t trans, int n, int k,
+                                          const float* alpha, float* A, int lda, float* B, int ldb, const float* beta, float* C, int ldc);
+/* replaces iclBLAS.h:1753 */
+ICLBLAS_API iclblasStatus_t iclblasStrmm(iclblasHandle_t handle, iclblasSideMode_t side, iclblasFillMode_t uplo, iclblasOperation_t transa,
+                                         iclblasDiagType_t diag, int m, int n, const float* alpha, float* A, int lda, float* B, int ldb,
+                                         float* C, int ldc);
 
 /* ======================================================================== */
 /* Extensions (new symbols; no reference counterpart).                      */

@@ -74,6 +74,18 @@ inline complex_t cfmaf(complex_t a, float b, complex_t c) { return fma(a, float2
 inline float sign(float v) { return v > 0.f ? 1.f : (v < 0.f ? -1.f : 0.f); }
 
 namespace clshim {
+// Runs a 2-D NDRange of gws0 x gws1 work-items sequentially.
+template <class F>
+inline void run_ndrange2(size_t gws0, size_t gws1, F&& f)
+{
+    for (size_t j = 0; j < gws1; ++j)
+        for (size_t i = 0; i < gws0; ++i) {
+            g_gid[0] = i;
+            g_gid[1] = j;
+            f();
+        }
+    g_gid[0] = g_gid[1] = 0;
+}
 // Runs a 1-D NDRange of `gws` work-items sequentially.
 template <class F>
 inline void run_ndrange(size_t gws, F&& f)

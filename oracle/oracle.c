@@ -804,3 +804,193 @@ void orc_dtrsm(int side, int uplo, int trans, int diag, int m, int n, double alp
         free(z);
     }
 }
+
+/* ------------------------------------------------------------------------ */
+/* Rank-1 updates, symmetric / Hermitian products, GEMM-shaped level 3      */
+/* ------------------------------------------------------------------------ */
+
+/* A(i,j) = fma(alpha, x_i*y_j, A(i,j)) in FP32: Sger_naive.cl:16-26 (the
+ * product rounded, then mad, restated as fmaf). */
+void orc_sger(int m, int n, float alpha, const float* x, int incx, const float* y, int incy, float* A, int lda)
+{
+    for (long j = 0; j < n; ++j)
+        for (long i = 0; i < m; ++i) {
+            const float p = x[i * incx] * y[j * incy];
+            A[j * lda + i] = fmaf(alpha, p, A[j * lda + i]);
+        }
+}
+
+/* A(i,j) += cmul(alpha, cmul(x_i, y_j or conj(y_j))) in FP32 with the
+ * reference's fma placement: Cgeru_naive.cl:18-33, Cgerc_naive.cl:18-32. */
+void orc_cger(int conj, int m, int n, orc_c32 alpha, const orc_c32* x, int incx, const orc_c32* y, int incy,
+              orc_c32* A, int lda)
+{
+    for (long j = 0; j < n; ++j) {
+        orc_c32 yv = y[j * incy];
+        if (conj) yv.im = -yv.im;
+        for (long i = 0; i < m; ++i) {
+            const orc_c32 t = cmul_fma(alpha, cmul_fma(x[i * incx], yv));
+            orc_c32* a = A + j * lda + i;
+            a->re = a->re + t.re;
+            a->im = a->im + t.im;
+        }
+    }
+}
+
+/* element (r, c) of the symmetric / Hermitian matrix whose uplo triangle is
+ * stored in A (tests/blas_funcs/test_symv.hpp:54-76: the other triangle read
+ * transposed, conjugated for Hermitian; a Hermitian diagonal's imaginary part
+ * is taken as 0) */
+static cd sym_elem(int uplo, int herm, const orc_c32* A, int lda, int r, int c)
+{
+    const int upper = (uplo == 0);
+    cd v;
+    if ((upper && c < r) || (!upper && c > r)) {
+        v = cd_of(A[(long)r * lda + c]);
+        if (herm) v = cd_conj(v);
+    } else {
+        v = cd_of(A[(long)c * lda + r]);
+    }
+    if (herm && r == c) v.im = 0.0;
+    return v;
+}
+
+/* y = alpha A x + beta y, A symmetric (uplo triangle stored).  The sum
+ * (A x)_r is cpu_symv's (tests/blas_funcs/test_symv.hpp:21-87: the element
+ * choice, accumulated in double), rounded to float once; the final step is
+ * the reference kernel's FP32 expression (Ssymv_naive_lower.cl:34-37:
+ * beta != 0 ? fma(alpha, s, beta*y) : alpha*s), so beta == 0 does not read
+ * y. */
+void orc_ssymv(int uplo, int n, float alpha, const float* A, int lda, const float* x, int incx, float beta, float* y,
+               int incy)
+{
+    const int upper = (uplo == 0);
+    for (int r = 0; r < n; ++r) {
+        double acc = 0.0;
+        for (int c = 0; c < n; ++c) {
+            const double a = ((upper && c < r) || (!upper && c > r)) ? A[(long)r * lda + c] : A[(long)c * lda + r];
+            acc += a * (double)x[(long)c * incx];
+        }
+        const float s = (float)acc;
+        float* yp = y + (long)r * incy;
+        *yp = (beta != 0.0f) ? fmaf(alpha, s, beta * *yp) : alpha * s;
+    }
+}
+
+/* Complex Hermitian y = alpha A x + beta y: the sum as cpu_symv<complex,
+ * true> (test_symv.hpp) in double, rounded once; then the reference kernel's
+ * FP32 step (Chemv_naive.cl:45-46: y = cmul(beta, y) + cmul(s, alpha), fma
+ * placement of complex.h.cl:32-34).  That kernel reads y even for beta == 0;
+ * here beta == 0 means y = cmul(s, alpha) without reading y.  (The FP32 final
+ * step matters: the reference's own test_Chemv.cpp naive_low_3x3 expects the
+ * FP32 cancellation of its 33.7 - 28.4 imaginary part, 5.2999954, which a
+ * double evaluation, 5.2999987, misses by 7 ulps.) */
+void orc_chemv(int uplo, int n, orc_c32 alpha, const orc_c32* A, int lda, const orc_c32* x, int incx, orc_c32 beta,
+               orc_c32* y, int incy)
+{
+    const int beta_zero = (beta.re == 0.0f && beta.im == 0.0f);
+    for (int r = 0; r < n; ++r) {
+        cd acc = cd_make(0, 0);
+        for (int c = 0; c < n; ++c) acc = cd_add(acc, cd_mul(sym_elem(uplo, 1, A, lda, r, c), cd_of(x[(long)c * incx])));
+        const orc_c32 s = c32_of(acc);
+        const orc_c32 t = cmul_fma(s, alpha);
+        orc_c32* yp = y + (long)r * incy;
+        if (beta_zero) {
+            *yp = t;
+        } else {
+            const orc_c32 b = cmul_fma(beta, *yp);
+            yp->re = b.re + t.re;
+            yp->im = b.im + t.im;
+        }
+    }
+}
+
+/* C = alpha op(A) op(B)^T (+ alpha op(B) op(A)^T when B != NULL) + beta C on
+ * the uplo triangle of C (upper 0, lower 1); op(X) = X (n x k) for trans == 0,
+ * X^T (X k x n) otherwise.  Restates Ssyrk_naive.cl:18-48 and
+ * Ssyr2k_naive.cl:18-49 in double; beta == 0 means C is not read (the
+ * kernels read it). */
+void orc_ssyr2k(int uplo, int trans, int n, int k, float alpha, const float* A, int lda, const float* B, int ldb,
+                float beta, float* C, int ldc)
+{
+    const int lower = (uplo == 1);
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i) {
+            if (lower ? (i < j) : (i > j)) continue;
+            double acc = 0.0;
+            for (int l = 0; l < k; ++l) {
+                const double ai = trans ? A[(long)i * lda + l] : A[(long)l * lda + i];
+                const double aj = trans ? A[(long)j * lda + l] : A[(long)l * lda + j];
+                if (!B) {
+                    acc += ai * aj;
+                } else {
+                    const double bi = trans ? B[(long)i * ldb + l] : B[(long)l * ldb + i];
+                    const double bj = trans ? B[(long)j * ldb + l] : B[(long)l * ldb + j];
+                    acc += ai * bj + bi * aj;
+                }
+            }
+            double out = (double)alpha * acc;
+            if (beta != 0.0f) out += (double)beta * (double)C[(long)j * ldc + i];
+            C[(long)j * ldc + i] = (float)out;
+        }
+}
+
+void orc_ssyrk(int uplo, int trans, int n, int k, float alpha, const float* A, int lda, float beta, float* C, int ldc)
+{
+    orc_ssyr2k(uplo, trans, n, k, alpha, A, lda, NULL, 0, beta, C, ldc);
+}
+
+/* C = alpha A B + beta C (side 0) or alpha B A + beta C (side 1), A
+ * symmetric with its uplo triangle stored: Ssymm_naive.cl:18-75 in double;
+ * beta == 0: C not read. */
+void orc_ssymm(int side, int uplo, int m, int n, float alpha, const float* A, int lda, const float* B, int ldb,
+               float beta, float* C, int ldc)
+{
+    const int upper = (uplo == 0);
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < m; ++i) {
+            double acc = 0.0;
+            const int kk = side == 0 ? m : n;
+            for (int l = 0; l < kk; ++l) {
+                int r = side == 0 ? i : l, c = side == 0 ? l : j;   /* A_sym(r, c) */
+                const double a = ((upper && c < r) || (!upper && c > r)) ? A[(long)r * lda + c] : A[(long)c * lda + r];
+                const double b = side == 0 ? B[(long)j * ldb + l] : B[(long)l * ldb + i];
+                acc += a * b;
+            }
+            double out = (double)alpha * acc;
+            if (beta != 0.0f) out += (double)beta * (double)C[(long)j * ldc + i];
+            C[(long)j * ldc + i] = (float)out;
+        }
+}
+
+/* C = alpha op(A) B (side 0) or alpha B op(A) (side 1), A triangular
+ * (uplo 0 upper / 1 lower, diag 1 unit), op by transa (1 and 2 both
+ * transpose: real data).  The operation documented by the reference's header
+ * (include/iclBLAS/iclBLAS.h:1720-1753), in double; C may be B. */
+void orc_strmm(int side, int uplo, int transa, int diag, int m, int n, float alpha, const float* A, int lda,
+               const float* B, int ldb, float* C, int ldc)
+{
+    const int lower = (uplo == 1), unit = (diag == 1), tr = (transa != 0);
+    const int na = side == 0 ? m : n;
+    double* out = (double*)malloc(sizeof(double) * (size_t)m * (size_t)n);
+    if (!out) return;
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < m; ++i) {
+            double acc = 0.0;
+            for (int l = 0; l < na; ++l) {
+                /* op(A)(r, c) */
+                const int r = side == 0 ? i : l, c = side == 0 ? l : j;
+                const int ar = tr ? c : r, ac = tr ? r : c;   /* element of A */
+                double a;
+                if (ar == ac) a = unit ? 1.0 : A[(long)ac * lda + ar];
+                else if (lower ? (ar > ac) : (ar < ac)) a = A[(long)ac * lda + ar];
+                else a = 0.0;
+                const double b = side == 0 ? B[(long)j * ldb + l] : B[(long)l * ldb + i];
+                acc += a * b;
+            }
+            out[(size_t)j * m + i] = (double)alpha * acc;
+        }
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < m; ++i) C[(long)j * ldc + i] = (float)out[(size_t)j * m + i];
+    free(out);
+}

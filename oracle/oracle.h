@@ -56,6 +56,22 @@ void  orc_srotg(float* a, float* b, float* c, float* s);
 void  orc_crotg(orc_c32* a, orc_c32* b, float* c, orc_c32* s);
 void  orc_srotmg(float* d1, float* d2, float* x1, float y1, float* param);
 
+/* ---- rank-1 updates, symmetric / Hermitian products, level 3 on GEMM ---- */
+void orc_sger(int m, int n, float alpha, const float* x, int incx, const float* y, int incy, float* A, int lda);
+void orc_cger(int conj, int m, int n, orc_c32 alpha, const orc_c32* x, int incx, const orc_c32* y, int incy,
+              orc_c32* A, int lda);
+void orc_ssymv(int uplo, int n, float alpha, const float* A, int lda, const float* x, int incx, float beta, float* y,
+               int incy);
+void orc_chemv(int uplo, int n, orc_c32 alpha, const orc_c32* A, int lda, const orc_c32* x, int incx, orc_c32 beta,
+               orc_c32* y, int incy);
+void orc_ssyrk(int uplo, int trans, int n, int k, float alpha, const float* A, int lda, float beta, float* C, int ldc);
+void orc_ssyr2k(int uplo, int trans, int n, int k, float alpha, const float* A, int lda, const float* B, int ldb,
+                float beta, float* C, int ldc);
+void orc_ssymm(int side, int uplo, int m, int n, float alpha, const float* A, int lda, const float* B, int ldb,
+               float beta, float* C, int ldc);
+void orc_strmm(int side, int uplo, int transa, int diag, int m, int n, float alpha, const float* A, int lda,
+               const float* B, int ldb, float* C, int ldc);
+
 /* ---- level 2 ---- */
 void orc_sgemv(int trans, int m, int n, float alpha, const float* A, int lda,
                const float* x, int incx, float beta, float* y, int incy);

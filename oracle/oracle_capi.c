@@ -410,3 +410,113 @@ iclblasStatus_t iclblasSrotmg(iclblasHandle_t h, float* d1, float* d2, float* x1
     orc_srotmg(d1, d2, x1, *y1, param);
     return ICLBLAS_STATUS_SUCCESS;
 }
+
+/* ---- rank-1 updates and symmetric / Hermitian products (iclBLAS_S.cpp,
+ *      iclBLAS_C.cpp: Sger, Ssymv, Cgeru, Cgerc, Chemv) ---- */
+iclblasStatus_t iclblasSger(iclblasHandle_t h, int m, int n, const float* alpha, float* x, int incx, float* y, int incy,
+                            float* A, int lda)
+{
+    if (m == 0 || n == 0 || *alpha == 0.f) return ICLBLAS_STATUS_SUCCESS;
+    if (m < 0 || n < 0 || incx == 0 || incy == 0) return ICLBLAS_STATUS_INVALID_VALUE;
+    vparams p = { P_N | P_M | P_X | P_INCX | P_Y | P_INCY | P_A | P_LDA, .n = n, .m = m, .incx = incx, .incy = incy,
+                  .lda = lda, .x = x, .y = y, .A = A };
+    CHECK(p, h);
+    orc_sger(m, n, *alpha, x, incx, y, incy, A, lda);
+    return ICLBLAS_STATUS_SUCCESS;
+}
+
+static iclblasStatus_t cger_orc(iclblasHandle_t h, int conj, int m, int n, const oclComplex_t* alpha, oclComplex_t* x,
+                                int incx, oclComplex_t* y, int incy, oclComplex_t* A, int lda)
+{
+    if (m == 0 || n == 0 || (alpha->val[0] == 0.f && alpha->val[1] == 0.f)) return ICLBLAS_STATUS_SUCCESS;
+    if (m < 0 || n < 0 || incx == 0) return ICLBLAS_STATUS_INVALID_VALUE;
+    vparams p = { P_N | P_M | P_X | P_INCX | P_Y | P_INCY | P_A | P_LDA, .n = n, .m = m, .incx = incx, .incy = incy,
+                  .lda = lda, .x = x, .y = y, .A = A };
+    CHECK(p, h);
+    orc_cger(conj, m, n, c32(alpha), (const orc_c32*)x, incx, (const orc_c32*)y, incy, (orc_c32*)A, lda);
+    return ICLBLAS_STATUS_SUCCESS;
+}
+
+iclblasStatus_t iclblasCgeru(iclblasHandle_t h, int m, int n, const oclComplex_t* alpha, oclComplex_t* x, int incx,
+                             oclComplex_t* y, int incy, oclComplex_t* A, int lda)
+{
+    return cger_orc(h, 0, m, n, alpha, x, incx, y, incy, A, lda);
+}
+
+iclblasStatus_t iclblasCgerc(iclblasHandle_t h, int m, int n, const oclComplex_t* alpha, oclComplex_t* x, int incx,
+                             oclComplex_t* y, int incy, oclComplex_t* A, int lda)
+{
+    return cger_orc(h, 1, m, n, alpha, x, incx, y, incy, A, lda);
+}
+
+iclblasStatus_t iclblasSsymv(iclblasHandle_t h, iclblasFillMode_t uplo, int n, const float* alpha, float* A, int lda,
+                             float* x, int incx, const float* beta, float* y, int incy)
+{
+    if (n == 0 || (*alpha == 0.f && *beta == 1.f)) return ICLBLAS_STATUS_SUCCESS;
+    if (n < 0 || incx == 0 || incy == 0) return ICLBLAS_STATUS_INVALID_VALUE;
+    vparams p = { P_N | P_X | P_INCX | P_Y | P_INCY | P_A | P_LDA, .n = n, .incx = incx, .incy = incy, .lda = lda,
+                  .x = x, .y = y, .A = A };
+    CHECK(p, h);
+    orc_ssymv(uplo, n, *alpha, A, lda, x, incx, *beta, y, incy);
+    return ICLBLAS_STATUS_SUCCESS;
+}
+
+iclblasStatus_t iclblasChemv(iclblasHandle_t h, iclblasFillMode_t uplo, int n, const oclComplex_t* alpha,
+                             oclComplex_t* A, int lda, oclComplex_t* x, int incx, const oclComplex_t* beta,
+                             oclComplex_t* y, int incy)
+{
+    if (n == 0 || (alpha->val[0] == 0.f && alpha->val[1] == 0.f && beta->val[0] == 1.f && beta->val[1] == 0.f))
+        return ICLBLAS_STATUS_SUCCESS;
+    if (n < 0 || incx == 0 || incy == 0) return ICLBLAS_STATUS_INVALID_VALUE;
+    vparams p = { P_N | P_X | P_INCX | P_Y | P_INCY | P_A | P_LDA, .n = n, .incx = incx, .incy = incy, .lda = lda,
+                  .x = x, .y = y, .A = A };
+    CHECK(p, h);
+    orc_chemv(uplo, n, c32(alpha), (const orc_c32*)A, lda, (const orc_c32*)x, incx, c32(beta), (orc_c32*)y, incy);
+    return ICLBLAS_STATUS_SUCCESS;
+}
+
+/* ---- level 3 (iclBLAS_S.cpp: Ssymm, Ssyrk, Ssyr2k, Strmm) ---- */
+iclblasStatus_t iclblasSsyrk(iclblasHandle_t h, iclblasFillMode_t uplo, iclblasOperation_t trans, int n, int k,
+                             const float* alpha, float* A, int lda, const float* beta, float* C, int ldc)
+{
+    if (n == 0 || k == 0 || (*alpha == 0.f && *beta == 1.f)) return ICLBLAS_STATUS_SUCCESS;
+    vparams p = { P_N | P_K | P_A | P_LDA | P_C | P_LDC, .n = n, .k = k, .lda = lda, .ldc = ldc, .A = A, .C = C };
+    CHECK(p, h);
+    orc_ssyrk(uplo, trans != ICLBLAS_OP_N, n, k, *alpha, A, lda, *beta, C, ldc);
+    return ICLBLAS_STATUS_SUCCESS;
+}
+
+iclblasStatus_t iclblasSsyr2k(iclblasHandle_t h, iclblasFillMode_t uplo, iclblasOperation_t trans, int n, int k,
+                              const float* alpha, float* A, int lda, float* B, int ldb, const float* beta, float* C,
+                              int ldc)
+{
+    if (n == 0 || k == 0 || (*alpha == 0.f && *beta == 1.f)) return ICLBLAS_STATUS_SUCCESS;
+    vparams p = { P_N | P_K | P_A | P_LDA | P_B | P_LDB | P_C | P_LDC, .n = n, .k = k, .lda = lda, .ldb = ldb,
+                  .ldc = ldc, .A = A, .B = B, .C = C };
+    CHECK(p, h);
+    orc_ssyr2k(uplo, trans != ICLBLAS_OP_N, n, k, *alpha, A, lda, B, ldb, *beta, C, ldc);
+    return ICLBLAS_STATUS_SUCCESS;
+}
+
+iclblasStatus_t iclblasSsymm(iclblasHandle_t h, iclblasSideMode_t side, iclblasFillMode_t uplo, int m, int n,
+                             const float* alpha, float* A, int lda, float* B, int ldb, const float* beta, float* C,
+                             int ldc)
+{
+    if (n == 0 || m == 0 || (*alpha == 0.f && *beta == 1.f)) return ICLBLAS_STATUS_SUCCESS;
+    vparams p = { P_N | P_M | P_A | P_LDA | P_B | P_LDB | P_C | P_LDC, .n = n, .m = m, .lda = lda, .ldb = ldb,
+                  .ldc = ldc, .A = A, .B = B, .C = C };
+    CHECK(p, h);
+    orc_ssymm(side, uplo, m, n, *alpha, A, lda, B, ldb, *beta, C, ldc);
+    return ICLBLAS_STATUS_SUCCESS;
+}
+
+iclblasStatus_t iclblasStrmm(iclblasHandle_t h, iclblasSideMode_t side, iclblasFillMode_t uplo,
+                             iclblasOperation_t transa, iclblasDiagType_t diag, int m, int n, const float* alpha,
+                             float* A, int lda, float* B, int ldb, float* C, int ldc)
+{
+    vparams p = { P_N | P_M | P_A | P_LDA | P_B | P_LDB | P_C | P_LDC, .n = n, .m = m, .lda = lda, .ldb = ldb,
+                  .ldc = ldc, .A = A, .B = B, .C = C };
+    CHECK(p, h);
+    orc_strmm(side, uplo, transa, diag, m, n, *alpha, A, lda, B, ldb, C, ldc);
+    return ICLBLAS_STATUS_SUCCESS;
+}

@@ -66,6 +66,45 @@ namespace ref_srotmg {
 #include "Srotmg/Srotmg_naive.cl"
 }
 
+namespace ref_sger {
+#include "Sger/Sger_naive.cl"
+}
+namespace ref_cgeru {
+#include "Cgeru/Cgeru_naive.cl"
+}
+#undef IDX
+namespace ref_cgerc {
+#include "Cgerc/Cgerc_naive.cl"
+}
+#undef IDX
+namespace ref_ssymv_lower {
+#include "Ssymv/Ssymv_naive_lower.cl"
+}
+#undef MAT_ACCESS
+namespace ref_ssymv_upper {
+#include "Ssymv/Ssymv_naive_upper.cl"
+}
+#undef MAT_ACCESS
+namespace ref_chemv {
+#include "Chemv/Chemv_naive.cl"
+}
+#undef ACCESS
+namespace ref_ssyrk {
+#include "Ssyrk/Ssyrk_naive.cl"
+}
+#undef ACCESS
+namespace ref_ssyr2k {
+#include "Ssyr2k/Ssyr2k_naive.cl"
+}
+#undef ACCESS
+namespace ref_ssymm {
+#include "Ssymm/Ssymm_naive.cl"
+}
+#undef ACCESS
+namespace ref_strmm {
+#include "Strmm/Strmm_naive.cl"
+}
+
 static complex_t c2(const float* p) { return complex_t(p[0], p[1]); }
 
 extern "C" {
@@ -178,6 +217,63 @@ void ref_naive_crotg(float* a, float* b, float* c, float* s)
 void ref_naive_srotmg(float* d1, float* d2, float* x1, float y1, float* param)
 {
     ref_srotmg::Srotmg_naive(d1, d2, x1, y1, param);
+}
+
+// Level-2/3 kernels with their NDRanges: Sger/Cgeru/Cgerc (m, n), Ssymv one
+// work-item, Chemv (n), Ssyrk/Ssyr2k (n, n), Ssymm/Strmm (m, n).
+void ref_naive_sger(int m, int n, float alpha, float* x, int incx, float* y, int incy, float* A, int lda)
+{
+    clshim::run_ndrange2(m, n, [&] { ref_sger::Sger_naive(alpha, x, incx, y, incy, A, lda); });
+}
+
+void ref_naive_cger(int conj, int m, int n, const float* alpha, float* x, int incx, float* y, int incy, float* A,
+                    int lda)
+{
+    clshim::run_ndrange2(m, n, [&] {
+        if (conj)
+            ref_cgerc::Cgerc_naive(c2(alpha), (complex_t*)x, incx, (complex_t*)y, incy, (complex_t*)A, lda);
+        else
+            ref_cgeru::Cgeru_naive(c2(alpha), (complex_t*)x, incx, (complex_t*)y, incy, (complex_t*)A, lda);
+    });
+}
+
+void ref_naive_ssymv(int uplo, int n, float alpha, float* A, int lda, float* x, int incx, float beta, float* y,
+                     int incy)
+{
+    if (uplo == 1) ref_ssymv_lower::Ssymv_naive_lower(n, alpha, A, lda, x, incx, beta, y, incy);
+    else ref_ssymv_upper::Ssymv_naive_upper(n, alpha, A, lda, x, incx, beta, y, incy);
+}
+
+void ref_naive_chemv(int uplo, int n, const float* alpha, float* A, int lda, float* x, int incx, const float* beta,
+                     float* y, int incy)
+{
+    clshim::run_ndrange(n, [&] {
+        ref_chemv::Chemv_naive(uplo, n, c2(alpha), (complex_t*)A, lda, (complex_t*)x, incx, c2(beta), (complex_t*)y,
+                               incy);
+    });
+}
+
+void ref_naive_ssyr2k(int uplo, int trans, int n, int k, float alpha, float* A, int lda, float* B, int ldb, float beta,
+                      float* C, int ldc)
+{
+    clshim::run_ndrange2(n, n, [&] {
+        if (B) ref_ssyr2k::Ssyr2k_naive(uplo, trans, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+        else ref_ssyrk::Ssyrk_naive(uplo, trans, n, k, alpha, A, lda, beta, C, ldc);
+    });
+}
+
+void ref_naive_ssymm(int side, int uplo, int m, int n, float alpha, float* A, int lda, float* B, int ldb, float beta,
+                     float* C, int ldc)
+{
+    clshim::run_ndrange2(m, n, [&] { ref_ssymm::Ssymm_naive(side, uplo, m, n, alpha, A, lda, B, ldb, beta, C, ldc); });
+}
+
+void ref_naive_strmm(int side, int uplo, int transa, int diag, int m, int n, float alpha, float* A, int lda, float* B,
+                     int ldb, float* C, int ldc)
+{
+    clshim::run_ndrange2(m, n, [&] {
+        ref_strmm::Strmm_naive(side, uplo, transa, diag, m, n, alpha, A, lda, B, ldb, C, ldc);
+    });
 }
 
 }  // extern "C"

@@ -14,6 +14,7 @@
 #include "test_axpy.hpp"
 #include "test_scal.hpp"
 #include "test_amax.hpp"
+#include "test_symv.hpp"
 
 using cf = std::complex<float>;
 using namespace iclgpu::tests;
@@ -84,5 +85,19 @@ void ref_cpu_cscal(int n, const float* alpha, float* x, int incx)
 // cpu_amax<float> = Isamax_reference - 1 (0-based)
 int ref_cpu_isamax(int n, const float* x, int incx) { int r = 0; cpu_amax<float>(n, x, incx, &r); return r; }
 int ref_cpu_icamax(int n, const float* x, int incx) { int r = 0; cpu_amax<cf>(n, (const cf*)x, incx, &r); return r; }
+
+// cpu_symv (tests/blas_funcs/test_symv.hpp:21-87), double accumulation
+void ref_cpu_ssymv(int uplo, int n, float alpha, const float* A, int lda, const float* x, int incx, float beta, float* y,
+                   int incy)
+{
+    cpu_symv<float>((iclblasFillMode_t)uplo, n, alpha, A, lda, x, incx, beta, y, incy);
+}
+
+void ref_cpu_chemv(int uplo, int n, const float* alpha, const float* A, int lda, const float* x, int incx,
+                   const float* beta, float* y, int incy)
+{
+    cpu_symv<cf, true>((iclblasFillMode_t)uplo, n, cf(alpha[0], alpha[1]), (const cf*)A, lda, (const cf*)x, incx,
+                       cf(beta[0], beta[1]), (cf*)y, incy);
+}
 
 }  // extern "C"

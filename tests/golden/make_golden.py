@@ -5,8 +5,10 @@ reference's CPU templates (tests/blas_funcs/*.hpp: cpu_gemm, cpu_dot,
 cpu_nrm2, cpu_asum, cpu_axpy, cpu_scal, cpu_amax; tests/blas_reference/
 blas_reference.cpp: Isamax_reference, Caxpy_reference) and its serial OpenCL
 kernels compiled as C++ (Sgemv/Cgemv/Strsv/Ctrsv/Strsm/Ctrsm/Sgemm/Cgemm
-_naive.cl and the level-1 Isamin/Icamin/Srot/Csrot/Crot/Srotm/Srotg/Crotg/
-Srotmg _naive.cl), all built from the reference's sources by oracle/Makefile.
+_naive.cl, the level-1 Isamin/Icamin/Srot/Csrot/Crot/Srotm/Srotg/Crotg/
+Srotmg _naive.cl, and Sger/Cgeru/Cgerc/Ssyrk/Ssyr2k/Ssymm _naive.cl with the
+cpu_symv template for Ssymv/Chemv), all built from the reference's sources by
+oracle/Makefile.
 
 Each case is stored under a key prefix "<case>/" with its inputs, scalar
 parameters and the reference output.  The fixture is committed; run this
@@ -77,7 +79,8 @@ def rotation_cases(R, d):
         R.ref_naive_csrot(n, P(x1), incx, P(y1), incy, float(c), float(s))
         d[k + "csrot_x"], d[k + "csrot_y"] = x1, y1
         x1, y1 = xc.copy(), yc.copy()
-        R.ref_naive_crot(n, P(x1), incx, P(y1), incy, float(c), P(O.cbox(sc)))
+        scb = O.cbox(sc)   # kept alive across the call
+        R.ref_naive_crot(n, P(x1), incx, P(y1), incy, float(c), P(scb))
         d[k + "crot_x"], d[k + "crot_y"] = x1, y1
         for flag in (-1, 0, 1):
             param = np.array([flag, 0.75, -1.5, 2.25, 0.125], np.float32)
@@ -112,6 +115,82 @@ def rotation_cases(R, d):
         R.ref_naive_srotmg(P(v[0:]), P(v[1:]), P(v[2:]), float(y1), P(param))
         outm[i, :3], outm[i, 3:] = v, param
     d["srotmg/in"], d["srotmg/out"] = rows, outm
+
+
+def level23_cases(R, d):
+    """Sger / Cgeru / Cgerc through their serial kernels (bit-exact FP32
+    expressions), Ssymv / Chemv through the cpu_symv template
+    (tests/blas_funcs/test_symv.hpp, double), Ssyrk / Ssyr2k / Ssymm through
+    their serial kernels (FP32 sums); own seed."""
+    rng = np.random.default_rng(20261205)
+    m, n, lda = 45, 31, 48
+    x = rng.uniform(-2, 2, m * 2).astype(np.float32)
+    y = rng.uniform(-2, 2, n).astype(np.float32)
+    A = rng.uniform(-2, 2, lda * n).astype(np.float32)
+    d["sger/x"], d["sger/y"], d["sger/A"] = x, y, A.copy()
+    d["sger/dims"] = np.array([m, n, 2, 1, lda], np.int32)
+    R.ref_naive_sger(m, n, 0.75, P(x), 2, P(y), 1, P(A), lda)
+    d["sger/out"] = A
+    xc = rng.uniform(-1, 1, (m, 2)).astype(np.float32).view(np.complex64).reshape(-1)
+    yc = rng.uniform(-1, 1, (n * 3, 2)).astype(np.float32).view(np.complex64).reshape(-1)
+    Ac = rng.uniform(-1, 1, (lda * n, 2)).astype(np.float32).view(np.complex64).reshape(-1)
+    al = np.complex64(0.5 - 0.25j)
+    alb = O.cbox(al)
+    for conj in (0, 1):
+        k = f"cger{conj}/"
+        A1 = Ac.copy()
+        d[k + "x"], d[k + "y"], d[k + "A"] = xc, yc, Ac.copy()
+        d[k + "dims"] = np.array([m, n, 1, 3, lda], np.int32)
+        d[k + "alpha"] = al
+        R.ref_naive_cger(conj, m, n, P(alb), P(xc), 1, P(yc), 3, P(A1), lda)
+        d[k + "out"] = A1
+    for uplo in (0, 1):
+        nn, ld = 77, 80
+        k = f"ssymv{uplo}/"
+        A = rng.uniform(-1, 1, ld * nn).astype(np.float32)
+        x = rng.uniform(-1, 1, nn).astype(np.float32)
+        y = rng.uniform(-1, 1, nn * 2).astype(np.float32)
+        d[k + "A"], d[k + "x"], d[k + "y"] = A, x, y.copy()
+        d[k + "dims"] = np.array([uplo, nn, ld, 1, 2], np.int32)
+        R.ref_cpu_ssymv(uplo, nn, 1.25, P(A), ld, P(x), 1, -0.5, P(y), 2)
+        d[k + "out"] = y
+        k = f"chemv{uplo}/"
+        A = rng.uniform(-1, 1, (ld * nn, 2)).astype(np.float32).view(np.complex64).reshape(-1)
+        x = rng.uniform(-1, 1, (nn * 2, 2)).astype(np.float32).view(np.complex64).reshape(-1)
+        y = rng.uniform(-1, 1, (nn, 2)).astype(np.float32).view(np.complex64).reshape(-1)
+        ab = np.array([0.5 - 1j, 0.25 + 0.5j], np.complex64)
+        ab0, ab1 = O.cbox(ab[0]), O.cbox(ab[1])
+        d[k + "A"], d[k + "x"], d[k + "y"], d[k + "ab"] = A, x, y.copy(), ab
+        d[k + "dims"] = np.array([uplo, nn, ld, 2, 1], np.int32)
+        R.ref_cpu_chemv(uplo, nn, P(ab0), P(A), ld, P(x), 2, P(ab1), P(y), 1)
+        d[k + "out"] = y
+        for trans in (0, 1):
+            nn, kk = 53, 21
+            ld = (nn if trans == 0 else kk) + 3
+            cols = kk if trans == 0 else nn
+            A = rng.uniform(-1, 1, ld * cols).astype(np.float32)
+            B = rng.uniform(-1, 1, ld * cols).astype(np.float32)
+            C = rng.uniform(-1, 1, (nn + 1) * nn).astype(np.float32)
+            for name, Bp in (("ssyrk", None), ("ssyr2k", B)):
+                k = f"{name}{uplo}{trans}/"
+                C1 = C.copy()
+                d[k + "A"], d[k + "B"], d[k + "C"] = A, B, C
+                d[k + "dims"] = np.array([uplo, trans, nn, kk, ld, nn + 1], np.int32)
+                R.ref_naive_ssyr2k(uplo, trans, nn, kk, 0.75, P(A), ld, None if Bp is None else P(Bp), ld, -0.5,
+                                   P(C1), nn + 1)
+                d[k + "out"] = C1
+        for side in (0, 1):
+            mm, nn = 41, 27
+            na = mm if side == 0 else nn
+            k = f"ssymm{side}{uplo}/"
+            A = rng.uniform(-1, 1, (na + 2) * na).astype(np.float32)
+            B = rng.uniform(-1, 1, (mm + 1) * nn).astype(np.float32)
+            C = rng.uniform(-1, 1, (mm + 3) * nn).astype(np.float32)
+            C1 = C.copy()
+            d[k + "A"], d[k + "B"], d[k + "C"] = A, B, C
+            d[k + "dims"] = np.array([side, uplo, mm, nn, na + 2, mm + 1, mm + 3], np.int32)
+            R.ref_naive_ssymm(side, uplo, mm, nn, 1.5, P(A), na + 2, P(B), mm + 1, 0.25, P(C1), mm + 3)
+            d[k + "out"] = C1
 
 
 def main():
@@ -276,6 +355,7 @@ def main():
                     d[k + "out"] = Bm
 
     rotation_cases(R, d)
+    level23_cases(R, d)
 
     np.savez_compressed(OUT, **d)
     print(f"wrote {OUT}: {len(d)} arrays, {os.path.getsize(OUT) / 1024:.0f} KiB")

@@ -74,6 +74,14 @@ def orc() -> C.CDLL:
             "orc_srotg": ([p, p, p, p], None),
             "orc_crotg": ([p, p, p, p], None),
             "orc_srotmg": ([p, p, p, f, p], None),
+            "orc_sger": ([i, i, f, p, i, p, i, p, i], None),
+            "orc_cger": ([i, i, i, C32, p, i, p, i, p, i], None),
+            "orc_ssymv": ([i, i, f, p, i, p, i, f, p, i], None),
+            "orc_chemv": ([i, i, C32, p, i, p, i, C32, p, i], None),
+            "orc_ssyrk": ([i, i, i, i, f, p, i, f, p, i], None),
+            "orc_ssyr2k": ([i, i, i, i, f, p, i, p, i, f, p, i], None),
+            "orc_ssymm": ([i, i, i, i, f, p, i, p, i, f, p, i], None),
+            "orc_strmm": ([i, i, i, i, i, i, f, p, i, p, i, p, i], None),
         }
         for name, (a, r) in sig.items():
             fn = getattr(L, name)
@@ -123,6 +131,15 @@ def ref() -> C.CDLL | None:
             "ref_naive_srotg": ([p, p, p, p], None),
             "ref_naive_crotg": ([p, p, p, p], None),
             "ref_naive_srotmg": ([p, p, p, f, p], None),
+            "ref_naive_sger": ([i, i, f, p, i, p, i, p, i], None),
+            "ref_naive_cger": ([i, i, i, p, p, i, p, i, p, i], None),
+            "ref_naive_ssymv": ([i, i, f, p, i, p, i, f, p, i], None),
+            "ref_naive_chemv": ([i, i, p, p, i, p, i, p, p, i], None),
+            "ref_naive_ssyr2k": ([i, i, i, i, f, p, i, p, i, f, p, i], None),
+            "ref_naive_ssymm": ([i, i, i, i, f, p, i, p, i, f, p, i], None),
+            "ref_naive_strmm": ([i, i, i, i, i, i, f, p, i, p, i, p, i], None),
+            "ref_cpu_ssymv": ([i, i, f, p, i, p, i, f, p, i], None),
+            "ref_cpu_chemv": ([i, i, p, p, i, p, i, p, p, i], None),
         }
         for name, (a, r) in sig.items():
             fn = getattr(L, name)
@@ -285,6 +302,38 @@ def srotmg(d1, d2, x1, y1, param):
     v = np.array([d1, d2, x1], dtype=np.float32)
     orc().orc_srotmg(_p(v[0:]), _p(v[1:]), _p(v[2:]), float(np.float32(y1)), _p(param))
     return tuple(v)
+
+
+def sger(m, n, alpha, x, incx, y, incy, A, lda):
+    orc().orc_sger(m, n, alpha, _p(x), incx, _p(y), incy, _p(A), lda)
+
+
+def cger(conj, m, n, alpha, x, incx, y, incy, A, lda):
+    orc().orc_cger(1 if conj else 0, m, n, c32(alpha), _p(x), incx, _p(y), incy, _p(A), lda)
+
+
+def ssymv(uplo, n, alpha, A, lda, x, incx, beta, y, incy):
+    orc().orc_ssymv(uplo, n, alpha, _p(A), lda, _p(x), incx, beta, _p(y), incy)
+
+
+def chemv(uplo, n, alpha, A, lda, x, incx, beta, y, incy):
+    orc().orc_chemv(uplo, n, c32(alpha), _p(A), lda, _p(x), incx, c32(beta), _p(y), incy)
+
+
+def ssyrk(uplo, trans, n, k, alpha, A, lda, beta, Cm, ldc):
+    orc().orc_ssyrk(uplo, trans, n, k, alpha, _p(A), lda, beta, _p(Cm), ldc)
+
+
+def ssyr2k(uplo, trans, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc):
+    orc().orc_ssyr2k(uplo, trans, n, k, alpha, _p(A), lda, _p(B), ldb, beta, _p(Cm), ldc)
+
+
+def ssymm(side, uplo, m, n, alpha, A, lda, B, ldb, beta, Cm, ldc):
+    orc().orc_ssymm(side, uplo, m, n, alpha, _p(A), lda, _p(B), ldb, beta, _p(Cm), ldc)
+
+
+def strmm(side, uplo, transa, diag, m, n, alpha, A, lda, B, ldb, Cm, ldc):
+    orc().orc_strmm(side, uplo, transa, diag, m, n, alpha, _p(A), lda, _p(B), ldb, _p(Cm), ldc)
 
 
 # ------------------------------------------------------------ data helpers

@@ -172,6 +172,63 @@ def test_oracle_rotation_generators():
         assert np.array_equal(bits(param), bits(want[3:]))
 
 
+def _l23_cases():
+    return cases("sger") + cases("cger") + cases("ssymv") + cases("chemv") + cases("ssyrk") + cases("ssyr2k") + \
+        cases("ssymm")
+
+
+def _l23_run(case, api):
+    """Runs one level-2/3 golden case through `api` (the oracle wrappers or
+    the GPU library); returns (result, expected, exact)."""
+    if case == "sger":
+        m, n, incx, incy, lda = (int(v) for v in g(case, "dims"))
+        A = g(case, "A").copy()
+        api["sger"](m, n, 0.75, g(case, "x"), incx, g(case, "y"), incy, A, lda)
+        return A, g(case, "out"), True
+    if case.startswith("cger"):
+        m, n, incx, incy, lda = (int(v) for v in g(case, "dims"))
+        A = g(case, "A").copy()
+        api["cger"](case.endswith("1"), m, n, complex(g(case, "alpha")), g(case, "x"), incx, g(case, "y"), incy, A, lda)
+        return A, g(case, "out"), True
+    if case.startswith("ssymv"):
+        uplo, n, lda, incx, incy = (int(v) for v in g(case, "dims"))
+        y = g(case, "y").copy()
+        api["ssymv"](uplo, n, 1.25, g(case, "A"), lda, g(case, "x"), incx, -0.5, y, incy)
+        return y, g(case, "out"), False
+    if case.startswith("chemv"):
+        uplo, n, lda, incx, incy = (int(v) for v in g(case, "dims"))
+        ab = g(case, "ab")
+        y = g(case, "y").copy()
+        api["chemv"](uplo, n, complex(ab[0]), g(case, "A"), lda, g(case, "x"), incx, complex(ab[1]), y, incy)
+        return y, g(case, "out"), False
+    if case.startswith("ssyr2k") or case.startswith("ssyrk"):
+        uplo, trans, n, k, lda, ldc = (int(v) for v in g(case, "dims"))
+        Cm = g(case, "C").copy()
+        if case.startswith("ssyr2k"):
+            api["ssyr2k"](uplo, trans, n, k, 0.75, g(case, "A"), lda, g(case, "B"), lda, -0.5, Cm, ldc)
+        else:
+            api["ssyrk"](uplo, trans, n, k, 0.75, g(case, "A"), lda, -0.5, Cm, ldc)
+        return Cm, g(case, "out"), False
+    side, uplo, m, n, lda, ldb, ldc = (int(v) for v in g(case, "dims"))
+    Cm = g(case, "C").copy()
+    api["ssymm"](side, uplo, m, n, 1.5, g(case, "A"), lda, g(case, "B"), ldb, 0.25, Cm, ldc)
+    return Cm, g(case, "out"), False
+
+
+ORACLE_API = {"sger": O.sger, "cger": O.cger, "ssymv": O.ssymv, "chemv": O.chemv, "ssyrk": O.ssyrk,
+              "ssyr2k": O.ssyr2k, "ssymm": O.ssymm}
+
+
+@pytest.mark.parametrize("case", _l23_cases())
+def test_oracle_level23(case):
+    got, want, exact = _l23_run(case, ORACLE_API)
+    if exact:
+        assert np.array_equal(bits(got), bits(want))
+    else:
+        assert O.rel_fro(got, want) <= TOL
+        assert np.array_equal(np.isnan(got), np.isnan(want))
+
+
 # ------------------------------------------------------------------ GPU library
 @pytest.mark.gpu
 def test_gpu_rotations_against_golden(handle):
@@ -297,3 +354,21 @@ def test_gpu_level3_level2_against_golden(handle):
             st = B.iclblasCtrsm(handle, side, uplo, trans, diag, m, n, complex(al), g(case, "A"), lda, Bm, ldb)
         assert st == B.SUCCESS
         assert O.rel_fro(Bm, g(case, "out")) <= TOL, case
+
+
+@pytest.mark.gpu
+def test_gpu_level23_against_golden(handle):
+    def st(fn):
+        def call(*a):
+            assert fn(handle, *a) == B.SUCCESS
+        return call
+    api = {"sger": st(B.iclblasSger),
+           "cger": lambda conj, *a: st(B.iclblasCgerc if conj else B.iclblasCgeru)(*a),
+           "ssymv": st(B.iclblasSsymv), "chemv": st(B.iclblasChemv), "ssyrk": st(B.iclblasSsyrk),
+           "ssyr2k": st(B.iclblasSsyr2k), "ssymm": st(B.iclblasSsymm)}
+    for case in _l23_cases():
+        got, want, exact = _l23_run(case, api)
+        if exact:
+            assert same(got, want), case
+        else:
+            assert O.rel_fro(got, want) <= TOL, case

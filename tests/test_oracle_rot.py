@@ -76,7 +76,8 @@ def test_rotations_match_naive_kernels(n, incx, incy):
         sc = complex(s, 0.5 * c - 0.3)
         x1, y1, x2, y2 = xc.copy(), yc.copy(), xc.copy(), yc.copy()
         O.crot(n, x1, incx, y1, incy, c, sc)
-        R.ref_naive_crot(n, _p(x2), incx, _p(y2), incy, c, _p(O.cbox(sc)))
+        scb = O.cbox(sc)   # kept alive across the call
+        R.ref_naive_crot(n, _p(x2), incx, _p(y2), incy, c, _p(scb))
         assert np.array_equal(bits(x1), bits(x2)) and np.array_equal(bits(y1), bits(y2))
 
 

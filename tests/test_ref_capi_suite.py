@@ -1,6 +1,7 @@
 """The reference's own C-API known-answer suite (tests/iclBLAS/test_<routine>.cpp
-of the clGPU tree: the 21 hot-path routines and the 13 level-1 copy / swap /
-rotation / iamin routines, 187 tests), compiled unmodified
+of the clGPU tree: the 21 hot-path routines, the 13 level-1 copy / swap /
+rotation / iamin routines and Sger, Cgeru, Cgerc, Ssymv, Chemv, Ssyrk, Ssyr2k,
+Ssymm; 221 tests), compiled unmodified
 against the reference's iclBLAS.h by oracle/Makefile:
 
   - linked against the CPU oracle (oracle/_ref/ref_capi_tests_oracle): pins
@@ -29,7 +30,7 @@ def _run(binary):
 def test_reference_suite_against_oracle():
     rc, out = _run(os.path.join(REF, "ref_capi_tests_oracle"))
     assert rc == 0, out[-4000:]
-    assert "[  PASSED  ] 187 tests." in out, out[-2000:]
+    assert "[  PASSED  ] 221 tests." in out, out[-2000:]
 
 
 @pytest.mark.gpu
@@ -40,4 +41,4 @@ def test_reference_suite_against_gpu_library(cuda):
     binary = os.path.join(REF, "ref_capi_tests_b200")
     rc, out = _run(binary)
     assert rc == 0, out[-4000:]
-    assert "[  PASSED  ] 187 tests." in out, out[-2000:]
+    assert "[  PASSED  ] 221 tests." in out, out[-2000:]
