@@ -633,6 +633,128 @@ def run_level1x_study(args, torch):
                               "algorithmic_bytes": nbytes[name]}), flush=True)
 
 
+def run_level23x_study(args, torch):
+    """Rank-1 updates, Ssymv / Chemv (HBM GB/s) and the GEMM-shaped level-3
+    routines (TFLOP/s in each math mode), device operands, U(-1,1) seed 3,
+    median of event-timed calls.  Algorithmic bytes: ger reads and writes A
+    (8 mn / 16 mn); symv / hemv read the stored triangle, x and y and write
+    y (4 or 8 x (n(n+1)/2 + 3n)).  Algorithmic flops: syrk n^2 k, syr2k
+    2 n^2 k, symm 2 m^2 n (left), trmm m^2 n (left); errors are relative
+    Frobenius against the same product in FP64 (torch, plumbing only)."""
+    from clgpu_b200 import iclblas as B
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(device=dev)
+    g = torch.Generator(device=dev).manual_seed(3)
+    peak, peak_kind = load_peaks()
+    only = set(args.only.split(",")) if args.only else None
+
+    def rnd(*shape, dtype=torch.float32):
+        t = torch.rand(*shape, generator=g, device=dev) * 2 - 1
+        if dtype == torch.complex64:
+            t = torch.complex(t, torch.rand(*shape, generator=g, device=dev) * 2 - 1)
+        return t
+
+    def timed(h, f, reps):
+        for _ in range(3):
+            B.check(f(h), "warmup")
+        torch.cuda.synchronize()
+        evs = []
+        for _ in range(reps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            B.check(f(h), "call")
+            e1.record(stream)
+            evs.append((e0, e1))
+        torch.cuda.synchronize()
+        return float(np.median([a.elapsed_time(b) for a, b in evs]))
+
+    with B.Handle() as h, torch.cuda.stream(stream):
+        h.set_stream(stream)
+        # ---- bandwidth-bound
+        n = 16384
+        nc = 8192
+        A = rnd(n * n)
+        x, y = rnd(n), rnd(n)
+        Ac = rnd(nc * nc, dtype=torch.complex64)
+        xc, yc = rnd(nc, dtype=torch.complex64), rnd(nc, dtype=torch.complex64)
+        hbm = [
+            ("sger", 8.0 * n * n, lambda hh: B.iclblasSger(hh, n, n, 0.5, x, 1, y, 1, A, n)),
+            ("cgeru", 16.0 * nc * nc, lambda hh: B.iclblasCgeru(hh, nc, nc, 0.5 + 0.25j, xc, 1, yc, 1, Ac, nc)),
+            ("cgerc", 16.0 * nc * nc, lambda hh: B.iclblasCgerc(hh, nc, nc, 0.5 + 0.25j, xc, 1, yc, 1, Ac, nc)),
+            ("ssymv_lower", 4.0 * (n * (n + 1) / 2 + 3 * n),
+             lambda hh: B.iclblasSsymv(hh, 1, n, 1.0, A, n, x, 1, 0.5, y, 1)),
+            ("ssymv_upper", 4.0 * (n * (n + 1) / 2 + 3 * n),
+             lambda hh: B.iclblasSsymv(hh, 0, n, 1.0, A, n, x, 1, 0.5, y, 1)),
+            ("chemv_lower", 8.0 * (nc * (nc + 1) / 2 + 3 * nc),
+             lambda hh: B.iclblasChemv(hh, 1, nc, 1.0 + 0j, Ac, nc, xc, 1, 0.5 + 0j, yc, 1)),
+        ]
+        for name, nbytes, f in hbm:
+            if only and name not in only:
+                continue
+            ms = timed(h, f, max(5, min(args.steps, 30)))
+            gbs = nbytes / (ms / 1e3) / 1e9
+            print(json.dumps({"routine": name, "ms": round(ms, 4), "gbs": round(gbs, 1),
+                              "frac_of_hbm": round(gbs / peak, 3), "peak_kind": peak_kind,
+                              "algorithmic_bytes": nbytes}), flush=True)
+        del A, Ac
+        torch.cuda.empty_cache()
+        # ---- GEMM-shaped
+        N = args.gemm_n if not args.quick else 2048
+        K = N
+        Aa, Bb, Cc = rnd(N * K), rnd(N * K), rnd(N * N)
+        Cw = torch.empty_like(Cc)
+        A64 = Aa.view(K, N).t().double()   # column-major N x K operand as a row-major torch matrix
+        B64 = Bb.view(K, N).t().double()
+        C64 = Cc.view(N, N).t().double()
+        refs = {
+            "ssyrk": lambda: torch.tril(1.0 * (A64 @ A64.t()) + 0.5 * C64),
+            "ssyr2k": lambda: torch.tril(1.0 * (A64 @ B64.t() + B64 @ A64.t()) + 0.5 * C64),
+            "ssymm": lambda: (torch.tril(A64) + torch.tril(A64, -1).t()) @ B64 + 0.5 * C64,
+            "strmm": lambda: torch.tril(A64) @ B64,
+        }
+        work = {"ssyrk": float(N) * N * K, "ssyr2k": 2.0 * N * N * K, "ssymm": 2.0 * N * N * N,
+                "strmm": float(N) * N * N}
+        calls = {
+            "ssyrk": lambda hh: B.iclblasSsyrk(hh, 1, 0, N, K, 1.0, Aa, N, 0.5, Cw, N),
+            "ssyr2k": lambda hh: B.iclblasSsyr2k(hh, 1, 0, N, K, 1.0, Aa, N, Bb, N, 0.5, Cw, N),
+            "ssymm": lambda hh: B.iclblasSsymm(hh, 0, 1, N, N, 1.0, Aa, N, Bb, N, 0.5, Cw, N),
+            "strmm": lambda hh: B.iclblasStrmm(hh, 0, 1, 0, 0, N, N, 1.0, Aa, N, Bb, N, Cw, N),
+        }
+        modes = [("fp32_simt", B.MATH_PLAIN_FP32), ("tf32", B.MATH_TF32), ("3xbf16", B.MATH_BF16X3),
+                 ("6xbf16", B.MATH_BF16X6)]
+        for name in ("ssyrk", "ssyr2k", "ssymm", "strmm"):
+            if only and name not in only:
+                continue
+            R = refs[name]()
+            mask = torch.tril(torch.ones(N, N, dtype=torch.bool, device=dev)) if name.startswith("ssyr") else None
+            for mname, mode in modes:
+                h.set_math_mode(mode)
+                # time the routine alone (the C reset is outside the events)
+                ts = []
+                for rep in range(4 if not args.quick else 2):
+                    Cw.copy_(Cc)
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    B.check(calls[name](h), name)
+                    e1.record(stream)
+                    torch.cuda.synchronize()
+                    if rep > 0:
+                        ts.append(e0.elapsed_time(e1))
+                ms = float(np.median(ts))
+                got = Cw.view(N, N).t().double()
+                if mask is not None:
+                    err = float(torch.linalg.norm((got - R)[mask]) / torch.linalg.norm(R[mask]))
+                else:
+                    err = float(torch.linalg.norm(got - R) / torch.linalg.norm(R))
+                print(json.dumps({"routine": name, "mode": mname, "n": N, "ms": round(ms, 3),
+                                  "tflops": round(work[name] / (ms / 1e3) / 1e12, 2),
+                                  "rel_fro_err_vs_fp64": err}), flush=True)
+            h.set_math_mode(B.MATH_PLAIN_FP32)
+
+
 def run_batched_study(args, torch):
     """Batched uneven TRSM + adjoint config: 512 instances, n ~ UniformInt[32,1024],
     nrhs ~ UniformInt[1,256], L built as in the STRSM config (diagonal U(1,2),
@@ -863,10 +985,11 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-operand (C ABI) leg")
     ap.add_argument("--only", default="", help="comma-separated subset of the sweep's calls")
     ap.add_argument("--n1", type=int, default=N1, help="level-1 vector length (default 2^28)")
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "gemm", "trsm", "batched", "level1x"],
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "gemm", "trsm", "batched", "level1x", "level23x"],
                     help="sweep: the bandwidth config (default); gemm / trsm / batched: the precision, "
                          "triangular-solve and batched-solve config studies; level1x: copy / swap / "
-                         "rotation / iamin bandwidth study")
+                         "rotation / iamin bandwidth study; level23x: ger / symv / hemv bandwidth and "
+                         "syrk / syr2k / symm / trmm throughput study")
     ap.add_argument("--trsm-m", type=int, default=8192)
     ap.add_argument("--trsm-n", type=int, default=4096)
     ap.add_argument("--trsv-n", type=int, default=16384)
@@ -914,6 +1037,9 @@ def main():
         return
     if args.workload == "level1x":
         run_level1x_study(args, torch)
+        return
+    if args.workload == "level23x":
+        run_level23x_study(args, torch)
         return
     if world > 1:
         torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))

@@ -9,23 +9,29 @@
 namespace iclb {
 
 cudaError_t sgemm_simt(iclblasHandle_t h, int ta, int tb, int m, int n, int k, float alpha, const float* A, int lda,
-                       const float* B, int ldb, float beta, float* C, int ldc);
+                       const float* B, int ldb, float beta, float* C, int ldc, int tri);
 cudaError_t cgemm_simt(iclblasHandle_t h, int ta, int tb, int m, int n, int k, cfloat alpha, const cfloat* A, int lda,
                        const cfloat* B, int ldb, cfloat beta, cfloat* C, int ldc);
 namespace tc {
 template <class T>
 cudaError_t gemm_tc(iclblasHandle_t h, int ta, int tb, int m, int n, int k, T alpha, const T* A, int lda, const T* B,
-                    int ldb, T beta, T* C, int ldc);
+                    int ldb, T beta, T* C, int ldc, int tri);
+}
+
+cudaError_t sgemm_tri(iclblasHandle_t h, int tri, int ta, int tb, int m, int n, int k, float alpha, const float* A,
+                      int lda, const float* B, int ldb, float beta, float* C, int ldc)
+{
+    if (m == 0 || n == 0) return cudaSuccess;
+    // k == 0 (C = beta*C) needs no products: the CUDA-core kernel handles it in every mode
+    if (h->math != ICLBLAS_MATH_PLAIN_FP32 && k > 0)
+        return tc::gemm_tc<float>(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, tri);
+    return sgemm_simt(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, tri);
 }
 
 cudaError_t sgemm(iclblasHandle_t h, int ta, int tb, int m, int n, int k, float alpha, const float* A, int lda,
                   const float* B, int ldb, float beta, float* C, int ldc)
 {
-    if (m == 0 || n == 0) return cudaSuccess;
-    // k == 0 (C = beta*C) needs no products: the CUDA-core kernel handles it in every mode
-    if (h->math != ICLBLAS_MATH_PLAIN_FP32 && k > 0)
-        return tc::gemm_tc<float>(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
-    return sgemm_simt(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    return sgemm_tri(h, 0, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
 }
 
 cudaError_t cgemm(iclblasHandle_t h, int ta, int tb, int m, int n, int k, cfloat alpha, const cfloat* A, int lda,
@@ -33,7 +39,7 @@ cudaError_t cgemm(iclblasHandle_t h, int ta, int tb, int m, int n, int k, cfloat
 {
     if (m == 0 || n == 0) return cudaSuccess;
     if (h->math != ICLBLAS_MATH_PLAIN_FP32 && k > 0)
-        return tc::gemm_tc<cfloat>(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+        return tc::gemm_tc<cfloat>(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, 0);
     return cgemm_simt(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
 }
 

@@ -13,6 +13,8 @@
 // double-buffered shared memory with register prefetch of the next k tile;
 // the global loads are arranged so consecutive threads read consecutive
 // addresses for each operand layout (op N vs T/C).
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace iclb {
@@ -89,7 +91,7 @@ struct Cfg {
 template <class T, int BM, int BN, int BK, int TM, int TN>
 __global__ void __launch_bounds__(Cfg<T, BM, BN, BK, TM, TN>::NT)
     gemm_simt_kernel(int ta, int tb, int m, int n, int k, T alpha, const T* __restrict__ A, long lda,
-                     const T* __restrict__ B, long ldb, T beta, T* __restrict__ C, long ldc)
+                     const T* __restrict__ B, long ldb, T beta, T* __restrict__ C, long ldc, int tri)
 {
     using CF = Cfg<T, BM, BN, BK, TM, TN>;
     constexpr int NT = CF::NT, TX = CF::TX;
@@ -101,6 +103,9 @@ __global__ void __launch_bounds__(Cfg<T, BM, BN, BK, TM, TN>::NT)
     const int tid = threadIdx.x;
     const int tx = tid % TX, ty = tid / TX;
     const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    // tri 1 / 2: only C's lower (row >= col) / upper triangle is formed;
+    // tiles wholly outside it have no work
+    if ((tri == 1 && m0 + BM - 1 < n0) || (tri == 2 && m0 > n0 + BN - 1)) return;
     const bool a_trans = ta != ICLBLAS_OP_N, a_conj = ta == ICLBLAS_OP_C;
     const bool b_trans = tb != ICLBLAS_OP_N, b_conj = tb == ICLBLAS_OP_C;
 
@@ -202,12 +207,14 @@ __global__ void __launch_bounds__(Cfg<T, BM, BN, BK, TM, TN>::NT)
 #pragma unroll
         for (int j = 0; j < TN; ++j) {
             const int gj = n0 + (j < TN / 2 ? tx * (TN / 2) + j : BN / 2 + tx * (TN / 2) + (j - TN / 2));
-            cv[j] = (read_c && gj < n) ? C[(long)gj * ldc + gi] : zero_v(T());
+            const bool in = tri == 0 || (tri == 1 ? gi >= gj : gi <= gj);
+            cv[j] = (read_c && gj < n && in) ? C[(long)gj * ldc + gi] : zero_v(T());
         }
 #pragma unroll
         for (int j = 0; j < TN; ++j) {
             const int gj = n0 + (j < TN / 2 ? tx * (TN / 2) + j : BN / 2 + tx * (TN / 2) + (j - TN / 2));
             if (gj >= n) continue;
+            if (tri != 0 && (tri == 1 ? gi < gj : gi > gj)) continue;
             C[(long)gj * ldc + gi] = epilogue(alpha, acc[i][j], beta, &cv[j]);
         }
     }
@@ -215,24 +222,25 @@ __global__ void __launch_bounds__(Cfg<T, BM, BN, BK, TM, TN>::NT)
 
 template <class T, int BM, int BN, int BK, int TM, int TN>
 cudaError_t launch(iclblasHandle_t h, int ta, int tb, int m, int n, int k, T alpha, const T* A, int lda, const T* B,
-                   int ldb, T beta, T* C, int ldc)
+                   int ldb, T beta, T* C, int ldc, int tri)
 {
     using CF = Cfg<T, BM, BN, BK, TM, TN>;
     dim3 grid(ceil_div(m, BM), ceil_div(n, BN));
     gemm_simt_kernel<T, BM, BN, BK, TM, TN><<<grid, CF::NT, 0, h->stream>>>(ta, tb, m, n, k, alpha, A, lda, B, ldb,
-                                                                            beta, C, ldc);
+                                                                            beta, C, ldc, tri);
     return cudaGetLastError();
 }
 
 }  // namespace
 
 cudaError_t sgemm_simt(iclblasHandle_t h, int ta, int tb, int m, int n, int k, float alpha, const float* A, int lda,
-                       const float* B, int ldb, float beta, float* C, int ldc)
+                       const float* B, int ldb, float beta, float* C, int ldc, int tri)
 {
-    const long big_tiles = (long)ceil_div(m, 128) * ceil_div(n, 128);
+    long big_tiles = (long)ceil_div(m, 128) * ceil_div(n, 128);
+    if (tri != 0) big_tiles = (big_tiles + std::min(ceil_div(m, 128), ceil_div(n, 128))) / 2;
     if (big_tiles >= h->sm_count)
-        return launch<float, 128, 128, 16, 8, 8>(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
-    return launch<float, 64, 64, 8, 4, 4>(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+        return launch<float, 128, 128, 16, 8, 8>(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, tri);
+    return launch<float, 64, 64, 8, 4, 4>(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, tri);
 }
 
 cudaError_t cgemm_simt(iclblasHandle_t h, int ta, int tb, int m, int n, int k, cfloat alpha, const cfloat* A, int lda,
@@ -240,8 +248,8 @@ cudaError_t cgemm_simt(iclblasHandle_t h, int ta, int tb, int m, int n, int k, c
 {
     const long big_tiles = (long)ceil_div(m, 64) * ceil_div(n, 64);
     if (big_tiles >= h->sm_count)
-        return launch<cfloat, 64, 64, 8, 4, 4>(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
-    return launch<cfloat, 32, 32, 8, 2, 2>(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+        return launch<cfloat, 64, 64, 8, 4, 4>(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, 0);
+    return launch<cfloat, 32, 32, 8, 2, 2>(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, 0);
 }
 
 }  // namespace iclb

@@ -82,6 +82,7 @@ struct Params {
     float* C;
     long ldc;          // in elements of the output type
     int* status;
+    int tri;           // 0: full C; 1: only row >= col is written; 2: only row <= col (real C)
 };
 
 // ---------------------------------------------------------------- PTX helpers
@@ -239,6 +240,58 @@ __device__ __forceinline__ void tile_coords(int t, int tiles_m, int tiles_n, int
     tn = in_band / rows;
 }
 
+// Tile rows [lo, hi) of tile column tn that hold an element of C's triangle
+// (tiles of bm x bn outputs).
+__device__ __forceinline__ void tri_rows(int tri, int tn, int tiles_m, int bm, int bn, int& lo, int& hi)
+{
+    if (tri == 1) {  // some row >= some column: last row of the tile >= first column
+        lo = (tn * bn) / bm;
+        hi = tiles_m;
+    } else {         // first row of the tile <= last column
+        lo = 0;
+        hi = min(tiles_m, (tn * bn + bn - 1) / bm + 1);
+    }
+    if (lo > hi) lo = hi;
+}
+
+// Number of tiles a CTA loop visits: all, or only those meeting C's triangle.
+__device__ __forceinline__ int tile_count(int tri, int tiles_m, int tiles_n, int bm, int bn)
+{
+    if (tri == 0) return tiles_m * tiles_n;
+    int c = 0;
+    for (int tn = 0; tn < tiles_n; ++tn) {
+        int lo, hi;
+        tri_rows(tri, tn, tiles_m, bm, bn, lo, hi);
+        c += hi - lo;
+    }
+    return c;
+}
+
+// Tile t of that visit order: the grouped order for a full C, column by
+// column over the triangle's tiles otherwise.
+__device__ __forceinline__ void tile_at(int tri, int t, int tiles_m, int tiles_n, int bm, int bn, int& tm, int& tn)
+{
+    if (tri == 0) {
+        tile_coords(t, tiles_m, tiles_n, tm, tn);
+        return;
+    }
+    for (tn = 0; tn < tiles_n; ++tn) {
+        int lo, hi;
+        tri_rows(tri, tn, tiles_m, bm, bn, lo, hi);
+        if (t < hi - lo) {
+            tm = lo + t;
+            return;
+        }
+        t -= hi - lo;
+    }
+    tm = 0;
+}
+
+__device__ __forceinline__ bool in_tri(int tri, int row, int col)
+{
+    return tri == 0 || (tri == 1 ? row >= col : row <= col);
+}
+
 template <bool TF32, int BN_>
 __global__ void __launch_bounds__(THREADS, 1)
     gemm_tc_kernel(const __grid_constant__ CUtensorMap mA0, const __grid_constant__ CUtensorMap mA1,
@@ -259,7 +312,7 @@ __global__ void __launch_bounds__(THREADS, 1)
 
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
     const int tiles_m = (p.M + BM - 1) / BM, tiles_n = (p.N + BN - 1) / BN;
-    const int ntiles = tiles_m * tiles_n;
+    const int ntiles = tile_count(p.tri, tiles_m, tiles_n, BM, BN);
     const int steps = p.kblocks * p.nprod;
 
     if (threadIdx.x == 0) {
@@ -293,7 +346,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             bool ok = true;
             for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
                 int tm, tn;
-                tile_coords(t, tiles_m, tiles_n, tm, tn);
+                tile_at(p.tri, t, tiles_m, tiles_n, BM, BN, tm, tn);
                 for (int st = 0; st < steps && ok; ++st) {
                     const int kb = st / p.nprod, pr = st % p.nprod;
                     if (!mbar_wait(&empty[s], ph ^ 1, abort_flag)) { ok = false; break; }
@@ -361,7 +414,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         bool ok = true;
         for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
             int tm, tn;
-            tile_coords(t, tiles_m, tiles_n, tm, tn);
+            tile_at(p.tri, t, tiles_m, tiles_n, BM, BN, tm, tn);
             float sum[EPI_COLS];
 #pragma unroll
             for (int j = 0; j < EPI_COLS; ++j) sum[j] = 0.f;
@@ -399,12 +452,13 @@ __global__ void __launch_bounds__(THREADS, 1)
 #pragma unroll
                         for (int j = 0; j < 8; ++j) {
                             const int col = col0 + j0 + j;
-                            cv[j] = (!beta_zero && col < p.N) ? p.C[(long)col * p.ldc + row] : 0.f;
+                            cv[j] = (!beta_zero && col < p.N && in_tri(p.tri, row, col)) ? p.C[(long)col * p.ldc + row]
+                                                                                          : 0.f;
                         }
 #pragma unroll
                         for (int j = 0; j < 8; ++j) {
                             const int col = col0 + j0 + j;
-                            if (col < p.N)
+                            if (col < p.N && in_tri(p.tri, row, col))
                                 p.C[(long)col * p.ldc + row] =
                                     beta_zero ? __fmul_rn(p.alpha_re, sum[j0 + j])
                                               : fmaf(p.alpha_re, sum[j0 + j], __fmul_rn(p.beta_re, cv[j]));
@@ -565,7 +619,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     const bool leader = rank == 0;
     const int pair = blockIdx.x / 2, npairs = gridDim.x / 2;
     const int tiles_m = (p.M + 2 * BM - 1) / (2 * BM), tiles_n = (p.N + BN - 1) / BN;
-    const int ntiles = tiles_m * tiles_n;
+    const int ntiles = tile_count(p.tri, tiles_m, tiles_n, 2 * BM, BN);
     const int steps = p.kblocks * p.nprod;
 
     if (threadIdx.x == 0) {
@@ -599,7 +653,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             bool ok = true;
             for (int t = pair; t < ntiles && ok; t += npairs) {
                 int tm, tn;
-                tile_coords(t, tiles_m, tiles_n, tm, tn);
+                tile_at(p.tri, t, tiles_m, tiles_n, 2 * BM, BN, tm, tn);
                 for (int st = 0; st < steps && ok; ++st) {
                     const int kb = st / p.nprod, pr = st % p.nprod;
                     if (!mbar_wait(&empty[s], ph ^ 1, abort_flag)) { ok = false; break; }
@@ -669,7 +723,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         bool ok = true;
         for (int t = pair; t < ntiles && ok; t += npairs) {
             int tm, tn;
-            tile_coords(t, tiles_m, tiles_n, tm, tn);
+            tile_at(p.tri, t, tiles_m, tiles_n, 2 * BM, BN, tm, tn);
             float sum[EPI_COLS];
 #pragma unroll
             for (int j = 0; j < EPI_COLS; ++j) sum[j] = 0.f;
@@ -705,12 +759,13 @@ __global__ void __launch_bounds__(THREADS, 1)
 #pragma unroll
                         for (int j = 0; j < 8; ++j) {
                             const int col = col0 + j0 + j;
-                            cv[j] = (!beta_zero && col < p.N) ? p.C[(long)col * p.ldc + row] : 0.f;
+                            cv[j] = (!beta_zero && col < p.N && in_tri(p.tri, row, col)) ? p.C[(long)col * p.ldc + row]
+                                                                                          : 0.f;
                         }
 #pragma unroll
                         for (int j = 0; j < 8; ++j) {
                             const int col = col0 + j0 + j;
-                            if (col < p.N)
+                            if (col < p.N && in_tri(p.tri, row, col))
                                 p.C[(long)col * p.ldc + row] =
                                     beta_zero ? __fmul_rn(p.alpha_re, sum[j0 + j])
                                               : fmaf(p.alpha_re, sum[j0 + j], __fmul_rn(p.beta_re, cv[j]));
@@ -1002,7 +1057,7 @@ cudaError_t run_split(iclblasHandle_t h, const T* S, int R, int K, long rs, long
 // (T = cfloat); the real GEMM then has M rows, 2N columns and 2K depth.
 template <class T>
 cudaError_t gemm_tc(iclblasHandle_t h, int ta, int tb, int m, int n, int k, T alpha, const T* A, int lda,
-                    const T* B, int ldb, T beta, T* C, int ldc)
+                    const T* B, int ldb, T beta, T* C, int ldc, int tri)
 {
     constexpr bool cplx = sizeof(T) == sizeof(cfloat);
     const ModeInfo mi = mode_info(h->math);
@@ -1066,6 +1121,7 @@ cudaError_t gemm_tc(iclblasHandle_t h, int ta, int tb, int m, int n, int k, T al
     p.C = (float*)C;
     p.ldc = ldc;
     p.status = h->ws.dev_status;
+    p.tri = cplx ? 0 : tri;
 
     if (pairs) {
         auto run2 = [&](auto kernel) -> cudaError_t {
@@ -1109,9 +1165,9 @@ cudaError_t gemm_tc(iclblasHandle_t h, int ta, int tb, int m, int n, int k, T al
 }
 
 template cudaError_t gemm_tc<float>(iclblasHandle_t, int, int, int, int, int, float, const float*, int, const float*,
-                                    int, float, float*, int);
+                                    int, float, float*, int, int);
 template cudaError_t gemm_tc<cfloat>(iclblasHandle_t, int, int, int, int, int, cfloat, const cfloat*, int,
-                                     const cfloat*, int, cfloat, cfloat*, int);
+                                     const cfloat*, int, cfloat, cfloat*, int, int);
 
 }  // namespace tc
 }  // namespace iclb

@@ -142,6 +142,11 @@ cudaError_t chemv(iclblasHandle_t h, int uplo, int n, cfloat alpha, const cfloat
 // ---------------------------------------------------------------- level 3
 cudaError_t sgemm(iclblasHandle_t h, int transa, int transb, int m, int n, int k, float alpha, const float* A,
                   int lda, const float* B, int ldb, float beta, float* C, int ldc);
+// S GEMM forming only one triangle of C: tri 1 writes (and reads, for beta)
+// only row >= col, tri 2 only row <= col; tiles outside the triangle are not
+// computed.  tri 0 is the plain GEMM.
+cudaError_t sgemm_tri(iclblasHandle_t h, int tri, int transa, int transb, int m, int n, int k, float alpha,
+                      const float* A, int lda, const float* B, int ldb, float beta, float* C, int ldc);
 cudaError_t cgemm(iclblasHandle_t h, int transa, int transb, int m, int n, int k, cfloat alpha, const cfloat* A,
                   int lda, const cfloat* B, int ldb, cfloat beta, cfloat* C, int ldc);
 cudaError_t strsm(iclblasHandle_t h, int side, int uplo, int trans, int diag, int m, int n, float alpha,

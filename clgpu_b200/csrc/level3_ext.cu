@@ -2,24 +2,23 @@
 //
 // All four are GEMM-shaped, so they run as S GEMM calls in the handle's math
 // mode (plain FP32 on the CUDA cores, or TF32 / 3xBF16 / 6xBF16 on the
-// tensor cores) plus small bandwidth-bound helper kernels:
-//   - Ssyrk / Ssyr2k: the output triangle is split recursively in halves;
-//     the off-diagonal block of each split is one GEMM (two for Ssyr2k)
-//     applying beta, and each diagonal leaf (at most kLeaf rows) is a full
-//     leaf x leaf product into solver scratch followed by a masked update of
-//     the stored triangle.  Flops: n^2 k (n^2 k x2 for Ssyr2k) plus the
-//     leaves' other halves, n kLeaf k.
+// tensor cores) plus small bandwidth-bound helper kernels.  Each GEMM is
+// kept large so that it fills the GPU: deep-K GEMMs with small outputs,
+// which a recursive halving down to small leaves produces, ran these
+// routines at a fifth of the GEMM rate.
+//   - Ssyrk / Ssyr2k: one GEMM (two for Ssyr2k) in the engines'
+//     triangular-output mode, which computes only the tiles meeting C's
+//     triangle and writes (and, for beta, reads) only the triangle.
 //   - Ssymm: the symmetric operand is expanded to a full matrix in solver
 //     scratch (its stored triangle read once) and multiplied by one GEMM.
-//   - Strmm: the triangular factor op(A) is split recursively; the
-//     off-diagonal block of each split is one GEMM accumulating into C, and
-//     each diagonal leaf is expanded (zeros outside the triangle, ones on a
-//     unit diagonal) and multiplied by one GEMM.  C is a separate output as
-//     in the reference's interface (iclBLAS.h:1753); when C overlaps B, B is
-//     first copied to solver scratch so the in-place call the reference's
-//     own test makes (C == B) gives the product of the original B.
-// Solver scratch holds the leaves, the expanded operands and the B copy; the
-// GEMMs may grow the general scratch without disturbing it.
+//   - Strmm: the triangle of A is expanded (zeros outside it, ones on a
+//     unit diagonal); C is formed in panels, each one GEMM over the non-zero
+//     part of the expanded factor.  C is a separate output as in the
+//     reference's interface (iclBLAS.h:1753); when C overlaps B, B is first
+//     copied to solver scratch so the in-place call the reference's own test
+//     makes (C == B) gives the product of the original B.
+// Solver scratch holds the expanded operands and the B copy; the GEMMs may
+// grow the general scratch without disturbing it.
 #include <algorithm>
 
 #include "common.cuh"
@@ -28,26 +27,8 @@ namespace iclb {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kLeaf = 256;
 
 // ------------------------------------------------------------------ helpers
-// C(i,j) over the stored triangle of an n x n block = W(i,j) (+ W(j,i) when
-// SYM2) + beta C(i,j); beta == 0 writes C without reading it.
-template <bool SYM2>
-__global__ void __launch_bounds__(kThreads) tri_update_kernel(int n, bool lower, const float* __restrict__ W, int ldw,
-                                                              float beta, float* C, long ldc)
-{
-    const long total = (long)n * n;
-    for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
-        const int i = (int)(e % n), j = (int)(e / n);
-        if (lower ? (i < j) : (i > j)) continue;
-        float v = W[(long)j * ldw + i];
-        if (SYM2) v = __fadd_rn(v, W[(long)i * ldw + j]);
-        float* c = C + (long)j * ldc + i;
-        *c = (beta != 0.f) ? fmaf(beta, *c, v) : v;
-    }
-}
-
 // Full n x n symmetric matrix F from the stored triangle of A.
 __global__ void __launch_bounds__(kThreads) symmetrize_kernel(int n, bool lower, const float* __restrict__ A, long lda,
                                                               float* __restrict__ F)
@@ -92,118 +73,80 @@ int grid_for(iclblasHandle_t h, long units)
     return (int)std::max<long>(g, 1);
 }
 
-// Split point: half of n rounded to a multiple of 64 (at least 64).
-int split_of(int n) { return std::max(64, ((n / 2) + 63) / 64 * 64); }
+// ------------------------------------------------------------------ panels
+// Panel width for a triangular dimension of t: about t/8, a multiple of 128,
+// within [256, 2048]; t itself when that is smaller.
+int panel_of(int t)
+{
+    int p = ((t + 7) / 8 + 127) / 128 * 128;
+    p = std::max(256, std::min(2048, p));
+    return std::min(p, t);
+}
 
 // ------------------------------------------------------------------ syrk / syr2k
+// One triangular-output GEMM (two for Ssyr2k): the GEMM engines skip the
+// tiles wholly outside C's triangle and mask the diagonal tiles, so the
+// flops are n^2 k plus the diagonal tiles' other halves.
 struct Rk {
     iclblasHandle_t h;
     bool lower, trans;  // trans: C = alpha op(A)^T op(B) with A, B k x n
-    int k;
+    int n, k;
     float alpha, beta;
     const float *A, *B;  // B == nullptr: syrk
     int lda, ldb;
     float* C;
     int ldc;
-    float* W;  // kLeaf x kLeaf leaf buffer
 
-    // pointer to rows [r, ...) of op(X) (X = A or B)
-    const float* rows(const float* X, int ld, int r) const { return trans ? X + (long)r * ld : X + r; }
-
-    // P = alpha * opX(rows r..) * opY(rows c..)^T (+ beta0 P), P an mr x nc block of C or W
-    cudaError_t prod(const float* X, int ldx, const float* Y, int ldy, int r, int c, int mr, int nc, float beta0,
-                     float* P, int ldp) const
+    cudaError_t run() const
     {
-        // trans == false: X is n x k, product X_r Y_c^T = gemm(N, T);
-        // trans == true:  X is k x n, product X_r^T Y_c = gemm(T, N).
-        return sgemm(h, trans ? 1 : 0, trans ? 0 : 1, mr, nc, k, alpha, rows(X, ldx, r), ldx, rows(Y, ldy, c), ldy,
-                     beta0, P, ldp);
-    }
-
-    cudaError_t run(int off, int n) const
-    {
-        if (n <= kLeaf) {
-            cudaError_t e = prod(A, lda, B ? B : A, B ? ldb : lda, off, off, n, n, 0.f, W, kLeaf);
-            if (e != cudaSuccess) return e;
-            float* Cb = C + (long)off * ldc + off;
-            if (B)
-                tri_update_kernel<true><<<grid_for(h, (long)n * n), kThreads, 0, h->stream>>>(n, lower, W, kLeaf, beta,
-                                                                                              Cb, ldc);
-            else
-                tri_update_kernel<false><<<grid_for(h, (long)n * n), kThreads, 0, h->stream>>>(n, lower, W, kLeaf,
-                                                                                               beta, Cb, ldc);
-            return cudaGetLastError();
-        }
-        const int n1 = split_of(n), n2 = n - n1;
-        cudaError_t e = run(off, n1);
-        if (e != cudaSuccess) return e;
-        e = run(off + n1, n2);
-        if (e != cudaSuccess) return e;
-        // off-diagonal block: lower C21 (rows off+n1.., cols off..), upper C12
-        const int r = lower ? off + n1 : off, c = lower ? off : off + n1;
-        const int mr = lower ? n2 : n1, nc = lower ? n1 : n2;
-        float* P = C + (long)c * ldc + r;
-        if (!B) return prod(A, lda, A, lda, r, c, mr, nc, beta, P, ldc);
-        e = prod(A, lda, B, ldb, r, c, mr, nc, beta, P, ldc);
-        if (e != cudaSuccess) return e;
-        return prod(B, ldb, A, lda, r, c, mr, nc, 1.f, P, ldc);
+        const int tri = lower ? 1 : 2;
+        // trans == false: op(X) = X (n x k), product X Y^T = gemm(N, T); else X^T Y = gemm(T, N)
+        const int ta = trans ? 1 : 0, tb = trans ? 0 : 1;
+        cudaError_t e = sgemm_tri(h, tri, ta, tb, n, n, k, alpha, A, lda, B ? B : A, B ? ldb : lda, beta, C, ldc);
+        if (e == cudaSuccess && B) e = sgemm_tri(h, tri, ta, tb, n, n, k, alpha, B, ldb, A, lda, 1.f, C, ldc);
+        return e;
     }
 };
 
 // ------------------------------------------------------------------ trmm
+// The triangle of A is expanded once into a dense matrix D (zeros outside
+// it, ones on a unit diagonal).  C is then formed in panels along the
+// triangular dimension, each one GEMM over the part of D's rows or columns
+// that is not zero for it: a fraction panel / dim of extra flops.
 struct Tm {
     iclblasHandle_t h;
-    bool left, lower, ta, unit;  // lower: A's stored triangle; ta: op(A) = A^T
+    bool left, ta, oplower;  // ta: op(A) = A^T; oplower: op(A) is lower triangular
     float alpha;
-    const float* A;
-    int lda;
+    const float* D;  // dense na x na expansion of A's triangle, ld = na
+    int na;
     const float* B;
     int ldb;
     float* C;
     int ldc;
-    int m, n;  // C is m x n
-    float* D;  // kLeaf x kLeaf leaf buffer
+    int m, n;
 
-    // op(A) block rows [r, r+nr) x cols [c, c+nc) as a GEMM operand: pointer and transpose flag
-    const float* opblk(int r, int c) const { return ta ? A + (long)r * lda + c : A + (long)c * lda + r; }
+    // op(D) block starting at (r, c), as a GEMM operand
+    const float* opblk(int r, int c) const { return ta ? D + (long)r * na + c : D + (long)c * na + r; }
 
-    // effective triangle of op(A)
-    bool op_lower() const { return lower != ta; }
-
-    // C rows/cols [off, off+t) <- alpha * op(A)[off.., off..] applied to B (left: rows, right: cols)
-    cudaError_t run(int off, int t, float beta0) const
+    cudaError_t run() const
     {
-        if (t <= kLeaf) {
-            expand_tri_kernel<<<grid_for(h, (long)t * t), kThreads, 0, h->stream>>>(
-                t, lower, unit, A + (long)off * lda + off, lda, D);
-            cudaError_t e = cudaGetLastError();
+        const int pw = panel_of(na);
+        for (int p0 = 0; p0 < na; p0 += pw) {
+            const int w = std::min(pw, na - p0);
+            cudaError_t e;
+            if (left) {
+                // C rows [p0, p0+w) = alpha op(D)[p0.., k0..k1) B[k0..k1, :]
+                const int k0 = oplower ? 0 : p0, k1 = oplower ? p0 + w : na;
+                e = sgemm(h, ta ? 1 : 0, 0, w, n, k1 - k0, alpha, opblk(p0, k0), na, B + k0, ldb, 0.f, C + p0, ldc);
+            } else {
+                // C cols [p0, p0+w) = alpha B[:, k0..k1) op(D)[k0..k1, p0..)
+                const int k0 = oplower ? p0 : 0, k1 = oplower ? na : p0 + w;
+                e = sgemm(h, 0, ta ? 1 : 0, m, w, k1 - k0, alpha, B + (long)k0 * ldb, ldb, opblk(k0, p0), na, 0.f,
+                          C + (long)p0 * ldc, ldc);
+            }
             if (e != cudaSuccess) return e;
-            if (left)
-                return sgemm(h, ta ? 1 : 0, 0, t, n, t, alpha, D, t, B + off, ldb, beta0, C + off, ldc);
-            return sgemm(h, 0, ta ? 1 : 0, m, t, t, alpha, B + (long)off * ldb, ldb, D, t, beta0,
-                         C + (long)off * ldc, ldc);
         }
-        const int t1 = split_of(t), t2 = t - t1;
-        const int o1 = off, o2 = off + t1;
-        const bool L = op_lower();
-        if (left) {
-            // C1 = a T11 B1 (+ a T12 B2 if upper); C2 = a T22 B2 (+ a T21 B1 if lower)
-            cudaError_t e = run(o1, t1, beta0);
-            if (e == cudaSuccess) e = run(o2, t2, beta0);
-            if (e != cudaSuccess) return e;
-            if (L)
-                return sgemm(h, ta ? 1 : 0, 0, t2, n, t1, alpha, opblk(o2, o1), lda, B + o1, ldb, 1.f, C + o2, ldc);
-            return sgemm(h, ta ? 1 : 0, 0, t1, n, t2, alpha, opblk(o1, o2), lda, B + o2, ldb, 1.f, C + o1, ldc);
-        }
-        // right: C1 = a B1 T11 (+ a B2 T21 if lower); C2 = a B2 T22 (+ a B1 T12 if upper)
-        cudaError_t e = run(o1, t1, beta0);
-        if (e == cudaSuccess) e = run(o2, t2, beta0);
-        if (e != cudaSuccess) return e;
-        if (L)
-            return sgemm(h, 0, ta ? 1 : 0, m, t1, t2, alpha, B + (long)o2 * ldb, ldb, opblk(o2, o1), lda, 1.f,
-                         C + (long)o1 * ldc, ldc);
-        return sgemm(h, 0, ta ? 1 : 0, m, t2, t1, alpha, B + (long)o1 * ldb, ldb, opblk(o1, o2), lda, 1.f,
-                     C + (long)o2 * ldc, ldc);
+        return cudaSuccess;
     }
 };
 
@@ -223,19 +166,15 @@ size_t extent_bytes(int rows, int cols, int ld)
 cudaError_t ssyrk(iclblasHandle_t h, int uplo, int trans, int n, int k, float alpha, const float* A, int lda,
                   float beta, float* C, int ldc)
 {
-    float* W = (float*)solver_scratch(h, sizeof(float) * kLeaf * kLeaf);
-    if (!W) return cudaErrorMemoryAllocation;
-    Rk r{h, uplo == ICLBLAS_FILL_MODE_LOWER, trans != ICLBLAS_OP_N, k, alpha, beta, A, nullptr, lda, 0, C, ldc, W};
-    return r.run(0, n);
+    Rk r{h, uplo == ICLBLAS_FILL_MODE_LOWER, trans != ICLBLAS_OP_N, n, k, alpha, beta, A, nullptr, lda, 0, C, ldc};
+    return r.run();
 }
 
 cudaError_t ssyr2k(iclblasHandle_t h, int uplo, int trans, int n, int k, float alpha, const float* A, int lda,
                    const float* B, int ldb, float beta, float* C, int ldc)
 {
-    float* W = (float*)solver_scratch(h, sizeof(float) * kLeaf * kLeaf);
-    if (!W) return cudaErrorMemoryAllocation;
-    Rk r{h, uplo == ICLBLAS_FILL_MODE_LOWER, trans != ICLBLAS_OP_N, k, alpha, beta, A, B, lda, ldb, C, ldc, W};
-    return r.run(0, n);
+    Rk r{h, uplo == ICLBLAS_FILL_MODE_LOWER, trans != ICLBLAS_OP_N, n, k, alpha, beta, A, B, lda, ldb, C, ldc};
+    return r.run();
 }
 
 cudaError_t ssymm(iclblasHandle_t h, int side, int uplo, int m, int n, float alpha, const float* A, int lda,
@@ -258,25 +197,30 @@ cudaError_t strmm(iclblasHandle_t h, int side, int uplo, int transa, int diag, i
 {
     if (alpha == 0.f)  // C = 0; A and B are not read
         return sgemm(h, 0, 0, m, n, 0, 0.f, nullptr, 1, nullptr, 1, 0.f, C, ldc);
+    const bool left = side == ICLBLAS_SIDE_LEFT;
+    const int na = left ? m : n;
     const bool copy_b = overlaps(B, extent_bytes(m, n, ldb), C, extent_bytes(m, n, ldc));
-    const size_t leaf_bytes = sizeof(float) * kLeaf * kLeaf;
+    const size_t d_bytes = ((sizeof(float) * (size_t)na * (size_t)na) + 255) & ~(size_t)255;
     const size_t bcopy_bytes = copy_b ? sizeof(float) * (size_t)m * (size_t)n : 0;
-    char* ws = (char*)solver_scratch(h, leaf_bytes + bcopy_bytes);
+    char* ws = (char*)solver_scratch(h, d_bytes + bcopy_bytes);
     if (!ws) return cudaErrorMemoryAllocation;
+    float* D = (float*)ws;
+    const bool lower = uplo == ICLBLAS_FILL_MODE_LOWER, ta = transa != ICLBLAS_OP_N;
+    expand_tri_kernel<<<grid_for(h, (long)na * na), kThreads, 0, h->stream>>>(na, lower, diag == ICLBLAS_DIAG_UNIT, A,
+                                                                             lda, D);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
     const float* Bsrc = B;
     int ldbs = ldb;
     if (copy_b) {
-        float* Bc = (float*)(ws + leaf_bytes);
+        float* Bc = (float*)(ws + d_bytes);
         copy_matrix_kernel<<<grid_for(h, (long)m * n), kThreads, 0, h->stream>>>(m, n, B, ldb, Bc, m);
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
         Bsrc = Bc;
         ldbs = m;
     }
-    const bool left = side == ICLBLAS_SIDE_LEFT;
-    Tm t{h, left, uplo == ICLBLAS_FILL_MODE_LOWER, transa != ICLBLAS_OP_N, diag == ICLBLAS_DIAG_UNIT,
-         alpha, A, lda, Bsrc, ldbs, C, ldc, m, n, (float*)ws};
-    return t.run(0, left ? m : n, 0.f);
+    Tm t{h, left, ta, lower != ta, alpha, D, na, Bsrc, ldbs, C, ldc, m, n};
+    return t.run();
 }
 
 }  // namespace iclb

@@ -99,13 +99,51 @@ __global__ void __launch_bounds__(kThreads) symv_tile_kernel(int n, const T* __r
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const long row0 = (long)I * TS, col0 = (long)J * TS;
     const bool diag = (I == J);
+    const long r0 = row0 + (long)lane * per;  // first row of this lane's word
+    const bool full_word = r0 + per <= n;
+
+    // Every word this thread reads is requested before anything else, so a
+    // CTA keeps its whole 64 KB (single) / 32 KB (complex) tile in flight.
+    T a[TL::PASSES][per];
+    if (VEC && row0 + TS <= n && col0 + TS <= n) {
+        // interior tile: every word is whole and in range, no conditions
+        const T* src = A + (col0 + w) * lda + r0;
+        float4 v[TL::PASSES];
+#pragma unroll
+        for (int p = 0; p < TL::PASSES; ++p) v[p] = ld_stream4((const float4*)(src + (long)p * kWarps * lda));
+#pragma unroll
+        for (int p = 0; p < TL::PASSES; ++p) {
+            const T* e = (const T*)&v[p];
+#pragma unroll
+            for (int k = 0; k < per; ++k) a[p][k] = e[k];
+        }
+    } else {
+#pragma unroll
+    for (int p = 0; p < TL::PASSES; ++p) {
+        const long c = col0 + w + (long)p * kWarps;
+        if (c < n && r0 < n) {
+            const T* src = A + c * lda + r0;
+            if (VEC && full_word) {
+                float4 v = ld_stream4((const float4*)src);
+                const T* e = (const T*)&v;
+#pragma unroll
+                for (int k = 0; k < per; ++k) a[p][k] = e[k];
+            } else {
+#pragma unroll
+                for (int k = 0; k < per; ++k) a[p][k] = (r0 + k < n) ? src[k] : zero_t(T());
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < per; ++k) a[p][k] = zero_t(T());
+        }
+    }
+    }
     for (int k = threadIdx.x; k < TS; k += kThreads) {
         xr[k] = (row0 + k < n) ? x[(row0 + k) * incx] : zero_t(T());
         xc[k] = (col0 + k < n) ? x[(col0 + k) * incx] : zero_t(T());
     }
     __syncthreads();
 
-    const long r0 = row0 + (long)lane * per;  // first row of this lane's word
     T racc[per];
     T xw[per];
 #pragma unroll
@@ -113,55 +151,29 @@ __global__ void __launch_bounds__(kThreads) symv_tile_kernel(int n, const T* __r
         racc[k] = zero_t(T());
         xw[k] = xr[lane * per + k];
     }
-    const bool full_word = r0 + per <= n;
-
-    constexpr int B = 4;  // words in flight per thread
-#pragma unroll 1
-    for (int p0 = 0; p0 < TL::PASSES; p0 += B) {
-        T a[B][per];
 #pragma unroll
-        for (int b = 0; b < B; ++b) {
-            const long c = col0 + w + (long)(p0 + b) * kWarps;
-            if (c < n && r0 < n) {
-                const T* src = A + c * lda + r0;
-                if (VEC && full_word) {
-                    float4 v = ld_stream4((const float4*)src);
-                    const T* e = (const T*)&v;
+    for (int p = 0; p < TL::PASSES; ++p) {
+        const int cl = w + p * kWarps;  // column within the tile
+        const long c = col0 + cl;
+        const T xcv = xc[cl];
+        T csum = zero_t(T());
 #pragma unroll
-                    for (int k = 0; k < per; ++k) a[b][k] = e[k];
-                } else {
-#pragma unroll
-                    for (int k = 0; k < per; ++k) a[b][k] = (r0 + k < n) ? src[k] : zero_t(T());
-                }
-            } else {
-#pragma unroll
-                for (int k = 0; k < per; ++k) a[b][k] = zero_t(T());
+        for (int k = 0; k < per; ++k) {
+            const long r = r0 + k;
+            T v = a[p][k];
+            bool in_row = true, in_col = true;
+            if (diag) {
+                // stored triangle only; the diagonal counts once (as a row term)
+                in_row = LOWER ? (r >= c) : (r <= c);
+                in_col = LOWER ? (r > c) : (r < c);
+                if (r == c && HERM) v = real_part(v);
             }
+            if (in_row) mac(racc[k], v, xcv);
+            if (in_col) mac(csum, HERM ? conj_t(v) : v, xw[k]);
         }
 #pragma unroll
-        for (int b = 0; b < B; ++b) {
-            const int cl = w + (p0 + b) * kWarps;  // column within the tile
-            const long c = col0 + cl;
-            const T xcv = xc[cl];
-            T csum = zero_t(T());
-#pragma unroll
-            for (int k = 0; k < per; ++k) {
-                const long r = r0 + k;
-                T v = a[b][k];
-                bool in_row = true, in_col = true;
-                if (diag) {
-                    // stored triangle only; the diagonal counts once (as a row term)
-                    in_row = LOWER ? (r >= c) : (r <= c);
-                    in_col = LOWER ? (r > c) : (r < c);
-                    if (r == c && HERM) v = real_part(v);
-                }
-                if (in_row) mac(racc[k], v, xcv);
-                if (in_col) mac(csum, HERM ? conj_t(v) : v, xw[k]);
-            }
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) csum = add_t(csum, shfl_xor_t(csum, o));
-            if (lane == 0) colp[cl] = csum;
-        }
+        for (int o = 16; o > 0; o >>= 1) csum = add_t(csum, shfl_xor_t(csum, o));
+        if (lane == 0) colp[cl] = csum;
     }
 #pragma unroll
     for (int k = 0; k < per; ++k) red[w][lane * per + k] = racc[k];

@@ -23,7 +23,7 @@
 namespace iclb {
 
 cudaError_t sgemm_simt(iclblasHandle_t h, int ta, int tb, int m, int n, int k, float alpha, const float* A, int lda,
-                       const float* B, int ldb, float beta, float* C, int ldc);
+                       const float* B, int ldb, float beta, float* C, int ldc, int tri);
 cudaError_t cgemm_simt(iclblasHandle_t h, int ta, int tb, int m, int n, int k, cfloat alpha, const cfloat* A, int lda,
                        const cfloat* B, int ldb, cfloat beta, cfloat* C, int ldc);
 
