@@ -7,10 +7,10 @@
 // formed from registers.  The triangle is cut into TS x TS tiles (TS = 128
 // single, 64 complex: 32 lanes x one 16-byte word of rows); one CTA per
 // stored tile (I, J):
-//   - lane l owns rows [l*per, l*per + per) of the tile, warp w the columns
-//     w, w+8, ...; A is read in 16-byte words down each column;
+//   - lane l owns rows [l*per, l*per + per) of the tile, warp w of W the
+//     columns w, w+W, ...; A is read in 16-byte words down each column;
 //   - row contributions sum in registers across the warp's columns and then
-//     across the 8 warps (shared memory);
+//     across the warps (shared memory);
 //   - column contributions sum over the word in registers and over the 32
 //     lanes of the column (shuffle tree);
 //   - diagonal tiles read only the stored triangle (elements outside it are
@@ -32,8 +32,7 @@
 namespace iclb {
 namespace {
 
-constexpr int kThreads = 256;
-constexpr int kWarps = kThreads / 32;
+constexpr int kThreads = 256;  // finish kernel
 
 bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 
@@ -59,11 +58,17 @@ __device__ __forceinline__ cfloat shfl_xor_t(cfloat v, int o)
     return cfloat{__shfl_xor_sync(0xffffffffu, v.re, o), __shfl_xor_sync(0xffffffffu, v.im, o)};
 }
 
+// Tile geometry.  Single: 128 x 128 tiles, 16 warps of 8 columns (512
+// threads, 64 registers: two CTAs and 32 warps per SM; 8 warps of 16 columns
+// ran at 0.80 of HBM peak instead of 0.84).  Complex: 64 x 64 tiles, 8 warps
+// of 8 columns (16 warps of 4 ran at 0.48 instead of 0.61).
 template <class T>
 struct Tile {
     static constexpr int per = (int)(16 / sizeof(T));  // elements per 16-byte word
     static constexpr int TS = 32 * per;                // tile rows = tile columns
-    static constexpr int PASSES = TS / kWarps;         // columns per warp
+    static constexpr int THREADS = sizeof(T) == 4 ? 512 : 256;
+    static constexpr int WARPS = THREADS / 32;
+    static constexpr int PASSES = TS / WARPS;          // columns per warp
 };
 
 // Stored tile number t -> (I, J) with I >= J (row-major over the lower block
@@ -77,21 +82,61 @@ __device__ __forceinline__ void tile_of(long t, int& I, int& J)
     J = (int)(t - i * (i + 1) / 2);
 }
 
+// Row and column products of one thread's words of a tile: racc[k] +=
+// A(r, c) x_c over the thread's columns, csum[p] = sum_k A(r, c) x_r (or
+// conj(A) for HERM).  DIAG: the tile is on the diagonal; only the stored
+// triangle counts and the diagonal counts once, as a row term.
+template <class T, bool LOWER, bool HERM, bool DIAG>
+__device__ __forceinline__ void tile_products(const T (&a)[Tile<T>::PASSES][Tile<T>::per], T (&racc)[Tile<T>::per],
+                                              T (&csum)[Tile<T>::PASSES], const T (&xw)[Tile<T>::per], const T* xc,
+                                              int w, long r0, long col0)
+{
+    constexpr int per = Tile<T>::per;
+#pragma unroll
+    for (int p = 0; p < Tile<T>::PASSES; ++p) {
+        const int cl = w + p * Tile<T>::WARPS;
+        const T xcv = xc[cl];
+        T cs = zero_t(T());
+#pragma unroll
+        for (int k = 0; k < per; ++k) {
+            T v = a[p][k];
+            if (DIAG) {
+                const long r = r0 + k, c = col0 + cl;
+                if (r == c && HERM) v = real_part(v);
+                if (LOWER ? (r >= c) : (r <= c)) mac(racc[k], v, xcv);
+                if (LOWER ? (r > c) : (r < c)) mac(cs, HERM ? conj_t(v) : v, xw[k]);
+            } else {
+                mac(racc[k], v, xcv);
+                mac(cs, HERM ? conj_t(v) : v, xw[k]);
+            }
+        }
+        csum[p] = cs;
+    }
+}
+
 template <class T, bool LOWER, bool HERM, bool VEC>
-__global__ void __launch_bounds__(kThreads) symv_tile_kernel(int n, const T* __restrict__ A, long lda,
-                                                             const T* __restrict__ x, long incx, T* __restrict__ Q,
-                                                             long qld)
+__global__ void __launch_bounds__(Tile<T>::THREADS) symv_tile_kernel(int n, int nb, const T* __restrict__ A, long lda,
+                                                                 const T* __restrict__ x, long incx,
+                                                                 T* __restrict__ Q, long qld)
 {
     using TL = Tile<T>;
     constexpr int per = TL::per, TS = TL::TS;
     __shared__ T xr[TS];              // x over the tile's rows
     __shared__ T xc[TS];              // x over the tile's columns
-    __shared__ T red[kWarps][TS + 1]; // row partials per warp
+    __shared__ T red[TL::WARPS][TS + 1]; // row partials per warp
     __shared__ T colp[TS];
 
+    // Consecutive CTAs take consecutive tiles of one block column (adjacent
+    // rows of the same columns: DRAM pages stay open): for upper storage the
+    // row-major lower enumeration transposed, for lower storage the same
+    // enumeration mirrored through the anti-diagonal.
     int I, J;
     tile_of(blockIdx.x, I, J);
-    if (!LOWER) {
+    if (LOWER) {
+        const int a = I, b = J;
+        I = nb - 1 - b;
+        J = nb - 1 - a;
+    } else {
         const int t = I;
         I = J;
         J = t;
@@ -110,7 +155,7 @@ __global__ void __launch_bounds__(kThreads) symv_tile_kernel(int n, const T* __r
         const T* src = A + (col0 + w) * lda + r0;
         float4 v[TL::PASSES];
 #pragma unroll
-        for (int p = 0; p < TL::PASSES; ++p) v[p] = ld_stream4((const float4*)(src + (long)p * kWarps * lda));
+        for (int p = 0; p < TL::PASSES; ++p) v[p] = ld_stream4((const float4*)(src + (long)p * TL::WARPS * lda));
 #pragma unroll
         for (int p = 0; p < TL::PASSES; ++p) {
             const T* e = (const T*)&v[p];
@@ -120,7 +165,7 @@ __global__ void __launch_bounds__(kThreads) symv_tile_kernel(int n, const T* __r
     } else {
 #pragma unroll
     for (int p = 0; p < TL::PASSES; ++p) {
-        const long c = col0 + w + (long)p * kWarps;
+        const long c = col0 + w + (long)p * TL::WARPS;
         if (c < n && r0 < n) {
             const T* src = A + c * lda + r0;
             if (VEC && full_word) {
@@ -138,7 +183,7 @@ __global__ void __launch_bounds__(kThreads) symv_tile_kernel(int n, const T* __r
         }
     }
     }
-    for (int k = threadIdx.x; k < TS; k += kThreads) {
+    for (int k = threadIdx.x; k < TS; k += TL::THREADS) {
         xr[k] = (row0 + k < n) ? x[(row0 + k) * incx] : zero_t(T());
         xc[k] = (col0 + k < n) ? x[(col0 + k) * incx] : zero_t(T());
     }
@@ -151,37 +196,42 @@ __global__ void __launch_bounds__(kThreads) symv_tile_kernel(int n, const T* __r
         racc[k] = zero_t(T());
         xw[k] = xr[lane * per + k];
     }
+    T csum[TL::PASSES];
+    if (diag)
+        tile_products<T, LOWER, HERM, true>(a, racc, csum, xw, xc, w, r0, col0);
+    else
+        tile_products<T, LOWER, HERM, false>(a, racc, csum, xw, xc, w, r0, col0);
+    // column sums over the 32 lanes, all PASSES columns at once: each step
+    // halves the values a lane carries (PASSES - 1 shuffles instead of
+    // 5 * PASSES), the last steps reduce the one value left
+    int bit = 16;
 #pragma unroll
-    for (int p = 0; p < TL::PASSES; ++p) {
-        const int cl = w + p * kWarps;  // column within the tile
-        const long c = col0 + cl;
-        const T xcv = xc[cl];
-        T csum = zero_t(T());
+    for (int hcount = TL::PASSES / 2; hcount >= 1; hcount /= 2) {
+        const bool up = (lane & bit) != 0;
 #pragma unroll
-        for (int k = 0; k < per; ++k) {
-            const long r = r0 + k;
-            T v = a[p][k];
-            bool in_row = true, in_col = true;
-            if (diag) {
-                // stored triangle only; the diagonal counts once (as a row term)
-                in_row = LOWER ? (r >= c) : (r <= c);
-                in_col = LOWER ? (r > c) : (r < c);
-                if (r == c && HERM) v = real_part(v);
-            }
-            if (in_row) mac(racc[k], v, xcv);
-            if (in_col) mac(csum, HERM ? conj_t(v) : v, xw[k]);
+        for (int i = 0; i < hcount; ++i) {
+            const T send = up ? csum[i] : csum[i + hcount];
+            const T keep = up ? csum[i + hcount] : csum[i];
+            csum[i] = add_t(keep, shfl_xor_t(send, bit));
         }
+        bit >>= 1;
+    }
+    for (int b = bit; b >= 1; b >>= 1) csum[0] = add_t(csum[0], shfl_xor_t(csum[0], b));
+    // lane bits above `bit` name the column this lane's sum belongs to
+    if ((lane & (2 * bit - 1)) == 0) {
+        int pcol = 0;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) csum = add_t(csum, shfl_xor_t(csum, o));
-        if (lane == 0) colp[cl] = csum;
+        for (int b = 16, v = TL::PASSES / 2; v >= 1; b >>= 1, v >>= 1)
+            if (lane & b) pcol += v;
+        colp[w + pcol * TL::WARPS] = csum[0];
     }
 #pragma unroll
     for (int k = 0; k < per; ++k) red[w][lane * per + k] = racc[k];
     __syncthreads();
-    for (int k = threadIdx.x; k < TS; k += kThreads) {
+    for (int k = threadIdx.x; k < TS; k += TL::THREADS) {
         T s = red[0][k];
 #pragma unroll
-        for (int ww = 1; ww < kWarps; ++ww) s = add_t(s, red[ww][k]);
+        for (int ww = 1; ww < TL::WARPS; ++ww) s = add_t(s, red[ww][k]);
         if (diag) {
             Q[(long)I * qld + row0 + k] = add_t(s, colp[k]);
         } else {
@@ -242,7 +292,7 @@ cudaError_t symv_tiles(iclblasHandle_t h, bool lower, int n, const T* A, int lda
     const bool vec = aligned16(A) && lda % Tile<T>::per == 0;
     const unsigned grid = (unsigned)tiles;
 #define SYMV_LAUNCH(L, V) \
-    symv_tile_kernel<T, L, HERM, V><<<grid, kThreads, 0, h->stream>>>(n, A, lda, x, incx, Q, qld)
+    symv_tile_kernel<T, L, HERM, V><<<grid, Tile<T>::THREADS, 0, h->stream>>>(n, nb, A, lda, x, incx, Q, qld)
     if (lower) {
         if (vec) SYMV_LAUNCH(true, true); else SYMV_LAUNCH(true, false);
     } else {
