@@ -755,6 +755,72 @@ def run_level23x_study(args, torch):
             h.set_math_mode(B.MATH_PLAIN_FP32)
 
 
+# ResNet-50's 1x1 convolutions as GEMMs (M = batch * H * W, K = input
+# channels, N = output channels), batch 32: the shapes the reference's
+# experimental/kernels/*.cl target.
+CONV1X1_SHAPES = [
+    ("56x56 64->256", 32 * 56 * 56, 64, 256), ("56x56 256->64", 32 * 56 * 56, 256, 64),
+    ("28x28 128->512", 32 * 28 * 28, 128, 512), ("28x28 512->128", 32 * 28 * 28, 512, 128),
+    ("14x14 256->1024", 32 * 14 * 14, 256, 1024), ("14x14 1024->256", 32 * 14 * 14, 1024, 256),
+    ("7x7 512->2048", 32 * 7 * 7, 512, 2048), ("7x7 2048->512", 32 * 7 * 7, 2048, 512),
+]
+
+
+def run_conv1x1_study(args, torch):
+    """ResNet-50 1x1-convolution GEMMs (activations M x K, weights K x N,
+    output M x N; synthetic U(-1,1), seed 5): HGEMM (half storage, FP32
+    accumulation) and SGEMM in every math mode, TFLOP/s = 2 M N K / event
+    time (median of 10), relative Frobenius error against FP64 (torch,
+    plumbing only)."""
+    from clgpu_b200 import iclblas as B
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(device=dev)
+    g = torch.Generator(device=dev).manual_seed(5)
+    modes = [("fp32_simt", B.MATH_PLAIN_FP32), ("tf32", B.MATH_TF32), ("3xbf16", B.MATH_BF16X3),
+             ("6xbf16", B.MATH_BF16X6)]
+    with B.Handle() as h, torch.cuda.stream(stream):
+        h.set_stream(stream)
+        for name, M, K, N in CONV1X1_SHAPES:
+            A = torch.rand(K, M, generator=g, device=dev) * 2 - 1     # column-major M x K
+            W = torch.rand(N, K, generator=g, device=dev) * 2 - 1     # column-major K x N
+            C = torch.empty(N, M, device=dev)
+            Ah, Wh, Ch = A.half(), W.half(), torch.empty(N, M, device=dev, dtype=torch.half)
+            ref = W.double() @ A.double()          # C^T (N x M) row-major = column-major M x N
+            refh = Wh.double() @ Ah.double()
+            flops = 2.0 * M * N * K
+
+            def timed(f):
+                for _ in range(3):
+                    B.check(f(), name)
+                torch.cuda.synchronize()
+                ts = []
+                for _ in range(10):
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    B.check(f(), name)
+                    e1.record(stream)
+                    torch.cuda.synchronize()
+                    ts.append(e0.elapsed_time(e1))
+                return float(np.median(ts))
+            ms = timed(lambda: B.iclblasHgemm(h, 0, 0, M, N, K, 1.0, Ah, M, Wh, K, 0.0, Ch, M))
+            err = float(torch.linalg.norm(Ch.double() - refh) / torch.linalg.norm(refh))
+            print(json.dumps({"shape": name, "M": M, "K": K, "N": N, "routine": "hgemm", "ms": round(ms, 4),
+                              "tflops": round(flops / (ms / 1e3) / 1e12, 1), "rel_fro_err_vs_fp64": err}),
+                  flush=True)
+            for mname, mode in modes:
+                h.set_math_mode(mode)
+                ms = timed(lambda: B.iclblasSgemm(h, 0, 0, M, N, K, 1.0, A, M, W, K, 0.0, C, M))
+                err = float(torch.linalg.norm(C.double() - ref) / torch.linalg.norm(ref))
+                print(json.dumps({"shape": name, "M": M, "K": K, "N": N, "routine": "sgemm", "mode": mname,
+                                  "ms": round(ms, 4), "tflops": round(flops / (ms / 1e3) / 1e12, 1),
+                                  "rel_fro_err_vs_fp64": err}), flush=True)
+            h.set_math_mode(B.MATH_PLAIN_FP32)
+            del A, W, C, Ah, Wh, Ch, ref, refh
+            torch.cuda.empty_cache()
+
+
 def run_batched_study(args, torch):
     """Batched uneven TRSM + adjoint config: 512 instances, n ~ UniformInt[32,1024],
     nrhs ~ UniformInt[1,256], L built as in the STRSM config (diagonal U(1,2),
@@ -985,11 +1051,12 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-operand (C ABI) leg")
     ap.add_argument("--only", default="", help="comma-separated subset of the sweep's calls")
     ap.add_argument("--n1", type=int, default=N1, help="level-1 vector length (default 2^28)")
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "gemm", "trsm", "batched", "level1x", "level23x"],
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "gemm", "trsm", "batched", "level1x", "level23x", "conv1x1"],
                     help="sweep: the bandwidth config (default); gemm / trsm / batched: the precision, "
                          "triangular-solve and batched-solve config studies; level1x: copy / swap / "
                          "rotation / iamin bandwidth study; level23x: ger / symv / hemv bandwidth and "
-                         "syrk / syr2k / symm / trmm throughput study")
+                         "syrk / syr2k / symm / trmm throughput study; conv1x1: ResNet-50 1x1-convolution "
+                         "GEMM shapes in HGEMM and every SGEMM mode")
     ap.add_argument("--trsm-m", type=int, default=8192)
     ap.add_argument("--trsm-n", type=int, default=4096)
     ap.add_argument("--trsv-n", type=int, default=16384)
@@ -1040,6 +1107,9 @@ def main():
         return
     if args.workload == "level23x":
         run_level23x_study(args, torch)
+        return
+    if args.workload == "conv1x1":
+        run_conv1x1_study(args, torch)
         return
     if world > 1:
         torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))

@@ -1347,6 +1347,37 @@ extern "C" iclblasStatus_t iclblasStrmm(iclblasHandle_t h, iclblasSideMode_t sid
 }
 
 // ------------------------------------------------------------------------
+// half-precision GEMM (extension; the reference ships FP16 GEMM only as the
+// stand-alone experimental/kernels/hgemm_buf_*.cl, outside its API)
+// ------------------------------------------------------------------------
+extern "C" iclblasStatus_t iclblasHgemm(iclblasHandle_t h, iclblasOperation_t transa, iclblasOperation_t transb, int m,
+                                        int n, int k, const float* alpha, const unsigned short* A, int lda,
+                                        const unsigned short* B, int ldb, const float* beta, unsigned short* C, int ldc)
+{
+    if (m < 0 || n < 0 || k < 0) return ICLBLAS_STATUS_INVALID_VALUE;
+    return guarded([&]() -> iclblasStatus_t {
+        Params p; p.present = P_N | P_M | P_K | P_A | P_LDA | P_B | P_LDB | P_C | P_LDC;
+        p.n = n; p.m = m; p.k = k; p.A = A; p.lda = lda; p.B = B; p.ldb = ldb; p.C = C; p.ldc = ldc;
+        VALIDATE(p, h);
+        if (!alpha || !beta) return ICLBLAS_STATUS_INVALID_VALUE;
+        if (transa < ICLBLAS_OP_N || transa > ICLBLAS_OP_C || transb < ICLBLAS_OP_N || transb > ICLBLAS_OP_C)
+            return ICLBLAS_STATUS_INVALID_VALUE;
+        const int ar = transa == ICLBLAS_OP_N ? m : k, ac = transa == ICLBLAS_OP_N ? k : m;
+        const int br = transb == ICLBLAS_OP_N ? k : n, bc = transb == ICLBLAS_OP_N ? n : k;
+        Stager st(h);
+        int ia = st.add(A, mat_extent(ar, ac, lda) * 2, false);
+        int ib = st.add(B, mat_extent(br, bc, ldb) * 2, false);
+        int ic = st.add(C, mat_extent(m, n, ldc) * 2, true, *beta != 0.f || ldc > m);
+        cudaError_t e = st.stage_in();
+        if (e == cudaSuccess)
+            e = iclb::hgemm(h, transa, transb, m, n, k, *alpha, st.dev<unsigned short>(ia), lda,
+                            st.dev<unsigned short>(ib), ldb, *beta, st.dev<unsigned short>(ic), ldc);
+        if (e == cudaSuccess) e = st.finish();
+        return map_cuda(e);
+    });
+}
+
+// ------------------------------------------------------------------------
 // adjoints (extension)
 // ------------------------------------------------------------------------
 extern "C" iclblasStatus_t iclblasStrsm_backward(iclblasHandle_t h, iclblasSideMode_t side, iclblasFillMode_t uplo,

@@ -4,6 +4,8 @@
 // scores (libs/blas/functions_base.hpp:164-223); here the routine maps
 // directly: PLAIN_FP32 runs the CUDA-core FFMA kernel (bit-identical to the
 // reference's FP32 FMA order), the tensor-core modes run the tcgen05 kernel.
+#include <cuda_fp16.h>
+
 #include "common.cuh"
 
 namespace iclb {
@@ -13,6 +15,8 @@ cudaError_t sgemm_simt(iclblasHandle_t h, int ta, int tb, int m, int n, int k, f
 cudaError_t cgemm_simt(iclblasHandle_t h, int ta, int tb, int m, int n, int k, cfloat alpha, const cfloat* A, int lda,
                        const cfloat* B, int ldb, cfloat beta, cfloat* C, int ldc);
 namespace tc {
+cudaError_t hgemm_tc(iclblasHandle_t h, int ta, int tb, int m, int n, int k, float alpha, const __half* A, int lda,
+                     const __half* B, int ldb, float beta, __half* C, int ldc);
 template <class T>
 cudaError_t gemm_tc(iclblasHandle_t h, int ta, int tb, int m, int n, int k, T alpha, const T* A, int lda, const T* B,
                     int ldb, T beta, T* C, int ldc, int tri);
@@ -32,6 +36,14 @@ cudaError_t sgemm(iclblasHandle_t h, int ta, int tb, int m, int n, int k, float 
                   const float* B, int ldb, float beta, float* C, int ldc)
 {
     return sgemm_tri(h, 0, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+}
+
+cudaError_t hgemm(iclblasHandle_t h, int ta, int tb, int m, int n, int k, float alpha, const void* A, int lda,
+                  const void* B, int ldb, float beta, void* C, int ldc)
+{
+    if (m == 0 || n == 0) return cudaSuccess;
+    return tc::hgemm_tc(h, ta, tb, m, n, k, alpha, (const __half*)A, lda, (const __half*)B, ldb, beta, (__half*)C,
+                        ldc);
 }
 
 cudaError_t cgemm(iclblasHandle_t h, int ta, int tb, int m, int n, int k, cfloat alpha, const cfloat* A, int lda,

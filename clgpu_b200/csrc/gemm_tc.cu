@@ -39,6 +39,7 @@
 // returns.  Every TMA load targets the issuing CTA's own shared memory.
 #include <cuda.h>
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include <algorithm>
 #include <mutex>
@@ -83,6 +84,8 @@ struct Params {
     long ldc;          // in elements of the output type
     int* status;
     int tri;           // 0: full C; 1: only row >= col is written; 2: only row <= col (real C)
+    int ab_fmt;        // kind::f16 operand format: 1 bf16 (split planes), 0 f16 (HGEMM)
+    int out_half;      // real C stored as IEEE half (HGEMM)
 };
 
 // ---------------------------------------------------------------- PTX helpers
@@ -367,7 +370,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     } else if (warp == 1) {
         // ---------------------------------------------------------- MMA issuer
         if (lane == 0) {
-            const uint32_t idesc = instr_desc(TF32 ? 2u : 1u, BN);
+            const uint32_t idesc = instr_desc(TF32 ? 2u : (uint32_t)p.ab_fmt, BN);
             int s = 0;
             uint32_t ph = 0;
             int acc = 0;
@@ -445,7 +448,28 @@ __global__ void __launch_bounds__(THREADS, 1)
             // C is read in groups of 8 columns before any of them is stored,
             // so the loads overlap (columns of C never alias for ldc >= M)
             if (row < p.M) {
-                if (!p.complex_out) {
+                if (p.out_half) {
+                    __half* const Ch = (__half*)p.C;
+#pragma unroll
+                    for (int j0 = 0; j0 < EPI_COLS; j0 += 8) {
+                        float cv[8];
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) {
+                            const int col = col0 + j0 + j;
+                            cv[j] = (!beta_zero && col < p.N && in_tri(p.tri, row, col))
+                                        ? __half2float(Ch[(long)col * p.ldc + row])
+                                        : 0.f;
+                        }
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) {
+                            const int col = col0 + j0 + j;
+                            if (col < p.N && in_tri(p.tri, row, col))
+                                Ch[(long)col * p.ldc + row] = __float2half_rn(
+                                    beta_zero ? __fmul_rn(p.alpha_re, sum[j0 + j])
+                                              : fmaf(p.alpha_re, sum[j0 + j], __fmul_rn(p.beta_re, cv[j])));
+                        }
+                    }
+                } else if (!p.complex_out) {
 #pragma unroll
                     for (int j0 = 0; j0 < EPI_COLS; j0 += 8) {
                         float cv[8];
@@ -675,7 +699,8 @@ __global__ void __launch_bounds__(THREADS, 1)
     } else if (warp == 1) {
         // ---------------------------------------------------------- MMA issuer (leader only)
         if (lane == 0 && leader) {
-            const uint32_t idesc = (1u << 4) | ((TF32 ? 2u : 1u) << 7) | ((TF32 ? 2u : 1u) << 10) |
+            const uint32_t fmt = TF32 ? 2u : (uint32_t)p.ab_fmt;
+            const uint32_t idesc = (1u << 4) | (fmt << 7) | (fmt << 10) |
                                    ((uint32_t)(BN >> 3) << 17) | ((uint32_t)((2 * BM) >> 4) << 24);
             int s = 0;
             uint32_t ph = 0;
@@ -752,7 +777,28 @@ __global__ void __launch_bounds__(THREADS, 1)
             const int col0 = tn * BN + half * EPI_COLS;
             const bool beta_zero = p.beta_re == 0.f && p.beta_im == 0.f;
             if (row < p.M) {
-                if (!p.complex_out) {
+                if (p.out_half) {
+                    __half* const Ch = (__half*)p.C;
+#pragma unroll
+                    for (int j0 = 0; j0 < EPI_COLS; j0 += 8) {
+                        float cv[8];
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) {
+                            const int col = col0 + j0 + j;
+                            cv[j] = (!beta_zero && col < p.N && in_tri(p.tri, row, col))
+                                        ? __half2float(Ch[(long)col * p.ldc + row])
+                                        : 0.f;
+                        }
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) {
+                            const int col = col0 + j0 + j;
+                            if (col < p.N && in_tri(p.tri, row, col))
+                                Ch[(long)col * p.ldc + row] = __float2half_rn(
+                                    beta_zero ? __fmul_rn(p.alpha_re, sum[j0 + j])
+                                              : fmaf(p.alpha_re, sum[j0 + j], __fmul_rn(p.beta_re, cv[j])));
+                        }
+                    }
+                } else if (!p.complex_out) {
 #pragma unroll
                     for (int j0 = 0; j0 < EPI_COLS; j0 += 8) {
                         float cv[8];
@@ -898,6 +944,36 @@ __global__ void __launch_bounds__(256) split_real_kernel(int R, int K, const flo
             if (o.nlev > 2)
                 *reinterpret_cast<__nv_bfloat162*>((__nv_bfloat16*)o.plane[2] + off) = __halves2bfloat162(la, lb);
         }
+    }
+}
+
+// IEEE half operands (HGEMM): the same 32 x 64 tiling, values copied into
+// the K-major padded plane unchanged (zeros past K).
+__global__ void __launch_bounds__(256) pack_half_kernel(int R, int K, const __half* __restrict__ S, long rs, long ks,
+                                                        __half* __restrict__ plane, long kpad)
+{
+    __shared__ __half tile[32][66];
+    const int k0 = blockIdx.x * 64, r0 = blockIdx.y * 32, t = threadIdx.x;
+    const __half zero = __float2half_rn(0.f);
+    if (rs == 1) {
+        for (int idx = t; idx < 32 * 64; idx += 256) {
+            const int rr = idx % 32, kk = idx / 32;
+            const int r = r0 + rr, k = k0 + kk;
+            tile[rr][kk] = (r < R && k < K) ? S[(long)r + (long)k * ks] : zero;
+        }
+    } else {
+        for (int idx = t; idx < 32 * 64; idx += 256) {
+            const int kk = idx % 64, rr = idx / 64;
+            const int r = r0 + rr, k = k0 + kk;
+            tile[rr][kk] = (r < R && k < K) ? S[(long)r * rs + k] : zero;
+        }
+    }
+    __syncthreads();
+    for (int idx = t; idx < 32 * 32; idx += 256) {
+        const int kp = idx % 32, rr = idx / 32;
+        const int r = r0 + rr, k = k0 + 2 * kp;
+        if (r >= R || k >= kpad) continue;
+        *reinterpret_cast<__half2*>(plane + (long)r * kpad + k) = __halves2half2(tile[rr][2 * kp], tile[rr][2 * kp + 1]);
     }
 }
 
@@ -1053,43 +1129,15 @@ cudaError_t run_split(iclblasHandle_t h, const T* S, int R, int K, long rs, long
 
 }  // namespace
 
-// Real or complex GEMM on the tensor cores.  `cplx` selects complex operands
-// (T = cfloat); the real GEMM then has M rows, 2N columns and 2K depth.
-template <class T>
-cudaError_t gemm_tc(iclblasHandle_t h, int ta, int tb, int m, int n, int k, T alpha, const T* A, int lda,
-                    const T* B, int ldb, T beta, T* C, int ldc, int tri)
+// Launches the persistent tcgen05 kernel over prepared K-major planes (A:
+// rows_a x kpad, B: rows_b x kpad, one per split level): CTA pairs
+// (256 x 256 tiles) when there are enough pair tiles to fill the GPU; else
+// single CTAs, with 128-wide tiles when 256-wide ones would leave a quarter
+// of the SMs idle.
+cudaError_t launch_engine(iclblasHandle_t h, const ModeInfo& mi, void* const* a_planes, void* const* b_planes,
+                          long rows_a, long rows_b, long kpad, Params& p)
 {
-    constexpr bool cplx = sizeof(T) == sizeof(cfloat);
-    const ModeInfo mi = mode_info(h->math);
-    const int esize = mi.tf32 ? 4 : 2;
-    const int kblk = ROW_BYTES / esize;
-    const long kreal = cplx ? 2L * k : (long)k;
-    const long kpad = (kreal + kblk - 1) / kblk * kblk;
-    const long rows_a = m, rows_b = cplx ? 2L * n : (long)n;
-    const size_t plane_a = (size_t)rows_a * kpad * esize, plane_b = (size_t)rows_b * kpad * esize;
-    const size_t align = 1024;
-    const size_t pa_al = (plane_a + align - 1) / align * align, pb_al = (plane_b + align - 1) / align * align;
-    char* ws = (char*)scratch(h, (pa_al + pb_al) * mi.nlev);
-    if (!ws) return cudaErrorMemoryAllocation;
-    SplitOut oa{}, ob{};
-    oa.nlev = ob.nlev = mi.nlev;
-    oa.tf32 = ob.tf32 = mi.tf32 ? 1 : 0;
-    oa.kpad = ob.kpad = kpad;
-    for (int l = 0; l < mi.nlev; ++l) {
-        oa.plane[l] = ws + l * pa_al;
-        ob.plane[l] = ws + mi.nlev * pa_al + l * pb_al;
-    }
-    // A: L[r=m][k] ; op N: S[m + k*lda] ; op T/C: S[k + m*lda]
-    const bool at = ta != ICLBLAS_OP_N, bt = tb != ICLBLAS_OP_N;
-    cudaError_t e = run_split<T>(h, A, m, k, at ? lda : 1, at ? 1 : lda, ta == ICLBLAS_OP_C, kCplxA, oa, rows_a);
-    if (e != cudaSuccess) return e;
-    // B: L[r=n][k] = op(B)[k][n] ; op N: S[k + n*ldb] ; op T/C: S[n + k*ldb]
-    e = run_split<T>(h, B, n, k, bt ? 1 : ldb, bt ? ldb : 1, tb == ICLBLAS_OP_C, kCplxB, ob, rows_b);
-    if (e != cudaSuccess) return e;
-
-    // CTA pairs (256 x 256 tiles) when there are enough pair tiles to fill the
-    // GPU; else single CTAs, with 128-wide tiles when 256-wide ones would leave
-    // a quarter of the SMs idle
+    const int m = (int)rows_a;
     const int pair_tiles = ceil_div(m, 2 * BM) * ceil_div((long)rows_b, 256);
     const bool pairs = pair_tiles * 2 >= h->sm_count;
     const int tiles256 = ceil_div(m, BM) * ceil_div((long)rows_b, 256);
@@ -1097,32 +1145,9 @@ cudaError_t gemm_tc(iclblasHandle_t h, int ta, int tb, int m, int n, int k, T al
     CUtensorMap ma[3], mb[3];
     for (int l = 0; l < 3; ++l) {
         const int ll = l < mi.nlev ? l : 0;
-        if (!make_map(&ma[l], oa.plane[ll], mi.tf32, rows_a, kpad, BM)) return cudaErrorInvalidValue;
-        if (!make_map(&mb[l], ob.plane[ll], mi.tf32, rows_b, kpad, bn)) return cudaErrorInvalidValue;
+        if (!make_map(&ma[l], a_planes[ll], mi.tf32, rows_a, kpad, BM)) return cudaErrorInvalidValue;
+        if (!make_map(&mb[l], b_planes[ll], mi.tf32, rows_b, kpad, bn)) return cudaErrorInvalidValue;
     }
-    Params p{};
-    p.M = m;
-    p.N = (int)rows_b;
-    p.kblocks = (int)(kpad / kblk);
-    p.nprod = mi.nprod;
-    // 6xBF16 drains the accumulator every K block (its FP32-level accuracy
-    // needs it: 2 blocks per chunk measured 5.9e-7 instead of 2.2e-7 at
-    // 8192^3); 3xBF16 every 4 blocks (its dropped products dominate: 3.84e-6
-    // instead of 3.78e-6, 9 % faster); TF32 accumulates the whole K in TMEM
-    p.chunk = mi.tf32 ? p.kblocks : (mi.nprod == 3 ? 4 : 1);
-    for (int i = 0; i < 6; ++i) { p.pa[i] = mi.pa[i]; p.pb[i] = mi.pb[i]; }
-    p.complex_out = cplx ? 1 : 0;
-    const float* al = (const float*)&alpha;
-    const float* be = (const float*)&beta;
-    p.alpha_re = al[0];
-    p.alpha_im = cplx ? al[1] : 0.f;
-    p.beta_re = be[0];
-    p.beta_im = cplx ? be[1] : 0.f;
-    p.C = (float*)C;
-    p.ldc = ldc;
-    p.status = h->ws.dev_status;
-    p.tri = cplx ? 0 : tri;
-
     if (pairs) {
         auto run2 = [&](auto kernel) -> cudaError_t {
             cudaError_t r = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
@@ -1162,6 +1187,118 @@ cudaError_t gemm_tc(iclblasHandle_t h, int ta, int tb, int m, int n, int k, T al
     };
     if (mi.tf32) return bn == 128 ? run(gemm_tc_kernel<true, 128>) : run(gemm_tc_kernel<true, 256>);
     return bn == 128 ? run(gemm_tc_kernel<false, 128>) : run(gemm_tc_kernel<false, 256>);
+}
+
+// Real or complex GEMM on the tensor cores.  `cplx` selects complex operands
+// (T = cfloat); the real GEMM then has M rows, 2N columns and 2K depth.
+template <class T>
+cudaError_t gemm_tc(iclblasHandle_t h, int ta, int tb, int m, int n, int k, T alpha, const T* A, int lda,
+                    const T* B, int ldb, T beta, T* C, int ldc, int tri)
+{
+    constexpr bool cplx = sizeof(T) == sizeof(cfloat);
+    const ModeInfo mi = mode_info(h->math);
+    const int esize = mi.tf32 ? 4 : 2;
+    const int kblk = ROW_BYTES / esize;
+    const long kreal = cplx ? 2L * k : (long)k;
+    const long kpad = (kreal + kblk - 1) / kblk * kblk;
+    const long rows_a = m, rows_b = cplx ? 2L * n : (long)n;
+    const size_t plane_a = (size_t)rows_a * kpad * esize, plane_b = (size_t)rows_b * kpad * esize;
+    const size_t align = 1024;
+    const size_t pa_al = (plane_a + align - 1) / align * align, pb_al = (plane_b + align - 1) / align * align;
+    char* ws = (char*)scratch(h, (pa_al + pb_al) * mi.nlev);
+    if (!ws) return cudaErrorMemoryAllocation;
+    SplitOut oa{}, ob{};
+    oa.nlev = ob.nlev = mi.nlev;
+    oa.tf32 = ob.tf32 = mi.tf32 ? 1 : 0;
+    oa.kpad = ob.kpad = kpad;
+    for (int l = 0; l < mi.nlev; ++l) {
+        oa.plane[l] = ws + l * pa_al;
+        ob.plane[l] = ws + mi.nlev * pa_al + l * pb_al;
+    }
+    // A: L[r=m][k] ; op N: S[m + k*lda] ; op T/C: S[k + m*lda]
+    const bool at = ta != ICLBLAS_OP_N, bt = tb != ICLBLAS_OP_N;
+    cudaError_t e = run_split<T>(h, A, m, k, at ? lda : 1, at ? 1 : lda, ta == ICLBLAS_OP_C, kCplxA, oa, rows_a);
+    if (e != cudaSuccess) return e;
+    // B: L[r=n][k] = op(B)[k][n] ; op N: S[k + n*ldb] ; op T/C: S[n + k*ldb]
+    e = run_split<T>(h, B, n, k, bt ? 1 : ldb, bt ? ldb : 1, tb == ICLBLAS_OP_C, kCplxB, ob, rows_b);
+    if (e != cudaSuccess) return e;
+
+    Params p{};
+    p.M = m;
+    p.N = (int)rows_b;
+    p.kblocks = (int)(kpad / kblk);
+    p.nprod = mi.nprod;
+    // 6xBF16 drains the accumulator every K block (its FP32-level accuracy
+    // needs it: 2 blocks per chunk measured 5.9e-7 instead of 2.2e-7 at
+    // 8192^3); 3xBF16 every 4 blocks (its dropped products dominate: 3.84e-6
+    // instead of 3.78e-6, 9 % faster); TF32 accumulates the whole K in TMEM
+    p.chunk = mi.tf32 ? p.kblocks : (mi.nprod == 3 ? 4 : 1);
+    for (int i = 0; i < 6; ++i) { p.pa[i] = mi.pa[i]; p.pb[i] = mi.pb[i]; }
+    p.complex_out = cplx ? 1 : 0;
+    const float* al = (const float*)&alpha;
+    const float* be = (const float*)&beta;
+    p.alpha_re = al[0];
+    p.alpha_im = cplx ? al[1] : 0.f;
+    p.beta_re = be[0];
+    p.beta_im = cplx ? be[1] : 0.f;
+    p.C = (float*)C;
+    p.ldc = ldc;
+    p.status = h->ws.dev_status;
+    p.tri = cplx ? 0 : tri;
+    p.ab_fmt = 1;
+    p.out_half = 0;
+    void* pa[3] = {oa.plane[0], oa.plane[1], oa.plane[2]};
+    void* pb[3] = {ob.plane[0], ob.plane[1], ob.plane[2]};
+    return launch_engine(h, mi, pa, pb, m, rows_b, kpad, p);
+}
+
+// HGEMM: IEEE half operands and result, products on the tensor cores with
+// the f16 operand format, the whole K accumulated in FP32 in TMEM, one
+// rounding of alpha * acc + beta * C to half.
+cudaError_t hgemm_tc(iclblasHandle_t h, int ta, int tb, int m, int n, int k, float alpha, const __half* A, int lda,
+                     const __half* B, int ldb, float beta, __half* C, int ldc)
+{
+    const int kblk = ROW_BYTES / 2;
+    const long kpad = std::max<long>(kblk, ((long)k + kblk - 1) / kblk * kblk);
+    const size_t align = 1024;
+    const size_t plane_a = ((size_t)m * kpad * 2 + align - 1) / align * align;
+    const size_t plane_b = ((size_t)n * kpad * 2 + align - 1) / align * align;
+    char* ws = (char*)scratch(h, plane_a + plane_b);
+    if (!ws) return cudaErrorMemoryAllocation;
+    __half* la = (__half*)ws;
+    __half* lb = (__half*)(ws + plane_a);
+    const bool at = ta != ICLBLAS_OP_N, bt = tb != ICLBLAS_OP_N;
+    // A: L[r=m][k] ; op N: S[m + k*lda] ; op T/C: S[k + m*lda]
+    pack_half_kernel<<<dim3((unsigned)ceil_div(kpad, 64L), (unsigned)ceil_div(m, 32)), 256, 0, h->stream>>>(
+        m, k, A, at ? lda : 1, at ? 1 : lda, la, kpad);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    // B: L[r=n][k] = op(B)[k][n] ; op N: S[k + n*ldb] ; op T/C: S[n + k*ldb]
+    pack_half_kernel<<<dim3((unsigned)ceil_div(kpad, 64L), (unsigned)ceil_div(n, 32)), 256, 0, h->stream>>>(
+        n, k, B, bt ? 1 : ldb, bt ? ldb : 1, lb, kpad);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    ModeInfo mi{};
+    mi.tf32 = false;
+    mi.nlev = 1;
+    mi.nprod = 1;
+    Params p{};
+    p.M = m;
+    p.N = n;
+    p.kblocks = (int)(kpad / kblk);
+    p.nprod = 1;
+    p.chunk = p.kblocks;
+    p.complex_out = 0;
+    p.alpha_re = alpha;
+    p.beta_re = beta;
+    p.C = (float*)C;
+    p.ldc = ldc;
+    p.status = h->ws.dev_status;
+    p.tri = 0;
+    p.ab_fmt = 0;
+    p.out_half = 1;
+    void* pa[3] = {la, la, la};
+    void* pb[3] = {lb, lb, lb};
+    return launch_engine(h, mi, pa, pb, m, n, kpad, p);
 }
 
 template cudaError_t gemm_tc<float>(iclblasHandle_t, int, int, int, int, int, float, const float*, int, const float*,

@@ -142,6 +142,10 @@ cudaError_t chemv(iclblasHandle_t h, int uplo, int n, cfloat alpha, const cfloat
 // ---------------------------------------------------------------- level 3
 cudaError_t sgemm(iclblasHandle_t h, int transa, int transb, int m, int n, int k, float alpha, const float* A,
                   int lda, const float* B, int ldb, float beta, float* C, int ldc);
+// GEMM on IEEE half storage (A, B and C hold 16-bit halves): tensor-core
+// products, FP32 accumulation, alpha * acc + beta * C rounded once to half.
+cudaError_t hgemm(iclblasHandle_t h, int transa, int transb, int m, int n, int k, float alpha, const void* A, int lda,
+                  const void* B, int ldb, float beta, void* C, int ldc);
 // S GEMM forming only one triangle of C: tri 1 writes (and reads, for beta)
 // only row >= col, tri 2 only row <= col; tiles outside the triangle are not
 // computed.  tri 0 is the plain GEMM.

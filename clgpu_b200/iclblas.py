@@ -109,6 +109,7 @@ _SIGS = {
     "iclblasSsyr2k": [_H, _I, _I, _I, _I, _P, _P, _I, _P, _I, _P, _P, _I],
     "iclblasSsymm": [_H, _I, _I, _I, _I, _P, _P, _I, _P, _I, _P, _P, _I],
     "iclblasStrmm": [_H, _I, _I, _I, _I, _I, _I, _P, _P, _I, _P, _I, _P, _I],
+    "iclblasHgemm": [_H, _I, _I, _I, _I, _I, _P, _P, _I, _P, _I, _P, _P, _I],
     "iclblasStrsv": [_H, _I, _I, _I, _I, _P, _I, _P, _I],
     "iclblasCtrsv": [_H, _I, _I, _I, _I, _P, _I, _P, _I],
     "iclblasSgemv": [_H, _I, _I, _I, _P, _P, _I, _P, _I, _P, _P, _I],
@@ -392,6 +393,12 @@ def iclblasSsymm(h, side, uplo, m, n, alpha, A, lda, B, ldb, beta, Cm, ldc):
 def iclblasStrmm(h, side, uplo, transa, diag, m, n, alpha, A, lda, B, ldb, Cm, ldc):
     return _call("iclblasStrmm", _h(h), side, uplo, transa, diag, m, n, C.byref(_fscalar(alpha)), ptr(A), lda,
                  ptr(B), ldb, ptr(Cm), ldc)
+
+
+def iclblasHgemm(h, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc):
+    """A, B, Cm: float16 arrays (numpy float16 / torch.half); alpha, beta: floats."""
+    return _call("iclblasHgemm", _h(h), transa, transb, m, n, k, C.byref(_fscalar(alpha)), ptr(A), lda, ptr(B), ldb,
+                 C.byref(_fscalar(beta)), ptr(Cm), ldc)
 
 
 def iclblasStrsv(h, uplo, trans, diag, n, A, lda, x, incx):

@@ -268,6 +268,18 @@ ICLBLAS_API iclblasStatus_t iclblasStrmm(iclblasHandle_t handle, iclblasSideMode
 /* Extensions (new symbols; no reference counterpart).                      */
 /* ======================================================================== */
 
+/* Half-precision GEMM: C = alpha op(A) op(B) + beta C with A, B and C in IEEE
+ * 754 binary16 (each element an unsigned short holding the bit pattern),
+ * column-major as the other routines.  Products run on the tensor cores,
+ * the K sum accumulates in FP32 and alpha * acc + beta * C is rounded to
+ * half once (round to nearest even).  alpha and beta are FP32 host scalars;
+ * beta == 0 writes C without reading it.  The reference ships FP16 GEMM only
+ * as stand-alone experimental OpenCL kernels (experimental/kernels/
+ * hgemm_buf_*.cl, for ResNet-50 1x1 convolutions), not through its API. */
+ICLBLAS_API iclblasStatus_t iclblasHgemm(iclblasHandle_t handle, iclblasOperation_t transa, iclblasOperation_t transb,
+                                         int m, int n, int k, const float* alpha, const unsigned short* A, int lda,
+                                         const unsigned short* B, int ldb, const float* beta, unsigned short* C, int ldc);
+
 /* Arithmetic used by S/C GEMM and by the trailing updates of S/C TRSM.
  *   PLAIN_FP32: FP32 FFMA on the CUDA cores (the drop-in default);
  *   TF32:       one TF32 product on the tensor cores, FP32 accumulate;

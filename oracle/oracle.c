@@ -994,3 +994,59 @@ void orc_strmm(int side, int uplo, int transa, int diag, int m, int n, float alp
         for (int i = 0; i < m; ++i) C[(long)j * ldc + i] = (float)out[(size_t)j * m + i];
     free(out);
 }
+
+/* ------------------------------------------------------------------------ */
+/* Half-precision GEMM (the library's HGEMM extension)                      */
+/* ------------------------------------------------------------------------ */
+
+/* IEEE 754 binary16 bit pattern -> value */
+static double half_value(uint16_t h)
+{
+    const int s = h >> 15, e = (h >> 10) & 31, f = h & 1023;
+    double v;
+    if (e == 0) v = ldexp((double)f, -24);
+    else if (e == 31) v = f ? NAN : INFINITY;
+    else v = ldexp((double)(f + 1024), e - 25);
+    return s ? -v : v;
+}
+
+/* value -> binary16, round to nearest even (one rounding from double) */
+static uint16_t half_bits(double x)
+{
+    if (isnan(x)) return 0x7e00;
+    const uint16_t sign = signbit(x) ? 0x8000 : 0;
+    double a = fabs(x);
+    if (a == 0.0) return sign;
+    int e2;
+    frexp(a, &e2);              /* a = m 2^e2, m in [0.5, 1) */
+    int E = e2 - 1;             /* 2^E <= a < 2^(E+1) */
+    if (E < -14) E = -14;       /* subnormal quantum 2^-24 */
+    const double q = ldexp(1.0, E - 10);
+    a = nearbyint(a / q) * q;   /* default rounding mode: nearest even */
+    if (a == 0.0) return sign;
+    if (a > 65504.0) return (uint16_t)(sign | 0x7c00);
+    frexp(a, &e2);
+    E = e2 - 1;
+    if (E < -14) return (uint16_t)(sign | (uint16_t)(a / ldexp(1.0, -24)));  /* subnormal */
+    const int f = (int)(a / ldexp(1.0, E - 10)) - 1024;
+    return (uint16_t)(sign | (uint16_t)((E + 15) << 10) | (uint16_t)f);
+}
+
+/* C = alpha op(A) op(B) + beta C on binary16 storage: products and sums in
+ * double, one rounding to half; beta == 0 means C is not read. */
+void orc_hgemm(int transa, int transb, int m, int n, int k, float alpha, const uint16_t* A, int lda,
+               const uint16_t* B, int ldb, float beta, uint16_t* C, int ldc)
+{
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < m; ++i) {
+            double acc = 0.0;
+            for (int l = 0; l < k; ++l) {
+                const double a = half_value(transa ? A[(long)i * lda + l] : A[(long)l * lda + i]);
+                const double b = half_value(transb ? B[(long)l * ldb + j] : B[(long)j * ldb + l]);
+                acc += a * b;
+            }
+            double out = (double)alpha * acc;
+            if (beta != 0.0f) out += (double)beta * half_value(C[(long)j * ldc + i]);
+            C[(long)j * ldc + i] = half_bits(out);
+        }
+}

@@ -21,6 +21,8 @@
 #ifndef ICLB_ORACLE_H
 #define ICLB_ORACLE_H
 
+#include <stdint.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -71,6 +73,10 @@ void orc_ssymm(int side, int uplo, int m, int n, float alpha, const float* A, in
                float beta, float* C, int ldc);
 void orc_strmm(int side, int uplo, int transa, int diag, int m, int n, float alpha, const float* A, int lda,
                const float* B, int ldb, float* C, int ldc);
+
+/* ---- half-precision GEMM (library extension; binary16 bit patterns) ---- */
+void orc_hgemm(int transa, int transb, int m, int n, int k, float alpha, const uint16_t* A, int lda,
+               const uint16_t* B, int ldb, float beta, uint16_t* C, int ldc);
 
 /* ---- level 2 ---- */
 void orc_sgemv(int trans, int m, int n, float alpha, const float* A, int lda,

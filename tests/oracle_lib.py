@@ -82,6 +82,7 @@ def orc() -> C.CDLL:
             "orc_ssyr2k": ([i, i, i, i, f, p, i, p, i, f, p, i], None),
             "orc_ssymm": ([i, i, i, i, f, p, i, p, i, f, p, i], None),
             "orc_strmm": ([i, i, i, i, i, i, f, p, i, p, i, p, i], None),
+            "orc_hgemm": ([i, i, i, i, i, f, p, i, p, i, f, p, i], None),
         }
         for name, (a, r) in sig.items():
             fn = getattr(L, name)
@@ -334,6 +335,11 @@ def ssymm(side, uplo, m, n, alpha, A, lda, B, ldb, beta, Cm, ldc):
 
 def strmm(side, uplo, transa, diag, m, n, alpha, A, lda, B, ldb, Cm, ldc):
     orc().orc_strmm(side, uplo, transa, diag, m, n, alpha, _p(A), lda, _p(B), ldb, _p(Cm), ldc)
+
+
+def hgemm(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc):
+    """A, B, Cm: float16 arrays (bit patterns passed through)."""
+    orc().orc_hgemm(ta, tb, m, n, k, alpha, _p(A), lda, _p(B), ldb, beta, _p(Cm), ldc)
 
 
 # ------------------------------------------------------------ data helpers
