@@ -19,6 +19,8 @@
 // kDevWaitTimeout in the device status word and every other CTA, which also
 // polls that word, returns; the host reports EXECUTION_FAILED.  Reads of
 // other CTAs' results go through L2 (ld.cg) so no stale L1 line is used.
+#include <type_traits>
+
 #include "common.cuh"
 #include "tma.cuh"
 
@@ -242,9 +244,8 @@ __global__ void __launch_bounds__(kThreads) trsv_kernel(int n, int lower_op, int
 //     later CTAs of its cluster (st.async on a transaction barrier), and the
 //     chain step runs on the 64 row threads alone, with no block-wide
 //     barrier between the arrival of x_prev and the hand-off of x.  At
-//     n = 16384 this took the call from 314 to 265 us; what remains is the
-//     walk of the last CTAs over their long rows (up to 256 tiles each,
-//     64 KiB in flight per CTA) rather than the chain.
+//     n = 16384 this took the call from 314 to 265 us, and the blocked FP64
+//     inverse below (13 instead of 44 us at the start) to 230 us.
 constexpr int FS = 4;
 constexpr int TILE_ELEMS = NB * NB;
 constexpr int kMaxCluster = 8;
@@ -255,6 +256,7 @@ struct FastSmem {
     // FP64 inverse while it is formed; then the same bytes hold the FP32
     // inverse and W (two [NB][NB + 1] float arrays)
     double R[NB][NB + 1];
+    double Tm[NB / 2][NB / 2 + 1];  // inverse doubling temporary (and 1 / diagonal before it)
     float xs[NB];
     float ys[NB];
     float zs[NB];
@@ -467,50 +469,99 @@ __global__ void __launch_bounds__(kThreads, 2)
     // element (r, c) of the op(A) tile in a stage
     auto tile = [&](const float* T, int r, int c) { return op == 0 ? T[c * NB + r] : T[r * NB + c]; };
 
-    // ---- diagonal block: FP64 inverse (one column per thread, t < 64), then FP32
+    // ---- diagonal block: FP64 inverse, then FP32
     int bad = tma::mbar_wait_bounded(&S.full[0], 0, kTrsvWaitNs) ? 0 : 1;
     if (__syncthreads_or(bad)) {
         bail(0);
         return;
     }
-    if (t < NB) {
+    {
+        // Blocked FP64 inverse on all threads: the four 16 x 16 diagonal
+        // blocks by substitution (one column per thread), then two doubling
+        // steps that form the off-diagonal blocks from products of the known
+        // inverses (16 -> 32 -> 64).  Rows and columns past nr are an identity
+        // (the box holds zeros there) and are cut off when the inverse is
+        // stored in FP32.  (One column per thread over all 64 rows took 44 us
+        // of every call's start.)
         const float* D = S.stage[0];
-        const int j = t;
-        for (int i = 0; i < NB; ++i) S.R[i][j] = 0.0;
         auto d = [&](int r, int c) -> double { return (double)tile(D, r, c); };
-        if (j < nr) {
+        double* rd = &S.Tm[0][0];  // 1 / diagonal, then the doubling temporary
+        for (int idx = t; idx < TILE_ELEMS; idx += kThreads) S.R[idx % NB][idx / NB] = 0.0;
+        if (t < NB) rd[t] = (unit || t >= nr) ? 1.0 : 1.0 / d(t, t);
+        __syncthreads();
+        if (t < NB) {
+            // thread t owns column j of diagonal block b; the column stays in
+            // registers (loops unrolled: the D reads pipeline)
+            const int b = (t / 16) * 16, j = t % 16;
+            double y[16];
             if (lower_op) {
-                for (int i = 0; i < nr; ++i) {
-                    // every thread walks the same (i, k): D reads are broadcasts
-                    double s0 = 0.0, s1 = 0.0;
-                    int k = 0;
-                    for (; k + 1 < i; k += 2) {
-                        s0 = fma(d(i, k), S.R[k][j], s0);
-                        s1 = fma(d(i, k + 1), S.R[k + 1][j], s1);
-                    }
-                    if (k < i) s0 = fma(d(i, k), S.R[k][j], s0);
-                    const double dii = unit ? 1.0 : d(i, i);
-                    double v = 0.0;
-                    if (i == j) v = 1.0 / dii;
-                    else if (i > j) v = -(s0 + s1) / dii;
-                    S.R[i][j] = v;
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    double acc = (i == j) ? 1.0 : 0.0;
+#pragma unroll
+                    for (int k = 0; k < i; ++k) acc = fma(-d(b + i, b + k), y[k], acc);
+                    y[i] = (i >= j) ? acc * rd[b + i] : 0.0;
                 }
             } else {
-                for (int i = nr - 1; i >= 0; --i) {
-                    double s0 = 0.0, s1 = 0.0;
-                    int k = i + 1;
-                    for (; k + 1 < nr; k += 2) {
-                        s0 = fma(d(i, k), S.R[k][j], s0);
-                        s1 = fma(d(i, k + 1), S.R[k + 1][j], s1);
-                    }
-                    if (k < nr) s0 = fma(d(i, k), S.R[k][j], s0);
-                    const double dii = unit ? 1.0 : d(i, i);
-                    double v = 0.0;
-                    if (i == j) v = 1.0 / dii;
-                    else if (i < j) v = -(s0 + s1) / dii;
-                    S.R[i][j] = v;
+#pragma unroll
+                for (int i = 15; i >= 0; --i) {
+                    double acc = (i == j) ? 1.0 : 0.0;
+#pragma unroll
+                    for (int k = i + 1; k < 16; ++k) acc = fma(-d(b + i, b + k), y[k], acc);
+                    y[i] = (i <= j) ? acc * rd[b + i] : 0.0;
                 }
             }
+#pragma unroll
+            for (int i = 0; i < 16; ++i) S.R[b + i][b + j] = y[i];
+        }
+        __syncthreads();
+        // doubling (h = 16, then 32), loops unrolled at compile-time h with two
+        // partial sums per output
+        auto doubling = [&](auto hc) {
+            constexpr int h = decltype(hc)::value;
+            constexpr int nout = (NB / (2 * h)) * h * h;
+            // T = C Y11 (lower: C the block below Y11) or C Y22 (upper: C right of Y11)
+            for (int idx = t; idx < nout; idx += kThreads) {
+                const int pr = idx / (h * h), e = idx % (h * h), r = e % h, c = e / h, o = pr * 2 * h;
+                double a0 = 0.0, a1 = 0.0;
+#pragma unroll
+                for (int k = 0; k < h; k += 2) {
+                    if (lower_op) {
+                        a0 = fma(d(o + h + r, o + k), S.R[o + k][o + c], a0);
+                        a1 = fma(d(o + h + r, o + k + 1), S.R[o + k + 1][o + c], a1);
+                    } else {
+                        a0 = fma(d(o + r, o + h + k), S.R[o + h + k][o + h + c], a0);
+                        a1 = fma(d(o + r, o + h + k + 1), S.R[o + h + k + 1][o + h + c], a1);
+                    }
+                }
+                S.Tm[pr * h + r][c] = a0 + a1;
+            }
+            __syncthreads();
+            // the off-diagonal block of the inverse: -Y22 T (lower) or -Y11 T (upper)
+            for (int idx = t; idx < nout; idx += kThreads) {
+                const int pr = idx / (h * h), e = idx % (h * h), r = e % h, c = e / h, o = pr * 2 * h;
+                double a0 = 0.0, a1 = 0.0;
+#pragma unroll
+                for (int k = 0; k < h; k += 2) {
+                    if (lower_op) {
+                        a0 = fma(S.R[o + h + r][o + h + k], S.Tm[pr * h + k][c], a0);
+                        a1 = fma(S.R[o + h + r][o + h + k + 1], S.Tm[pr * h + k + 1][c], a1);
+                    } else {
+                        a0 = fma(S.R[o + r][o + k], S.Tm[pr * h + k][c], a0);
+                        a1 = fma(S.R[o + r][o + k + 1], S.Tm[pr * h + k + 1][c], a1);
+                    }
+                }
+                if (lower_op) S.R[o + h + r][o + c] = -(a0 + a1);
+                else S.R[o + r][o + h + c] = -(a0 + a1);
+            }
+            __syncthreads();
+        };
+        doubling(std::integral_constant<int, 16>{});
+        doubling(std::integral_constant<int, 32>{});
+        // rows and columns past nr: zero
+        for (int idx = t; idx < TILE_ELEMS; idx += kThreads) {
+            const int r = idx % NB, c = idx / NB;
+            if (r >= nr || c >= nr) S.R[r][c] = 0.0;
         }
     }
     __syncthreads();
