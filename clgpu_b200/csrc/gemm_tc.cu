@@ -22,9 +22,7 @@
 //                 and one thread issues tcgen05.mma (M=128, N=256, K=32 bytes
 //                 per instruction, 4 per stage) and tcgen05.commit;
 //      warps 2-9  epilogue: two warps per 32-lane TMEM quarter, 128 columns
-//                 each.  They drain the accumulator into FP32 registers
-//                 once per chunk of K blocks and store alpha*sum + beta*C
-//                 (coalesced column-major) at the end of the tile.
+//                 each (two halves of four warps).
 //    Each pipeline stage is one (K block, product) pair.  The BF16 modes run
 //    the products of every K block small-first -- 3xBF16: mid*hi, hi*mid,
 //    hi*hi; 6xBF16: lo*hi, hi*lo, mid*mid, mid*hi, hi*mid, hi*hi -- into a
@@ -34,6 +32,22 @@
 //    keeps that loss at the chunk's size, and the chunks are summed in FP32
 //    in registers (the two accumulator buffers let the next chunk's MMAs run
 //    while the previous chunk is drained).  TF32 uses one chunk per tile.
+// 3. Epilogue.  Single-chunk tiles (TF32, HGEMM) are read from TMEM 16
+//    columns at a time; each half of the epilogue warps writes alpha*acc
+//    (+ beta*C) into a 128 x 16 shared-memory box laid out like C and one
+//    thread stores it with TMA (C read by TMA for beta != 0), double
+//    buffered.  Column-at-a-time stores of a warp's 32 rows (64 or 128 B per
+//    column) ran these kernels at a fifth of the HBM write rate when the
+//    epilogue, not the MMA, bounds the tile (small K).  A TMA store clips the
+//    contiguous dimension only at 16-byte granularity, so the C map stops at
+//    M rounded down to 16 bytes and the last few rows are stored directly.
+//    The BF16 modes, whose MMA work per tile is 3-6x longer, keep their
+//    running sum in registers and store directly; triangular output and a
+//    C that TMA cannot address (16-byte alignment) take the direct path too.
+// 4. HGEMM operands are read in place in either layout: K-major (op T of A,
+//    op N of B) through the plane descriptors, MN-major (op N of A, op T of
+//    B) as boxes of 64 rows x 64 K with an MN-major shared-memory descriptor;
+//    only an operand TMA cannot address is packed first.
 // Every mbarrier wait is bounded; on timeout the kernel records
 // kDevWaitTimeout, waits (bounded) for its own TMA copies, frees TMEM and
 // returns.  Every TMA load targets the issuing CTA's own shared memory.
@@ -55,7 +69,14 @@ constexpr int BM = 128;
 constexpr int ROW_BYTES = 128;                  // one K block per tile row
 constexpr int A_TILE = BM * ROW_BYTES;          // 16 KiB
 constexpr int RING_BYTES = 192 * 1024;          // the stage ring
-constexpr int SMEM_BYTES = RING_BYTES + 1024 /*barriers*/ + 1024 /*alignment*/;
+constexpr int EPI_GROUP = 16;                  // output columns per staged store
+constexpr int EPI_BUF_BYTES = 8192;             // one staging buffer: 128 rows x 16 FP32 columns
+constexpr int EPI_STAGE_BYTES = 4 * EPI_BUF_BYTES;  // two buffers for each half of the epilogue warps
+constexpr int MN_CHUNK_BYTES = 8192;            // MN-major operand: 64 rows x 64 K of 16-bit values
+constexpr int SMEM_BYTES = RING_BYTES + 1024 /*barriers*/ + EPI_STAGE_BYTES + 1024 /*alignment*/;
+static_assert(SMEM_BYTES <= 232448, "shared memory per CTA");
+// the BF16 modes store directly and leave the staging area to the L1 cache
+constexpr int SMEM_BYTES_DIRECT = SMEM_BYTES - EPI_STAGE_BYTES;
 // Output tile 128 x BN: 256 columns, or 128 when the 256-wide tiles would
 // leave a quarter or more of the SMs idle (more, smaller tiles).
 template <int BN_>
@@ -86,6 +107,9 @@ struct Params {
     int tri;           // 0: full C; 1: only row >= col is written; 2: only row <= col (real C)
     int ab_fmt;        // kind::f16 operand format: 1 bf16 (split planes), 0 f16 (HGEMM)
     int out_half;      // real C stored as IEEE half (HGEMM)
+    int a_mn, b_mn;    // operand stored MN-major (its rows contiguous; 16-bit operands only)
+    int c_tma;         // C written (and, for beta != 0, read) through the C tensor map
+    int m_tma;         // rows the C tensor map covers (M rounded down to 16 bytes)
 };
 
 // ---------------------------------------------------------------- PTX helpers
@@ -211,6 +235,21 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v)
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// 32 lanes x 16 consecutive columns of FP32 from TMEM.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v)
+{
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
 // Shared-memory matrix descriptor, K-major, 128-byte swizzle: rows of 128 B,
 // 8-row groups 1024 B apart (SBO), version 1, layout type 2.
 __device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t saddr)
@@ -224,12 +263,28 @@ __device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t saddr)
     return d;
 }
 
-// Instruction descriptor: FP32 accumulator, A/B format (1 = BF16, 2 = TF32),
-// both K-major, N = 256, M = 128.
-__host__ __device__ constexpr uint32_t instr_desc(uint32_t ab_format, int bn)
+// Shared-memory matrix descriptor, MN-major, 128-byte swizzle: rows of 128 B
+// hold 64 consecutive M (or N) indices of one K index; 8-K groups 1024 B
+// apart (SBO); the next 64 M indices 8 KiB further (LBO: one TMA box of
+// 64 x 64).  One MMA (K = 16) spans two 8-K groups, so the start address
+// advances by 2048 B per MMA.
+__device__ __forceinline__ uint64_t smem_desc_mn_sw128(uint32_t saddr)
 {
-    return (1u << 4) | (ab_format << 7) | (ab_format << 10) | ((uint32_t)(bn >> 3) << 17) |
-           ((uint32_t)(BM >> 4) << 24);
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)(MN_CHUNK_BYTES >> 4) << 16;  // leading byte offset: next 64 rows
+    d |= (uint64_t)(1024u >> 4) << 32;           // stride byte offset: next 8 K indices
+    d |= (uint64_t)1u << 46;
+    d |= (uint64_t)2u << 61;
+    return d;
+}
+
+// Instruction descriptor: FP32 accumulator, A/B format (0 = F16, 1 = BF16,
+// 2 = TF32), A / B K-major or MN-major (bits 15, 16), N = bn, M = 128.
+__host__ __device__ constexpr uint32_t instr_desc(uint32_t ab_format, int bn, int a_mn = 0, int b_mn = 0)
+{
+    return (1u << 4) | (ab_format << 7) | (ab_format << 10) | ((uint32_t)a_mn << 15) | ((uint32_t)b_mn << 16) |
+           ((uint32_t)(bn >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
 }
 
 __device__ __forceinline__ void tile_coords(int t, int tiles_m, int tiles_n, int& tm, int& tn)
@@ -295,11 +350,290 @@ __device__ __forceinline__ bool in_tri(int tri, int row, int col)
     return tri == 0 || (tri == 1 ? row >= col : row <= col);
 }
 
-template <bool TF32, int BN_>
+// One operand tile (rows x one K block) into shared memory: a single box for
+// K-major storage, boxes of 64 rows x 64 K at 8 KiB steps for MN-major.
+__device__ __forceinline__ void load_operand(uint8_t* dst, const CUtensorMap* map, int mn, int rows, int kx, int r0,
+                                             uint64_t* bar)
+{
+    if (mn) {
+        for (int i = 0; i < rows / 64; ++i) tma_load_2d(dst + i * MN_CHUNK_BYTES, map, r0 + i * 64, kx, bar);
+    } else {
+        tma_load_2d(dst, map, kx, r0, bar);
+    }
+}
+
+// ---------------------------------------------------------------- epilogue stores
+// The four epilogue warps that share one half of the tile's columns
+// synchronise on a named barrier of their own (ids 1 and 2; 0 is
+// __syncthreads).
+__device__ __forceinline__ void group_sync(int id) { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
+// true when v holds in every thread of the group
+__device__ __forceinline__ bool group_all(int id, bool v)
+{
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.b32 p, %1, 0;\n\t"
+        "bar.red.and.pred q, %2, 128, p;\n\t"
+        "selp.b32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)v), "r"(id)
+        : "memory");
+    return r != 0;
+}
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, const void* smem_src, int x, int y)
+{
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];"
+                 ::"l"((uint64_t)map), "r"(x), "r"(y), "r"(smem_u32(smem_src))
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read1() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// State of one half's staged stores.
+struct EpiGroup {
+    uint8_t* buf;   // two staging buffers of EPI_BUF_BYTES
+    uint64_t* bar;  // their load barriers (beta != 0)
+    int id;         // named barrier of the half
+    bool leader;    // the thread that issues the copies
+    int gi;         // groups staged so far: buffer gi & 1, barrier parity (gi >> 1) & 1
+};
+
+// Output element type of a kernel instantiation: FP32, IEEE half (HGEMM),
+// or complex FP32 with the real GEMM's columns 2j, 2j+1 holding (re, im) of
+// column j.
+enum : int { OUT_F32 = 0, OUT_F16 = 1, OUT_C64 = 2 };
+
+// alpha * v + beta * c with the rounding of the reference's real GEMM
+// epilogue (beta == 0: C is not read)
+__device__ __forceinline__ float axpby(const Params& p, bool beta_zero, float v, float c)
+{
+    return beta_zero ? __fmul_rn(p.alpha_re, v) : fmaf(p.alpha_re, v, __fmul_rn(p.beta_re, c));
+}
+__device__ __forceinline__ float2 caxpby(const Params& p, bool beta_zero, float re, float im, float2 c)
+{
+    float2 o;
+    o.x = fmaf(p.alpha_re, re, -p.alpha_im * im);
+    o.y = fmaf(p.alpha_re, im, p.alpha_im * re);
+    if (!beta_zero) {
+        o.x += fmaf(p.beta_re, c.x, -p.beta_im * c.y);
+        o.y += fmaf(p.beta_re, c.y, p.beta_im * c.x);
+    }
+    return o;
+}
+
+// Direct epilogue, one group of 16 columns of one row (C not reachable by
+// TMA, triangular output, or the rows a TMA store cannot clip exactly); C
+// is read before any of the group is stored, so the loads overlap (columns
+// of C never alias for ldc >= M).
+template <int OUT, int W>
+__device__ __forceinline__ void direct_group(const float (&v)[W], const Params& p, int row, int cx)
+{
+    if (row >= p.M) return;
+    const bool beta_zero = p.beta_re == 0.f && p.beta_im == 0.f;
+    if constexpr (OUT == OUT_C64) {
+        float2* const C2 = (float2*)p.C;
+        float2 cv[W / 2];
+#pragma unroll
+        for (int j = 0; j < W / 2; ++j) {
+            const int col = cx + 2 * j;
+            cv[j] = (!beta_zero && col < p.N) ? C2[(long)(col >> 1) * p.ldc + row] : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int j = 0; j < W / 2; ++j) {
+            const int col = cx + 2 * j;
+            if (col < p.N) C2[(long)(col >> 1) * p.ldc + row] = caxpby(p, beta_zero, v[2 * j], v[2 * j + 1], cv[j]);
+        }
+    } else {
+        using T = typename std::conditional<OUT == OUT_F16, __half, float>::type;
+        T* const Ct = (T*)p.C;
+        float cv[W];
+#pragma unroll
+        for (int j = 0; j < W; ++j) {
+            const int col = cx + j;
+            cv[j] = (!beta_zero && col < p.N && in_tri(p.tri, row, col)) ? (float)Ct[(long)col * p.ldc + row] : 0.f;
+        }
+#pragma unroll
+        for (int j = 0; j < W; ++j) {
+            const int col = cx + j;
+            if (col < p.N && in_tri(p.tri, row, col)) Ct[(long)col * p.ldc + row] = (T)axpby(p, beta_zero, v[j], cv[j]);
+        }
+    }
+}
+
+// Staged epilogue, one group of 16 columns of one half of a CTA's tile
+// (128 rows): the half's four warps write alpha*v (+ beta*C) into a buffer
+// laid out as C's own column-major box, and one thread stores the box with
+// TMA, which clips columns past C's edge.  Along the rows a TMA store clips
+// only at 16-byte granularity, so the map covers the first m_tma rows (M
+// rounded down to 16 bytes) and the rows in [m_tma, M) are stored directly
+// by their threads.  For beta != 0 the same box of C is first loaded into
+// the buffer by TMA.  A buffer is refilled once the store that last read it
+// has finished reading.  The arithmetic is that of the direct stores.
+// Returns false (in every thread of the half) when a wait gave up; the
+// leader's load into the current buffer may then still be in flight.
+template <int OUT>
+__device__ __forceinline__ bool stage_group(const float (&v)[EPI_GROUP], const Params& p, const CUtensorMap* mC,
+                                            EpiGroup& eg, int r, int row0, int cx, volatile int* abort_flag)
+{
+    constexpr uint32_t box_bytes = OUT == OUT_F16 ? EPI_BUF_BYTES / 2 : EPI_BUF_BYTES;
+    const bool beta_zero = p.beta_re == 0.f && p.beta_im == 0.f;
+    const int b = eg.gi & 1;
+    const uint32_t ph = (uint32_t)(eg.gi >> 1) & 1u;
+    uint8_t* buf = eg.buf + b * EPI_BUF_BYTES;
+    const int x = OUT == OUT_C64 ? 2 * row0 : row0, y = OUT == OUT_C64 ? cx / 2 : cx;
+    if (eg.leader) {
+        bulk_wait_read1();
+        if (!beta_zero) {
+            mbar_expect_tx(&eg.bar[b], box_bytes);
+            tma_load_2d(buf, mC, x, y, &eg.bar[b]);
+        }
+    }
+    group_sync(eg.id);
+    const bool lok = beta_zero || mbar_wait(&eg.bar[b], ph, abort_flag);
+    if (lok) {
+        if (row0 + r < p.m_tma) {
+            if constexpr (OUT == OUT_C64) {
+                float2* const sb = (float2*)buf + r;
+#pragma unroll
+                for (int j = 0; j < EPI_GROUP / 2; ++j)
+                    sb[j * 128] = caxpby(p, beta_zero, v[2 * j], v[2 * j + 1], beta_zero ? make_float2(0.f, 0.f) : sb[j * 128]);
+            } else {
+                using T = typename std::conditional<OUT == OUT_F16, __half, float>::type;
+                T* const sb = (T*)buf + r;
+#pragma unroll
+                for (int j = 0; j < EPI_GROUP; ++j)
+                    sb[j * 128] = (T)axpby(p, beta_zero, v[j], beta_zero ? 0.f : (float)sb[j * 128]);
+            }
+        } else {
+            direct_group<OUT, EPI_GROUP>(v, p, row0 + r, cx);  // rows past the map (none past M)
+        }
+    }
+    fence_async_smem();
+    if (!group_all(eg.id, lok)) return false;
+    if (eg.leader) {
+        tma_store_2d(mC, buf, x, y);
+        bulk_commit();
+    }
+    ++eg.gi;
+    return true;
+}
+
+// The epilogue warps' loops over a CTA's tiles (tiles of tile_rows x BN;
+// this CTA's rows start row_off into each).  Warp w serves TMEM lane quarter
+// w % 4 and one half (EPI_COLS columns) of the tile.
+//
+// Single chunk (the whole K in one accumulator: TF32, HGEMM): 16 columns at a
+// time straight from TMEM into the staged (or direct) stores; the
+// accumulator is released after the last group.
+template <int OUT, int BN, int EPI_COLS, class Arrive>
+__device__ __forceinline__ void epilogue_single(const Params& p, const CUtensorMap* mC, int t0, int tstep, int ntiles,
+                                                int tiles_m, int tiles_n, int tile_rows, int row_off,
+                                                uint32_t tmem_base, uint64_t* tfull, Arrive arrive, uint8_t* epi_buf,
+                                                uint64_t* cbar, volatile int* abort_flag)
+{
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const int q = warp & 3, half = (warp - 2) / 4;
+    const int r = q * 32 + lane;  // row within the CTA's 128
+    EpiGroup eg{epi_buf + half * 2 * EPI_BUF_BYTES, cbar + half * 2, 1 + half, q == 0 && lane == 0, 0};
+    int acc = 0;
+    uint32_t acc_ph = 0;
+    for (int t = t0; t < ntiles; t += tstep) {
+        int w = 1;
+        if (lane == 0) w = mbar_wait(&tfull[acc], acc_ph, abort_flag) ? 1 : 0;
+        // the half's four warps leave together (a warp that gave up has set
+        // the abort flag, so the others' waits end too)
+        if (!group_all(eg.id, __shfl_sync(0xffffffffu, w, 0) != 0)) break;
+        tc_fence_after();
+        int tm, tn;
+        tile_at(p.tri, t, tiles_m, tiles_n, tile_rows, BN, tm, tn);
+        const int row0 = tm * tile_rows + row_off, col0 = tn * BN + half * EPI_COLS;
+        const uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN + half * EPI_COLS);
+        bool stored = true;
+#pragma unroll 1
+        for (int g = 0; g < EPI_COLS / EPI_GROUP && stored; ++g) {
+            float v[EPI_GROUP];
+            tmem_ld16(taddr + (uint32_t)(g * EPI_GROUP), v);
+            if (p.c_tma)
+                stored = stage_group<OUT>(v, p, mC, eg, r, row0, col0 + g * EPI_GROUP, abort_flag);
+            else
+                direct_group<OUT, EPI_GROUP>(v, p, row0 + r, col0 + g * EPI_GROUP);
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) arrive(acc);
+        if (++acc == 2) { acc = 0; acc_ph ^= 1; }
+        if (!stored) {
+            if (eg.leader) mbar_drain(&eg.bar[eg.gi & 1], (uint32_t)(eg.gi >> 1) & 1u);
+            break;
+        }
+    }
+    if (eg.leader) bulk_wait_all();
+}
+
+// Several chunks (the BF16 modes): each chunk is drained into FP32 registers
+// and released at once; the sum is stored directly (these stores overlap the
+// longer MMA work of the next tile).  Nothing but the running sum stays live
+// across the chunk loop.
+template <int OUT, int BN, int EPI_COLS, class Arrive>
+__device__ __forceinline__ void epilogue_multi(const Params& p, int t0, int tstep, int ntiles, int tiles_m,
+                                               int tiles_n, int tile_rows, int row_off, uint32_t tmem_base,
+                                               uint64_t* tfull, Arrive arrive, volatile int* abort_flag)
+{
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const int q = warp & 3, half = (warp - 2) / 4;
+    const int nchunks = (p.kblocks + p.chunk - 1) / p.chunk;
+    int acc = 0;
+    uint32_t acc_ph = 0;
+    bool ok = true;
+    for (int t = t0; t < ntiles && ok; t += tstep) {
+        float sum[EPI_COLS];
+#pragma unroll
+        for (int j = 0; j < EPI_COLS; ++j) sum[j] = 0.f;
+        for (int c = 0; c < nchunks; ++c) {
+            int w = 1;
+            if (lane == 0) w = mbar_wait(&tfull[acc], acc_ph, abort_flag) ? 1 : 0;
+            ok = __shfl_sync(0xffffffffu, w, 0) != 0;
+            if (!ok) break;
+            tc_fence_after();
+            const uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN + half * EPI_COLS);
+#pragma unroll
+            for (int g = 0; g < EPI_COLS / 32; ++g) {
+                float v[32];
+                tmem_ld32(taddr + (uint32_t)(g * 32), v);
+#pragma unroll
+                for (int j = 0; j < 32; ++j) sum[g * 32 + j] += v[j];
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) arrive(acc);
+            if (++acc == 2) { acc = 0; acc_ph ^= 1; }
+        }
+        if (!ok) break;
+        int tm, tn;
+        tile_at(p.tri, t, tiles_m, tiles_n, tile_rows, BN, tm, tn);
+        const int row = tm * tile_rows + row_off + q * 32 + lane;
+        const int col0 = tn * BN + half * EPI_COLS;
+        if (row < p.M) {
+#pragma unroll
+            for (int g = 0; g < EPI_COLS / 8; ++g) {
+                float v[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) v[j] = sum[g * 8 + j];
+                direct_group<OUT, 8>(v, p, row, col0 + g * 8);
+            }
+        }
+    }
+}
+
+template <bool TF32, int BN_, int OUT>
 __global__ void __launch_bounds__(THREADS, 1)
     gemm_tc_kernel(const __grid_constant__ CUtensorMap mA0, const __grid_constant__ CUtensorMap mA1,
                    const __grid_constant__ CUtensorMap mA2, const __grid_constant__ CUtensorMap mB0,
-                   const __grid_constant__ CUtensorMap mB1, const __grid_constant__ CUtensorMap mB2, Params p)
+                   const __grid_constant__ CUtensorMap mB1, const __grid_constant__ CUtensorMap mB2,
+                   const __grid_constant__ CUtensorMap mC, Params p)
 {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -312,11 +646,14 @@ __global__ void __launch_bounds__(THREADS, 1)
     uint64_t* tempty = tfull + 2;
     uint32_t* tmem_slot = (uint32_t*)(tempty + 2);
     volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
+    uint64_t* cbar = (uint64_t*)(smem + RING_BYTES + 512);  // [half][buffer] C-load barriers
+    uint8_t* epi_buf = smem + RING_BYTES + 1024;             // [half][buffer] staging
 
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
     const int tiles_m = (p.M + BM - 1) / BM, tiles_n = (p.N + BN - 1) / BN;
     const int ntiles = tile_count(p.tri, tiles_m, tiles_n, BM, BN);
     const int steps = p.kblocks * p.nprod;
+    constexpr bool MN_OK = OUT == OUT_F16;  // MN-major operands: HGEMM only
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) {
@@ -327,6 +664,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             mbar_init(&tfull[a], 1);
             mbar_init(&tempty[a], EPI_WARPS);  // one arrive per epilogue warp
         }
+        for (int i = 0; i < 4; ++i) mbar_init(&cbar[i], 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -357,8 +695,8 @@ __global__ void __launch_bounds__(THREADS, 1)
                     uint8_t* sb = sa + A_TILE;
                     mbar_expect_tx(&full[s], STAGE_BYTES);
                     const int kx = kb * (TF32 ? 32 : 64);
-                    tma_load_2d(sa, ma[p.pa[pr]], kx, tm * BM, &full[s]);
-                    tma_load_2d(sb, mb[p.pb[pr]], kx, tn * BN, &full[s]);
+                    load_operand(sa, ma[p.pa[pr]], MN_OK && p.a_mn, BM, kx, tm * BM, &full[s]);
+                    load_operand(sb, mb[p.pb[pr]], MN_OK && p.b_mn, BN, kx, tn * BN, &full[s]);
                     if (++s == STAGES) { s = 0; ph ^= 1; }
                 }
             }
@@ -370,7 +708,9 @@ __global__ void __launch_bounds__(THREADS, 1)
     } else if (warp == 1) {
         // ---------------------------------------------------------- MMA issuer
         if (lane == 0) {
-            const uint32_t idesc = instr_desc(TF32 ? 2u : (uint32_t)p.ab_fmt, BN);
+            const int a_mn = MN_OK && p.a_mn, b_mn = MN_OK && p.b_mn;
+            const uint32_t idesc = instr_desc(TF32 ? 2u : (uint32_t)p.ab_fmt, BN, a_mn, b_mn);
+            const uint64_t a_step = a_mn ? 128 : 2, b_step = b_mn ? 128 : 2;  // per MMA, 16-byte units
             int s = 0;
             uint32_t ph = 0;
             int acc = 0;
@@ -388,11 +728,11 @@ __global__ void __launch_bounds__(THREADS, 1)
                         tc_fence_after();
                         const uint32_t sa = smem_u32(tiles + s * STAGE_BYTES);
                         const uint32_t sb = sa + A_TILE;
-                        const uint64_t da = smem_desc_sw128(sa), db = smem_desc_sw128(sb);
+                        const uint64_t da = a_mn ? smem_desc_mn_sw128(sa) : smem_desc_sw128(sa);
+                        const uint64_t db = b_mn ? smem_desc_mn_sw128(sb) : smem_desc_sw128(sb);
 #pragma unroll
                         for (int kk = 0; kk < 4; ++kk)  // 4 x 32 bytes of K per stage
-                            umma<TF32>(d, da + (uint64_t)(2 * kk), db + (uint64_t)(2 * kk), idesc,
-                                       (st > c0 || kk > 0) ? 1u : 0u);
+                            umma<TF32>(d, da + a_step * kk, db + b_step * kk, idesc, (st > c0 || kk > 0) ? 1u : 0u);
                         umma_commit(&empty[s]);
                         if (++s == STAGES) { s = 0; ph ^= 1; }
                     }
@@ -408,116 +748,13 @@ __global__ void __launch_bounds__(THREADS, 1)
         }
     } else {
         // ---------------------------------------------------------- epilogue
-        const int ew = warp - 2;
-        const int q = warp & 3;             // TMEM lane quarter this warp may access
-        const int half = ew / 4;            // columns [half*EPI_COLS, (half+1)*EPI_COLS) of the tile
-        const int nchunks = (p.kblocks + p.chunk - 1) / p.chunk;
-        int acc = 0;
-        uint32_t acc_ph = 0;
-        bool ok = true;
-        for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-            int tm, tn;
-            tile_at(p.tri, t, tiles_m, tiles_n, BM, BN, tm, tn);
-            float sum[EPI_COLS];
-#pragma unroll
-            for (int j = 0; j < EPI_COLS; ++j) sum[j] = 0.f;
-            for (int c = 0; c < nchunks; ++c) {
-                int w = 1;
-                if (lane == 0) w = mbar_wait(&tfull[acc], acc_ph, abort_flag) ? 1 : 0;
-                ok = __shfl_sync(0xffffffffu, w, 0) != 0;
-                if (!ok) break;
-                tc_fence_after();
-                const uint32_t taddr =
-                    tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN + half * EPI_COLS);
-#pragma unroll
-                for (int g = 0; g < EPI_COLS / 32; ++g) {
-                    float v[32];
-                    tmem_ld32(taddr + (uint32_t)(g * 32), v);
-#pragma unroll
-                    for (int j = 0; j < 32; ++j) sum[g * 32 + j] += v[j];
-                }
-                tc_fence_before();
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&tempty[acc]);
-                if (++acc == 2) { acc = 0; acc_ph ^= 1; }
-            }
-            if (!ok) break;
-            const int row = tm * BM + q * 32 + lane;
-            const int col0 = tn * BN + half * EPI_COLS;
-            const bool beta_zero = p.beta_re == 0.f && p.beta_im == 0.f;
-            // C is read in groups of 8 columns before any of them is stored,
-            // so the loads overlap (columns of C never alias for ldc >= M)
-            if (row < p.M) {
-                if (p.out_half) {
-                    __half* const Ch = (__half*)p.C;
-#pragma unroll
-                    for (int j0 = 0; j0 < EPI_COLS; j0 += 8) {
-                        float cv[8];
-#pragma unroll
-                        for (int j = 0; j < 8; ++j) {
-                            const int col = col0 + j0 + j;
-                            cv[j] = (!beta_zero && col < p.N && in_tri(p.tri, row, col))
-                                        ? __half2float(Ch[(long)col * p.ldc + row])
-                                        : 0.f;
-                        }
-#pragma unroll
-                        for (int j = 0; j < 8; ++j) {
-                            const int col = col0 + j0 + j;
-                            if (col < p.N && in_tri(p.tri, row, col))
-                                Ch[(long)col * p.ldc + row] = __float2half_rn(
-                                    beta_zero ? __fmul_rn(p.alpha_re, sum[j0 + j])
-                                              : fmaf(p.alpha_re, sum[j0 + j], __fmul_rn(p.beta_re, cv[j])));
-                        }
-                    }
-                } else if (!p.complex_out) {
-#pragma unroll
-                    for (int j0 = 0; j0 < EPI_COLS; j0 += 8) {
-                        float cv[8];
-#pragma unroll
-                        for (int j = 0; j < 8; ++j) {
-                            const int col = col0 + j0 + j;
-                            cv[j] = (!beta_zero && col < p.N && in_tri(p.tri, row, col)) ? p.C[(long)col * p.ldc + row]
-                                                                                          : 0.f;
-                        }
-#pragma unroll
-                        for (int j = 0; j < 8; ++j) {
-                            const int col = col0 + j0 + j;
-                            if (col < p.N && in_tri(p.tri, row, col))
-                                p.C[(long)col * p.ldc + row] =
-                                    beta_zero ? __fmul_rn(p.alpha_re, sum[j0 + j])
-                                              : fmaf(p.alpha_re, sum[j0 + j], __fmul_rn(p.beta_re, cv[j]));
-                        }
-                    }
-                } else {
-                    float2* const C2 = (float2*)p.C;
-#pragma unroll
-                    for (int j0 = 0; j0 < EPI_COLS; j0 += 8) {
-                        float2 cv[4];
-#pragma unroll
-                        for (int j = 0; j < 4; ++j) {
-                            const int col = col0 + j0 + 2 * j;
-                            cv[j] = (!beta_zero && col < p.N) ? C2[(long)(col >> 1) * p.ldc + row]
-                                                              : make_float2(0.f, 0.f);
-                        }
-#pragma unroll
-                        for (int j = 0; j < 4; ++j) {
-                            const int col = col0 + j0 + 2 * j;
-                            if (col < p.N) {
-                                const float re = sum[j0 + 2 * j], im = sum[j0 + 2 * j + 1];
-                                float2 r;
-                                r.x = fmaf(p.alpha_re, re, -p.alpha_im * im);
-                                r.y = fmaf(p.alpha_re, im, p.alpha_im * re);
-                                if (!beta_zero) {
-                                    r.x += fmaf(p.beta_re, cv[j].x, -p.beta_im * cv[j].y);
-                                    r.y += fmaf(p.beta_re, cv[j].y, p.beta_im * cv[j].x);
-                                }
-                                C2[(long)(col >> 1) * p.ldc + row] = r;
-                            }
-                        }
-                    }
-                }
-            }
-        }
+        auto arrive = [&](int a) { mbar_arrive(&tempty[a]); };
+        if constexpr (TF32 || OUT == OUT_F16)
+            epilogue_single<OUT, BN, EPI_COLS>(p, &mC, blockIdx.x, gridDim.x, ntiles, tiles_m, tiles_n, BM, 0,
+                                                tmem_base, tfull, arrive, epi_buf, cbar, abort_flag);
+        else
+            epilogue_multi<OUT, BN, EPI_COLS>(p, blockIdx.x, gridDim.x, ntiles, tiles_m, tiles_n, BM, 0, tmem_base,
+                                               tfull, arrive, abort_flag);
     }
 
     __syncthreads();
@@ -620,11 +857,12 @@ __device__ __forceinline__ void dealloc_pair(uint32_t taddr, uint32_t ncols)
 }
 }  // namespace two_sm
 
-template <bool TF32>
+template <bool TF32, int OUT>
 __global__ void __launch_bounds__(THREADS, 1)
     gemm_tc2_kernel(const __grid_constant__ CUtensorMap mA0, const __grid_constant__ CUtensorMap mA1,
                     const __grid_constant__ CUtensorMap mA2, const __grid_constant__ CUtensorMap mB0,
-                    const __grid_constant__ CUtensorMap mB1, const __grid_constant__ CUtensorMap mB2, Params p)
+                    const __grid_constant__ CUtensorMap mB1, const __grid_constant__ CUtensorMap mB2,
+                    const __grid_constant__ CUtensorMap mC, Params p)
 {
     using namespace two_sm;
     constexpr int EPI_COLS = BN / 2;  // columns per epilogue warp
@@ -637,6 +875,8 @@ __global__ void __launch_bounds__(THREADS, 1)
     uint64_t* tempty = tfull + 2;
     uint32_t* tmem_slot = (uint32_t*)(tempty + 2);
     volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
+    uint64_t* cbar = (uint64_t*)(smem + RING_BYTES + 512);  // [half][buffer] C-load barriers
+    uint8_t* epi_buf = smem + RING_BYTES + 1024;             // [half][buffer] staging
 
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
     const uint32_t rank = cta_rank();
@@ -645,6 +885,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     const int tiles_m = (p.M + 2 * BM - 1) / (2 * BM), tiles_n = (p.N + BN - 1) / BN;
     const int ntiles = tile_count(p.tri, tiles_m, tiles_n, 2 * BM, BN);
     const int steps = p.kblocks * p.nprod;
+    constexpr bool MN_OK = OUT == OUT_F16;  // MN-major operands: HGEMM only
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) {
@@ -655,6 +896,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             mbar_init(&tfull[a], 1);
             mbar_init(&tempty[a], 2 * EPI_WARPS);  // every epilogue warp of both CTAs
         }
+        for (int i = 0; i < 4; ++i) mbar_init(&cbar[i], 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -686,8 +928,19 @@ __global__ void __launch_bounds__(THREADS, 1)
                     if (leader) mbar_expect_tx(&full[s], 2 * STAGE_BYTES);
                     const uint32_t bar = map_rank(&full[s], 0);
                     const int kx = kb * (TF32 ? 32 : 64);
-                    tma_load_2d_pair(sa, ma[p.pa[pr]], kx, tm * 2 * BM + (int)rank * BM, bar);
-                    tma_load_2d_pair(sb, mb[p.pb[pr]], kx, tn * BN + (int)rank * 128, bar);
+                    const int ra = tm * 2 * BM + (int)rank * BM, rb = tn * BN + (int)rank * 128;
+                    if (MN_OK && p.a_mn) {
+                        for (int i = 0; i < BM / 64; ++i)
+                            tma_load_2d_pair(sa + i * MN_CHUNK_BYTES, ma[p.pa[pr]], ra + i * 64, kx, bar);
+                    } else {
+                        tma_load_2d_pair(sa, ma[p.pa[pr]], kx, ra, bar);
+                    }
+                    if (MN_OK && p.b_mn) {
+                        for (int i = 0; i < 128 / 64; ++i)
+                            tma_load_2d_pair(sb + i * MN_CHUNK_BYTES, mb[p.pb[pr]], rb + i * 64, kx, bar);
+                    } else {
+                        tma_load_2d_pair(sb, mb[p.pb[pr]], kx, rb, bar);
+                    }
                     if (++s == STAGES) { s = 0; ph ^= 1; }
                 }
             }
@@ -700,8 +953,11 @@ __global__ void __launch_bounds__(THREADS, 1)
         // ---------------------------------------------------------- MMA issuer (leader only)
         if (lane == 0 && leader) {
             const uint32_t fmt = TF32 ? 2u : (uint32_t)p.ab_fmt;
-            const uint32_t idesc = (1u << 4) | (fmt << 7) | (fmt << 10) |
-                                   ((uint32_t)(BN >> 3) << 17) | ((uint32_t)((2 * BM) >> 4) << 24);
+            const int a_mn = MN_OK && p.a_mn, b_mn = MN_OK && p.b_mn;
+            const uint32_t idesc = (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)a_mn << 15) |
+                                   ((uint32_t)b_mn << 16) | ((uint32_t)(BN >> 3) << 17) |
+                                   ((uint32_t)((2 * BM) >> 4) << 24);
+            const uint64_t a_step = a_mn ? 128 : 2, b_step = b_mn ? 128 : 2;  // per MMA, 16-byte units
             int s = 0;
             uint32_t ph = 0;
             int acc = 0;
@@ -719,10 +975,11 @@ __global__ void __launch_bounds__(THREADS, 1)
                         tc_fence_after();
                         const uint32_t sa = smem_u32(tiles + s * STAGE_BYTES);
                         const uint32_t sb = sa + A_TILE;
-                        const uint64_t da = smem_desc_sw128(sa), db = smem_desc_sw128(sb);
+                        const uint64_t da = a_mn ? smem_desc_mn_sw128(sa) : smem_desc_sw128(sa);
+                        const uint64_t db = b_mn ? smem_desc_mn_sw128(sb) : smem_desc_sw128(sb);
 #pragma unroll
                         for (int kk = 0; kk < 4; ++kk)
-                            umma_pair<TF32>(d, da + (uint64_t)(2 * kk), db + (uint64_t)(2 * kk), idesc,
+                            umma_pair<TF32>(d, da + a_step * kk, db + b_step * kk, idesc,
                                             (st > c0 || kk > 0) ? 1u : 0u);
                         commit_both(&empty[s]);
                         if (++s == STAGES) { s = 0; ph ^= 1; }
@@ -738,115 +995,14 @@ __global__ void __launch_bounds__(THREADS, 1)
         }
     } else {
         // ---------------------------------------------------------- epilogue (both CTAs)
-        const int ew = warp - 2;
-        const int q = warp & 3;
-        const int half = ew / 4;
-        const int nchunks = (p.kblocks + p.chunk - 1) / p.chunk;
         const uint32_t tempty_leader[2] = {map_rank(&tempty[0], 0), map_rank(&tempty[1], 0)};
-        int acc = 0;
-        uint32_t acc_ph = 0;
-        bool ok = true;
-        for (int t = pair; t < ntiles && ok; t += npairs) {
-            int tm, tn;
-            tile_at(p.tri, t, tiles_m, tiles_n, 2 * BM, BN, tm, tn);
-            float sum[EPI_COLS];
-#pragma unroll
-            for (int j = 0; j < EPI_COLS; ++j) sum[j] = 0.f;
-            for (int c = 0; c < nchunks; ++c) {
-                int w = 1;
-                if (lane == 0) w = mbar_wait(&tfull[acc], acc_ph, abort_flag) ? 1 : 0;
-                ok = __shfl_sync(0xffffffffu, w, 0) != 0;
-                if (!ok) break;
-                tc_fence_after();
-                const uint32_t taddr =
-                    tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN + half * EPI_COLS);
-#pragma unroll
-                for (int g = 0; g < EPI_COLS / 32; ++g) {
-                    float v[32];
-                    tmem_ld32(taddr + (uint32_t)(g * 32), v);
-#pragma unroll
-                    for (int j = 0; j < 32; ++j) sum[g * 32 + j] += v[j];
-                }
-                tc_fence_before();
-                __syncwarp();
-                if (lane == 0) arrive_remote(tempty_leader[acc]);
-                if (++acc == 2) { acc = 0; acc_ph ^= 1; }
-            }
-            if (!ok) break;
-            const int row = tm * 2 * BM + (int)rank * BM + q * 32 + lane;
-            const int col0 = tn * BN + half * EPI_COLS;
-            const bool beta_zero = p.beta_re == 0.f && p.beta_im == 0.f;
-            if (row < p.M) {
-                if (p.out_half) {
-                    __half* const Ch = (__half*)p.C;
-#pragma unroll
-                    for (int j0 = 0; j0 < EPI_COLS; j0 += 8) {
-                        float cv[8];
-#pragma unroll
-                        for (int j = 0; j < 8; ++j) {
-                            const int col = col0 + j0 + j;
-                            cv[j] = (!beta_zero && col < p.N && in_tri(p.tri, row, col))
-                                        ? __half2float(Ch[(long)col * p.ldc + row])
-                                        : 0.f;
-                        }
-#pragma unroll
-                        for (int j = 0; j < 8; ++j) {
-                            const int col = col0 + j0 + j;
-                            if (col < p.N && in_tri(p.tri, row, col))
-                                Ch[(long)col * p.ldc + row] = __float2half_rn(
-                                    beta_zero ? __fmul_rn(p.alpha_re, sum[j0 + j])
-                                              : fmaf(p.alpha_re, sum[j0 + j], __fmul_rn(p.beta_re, cv[j])));
-                        }
-                    }
-                } else if (!p.complex_out) {
-#pragma unroll
-                    for (int j0 = 0; j0 < EPI_COLS; j0 += 8) {
-                        float cv[8];
-#pragma unroll
-                        for (int j = 0; j < 8; ++j) {
-                            const int col = col0 + j0 + j;
-                            cv[j] = (!beta_zero && col < p.N && in_tri(p.tri, row, col)) ? p.C[(long)col * p.ldc + row]
-                                                                                          : 0.f;
-                        }
-#pragma unroll
-                        for (int j = 0; j < 8; ++j) {
-                            const int col = col0 + j0 + j;
-                            if (col < p.N && in_tri(p.tri, row, col))
-                                p.C[(long)col * p.ldc + row] =
-                                    beta_zero ? __fmul_rn(p.alpha_re, sum[j0 + j])
-                                              : fmaf(p.alpha_re, sum[j0 + j], __fmul_rn(p.beta_re, cv[j]));
-                        }
-                    }
-                } else {
-                    float2* const C2 = (float2*)p.C;
-#pragma unroll
-                    for (int j0 = 0; j0 < EPI_COLS; j0 += 8) {
-                        float2 cv[4];
-#pragma unroll
-                        for (int j = 0; j < 4; ++j) {
-                            const int col = col0 + j0 + 2 * j;
-                            cv[j] = (!beta_zero && col < p.N) ? C2[(long)(col >> 1) * p.ldc + row]
-                                                              : make_float2(0.f, 0.f);
-                        }
-#pragma unroll
-                        for (int j = 0; j < 4; ++j) {
-                            const int col = col0 + j0 + 2 * j;
-                            if (col < p.N) {
-                                const float re = sum[j0 + 2 * j], im = sum[j0 + 2 * j + 1];
-                                float2 r;
-                                r.x = fmaf(p.alpha_re, re, -p.alpha_im * im);
-                                r.y = fmaf(p.alpha_re, im, p.alpha_im * re);
-                                if (!beta_zero) {
-                                    r.x += fmaf(p.beta_re, cv[j].x, -p.beta_im * cv[j].y);
-                                    r.y += fmaf(p.beta_re, cv[j].y, p.beta_im * cv[j].x);
-                                }
-                                C2[(long)(col >> 1) * p.ldc + row] = r;
-                            }
-                        }
-                    }
-                }
-            }
-        }
+        auto arrive = [&](int a) { arrive_remote(tempty_leader[a]); };
+        if constexpr (TF32 || OUT == OUT_F16)
+            epilogue_single<OUT, BN, EPI_COLS>(p, &mC, pair, npairs, ntiles, tiles_m, tiles_n, 2 * BM,
+                                                (int)rank * BM, tmem_base, tfull, arrive, epi_buf, cbar, abort_flag);
+        else
+            epilogue_multi<OUT, BN, EPI_COLS>(p, pair, npairs, ntiles, tiles_m, tiles_n, 2 * BM, (int)rank * BM,
+                                               tmem_base, tfull, arrive, abort_flag);
     }
 
     __syncthreads();
@@ -1061,18 +1217,65 @@ EncodeTiledFn encode_fn()
     return fn;
 }
 
-bool make_map(CUtensorMap* m, void* base, bool tf32, long rows, long kpad, int box_rows)
+// One operand as the engine reads it: a prepared K-major plane, or the
+// caller's own 16-bit array in either layout.
+struct Operand {
+    const void* base;
+    long rows;  // M (A) or N (B)
+    long kext;  // K extent; the copies zero-fill past it
+    long ld;    // elements between consecutive rows (K-major) or consecutive K indices (MN-major)
+    bool mn;    // MN-major: the rows are contiguous
+};
+
+bool make_operand_map(CUtensorMap* m, const Operand& o, bool tf32, int box_rows)
 {
     EncodeTiledFn f = encode_fn();
     if (!f) return false;
     const int esize = tf32 ? 4 : 2;
-    cuuint64_t dims[2] = {(cuuint64_t)kpad, (cuuint64_t)rows};
-    cuuint64_t strides[1] = {(cuuint64_t)(kpad * esize)};
-    cuuint32_t box[2] = {(cuuint32_t)(ROW_BYTES / esize), (cuuint32_t)box_rows};
+    const cuuint32_t kbox = ROW_BYTES / esize;
+    cuuint64_t dims[2] = {(cuuint64_t)o.kext, (cuuint64_t)o.rows};
+    cuuint32_t box[2] = {kbox, (cuuint32_t)box_rows};
+    if (o.mn) {  // boxes of 64 rows x 64 K (16-bit operands only)
+        if (tf32) return false;
+        dims[0] = (cuuint64_t)o.rows;
+        dims[1] = (cuuint64_t)o.kext;
+        box[1] = kbox;
+    }
+    cuuint64_t strides[1] = {(cuuint64_t)(o.ld * esize)};
     cuuint32_t estr[2] = {1, 1};
-    CUresult r = f(m, tf32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims,
-                   strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    CUresult r = f(m, tf32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2,
+                   const_cast<void*>(o.base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+// C as boxes of 128 rows x 16 columns (complex: 8 columns of (re, im)
+// pairs), unswizzled, for the staged epilogue.  False when C cannot be
+// addressed that way (alignment, triangular output).
+bool make_c_map(CUtensorMap* m, Params& p)
+{
+    EncodeTiledFn f = encode_fn();
+    if (!f || p.tri != 0 || !p.C || p.M <= 0 || p.N <= 0 || ((uintptr_t)p.C & 15) != 0) return false;
+    const int esize = p.out_half ? 2 : (p.complex_out ? 8 : 4);
+    const long pitch = p.ldc * esize;
+    if (pitch % 16 != 0 || pitch >= (1L << 40)) return false;
+    // a store clips rows only at 16-byte granularity: the map stops at the
+    // last whole 16 bytes of each column, the rest are stored directly
+    p.m_tma = p.M - p.M % (16 / esize);
+    if (p.m_tma == 0) return false;
+    cuuint64_t dims[2] = {(cuuint64_t)p.m_tma, (cuuint64_t)p.N};
+    cuuint32_t box[2] = {128, (cuuint32_t)EPI_GROUP};
+    if (p.complex_out) {
+        dims[0] = 2 * (cuuint64_t)p.m_tma;
+        dims[1] = (cuuint64_t)(p.N / 2);
+        box[0] = 256;
+        box[1] = EPI_GROUP / 2;
+    }
+    cuuint64_t strides[1] = {(cuuint64_t)pitch};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = f(m, p.out_half ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void*)p.C,
+                   dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                   CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS;
 }
 
@@ -1129,28 +1332,35 @@ cudaError_t run_split(iclblasHandle_t h, const T* S, int R, int K, long rs, long
 
 }  // namespace
 
-// Launches the persistent tcgen05 kernel over prepared K-major planes (A:
-// rows_a x kpad, B: rows_b x kpad, one per split level): CTA pairs
-// (256 x 256 tiles) when there are enough pair tiles to fill the GPU; else
-// single CTAs, with 128-wide tiles when 256-wide ones would leave a quarter
-// of the SMs idle.
-cudaError_t launch_engine(iclblasHandle_t h, const ModeInfo& mi, void* const* a_planes, void* const* b_planes,
-                          long rows_a, long rows_b, long kpad, Params& p)
+// Launches the persistent tcgen05 kernel over the operands (one per split
+// level): CTA pairs (256 x 256 tiles) when there are enough pair tiles to
+// fill the GPU; else single CTAs, with 128-wide tiles when 256-wide ones
+// would leave a quarter of the SMs idle.
+cudaError_t launch_engine(iclblasHandle_t h, const ModeInfo& mi, const Operand* a, const Operand* b, Params& p)
 {
+    const long rows_a = a[0].rows, rows_b = b[0].rows;
     const int m = (int)rows_a;
     const int pair_tiles = ceil_div(m, 2 * BM) * ceil_div((long)rows_b, 256);
     const bool pairs = pair_tiles * 2 >= h->sm_count;
     const int tiles256 = ceil_div(m, BM) * ceil_div((long)rows_b, 256);
     const int bn = pairs ? 128 : (tiles256 * 4 < h->sm_count * 3 ? 128 : 256);  // B box rows
-    CUtensorMap ma[3], mb[3];
+    CUtensorMap ma[3], mb[3], mc;
     for (int l = 0; l < 3; ++l) {
         const int ll = l < mi.nlev ? l : 0;
-        if (!make_map(&ma[l], a_planes[ll], mi.tf32, rows_a, kpad, BM)) return cudaErrorInvalidValue;
-        if (!make_map(&mb[l], b_planes[ll], mi.tf32, rows_b, kpad, bn)) return cudaErrorInvalidValue;
+        if (!make_operand_map(&ma[l], a[ll], mi.tf32, BM)) return cudaErrorInvalidValue;
+        if (!make_operand_map(&mb[l], b[ll], mi.tf32, bn)) return cudaErrorInvalidValue;
     }
+    p.a_mn = a[0].mn ? 1 : 0;
+    p.b_mn = b[0].mn ? 1 : 0;
+    // staged stores in the single-chunk kernels (TF32, HGEMM); the BF16
+    // modes' stores overlap their longer MMA work and go direct
+    const bool single = mi.tf32 || p.out_half;  // the whole K in one accumulator
+    p.c_tma = single && make_c_map(&mc, p) ? 1 : 0;
+    const int smem = single ? SMEM_BYTES : SMEM_BYTES_DIRECT;
+    if (!p.c_tma) mc = ma[0];  // unused by the kernel
     if (pairs) {
         auto run2 = [&](auto kernel) -> cudaError_t {
-            cudaError_t r = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+            cudaError_t r = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
             if (r != cudaSuccess) return r;
             cudaLaunchConfig_t cfg = {};
             cudaLaunchAttribute attr[1];
@@ -1159,7 +1369,7 @@ cudaError_t launch_engine(iclblasHandle_t h, const ModeInfo& mi, void* const* a_
             attr[0].val.clusterDim.y = 1;
             attr[0].val.clusterDim.z = 1;
             cfg.blockDim = dim3(THREADS);
-            cfg.dynamicSmemBytes = SMEM_BYTES;
+            cfg.dynamicSmemBytes = smem;
             cfg.stream = h->stream;
             cfg.attrs = attr;
             cfg.numAttrs = 1;
@@ -1171,22 +1381,29 @@ cudaError_t launch_engine(iclblasHandle_t h, const ModeInfo& mi, void* const* a_
                 max_clusters = std::max(1, h->sm_count / 2);
             }
             cfg.gridDim = dim3(2 * std::min(pair_tiles, max_clusters));
-            r = cudaLaunchKernelEx(&cfg, kernel, ma[0], ma[1], ma[2], mb[0], mb[1], mb[2], p);
+            r = cudaLaunchKernelEx(&cfg, kernel, ma[0], ma[1], ma[2], mb[0], mb[1], mb[2], mc, p);
             if (r != cudaSuccess) return r;
             return cudaGetLastError();
         };
-        return mi.tf32 ? run2(gemm_tc2_kernel<true>) : run2(gemm_tc2_kernel<false>);
+        if (p.out_half) return run2(gemm_tc2_kernel<false, OUT_F16>);
+        if (p.complex_out) return mi.tf32 ? run2(gemm_tc2_kernel<true, OUT_C64>) : run2(gemm_tc2_kernel<false, OUT_C64>);
+        return mi.tf32 ? run2(gemm_tc2_kernel<true, OUT_F32>) : run2(gemm_tc2_kernel<false, OUT_F32>);
     }
     const int tiles = ceil_div(m, BM) * ceil_div((long)rows_b, bn);
     const int grid = std::min(tiles, h->sm_count);
     auto run = [&](auto kernel) -> cudaError_t {
-        cudaError_t r = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+        cudaError_t r = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (r != cudaSuccess) return r;
-        kernel<<<grid, THREADS, SMEM_BYTES, h->stream>>>(ma[0], ma[1], ma[2], mb[0], mb[1], mb[2], p);
+        kernel<<<grid, THREADS, smem, h->stream>>>(ma[0], ma[1], ma[2], mb[0], mb[1], mb[2], mc, p);
         return cudaGetLastError();
     };
-    if (mi.tf32) return bn == 128 ? run(gemm_tc_kernel<true, 128>) : run(gemm_tc_kernel<true, 256>);
-    return bn == 128 ? run(gemm_tc_kernel<false, 128>) : run(gemm_tc_kernel<false, 256>);
+    if (p.out_half) return bn == 128 ? run(gemm_tc_kernel<false, 128, OUT_F16>) : run(gemm_tc_kernel<false, 256, OUT_F16>);
+    if (p.complex_out) {
+        if (mi.tf32) return bn == 128 ? run(gemm_tc_kernel<true, 128, OUT_C64>) : run(gemm_tc_kernel<true, 256, OUT_C64>);
+        return bn == 128 ? run(gemm_tc_kernel<false, 128, OUT_C64>) : run(gemm_tc_kernel<false, 256, OUT_C64>);
+    }
+    if (mi.tf32) return bn == 128 ? run(gemm_tc_kernel<true, 128, OUT_F32>) : run(gemm_tc_kernel<true, 256, OUT_F32>);
+    return bn == 128 ? run(gemm_tc_kernel<false, 128, OUT_F32>) : run(gemm_tc_kernel<false, 256, OUT_F32>);
 }
 
 // Real or complex GEMM on the tensor cores.  `cplx` selects complex operands
@@ -1247,36 +1464,55 @@ cudaError_t gemm_tc(iclblasHandle_t h, int ta, int tb, int m, int n, int k, T al
     p.tri = cplx ? 0 : tri;
     p.ab_fmt = 1;
     p.out_half = 0;
-    void* pa[3] = {oa.plane[0], oa.plane[1], oa.plane[2]};
-    void* pb[3] = {ob.plane[0], ob.plane[1], ob.plane[2]};
-    return launch_engine(h, mi, pa, pb, m, rows_b, kpad, p);
+    Operand pa[3], pb[3];
+    for (int l = 0; l < 3; ++l) {
+        pa[l] = Operand{oa.plane[l], rows_a, kpad, kpad, false};
+        pb[l] = Operand{ob.plane[l], rows_b, kpad, kpad, false};
+    }
+    return launch_engine(h, mi, pa, pb, p);
 }
 
 // HGEMM: IEEE half operands and result, products on the tensor cores with
 // the f16 operand format, the whole K accumulated in FP32 in TMEM, one
-// rounding of alpha * acc + beta * C to half.
+// rounding of alpha * acc + beta * C to half.  The tensor core reads either
+// operand layout, so each operand is read in place (A: MN-major for op N,
+// K-major for op T / C; B the other way round) when TMA can address it
+// (16-byte aligned base and leading dimension); otherwise it is first
+// packed K-major into scratch.
 cudaError_t hgemm_tc(iclblasHandle_t h, int ta, int tb, int m, int n, int k, float alpha, const __half* A, int lda,
                      const __half* B, int ldb, float beta, __half* C, int ldc)
 {
     const int kblk = ROW_BYTES / 2;
     const long kpad = std::max<long>(kblk, ((long)k + kblk - 1) / kblk * kblk);
-    const size_t align = 1024;
-    const size_t plane_a = ((size_t)m * kpad * 2 + align - 1) / align * align;
-    const size_t plane_b = ((size_t)n * kpad * 2 + align - 1) / align * align;
-    char* ws = (char*)scratch(h, plane_a + plane_b);
-    if (!ws) return cudaErrorMemoryAllocation;
-    __half* la = (__half*)ws;
-    __half* lb = (__half*)(ws + plane_a);
     const bool at = ta != ICLBLAS_OP_N, bt = tb != ICLBLAS_OP_N;
-    // A: L[r=m][k] ; op N: S[m + k*lda] ; op T/C: S[k + m*lda]
-    pack_half_kernel<<<dim3((unsigned)ceil_div(kpad, 64L), (unsigned)ceil_div(m, 32)), 256, 0, h->stream>>>(
-        m, k, A, at ? lda : 1, at ? 1 : lda, la, kpad);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    // B: L[r=n][k] = op(B)[k][n] ; op N: S[k + n*ldb] ; op T/C: S[n + k*ldb]
-    pack_half_kernel<<<dim3((unsigned)ceil_div(kpad, 64L), (unsigned)ceil_div(n, 32)), 256, 0, h->stream>>>(
-        n, k, B, bt ? 1 : ldb, bt ? ldb : 1, lb, kpad);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    auto in_place = [&](const __half* X, int ld) { return k > 0 && ((uintptr_t)X & 15) == 0 && ld % 8 == 0; };
+    const bool a_direct = in_place(A, lda), b_direct = in_place(B, ldb);
+    Operand oa{A, m, k, lda, !at}, ob{B, n, k, ldb, bt};
+    if (!a_direct || !b_direct) {
+        const size_t align = 1024;
+        const size_t plane_a = a_direct ? 0 : ((size_t)m * kpad * 2 + align - 1) / align * align;
+        const size_t plane_b = b_direct ? 0 : ((size_t)n * kpad * 2 + align - 1) / align * align;
+        char* ws = (char*)scratch(h, plane_a + plane_b);
+        if (!ws) return cudaErrorMemoryAllocation;
+        if (!a_direct) {
+            __half* la = (__half*)ws;
+            // A: L[r=m][k] ; op N: S[m + k*lda] ; op T/C: S[k + m*lda]
+            pack_half_kernel<<<dim3((unsigned)ceil_div(kpad, 64L), (unsigned)ceil_div(m, 32)), 256, 0, h->stream>>>(
+                m, k, A, at ? lda : 1, at ? 1 : lda, la, kpad);
+            cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess) return e;
+            oa = Operand{la, m, kpad, kpad, false};
+        }
+        if (!b_direct) {
+            __half* lb = (__half*)(ws + plane_a);
+            // B: L[r=n][k] = op(B)[k][n] ; op N: S[k + n*ldb] ; op T/C: S[n + k*ldb]
+            pack_half_kernel<<<dim3((unsigned)ceil_div(kpad, 64L), (unsigned)ceil_div(n, 32)), 256, 0, h->stream>>>(
+                n, k, B, bt ? 1 : ldb, bt ? ldb : 1, lb, kpad);
+            cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess) return e;
+            ob = Operand{lb, n, kpad, kpad, false};
+        }
+    }
     ModeInfo mi{};
     mi.tf32 = false;
     mi.nlev = 1;
@@ -1296,9 +1532,8 @@ cudaError_t hgemm_tc(iclblasHandle_t h, int ta, int tb, int m, int n, int k, flo
     p.tri = 0;
     p.ab_fmt = 0;
     p.out_half = 1;
-    void* pa[3] = {la, la, la};
-    void* pb[3] = {lb, lb, lb};
-    return launch_engine(h, mi, pa, pb, m, n, kpad, p);
+    const Operand pa[3] = {oa, oa, oa}, pb[3] = {ob, ob, ob};
+    return launch_engine(h, mi, pa, pb, p);
 }
 
 template cudaError_t gemm_tc<float>(iclblasHandle_t, int, int, int, int, int, float, const float*, int, const float*,

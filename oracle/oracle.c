@@ -1037,16 +1037,31 @@ static uint16_t half_bits(double x)
 void orc_hgemm(int transa, int transb, int m, int n, int k, float alpha, const uint16_t* A, int lda,
                const uint16_t* B, int ldb, float beta, uint16_t* C, int ldc)
 {
+    /* op(A) rows and op(B) columns converted once, K-contiguous (the sums
+       run over l in the same order as a direct loop) */
+    double* Ad = (double*)malloc(sizeof(double) * ((size_t)m * (size_t)k + 1));
+    double* Bd = (double*)malloc(sizeof(double) * ((size_t)n * (size_t)k + 1));
+    if (!Ad || !Bd) {
+        free(Ad);
+        free(Bd);
+        return;
+    }
+    for (int i = 0; i < m; ++i)
+        for (int l = 0; l < k; ++l)
+            Ad[(size_t)i * k + l] = half_value(transa ? A[(long)i * lda + l] : A[(long)l * lda + i]);
+    for (int j = 0; j < n; ++j)
+        for (int l = 0; l < k; ++l)
+            Bd[(size_t)j * k + l] = half_value(transb ? B[(long)l * ldb + j] : B[(long)j * ldb + l]);
     for (int j = 0; j < n; ++j)
         for (int i = 0; i < m; ++i) {
+            const double* a = Ad + (size_t)i * k;
+            const double* b = Bd + (size_t)j * k;
             double acc = 0.0;
-            for (int l = 0; l < k; ++l) {
-                const double a = half_value(transa ? A[(long)i * lda + l] : A[(long)l * lda + i]);
-                const double b = half_value(transb ? B[(long)l * ldb + j] : B[(long)j * ldb + l]);
-                acc += a * b;
-            }
+            for (int l = 0; l < k; ++l) acc += a[l] * b[l];
             double out = (double)alpha * acc;
             if (beta != 0.0f) out += (double)beta * half_value(C[(long)j * ldc + i]);
             C[(long)j * ldc + i] = half_bits(out);
         }
+    free(Ad);
+    free(Bd);
 }

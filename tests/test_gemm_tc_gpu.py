@@ -161,3 +161,42 @@ def test_cgemm_tensor_core_cta_pairs(handle):
     handle.set_math_mode(B.MATH_BF16X3)
     assert B.iclblasCgemm(handle, 0, 0, m, n, k, al, A, m, Bm, k, be, Cm, m) == B.SUCCESS
     assert O.rel_fro(Cm.reshape(n, m).T, ref) <= BARS[B.MATH_BF16X3]
+
+
+@pytest.mark.parametrize("mode", [B.MATH_TF32, B.MATH_BF16X3, B.MATH_BF16X6])
+@pytest.mark.parametrize("m,n,k", [(300, 217, 70), (2560 + 37, 2048 + 5, 96)])
+def test_sgemm_tensor_core_staged_c_edges(handle, mode, m, n, k):
+    """ldc a multiple of 4 floats: C is read and written through TMA boxes
+    (single CTAs and CTA pairs), which must clip at row m and column n and
+    leave the rows between m and ldc untouched."""
+    rng = np.random.default_rng(1300 + mode + m)
+    ldc = (m + 3) // 4 * 4 + 4
+    A = O.colmajor(m, k, m, rng)
+    Bm = O.colmajor(k, n, k + 1, rng)
+    Cm = O.colmajor(m, n, ldc, rng)
+    ref = _dref(0, 0, m, n, k, 1.5, A, m, Bm, k + 1, -0.75, Cm, ldc)
+    handle.set_math_mode(mode)
+    assert B.iclblasSgemm(handle, 0, 0, m, n, k, 1.5, A, m, Bm, k + 1, -0.75, Cm, ldc) == B.SUCCESS
+    got, want = Cm.reshape(n, ldc), ref.reshape(n, ldc)
+    assert O.rel_fro(got[:, :m], want[:, :m]) <= BARS[mode]
+    assert np.array_equal(got[:, m:], want[:, m:].astype(np.float32))
+
+
+@pytest.mark.parametrize("m,n", [(150, 131), (2560 + 3, 1030)])
+def test_cgemm_tensor_core_staged_c_edges(handle, m, n):
+    """Complex C through TMA boxes of (re, im) pairs: ragged edges, ldc even."""
+    k = 45
+    rng = np.random.default_rng(1400 + m)
+    ldc = m + (m % 2) + 2
+    A = O.colmajor(m, k, m, rng, np.complex64)
+    Bm = O.colmajor(k, n, k, rng, np.complex64)
+    Cm = O.colmajor(m, n, ldc, rng, np.complex64)
+    C0 = Cm.copy()
+    al, be = 0.5 - 1.0j, -0.25 + 0.75j
+    Ad = A.astype(np.complex128).reshape(k, m).T
+    Bd = Bm.astype(np.complex128).reshape(n, k).T
+    ref = al * (Ad @ Bd) + be * Cm.astype(np.complex128).reshape(n, ldc).T[:m]
+    handle.set_math_mode(B.MATH_BF16X6)
+    assert B.iclblasCgemm(handle, 0, 0, m, n, k, al, A, m, Bm, k, be, Cm, ldc) == B.SUCCESS
+    assert O.rel_fro(Cm.reshape(n, ldc).T[:m], ref) <= BARS[B.MATH_BF16X6]
+    assert np.array_equal(Cm.reshape(n, ldc)[:, m:], C0.reshape(n, ldc)[:, m:])

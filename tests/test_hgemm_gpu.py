@@ -43,13 +43,26 @@ def host(t):
     return t.cpu().numpy()
 
 
-@pytest.mark.parametrize("m,n,k", [(1, 1, 1), (128, 128, 64), (300, 517, 129), (1000, 999, 2049), (33, 2000, 5)])
+def _ld(rows, aligned, extra):
+    """Leading dimension: a multiple of 8 halves (16 bytes: operands read in
+    place, C stored through TMA) or rows + extra (packed operands, direct
+    stores)."""
+    return (rows + 7) // 8 * 8 + 8 if aligned else rows + extra
+
+
+_SIZES = [(1, 1, 1), (128, 128, 64), (300, 517, 129), (1000, 999, 2049), (33, 2000, 5)]
+# every size with packed operands; the in-place layouts on the sizes the
+# oracle finishes quickly
+_CASES = [s + (False,) for s in _SIZES] + [s + (True,) for s in _SIZES if s[2] < 1000]
+
+
+@pytest.mark.parametrize("m,n,k,aligned", _CASES)
 @pytest.mark.parametrize("ta,tb", [(0, 0), (1, 0), (0, 1), (1, 1)])
-def test_hgemm_vs_oracle(handle, m, n, k, ta, tb):
+def test_hgemm_vs_oracle(handle, m, n, k, ta, tb, aligned):
     rng = np.random.default_rng(m + n + k + 2 * ta + tb)
-    lda = (k if ta else m) + 1
-    ldb = (n if tb else k) + 2
-    ldc = m + 3
+    lda = _ld(k if ta else m, aligned, 1)
+    ldb = _ld(n if tb else k, aligned, 2)
+    ldc = _ld(m, aligned, 3)
     A = rng.uniform(-1, 1, lda * (m if ta else k)).astype(np.float16)
     Bm = rng.uniform(-1, 1, ldb * (k if tb else n)).astype(np.float16)
     Cm = rng.uniform(-1, 1, ldc * n).astype(np.float16)
