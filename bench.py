@@ -769,9 +769,12 @@ CONV1X1_SHAPES = [
 def run_conv1x1_study(args, torch):
     """ResNet-50 1x1-convolution GEMMs (activations M x K, weights K x N,
     output M x N; synthetic U(-1,1), seed 5): HGEMM (half storage, FP32
-    accumulation) and SGEMM in every math mode, TFLOP/s = 2 M N K / event
-    time (median of 10), relative Frobenius error against FP64 (torch,
-    plumbing only)."""
+    accumulation) and SGEMM in every math mode.  TFLOP/s = 2 M N K / the
+    event time per call of 20 back-to-back calls (median of 3 batches; the
+    host work of a call overlaps the previous call's kernels), and
+    `single_call_us` = one call between two events (median of 10; includes
+    the host work).  Relative Frobenius error against FP64 (torch, plumbing
+    only)."""
     from clgpu_b200 import iclblas as B
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
@@ -803,19 +806,31 @@ def run_conv1x1_study(args, torch):
                     e1.record(stream)
                     torch.cuda.synchronize()
                     ts.append(e0.elapsed_time(e1))
-                return float(np.median(ts))
-            ms = timed(lambda: B.iclblasHgemm(h, 0, 0, M, N, K, 1.0, Ah, M, Wh, K, 0.0, Ch, M))
-            err = float(torch.linalg.norm(Ch.double() - refh) / torch.linalg.norm(refh))
-            print(json.dumps({"shape": name, "M": M, "K": K, "N": N, "routine": "hgemm", "ms": round(ms, 4),
-                              "tflops": round(flops / (ms / 1e3) / 1e12, 1), "rel_fro_err_vs_fp64": err}),
-                  flush=True)
+                bs = []
+                for _ in range(3):
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    for _ in range(20):
+                        B.check(f(), name)
+                    e1.record(stream)
+                    torch.cuda.synchronize()
+                    bs.append(e0.elapsed_time(e1) / 20)
+                return float(np.median(bs)), float(np.median(ts))
+
+            def line(extra, ms, single, err):
+                d = {"shape": name, "M": M, "K": K, "N": N, **extra, "ms": round(ms, 4),
+                     "tflops": round(flops / (ms / 1e3) / 1e12, 1), "single_call_us": round(single * 1e3, 1),
+                     "rel_fro_err_vs_fp64": err}
+                print(json.dumps(d), flush=True)
+            ms, single = timed(lambda: B.iclblasHgemm(h, 0, 0, M, N, K, 1.0, Ah, M, Wh, K, 0.0, Ch, M))
+            line({"routine": "hgemm"}, ms, single,
+                 float(torch.linalg.norm(Ch.double() - refh) / torch.linalg.norm(refh)))
             for mname, mode in modes:
                 h.set_math_mode(mode)
-                ms = timed(lambda: B.iclblasSgemm(h, 0, 0, M, N, K, 1.0, A, M, W, K, 0.0, C, M))
-                err = float(torch.linalg.norm(C.double() - ref) / torch.linalg.norm(ref))
-                print(json.dumps({"shape": name, "M": M, "K": K, "N": N, "routine": "sgemm", "mode": mname,
-                                  "ms": round(ms, 4), "tflops": round(flops / (ms / 1e3) / 1e12, 1),
-                                  "rel_fro_err_vs_fp64": err}), flush=True)
+                ms, single = timed(lambda: B.iclblasSgemm(h, 0, 0, M, N, K, 1.0, A, M, W, K, 0.0, C, M))
+                line({"routine": "sgemm", "mode": mname}, ms, single,
+                     float(torch.linalg.norm(C.double() - ref) / torch.linalg.norm(ref)))
             h.set_math_mode(B.MATH_PLAIN_FP32)
             del A, W, C, Ah, Wh, Ch, ref, refh
             torch.cuda.empty_cache()
