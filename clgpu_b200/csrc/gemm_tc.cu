@@ -235,20 +235,19 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v)
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// 32 lanes x 64 consecutive columns of FP32 from TMEM; the wait is in the
-// same statement, so no register is read before the load has completed.
-__device__ __forceinline__ void tmem_ld64(uint32_t taddr, float* v)
+// 32 lanes x 16 consecutive columns of FP32 from TMEM.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v)
 {
-    uint32_t r[64];
+    uint32_t r[16];
     asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x64.b32 "
-        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47,%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%64];\n\t"
-        "tcgen05.wait::ld.sync.aligned;"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]), "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]), "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]), "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]), "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
-        : "r"(taddr)
-        : "memory");
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-    for (int i = 0; i < 64; ++i) v[i] = __uint_as_float(r[i]);
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
 // Shared-memory matrix descriptor, K-major, 128-byte swizzle: rows of 128 B,
@@ -553,24 +552,14 @@ __device__ __forceinline__ void epilogue_single(const Params& p, const CUtensorM
         const int row0 = tm * tile_rows + row_off, col0 = tn * BN + half * EPI_COLS;
         const uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN + half * EPI_COLS);
         bool stored = true;
-        // 64 columns per TMEM load (one round trip for four groups)
-        constexpr int LOAD_COLS = 64;
-        static_assert(EPI_COLS % LOAD_COLS == 0, "epilogue columns");
 #pragma unroll 1
-        for (int c0 = 0; c0 < EPI_COLS && stored; c0 += LOAD_COLS) {
-            float v[LOAD_COLS];
-            tmem_ld64(taddr + (uint32_t)c0, v);
-#pragma unroll
-            for (int g = 0; g < LOAD_COLS / EPI_GROUP; ++g) {
-                float w16[EPI_GROUP];
-#pragma unroll
-                for (int j = 0; j < EPI_GROUP; ++j) w16[j] = v[g * EPI_GROUP + j];
-                if (p.c_tma) {
-                    if (stored) stored = stage_group<OUT>(w16, p, mC, eg, r, row0, col0 + c0 + g * EPI_GROUP, abort_flag);
-                } else {
-                    direct_group<OUT, EPI_GROUP>(w16, p, row0 + r, col0 + c0 + g * EPI_GROUP);
-                }
-            }
+        for (int g = 0; g < EPI_COLS / EPI_GROUP && stored; ++g) {
+            float v[EPI_GROUP];
+            tmem_ld16(taddr + (uint32_t)(g * EPI_GROUP), v);
+            if (p.c_tma)
+                stored = stage_group<OUT>(v, p, mC, eg, r, row0, col0 + g * EPI_GROUP, abort_flag);
+            else
+                direct_group<OUT, EPI_GROUP>(v, p, row0 + r, col0 + g * EPI_GROUP);
         }
         tc_fence_before();
         __syncwarp();
