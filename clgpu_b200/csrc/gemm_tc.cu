@@ -628,7 +628,7 @@ __device__ __forceinline__ void epilogue_multi(const Params& p, int t0, int tste
     }
 }
 
-template <bool TF32, int BN_, int OUT>
+template <bool TF32, int BN_, int OUT, bool SINGLE>
 __global__ void __launch_bounds__(THREADS, 1)
     gemm_tc_kernel(const __grid_constant__ CUtensorMap mA0, const __grid_constant__ CUtensorMap mA1,
                    const __grid_constant__ CUtensorMap mA2, const __grid_constant__ CUtensorMap mB0,
@@ -749,7 +749,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     } else {
         // ---------------------------------------------------------- epilogue
         auto arrive = [&](int a) { mbar_arrive(&tempty[a]); };
-        if constexpr (TF32 || OUT == OUT_F16)
+        if constexpr (SINGLE)
             epilogue_single<OUT, BN, EPI_COLS>(p, &mC, blockIdx.x, gridDim.x, ntiles, tiles_m, tiles_n, BM, 0,
                                                 tmem_base, tfull, arrive, epi_buf, cbar, abort_flag);
         else
@@ -857,7 +857,7 @@ __device__ __forceinline__ void dealloc_pair(uint32_t taddr, uint32_t ncols)
 }
 }  // namespace two_sm
 
-template <bool TF32, int OUT>
+template <bool TF32, int OUT, bool SINGLE>
 __global__ void __launch_bounds__(THREADS, 1)
     gemm_tc2_kernel(const __grid_constant__ CUtensorMap mA0, const __grid_constant__ CUtensorMap mA1,
                     const __grid_constant__ CUtensorMap mA2, const __grid_constant__ CUtensorMap mB0,
@@ -997,7 +997,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         // ---------------------------------------------------------- epilogue (both CTAs)
         const uint32_t tempty_leader[2] = {map_rank(&tempty[0], 0), map_rank(&tempty[1], 0)};
         auto arrive = [&](int a) { arrive_remote(tempty_leader[a]); };
-        if constexpr (TF32 || OUT == OUT_F16)
+        if constexpr (SINGLE)
             epilogue_single<OUT, BN, EPI_COLS>(p, &mC, pair, npairs, ntiles, tiles_m, tiles_n, 2 * BM,
                                                 (int)rank * BM, tmem_base, tfull, arrive, epi_buf, cbar, abort_flag);
         else
@@ -1352,9 +1352,10 @@ cudaError_t launch_engine(iclblasHandle_t h, const ModeInfo& mi, const Operand* 
     }
     p.a_mn = a[0].mn ? 1 : 0;
     p.b_mn = b[0].mn ? 1 : 0;
-    // staged stores in the single-chunk kernels (TF32, HGEMM); the BF16
-    // modes' stores overlap their longer MMA work and go direct
-    const bool single = mi.tf32 || p.out_half;  // the whole K in one accumulator
+    // staged stores in the single-chunk kernels: the whole K in one
+    // accumulator (TF32, HGEMM, and the BF16 modes when K fits one chunk); a
+    // multi-chunk tile's stores overlap its longer MMA work and go direct
+    const bool single = mi.tf32 || p.out_half || p.kblocks <= p.chunk;
     p.c_tma = single && make_c_map(&mc, p) ? 1 : 0;
     const int smem = single ? SMEM_BYTES : SMEM_BYTES_DIRECT;
     if (!p.c_tma) mc = ma[0];  // unused by the kernel
@@ -1385,9 +1386,12 @@ cudaError_t launch_engine(iclblasHandle_t h, const ModeInfo& mi, const Operand* 
             if (r != cudaSuccess) return r;
             return cudaGetLastError();
         };
-        if (p.out_half) return run2(gemm_tc2_kernel<false, OUT_F16>);
-        if (p.complex_out) return mi.tf32 ? run2(gemm_tc2_kernel<true, OUT_C64>) : run2(gemm_tc2_kernel<false, OUT_C64>);
-        return mi.tf32 ? run2(gemm_tc2_kernel<true, OUT_F32>) : run2(gemm_tc2_kernel<false, OUT_F32>);
+        if (p.out_half) return run2(gemm_tc2_kernel<false, OUT_F16, true>);
+        if (mi.tf32)
+            return p.complex_out ? run2(gemm_tc2_kernel<true, OUT_C64, true>) : run2(gemm_tc2_kernel<true, OUT_F32, true>);
+        if (p.complex_out)
+            return single ? run2(gemm_tc2_kernel<false, OUT_C64, true>) : run2(gemm_tc2_kernel<false, OUT_C64, false>);
+        return single ? run2(gemm_tc2_kernel<false, OUT_F32, true>) : run2(gemm_tc2_kernel<false, OUT_F32, false>);
     }
     const int tiles = ceil_div(m, BM) * ceil_div((long)rows_b, bn);
     const int grid = std::min(tiles, h->sm_count);
@@ -1397,13 +1401,20 @@ cudaError_t launch_engine(iclblasHandle_t h, const ModeInfo& mi, const Operand* 
         kernel<<<grid, THREADS, smem, h->stream>>>(ma[0], ma[1], ma[2], mb[0], mb[1], mb[2], mc, p);
         return cudaGetLastError();
     };
-    if (p.out_half) return bn == 128 ? run(gemm_tc_kernel<false, 128, OUT_F16>) : run(gemm_tc_kernel<false, 256, OUT_F16>);
-    if (p.complex_out) {
-        if (mi.tf32) return bn == 128 ? run(gemm_tc_kernel<true, 128, OUT_C64>) : run(gemm_tc_kernel<true, 256, OUT_C64>);
-        return bn == 128 ? run(gemm_tc_kernel<false, 128, OUT_C64>) : run(gemm_tc_kernel<false, 256, OUT_C64>);
+    // instantiations: TF32 and HGEMM always single-chunk; the BF16 modes
+    // single-chunk when the whole K fits one chunk (K <= 64 * chunk)
+    auto pick = [&](auto k128, auto k256) { return bn == 128 ? run(k128) : run(k256); };
+    if (p.out_half) return pick(gemm_tc_kernel<false, 128, OUT_F16, true>, gemm_tc_kernel<false, 256, OUT_F16, true>);
+    if (mi.tf32) {
+        if (p.complex_out) return pick(gemm_tc_kernel<true, 128, OUT_C64, true>, gemm_tc_kernel<true, 256, OUT_C64, true>);
+        return pick(gemm_tc_kernel<true, 128, OUT_F32, true>, gemm_tc_kernel<true, 256, OUT_F32, true>);
     }
-    if (mi.tf32) return bn == 128 ? run(gemm_tc_kernel<true, 128, OUT_F32>) : run(gemm_tc_kernel<true, 256, OUT_F32>);
-    return bn == 128 ? run(gemm_tc_kernel<false, 128, OUT_F32>) : run(gemm_tc_kernel<false, 256, OUT_F32>);
+    if (p.complex_out) {
+        if (single) return pick(gemm_tc_kernel<false, 128, OUT_C64, true>, gemm_tc_kernel<false, 256, OUT_C64, true>);
+        return pick(gemm_tc_kernel<false, 128, OUT_C64, false>, gemm_tc_kernel<false, 256, OUT_C64, false>);
+    }
+    if (single) return pick(gemm_tc_kernel<false, 128, OUT_F32, true>, gemm_tc_kernel<false, 256, OUT_F32, true>);
+    return pick(gemm_tc_kernel<false, 128, OUT_F32, false>, gemm_tc_kernel<false, 256, OUT_F32, false>);
 }
 
 // Real or complex GEMM on the tensor cores.  `cplx` selects complex operands
