@@ -69,7 +69,10 @@ constexpr int BM = 128;
 constexpr int ROW_BYTES = 128;                  // one K block per tile row
 constexpr int A_TILE = BM * ROW_BYTES;          // 16 KiB
 constexpr int RING_BYTES = 192 * 1024;          // the stage ring
-constexpr int EPI_GROUP = 16;                  // output columns per staged store
+constexpr int EPI_GROUP = 16;                  // FP32 output columns per staged store (half: 32)
+// output columns per staged store: one 8 KiB buffer of 128 rows
+template <int OUT>
+constexpr int group_cols() { return OUT == 1 /*half*/ ? 32 : EPI_GROUP; }
 constexpr int EPI_BUF_BYTES = 8192;             // one staging buffer: 128 rows x 16 FP32 columns
 constexpr int EPI_STAGE_BYTES = 4 * EPI_BUF_BYTES;  // two buffers for each half of the epilogue warps
 constexpr int MN_CHUNK_BYTES = 8192;            // MN-major operand: 64 rows x 64 K of 16-bit values
@@ -475,10 +478,11 @@ __device__ __forceinline__ void direct_group(const float (&v)[W], const Params& 
 // Returns false (in every thread of the half) when a wait gave up; the
 // leader's load into the current buffer may then still be in flight.
 template <int OUT>
-__device__ __forceinline__ bool stage_group(const float (&v)[EPI_GROUP], const Params& p, const CUtensorMap* mC,
+__device__ __forceinline__ bool stage_group(const float (&v)[group_cols<OUT>()], const Params& p, const CUtensorMap* mC,
                                             EpiGroup& eg, int r, int row0, int cx, volatile int* abort_flag)
 {
-    constexpr uint32_t box_bytes = OUT == OUT_F16 ? EPI_BUF_BYTES / 2 : EPI_BUF_BYTES;
+    constexpr int GW = group_cols<OUT>();
+    constexpr uint32_t box_bytes = EPI_BUF_BYTES;
     const bool beta_zero = p.beta_re == 0.f && p.beta_im == 0.f;
     const int b = eg.gi & 1;
     const uint32_t ph = (uint32_t)(eg.gi >> 1) & 1u;
@@ -498,17 +502,17 @@ __device__ __forceinline__ bool stage_group(const float (&v)[EPI_GROUP], const P
             if constexpr (OUT == OUT_C64) {
                 float2* const sb = (float2*)buf + r;
 #pragma unroll
-                for (int j = 0; j < EPI_GROUP / 2; ++j)
+                for (int j = 0; j < GW / 2; ++j)
                     sb[j * 128] = caxpby(p, beta_zero, v[2 * j], v[2 * j + 1], beta_zero ? make_float2(0.f, 0.f) : sb[j * 128]);
             } else {
                 using T = typename std::conditional<OUT == OUT_F16, __half, float>::type;
                 T* const sb = (T*)buf + r;
 #pragma unroll
-                for (int j = 0; j < EPI_GROUP; ++j)
+                for (int j = 0; j < GW; ++j)
                     sb[j * 128] = (T)axpby(p, beta_zero, v[j], beta_zero ? 0.f : (float)sb[j * 128]);
             }
         } else {
-            direct_group<OUT, EPI_GROUP>(v, p, row0 + r, cx);  // rows past the map (none past M)
+            direct_group<OUT, GW>(v, p, row0 + r, cx);  // rows past the map (none past M)
         }
     }
     fence_async_smem();
@@ -537,6 +541,8 @@ __device__ __forceinline__ void epilogue_single(const Params& p, const CUtensorM
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
     const int q = warp & 3, half = (warp - 2) / 4;
     const int r = q * 32 + lane;  // row within the CTA's 128
+    constexpr int GW = group_cols<OUT>();
+    static_assert(EPI_COLS % GW == 0, "epilogue columns");
     EpiGroup eg{epi_buf + half * 2 * EPI_BUF_BYTES, cbar + half * 2, 1 + half, q == 0 && lane == 0, 0};
     int acc = 0;
     uint32_t acc_ph = 0;
@@ -553,13 +559,16 @@ __device__ __forceinline__ void epilogue_single(const Params& p, const CUtensorM
         const uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN + half * EPI_COLS);
         bool stored = true;
 #pragma unroll 1
-        for (int g = 0; g < EPI_COLS / EPI_GROUP && stored; ++g) {
-            float v[EPI_GROUP];
-            tmem_ld16(taddr + (uint32_t)(g * EPI_GROUP), v);
-            if (p.c_tma)
-                stored = stage_group<OUT>(v, p, mC, eg, r, row0, col0 + g * EPI_GROUP, abort_flag);
+        for (int g = 0; g < EPI_COLS / GW && stored; ++g) {
+            float v[GW];
+            if constexpr (GW == 32)
+                tmem_ld32(taddr + (uint32_t)(g * GW), v);
             else
-                direct_group<OUT, EPI_GROUP>(v, p, row0 + r, col0 + g * EPI_GROUP);
+                tmem_ld16(taddr + (uint32_t)(g * GW), v);
+            if (p.c_tma)
+                stored = stage_group<OUT>(v, p, mC, eg, r, row0, col0 + g * GW, abort_flag);
+            else
+                direct_group<OUT, GW>(v, p, row0 + r, col0 + g * GW);
         }
         tc_fence_before();
         __syncwarp();
@@ -1264,7 +1273,7 @@ bool make_c_map(CUtensorMap* m, Params& p)
     p.m_tma = p.M - p.M % (16 / esize);
     if (p.m_tma == 0) return false;
     cuuint64_t dims[2] = {(cuuint64_t)p.m_tma, (cuuint64_t)p.N};
-    cuuint32_t box[2] = {128, (cuuint32_t)EPI_GROUP};
+    cuuint32_t box[2] = {128, (cuuint32_t)(p.out_half ? 32 : EPI_GROUP)};
     if (p.complex_out) {
         dims[0] = 2 * (cuuint64_t)p.m_tma;
         dims[1] = (cuuint64_t)(p.N / 2);
