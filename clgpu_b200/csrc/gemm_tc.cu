@@ -56,6 +56,7 @@
 #include <cuda_fp16.h>
 
 #include <algorithm>
+#include <map>
 #include <mutex>
 #include <type_traits>
 
@@ -1341,6 +1342,53 @@ cudaError_t run_split(iclblasHandle_t h, const T* S, int R, int K, long rs, long
 
 }  // namespace
 
+// Launch facts that are fixed per kernel and device, found once: the
+// dynamic shared-memory opt-in is set, and (CTA-pair kernels) the number of
+// clusters that fit at once is queried (0 for single-CTA kernels).
+struct KernelFacts {
+    cudaError_t status;
+    int max_clusters;
+};
+
+template <class K>
+KernelFacts kernel_facts(K kernel, int smem, bool pairs, iclblasHandle_t h)
+{
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, KernelFacts> known;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const std::pair<const void*, int> key((const void*)kernel, dev);
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = known.find(key);
+        if (it != known.end()) return it->second;
+    }
+    KernelFacts f{cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), 0};
+    if (f.status == cudaSuccess && pairs) {
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = 2;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.blockDim = dim3(THREADS);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = h->stream;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        cfg.gridDim = dim3(2 * std::max(1, h->sm_count / 2));
+        if (cudaOccupancyMaxActiveClusters(&f.max_clusters, kernel, &cfg) != cudaSuccess || f.max_clusters < 1) {
+            cudaGetLastError();
+            f.max_clusters = std::max(1, h->sm_count / 2);
+        }
+    }
+    if (f.status == cudaSuccess) {
+        std::lock_guard<std::mutex> lock(mu);
+        known[key] = f;
+    }
+    return f;
+}
+
 // Launches the persistent tcgen05 kernel over the operands (one per split
 // level): CTA pairs (256 x 256 tiles) when there are enough pair tiles to
 // fill the GPU; else single CTAs, with 128-wide tiles when 256-wide ones
@@ -1370,8 +1418,8 @@ cudaError_t launch_engine(iclblasHandle_t h, const ModeInfo& mi, const Operand* 
     if (!p.c_tma) mc = ma[0];  // unused by the kernel
     if (pairs) {
         auto run2 = [&](auto kernel) -> cudaError_t {
-            cudaError_t r = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-            if (r != cudaSuccess) return r;
+            const KernelFacts f = kernel_facts(kernel, smem, true, h);
+            if (f.status != cudaSuccess) return f.status;
             cudaLaunchConfig_t cfg = {};
             cudaLaunchAttribute attr[1];
             attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -1384,14 +1432,8 @@ cudaError_t launch_engine(iclblasHandle_t h, const ModeInfo& mi, const Operand* 
             cfg.attrs = attr;
             cfg.numAttrs = 1;
             // as many pairs as can be resident at once (persistent), at most one per tile
-            int max_clusters = 0;
-            cfg.gridDim = dim3(2 * std::max(1, h->sm_count / 2));
-            if (cudaOccupancyMaxActiveClusters(&max_clusters, kernel, &cfg) != cudaSuccess || max_clusters < 1) {
-                cudaGetLastError();
-                max_clusters = std::max(1, h->sm_count / 2);
-            }
-            cfg.gridDim = dim3(2 * std::min(pair_tiles, max_clusters));
-            r = cudaLaunchKernelEx(&cfg, kernel, ma[0], ma[1], ma[2], mb[0], mb[1], mb[2], mc, p);
+            cfg.gridDim = dim3(2 * std::min(pair_tiles, f.max_clusters));
+            const cudaError_t r = cudaLaunchKernelEx(&cfg, kernel, ma[0], ma[1], ma[2], mb[0], mb[1], mb[2], mc, p);
             if (r != cudaSuccess) return r;
             return cudaGetLastError();
         };
@@ -1405,8 +1447,8 @@ cudaError_t launch_engine(iclblasHandle_t h, const ModeInfo& mi, const Operand* 
     const int tiles = ceil_div(m, BM) * ceil_div((long)rows_b, bn);
     const int grid = std::min(tiles, h->sm_count);
     auto run = [&](auto kernel) -> cudaError_t {
-        cudaError_t r = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (r != cudaSuccess) return r;
+        const KernelFacts f = kernel_facts(kernel, smem, false, h);
+        if (f.status != cudaSuccess) return f.status;
         kernel<<<grid, THREADS, smem, h->stream>>>(ma[0], ma[1], ma[2], mb[0], mb[1], mb[2], mc, p);
         return cudaGetLastError();
     };
