@@ -1,9 +1,11 @@
-// Tensor-core GEMM for the TF32 / 3xBF16 / 6xBF16 math modes (sm_100a).
+// Tensor-core GEMM for the TF32 / 3xBF16 / 6xBF16 math modes and HGEMM
+// (sm_100a).
 //
-// C = alpha*op(A)*op(B) + beta*C in FP32 (and complex FP32) computed on the
-// 5th-generation tensor cores.  No reference counterpart: the reference's
-// GEMMs are FP32 SIMD kernels; this is the split-precision mode of the
-// north_star.
+// C = alpha*op(A)*op(B) + beta*C in FP32 (and complex FP32, or IEEE half for
+// HGEMM) computed on the 5th-generation tensor cores.  No reference
+// counterpart: the reference's GEMMs are FP32 SIMD kernels; these are the
+// library's split-precision math modes (FP32 accuracy from BF16 products)
+// and its half-precision GEMM.
 //
 // 1. Pre-pass (split kernel): each operand op(X) is rewritten K-major (row r
 //    holds its K values contiguously, zero-padded to a multiple of the
