@@ -395,6 +395,7 @@ __device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, const void*
 }
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_read1() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
@@ -491,16 +492,9 @@ __device__ __forceinline__ bool stage_group(const float (&v)[group_cols<OUT>()],
     const uint32_t ph = (uint32_t)(eg.gi >> 1) & 1u;
     uint8_t* buf = eg.buf + b * EPI_BUF_BYTES;
     const int x = OUT == OUT_C64 ? 2 * row0 : row0, y = OUT == OUT_C64 ? cx / 2 : cx;
-    if (eg.leader) {
-        bulk_wait_read1();
-        if (!beta_zero) {
-            mbar_expect_tx(&eg.bar[b], box_bytes);
-            tma_load_2d(buf, mC, x, y, &eg.bar[b]);
-        }
-    }
-    group_sync(eg.id);
-    const bool lok = beta_zero || mbar_wait(&eg.bar[b], ph, abort_flag);
-    if (lok) {
+    // this thread's row of the group into the buffer (C from the buffer for
+    // beta != 0), or straight to C for the rows past the map
+    auto fill = [&]() {
         if (row0 + r < p.m_tma) {
             if constexpr (OUT == OUT_C64) {
                 float2* const sb = (float2*)buf + r;
@@ -517,7 +511,31 @@ __device__ __forceinline__ bool stage_group(const float (&v)[group_cols<OUT>()],
         } else {
             direct_group<OUT, GW>(v, p, row0 + r, cx);  // rows past the map (none past M)
         }
+    };
+    if (beta_zero) {
+        // One barrier per group.  This group's buffer was last read by the
+        // store two groups back, which the leader saw finish reading before
+        // the previous group's barrier; before this group's barrier it waits
+        // for the previous group's store, whose buffer the next group fills.
+        fill();
+        fence_async_smem();
+        if (eg.leader) bulk_wait_read0();
+        group_sync(eg.id);
+        if (eg.leader) {
+            tma_store_2d(mC, buf, x, y);
+            bulk_commit();
+        }
+        ++eg.gi;
+        return true;
     }
+    if (eg.leader) {
+        bulk_wait_read1();
+        mbar_expect_tx(&eg.bar[b], box_bytes);
+        tma_load_2d(buf, mC, x, y, &eg.bar[b]);
+    }
+    group_sync(eg.id);
+    const bool lok = mbar_wait(&eg.bar[b], ph, abort_flag);
+    if (lok) fill();
     fence_async_smem();
     if (!group_all(eg.id, lok)) return false;
     if (eg.leader) {
