@@ -121,3 +121,24 @@ def test_hgemm_argument_rules(handle):
     assert B.iclblasHgemm(handle, 0, 0, 0, 2, 2, 1.0, None, 1, None, 1, 0.0, None, 1) == B.SUCCESS
     assert B.iclblasHgemm(handle, 0, 0, 2, 2, 2, 1.0, a, 0, a, 2, 0.0, a, 2) == B.INVALID_VALUE
     assert B.iclblasHgemm(handle, 5, 0, 2, 2, 2, 1.0, a, 2, a, 2, 0.0, a, 2) == B.INVALID_VALUE
+
+
+@pytest.mark.parametrize("ta,tb", [(0, 0), (1, 1)])
+def test_hgemm_device_pairs_beta_vs_fp64(handle, ta, tb):
+    """CTA-pair tiles (enough 256 x 256 tiles), operands read in place, C read
+    and written through TMA boxes (beta != 0), ragged m and n."""
+    import torch
+    m, n, k = 2560 + 40, 2048 + 24, 200
+    g = torch.Generator(device="cuda").manual_seed(11 + ta)
+    ar, ac = (k, m) if ta else (m, k)
+    br, bc = (n, k) if tb else (k, n)
+    A = (torch.rand(ac, ar, generator=g, device="cuda") * 2 - 1).half()   # column-major ar x ac
+    Bt = (torch.rand(bc, br, generator=g, device="cuda") * 2 - 1).half()  # column-major br x bc
+    C0 = (torch.rand(n, m, generator=g, device="cuda") * 2 - 1).half()   # column-major m x n
+    Cm = C0.clone()
+    assert B.iclblasHgemm(handle, ta, tb, m, n, k, 1.5, A, ar, Bt, br, 0.5, Cm, m) == B.SUCCESS
+    opA = A.double().t() if ta == 0 else A.double()      # m x k
+    opB = Bt.double().t() if tb == 0 else Bt.double()    # k x n
+    ref = 1.5 * (opA @ opB) + 0.5 * C0.double().t()      # m x n
+    err = float(torch.linalg.norm(Cm.double().t() - ref) / torch.linalg.norm(ref))
+    assert err <= 5e-4, err
