@@ -73,9 +73,13 @@ constexpr int ROW_BYTES = 128;                  // one K block per tile row
 constexpr int A_TILE = BM * ROW_BYTES;          // 16 KiB
 constexpr int RING_BYTES = 192 * 1024;          // the stage ring
 constexpr int EPI_GROUP = 16;                  // FP32 output columns per staged store (half: 32)
+// Output element type of a kernel instantiation: FP32, IEEE half (HGEMM),
+// or complex FP32 with the real GEMM's columns 2j, 2j+1 holding (re, im) of
+// column j.
+enum : int { OUT_F32 = 0, OUT_F16 = 1, OUT_C64 = 2 };
 // output columns per staged store: one 8 KiB buffer of 128 rows
 template <int OUT>
-constexpr int group_cols() { return OUT == 1 /*half*/ ? 32 : EPI_GROUP; }
+constexpr int group_cols() { return OUT == OUT_F16 ? 32 : EPI_GROUP; }
 constexpr int EPI_BUF_BYTES = 8192;             // one staging buffer: 128 rows x 16 FP32 columns
 constexpr int EPI_STAGE_BYTES = 4 * EPI_BUF_BYTES;  // two buffers for each half of the epilogue warps
 constexpr int MN_CHUNK_BYTES = 8192;            // MN-major operand: 64 rows x 64 K of 16-bit values
@@ -407,11 +411,6 @@ struct EpiGroup {
     bool leader;    // the thread that issues the copies
     int gi;         // groups staged so far: buffer gi & 1, barrier parity (gi >> 1) & 1
 };
-
-// Output element type of a kernel instantiation: FP32, IEEE half (HGEMM),
-// or complex FP32 with the real GEMM's columns 2j, 2j+1 holding (re, im) of
-// column j.
-enum : int { OUT_F32 = 0, OUT_F16 = 1, OUT_C64 = 2 };
 
 // alpha * v + beta * c with the rounding of the reference's real GEMM
 // epilogue (beta == 0: C is not read)
