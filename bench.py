@@ -15,12 +15,19 @@ no L2 flush is needed between steps.
   roofline  dominant kernel's algorithmic bytes / its mean event-timed
           duration, against the measured HBM copy bandwidth;
   cpu_baseline  the reference's own CPU code for the same routines
-          (oracle/_ref, built from the reference's sources) on a bounded
-          sample, 1 thread.
+          (oracle/_ref, built from the reference's sources) on the full
+          config, 1 thread, 2 steps.
+
+The same line carries the metric's first clause, timed in the same run with
+its own clock record: SGEMM 8192^3 and STRSM 8192x4096 in plain FP32 and the
+tensor-core split modes (3xBF16, 6xBF16, TF32; STRSM also 3xBF16 + one
+refinement step) with their errors against FP64 (`sgemm_8192`,
+`strsm_8192x4096`), and config 1, plain SGEMM 512^3, beside the reference's
+cpu_gemm on one and on all host cores (`sgemm_512_config`).
 
 `--impl reference` times the reference's CPU implementation with every host
-thread on a bounded sample of the same workload.  Multi-GPU (torchrun): each
-rank runs an independent replica (BLAS calls do not shard), weak scaling.
+thread on the full sweep config.  Multi-GPU (torchrun): each rank runs an
+independent replica (BLAS calls do not shard), weak scaling.
 """
 from __future__ import annotations
 
@@ -356,6 +363,212 @@ def run_ours(args, rank, world, torch):
         "clocks": clocks,
     }
     return out
+
+
+# ---------------------------------------------------------------- precision legs of the default run
+def fp32_fma_peak_tflops(torch, dev):
+    """Nominal FP32 FMA peak of the GPU: SMs x 128 lanes x 2 flops x max SM clock."""
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    mhz = 1965.0
+    pp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pp):
+        mhz = float(json.load(open(pp)).get("sm_max_mhz", mhz))
+    return sms * 128 * 2 * mhz * 1e6 / 1e12
+
+
+def run_precision_legs(torch, dev, B, n_gemm=8192, trsm_m=8192, trsm_n=4096):
+    """The metric's first clause, timed in the default run: SGEMM 8192^3 NN
+    (U(-1,1), seed 2) in plain FP32 (CUDA cores), TF32, 3xBF16 and 6xBF16;
+    STRSM 8192 x 4096 left/lower/N/non-unit (diagonal U(1,2), strictly lower
+    N(0,1)/sqrt(M), B U(-1,1), seed 3) in plain FP32, TF32, 3xBF16, 6xBF16
+    and 3xBF16 + one refinement step; and config 1 itself, plain SGEMM NN
+    512^3 alpha 1.5 beta 0.5 (seed 0), beside the reference's cpu_gemm on 1
+    and on all host cores.  Device operands, CUDA events on the launching
+    stream, median of 5 calls after one untimed call; errors are relative
+    Frobenius against FP64 (torch float64 on the GPU, plumbing only); TFLOP/s
+    count the algorithmic 2MNK (GEMM) and M^2 N (TRSM) flops only."""
+    stream = torch.cuda.Stream(device=dev)
+    peaks = {}
+    pp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pp):
+        peaks = json.load(open(pp))
+    bf16_sus = peaks.get("bf16_tflops_sustained")
+    fp32_peak = fp32_fma_peak_tflops(torch, dev)
+    nprod = {B.MATH_TF32: 1, B.MATH_BF16X3: 3, B.MATH_BF16X6: 6}
+    out = {}
+
+    def med(fn, reps=5):
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            ts.append((e0, e1))
+        torch.cuda.synchronize()
+        return float(np.median([a.elapsed_time(b) for a, b in ts]))
+
+    def roof(mode, flops, ms):
+        tf = flops / (ms / 1e3) / 1e12
+        if mode == B.MATH_PLAIN_FP32:
+            return {"bound": "fp32_fma", "peak": round(fp32_peak, 1), "peak_source": "nominal (SMs x 128 x 2 x max clock)",
+                    "frac": round(tf / fp32_peak, 3)}
+        if not bf16_sus:
+            return None
+        ex = nprod[mode] * tf
+        # TF32 runs at half the BF16 rate per product
+        eff = ex * (2.0 if mode == B.MATH_TF32 else 1.0)
+        return {"bound": "tensor", "executed_tflops": round(ex, 1), "peak": bf16_sus,
+                "peak_source": "measured sustained bf16 (TF32 products counted at twice their cost)",
+                "frac": round(eff / bf16_sus, 3)}
+
+    names = {B.MATH_PLAIN_FP32: "fp32", B.MATH_TF32: "tf32", B.MATH_BF16X3: "3xbf16", B.MATH_BF16X6: "6xbf16"}
+    with B.Handle() as h, torch.cuda.stream(stream), Clocks(dev.index) as clk:
+        h.set_stream(stream)
+        t_wait = time.time()
+        while not clk.started() and time.time() - t_wait < 5.0:
+            time.sleep(0.05)
+        clk.mark_start()
+        # ---- SGEMM n^3 NN
+        n = n_gemm
+        g = torch.Generator(device=dev).manual_seed(2)
+        A = torch.rand(n * n, generator=g, device=dev) * 2 - 1
+        Bm = torch.rand(n * n, generator=g, device=dev) * 2 - 1
+        C = torch.empty(n * n, device=dev)
+        ref = A.view(n, n).t().double() @ Bm.view(n, n).t().double()
+        refn = torch.linalg.norm(ref).item()
+        fl = 2.0 * n * n * n
+        res = {}
+        for mode in (B.MATH_PLAIN_FP32, B.MATH_TF32, B.MATH_BF16X3, B.MATH_BF16X6):
+            h.set_math_mode(mode)
+            ms = med(lambda: B.check(B.iclblasSgemm(h, 0, 0, n, n, n, 1.0, A, n, Bm, n, 0.0, C, n), "sgemm"))
+            err = torch.linalg.norm(C.view(n, n).t().double() - ref).item() / refn
+            res[names[mode]] = {"tflops": round(fl / (ms / 1e3) / 1e12, 2), "ms": round(ms, 3),
+                                "rel_err_vs_fp64": float("%.3g" % err), "roofline": roof(mode, fl, ms)}
+        base = res["fp32"]["tflops"]
+        for k in res:
+            res[k]["x_plain_fp32"] = round(res[k]["tflops"] / base, 2)
+        out["sgemm_8192"] = {"config": f"SGEMM NN {n}^3 fp32, U(-1,1) seed 2, alpha 1 beta 0", **res}
+        del A, Bm, C, ref
+        torch.cuda.empty_cache()
+
+        # ---- STRSM M x N left / lower / N / non-unit
+        m, nr = trsm_m, trsm_n
+        g = torch.Generator(device=dev).manual_seed(3)
+        L = torch.tril(torch.randn(m, m, generator=g, device=dev) / m ** 0.5, -1)
+        L = L + torch.diag(torch.rand(m, generator=g, device=dev) + 1.0)
+        Acm = L.t().contiguous().reshape(-1)
+        B0 = (torch.rand(nr, m, generator=g, device=dev) * 2 - 1).reshape(-1)
+        X64 = torch.linalg.solve_triangular(L.double(), B0.view(nr, m).t().double(), upper=False)
+        x64n = torch.linalg.norm(X64).item()
+        del L
+        Bw = torch.empty_like(B0)
+        Bt = torch.empty_like(B0)
+        fl = float(m) * m * nr
+        ms_copy = med(lambda: Bt.copy_(B0))
+        res = {}
+        for mode, steps in ((B.MATH_PLAIN_FP32, 0), (B.MATH_TF32, 0), (B.MATH_BF16X3, 0), (B.MATH_BF16X6, 0),
+                            (B.MATH_BF16X3, 1)):
+            h.set_math_mode(mode)
+            h.set_trsm_refinement(steps)
+
+            def run():
+                Bw.copy_(B0)
+                B.check(B.iclblasStrsm(h, 0, 1, 0, 0, m, nr, 1.0, Acm, m, Bw, m), "strsm")
+            ms = max(med(run) - ms_copy, 1e-6)
+            err = torch.linalg.norm(Bw.view(nr, m).t().double() - X64).item() / x64n
+            key = names[mode] + (f"+refine{steps}" if steps else "")
+            r = {"tflops": round(fl / (ms / 1e3) / 1e12, 2), "ms": round(ms, 3),
+                 "rel_err_vs_fp64": float("%.3g" % err)}
+            if steps == 0:
+                r["roofline"] = roof(mode, fl, ms)
+            res[key] = r
+        h.set_trsm_refinement(0)
+        h.set_math_mode(B.MATH_PLAIN_FP32)
+        base = res["fp32"]["tflops"]
+        for k in res:
+            res[k]["x_plain_fp32"] = round(res[k]["tflops"] / base, 2)
+        out["strsm_8192x4096"] = {"config": f"STRSM left/lower/N/non-unit M={m} NRHS={nr} fp32, seed 3", **res}
+        del Acm, B0, X64, Bw, Bt
+        torch.cuda.empty_cache()
+
+        # ---- config 1: plain SGEMM 512^3, alpha 1.5, beta 0.5
+        n = 512
+        rng = np.random.default_rng(0)
+        Ah = rng.uniform(-1, 1, n * n).astype(np.float32)
+        Bh = rng.uniform(-1, 1, n * n).astype(np.float32)
+        Ch = rng.uniform(-1, 1, n * n).astype(np.float32)
+        Ad, Bd, C0 = (torch.from_numpy(v).to(dev) for v in (Ah, Bh, Ch))
+        Cd = C0.clone()
+        fl = 2.0 * n ** 3
+        ms = med(lambda: B.check(B.iclblasSgemm(h, 0, 0, n, n, n, 1.5, Ad, n, Bd, n, 0.5, Cd, n), "sgemm"), reps=50)
+        Cd.copy_(C0)
+        B.check(B.iclblasSgemm(h, 0, 0, n, n, n, 1.5, Ad, n, Bd, n, 0.5, Cd, n), "sgemm")
+        torch.cuda.synchronize()
+        got = Cd.cpu().numpy()
+        # host operands through the C ABI (copies in and out inside the call)
+        Cw = Ch.copy()
+        t0 = time.perf_counter()
+        for _ in range(20):
+            Cw[:] = Ch
+            B.check(B.iclblasSgemm(h, 0, 0, n, n, n, 1.5, Ah, n, Bh, n, 0.5, Cw, n), "sgemm host")
+        host_ms = (time.perf_counter() - t0) / 20 * 1e3
+        clk.mark_end()
+    out["precision_clocks"] = clk.summary()
+
+    # CPU: the reference's cpu_gemm (double accumulation), 1 core and all cores
+    cpu = cpu_sgemm_512(Ah, Bh, Ch, n)
+    err = float(np.linalg.norm(got.astype(np.float64) - cpu["C"]) / np.linalg.norm(cpu["C"]))
+    out["sgemm_512_config"] = {
+        "config": "SGEMM NN 512^3 fp32, lda=ldb=ldc=512, alpha 1.5, beta 0.5, U(-1,1) seed 0",
+        "gpu_tflops": round(fl / (ms / 1e3) / 1e12, 2), "gpu_us": round(ms * 1e3, 1),
+        "gpu_host_operands_us": round(host_ms * 1e3, 1),
+        "rel_err_vs_cpu_gemm": float("%.3g" % err),
+        "cpu_gemm_1core_ms": round(cpu["t1"] * 1e3, 2), "cpu_gemm_ncore_ms": round(cpu["tn"] * 1e3, 2),
+        "cpu_cores": cpu["cores"], "cpu_kind": cpu["kind"],
+        "cpu_gemm_1core_gflops": round(fl / cpu["t1"] / 1e9, 2), "cpu_gemm_ncore_gflops": round(fl / cpu["tn"] / 1e9, 2),
+    }
+    return out
+
+
+def cpu_sgemm_512(Ah, Bh, Ch, n):
+    """The reference's cpu_gemm template (double accumulation, compiled in
+    oracle/_ref; the oracle's double GEMM if the reference was not built)
+    on config 1, on one core and split by column blocks over every host core."""
+    import ctypes as C
+    import oracle_lib as O
+    R = O.ref()
+    kind = "reference" if R is not None else "port"
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+
+    def run(c0, c1, Cout):
+        if c1 <= c0:
+            return
+        if R is not None:
+            R.ref_cpu_sgemm(0, 0, n, c1 - c0, n, 1.5, Ah.ctypes.data, n, Bh.ctypes.data + 4 * c0 * n, n, 0.5,
+                            Cout.ctypes.data + 4 * c0 * n, n)
+        else:
+            A64, B64 = Ah.astype(np.float64), Bh[c0 * n:c1 * n].astype(np.float64)
+            C64 = Ch[c0 * n:c1 * n].astype(np.float64)
+            O.dgemm(0, 0, n, c1 - c0, n, 1.5, A64, n, B64, n, 0.5, C64, n)
+            Cout[c0 * n:c1 * n] = C64
+    out1 = Ch.copy()
+    t0 = time.perf_counter()
+    run(0, n, out1)
+    t1 = time.perf_counter() - t0
+    outn = Ch.copy()
+    b = np.linspace(0, n, cores + 1).astype(int)
+    ts = [threading.Thread(target=run, args=(int(b[i]), int(b[i + 1]), outn)) for i in range(cores)]
+    t0 = time.perf_counter()
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    tn = time.perf_counter() - t0
+    return {"C": out1.astype(np.float64), "t1": t1, "tn": tn, "cores": cores, "kind": kind}
 
 
 # ---------------------------------------------------------------- GEMM precision study
@@ -967,42 +1180,69 @@ def run_batched_study(args, torch):
 
 
 # ---------------------------------------------------------------- CPU (reference code)
-SAMPLE_N1 = 1 << 24
-SAMPLE_GN = 4096
-SAMPLE_CN = 2048
+class CpuSweep:
+    """The sweep on the host cores through the reference's own CPU code
+    (oracle/_ref/libiclref.so: its double-accumulating templates and serial
+    kernels; the oracle port if the reference was not built), on operands of
+    the given sizes (default: the full config, n = 2^28, SGEMV 16384^2,
+    CGEMV 8192^2).  With threads > 1 every routine is split into
+    independent chunks run concurrently (ctypes releases the GIL); the
+    chunked reductions' partial results are not combined (timing only)."""
 
+    def __init__(self, threads: int, n=N1, gn=GEMV_N, cn=CGEMV_N):
+        import ctypes as C
+        import oracle_lib as O
+        R = O.ref()
+        self.kind = "reference" if R is not None else "port"
+        self.threads = threads
+        self.sizes = (n, gn, cn)
+        rng = np.random.default_rng(1)
+        x = rng.random(n, dtype=np.float32) * 2 - 1
+        y = rng.random(n, dtype=np.float32) * 2 - 1
+        A = rng.random(gn * gn, dtype=np.float32) * 2 - 1
+        gx = rng.random(gn, dtype=np.float32) * 2 - 1
+        gy = rng.random(gn, dtype=np.float32) * 2 - 1
+        CA = (rng.random(2 * cn * cn, dtype=np.float32) * 2 - 1).view(np.complex64)
+        cx = (rng.random(2 * cn, dtype=np.float32) * 2 - 1).view(np.complex64)
+        cy = (rng.random(2 * cn, dtype=np.float32) * 2 - 1).view(np.complex64)
+        self._keep = (x, y, A, gx, gy, CA, cx, cy)
+        al = O.cbox(1 + 1j)
+        be = O.cbox(0.5)
+        self._keep2 = (al, be)
+        P = lambda a, off=0: C.c_void_p(a.ctypes.data + off * a.itemsize)  # noqa: E731
+        if R is not None:
+            self.ops = [
+                ("saxpy", lambda o, c: R.ref_cpu_saxpy(c, 0.5, P(x, o), 1, P(y, o), 1), n),
+                ("sdot", lambda o, c: R.ref_cpu_sdot(c, P(x, o), 1, P(y, o), 1), n),
+                ("snrm2", lambda o, c: R.ref_cpu_snrm2(c, P(x, o), 1), n),
+                ("sasum", lambda o, c: R.ref_cpu_sasum(c, P(x, o), 1), n),
+                ("isamax", lambda o, c: R.ref_cpu_isamax(c, P(x, o), 1), n),
+                # rows of y for op N, columns (outputs) for op T
+                ("sgemv_n", lambda o, c: R.ref_naive_sgemv(0, c, gn, 1.0, P(A, o), gn, P(gx), 1, 0.5, P(gy, o), 1), gn),
+                ("sgemv_t", lambda o, c: R.ref_naive_sgemv(1, gn, c, 1.0, P(A, o * gn), gn, P(gx), 1, 0.5, P(gy, o), 1), gn),
+                ("cgemv_n", lambda o, c: R.ref_naive_cgemv(0, c, cn, P(al), P(CA, o), cn, P(cx), 1, P(be), P(cy, o), 1), cn),
+                ("cgemv_c", lambda o, c: R.ref_naive_cgemv(2, cn, c, P(al), P(CA, o * cn), cn, P(cx), 1, P(be), P(cy, o), 1), cn),
+            ]
+        else:
+            Lo = O.orc()
+            c32a, c32b = O.c32(1 + 1j), O.c32(0.5)
+            self.ops = [
+                ("saxpy", lambda o, c: Lo.orc_saxpy(c, 0.5, P(x, o), 1, P(y, o), 1), n),
+                ("sdot", lambda o, c: Lo.orc_sdot(c, P(x, o), 1, P(y, o), 1), n),
+                ("snrm2", lambda o, c: Lo.orc_snrm2(c, P(x, o), 1), n),
+                ("sasum", lambda o, c: Lo.orc_sasum(c, P(x, o), 1), n),
+                ("isamax", lambda o, c: Lo.orc_isamax(c, P(x, o), 1), n),
+                ("sgemv_n", lambda o, c: Lo.orc_sgemv(0, c, gn, 1.0, P(A, o), gn, P(gx), 1, 0.5, P(gy, o), 1), gn),
+                ("sgemv_t", lambda o, c: Lo.orc_sgemv(1, gn, c, 1.0, P(A, o * gn), gn, P(gx), 1, 0.5, P(gy, o), 1), gn),
+                ("cgemv_n", lambda o, c: Lo.orc_cgemv(0, c, cn, c32a, P(CA, o), cn, P(cx), 1, c32b, P(cy, o), 1), cn),
+                ("cgemv_c", lambda o, c: Lo.orc_cgemv(2, cn, c, c32a, P(CA, o * cn), cn, P(cx), 1, c32b, P(cy, o), 1), cn),
+            ]
+        self.total_bytes = sum(sweep_bytes(n, gn, cn).values())
 
-def cpu_sweep(threads: int, reps: int = 3):
-    """Times the reference's own CPU code (oracle/_ref/libiclref.so; the
-    oracle port if the reference was not built) on a bounded sample of the
-    sweep: level-1 at n = 2^24, SGEMV 4096^2, CGEMV 2048^2.  With threads > 1
-    every routine is split into independent chunks run concurrently (ctypes
-    releases the GIL)."""
-    import ctypes as C
-    import oracle_lib as O
-    R = O.ref()
-    kind = "reference" if R is not None else "port"
-    rng = np.random.default_rng(1)
-    n, gn, cn = SAMPLE_N1, SAMPLE_GN, SAMPLE_CN
-    x = rng.uniform(-1, 1, n).astype(np.float32)
-    y = rng.uniform(-1, 1, n).astype(np.float32)
-    A = rng.uniform(-1, 1, gn * gn).astype(np.float32)
-    gx = rng.uniform(-1, 1, gn).astype(np.float32)
-    gy = rng.uniform(-1, 1, gn).astype(np.float32)
-    CA = O.colmajor(cn, cn, cn, rng, np.complex64)
-    cx = O.colmajor(cn, 1, cn, rng, np.complex64)
-    cy = O.colmajor(cn, 1, cn, rng, np.complex64)
-    al = O.cbox(1 + 1j)
-    be = O.cbox(0.5)
-    P = lambda a, off=0: C.c_void_p(a.ctypes.data + off * a.itemsize)  # noqa: E731
-
-    def chunks(total, parts):
-        b = np.linspace(0, total, parts + 1).astype(int)
-        return [(int(b[i]), int(b[i + 1] - b[i])) for i in range(parts) if b[i + 1] > b[i]]
-
-    def par(fn, total):
-        cs = chunks(total, threads)
-        if threads == 1:
+    def _par(self, fn, total):
+        b = np.linspace(0, total, self.threads + 1).astype(int)
+        cs = [(int(b[i]), int(b[i + 1] - b[i])) for i in range(self.threads) if b[i + 1] > b[i]]
+        if self.threads == 1:
             for o, c in cs:
                 fn(o, c)
             return
@@ -1012,47 +1252,33 @@ def cpu_sweep(threads: int, reps: int = 3):
         for t in ts:
             t.join()
 
-    if R is not None:
-        ops = [
-            ("saxpy", lambda o, c: R.ref_cpu_saxpy(c, 0.5, P(x, o), 1, P(y, o), 1), n),
-            ("sdot", lambda o, c: R.ref_cpu_sdot(c, P(x, o), 1, P(y, o), 1), n),
-            ("snrm2", lambda o, c: R.ref_cpu_snrm2(c, P(x, o), 1), n),
-            ("sasum", lambda o, c: R.ref_cpu_sasum(c, P(x, o), 1), n),
-            ("isamax", lambda o, c: R.ref_cpu_isamax(c, P(x, o), 1), n),
-            # rows of y for op N, columns (outputs) for op T
-            ("sgemv_n", lambda o, c: R.ref_naive_sgemv(0, c, gn, 1.0, P(A, o), gn, P(gx), 1, 0.5, P(gy, o), 1), gn),
-            ("sgemv_t", lambda o, c: R.ref_naive_sgemv(1, gn, c, 1.0, P(A, o * gn), gn, P(gx), 1, 0.5, P(gy, o), 1), gn),
-            ("cgemv_n", lambda o, c: R.ref_naive_cgemv(0, c, cn, P(al), P(CA, o), cn, P(cx), 1, P(be), P(cy, o), 1), cn),
-            ("cgemv_c", lambda o, c: R.ref_naive_cgemv(2, cn, c, P(al), P(CA, o * cn), cn, P(cx), 1, P(be), P(cy, o), 1), cn),
-        ]
-    else:
-        Lo = O.orc()
-        c32a, c32b = O.c32(1 + 1j), O.c32(0.5)
-        ops = [
-            ("saxpy", lambda o, c: Lo.orc_saxpy(c, 0.5, P(x, o), 1, P(y, o), 1), n),
-            ("sdot", lambda o, c: Lo.orc_sdot(c, P(x, o), 1, P(y, o), 1), n),
-            ("snrm2", lambda o, c: Lo.orc_snrm2(c, P(x, o), 1), n),
-            ("sasum", lambda o, c: Lo.orc_sasum(c, P(x, o), 1), n),
-            ("isamax", lambda o, c: Lo.orc_isamax(c, P(x, o), 1), n),
-            ("sgemv_n", lambda o, c: Lo.orc_sgemv(0, c, gn, 1.0, P(A, o), gn, P(gx), 1, 0.5, P(gy, o), 1), gn),
-            ("sgemv_t", lambda o, c: Lo.orc_sgemv(1, gn, c, 1.0, P(A, o * gn), gn, P(gx), 1, 0.5, P(gy, o), 1), gn),
-            ("cgemv_n", lambda o, c: Lo.orc_cgemv(0, c, cn, c32a, P(CA, o), cn, P(cx), 1, c32b, P(cy, o), 1), cn),
-            ("cgemv_c", lambda o, c: Lo.orc_cgemv(2, cn, c, c32a, P(CA, o * cn), cn, P(cx), 1, c32b, P(cy, o), 1), cn),
-        ]
-    bytes_per = sweep_bytes(n, gn, cn)
-    total_bytes = sum(bytes_per.values())
-    times = []
-    for _ in range(reps):
+    def step(self) -> float:
+        """One pass of the sweep; returns its wall time in seconds."""
         t0 = time.perf_counter()
-        for name, fn, total in ops:
-            par(fn, total)
-        times.append(time.perf_counter() - t0)
-    t = float(np.median(times))
+        for _, fn, total in self.ops:
+            self._par(fn, total)
+        return time.perf_counter() - t0
+
+    def describe(self, reps: int) -> str:
+        n, gn, cn = self.sizes
+        what = ("reference CPU templates + serial kernels (oracle/_ref)" if self.kind == "reference"
+                else "oracle port")
+        size = ("the full config" if self.sizes == (N1, GEMV_N, CGEMV_N) else
+                f"level-1 n={n}, SGEMV {gn}^2 N+T, CGEMV {cn}^2 N+C")
+        return f"{size} (level-1 n={n}, SGEMV {gn}^2 N+T, CGEMV {cn}^2 N+C); {reps} timed step(s); {what}"
+
+
+def cpu_sweep(threads: int, reps: int = 3, warmup: int = 0, sizes=(N1, GEMV_N, CGEMV_N)):
+    """Times the sweep on the host cores (CpuSweep): `warmup` untimed steps,
+    then `reps` timed ones; value = algorithmic bytes / mean step time."""
+    cs = CpuSweep(threads, *sizes)
+    for _ in range(warmup):
+        cs.step()
+    times = [cs.step() for _ in range(reps)]
+    t = float(np.mean(times))
     return {
-        "value": round(total_bytes / t / 1e9, 3), "unit": "GB/s", "cores": threads, "kind": kind,
-        "sample": f"sweep at level-1 n=2^24, SGEMV {gn}^2 N+T, CGEMV {cn}^2 N+C; median of {reps}; "
-                  f"{'reference CPU templates + serial kernels (oracle/_ref)' if kind == 'reference' else 'oracle port'}",
-        "seconds_per_step": round(t, 3),
+        "value": round(cs.total_bytes / t / 1e9, 3), "unit": "GB/s", "cores": threads, "kind": cs.kind,
+        "sample": cs.describe(reps), "seconds_per_step": round(t, 3),
     }
 
 
@@ -1064,6 +1290,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-operand (C ABI) leg")
+    ap.add_argument("--no-precision", action="store_true",
+                    help="skip the SGEMM 8192^3 / STRSM 8192x4096 / SGEMM 512^3 legs of the default run")
     ap.add_argument("--only", default="", help="comma-separated subset of the sweep's calls")
     ap.add_argument("--n1", type=int, default=N1, help="level-1 vector length (default 2^28)")
     ap.add_argument("--workload", default="sweep", choices=["sweep", "gemm", "trsm", "batched", "level1x", "level23x", "conv1x1"],
@@ -1087,10 +1315,8 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        threads = os.cpu_count() or 1
-        for _ in range(max(0, min(args.warmup, 1))):
-            cpu_sweep(threads, reps=1)
-        res = cpu_sweep(threads, reps=max(1, args.steps))
+        threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+        res = cpu_sweep(threads, reps=max(1, args.steps), warmup=args.warmup)
         line = {
             "metric": "level-1/2 sweep aggregate HBM bandwidth (SAXPY/SDOT/SNRM2/SASUM/ISAMAX n=2^28, "
                       "SGEMV 16384^2 N+T, CGEMV 8192^2 N+C)",
@@ -1129,8 +1355,11 @@ def main():
     if world > 1:
         torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     out = run_ours(args, rank, world, torch)
+    if world == 1 and not args.only and not args.no_precision:
+        from clgpu_b200 import iclblas as B
+        out.update(run_precision_legs(torch, torch.device("cuda", 0), B))
     if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.only:
-        out["cpu_baseline"] = {k: v for k, v in cpu_sweep(1, reps=3).items() if k != "seconds_per_step"}
+        out["cpu_baseline"] = {k: v for k, v in cpu_sweep(1, reps=2).items() if k != "seconds_per_step"}
     if rank == 0:
         print(json.dumps(out))
     if world > 1:

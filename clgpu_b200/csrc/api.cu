@@ -16,6 +16,7 @@
 #include <stdexcept>
 
 #include "internal.h"
+#include "memkind.h"
 
 using iclb::cfloat;
 
@@ -25,6 +26,7 @@ iclblasStatus_t map_cuda(cudaError_t e)
 {
     if (e == cudaSuccess) return ICLBLAS_STATUS_SUCCESS;
     if (e == cudaErrorMemoryAllocation) return ICLBLAS_STATUS_ALLOC_FAILED;
+    if (e == cudaErrorInvalidDevicePointer) return ICLBLAS_STATUS_INVALID_VALUE;   // another GPU's memory
     if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return ICLBLAS_STATUS_NOT_INITIALIZED;
     if (e == cudaErrorNoKernelImageForDevice || e == cudaErrorInvalidDeviceFunction) return ICLBLAS_STATUS_ARCH_MISMATCH;
     return ICLBLAS_STATUS_EXECUTION_FAILED;
@@ -73,17 +75,21 @@ int validate(const Params& p, iclblasHandle_t h)
         if (v_ > 0) return (iclblasStatus_t)v_;                                 \
     } while (0)
 
-// Can the device dereference `p` directly?
-bool is_device_ptr(const void* p)
+// Where `p` lives, seen from `device` (memkind.h).
+iclb::MemKind mem_kind(const void* p, int device)
 {
     cudaPointerAttributes a;
     cudaError_t e = cudaPointerGetAttributes(&a, p);
     if (e != cudaSuccess) {
         cudaGetLastError();
-        return false;
+        return iclb::MemKind::Host;
     }
-    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+    return iclb::classify_memory((int)a.type, a.device, device);
 }
+
+// Can the handle's GPU dereference `p` directly?  Device memory of another
+// GPU is not: without peer access a kernel reading it faults.
+bool is_device_ptr(iclblasHandle_t h, const void* p) { return mem_kind(p, h->device) == iclb::MemKind::Device; }
 
 size_t vec_extent(int n, int inc) { return n > 0 ? (size_t)(n - 1) * (size_t)inc + 1 : 0; }
 size_t mat_extent(int rows, int cols, int ld)
@@ -108,10 +114,16 @@ public:
         o.bytes = bytes;
         o.out = out;
         o.in = in;
-        o.staged = !is_device_ptr(p);
+        const iclb::MemKind k = mem_kind(p, h_->device);
+        foreign_ |= k == iclb::MemKind::OtherDevice;
+        o.staged = k == iclb::MemKind::Host;
         o.dev = o.staged ? nullptr : o.user;
         return n_++;
     }
+
+    // An operand in another GPU's memory ends the call with INVALID_VALUE
+    // before any copy or launch (map_cuda maps this error to it).
+    cudaError_t rejected() const { return foreign_ ? cudaErrorInvalidDevicePointer : cudaSuccess; }
 
     // Device addresses for the staged operands (grows the staging buffer).
     cudaError_t reserve()
@@ -141,6 +153,7 @@ public:
 
     cudaError_t stage_in()
     {
+        if (foreign_) return rejected();
         cudaError_t e = reserve();
         if (e != cudaSuccess) return e;
         for (int i = 0; i < n_; ++i) {
@@ -169,6 +182,7 @@ public:
     cudaError_t run_chunked(long n, const int* incs, size_t esize, F&& launch, bool& used)
     {
         used = false;
+        if (foreign_) return rejected();
         bool any = false;
         size_t total = 0;
         for (int i = 0; i < n_; ++i) {
@@ -243,6 +257,7 @@ private:
     Op ops_[6];
     int n_ = 0;
     bool any_staged_ = false;
+    bool foreign_ = false;
 };
 
 // Reads a device status word after a blocking call (kernels with bounded
@@ -266,9 +281,18 @@ iclblasStatus_t check_device_status(iclblasHandle_t h)
 void zero_result(iclblasHandle_t h, void* result, size_t bytes)
 {
     if (!result) return;
-    if (is_device_ptr(result)) {
+    int dev = 0;
+    if (handle_ok(h)) dev = h->device;
+    else cudaGetDevice(&dev);
+    const iclb::MemKind k = mem_kind(result, dev);
+    if (k == iclb::MemKind::Device) {
         if (handle_ok(h)) cudaMemsetAsync(result, 0, bytes, h->stream);
         else cudaMemset(result, 0, bytes);
+    } else if (k == iclb::MemKind::OtherDevice) {
+        // a copy (not a kernel) reaches another GPU's memory through unified addressing
+        const long long zero[2] = {0, 0};
+        cudaMemcpy(result, zero, bytes, cudaMemcpyDefault);
+        cudaGetLastError();
     } else {
         std::memset(result, 0, bytes);
     }
@@ -599,7 +623,7 @@ extern "C" iclblasStatus_t iclblasSdotNoAlloc(iclblasHandle_t h, int n, const fl
         p.n = n; p.x = x; p.incx = incx; p.y = y; p.incy = incy;
         VALIDATE(p, h);
         if (!result) return ICLBLAS_STATUS_INVALID_VALUE;
-        if (!is_device_ptr(x) || !is_device_ptr(y) || !is_device_ptr(result)) return ICLBLAS_STATUS_INVALID_VALUE;
+        if (!is_device_ptr(h, x) || !is_device_ptr(h, y) || !is_device_ptr(h, result)) return ICLBLAS_STATUS_INVALID_VALUE;
         cudaError_t e = iclb::sdot_noalloc(h, n, x, incx, y, incy, result);
         if (e == cudaErrorNotSupported) return ICLBLAS_STATUS_NOT_SUPPORTED;
         return map_cuda(e);
@@ -662,7 +686,12 @@ extern "C" iclblasStatus_t iclblasSrotm(iclblasHandle_t h, int n, float* x, int 
     // Host parameters are read here (the reference's early return for the
     // identity flag -2, iclBLAS_S.cpp:194-195); device parameters are read
     // by the kernel, which skips every flag outside {-1, 0, 1}.
-    const bool dev_param = is_device_ptr(param);
+    int dev = 0;
+    if (handle_ok(h)) dev = h->device;
+    else cudaGetDevice(&dev);
+    const iclb::MemKind pk = mem_kind(param, dev);
+    if (pk == iclb::MemKind::OtherDevice) return ICLBLAS_STATUS_INVALID_VALUE;
+    const bool dev_param = pk == iclb::MemKind::Device;
     if (!dev_param && param[0] == -2.f) return ICLBLAS_STATUS_SUCCESS;
     return pair_call<float>(h, n, x, incx, true, y, incy, true, [&](int nn, float* dx, float* dy) {
         return iclb::srotm(h, nn, dx, incx, dy, incy, dev_param ? nullptr : param, dev_param ? param : nullptr);
@@ -1457,7 +1486,7 @@ bool plan_ok(iclblasBatchPlan_t p, int kind) { return p != nullptr && p->tag == 
 bool op_ok(int t) { return t >= ICLBLAS_OP_N && t <= ICLBLAS_OP_C; }
 
 // Arrays of per-instance pointers must be device memory (the kernels read them).
-bool ptr_array_ok(const void* p) { return p != nullptr && is_device_ptr(p); }
+bool ptr_array_ok(iclblasHandle_t h, const void* p) { return p != nullptr && is_device_ptr(h, p); }
 
 }  // namespace
 
@@ -1531,7 +1560,7 @@ extern "C" iclblasStatus_t iclblasStrsmBatchedUneven(iclblasHandle_t h, iclblasB
     return guarded([&]() -> iclblasStatus_t {
         if (!handle_ok(h) || !plan_ok(plan, 0) || !alpha) return ICLBLAS_STATUS_INVALID_VALUE;
         if (plan->batch == 0) return ICLBLAS_STATUS_SUCCESS;
-        if (plan->device != h->device || !ptr_array_ok(A) || !ptr_array_ok(B)) return ICLBLAS_STATUS_INVALID_VALUE;
+        if (plan->device != h->device || !ptr_array_ok(h, A) || !ptr_array_ok(h, B)) return ICLBLAS_STATUS_INVALID_VALUE;
         return map_cuda(iclb::batch_trsm(h, plan, *alpha, A, B));
     });
 }
@@ -1543,7 +1572,7 @@ extern "C" iclblasStatus_t iclblasSgemmBatchedUneven(iclblasHandle_t h, iclblasB
     return guarded([&]() -> iclblasStatus_t {
         if (!handle_ok(h) || !plan_ok(plan, 1) || !alpha || !beta) return ICLBLAS_STATUS_INVALID_VALUE;
         if (plan->batch == 0) return ICLBLAS_STATUS_SUCCESS;
-        if (plan->device != h->device || !ptr_array_ok(A) || !ptr_array_ok(B) || !ptr_array_ok(C))
+        if (plan->device != h->device || !ptr_array_ok(h, A) || !ptr_array_ok(h, B) || !ptr_array_ok(h, C))
             return ICLBLAS_STATUS_INVALID_VALUE;
         return map_cuda(iclb::batch_gemm(h, plan, *alpha, A, B, *beta, C));
     });
@@ -1556,8 +1585,8 @@ extern "C" iclblasStatus_t iclblasStrsmBatchedUnevenBackward(iclblasHandle_t h, 
     return guarded([&]() -> iclblasStatus_t {
         if (!handle_ok(h) || !plan_ok(plan, 0) || !alpha) return ICLBLAS_STATUS_INVALID_VALUE;
         if (plan->batch == 0) return ICLBLAS_STATUS_SUCCESS;
-        if (plan->device != h->device || !ptr_array_ok(A) || !ptr_array_ok(X) || !ptr_array_ok(G) ||
-            (dA && !ptr_array_ok(dA)))
+        if (plan->device != h->device || !ptr_array_ok(h, A) || !ptr_array_ok(h, X) || !ptr_array_ok(h, G) ||
+            (dA && !ptr_array_ok(h, dA)))
             return ICLBLAS_STATUS_INVALID_VALUE;
         return map_cuda(iclb::batch_trsm_backward(h, plan, *alpha, A, X, G, dA));
     });

@@ -1,7 +1,7 @@
 // GEMM dispatch by the handle's math mode.
 //
 // The reference picks among seven SGEMM implementations by summed accept()
-// scores (libs/blas/functions_base.hpp:164-223); here the routine maps
+// scores (include/iclgpu/functions_base.hpp:164-223); here the routine maps
 // directly: PLAIN_FP32 runs the CUDA-core FFMA kernel (bit-identical to the
 // reference's FP32 FMA order), the tensor-core modes run the tcgen05 kernel.
 #include <cuda_fp16.h>

@@ -1091,12 +1091,20 @@ __device__ __forceinline__ void put(const SplitOut& o, long idx, float x)
 // Real operands: 32 rows x 64 K per block (256 threads).  Reads are coalesced
 // along the source's contiguous dimension (through shared memory); each
 // thread then writes two consecutive K values: one bfloat162 per plane, or a
-// float2 for TF32 (128- or 256-byte rows per warp).
+// float2 for TF32 (128- or 256-byte rows per warp).  Row r goes to
+// plane + r * o.kpad, K values [0, kw) (zeros for k >= K; kw even).
+// `tri` masks L to a triangle (1: keep k <= r, 2: keep k >= r; `unit` puts 1
+// on the diagonal); tiles wholly outside the kept triangle are left
+// unwritten.  blockIdx.z selects one of several equal operands: source
+// + z * szs, destination row offset + z * dzs.
 __global__ void __launch_bounds__(256) split_real_kernel(int R, int K, const float* __restrict__ S, long rs, long ks,
-                                                         SplitOut o)
+                                                         SplitOut o, long kw, int tri, int unit, long szs, long dzs)
 {
     __shared__ float tile[32][65];
     const int k0 = blockIdx.x * 64, r0 = blockIdx.y * 32, t = threadIdx.x;
+    if ((tri == 1 && k0 > r0 + 31) || (tri == 2 && k0 + 63 < r0)) return;
+    S += (long)blockIdx.z * szs;
+    const long dz = (long)blockIdx.z * dzs;
     if (rs == 1) {  // contiguous along r
         for (int idx = t; idx < 32 * 64; idx += 256) {
             const int rr = idx % 32, kk = idx / 32;
@@ -1114,9 +1122,14 @@ __global__ void __launch_bounds__(256) split_real_kernel(int R, int K, const flo
     for (int idx = t; idx < 32 * 32; idx += 256) {
         const int kp = idx % 32, rr = idx / 32;
         const int r = r0 + rr, k = k0 + 2 * kp;
-        if (r >= R || k >= o.kpad) continue;
-        const float a = tile[rr][2 * kp], b = tile[rr][2 * kp + 1];
-        const long off = (long)r * o.kpad + k;  // even: 4- and 8-byte aligned pairs
+        if (r >= R || k >= kw) continue;
+        float a = tile[rr][2 * kp], b = tile[rr][2 * kp + 1];
+        if (tri) {
+            const bool ka = tri == 1 ? k <= r : k >= r, kb = tri == 1 ? k + 1 <= r : k + 1 >= r;
+            a = ka ? ((unit && k == r) ? 1.f : a) : 0.f;
+            b = kb ? ((unit && k + 1 == r) ? 1.f : b) : 0.f;
+        }
+        const long off = ((long)r + dz) * o.kpad + k;  // even: 4- and 8-byte aligned pairs
         if (o.tf32) {
             *reinterpret_cast<float2*>((float*)o.plane[0] + off) = make_float2(to_tf32(a), to_tf32(b));
         } else {
@@ -1337,13 +1350,31 @@ ModeInfo mode_info(iclblasMathMode_t mode)
     return mi;
 }
 
+// The mode's share of the kernel parameters for a K extent of kext elements:
+// K blocks, products per block (in the small-first order) and TMEM chunking.
+// 6xBF16 drains the accumulator every K block (its FP32-level accuracy
+// needs it: 2 blocks per chunk measured 5.9e-7 instead of 2.2e-7 at
+// 8192^3); 3xBF16 every 4 blocks (its dropped products dominate: 3.84e-6
+// instead of 3.78e-6, 9 % faster); TF32 accumulates the whole K in TMEM.
+void set_mode_params(Params& p, const ModeInfo& mi, long kext)
+{
+    const int kblk = ROW_BYTES / (mi.tf32 ? 4 : 2);
+    p.kblocks = (int)((kext + kblk - 1) / kblk);
+    p.nprod = mi.nprod;
+    p.chunk = mi.tf32 ? p.kblocks : (mi.nprod == 3 ? 4 : 1);
+    for (int i = 0; i < 6; ++i) {
+        p.pa[i] = mi.pa[i];
+        p.pb[i] = mi.pb[i];
+    }
+}
+
 template <class T>
 cudaError_t run_split(iclblasHandle_t h, const T* S, int R, int K, long rs, long ks, int conj, int mode,
                       const SplitOut& o, long out_rows)
 {
     if (std::is_same<T, float>::value) {
         dim3 grid((unsigned)ceil_div(o.kpad, 64L), (unsigned)ceil_div(R, 32));
-        split_real_kernel<<<grid, 256, 0, h->stream>>>(R, K, (const float*)S, rs, ks, o);
+        split_real_kernel<<<grid, 256, 0, h->stream>>>(R, K, (const float*)S, rs, ks, o, o.kpad, 0, 0, 0, 0);
         return cudaGetLastError();
     }
     dim3 grid(ceil_div(K, 32), ceil_div(R, 32));
@@ -1374,14 +1405,15 @@ KernelFacts kernel_facts(K kernel, int smem, bool pairs, iclblasHandle_t h)
 {
     static std::mutex mu;
     static std::map<std::pair<const void*, int>, KernelFacts> known;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    const std::pair<const void*, int> key((const void*)kernel, dev);
+    const std::pair<const void*, int> key((const void*)kernel, h->device);
     {
         std::lock_guard<std::mutex> lock(mu);
         auto it = known.find(key);
         if (it != known.end()) return it->second;
     }
+    // the attribute and the occupancy query apply to the current device
+    DeviceGuard guard(h->device);
+    if (guard.status() != cudaSuccess) return KernelFacts{guard.status(), 0};
     KernelFacts f{cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), 0};
     if (f.status == cudaSuccess && pairs) {
         cudaLaunchConfig_t cfg = {};
@@ -1524,14 +1556,7 @@ cudaError_t gemm_tc(iclblasHandle_t h, int ta, int tb, int m, int n, int k, T al
     Params p{};
     p.M = m;
     p.N = (int)rows_b;
-    p.kblocks = (int)(kpad / kblk);
-    p.nprod = mi.nprod;
-    // 6xBF16 drains the accumulator every K block (its FP32-level accuracy
-    // needs it: 2 blocks per chunk measured 5.9e-7 instead of 2.2e-7 at
-    // 8192^3); 3xBF16 every 4 blocks (its dropped products dominate: 3.84e-6
-    // instead of 3.78e-6, 9 % faster); TF32 accumulates the whole K in TMEM
-    p.chunk = mi.tf32 ? p.kblocks : (mi.nprod == 3 ? 4 : 1);
-    for (int i = 0; i < 6; ++i) { p.pa[i] = mi.pa[i]; p.pb[i] = mi.pb[i]; }
+    set_mode_params(p, mi, kpad);
     p.complex_out = cplx ? 1 : 0;
     const float* al = (const float*)&alpha;
     const float* be = (const float*)&beta;
@@ -1617,10 +1642,71 @@ cudaError_t hgemm_tc(iclblasHandle_t h, int ta, int tb, int m, int n, int k, flo
     return launch_engine(h, mi, pa, pb, p);
 }
 
+// Products of pre-split operands (declared in internal.h): the engine over
+// sub-boxes of plane sets split once by the caller.
+cudaError_t gemm_planes_tc(iclblasHandle_t h, const GemmPlanes& a, long ar0, long ak0, const GemmPlanes& b, long br0,
+                           long bk0, int m, int n, int k, float alpha, float beta, float* C, int ldc)
+{
+    const ModeInfo mi = mode_info(h->math);
+    if (h->math == ICLBLAS_MATH_PLAIN_FP32 || k <= 0 || a.tf32 != (mi.tf32 ? 1 : 0) ||
+        b.tf32 != (mi.tf32 ? 1 : 0) || a.nlev < mi.nlev || b.nlev < mi.nlev)
+        return cudaErrorInvalidValue;
+    const long esize = mi.tf32 ? 4 : 2;
+    Params p{};
+    p.M = m;
+    p.N = n;
+    set_mode_params(p, mi, k);
+    p.alpha_re = alpha;
+    p.beta_re = beta;
+    p.C = C;
+    p.ldc = ldc;
+    p.status = h->ws.dev_status;
+    p.ab_fmt = 1;
+    Operand oa[3], ob[3];
+    for (int l = 0; l < 3; ++l) {
+        const int la = l < a.nlev ? l : 0, lb = l < b.nlev ? l : 0;
+        oa[l] = Operand{(const char*)a.plane[la] + (ar0 * a.pitch + ak0) * esize, m, k, a.pitch, false};
+        ob[l] = Operand{(const char*)b.plane[lb] + (br0 * b.pitch + bk0) * esize, n, k, b.pitch, false};
+    }
+    return launch_engine(h, mi, oa, ob, p);
+}
+
+cudaError_t split_planes_tc(iclblasHandle_t h, const float* S, int R, int K, long rs, long ks, const GemmPlanes& dst,
+                            long row0, long k0, long kw, int tri, int unit, int nz, long szs, long dzs)
+{
+    if (R <= 0 || kw <= 0 || nz <= 0) return cudaSuccess;
+    if ((kw & 1) || (k0 & 1) || nz > 65535) return cudaErrorInvalidValue;
+    const long esize = dst.tf32 ? 4 : 2;
+    SplitOut o{};
+    o.nlev = dst.nlev;
+    o.tf32 = dst.tf32;
+    o.kpad = dst.pitch;
+    for (int l = 0; l < dst.nlev; ++l) o.plane[l] = (char*)dst.plane[l] + (row0 * dst.pitch + k0) * esize;
+    dim3 grid((unsigned)ceil_div(kw, 64L), (unsigned)ceil_div(R, 32), (unsigned)nz);
+    split_real_kernel<<<grid, 256, 0, h->stream>>>(R, K, S, rs, ks, o, kw, tri, unit, szs, dzs);
+    return cudaGetLastError();
+}
+
 template cudaError_t gemm_tc<float>(iclblasHandle_t, int, int, int, int, int, float, const float*, int, const float*,
                                     int, float, float*, int, int);
 template cudaError_t gemm_tc<cfloat>(iclblasHandle_t, int, int, int, int, int, cfloat, const cfloat*, int,
                                      const cfloat*, int, cfloat, cfloat*, int, int);
 
 }  // namespace tc
+
+int plane_esize(iclblasMathMode_t mode) { return mode == ICLBLAS_MATH_TF32 ? 4 : 2; }
+int plane_levels(iclblasMathMode_t mode) { return tc::mode_info(mode).nlev; }
+
+cudaError_t split_planes(iclblasHandle_t h, const float* S, int R, int K, long rs, long ks, const GemmPlanes& dst,
+                         long row0, long k0, long kw, int tri, int unit, int nz, long szs, long dzs)
+{
+    return tc::split_planes_tc(h, S, R, K, rs, ks, dst, row0, k0, kw, tri, unit, nz, szs, dzs);
+}
+
+cudaError_t gemm_planes(iclblasHandle_t h, const GemmPlanes& a, long ar0, long ak0, const GemmPlanes& b, long br0,
+                        long bk0, int m, int n, int k, float alpha, float beta, float* C, int ldc)
+{
+    if (m <= 0 || n <= 0) return cudaSuccess;
+    return tc::gemm_planes_tc(h, a, ar0, ak0, b, br0, bk0, m, n, k, alpha, beta, C, ldc);
+}
 }  // namespace iclb

@@ -48,6 +48,38 @@ cudaError_t sgemm_backward(iclblasHandle_t h, int ta, int tb, int m, int n, int 
                            const float* B, int ldb, float beta, const float* G, int ldg, float* dA, int ldda,
                            float* dB, int lddb, float* dC, int lddc);
 
+// ---------------------------------------------------------------- pre-split GEMM operands
+// Real operands of the tensor-core modes held as split planes, for products
+// whose operands are reused (TRSM splits its triangle once per call and
+// each solved block once).  A plane set stores rows of K values contiguously
+// (K-major), `pitch` elements per row (a multiple of 64 elements for BF16,
+// 32 for TF32), in `nlev` planes: BF16 hi, mid, lo (3xBF16 reads two, 6xBF16
+// three) or one TF32-rounded FP32 plane.
+struct GemmPlanes {
+    void* plane[3] = {nullptr, nullptr, nullptr};
+    int nlev = 0;
+    int tf32 = 0;
+    long pitch = 0;
+};
+// Element size and levels of the planes of `mode` (a tensor-core mode).
+int plane_esize(iclblasMathMode_t mode);
+int plane_levels(iclblasMathMode_t mode);
+// Splits the real operand L[r][k] = S[r*rs + k*ks] (r < R, k < K) into rows
+// row0.. of `dst`, K values [k0, k0 + kw) (zeros past K; kw even, k0 even).
+// tri: 1 keeps k <= r, 2 keeps k >= r (unit: 1 on the diagonal); blocks
+// wholly outside the triangle are not written.  nz operands at source
+// stride szs and destination row stride dzs are split in one launch.
+cudaError_t split_planes(iclblasHandle_t h, const float* S, int R, int K, long rs, long ks, const GemmPlanes& dst,
+                         long row0, long k0, long kw, int tri = 0, int unit = 0, int nz = 1, long szs = 0,
+                         long dzs = 0);
+// C (m x n, column-major) = alpha * A' B'^T + beta * C in the handle's math
+// mode, A' = rows [ar0, ar0 + m) x K [ak0, ak0 + k) of planes a and B' =
+// rows [br0, br0 + n) x the same K range [bk0, bk0 + k) of planes b.  K
+// offsets and the row pitch keep every sub-box 16-byte aligned when ak0 and
+// bk0 are multiples of 8.
+cudaError_t gemm_planes(iclblasHandle_t h, const GemmPlanes& a, long ar0, long ak0, const GemmPlanes& b, long br0,
+                        long bk0, int m, int n, int k, float alpha, float beta, float* C, int ldc);
+
 }  // namespace iclb
 
 struct iclblasContext {
@@ -72,6 +104,31 @@ struct iclblasContext {
 };
 
 namespace iclb {
+
+// Makes `device` current for a scope and restores the previous device.
+class DeviceGuard {
+public:
+    explicit DeviceGuard(int device)
+    {
+        status_ = cudaGetDevice(&prev_);
+        if (status_ == cudaSuccess && prev_ != device) {
+            status_ = cudaSetDevice(device);
+            switched_ = status_ == cudaSuccess;
+        }
+    }
+    ~DeviceGuard()
+    {
+        if (switched_) cudaSetDevice(prev_);
+    }
+    cudaError_t status() const { return status_; }
+    DeviceGuard(const DeviceGuard&) = delete;
+    DeviceGuard& operator=(const DeviceGuard&) = delete;
+
+private:
+    int prev_ = 0;
+    bool switched_ = false;
+    cudaError_t status_ = cudaSuccess;
+};
 
 // Returns scratch of at least `bytes` (256-byte aligned) or nullptr.
 void* scratch(iclblasHandle_t h, size_t bytes);

@@ -521,26 +521,61 @@ static __device__ __align__(256) SdotNoAllocScratch g_sdot_noalloc_scratch;
 namespace {
 constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mu;
-SdotNoAllocScratch* g_noalloc_addr[kMaxDevices] = {};
+struct NoAllocAddr {
+    unsigned long long ctx_id = 0;   // CUDA context the address belongs to (0: none yet)
+    SdotNoAllocScratch* ptr = nullptr;
+};
+NoAllocAddr g_noalloc_addr[kMaxDevices];
 
-// Device address of the scratch on `device`, looked up once per device with
-// that device current.
+// Unique ID of the current CUDA context (cuCtxGetId through the runtime's
+// driver entry point; IDs are never reused within a process), 0 if unknown.
+unsigned long long current_context_id()
+{
+    using GetCurrent = int (*)(void**);
+    using GetId = int (*)(void*, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = (GetCurrent)p;
+        p = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = (GetId)p;
+        cudaGetLastError();
+    });
+    void* ctx = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+    return id;
+}
+
+// Device address of the scratch on `device`, looked up with that device
+// current once per device and CUDA context: cudaDeviceReset destroys the
+// device's primary context, and the next call looks the address up again
+// in the new one.
 cudaError_t noalloc_scratch_addr(int device, SdotNoAllocScratch** out)
 {
     if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_addr[device]) {
-        int cur = -1;
-        cudaError_t e = cudaGetDevice(&cur);
-        if (e != cudaSuccess) return e;
-        if (cur != device && (e = cudaSetDevice(device)) != cudaSuccess) return e;
+    DeviceGuard guard(device);
+    if (guard.status() != cudaSuccess) return guard.status();
+    // (the handle's calls made this device's primary context current; with
+    // the context unknown the address is looked up on every call)
+    const unsigned long long ctx = current_context_id();
+    NoAllocAddr& a = g_noalloc_addr[device];
+    if (!a.ptr || ctx == 0 || a.ctx_id != ctx) {
         void* ptr = nullptr;
-        e = cudaGetSymbolAddress(&ptr, g_sdot_noalloc_scratch);
-        if (cur != device) cudaSetDevice(cur);
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_sdot_noalloc_scratch);
         if (e != cudaSuccess) return e;
-        g_noalloc_addr[device] = (SdotNoAllocScratch*)ptr;
+        a.ptr = (SdotNoAllocScratch*)ptr;
+        a.ctx_id = ctx;
     }
-    *out = g_noalloc_addr[device];
+    *out = a.ptr;
     return cudaSuccess;
 }
 }  // namespace

@@ -14,6 +14,9 @@
  *     copies them to the device, runs, copies outputs back and returns when
  *     the results are in host memory) or DEVICE pointers (extension: the call
  *     is enqueued on the handle's stream and returns without waiting);
+ *     device memory must belong to the GPU the handle was created on (or be
+ *     managed memory): another GPU's memory gives INVALID_VALUE, before any
+ *     copy or launch;
  *   - result arguments of reductions (dot/nrm2/asum/iamax) follow the same
  *     rule: a host pointer is written before return, a device pointer is
  *     written by the device in stream order;
@@ -114,15 +117,19 @@ ICLBLAS_API iclblasStatus_t iclblasSdot(iclblasHandle_t handle, int n, float* x,
  * scratch (one FP64 partial per thread block, at most 4096, and a ticket
  * counter: 32 KiB + 256 B) in a fixed array compiled into the library, which
  * every GPU that loads the library holds until the process exits.
- *   - x, y and result must be device pointers (INVALID_VALUE otherwise:
- *     staging host data would allocate); the call is asynchronous on the
+ *   - x, y and result must be device pointers on the handle's GPU
+ *     (INVALID_VALUE otherwise: staging host data would allocate, and a
+ *     kernel cannot read another GPU's memory); the call is asynchronous on the
  *     handle's stream and its result equals iclblasSdot's;
  *   - a call needing more than 4096 partials -- one per block, with
  *     min(ceil(n/1024), 8 x SM count) blocks for unit-stride 16-byte-aligned
  *     operands and min(ceil(n/256), 8 x SM count) otherwise -- returns
  *     NOT_SUPPORTED;
  *   - the first call on each device looks up the array's device address
- *     (cudaGetSymbolAddress); make that first call before any stream capture;
+ *     (cudaGetSymbolAddress) in the CUDA runtime's context of that device
+ *     (its primary context; a context made current through the driver API is
+ *     not supported), and looks it up again once that context has changed
+ *     (after cudaDeviceReset); make that first call before any stream capture;
  *   - all calls share the one array, which keeps the previous call's
  *     contents (the counter is cleared at the start of each call): calls that
  *     overlap on the GPU (other streams or handles at the same time) race and
