@@ -340,6 +340,29 @@ void* iclb::scratch(iclblasHandle_t h, size_t bytes)
     return h->ws.scratch;
 }
 
+cudaError_t iclb::fork_side(iclblasHandle_t h, cudaStream_t* side)
+{
+    cudaError_t e;
+    if (!h->aux_stream && (e = cudaStreamCreateWithFlags(&h->aux_stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return e;
+    if (!h->fork_ev && (e = cudaEventCreateWithFlags(&h->fork_ev, cudaEventDisableTiming)) != cudaSuccess) return e;
+    if (!h->join_ev && (e = cudaEventCreateWithFlags(&h->join_ev, cudaEventDisableTiming)) != cudaSuccess) return e;
+    if ((e = cudaEventRecord(h->fork_ev, h->stream)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(h->aux_stream, h->fork_ev, 0)) != cudaSuccess) return e;
+    *side = h->aux_stream;
+    return cudaSuccess;
+}
+
+cudaError_t iclb::join_side(iclblasHandle_t h)
+{
+    cudaError_t e = cudaEventRecord(h->join_ev, h->aux_stream);
+    if (e != cudaSuccess) return e;
+    return cudaStreamWaitEvent(h->stream, h->join_ev, 0);
+}
+
+iclb::StreamScope::StreamScope(iclblasHandle_t h, cudaStream_t s) : h_(h), saved_(h->stream) { h->stream = s; }
+iclb::StreamScope::~StreamScope() { h_->stream = saved_; }
+
 void* iclb::solver_scratch(iclblasHandle_t h, size_t bytes)
 {
     bytes = (bytes + 255) & ~(size_t)255;
@@ -405,6 +428,8 @@ extern "C" iclblasStatus_t iclblasDestroy(iclblasHandle_t handle)
         }
         for (int c = 0; c < iclblasContext::kMaxChunks; ++c)
             if (handle->chunk_ev[c]) cudaEventDestroy(handle->chunk_ev[c]);
+        if (handle->fork_ev) cudaEventDestroy(handle->fork_ev);
+        if (handle->join_ev) cudaEventDestroy(handle->join_ev);
         cudaFree(handle->ws.counters);
         cudaFree(handle->ws.dev_status);
         cudaStreamDestroy(handle->own_stream);

@@ -43,9 +43,10 @@
 //    epilogue, not the MMA, bounds the tile (small K).  A TMA store clips the
 //    contiguous dimension only at 16-byte granularity, so the C map stops at
 //    M rounded down to 16 bytes and the last few rows are stored directly.
-//    The BF16 modes, whose MMA work per tile is 3-6x longer, keep their
-//    running sum in registers and store directly; triangular output and a
-//    C that TMA cannot address (16-byte alignment) take the direct path too.
+//    The BF16 modes with several chunks keep their running sum in registers
+//    and stage it the same way once the last chunk is drained; triangular
+//    output and a C that TMA cannot address (16-byte alignment) are stored
+//    directly.
 // 4. HGEMM operands are read in place in either layout: K-major (op T of A,
 //    op N of B) through the plane descriptors, MN-major (op N of A, op T of
 //    B) as boxes of 64 rows x 64 K with an MN-major shared-memory descriptor;
@@ -85,8 +86,6 @@ constexpr int EPI_STAGE_BYTES = 4 * EPI_BUF_BYTES;  // two buffers for each half
 constexpr int MN_CHUNK_BYTES = 8192;            // MN-major operand: 64 rows x 64 K of 16-bit values
 constexpr int SMEM_BYTES = RING_BYTES + 1024 /*barriers*/ + EPI_STAGE_BYTES + 1024 /*alignment*/;
 static_assert(SMEM_BYTES <= 232448, "shared memory per CTA");
-// the BF16 modes store directly and leave the staging area to the L1 cache
-constexpr int SMEM_BYTES_DIRECT = SMEM_BYTES - EPI_STAGE_BYTES;
 // Output tile 128 x BN: 256 columns, or 128 when the 256-wide tiles would
 // leave a quarter or more of the SMs idle (more, smaller tiles).
 template <int BN_>
@@ -603,16 +602,22 @@ __device__ __forceinline__ void epilogue_single(const Params& p, const CUtensorM
 }
 
 // Several chunks (the BF16 modes): each chunk is drained into FP32 registers
-// and released at once; the sum is stored directly (these stores overlap the
-// longer MMA work of the next tile).  Nothing but the running sum stays live
-// across the chunk loop.
+// and released at once; only the running sum stays live across the chunk
+// loop.  The sum is stored through the staged TMA path when C allows it
+// (direct column-at-a-time stores of a 128-row tile took 5.5 us, a third of
+// a 512 x 4096 x 512 3xBF16 call), else directly.
 template <int OUT, int BN, int EPI_COLS, class Arrive>
-__device__ __forceinline__ void epilogue_multi(const Params& p, int t0, int tstep, int ntiles, int tiles_m,
-                                               int tiles_n, int tile_rows, int row_off, uint32_t tmem_base,
-                                               uint64_t* tfull, Arrive arrive, volatile int* abort_flag)
+__device__ __forceinline__ void epilogue_multi(const Params& p, const CUtensorMap* mC, int t0, int tstep, int ntiles,
+                                               int tiles_m, int tiles_n, int tile_rows, int row_off,
+                                               uint32_t tmem_base, uint64_t* tfull, Arrive arrive, uint8_t* epi_buf,
+                                               uint64_t* cbar, volatile int* abort_flag)
 {
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
     const int q = warp & 3, half = (warp - 2) / 4;
+    const int r = q * 32 + lane;  // row within the CTA's 128
+    constexpr int GW = group_cols<OUT>();
+    static_assert(EPI_COLS % GW == 0 && EPI_COLS % 8 == 0, "epilogue columns");
+    EpiGroup eg{epi_buf + half * 2 * EPI_BUF_BYTES, cbar + half * 2, 1 + half, q == 0 && lane == 0, 0};
     const int nchunks = (p.kblocks + p.chunk - 1) / p.chunk;
     int acc = 0;
     uint32_t acc_ph = 0;
@@ -640,21 +645,37 @@ __device__ __forceinline__ void epilogue_multi(const Params& p, int t0, int tste
             if (lane == 0) arrive(acc);
             if (++acc == 2) { acc = 0; acc_ph ^= 1; }
         }
+        // the half's four warps go on together (a warp that gave up has set
+        // the abort flag, so the others' waits end too)
+        ok = group_all(eg.id, ok);
         if (!ok) break;
         int tm, tn;
         tile_at(p.tri, t, tiles_m, tiles_n, tile_rows, BN, tm, tn);
-        const int row = tm * tile_rows + row_off + q * 32 + lane;
+        const int row0 = tm * tile_rows + row_off;
         const int col0 = tn * BN + half * EPI_COLS;
-        if (row < p.M) {
+        if (p.c_tma) {
+#pragma unroll
+            for (int g = 0; g < EPI_COLS / GW; ++g) {
+                float v[GW];
+#pragma unroll
+                for (int j = 0; j < GW; ++j) v[j] = sum[g * GW + j];
+                if (ok) ok = stage_group<OUT>(v, p, mC, eg, r, row0, col0 + g * GW, abort_flag);
+            }
+            if (!ok) {
+                if (eg.leader) mbar_drain(&eg.bar[eg.gi & 1], (uint32_t)(eg.gi >> 1) & 1u);
+                break;
+            }
+        } else if (row0 + r < p.M) {
 #pragma unroll
             for (int g = 0; g < EPI_COLS / 8; ++g) {
                 float v[8];
 #pragma unroll
                 for (int j = 0; j < 8; ++j) v[j] = sum[g * 8 + j];
-                direct_group<OUT, 8>(v, p, row, col0 + g * 8);
+                direct_group<OUT, 8>(v, p, row0 + r, col0 + g * 8);
             }
         }
     }
+    if (eg.leader) bulk_wait_all();
 }
 
 template <bool TF32, int BN_, int OUT, bool SINGLE>
@@ -782,8 +803,8 @@ __global__ void __launch_bounds__(THREADS, 1)
             epilogue_single<OUT, BN, EPI_COLS>(p, &mC, blockIdx.x, gridDim.x, ntiles, tiles_m, tiles_n, BM, 0,
                                                 tmem_base, tfull, arrive, epi_buf, cbar, abort_flag);
         else
-            epilogue_multi<OUT, BN, EPI_COLS>(p, blockIdx.x, gridDim.x, ntiles, tiles_m, tiles_n, BM, 0, tmem_base,
-                                               tfull, arrive, abort_flag);
+            epilogue_multi<OUT, BN, EPI_COLS>(p, &mC, blockIdx.x, gridDim.x, ntiles, tiles_m, tiles_n, BM, 0,
+                                               tmem_base, tfull, arrive, epi_buf, cbar, abort_flag);
     }
 
     __syncthreads();
@@ -1030,8 +1051,8 @@ __global__ void __launch_bounds__(THREADS, 1)
             epilogue_single<OUT, BN, EPI_COLS>(p, &mC, pair, npairs, ntiles, tiles_m, tiles_n, 2 * BM,
                                                 (int)rank * BM, tmem_base, tfull, arrive, epi_buf, cbar, abort_flag);
         else
-            epilogue_multi<OUT, BN, EPI_COLS>(p, pair, npairs, ntiles, tiles_m, tiles_n, 2 * BM, (int)rank * BM,
-                                               tmem_base, tfull, arrive, abort_flag);
+            epilogue_multi<OUT, BN, EPI_COLS>(p, &mC, pair, npairs, ntiles, tiles_m, tiles_n, 2 * BM,
+                                               (int)rank * BM, tmem_base, tfull, arrive, epi_buf, cbar, abort_flag);
     }
 
     __syncthreads();
@@ -1460,12 +1481,12 @@ cudaError_t launch_engine(iclblasHandle_t h, const ModeInfo& mi, const Operand* 
     }
     p.a_mn = a[0].mn ? 1 : 0;
     p.b_mn = b[0].mn ? 1 : 0;
-    // staged stores in the single-chunk kernels: the whole K in one
-    // accumulator (TF32, HGEMM, and the BF16 modes when K fits one chunk); a
-    // multi-chunk tile's stores overlap its longer MMA work and go direct
+    // single-chunk kernels hold the whole K in one accumulator (TF32, HGEMM,
+    // and the BF16 modes when K fits one chunk); both forms store C through
+    // TMA boxes whenever C allows it
     const bool single = mi.tf32 || p.out_half || p.kblocks <= p.chunk;
-    p.c_tma = single && make_c_map(&mc, p) ? 1 : 0;
-    const int smem = single ? SMEM_BYTES : SMEM_BYTES_DIRECT;
+    p.c_tma = make_c_map(&mc, p) ? 1 : 0;
+    const int smem = SMEM_BYTES;
     if (!p.c_tma) mc = ma[0];  // unused by the kernel
     if (pairs) {
         auto run2 = [&](auto kernel) -> cudaError_t {
@@ -1651,6 +1672,10 @@ cudaError_t gemm_planes_tc(iclblasHandle_t h, const GemmPlanes& a, long ar0, lon
     if (h->math == ICLBLAS_MATH_PLAIN_FP32 || k <= 0 || a.tf32 != (mi.tf32 ? 1 : 0) ||
         b.tf32 != (mi.tf32 ? 1 : 0) || a.nlev < mi.nlev || b.nlev < mi.nlev)
         return cudaErrorInvalidValue;
+    // the tensor maps cover exactly the sub-boxes: keep them inside the planes
+    if (ar0 < 0 || ak0 < 0 || br0 < 0 || bk0 < 0 || ar0 + m > a.rows || br0 + n > b.rows || ak0 + k > a.pitch ||
+        bk0 + k > b.pitch || (ak0 & 7) || (bk0 & 7))
+        return cudaErrorInvalidValue;
     const long esize = mi.tf32 ? 4 : 2;
     Params p{};
     p.M = m;
@@ -1675,7 +1700,9 @@ cudaError_t split_planes_tc(iclblasHandle_t h, const float* S, int R, int K, lon
                             long row0, long k0, long kw, int tri, int unit, int nz, long szs, long dzs)
 {
     if (R <= 0 || kw <= 0 || nz <= 0) return cudaSuccess;
-    if ((kw & 1) || (k0 & 1) || nz > 65535) return cudaErrorInvalidValue;
+    if ((kw & 1) || (k0 & 1) || nz > 65535 || row0 < 0 || k0 < 0 || k0 + kw > dst.pitch ||
+        row0 + (long)(nz - 1) * dzs + R > dst.rows)
+        return cudaErrorInvalidValue;
     const long esize = dst.tf32 ? 4 : 2;
     SplitOut o{};
     o.nlev = dst.nlev;

@@ -60,6 +60,7 @@ struct GemmPlanes {
     int nlev = 0;
     int tf32 = 0;
     long pitch = 0;
+    long rows = 0;   // rows each plane holds: every access stays below rows x pitch
 };
 // Element size and levels of the planes of `mode` (a tensor-core mode).
 int plane_esize(iclblasMathMode_t mode);
@@ -68,7 +69,9 @@ int plane_levels(iclblasMathMode_t mode);
 // row0.. of `dst`, K values [k0, k0 + kw) (zeros past K; kw even, k0 even).
 // tri: 1 keeps k <= r, 2 keeps k >= r (unit: 1 on the diagonal); blocks
 // wholly outside the triangle are not written.  nz operands at source
-// stride szs and destination row stride dzs are split in one launch.
+// stride szs and destination row stride dzs are split in one launch.  A
+// write range outside dst (rows x pitch) returns cudaErrorInvalidValue
+// before any launch.
 cudaError_t split_planes(iclblasHandle_t h, const float* S, int R, int K, long rs, long ks, const GemmPlanes& dst,
                          long row0, long k0, long kw, int tri = 0, int unit = 0, int nz = 1, long szs = 0,
                          long dzs = 0);
@@ -76,7 +79,8 @@ cudaError_t split_planes(iclblasHandle_t h, const float* S, int R, int K, long r
 // mode, A' = rows [ar0, ar0 + m) x K [ak0, ak0 + k) of planes a and B' =
 // rows [br0, br0 + n) x the same K range [bk0, bk0 + k) of planes b.  K
 // offsets and the row pitch keep every sub-box 16-byte aligned when ak0 and
-// bk0 are multiples of 8.
+// bk0 are multiples of 8.  A sub-box outside its plane set (rows x pitch)
+// returns cudaErrorInvalidValue before any launch.
 cudaError_t gemm_planes(iclblasHandle_t h, const GemmPlanes& a, long ar0, long ak0, const GemmPlanes& b, long br0,
                         long bk0, int m, int n, int k, float alpha, float beta, float* C, int ldc);
 
@@ -101,6 +105,9 @@ struct iclblasContext {
     cudaStream_t aux_stream = nullptr;
     static constexpr int kMaxChunks = 32;
     cudaEvent_t chunk_ev[kMaxChunks] = {};
+    // Fork / join of work on the second stream within one call (created on
+    // first use).
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
 };
 
 namespace iclb {
@@ -128,6 +135,25 @@ private:
     int prev_ = 0;
     bool switched_ = false;
     cudaError_t status_ = cudaSuccess;
+};
+
+// Work of one call on two streams: fork() makes the handle's second stream
+// wait for everything issued so far on the handle's stream; join() makes the
+// handle's stream wait for everything issued so far on the second stream.
+// Both streams and the events are created on first use.
+cudaError_t fork_side(iclblasHandle_t h, cudaStream_t* side);
+cudaError_t join_side(iclblasHandle_t h);
+// Issues the launches of a scope on another stream (restored at scope exit).
+class StreamScope {
+public:
+    StreamScope(iclblasHandle_t h, cudaStream_t s);
+    ~StreamScope();
+    StreamScope(const StreamScope&) = delete;
+    StreamScope& operator=(const StreamScope&) = delete;
+
+private:
+    iclblasHandle_t h_;
+    cudaStream_t saved_;
 };
 
 // Returns scratch of at least `bytes` (256-byte aligned) or nullptr.

@@ -17,6 +17,7 @@
 // working type, and applied as GEMMs.  Every GEMM uses the handle's math mode
 // (the plain FP32 default is the CUDA-core kernel).
 #include <algorithm>
+#include <type_traits>
 
 #include "common.cuh"
 
@@ -442,6 +443,94 @@ struct Solver {
     }
 };
 
+// The tensor-core modes on real operands: the solve's GEMMs read operands
+// split into BF16 / TF32 planes once per call instead of splitting both
+// operands inside every GEMM.  Planes (K-major rows):
+//   pa    M = op(A) (left) or M^T (right), masked to its triangle, na x na;
+//         split once per call (blocks outside the triangle are never read)
+//   pinv  the leaves' FP64-formed inverses rounded to FP32: leaf bb's rows
+//         at bb*big (left: rows of inv; right: rows of inv^T); once per call
+//   px    the solved blocks of X as the update GEMMs read them (left: row j
+//         = right-hand side j, K = row of X; right: row i = row of X, K =
+//         column of X); each leaf writes its block once, after its solve
+//   pb    one leaf block of the updated B, split just before its leaf GEMM
+// Left:  update B[so] -= M[so, fo] X[fo]:    pa rows so, K fo  x  px K fo
+//        leaf   X_o = inv_o B_o:              pinv rows o       x  pb
+// Right: update B[:, so] -= X[:, fo] M[fo, so]:  px K fo  x  pa rows so, K fo
+//        leaf   X_o = B_o inv_o:              pb  x  pinv rows o
+struct PlaneSolver {
+    iclblasHandle_t h;
+    int left, m_lower, nrhs, big;
+    float* B;
+    long ldb;
+    GemmPlanes pa, pinv, px, pb;
+
+    // Leaf block [o, o + sz) of B (left: rows, right: columns) into planes
+    // `dst` at K offset k0 (left: L[j][k] = B[o + k, j]; right: L[i][k] =
+    // B[i, o + k]).  An odd size writes one zero past the block.
+    cudaError_t split_block(const GemmPlanes& dst, long k0, int o, int sz) const
+    {
+        const long kw = (sz + 1) & ~1;
+        if (left) return split_planes(h, B + o, nrhs, sz, ldb, 1, dst, 0, k0, kw);
+        return split_planes(h, B + (long)o * ldb, nrhs, sz, 1, ldb, dst, 0, k0, kw);
+    }
+
+    cudaError_t solve(int o, int sz) const
+    {
+        if (sz <= big) {
+            const long r0 = (long)(o / big) * big;
+            cudaError_t e = split_block(pb, 0, o, sz);
+            if (e != cudaSuccess) return e;
+            if (left) e = gemm_planes(h, pinv, r0, 0, pb, 0, 0, sz, nrhs, sz, 1.f, 0.f, B + o, (int)ldb);
+            else e = gemm_planes(h, pb, 0, 0, pinv, r0, 0, nrhs, sz, sz, 1.f, 0.f, B + (long)o * ldb, (int)ldb);
+            if (e != cudaSuccess) return e;
+            return split_block(px, o, o, sz);
+        }
+        const int nleaf = (sz + big - 1) / big;
+        const int h1 = (nleaf / 2) * big;
+        const int o1 = o, s1 = h1, o2 = o + h1, s2 = sz - h1;
+        const bool forward = left ? m_lower : !m_lower;
+        const int fo = forward ? o1 : o2, fs = forward ? s1 : s2;
+        const int so = forward ? o2 : o1, ss = forward ? s2 : s1;
+        cudaError_t e = solve(fo, fs);
+        if (e != cudaSuccess) return e;
+        if (left) e = gemm_planes(h, pa, so, fo, px, 0, fo, ss, nrhs, fs, -1.f, 1.f, B + so, (int)ldb);
+        else e = gemm_planes(h, px, 0, fo, pa, so, fo, nrhs, ss, fs, -1.f, 1.f, B + (long)so * ldb, (int)ldb);
+        if (e != cudaSuccess) return e;
+        return solve(so, ss);
+    }
+
+    // The right-hand sides are independent: with enough of them, the second
+    // half (rows of px / pb and columns (left) or rows (right) of B from
+    // `cut` on) is solved on the handle's second stream while the first
+    // half runs, so the latencies of the small leaf steps of one half
+    // overlap the other half's work.
+    cudaError_t solve_split(int o, int sz) const
+    {
+        const int cut = nrhs >= 1024 ? (nrhs / 2) / 64 * 64 : 0;
+        if (cut == 0) return solve(o, sz);
+        PlaneSolver lo = *this, hi = *this;
+        lo.nrhs = cut;
+        hi.nrhs = nrhs - cut;
+        hi.B = B + (left ? (long)cut * ldb : (long)cut);
+        for (GemmPlanes* g : {&hi.px, &hi.pb}) {
+            const long esize = g->tf32 ? 4 : 2;
+            for (int l = 0; l < g->nlev; ++l) g->plane[l] = (char*)g->plane[l] + (long)cut * g->pitch * esize;
+            g->rows -= cut;
+        }
+        lo.px.rows = lo.pb.rows = cut;
+        cudaStream_t side = nullptr;
+        cudaError_t e = fork_side(h, &side);
+        if (e != cudaSuccess) return e;
+        {
+            StreamScope on_side(h, side);
+            if ((e = hi.solve(o, sz)) != cudaSuccess) return e;
+        }
+        if ((e = lo.solve(o, sz)) != cudaSuccess) return e;
+        return join_side(h);
+    }
+};
+
 // B[:, :] *= alpha for an m x n column-major block.
 template <class T>
 __global__ void scale_kernel(int m, int n, T alpha, T* __restrict__ B, long ldb)
@@ -490,40 +579,109 @@ cudaError_t trsm_impl(iclblasHandle_t h, int side, int uplo, int trans, int diag
     // refinement: masked leaf blocks, a copy of B, the residual / correction
     const int steps = h->trsm_refine;
     const size_t mn = (size_t)m * n;
+    // tensor-core modes on real data: operand planes split once per call
+    const bool planes = std::is_same<T, float>::value && h->math != ICLBLAS_MATH_PLAIN_FP32;
+    const int nlev = planes ? plane_levels(h->math) : 0;
+    const long esize = planes ? plane_esize(h->math) : 0;
+    const long pitch_m = ((long)na + 63) / 64 * 64;
+    const size_t pa_b = al((size_t)na * pitch_m * esize), pinv_b = al((size_t)nbig * big * big * esize);
+    const size_t px_b = al((size_t)s.nrhs * pitch_m * esize), pb_b = al((size_t)s.nrhs * big * esize);
+    const size_t plane_bytes = planes ? nlev * (pa_b + pinv_b + px_b + pb_b) : 0;
     const size_t bytes = al(sizeof(W) * inv_w) + al(sizeof(W) * tmp_w) + al(sizeof(T) * inv_w) +
                          al(sizeof(T) * leaf_t) +
-                         (steps > 0 ? al(sizeof(T) * inv_w) + 2 * al(sizeof(T) * mn) : 0);
+                         (steps > 0 ? al(sizeof(T) * inv_w) + 2 * al(sizeof(T) * mn) : 0) + plane_bytes;
     char* ws = (char*)solver_scratch(h, bytes);
     if (!ws) return cudaErrorMemoryAllocation;
     W* invd = (W*)ws;
     W* dtmp = (W*)(ws + al(sizeof(W) * inv_w));
     T* inv32 = (T*)(ws + al(sizeof(W) * inv_w) + al(sizeof(W) * tmp_w));
     s.tmp = (T*)(ws + al(sizeof(W) * inv_w) + al(sizeof(W) * tmp_w) + al(sizeof(T) * inv_w));
-    T* mtri = (T*)((char*)s.tmp + al(sizeof(T) * leaf_t));
-    T* b0 = (T*)((char*)mtri + al(sizeof(T) * inv_w));
-    T* res = (T*)((char*)b0 + al(sizeof(T) * mn));
-    cudaError_t e = cudaMemsetAsync(invd, 0, sizeof(W) * inv_w, h->stream);
-    if (e != cudaSuccess) return e;
-    const size_t sm_inv = sizeof(W) * 2 * NB * (NB + 1);
-    if ((e = cudaFuncSetAttribute(trsm_inv_diag_kernel<T, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)sm_inv)) != cudaSuccess)
-        return e;
-    trsm_inv_diag_kernel<T, NB><<<nsmall, NB, sm_inv, h->stream>>>(na, s.op, s.m_lower, s.unit, big, A, lda, invd);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    constexpr int TS = NB;  // doubling tile: 64 real, 32 complex
-    for (int sz = NB; sz < big; sz *= 2) {
-        dim3 grid(sz / TS, sz / TS, nbig * (big / (2 * sz)));
-        trsm_inv_double_kernel<T, TS, 0><<<grid, 256, 0, h->stream>>>(na, s.op, s.m_lower, sz, big, A, lda, invd,
-                                                                       dtmp);
-        trsm_inv_double_kernel<T, TS, 1><<<grid, 256, 0, h->stream>>>(na, s.op, s.m_lower, sz, big, A, lda, invd,
-                                                                       dtmp);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    // the refinement regions exist only when steps > 0; the planes follow
+    // whatever was allocated before them
+    char* tail = (char*)s.tmp + al(sizeof(T) * leaf_t);
+    T *mtri = nullptr, *b0 = nullptr, *res = nullptr;
+    if (steps > 0) {
+        mtri = (T*)tail;
+        tail += al(sizeof(T) * inv_w);
+        b0 = (T*)tail;
+        tail += al(sizeof(T) * mn);
+        res = (T*)tail;
+        tail += al(sizeof(T) * mn);
     }
-    {
+    char* pl = tail;
+    PlaneSolver ps{};
+    if (planes) {
+        ps.h = h;
+        ps.left = s.left;
+        ps.m_lower = s.m_lower;
+        ps.nrhs = s.nrhs;
+        ps.big = big;
+        ps.B = (float*)B;
+        ps.ldb = ldb;
+        GemmPlanes* sets[4] = {&ps.pa, &ps.pinv, &ps.px, &ps.pb};
+        const size_t sizes[4] = {pa_b, pinv_b, px_b, pb_b};
+        const long pitches[4] = {pitch_m, big, pitch_m, big};
+        const long rows[4] = {na, (long)nbig * big, s.nrhs, s.nrhs};
+        for (int q = 0; q < 4; ++q) {
+            sets[q]->rows = rows[q];
+            sets[q]->nlev = nlev;
+            sets[q]->tf32 = h->math == ICLBLAS_MATH_TF32 ? 1 : 0;
+            sets[q]->pitch = pitches[q];
+            for (int l = 0; l < nlev; ++l) {
+                sets[q]->plane[l] = pl;
+                pl += sizes[q];
+            }
+        }
+    }
+    // FP64 inverses of the leaves' diagonal blocks, rounded to the working
+    // type (and, on the plane path, split into the inverse planes)
+    auto form_inverses = [&]() -> cudaError_t {
+        cudaError_t e = cudaMemsetAsync(invd, 0, sizeof(W) * inv_w, h->stream);
+        if (e != cudaSuccess) return e;
+        const size_t sm_inv = sizeof(W) * 2 * NB * (NB + 1);
+        if ((e = cudaFuncSetAttribute(trsm_inv_diag_kernel<T, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)sm_inv)) != cudaSuccess)
+            return e;
+        trsm_inv_diag_kernel<T, NB><<<nsmall, NB, sm_inv, h->stream>>>(na, s.op, s.m_lower, s.unit, big, A, lda,
+                                                                        invd);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        constexpr int TS = NB;  // doubling tile: 64 real, 32 complex
+        for (int sz = NB; sz < big; sz *= 2) {
+            dim3 grid(sz / TS, sz / TS, nbig * (big / (2 * sz)));
+            trsm_inv_double_kernel<T, TS, 0><<<grid, 256, 0, h->stream>>>(na, s.op, s.m_lower, sz, big, A, lda, invd,
+                                                                           dtmp);
+            trsm_inv_double_kernel<T, TS, 1><<<grid, 256, 0, h->stream>>>(na, s.op, s.m_lower, sz, big, A, lda, invd,
+                                                                           dtmp);
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        }
         const long cnt = (long)inv_w;
         const int g = (int)std::min<long>((cnt + 255) / 256, (long)h->sm_count * 8);
         narrow_kernel<T><<<g, 256, 0, h->stream>>>(cnt, invd, inv32);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if (!planes) return cudaSuccess;
+        // left: rows of inv; right: rows of inv^T
+        return split_planes(h, (const float*)inv32, big, big, s.left ? 1 : big, s.left ? big : 1, ps.pinv, 0, 0, big,
+                            0, 0, nbig, (long)big * big, big);
+    };
+    cudaError_t e;
+    if (planes) {
+        // the inverses (compute-bound, FP64) form on the second stream while
+        // the triangle M (left) or M^T (right), masked, is split (HBM-bound)
+        cudaStream_t side = nullptr;
+        if ((e = fork_side(h, &side)) != cudaSuccess) return e;
+        {
+            StreamScope on_side(h, side);
+            if ((e = form_inverses()) != cudaSuccess) return e;
+        }
+        const bool ml = s.m_lower != 0;
+        const int tri = s.left ? (ml ? 1 : 2) : (ml ? 2 : 1);
+        const bool rows_contig = s.left ? s.op == ICLBLAS_OP_N : s.op != ICLBLAS_OP_N;
+        e = split_planes(h, (const float*)A, na, na, rows_contig ? 1 : lda, rows_contig ? lda : 1, ps.pa, 0, 0,
+                         (na + 1) & ~1, tri, s.unit);
+        if (e == cudaSuccess) e = join_side(h);
+        if (e != cudaSuccess) return e;
+    } else if ((e = form_inverses()) != cudaSuccess) {
+        return e;
     }
     s.inv = inv32;
     if (steps > 0) {
@@ -536,7 +694,7 @@ cudaError_t trsm_impl(iclblasHandle_t h, int side, int uplo, int trans, int diag
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         s.mtri = mtri;
     }
-    e = s.solve(0, na);
+    e = planes ? ps.solve_split(0, na) : s.solve(0, na);
     if (e != cudaSuccess) return e;
     for (int it = 0; it < steps; ++it) {
         // R = B0 - M X with FP32-accurate products (6xBF16 on the tensor cores,
@@ -550,10 +708,18 @@ cudaError_t trsm_impl(iclblasHandle_t h, int side, int uplo, int trans, int diag
         e = s.residual(0, na, B, ldb, res, m);
         h->math = mode;
         if (e != cudaSuccess) return e;
-        Solver<T> c = s;
-        c.B = res;
-        c.ldb = m;
-        if ((e = c.solve(0, na)) != cudaSuccess) return e;
+        if (planes) {
+            PlaneSolver c = ps;
+            c.B = (float*)res;
+            c.ldb = m;
+            e = c.solve_split(0, na);
+        } else {
+            Solver<T> c = s;
+            c.B = res;
+            c.ldb = m;
+            e = c.solve(0, na);
+        }
+        if (e != cudaSuccess) return e;
         const long total = (long)m * n;
         const int grid = (int)std::min<long>((total + 255) / 256, (long)h->sm_count * 8);
         const T sc = it == steps - 1 ? alpha : Gemm<T>::one();
