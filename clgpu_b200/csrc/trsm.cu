@@ -168,6 +168,106 @@ __global__ void __launch_bounds__(NB) trsm_inv_diag_kernel(int n, int op, int m_
     for (int idx = threadIdx.x; idx < NB * NB; idx += NB) out[(long)(idx / NB) * big + idx % NB] = Y[idx % NB][idx / NB];
 }
 
+// The same inverses for real 64 x 64 blocks on 256 threads: the four 16 x 16
+// diagonal blocks by substitution (one column per thread, the column in
+// registers), then two doubling steps (16 -> 32 -> 64) forming each
+// off-diagonal block from products of known inverses.  Padding rows and
+// columns (at or beyond n) are an identity, as above.  One column per
+// thread over all 64 rows (trsm_inv_diag_kernel) is a 64-step dependent
+// chain per thread.
+__global__ void __launch_bounds__(256) trsm_inv_diag64_kernel(int n, int op, int m_lower, int unit, int big,
+                                                               const float* __restrict__ A, long lda,
+                                                               double* __restrict__ inv)
+{
+    constexpr int NB = 64;
+    extern __shared__ uint8_t smem_raw[];
+    double(*M)[NB + 1] = (double(*)[NB + 1])smem_raw;       // the block of op(A), padded
+    double(*R)[NB + 1] = M + NB;                              // its inverse
+    double(*Tm)[NB / 2 + 1] = (double(*)[NB / 2 + 1])(R + NB);  // doubling temporary
+    double* rd = &Tm[0][0] + (NB / 2) * (NB / 2 + 1);          // 1 / diagonal
+    const int t = threadIdx.x, o = blockIdx.x * NB, nb = max(0, min(NB, n - o));
+    for (int idx = t; idx < NB * NB; idx += 256) {
+        const int r = idx % NB, c = idx / NB;  // A-local (r, c): coalesced down A's columns
+        double v = (r == c && r >= nb) ? 1.0 : 0.0;
+        if (r < nb && c < nb) v = (double)A[(long)(o + c) * lda + (o + r)];
+        if (op == 0) M[r][c] = v;
+        else M[c][r] = v;
+        R[r][c] = 0.0;
+    }
+    __syncthreads();
+    if (t < NB) rd[t] = unit ? 1.0 : 1.0 / M[t][t];
+    __syncthreads();
+    if (t < NB) {
+        const int b = (t / 16) * 16, j = t % 16;
+        double y[16];
+        if (m_lower) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                double acc = (i == j) ? 1.0 : 0.0;
+#pragma unroll
+                for (int k = 0; k < i; ++k) acc = fma(-M[b + i][b + k], y[k], acc);
+                y[i] = (i >= j) ? acc * rd[b + i] : 0.0;
+            }
+        } else {
+#pragma unroll
+            for (int i = 15; i >= 0; --i) {
+                double acc = (i == j) ? 1.0 : 0.0;
+#pragma unroll
+                for (int k = i + 1; k < 16; ++k) acc = fma(-M[b + i][b + k], y[k], acc);
+                y[i] = (i <= j) ? acc * rd[b + i] : 0.0;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 16; ++i) R[b + i][b + j] = y[i];
+    }
+    __syncthreads();
+    // lower M = [[P, 0], [C, Q]]: off-diagonal inverse block -Q^-1 C P^-1;
+    // upper M = [[P, C], [0, Q]]: -P^-1 C Q^-1
+    auto doubling = [&](auto hc) {
+        constexpr int h = decltype(hc)::value;
+        constexpr int nout = (NB / (2 * h)) * h * h;
+        for (int idx = t; idx < nout; idx += 256) {
+            const int pr = idx / (h * h), e = idx % (h * h), r = e % h, c = e / h, q = pr * 2 * h;
+            double a0 = 0.0, a1 = 0.0;
+#pragma unroll
+            for (int k = 0; k < h; k += 2) {
+                if (m_lower) {
+                    a0 = fma(M[q + h + r][q + k], R[q + k][q + c], a0);
+                    a1 = fma(M[q + h + r][q + k + 1], R[q + k + 1][q + c], a1);
+                } else {
+                    a0 = fma(M[q + r][q + h + k], R[q + h + k][q + h + c], a0);
+                    a1 = fma(M[q + r][q + h + k + 1], R[q + h + k + 1][q + h + c], a1);
+                }
+            }
+            Tm[pr * h + r][c] = a0 + a1;
+        }
+        __syncthreads();
+        for (int idx = t; idx < nout; idx += 256) {
+            const int pr = idx / (h * h), e = idx % (h * h), r = e % h, c = e / h, q = pr * 2 * h;
+            double a0 = 0.0, a1 = 0.0;
+#pragma unroll
+            for (int k = 0; k < h; k += 2) {
+                if (m_lower) {
+                    a0 = fma(R[q + h + r][q + h + k], Tm[pr * h + k][c], a0);
+                    a1 = fma(R[q + h + r][q + h + k + 1], Tm[pr * h + k + 1][c], a1);
+                } else {
+                    a0 = fma(R[q + r][q + k], Tm[pr * h + k][c], a0);
+                    a1 = fma(R[q + r][q + k + 1], Tm[pr * h + k + 1][c], a1);
+                }
+            }
+            if (m_lower) R[q + h + r][q + c] = -(a0 + a1);
+            else R[q + r][q + h + c] = -(a0 + a1);
+        }
+        __syncthreads();
+    };
+    doubling(std::integral_constant<int, 16>{});
+    doubling(std::integral_constant<int, 32>{});
+    const int bb = o / big, lo = o % big;
+    double* out = inv + (long)bb * big * big + (long)lo * big + lo;
+    for (int idx = t; idx < NB * NB; idx += 256) out[(long)(idx / NB) * big + idx % NB] = R[idx % NB][idx / NB];
+}
+constexpr size_t kInvDiag64Smem = sizeof(double) * (2 * 64 * 65 + 32 * 33 + 64);
+
 // One doubling step of the block inverses: for every 2s x 2s diagonal block
 // (offset o in big block bb) whose two s x s diagonal inverses are known,
 //   lower M = [[P, 0], [C, Q]]:  inv = [[P^-1, 0], [-Q^-1 C P^-1, Q^-1]]
@@ -638,12 +738,20 @@ cudaError_t trsm_impl(iclblasHandle_t h, int side, int uplo, int trans, int diag
     auto form_inverses = [&]() -> cudaError_t {
         cudaError_t e = cudaMemsetAsync(invd, 0, sizeof(W) * inv_w, h->stream);
         if (e != cudaSuccess) return e;
-        const size_t sm_inv = sizeof(W) * 2 * NB * (NB + 1);
-        if ((e = cudaFuncSetAttribute(trsm_inv_diag_kernel<T, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)sm_inv)) != cudaSuccess)
-            return e;
-        trsm_inv_diag_kernel<T, NB><<<nsmall, NB, sm_inv, h->stream>>>(na, s.op, s.m_lower, s.unit, big, A, lda,
-                                                                        invd);
+        if constexpr (std::is_same<T, float>::value) {
+            if ((e = cudaFuncSetAttribute(trsm_inv_diag64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)kInvDiag64Smem)) != cudaSuccess)
+                return e;
+            trsm_inv_diag64_kernel<<<nsmall, 256, kInvDiag64Smem, h->stream>>>(na, s.op, s.m_lower, s.unit, big, A,
+                                                                              lda, (double*)invd);
+        } else {
+            const size_t sm_inv = sizeof(W) * 2 * NB * (NB + 1);
+            if ((e = cudaFuncSetAttribute(trsm_inv_diag_kernel<T, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)sm_inv)) != cudaSuccess)
+                return e;
+            trsm_inv_diag_kernel<T, NB><<<nsmall, NB, sm_inv, h->stream>>>(na, s.op, s.m_lower, s.unit, big, A,
+                                                                            lda, invd);
+        }
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         constexpr int TS = NB;  // doubling tile: 64 real, 32 complex
         for (int sz = NB; sz < big; sz *= 2) {
