@@ -168,7 +168,7 @@ class Clocks:
 class Sweep:
     """Operands of the sweep on one GPU and the calls that make one step."""
 
-    def __init__(self, torch, dev, B, host: bool, n1: int = N1, only=None):
+    def __init__(self, torch, dev, B, host: bool, n1: int = N1, only=None, pageable: bool = False):
         self.B = B
         self.only = only
         g = torch.Generator(device="cpu").manual_seed(1)
@@ -178,7 +178,7 @@ class Sweep:
             if dtype == torch.complex64:
                 t = torch.complex(t, torch.rand(shape, generator=g, dtype=torch.float32) * 2 - 1)
             if host:
-                return t.pin_memory()
+                return t if pageable else t.pin_memory()   # pageable: ordinary (malloc'd) host memory
             return t.to(dev)
 
         def want(*names):
@@ -198,8 +198,10 @@ class Sweep:
         self.cx = mk((CGEMV_N,), torch.complex64) if cg else None
         self.cy = mk((CGEMV_N,), torch.complex64) if cg else None
         if host:
-            self.r = torch.zeros(1, dtype=torch.float32).pin_memory()
-            self.ri = torch.zeros(1, dtype=torch.int32).pin_memory()
+            self.r = torch.zeros(1, dtype=torch.float32)
+            self.ri = torch.zeros(1, dtype=torch.int32)
+            if not pageable:
+                self.r, self.ri = self.r.pin_memory(), self.ri.pin_memory()
         else:
             self.r = torch.zeros(1, dtype=torch.float32, device=dev)
             self.ri = torch.zeros(1, dtype=torch.int32, device=dev)
@@ -334,6 +336,28 @@ def run_ours(args, rank, world, torch):
                    "ms_per_step": round(e2e_ms / e2e_steps, 3),
                    "path": "C ABI with pinned host operands; copies in/out inside every call"}
             del swh
+            # the same calls on pageable (ordinary malloc'd) host memory, what a
+            # drop-in caller of the reference's API passes
+            swp = Sweep(torch, dev, B, host=True, n1=args.n1, only=only, pageable=True)
+            callsp = swp.calls(h)
+            for name, f in callsp:
+                B.check(f(), name)
+            torch.cuda.synchronize()
+            if world > 1:
+                torch.distributed.barrier()
+            p0 = torch.cuda.Event(enable_timing=True)
+            p1 = torch.cuda.Event(enable_timing=True)
+            p0.record(stream)
+            for name, f in callsp:
+                B.check(f(), name)
+            p1.record(stream)
+            torch.cuda.synchronize()
+            pg_ms = max_over_ranks(torch, p0.elapsed_time(p1), dev, world)
+            e2e["pageable"] = {"value": round(aggregate_gbs(world, step_bytes, 1, pg_ms), 2), "unit": "GB/s",
+                               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": 1,
+                               "ms_per_step": round(pg_ms, 3),
+                               "path": "C ABI with pageable host operands (ordinary host memory)"}
+            del swp
 
     out = {
         "metric": "level-1/2 sweep aggregate HBM bandwidth (SAXPY/SDOT/SNRM2/SASUM/ISAMAX n=2^28, "
@@ -1126,6 +1150,8 @@ def run_batched_study(args, torch):
         h.set_stream(stream)
         plan = B.BatchPlan(h, "trsm", side=0, uplo=1, trans=0, diag=0, m=[int(v) for v in ns],
                            n=[int(v) for v in rs], lda=[int(v) for v in ns], ldb=[int(v) for v in ns])
+        # the adjoint uses the forward call's diagonal-block inverses (same A)
+        B.check(plan.set_inverse_reuse(True), "set_inverse_reuse")
         _, width, ctas = plan.info()
 
         def step():
@@ -1177,6 +1203,120 @@ def run_batched_study(args, torch):
         del graph, rgraph
         plan.destroy()
     return out
+
+
+# ---------------------------------------------------------------- single-routine cases for profiles
+def kernel_cases(torch, dev, B, h):
+    """Named single-routine cases (name -> thunk) at sizes larger than L2 and
+    a few GB on the device at most, for ncu captures of one kernel each:
+    complex level-1 at n = 2^25 (256 MiB per vector), CTRSV 8192 and STRSV
+    8192 with lda = n + 1 (the kernel for a leading dimension TMA cannot
+    address), plain SGEMM and TF32 SGEMM at 4096^3 (the CUDA-core kernel; the
+    split pre-pass), STRSM 3xBF16 8192 x 4096 (the FP64 inverse kernels and
+    the update GEMMs on operand planes) and the batched TRSM forward + adjoint
+    at 128 instances of the batched config's size distribution."""
+    g = torch.Generator(device=dev).manual_seed(6)
+
+    def rnd(k, cplx=False):
+        t = torch.rand(k, generator=g, device=dev) * 2 - 1
+        return torch.complex(t, torch.rand(k, generator=g, device=dev) * 2 - 1) if cplx else t
+
+    nc = 1 << 25
+    cx, cy = rnd(nc, True), rnd(nc, True)
+    rf = torch.zeros(1, device=dev)
+    rc = torch.zeros(1, dtype=torch.complex64, device=dev)
+    ri = torch.zeros(1, dtype=torch.int32, device=dev)
+    nt = 8192
+
+    def tri(n, cplx):
+        L = torch.tril(torch.randn(n, n, generator=g, device=dev) / n ** 0.5, -1) + torch.diag(
+            torch.rand(n, generator=g, device=dev) + 1)
+        return L.to(torch.complex64) if cplx else L
+    Lc = tri(nt, True).t().contiguous().reshape(-1)
+    xc = rnd(nt, True)
+    Ls = torch.zeros(nt * (nt + 1), device=dev)
+    Ls.view(nt, nt + 1)[:, :nt] = tri(nt, False).t()   # column-major, lda = n + 1
+    xs = rnd(nt)
+    ng = 4096
+    Ag, Bg, Cg = rnd(ng * ng), rnd(ng * ng), torch.zeros(ng * ng, device=dev)
+    mt, nr = 8192, 4096
+    At = tri(mt, False).t().contiguous().reshape(-1)
+    Bt0 = rnd(mt * nr)
+    Bt = Bt0.clone()
+    # batched: 128 instances, n ~ UniformInt[32,1024], nrhs ~ UniformInt[1,256]
+    rng = np.random.default_rng(4)
+    bn, br = rng.integers(32, 1025, 128), rng.integers(1, 257, 128)
+    bA = [tri(int(n), False).t().contiguous().reshape(-1) for n in bn]
+    bX = [rnd(int(n) * int(r)) for n, r in zip(bn, br)]
+    bG = [rnd(int(n) * int(r)) for n, r in zip(bn, br)]
+    bdA = [torch.empty(int(n) * int(n), device=dev) for n in bn]
+    P = lambda ts: torch.tensor([t.data_ptr() for t in ts], dtype=torch.int64, device=dev)  # noqa: E731
+    pA, pX, pG, pdA = P(bA), P(bX), P(bG), P(bdA)
+    plan = B.BatchPlan(h, "trsm", side=0, uplo=1, trans=0, diag=0, m=[int(v) for v in bn], n=[int(v) for v in br],
+                       lda=[int(v) for v in bn], ldb=[int(v) for v in bn])
+
+    def mode_call(mode, f):
+        def run():
+            h.set_math_mode(mode)
+            f()
+            h.set_math_mode(B.MATH_PLAIN_FP32)
+        return run
+
+    def strsm():
+        Bt.copy_(Bt0)
+        B.check(B.iclblasStrsm(h, 0, 1, 0, 0, mt, nr, 1.0, At, mt, Bt, mt), "strsm")
+
+    cases = {
+        "caxpy": lambda: B.check(B.iclblasCaxpy(h, nc, 0.5 - 0.25j, cx, 1, cy, 1), "caxpy"),
+        "cscal": lambda: B.check(B.iclblasCscal(h, nc, 0.5 - 0.25j, cx, 1), "cscal"),
+        "cdotu": lambda: B.check(B.iclblasCdotu(h, nc, cx, 1, cy, 1, rc), "cdotu"),
+        "cdotc": lambda: B.check(B.iclblasCdotc(h, nc, cx, 1, cy, 1, rc), "cdotc"),
+        "scnrm2": lambda: B.check(B.iclblasScnrm2(h, nc, cx, 1, rf), "scnrm2"),
+        "scasum": lambda: B.check(B.iclblasScasum(h, nc, cx, 1, rf), "scasum"),
+        "icamax": lambda: B.check(B.iclblasIcamax(h, nc, cx, 1, ri), "icamax"),
+        "ctrsv": lambda: B.check(B.iclblasCtrsv(h, 1, 0, 0, nt, Lc, nt, xc, 1), "ctrsv"),
+        "strsv_lda": lambda: B.check(B.iclblasStrsv(h, 1, 0, 0, nt, Ls, nt + 1, xs, 1), "strsv"),
+        "sgemm_plain": lambda: B.check(B.iclblasSgemm(h, 0, 0, ng, ng, ng, 1.0, Ag, ng, Bg, ng, 0.0, Cg, ng), "sgemm"),
+        "sgemm_tf32": mode_call(B.MATH_TF32, lambda: B.check(
+            B.iclblasSgemm(h, 0, 0, ng, ng, ng, 1.0, Ag, ng, Bg, ng, 0.0, Cg, ng), "sgemm")),
+        "strsm_3xbf16": mode_call(B.MATH_BF16X3, strsm),
+        "batched_trsm": lambda: (B.check(B.iclblasStrsmBatchedUneven(h, plan, 1.0, pA, pX), "batched"),
+                                 B.check(B.iclblasStrsmBatchedUnevenBackward(h, plan, 1.0, pA, pX, pG, pdA),
+                                         "batched adjoint")),
+    }
+    return cases, plan
+
+
+def run_kernel_cases(args, torch):
+    """Runs the named cases of kernel_cases (all, or --only a,b): --warmup
+    untimed calls, then --steps calls between two CUDA events; one JSON line
+    per case."""
+    from clgpu_b200 import iclblas as B
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(device=dev)
+    only = set(args.only.split(",")) if args.only else None
+    with B.Handle() as h, torch.cuda.stream(stream):
+        h.set_stream(stream)
+        cases, plan = kernel_cases(torch, dev, B, h)
+        torch.cuda.synchronize()
+        for name, f in cases.items():
+            if only and name not in only:
+                continue
+            for _ in range(args.warmup):
+                f()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.steps):
+                f()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            assert h.synchronize() == B.SUCCESS
+            print(json.dumps({"case": name, "ms_per_call": round(e0.elapsed_time(e1) / max(args.steps, 1), 4)}),
+                  flush=True)
+        plan.destroy()
 
 
 # ---------------------------------------------------------------- CPU (reference code)
@@ -1294,12 +1434,14 @@ def main():
                     help="skip the SGEMM 8192^3 / STRSM 8192x4096 / SGEMM 512^3 legs of the default run")
     ap.add_argument("--only", default="", help="comma-separated subset of the sweep's calls")
     ap.add_argument("--n1", type=int, default=N1, help="level-1 vector length (default 2^28)")
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "gemm", "trsm", "batched", "level1x", "level23x", "conv1x1"],
+    ap.add_argument("--workload", default="sweep",
+                    choices=["sweep", "gemm", "trsm", "batched", "level1x", "level23x", "conv1x1", "kernels"],
                     help="sweep: the bandwidth config (default); gemm / trsm / batched: the precision, "
                          "triangular-solve and batched-solve config studies; level1x: copy / swap / "
                          "rotation / iamin bandwidth study; level23x: ger / symv / hemv bandwidth and "
                          "syrk / syr2k / symm / trmm throughput study; conv1x1: ResNet-50 1x1-convolution "
-                         "GEMM shapes in HGEMM and every SGEMM mode")
+                         "GEMM shapes in HGEMM and every SGEMM mode; kernels: named single-routine "
+                         "cases (--only) for ncu captures")
     ap.add_argument("--trsm-m", type=int, default=8192)
     ap.add_argument("--trsm-n", type=int, default=4096)
     ap.add_argument("--trsv-n", type=int, default=16384)
@@ -1351,6 +1493,9 @@ def main():
         return
     if args.workload == "conv1x1":
         run_conv1x1_study(args, torch)
+        return
+    if args.workload == "kernels":
+        run_kernel_cases(args, torch)
         return
     if world > 1:
         torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))

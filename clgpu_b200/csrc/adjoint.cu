@@ -11,15 +11,18 @@
 // GEMM, C = alpha*op(A)*op(B) + beta*C:
 //     d op(A) = alpha * G op(B)^T,  d op(B) = alpha * op(A)^T G,  dC = beta * G.
 // The products run through the library's GEMM and TRSM (and so follow the
-// handle's math mode); one small kernel masks the triangle.
+// handle's math mode).  dA is formed by the triangular-output GEMM, which
+// computes only the tiles meeting the stored triangle; one small kernel then
+// zeroes the other triangle (and a unit diagonal).
 #include "common.cuh"
 
 namespace iclb {
 
 namespace {
 
-// Zero the entries of the n x n block that are not on the stored triangle;
-// with a unit diagonal the diagonal is not an input either.
+// Zero the entries of the n x n block that are not on the stored triangle
+// (the triangular-output GEMM leaves them untouched); with a unit diagonal
+// the diagonal is not an input either.
 __global__ void mask_triangle_kernel(int n, int lower, int unit, float* __restrict__ D, long ldd)
 {
     const long total = (long)n * n;
@@ -61,14 +64,16 @@ cudaError_t strsm_backward(iclblasHandle_t h, int side, int uplo, int trans, int
     if (e != cudaSuccess) return e;
     if (dA) {
         const int na = left ? m : n;
+        // only the stored triangle of dA is formed (1: row >= col, 2: row <= col)
+        const int tri = uplo == ICLBLAS_FILL_MODE_LOWER ? 1 : 2;
         if (left) {
             // dM = -W X^T (m x m, inner n); dA = dM or dM^T = -X W^T
-            e = t ? sgemm(h, ICLBLAS_OP_N, ICLBLAS_OP_T, m, m, n, -1.f, X, ldx, G, ldg, 0.f, dA, ldda)
-                  : sgemm(h, ICLBLAS_OP_N, ICLBLAS_OP_T, m, m, n, -1.f, G, ldg, X, ldx, 0.f, dA, ldda);
+            e = t ? sgemm_tri(h, tri, ICLBLAS_OP_N, ICLBLAS_OP_T, m, m, n, -1.f, X, ldx, G, ldg, 0.f, dA, ldda)
+                  : sgemm_tri(h, tri, ICLBLAS_OP_N, ICLBLAS_OP_T, m, m, n, -1.f, G, ldg, X, ldx, 0.f, dA, ldda);
         } else {
             // dM = -X^T W (n x n, inner m); dA = dM or dM^T = -W^T X
-            e = t ? sgemm(h, ICLBLAS_OP_T, ICLBLAS_OP_N, n, n, m, -1.f, G, ldg, X, ldx, 0.f, dA, ldda)
-                  : sgemm(h, ICLBLAS_OP_T, ICLBLAS_OP_N, n, n, m, -1.f, X, ldx, G, ldg, 0.f, dA, ldda);
+            e = t ? sgemm_tri(h, tri, ICLBLAS_OP_T, ICLBLAS_OP_N, n, n, m, -1.f, G, ldg, X, ldx, 0.f, dA, ldda)
+                  : sgemm_tri(h, tri, ICLBLAS_OP_T, ICLBLAS_OP_N, n, n, m, -1.f, X, ldx, G, ldg, 0.f, dA, ldda);
         }
         if (e != cudaSuccess) return e;
         mask_triangle_kernel<<<grid_for(h, (long)na * na), 256, 0, h->stream>>>(

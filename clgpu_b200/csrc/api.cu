@@ -116,7 +116,8 @@ public:
         o.in = in;
         const iclb::MemKind k = mem_kind(p, h_->device);
         foreign_ |= k == iclb::MemKind::OtherDevice;
-        o.staged = k == iclb::MemKind::Host;
+        o.pageable = k == iclb::MemKind::Pageable;
+        o.staged = k == iclb::MemKind::Host || o.pageable;
         o.dev = o.staged ? nullptr : o.user;
         return n_++;
     }
@@ -161,7 +162,10 @@ public:
             if (!o.staged) continue;
             any_staged_ = true;
             if (!o.in) continue;
-            e = cudaMemcpyAsync(o.dev, o.user, o.bytes, cudaMemcpyHostToDevice, h_->stream);
+            if (o.pageable && o.bytes >= kBounceMin)
+                e = iclb::copy_pageable_h2d(h_, o.dev, o.user, o.bytes);
+            else
+                e = cudaMemcpyAsync(o.dev, o.user, o.bytes, cudaMemcpyHostToDevice, h_->stream);
             if (e != cudaSuccess) return e;
         }
         return cudaSuccess;
@@ -188,6 +192,8 @@ public:
         for (int i = 0; i < n_; ++i) {
             any |= ops_[i].staged;
             total += ops_[i].bytes;
+            // pageable operands go through the bounce buffers of stage_in / finish
+            if (ops_[i].pageable) return cudaSuccess;
         }
         constexpr long kChunk = 1L << 24;  // elements per chunk
         if (!any || total < ((size_t)64 << 20) || n < 2 * kChunk) return cudaSuccess;
@@ -239,7 +245,9 @@ public:
         for (int i = 0; i < n_; ++i) {
             const Op& o = ops_[i];
             if (o.staged && o.out) {
-                cudaError_t e = cudaMemcpyAsync(o.user, o.dev, o.bytes, cudaMemcpyDeviceToHost, h_->stream);
+                cudaError_t e = (o.pageable && o.bytes >= kBounceMin)
+                                    ? iclb::copy_pageable_d2h(h_, o.user, o.dev, o.bytes)
+                                    : cudaMemcpyAsync(o.user, o.dev, o.bytes, cudaMemcpyDeviceToHost, h_->stream);
                 if (e != cudaSuccess) return e;
             }
         }
@@ -247,11 +255,14 @@ public:
     }
 
 private:
+    // pageable operands at least this large move through the bounce buffers
+    // (smaller ones: a plain copy, which the driver stages itself)
+    static constexpr size_t kBounceMin = (size_t)4 << 20;
     struct Op {
         void* user;
         void* dev;
         size_t bytes;
-        bool out, in, staged;
+        bool out, in, staged, pageable;
     };
     iclblasHandle_t h_;
     Op ops_[6];
@@ -430,6 +441,7 @@ extern "C" iclblasStatus_t iclblasDestroy(iclblasHandle_t handle)
             if (handle->chunk_ev[c]) cudaEventDestroy(handle->chunk_ev[c]);
         if (handle->fork_ev) cudaEventDestroy(handle->fork_ev);
         if (handle->join_ev) cudaEventDestroy(handle->join_ev);
+        iclb::free_bounce(handle);
         cudaFree(handle->ws.counters);
         cudaFree(handle->ws.dev_status);
         cudaStreamDestroy(handle->own_stream);
@@ -984,7 +996,8 @@ extern "C" iclblasStatus_t iclblasSgemv(iclblasHandle_t h, iclblasOperation_t tr
         Stager st(h);
         int ia = st.add(A, mat_extent(m, n, lda) * sizeof(float), false);
         int ix = st.add(x, vec_extent(xl, incx) * sizeof(float), false);
-        int iy = st.add(y, vec_extent(yl, incy) * sizeof(float), true);
+        // beta == 0: y is written without being read (contiguous y: nothing to copy in)
+        int iy = st.add(y, vec_extent(yl, incy) * sizeof(float), true, *beta != 0.f || incy != 1);
         cudaError_t e = st.stage_in();
         if (e == cudaSuccess)
             e = iclb::sgemv(h, trans, m, n, *alpha, st.dev<float>(ia), lda, st.dev<float>(ix), incx, *beta,
@@ -1012,7 +1025,8 @@ extern "C" iclblasStatus_t iclblasCgemv(iclblasHandle_t h, iclblasOperation_t tr
         Stager st(h);
         int ia = st.add(A, mat_extent(m, n, lda) * sizeof(cfloat), false);
         int ix = st.add(x, vec_extent(xl, incx) * sizeof(cfloat), false);
-        int iy = st.add(y, vec_extent(yl, incy) * sizeof(cfloat), true);
+        // beta == 0: y is written without being read (contiguous y: nothing to copy in)
+        int iy = st.add(y, vec_extent(yl, incy) * sizeof(cfloat), true, b.re != 0.f || b.im != 0.f || incy != 1);
         cudaError_t e = st.stage_in();
         if (e == cudaSuccess)
             e = iclb::cgemv(h, trans, m, n, a, st.dev<cfloat>(ia), lda, st.dev<cfloat>(ix), incx, b,
@@ -1205,7 +1219,8 @@ extern "C" iclblasStatus_t iclblasSgemm(iclblasHandle_t h, iclblasOperation_t tr
         Stager st(h);
         int ia = st.add(A, mat_extent(ar, ac, lda) * sizeof(float), false);
         int ib = st.add(B, mat_extent(br, bc, ldb) * sizeof(float), false);
-        int ic = st.add(C, mat_extent(m, n, ldc) * sizeof(float), true);
+        // beta == 0: C is written without being read (ldc == m: nothing to copy in)
+        int ic = st.add(C, mat_extent(m, n, ldc) * sizeof(float), true, *beta != 0.f || ldc != m);
         cudaError_t e = st.stage_in();
         if (e == cudaSuccess)
             e = iclb::sgemm(h, transa, transb, m, n, k, *alpha, st.dev<float>(ia), lda, st.dev<float>(ib), ldb, *beta,
@@ -1232,7 +1247,9 @@ extern "C" iclblasStatus_t iclblasCgemm(iclblasHandle_t h, iclblasOperation_t tr
         Stager st(h);
         int ia = st.add(A, mat_extent(ar, ac, lda) * sizeof(cfloat), false);
         int ib = st.add(B, mat_extent(br, bc, ldb) * sizeof(cfloat), false);
-        int ic = st.add(C, mat_extent(m, n, ldc) * sizeof(cfloat), true);
+        // beta == 0: C is written without being read (ldc == m: nothing to copy in)
+        const cfloat bv = cf(beta);
+        int ic = st.add(C, mat_extent(m, n, ldc) * sizeof(cfloat), true, bv.re != 0.f || bv.im != 0.f || ldc != m);
         cudaError_t e = st.stage_in();
         if (e == cudaSuccess)
             e = iclb::cgemm(h, transa, transb, m, n, k, cf(alpha), st.dev<cfloat>(ia), lda, st.dev<cfloat>(ib), ldb,
@@ -1361,7 +1378,8 @@ extern "C" iclblasStatus_t iclblasSsymm(iclblasHandle_t h, iclblasSideMode_t sid
         Stager st(h);
         int ia = st.add(A, mat_extent(na, na, lda) * sizeof(float), false);
         int ib = st.add(B, mat_extent(m, n, ldb) * sizeof(float), false);
-        int ic = st.add(C, mat_extent(m, n, ldc) * sizeof(float), true);
+        // beta == 0: C is written without being read (ldc == m: nothing to copy in)
+        int ic = st.add(C, mat_extent(m, n, ldc) * sizeof(float), true, *beta != 0.f || ldc != m);
         cudaError_t e = st.stage_in();
         if (e == cudaSuccess)
             e = iclb::ssymm(h, side, uplo, m, n, *alpha, st.dev<float>(ia), lda, st.dev<float>(ib), ldb, *beta,
@@ -1576,6 +1594,13 @@ extern "C" iclblasStatus_t iclblasBatchPlanGetInfo(iclblasBatchPlan_t plan, doub
     if (flops) *flops = plan->flops;
     if (tile_width) *tile_width = plan->main.rc;
     if (ctas_per_sm) *ctas_per_sm = plan->main.ctas_per_sm;
+    return ICLBLAS_STATUS_SUCCESS;
+}
+
+extern "C" iclblasStatus_t iclblasBatchPlanSetInverseReuse(iclblasBatchPlan_t plan, int reuse)
+{
+    if (!plan_ok(plan, 0) || (reuse != 0 && reuse != 1)) return ICLBLAS_STATUS_INVALID_VALUE;
+    plan->reuse_inv = reuse == 1;
     return ICLBLAS_STATUS_SUCCESS;
 }
 

@@ -980,6 +980,7 @@ cudaError_t batch_trsm(iclblasHandle_t h, const iclblasBatchPlan* p, float alpha
     cudaError_t e = launch_inv(h, p->inv_items, p->n_inv, p->main.dims, p->inv_off, lower_op, op,
                                p->diag == ICLBLAS_DIAG_UNIT, A, p->inv);
     if (e != cudaSuccess) return e;
+    p->inv_formed = true;
     return launch_trsm(h, p->main, p->counter, p->inv_off, p->inv, lower_op, op, 0, right, alpha, A, B);
 }
 
@@ -1005,7 +1006,9 @@ cudaError_t batch_trsm_backward(iclblasHandle_t h, const iclblasBatchPlan* p, fl
     // the adjoint solves with the transposed operator, reading them transposed
     const int f_lower = lower_op_of(p->uplo, p->trans) ^ (right ? 1 : 0);
     const int f_op = op ^ (right ? 1 : 0);
-    cudaError_t e = launch_inv(h, p->inv_items, p->n_inv, p->main.dims, p->inv_off, f_lower, f_op, unit, A, p->inv);
+    cudaError_t e = cudaSuccess;
+    if (!(p->reuse_inv && p->inv_formed))
+        e = launch_inv(h, p->inv_items, p->n_inv, p->main.dims, p->inv_off, f_lower, f_op, unit, A, p->inv);
     if (e == cudaSuccess)
         e = launch_trsm(h, p->main, p->counter, p->inv_off, p->inv, !f_lower, !f_op, 1, right, alpha, A, G);
     if (e != cudaSuccess || !dA) return e;

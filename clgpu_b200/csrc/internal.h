@@ -108,6 +108,11 @@ struct iclblasContext {
     // Fork / join of work on the second stream within one call (created on
     // first use).
     cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+    // Two pinned bounce buffers for copies of pageable host memory, each with
+    // the event of the last copy that used it (allocated on first use).
+    void* bounce[2] = {nullptr, nullptr};
+    cudaEvent_t bounce_ev[2] = {nullptr, nullptr};
+    bool bounce_busy[2] = {false, false};
 };
 
 namespace iclb {
@@ -155,6 +160,16 @@ private:
     iclblasHandle_t h_;
     cudaStream_t saved_;
 };
+
+// Copies between pageable host memory and the device through the handle's
+// pinned bounce buffers (host_copy.cu), on the handle's stream: h2d returns
+// once every chunk has been handed to the DMA engine (later work on the
+// stream sees the data), d2h once the data is in host memory.
+cudaError_t copy_pageable_h2d(iclblasHandle_t h, void* dst_dev, const void* src_host, size_t bytes);
+cudaError_t copy_pageable_d2h(iclblasHandle_t h, void* dst_host, const void* src_dev, size_t bytes);
+cudaError_t free_bounce(iclblasHandle_t h);
+// memcpy between host buffers on the process-wide pool of copy threads.
+void host_copy(void* dst, const void* src, size_t bytes);
 
 // Returns scratch of at least `bytes` (256-byte aligned) or nullptr.
 void* scratch(iclblasHandle_t h, size_t bytes);
@@ -291,6 +306,10 @@ struct iclblasBatchPlan {
     long* inv_off = nullptr;
     int2* inv_items = nullptr;
     int n_inv = 0;
+    // the backward call may use the inverses of the last forward call
+    // (iclblasBatchPlanSetInverseReuse); inv_formed: a forward call formed them
+    bool reuse_inv = false;
+    mutable bool inv_formed = false;
 };
 
 namespace iclb {

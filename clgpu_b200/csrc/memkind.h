@@ -10,16 +10,18 @@
 namespace iclb {
 
 enum class MemKind {
-    Host = 0,          // staged through the handle's device buffer
+    Host = 0,          // pinned (page-locked) host memory: staged by direct DMA
     Device = 1,        // the handle's GPU (or managed memory): used in place
     OtherDevice = 2,   // another GPU's memory: rejected (INVALID_VALUE)
+    Pageable = 3,      // ordinary host memory: staged through pinned bounce buffers
 };
 
 inline MemKind classify_memory(int memory_type, int pointer_device, int handle_device)
 {
     if (memory_type == 3) return MemKind::Device;
     if (memory_type == 2) return pointer_device == handle_device ? MemKind::Device : MemKind::OtherDevice;
-    return MemKind::Host;
+    if (memory_type == 1) return MemKind::Host;
+    return MemKind::Pageable;
 }
 
 }  // namespace iclb

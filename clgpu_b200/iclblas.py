@@ -124,6 +124,7 @@ _SIGS = {
     "iclblasSgemmBatchedPlanCreate": [_H, _I, _I, _I, _P, _P, _P, _P, _P, _P, C.POINTER(_P)],
     "iclblasBatchPlanDestroy": [_P],
     "iclblasBatchPlanGetInfo": [_P, C.POINTER(C.c_double), C.POINTER(_I), C.POINTER(_I)],
+    "iclblasBatchPlanSetInverseReuse": [_P, _I],
     "iclblasStrsmBatchedUneven": [_H, _P, _P, _P, _P],
     "iclblasSgemmBatchedUneven": [_H, _P, _P, _P, _P, _P, _P],
     "iclblasStrsmBatchedUnevenBackward": [_H, _P, _P, _P, _P, _P, _P],
@@ -481,6 +482,10 @@ class BatchPlan:
         f, w, c = C.c_double(), C.c_int(), C.c_int()
         check(_call("iclblasBatchPlanGetInfo", self.value, C.byref(f), C.byref(w), C.byref(c)))
         return f.value, w.value, c.value
+
+    def set_inverse_reuse(self, reuse: bool) -> int:
+        """TRSM plans: the backward call reuses the forward call's inverses."""
+        return _call("iclblasBatchPlanSetInverseReuse", self.value, 1 if reuse else 0)
 
     def destroy(self):
         if self.value:

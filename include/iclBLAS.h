@@ -372,6 +372,14 @@ ICLBLAS_API iclblasStatus_t iclblasBatchPlanDestroy(iclblasBatchPlan_t plan);
  * tuned launch shape (tile width, CTAs per SM); any output may be NULL. */
 ICLBLAS_API iclblasStatus_t iclblasBatchPlanGetInfo(iclblasBatchPlan_t plan, double* flops, int* tile_width,
                                                     int* ctas_per_sm);
+/* TRSM plans: with reuse = 1, iclblasStrsmBatchedUnevenBackward uses the
+ * diagonal-block inverses formed by the plan's most recent
+ * iclblasStrsmBatchedUneven call instead of forming them again (it forms
+ * them when no forward call has run yet).  The caller promises that the
+ * triangles A_i are unchanged since that forward call and that the two
+ * calls run in order on one stream.  0 (the default) forms them in every
+ * call.  INVALID_VALUE for a GEMM plan or another value. */
+ICLBLAS_API iclblasStatus_t iclblasBatchPlanSetInverseReuse(iclblasBatchPlan_t plan, int reuse);
 ICLBLAS_API iclblasStatus_t iclblasStrsmBatchedUneven(iclblasHandle_t handle, iclblasBatchPlan_t plan,
                                                       const float* alpha, const float* const* A, float* const* B);
 ICLBLAS_API iclblasStatus_t iclblasSgemmBatchedUneven(iclblasHandle_t handle, iclblasBatchPlan_t plan,

@@ -304,3 +304,36 @@ def test_tune_cache_file(tmp_path):
     assert r2.returncode == 0, r2.stderr
     assert r1.stdout.split() == r2.stdout.split()
     assert len(cache.read_text().splitlines()) == 1   # read back, not re-tuned
+
+
+def test_batched_adjoint_reuses_forward_inverses(handle, cuda):
+    """With inverse reuse the adjoint skips forming the diagonal-block
+    inverses and uses the forward call's: results bit-identical to a plan
+    that forms them again.  GEMM plans have no inverses to reuse."""
+    handle.set_stream(torch.cuda.current_stream())
+    rng = np.random.default_rng(31)
+    batch = 17
+    ms, ns = rng.integers(1, 400, batch), rng.integers(1, 90, batch)
+    As = [tri_np(int(m), True, rng) for m in ms]
+    Bs = [rng.standard_normal(int(m) * int(n)).astype(np.float32) for m, n in zip(ms, ns)]
+    Gs = [rng.standard_normal(int(m) * int(n)).astype(np.float32) for m, n in zip(ms, ns)]
+    kw = dict(side=0, uplo=1, trans=0, diag=0, m=list(ms), n=list(ns), lda=list(ms), ldb=list(ms))
+    outs = []
+    for reuse in (False, True):
+        plan = B.BatchPlan(handle, "trsm", **kw)
+        assert plan.set_inverse_reuse(reuse) == B.SUCCESS
+        dA = [torch.from_numpy(a).to(cuda) for a in As]
+        dX = [torch.from_numpy(b).to(cuda) for b in Bs]
+        dG = [torch.from_numpy(g).to(cuda) for g in Gs]
+        ddA = [torch.empty(int(m) * int(m), device=cuda) for m in ms]
+        pa, px, pg, pda = ptrs(dA, cuda), ptrs(dX, cuda), ptrs(dG, cuda), ptrs(ddA, cuda)
+        assert B.iclblasStrsmBatchedUneven(handle, plan, 0.5, pa, px) == B.SUCCESS
+        assert B.iclblasStrsmBatchedUnevenBackward(handle, plan, 0.5, pa, px, pg, pda) == B.SUCCESS
+        torch.cuda.synchronize()
+        outs.append([t.cpu().numpy() for t in dX + dG + ddA])
+        plan.destroy()
+    for a, b in zip(*outs):
+        assert np.array_equal(a, b)
+    gplan = B.BatchPlan(handle, "gemm", transa=0, transb=0, m=[4], n=[4], k=[4], lda=[4], ldb=[4], ldc=[4])
+    assert gplan.set_inverse_reuse(True) == B.INVALID_VALUE
+    gplan.destroy()

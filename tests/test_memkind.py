@@ -1,9 +1,10 @@
 """The rule that decides how the library treats an array argument
-(clgpu_b200/csrc/memkind.h), checked on the CPU: host memory is staged,
-memory of the handle's GPU (or managed memory) is used in place, and device
-memory of any other GPU is rejected before a copy or a kernel could touch
-it.  The header has no CUDA dependency, so it compiles here with g++ alone;
-no kernel is launched."""
+(clgpu_b200/csrc/memkind.h), checked on the CPU: pinned host memory is
+staged by direct DMA, ordinary (pageable) host memory through the handle's
+pinned bounce buffers, memory of the handle's GPU (or managed memory) is used
+in place, and device memory of any other GPU is rejected before a copy or a
+kernel could touch it.  The header has no CUDA dependency, so it compiles
+here with g++ alone; no kernel is launched."""
 import os
 import shutil
 import subprocess
@@ -21,7 +22,7 @@ int main() {
     int bad = 0;
     // cudaMemoryType: 0 unregistered, 1 host (pinned), 2 device, 3 managed
     struct { int type, ptr_dev, handle_dev; MemKind want; } cases[] = {
-        {0, -2, 0, MemKind::Host},          // malloc'd memory
+        {0, -2, 0, MemKind::Pageable},      // malloc'd memory: through the pinned bounce buffers
         {1, 0, 0, MemKind::Host},           // pinned host memory is staged too
         {1, 3, 0, MemKind::Host},
         {2, 0, 0, MemKind::Device},         // the handle's GPU
