@@ -236,11 +236,20 @@ cudaError_t launch(iclblasHandle_t h, int ta, int tb, int m, int n, int k, T alp
 cudaError_t sgemm_simt(iclblasHandle_t h, int ta, int tb, int m, int n, int k, float alpha, const float* A, int lda,
                        const float* B, int ldb, float beta, float* C, int ldc, int tri)
 {
-    long big_tiles = (long)ceil_div(m, 128) * ceil_div(n, 128);
-    if (tri != 0) big_tiles = (big_tiles + std::min(ceil_div(m, 128), ceil_div(n, 128))) / 2;
-    if (big_tiles >= h->sm_count)
+    // the largest tile that still gives every SM a CTA: 128 x 128 (256
+    // threads, 8 x 8 outputs each), 64 x 64 (256 threads, 4 x 4), or for small
+    // products 32 x 32 (64 threads, 4 x 4; config 1's 512^3 has 16 tiles of
+    // 128 x 128 and 64 of 64 x 64)
+    auto tiles = [&](int t) {
+        long c = (long)ceil_div(m, t) * ceil_div(n, t);
+        if (tri != 0) c = (c + std::min(ceil_div(m, t), ceil_div(n, t))) / 2;
+        return c;
+    };
+    if (tiles(128) >= h->sm_count)
         return launch<float, 128, 128, 16, 8, 8>(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, tri);
-    return launch<float, 64, 64, 8, 4, 4>(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, tri);
+    if (tiles(64) >= h->sm_count)
+        return launch<float, 64, 64, 8, 4, 4>(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, tri);
+    return launch<float, 32, 32, 8, 4, 4>(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, tri);
 }
 
 cudaError_t cgemm_simt(iclblasHandle_t h, int ta, int tb, int m, int n, int k, cfloat alpha, const cfloat* A, int lda,
