@@ -41,6 +41,10 @@ __device__ __forceinline__ unsigned long long global_ns()
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
 }
+// Orders this thread's earlier shared-memory accesses (generic proxy) before
+// later TMA (async proxy) accesses of the same bytes; a barrier after it
+// extends that to the thread that issues the copy.
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 // Waits for phase `parity` of `bar` for at most `limit_ns`; false on timeout.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, unsigned long long limit_ns)
 {

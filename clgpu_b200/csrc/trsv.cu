@@ -19,6 +19,8 @@
 // kDevWaitTimeout in the device status word and every other CTA, which also
 // polls that word, returns; the host reports EXECUTION_FAILED.  Reads of
 // other CTAs' results go through L2 (ld.cg) so no stale L1 line is used.
+#include <atomic>
+#include <cstddef>
 #include <type_traits>
 
 #include "common.cuh"
@@ -221,55 +223,87 @@ __global__ void __launch_bounds__(kThreads) trsv_kernel(int n, int lower_op, int
 // ---------------------------------------------------------------- STRSV, TMA path
 // Float TRSV when A is 16-byte aligned with lda a multiple of 4 and >= n
 // (the usual case).  Same ticket-ordered one-launch structure as above, with
-// changes that shorten the chain of dependent block solves:
-//   - tiles arrive by TMA (one 64 x 64 box per cp.async.bulk.tensor) into a
-//     4-stage shared-memory ring, so up to 64 KiB per CTA are in flight while
-//     the CTA waits for earlier blocks, and two CTAs fit on an SM;
-//   - the first box is the diagonal block D, inverted in FP64 (then kept in
-//     FP32) before the CTA needs it; the second box is the tile T next to D
-//     (the block solved just before this one), turned into W = inv(D) T
-//     while earlier blocks are still being solved; then the remaining tiles
-//     in solve order.  Once all but the last earlier block are known, the CTA
-//     forms z = inv(D) (b - sum of those tiles' products), so its own step of
-//     the chain, when the last block x_prev is published, is
-//     x = z - W x_prev: one 64 x 64 product and a publication;
+// blocks of RB = 128 rows, one CTA of 256 threads per block (one CTA per SM),
+// and changes that shorten the chain of dependent block solves:
+//   - tiles arrive by TMA (boxes of 128 rows x 64 columns of op(A), half a
+//     block's columns each) into a 6-stage shared-memory ring, so 192 KiB per
+//     CTA are in flight while the CTA waits for earlier blocks;
+//   - the first two boxes are the diagonal block D, inverted in FP64: both
+//     64 x 64 diagonal halves at once (16 x 16 blocks by substitution, then
+//     two doubling steps), then the off-diagonal half from those two
+//     (-inv(D22) D21 inv(D11) for a lower D), each product register-tiled.
+//     The inverse is kept in FP32 in registers: each thread holds 4 rows x
+//     16 columns, so a product with a vector takes 4 16-byte shared-memory
+//     reads per thread (not 64 broadcast words: 8 warps reading a vector
+//     word by word spend the SM's shared-memory bandwidth) and a butterfly
+//     over the 8 lanes sharing the rows.  The FP64 workspace overlays the
+//     ring before the ring is used;
+//   - the next two boxes are the tile T next to D (the block solved just
+//     before this one), kept in registers in the same layout; then the
+//     remaining tiles in solve order, consumed with 16-byte reads along the
+//     stage's contiguous direction into per-thread partial row sums.  Once
+//     all but the last earlier block are known, the CTA holds
+//     y = b - (sum of those tiles' products), so its own step of the chain,
+//     when the last block x_prev is published, is x = inv(D) (y - T x_prev):
+//     two register products with one barrier between them, and the
+//     publication;
 //   - each solved entry is published as one 64-bit word (value, call epoch):
 //     a consumer polls the entries it needs directly, with no separate flag.
 //     The epoch lives in device memory: each CTA reads the last launch's
 //     epoch at its start and uses the next one; the CTA that solves the last
 //     block stores it back once everything is published (every other CTA has
 //     read it by then), so replays of a captured launch get fresh epochs;
-//   - launched as clusters of 8 consecutive blocks (when the GPU can place
-//     one), a solved block also goes straight into the shared memory of the
-//     later CTAs of its cluster (st.async on a transaction barrier), and the
-//     chain step runs on the 64 row threads alone, with no block-wide
-//     barrier between the arrival of x_prev and the hand-off of x.  At
-//     n = 16384 this took the call from 314 to 265 us, and the blocked FP64
-//     inverse below (13 instead of 44 us at the start) to 230 us.
-constexpr int FS = 4;
-constexpr int TILE_ELEMS = NB * NB;
+//   - launched as clusters of CL consecutive blocks, a solved block also goes
+//     straight into the shared memory of the later CTAs of its cluster
+//     (st.async on a transaction barrier), so CL - 1 of every CL steps of the
+//     chain skip the global-memory round trip.  CL is the largest of 8, 4, 2
+//     for which the GPU holds every cluster of the launch at once (a cluster
+//     that can only start when another has finished starts its own setup
+//     late and then streams its tiles alone).
+// Against 64-row blocks (two CTAs per SM, n = 16384 in 230 us) the chain has
+// half the steps and half the hand-offs between clusters.
+constexpr int RB = 128;  // rows (and columns) of a block
+constexpr int HB = 64;   // columns of op(A) in one stage
+constexpr int STAGE_ELEMS = RB * HB;
+constexpr int FS = 6;
 constexpr int kMaxCluster = 8;
+constexpr int XQ = 8 * 20;  // a block's 128 entries in shared memory: 8 groups of 16, 20 floats apart
 constexpr unsigned long long kTrsvWaitNs = 2000000000ull;  // a wait gives up after 2 s
 
+// shared-memory index of entry c (0 .. 127) of a block's entries (the
+// padding keeps the 16-byte reads of 8 threads with different groups in
+// different banks)
+__device__ __forceinline__ int qidx(int c) { return (c >> 4) * 20 + (c & 15); }
+
+// FP64 workspace of the diagonal-block inverse, in doubles: the inverses of
+// the two 64 x 64 diagonal halves, the off-diagonal half, and two doubling
+// temporaries.  It starts at stage 2 of the ring.
+constexpr int kY = HB * (HB + 1);
+constexpr int kTm = 32 * 33;
+constexpr int kInvDoubles = 3 * kY + 2 * kTm;
+static_assert(kInvDoubles * 8 <= (FS - 2) * STAGE_ELEMS * 4, "inverse workspace inside the ring");
+
 struct FastSmem {
-    float stage[FS][TILE_ELEMS];
-    // FP64 inverse while it is formed; then the same bytes hold the FP32
-    // inverse and W (two [NB][NB + 1] float arrays)
-    double R[NB][NB + 1];
-    double Tm[NB / 2][NB / 2 + 1];  // inverse doubling temporary (and 1 / diagonal before it)
-    float xs[NB];
-    float ys[NB];
-    float zs[NB];
-    float part[4][NB];
+    float stage[FS][STAGE_ELEMS];
     // cluster launches: the solved blocks of the earlier CTAs of this
     // cluster, delivered into this CTA's shared memory by st.async, one
     // transaction barrier per source rank
-    float xin[kMaxCluster][NB];
+    float xin[kMaxCluster][XQ];
+    float xs[XQ];  // entries of the block being streamed, from the published words
+    float xp[XQ];  // x_prev, from the published words
+    float y[XQ];   // b - the products of the tiles of blocks 0 .. s-2
+    float y2[XQ];  // y - T x_prev
+    float part[16][RB];  // partial row sums of the streamed tiles
     uint64_t xbar[kMaxCluster];
     uint64_t full[FS];
     unsigned s, epoch, cl;
     int failed;  // a wait of the chain step gave up
 };
+static_assert(sizeof(FastSmem) + 1024 <= 232448, "STRSV shared memory");
+static_assert(offsetof(FastSmem, xin) % 16 == 0 && offsetof(FastSmem, xs) % 16 == 0 &&
+                  offsetof(FastSmem, xp) % 16 == 0 && offsetof(FastSmem, y) % 16 == 0 &&
+                  offsetof(FastSmem, y2) % 16 == 0,
+              "16-byte reads of block entries");
 
 __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p)
 {
@@ -332,6 +366,47 @@ __device__ __forceinline__ bool xbar_wait_bounded(uint64_t* bar, unsigned long l
         if (tma::global_ns() - t0 > limit_ns) return false;
     return true;
 }
+// polls a published (value, epoch) word until it carries `epoch`; false when
+// the wait gives up or another CTA has recorded a failure
+__device__ __forceinline__ bool poll_word(const unsigned long long* src, unsigned epoch, const int* status,
+                                          float& v)
+{
+    unsigned long long w = ld_relaxed_u64(src);
+    if ((unsigned)(w >> 32) != epoch) {
+        const unsigned long long t0 = tma::global_ns();
+        for (;;) {
+            w = ld_relaxed_u64(src);
+            if ((unsigned)(w >> 32) == epoch) break;
+            if (ld_volatile(status) != kDevOk || tma::global_ns() - t0 > kTrsvWaitNs) return false;
+        }
+    }
+    v = __uint_as_float((unsigned)w);
+    return true;
+}
+
+// FP64 product tile of the diagonal-block inverse: acc(i, j) = sum_k A(r, k)
+// B(k, c) for rows r = r0 + i*rs and columns c = c0 + j*cs (interleaved, so
+// that a warp reads consecutive columns of B and few rows of A)
+template <int TR, int TC, int K, class FA, class FB>
+__device__ __forceinline__ void dtile(double (&acc)[TR][TC], int r0, int rs, int c0, int cs, FA A, FB B)
+{
+#pragma unroll
+    for (int i = 0; i < TR; ++i)
+#pragma unroll
+        for (int j = 0; j < TC; ++j) acc[i][j] = 0.0;
+#pragma unroll 4
+    for (int k = 0; k < K; ++k) {
+        double a[TR], b[TC];
+#pragma unroll
+        for (int i = 0; i < TR; ++i) a[i] = A(r0 + i * rs, k);
+#pragma unroll
+        for (int j = 0; j < TC; ++j) b[j] = B(k, c0 + j * cs);
+#pragma unroll
+        for (int i = 0; i < TR; ++i)
+#pragma unroll
+            for (int j = 0; j < TC; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+}
 
 // CL = 1: one CTA per block, every solved block handed on through global
 // memory.  CL > 1 (a cluster launch): the CTAs of a cluster solve CL
@@ -343,16 +418,16 @@ __device__ __forceinline__ bool xbar_wait_bounded(uint64_t* bar, unsigned long l
 // barrier before it exits, so no CTA leaves while another may still write
 // into its shared memory.
 template <int CL>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, 1)
     strsv_tma_kernel(const __grid_constant__ CUtensorMap amap, int n, int lower_op, int op, int unit, float* x,
                      long incx, unsigned long long* pub, unsigned* ticket, unsigned* epoch_word, int* status)
 {
     extern __shared__ unsigned char smem_raw[];
-    FastSmem& S = *reinterpret_cast<FastSmem*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    float(*IV)[NB + 1] = reinterpret_cast<float(*)[NB + 1]>(&S.R[0][0]);
-    float(*W)[NB + 1] = IV + NB;
+    // 1024-byte aligned; an offset from the array (not an integer cast) keeps
+    // the accesses in the shared address space
+    FastSmem& S = *reinterpret_cast<FastSmem*>(smem_raw + ((1024u - (tma::smem_u32(smem_raw) & 1023u)) & 1023u));
     const int t = threadIdx.x;
-    const int nb = (n + NB - 1) / NB;
+    const int nb = (n + RB - 1) / RB;
     const unsigned rank = CL > 1 ? cluster_rank() : 0u;
     if (t == 0) {
         unsigned e = *(volatile unsigned*)epoch_word + 1u;
@@ -361,10 +436,10 @@ __global__ void __launch_bounds__(kThreads, 2)
         for (int i = 0; i < FS; ++i) tma::mbar_init(&S.full[i], 1);
         S.failed = 0;
         if constexpr (CL > 1) {
-            // one arrival (this one, declaring the bytes) plus NB floats per earlier rank
+            // one arrival (this one, declaring the bytes) plus RB floats per earlier rank
             for (unsigned r = 0; r < (unsigned)CL; ++r) tma::mbar_init(&S.xbar[r], 1);
             tma::mbar_init_fence();
-            for (unsigned r = 0; r < rank; ++r) tma::mbar_expect_tx(&S.xbar[r], NB * 4);
+            for (unsigned r = 0; r < rank; ++r) tma::mbar_expect_tx(&S.xbar[r], RB * 4);
         } else {
             tma::mbar_init_fence();
         }
@@ -392,30 +467,35 @@ __global__ void __launch_bounds__(kThreads, 2)
         return;
     }
     auto blk = [&](int p) { return lower_op ? p : nb - 1 - p; };
-    const int kb = blk(s), r0 = kb * NB, nr = min(NB, n - r0);
-    // loads: 0 the diagonal block, 1 the tile of block s-1 (s >= 1), then the
-    // tiles of blocks 0 .. s-2 in solve order
-    const int nloads = s + 1;
-    auto load_block = [&](int i) { return i == 0 ? kb : (i == 1 ? blk(s - 1) : blk(i - 2)); };
+    const int kb = blk(s), r0 = kb * RB, nr = min(RB, n - r0);
+    // loads, numbered: 0 and 1 the two halves of D; 2 and 3 the halves of the
+    // tile of block s-1 (s >= 1); then 4 + 2i + h half h of the tile of block
+    // i, i = 0 .. s-2 in solve order.  Load L goes to stage L % FS and
+    // completes phase L / FS of that stage's barrier; it is issued once load
+    // L - FS has been consumed.
+    const int nloads = s == 0 ? 2 : 4 + 2 * (s - 1);
     int issued = 0;  // (thread 0)
-    auto issue = [&](int i) {
-        issued = i + 1;
-        const int cb = load_block(i);
-        uint64_t* bar = &S.full[i % FS];
-        tma::mbar_expect_tx(bar, TILE_ELEMS * 4);
-        if (op == 0) tma::load_2d(S.stage[i % FS], &amap, r0, cb * NB, bar);   // A[r0.., cb*NB..]
-        else tma::load_2d(S.stage[i % FS], &amap, cb * NB, r0, bar);           // A[cb*NB.., r0..]
+    auto issue = [&](int L) {
+        issued = L + 1;
+        const int cb = L < 2 ? kb : (L < 4 ? blk(s - 1) : blk((L - 4) >> 1));
+        const int c = cb * RB + (L & 1) * HB;
+        uint64_t* bar = &S.full[L % FS];
+        tma::mbar_expect_tx(bar, STAGE_ELEMS * 4);
+        if (op == 0) tma::load_2d(S.stage[L % FS], &amap, r0, c, bar);  // A[r0 .. +127, c .. +63]
+        else tma::load_2d(S.stage[L % FS], &amap, c, r0, bar);          // A[c .. +63, r0 .. +127]
     };
-    if (t == 0)
-        for (int i = 0; i < min(FS, nloads); ++i) issue(i);
-    const float b = t < nr ? x[(long)(r0 + t) * incx] : 0.f;
+    auto wait_load = [&](int L) { return tma::mbar_wait_bounded(&S.full[L % FS], (L / FS) & 1, kTrsvWaitNs); };
+    if (t == 0) {
+        issue(0);
+        issue(1);
+    }
+    const float b = (t < nr) ? x[(long)(r0 + t) * incx] : 0.f;  // (threads t < RB)
     // on a failed wait: record it, let this CTA's copies still in flight land
     // (each wait bounded), then leave
     auto bail = [&](int consumed) {
         if (t == 0) {
             atomicOr(status, (int)kDevWaitTimeout);
-            for (int j = consumed; j < issued; ++j)
-                tma::mbar_wait_bounded(&S.full[j % FS], (j / FS) & 1, kTrsvWaitNs);
+            for (int L = consumed; L < issued; ++L) wait_load(L);
             // bytes other CTAs of the cluster may still be sending here
             if constexpr (CL > 1)
                 for (unsigned r = 0; r < rank; ++r) xbar_wait_bounded(&S.xbar[r], kTrsvWaitNs);
@@ -425,303 +505,352 @@ __global__ void __launch_bounds__(kThreads, 2)
             cluster_sync_all();
         }
     };
-    // waits for the solved entries of the block with solve index p (row c0,
-    // nc rows): from this CTA's shared memory when an earlier CTA of the
-    // cluster solved it, else from the published words (threads t < 64 poll)
-    auto fetch_x = [&](int p, int c0, int nc) -> int {
-        int bad = 0;
+    // the solved entries of the block with solve index p: this CTA's own
+    // shared memory when an earlier CTA of the cluster solved it (every
+    // thread waits on the transaction barrier), else the published words
+    // (threads t < RB poll, into `buf`; the caller's barrier publishes them)
+    auto fetch_x = [&](int p, float* buf, int& bad) -> const float* {
         if (CL > 1 && p >= cfirst) {
-            const int src = p - cfirst;
-            if (t < NB) {
-                if (!xbar_wait_bounded(&S.xbar[src], kTrsvWaitNs)) {
-                    atomicOr(status, (int)kDevWaitTimeout);
-                    bad = 1;
-                }
-                S.xs[t] = t < nc ? S.xin[src][t] : 0.f;
+            if (!xbar_wait_bounded(&S.xbar[p - cfirst], kTrsvWaitNs)) {
+                atomicOr(status, (int)kDevWaitTimeout);
+                bad = 1;
             }
-            return bad;
+            return S.xin[p - cfirst];
         }
-        if (t < NB) {
+        const int c0 = blk(p) * RB, nc = min(RB, n - c0);
+        if (t < RB) {
             float v = 0.f;
-            if (t < nc) {
-                const unsigned long long* src = pub + c0 + t;
-                unsigned long long w = ld_relaxed_u64(src);
-                if ((unsigned)(w >> 32) != epoch) {
-                    const unsigned long long t0 = tma::global_ns();
-                    for (;;) {
-                        w = ld_relaxed_u64(src);
-                        if ((unsigned)(w >> 32) == epoch) break;
-                        if (ld_volatile(status) != kDevOk) { bad = 1; break; }
-                        if (tma::global_ns() - t0 > kTrsvWaitNs) {
-                            atomicOr(status, (int)kDevWaitTimeout);
-                            bad = 1;
-                            break;
-                        }
-                    }
-                }
-                v = __uint_as_float((unsigned)w);
+            if (t < nc && !poll_word(pub + c0 + t, epoch, status, v)) {
+                atomicOr(status, (int)kDevWaitTimeout);
+                bad = 1;
             }
-            S.xs[t] = v;
+            buf[qidx(t)] = v;
         }
-        return bad;
+        return buf;
     };
-    const int rN = t % NB, gN = t / NB;      // row, group of 16 columns
-    // element (r, c) of the op(A) tile in a stage
-    auto tile = [&](const float* T, int r, int c) { return op == 0 ? T[c * NB + r] : T[r * NB + c]; };
+    // op(A) element (r, c) of a stage: r < 128, c < 64
+    auto el = [&](const float* T, int r, int c) { return op == 0 ? T[c * RB + r] : T[r * HB + c]; };
+    // register layout of a 128 x 128 matrix (inv(D), and the tile of block
+    // s-1): the thread holds rows R0 .. R0+3, columns cg*16 .. cg*16+15
+    const int lane = t & 31, warp = t >> 5;
+    const int cg = lane & 7, R0 = warp * 16 + (lane >> 3) * 4;
+    // out[k] = row R0+k of M times v (v in the block-entry layout), in every
+    // lane of the 8 that share the rows: 4 16-byte reads, 64 FMAs, and a
+    // butterfly over the column groups
+    auto mv = [&](const float(&m)[4][16], const float* v, float(&out)[4]) {
+        const float* vp = v + cg * 20;
+        float4 q[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) q[i] = *reinterpret_cast<const float4*>(vp + 4 * i);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            float a0 = 0.f, a1 = 0.f;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                a0 = fmaf(m[k][4 * i], q[i].x, a0);
+                a1 = fmaf(m[k][4 * i + 1], q[i].y, a1);
+                a0 = fmaf(m[k][4 * i + 2], q[i].z, a0);
+                a1 = fmaf(m[k][4 * i + 3], q[i].w, a1);
+            }
+            out[k] = a0 + a1;
+        }
+#pragma unroll
+        for (int o = 1; o < 8; o <<= 1)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) out[k] += __shfl_xor_sync(0xffffffffu, out[k], o);
+    };
+    auto pick = [](const float(&o)[4], int k) { return k == 0 ? o[0] : (k == 1 ? o[1] : (k == 2 ? o[2] : o[3])); };
 
-    // ---- diagonal block: FP64 inverse, then FP32
-    int bad = tma::mbar_wait_bounded(&S.full[0], 0, kTrsvWaitNs) ? 0 : 1;
+    // ---- diagonal block: FP64 inverse, kept in FP32 registers
+    int bad = (wait_load(0) && wait_load(1)) ? 0 : 1;
     if (__syncthreads_or(bad)) {
         bail(0);
         return;
     }
+    float iv[4][16];  // inv(D)[R0 + k][cg*16 + j]
     {
-        // Blocked FP64 inverse on all threads: the four 16 x 16 diagonal
-        // blocks by substitution (one column per thread), then two doubling
-        // steps that form the off-diagonal blocks from products of the known
-        // inverses (16 -> 32 -> 64).  Rows and columns past nr are an identity
-        // (the box holds zeros there) and are cut off when the inverse is
-        // stored in FP32.  (One column per thread over all 64 rows took 44 us
-        // of every call's start.)
-        const float* D = S.stage[0];
-        auto d = [&](int r, int c) -> double { return (double)tile(D, r, c); };
-        double* rd = &S.Tm[0][0];  // 1 / diagonal, then the doubling temporary
-        for (int idx = t; idx < TILE_ELEMS; idx += kThreads) S.R[idx % NB][idx / NB] = 0.0;
-        if (t < NB) rd[t] = (unit || t >= nr) ? 1.0 : 1.0 / d(t, t);
+        double* ws = reinterpret_cast<double*>(&S.stage[2][0]);
+        double(*Y)[HB][HB + 1] = reinterpret_cast<double(*)[HB][HB + 1]>(ws);   // inverses of D11, D22
+        double(*Yc)[HB + 1] = reinterpret_cast<double(*)[HB + 1]>(ws + 2 * kY);  // the off-diagonal half
+        double(*Tm)[32][33] = reinterpret_cast<double(*)[32][33]>(ws + 3 * kY);  // doubling temporaries
+        // element (r, c) of D, r, c < 128; rows and columns past nr are zero (box fill)
+        auto d = [&](int r, int c) -> double { return (double)el(S.stage[c >> 6], r, c & (HB - 1)); };
+        double* rd = &Tm[0][0][0];  // 1 / diagonal, until the doubling steps use Tm
+        for (int idx = t; idx < 2 * kY; idx += kThreads) (&Y[0][0][0])[idx] = 0.0;
+        if (t < RB) rd[t] = (unit || t >= nr) ? 1.0 : 1.0 / d(t, t);
         __syncthreads();
-        if (t < NB) {
-            // thread t owns column j of diagonal block b; the column stays in
-            // registers (loops unrolled: the D reads pipeline)
-            const int b = (t / 16) * 16, j = t % 16;
+        if (t < RB) {
+            // thread t owns column j of the 16 x 16 diagonal block at b of
+            // half hb; the column stays in registers
+            const int hb = t >> 6, b = ((t & (HB - 1)) >> 4) * 16, j = t & 15, o = hb * HB + b;
             double y[16];
             if (lower_op) {
 #pragma unroll
                 for (int i = 0; i < 16; ++i) {
                     double acc = (i == j) ? 1.0 : 0.0;
 #pragma unroll
-                    for (int k = 0; k < i; ++k) acc = fma(-d(b + i, b + k), y[k], acc);
-                    y[i] = (i >= j) ? acc * rd[b + i] : 0.0;
+                    for (int k = 0; k < i; ++k) acc = fma(-d(o + i, o + k), y[k], acc);
+                    y[i] = (i >= j) ? acc * rd[o + i] : 0.0;
                 }
             } else {
 #pragma unroll
                 for (int i = 15; i >= 0; --i) {
                     double acc = (i == j) ? 1.0 : 0.0;
 #pragma unroll
-                    for (int k = i + 1; k < 16; ++k) acc = fma(-d(b + i, b + k), y[k], acc);
-                    y[i] = (i <= j) ? acc * rd[b + i] : 0.0;
+                    for (int k = i + 1; k < 16; ++k) acc = fma(-d(o + i, o + k), y[k], acc);
+                    y[i] = (i <= j) ? acc * rd[o + i] : 0.0;
                 }
             }
 #pragma unroll
-            for (int i = 0; i < 16; ++i) S.R[b + i][b + j] = y[i];
+            for (int i = 0; i < 16; ++i) Y[hb][b + i][b + j] = y[i];
         }
         __syncthreads();
-        // doubling (h = 16, then 32), loops unrolled at compile-time h with two
-        // partial sums per output
+        // doubling inside both halves at once (h = 16, then 32): the
+        // off-diagonal h x h block of each 2h x 2h diagonal block is
+        // -Y22 C Y11 (lower: C below Y11) or -Y11 C Y22 (upper: C right of
+        // Y11).  64 / h products of h x h at a time, a TR x TC tile per thread
         auto doubling = [&](auto hc) {
             constexpr int h = decltype(hc)::value;
-            constexpr int nout = (NB / (2 * h)) * h * h;
-            // T = C Y11 (lower: C the block below Y11) or C Y22 (upper: C right of Y11)
-            for (int idx = t; idx < nout; idx += kThreads) {
-                const int pr = idx / (h * h), e = idx % (h * h), r = e % h, c = e / h, o = pr * 2 * h;
-                double a0 = 0.0, a1 = 0.0;
+            constexpr int G = 64 / h, TPG = kThreads / G;  // products, threads per product
+            constexpr int TR = 2, TC = h / 8, RS = h / TR;  // 8 thread columns, RS thread rows
+            const int gid = t / TPG, u = t % TPG, hb = gid / (G / 2), pr = gid % (G / 2);
+            const int ob = hb * HB, o = pr * 2 * h, tr = u / 8, tcl = u % 8;
+            double acc[TR][TC];
+            if (lower_op)
+                dtile<TR, TC, h>(
+                    acc, tr, RS, tcl, 8, [&](int r, int k) { return d(ob + o + h + r, ob + o + k); },
+                    [&](int k, int c) { return Y[hb][o + k][o + c]; });
+            else
+                dtile<TR, TC, h>(
+                    acc, tr, RS, tcl, 8, [&](int r, int k) { return d(ob + o + r, ob + o + h + k); },
+                    [&](int k, int c) { return Y[hb][o + h + k][o + h + c]; });
 #pragma unroll
-                for (int k = 0; k < h; k += 2) {
-                    if (lower_op) {
-                        a0 = fma(d(o + h + r, o + k), S.R[o + k][o + c], a0);
-                        a1 = fma(d(o + h + r, o + k + 1), S.R[o + k + 1][o + c], a1);
-                    } else {
-                        a0 = fma(d(o + r, o + h + k), S.R[o + h + k][o + h + c], a0);
-                        a1 = fma(d(o + r, o + h + k + 1), S.R[o + h + k + 1][o + h + c], a1);
-                    }
-                }
-                S.Tm[pr * h + r][c] = a0 + a1;
-            }
+            for (int i = 0; i < TR; ++i)
+#pragma unroll
+                for (int j = 0; j < TC; ++j) Tm[hb][pr * h + tr + i * RS][tcl + 8 * j] = acc[i][j];
             __syncthreads();
-            // the off-diagonal block of the inverse: -Y22 T (lower) or -Y11 T (upper)
-            for (int idx = t; idx < nout; idx += kThreads) {
-                const int pr = idx / (h * h), e = idx % (h * h), r = e % h, c = e / h, o = pr * 2 * h;
-                double a0 = 0.0, a1 = 0.0;
+            if (lower_op)
+                dtile<TR, TC, h>(
+                    acc, tr, RS, tcl, 8, [&](int r, int k) { return Y[hb][o + h + r][o + h + k]; },
+                    [&](int k, int c) { return Tm[hb][pr * h + k][c]; });
+            else
+                dtile<TR, TC, h>(
+                    acc, tr, RS, tcl, 8, [&](int r, int k) { return Y[hb][o + r][o + k]; },
+                    [&](int k, int c) { return Tm[hb][pr * h + k][c]; });
 #pragma unroll
-                for (int k = 0; k < h; k += 2) {
-                    if (lower_op) {
-                        a0 = fma(S.R[o + h + r][o + h + k], S.Tm[pr * h + k][c], a0);
-                        a1 = fma(S.R[o + h + r][o + h + k + 1], S.Tm[pr * h + k + 1][c], a1);
-                    } else {
-                        a0 = fma(S.R[o + r][o + k], S.Tm[pr * h + k][c], a0);
-                        a1 = fma(S.R[o + r][o + k + 1], S.Tm[pr * h + k + 1][c], a1);
-                    }
+            for (int i = 0; i < TR; ++i)
+#pragma unroll
+                for (int j = 0; j < TC; ++j) {
+                    const int r = tr + i * RS, c = tcl + 8 * j;
+                    if (lower_op) Y[hb][o + h + r][o + c] = -acc[i][j];
+                    else Y[hb][o + r][o + h + c] = -acc[i][j];
                 }
-                if (lower_op) S.R[o + h + r][o + c] = -(a0 + a1);
-                else S.R[o + r][o + h + c] = -(a0 + a1);
-            }
             __syncthreads();
         };
         doubling(std::integral_constant<int, 16>{});
         doubling(std::integral_constant<int, 32>{});
-        // rows and columns past nr: zero
-        for (int idx = t; idx < TILE_ELEMS; idx += kThreads) {
-            const int r = idx % NB, c = idx / NB;
-            if (r >= nr || c >= nr) S.R[r][c] = 0.0;
-        }
-    }
-    __syncthreads();
-    {
-        float v[TILE_ELEMS / kThreads];
+        // the off-diagonal half: lower D: -inv(D22) (D21 inv(D11)); upper D:
+        // -inv(D11) (D12 inv(D22)); 4 x 4 outputs per thread
+        {
+            const int tr = t / 16, tcl = t % 16;
+            double acc[4][4];
+            if (lower_op)
+                dtile<4, 4, HB>(
+                    acc, tr, 16, tcl, 16, [&](int r, int k) { return d(HB + r, k); },
+                    [&](int k, int c) { return Y[0][k][c]; });
+            else
+                dtile<4, 4, HB>(
+                    acc, tr, 16, tcl, 16, [&](int r, int k) { return d(r, HB + k); },
+                    [&](int k, int c) { return Y[1][k][c]; });
 #pragma unroll
-        for (int u = 0; u < TILE_ELEMS / kThreads; ++u) {
-            const int idx = t + kThreads * u;
-            v[u] = (float)S.R[idx % NB][idx / NB];
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) Yc[tr + 16 * i][tcl + 16 * j] = acc[i][j];
+            __syncthreads();
+            const int yl = lower_op ? 1 : 0;
+            dtile<4, 4, HB>(
+                acc, tr, 16, tcl, 16, [&](int r, int k) { return Y[yl][r][k]; },
+                [&](int k, int c) { return Yc[k][c]; });
+            __syncthreads();
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) Yc[tr + 16 * i][tcl + 16 * j] = -acc[i][j];
         }
         __syncthreads();
+        // this thread's entries of the inverse, in FP32; rows and columns
+        // past nr are cut off
 #pragma unroll
-        for (int u = 0; u < TILE_ELEMS / kThreads; ++u) {
-            const int idx = t + kThreads * u;
-            IV[idx % NB][idx / NB] = v[u];
+        for (int k = 0; k < 4; ++k) {
+            const int R = R0 + k, rr = R & (HB - 1);
+            const bool right = cg >= 4;  // columns 64 .. 127
+            const double* src;           // row R of the 64 x 64 piece holding the columns
+            if (lower_op) src = R < HB ? (right ? nullptr : Y[0][rr]) : (right ? Y[1][rr] : Yc[rr]);
+            else src = R < HB ? (right ? Yc[rr] : Y[0][rr]) : (right ? Y[1][rr] : nullptr);
+            const bool keep = src != nullptr && R < nr;
+            const int c0 = (cg & 3) * 16;
+#pragma unroll
+            for (int j = 0; j < 16; ++j) iv[k][j] = (keep && cg * 16 + j < nr) ? (float)src[c0 + j] : 0.f;
         }
+        // D (stages 0, 1) and the FP64 workspace (stages 2 on) are free; the
+        // stores to them come before the copies that reuse the stages
+        tma::fence_proxy_async_smem();
+        __syncthreads();
     }
-    __syncthreads();
-    if (t == 0 && FS < nloads) issue(FS);
+    if (t == 0)
+        for (int L = 2; L < min(2 + FS, nloads); ++L) issue(L);
 
-    // ---- W = inv(D) T for the tile of block s-1
+    // ---- the tile T of block s-1, kept in registers in the same layout
+    float tc[4][16];
     if (s >= 1) {
-        bad = tma::mbar_wait_bounded(&S.full[1], 0, kTrsvWaitNs) ? 0 : 1;
+        bad = (wait_load(2) && wait_load(3)) ? 0 : 1;
         if (__syncthreads_or(bad)) {
-            bail(1);
+            bail(2);
             return;
         }
-        const float* T = S.stage[1];
-        float acc[16];
-#pragma unroll
-        for (int jj = 0; jj < 16; ++jj) acc[jj] = 0.f;
-        for (int k = 0; k < NB; ++k) {
-            const float a = IV[rN][k];
-#pragma unroll
-            for (int jj = 0; jj < 16; ++jj) acc[jj] = fmaf(a, tile(T, k, gN * 16 + jj), acc[jj]);
-        }
-#pragma unroll
-        for (int jj = 0; jj < 16; ++jj) W[rN][gN * 16 + jj] = acc[jj];
-        __syncthreads();
-        if (t == 0 && FS + 1 < nloads) issue(FS + 1);
-    }
-
-    // ---- the other earlier blocks, in solve order
-    const int lane = t & 31, warp = t >> 5;
-    float accN = 0.f;
-    float accT[8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i) accT[i] = 0.f;
-    for (int i = 2; i <= s; ++i) {
-        const int c0 = blk(i - 2) * NB, nc = min(NB, n - c0);
-        bad = tma::mbar_wait_bounded(&S.full[i % FS], (i / FS) & 1, kTrsvWaitNs) ? 0 : 1;
-        bad |= fetch_x(i - 2, c0, nc);
-        if (__syncthreads_or(bad)) {
-            bail(i);
-            return;
-        }
-        const float* T = S.stage[i % FS];
+        const float* T = S.stage[2 + (cg >> 2)];
+        const int c0 = (cg & 3) * 16;  // first column inside the stage
         if (op == 0) {
 #pragma unroll
-            for (int jj = 0; jj < 16; ++jj) {
-                const int c = gN * 16 + jj;
-                accN = fmaf(-T[c * NB + rN], S.xs[c], accN);
+            for (int j = 0; j < 16; ++j) {
+                const float4 v = *reinterpret_cast<const float4*>(&T[(c0 + j) * RB + R0]);
+                tc[0][j] = v.x;
+                tc[1][j] = v.y;
+                tc[2][j] = v.z;
+                tc[3][j] = v.w;
             }
         } else {
-            const float x0 = S.xs[lane], x1 = S.xs[lane + 32];
 #pragma unroll
-            for (int ii = 0; ii < 8; ++ii) {
-                const int r = warp * 8 + ii;
-                accT[ii] = fmaf(-T[r * NB + lane], x0, accT[ii]);
-                accT[ii] = fmaf(-T[r * NB + lane + 32], x1, accT[ii]);
-            }
-        }
-        __syncthreads();
-        if (t == 0 && i + FS < nloads) issue(i + FS);
-    }
-
-    // ---- z = inv(D) (b - row sums)
-    if (op == 0) {
-        S.part[gN][rN] = accN;
-    } else {
+            for (int k = 0; k < 4; ++k)
 #pragma unroll
-        for (int ii = 0; ii < 8; ++ii) {
-            const float v = warp_sum(accT[ii]);
-            if (lane == 0) S.part[0][warp * 8 + ii] = v;
-        }
-    }
-    __syncthreads();
-    if (t < NB) {
-        const float sum = op == 0 ? (S.part[0][t] + S.part[1][t]) + (S.part[2][t] + S.part[3][t]) : S.part[0][t];
-        S.ys[t] = t < nr ? b + sum : 0.f;
-    }
-    __syncthreads();
-    {
-        float acc = 0.f;
-#pragma unroll
-        for (int jj = 0; jj < 16; ++jj) acc = fmaf(IV[rN][gN * 16 + jj], S.ys[gN * 16 + jj], acc);
-        S.part[gN][rN] = acc;
-    }
-    __syncthreads();
-    if (t < NB) S.zs[t] = (S.part[0][t] + S.part[1][t]) + (S.part[2][t] + S.part[3][t]);
-
-    // ---- this block's step of the chain: x = z - W x_prev, on the 64
-    // threads that own the rows: from the arrival of x_prev to the hand-off
-    // of x there is no block-wide barrier (the global path synchronises the
-    // two warps only)
-    if (t < NB) {
-        float xf = S.zs[t];
-        bool ok = true;
-        if (s >= 1) {
-            const int p = s - 1, c0 = blk(p) * NB, nc = min(NB, n - c0);
-            const float* xp = S.xs;
-            if (CL > 1 && p >= cfirst) {
-                ok = xbar_wait_bounded(&S.xbar[p - cfirst], kTrsvWaitNs);
-                xp = S.xin[p - cfirst];
-            } else {
-                float v = 0.f;
-                if (t < nc) {
-                    const unsigned long long* src = pub + c0 + t;
-                    unsigned long long w = ld_relaxed_u64(src);
-                    if ((unsigned)(w >> 32) != epoch) {
-                        const unsigned long long t0 = tma::global_ns();
-                        for (;;) {
-                            w = ld_relaxed_u64(src);
-                            if ((unsigned)(w >> 32) == epoch) break;
-                            if (ld_volatile(status) != kDevOk || tma::global_ns() - t0 > kTrsvWaitNs) {
-                                ok = false;
-                                break;
-                            }
-                        }
-                    }
-                    v = __uint_as_float((unsigned)w);
+                for (int q = 0; q < 4; ++q) {
+                    const float4 v = *reinterpret_cast<const float4*>(&T[(R0 + k) * HB + c0 + 4 * q]);
+                    tc[k][4 * q] = v.x;
+                    tc[k][4 * q + 1] = v.y;
+                    tc[k][4 * q + 2] = v.z;
+                    tc[k][4 * q + 3] = v.w;
                 }
-                S.xs[t] = v;
-                asm volatile("bar.sync 1, %0;" ::"n"(NB) : "memory");  // the 64 row threads
-            }
-            float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+        }
+        // the registers are not read until the chain step: the reads of
+        // stages 2 and 3 must be complete before the copies that reuse them
+        tma::fence_proxy_async_smem();
+        __syncthreads();
+        if (t == 0)
+            for (int L = 2 + FS; L < min(4 + FS, nloads); ++L) issue(L);
+    }
+
+    // ---- the other earlier blocks, in solve order: y = b - their products.
+    // Each thread keeps partial row sums in registers; 16-byte reads run
+    // along the stage's contiguous direction.
+    //   op N (stage column-major): rows 4*lane .. +3, columns warp*8 .. +7
+    //   op T (stage row-major): rows (2*warp + lane/16)*8 .. +7, columns
+    //   4*(lane%16) .. +3
+    float acc[8];
 #pragma unroll
-            for (int j = 0; j < NB; j += 4) {
-                a0 = fmaf(W[t][j], xp[j], a0);
-                a1 = fmaf(W[t][j + 1], xp[j + 1], a1);
-                a2 = fmaf(W[t][j + 2], xp[j + 2], a2);
-                a3 = fmaf(W[t][j + 3], xp[j + 3], a3);
+    for (int k = 0; k < 8; ++k) acc[k] = 0.f;
+    for (int i = 0; i + 1 < s; ++i) {
+        bad = 0;
+        const float* xv = fetch_x(i, S.xs, bad);
+        for (int hh = 0; hh < 2; ++hh) {
+            const int L = 4 + 2 * i + hh;
+            if (!wait_load(L)) bad = 1;
+            if (__syncthreads_or(bad)) {
+                bail(L);
+                return;
             }
-            xf -= (a0 + a1) + (a2 + a3);
+            const float* T = S.stage[L % FS];
+            if (op == 0) {
+                const int c0 = warp * 8;
+                const float* xq = xv + qidx(hh * HB + c0);
+                const float4 xa = *reinterpret_cast<const float4*>(xq);
+                const float4 xb = *reinterpret_cast<const float4*>(xq + 4);
+                const float xk[8] = {xa.x, xa.y, xa.z, xa.w, xb.x, xb.y, xb.z, xb.w};
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    const float4 v = *reinterpret_cast<const float4*>(&T[(c0 + k) * RB + 4 * lane]);
+                    acc[0] = fmaf(-v.x, xk[k], acc[0]);
+                    acc[1] = fmaf(-v.y, xk[k], acc[1]);
+                    acc[2] = fmaf(-v.z, xk[k], acc[2]);
+                    acc[3] = fmaf(-v.w, xk[k], acc[3]);
+                }
+            } else {
+                const int cq = lane & 15, rb = (2 * warp + (lane >> 4)) * 8;
+                const float4 xa = *reinterpret_cast<const float4*>(xv + qidx(hh * HB + 4 * cq));
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    const float4 v = *reinterpret_cast<const float4*>(&T[(rb + k) * HB + 4 * cq]);
+                    acc[k] = fmaf(-v.x, xa.x, acc[k]);
+                    acc[k] = fmaf(-v.y, xa.y, acc[k]);
+                    acc[k] = fmaf(-v.z, xa.z, acc[k]);
+                    acc[k] = fmaf(-v.w, xa.w, acc[k]);
+                }
+            }
+            __syncthreads();
+            if (t == 0 && L + FS < nloads) issue(L + FS);
         }
-        if (ok) {
-            if (t < nr) {
-                x[(long)(r0 + t) * incx] = xf;
-                st_relaxed_u64(pub + r0 + t, ((unsigned long long)epoch << 32) | __float_as_uint(xf));
-            }
-            // hand the block to the later CTAs of the cluster that have blocks
-            if constexpr (CL > 1) {
-                const float v = t < nr ? xf : 0.f;
-                for (unsigned d = rank + 1u; d < (unsigned)CL && cfirst + (int)d < nb; ++d)
-                    st_async_f32(map_to(&S.xin[rank][t], d), v, map_to(&S.xbar[rank], d));
-            }
+    }
+    if (op == 0) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) S.part[warp][4 * lane + k] = acc[k];
+    } else {
+        const int cq = lane & 15, rb = (2 * warp + (lane >> 4)) * 8;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) S.part[cq][rb + k] = acc[k];
+    }
+    __syncthreads();
+    if (t < RB) {
+        float sum = 0.f;
+        const int np = op == 0 ? 8 : 16;
+        for (int p = 0; p < np; ++p) sum += S.part[p][t];
+        S.y[qidx(t)] = t < nr ? b + sum : 0.f;
+    }
+    __syncthreads();
+
+    // ---- this block's step of the chain: x = inv(D) (y - T x_prev).  From
+    // the arrival of x_prev to the hand-off of x: two register products and
+    // one barrier (one more on the global path, after the polls)
+    bool ok = true;
+    float o[4];
+    const int own = cg & 3, row = R0 + own;  // the row this lane publishes
+    if (s >= 1) {
+        const int p = s - 1;
+        const float* xpv;
+        if (CL > 1 && p >= cfirst) {
+            ok = __all_sync(0xffffffffu, xbar_wait_bounded(&S.xbar[p - cfirst], kTrsvWaitNs));
+            xpv = S.xin[p - cfirst];
         } else {
-            atomicOr(status, (int)kDevWaitTimeout);
-            S.failed = 1;
+            const int c0 = blk(p) * RB, nc = min(RB, n - c0);
+            if (t < RB) {
+                float v = 0.f;
+                if (t < nc && !poll_word(pub + c0 + t, epoch, status, v)) ok = false;
+                S.xp[qidx(t)] = v;
+            }
+            ok = __syncthreads_and(ok);
+            xpv = S.xp;
         }
+        mv(tc, xpv, o);
+        if (cg < 4) S.y2[qidx(row)] = S.y[qidx(row)] - pick(o, own);
+    } else {
+        if (cg < 4) S.y2[qidx(row)] = S.y[qidx(row)];
+    }
+    __syncthreads();
+    mv(iv, S.y2, o);
+    const float xf = pick(o, own);
+    if (ok) {
+        if (cg < 4) {
+            if (row < nr) {
+                x[(long)(r0 + row) * incx] = xf;
+                st_relaxed_u64(pub + r0 + row, ((unsigned long long)epoch << 32) | __float_as_uint(xf));
+            }
+        } else if constexpr (CL > 1) {
+            // hand the block to the later CTAs of the cluster that have blocks
+            const float v = row < nr ? xf : 0.f;
+            for (unsigned dd = rank + 1u; dd < (unsigned)CL && cfirst + (int)dd < nb; ++dd)
+                st_async_f32(map_to(&S.xin[rank][qidx(row)], dd), v, map_to(&S.xbar[rank], dd));
+        }
+    } else {
+        atomicOr(status, (int)kDevWaitTimeout);
+        S.failed = 1;
     }
     __syncthreads();
     if (t == 0) {
@@ -735,12 +864,67 @@ __global__ void __launch_bounds__(kThreads, 2)
     if constexpr (CL > 1) cluster_sync_all();
 }
 
+// the number of clusters of CL CTAs of the STRSV kernel the current device
+// holds at once (0: none), asked once per device and cluster size
+template <int CL>
+int strsv_cluster_capacity(int device, int smem)
+{
+    static std::atomic<int> cap[64];  // capacity + 1; 0: not asked yet
+    std::atomic<int>& c = cap[device & 63];
+    int v = c.load();
+    if (v == 0) {
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = CL;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(CL);
+        cfg.blockDim = dim3(kThreads);
+        cfg.dynamicSmemBytes = smem;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int clusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&clusters, strsv_tma_kernel<CL>, &cfg) != cudaSuccess) {
+            cudaGetLastError();
+            clusters = 0;
+        }
+        v = clusters + 1;
+        c.store(v);
+    }
+    return v - 1;
+}
+
+template <int CL>
+cudaError_t strsv_launch(iclblasHandle_t h, int smem, int nb, const CUtensorMap& map, int n, int lower_op, int op,
+                         int unit, float* x, int incx, unsigned* ticket, unsigned* epoch_word)
+{
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = CL;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3((unsigned)((nb + CL - 1) / CL * CL));
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = h->stream;
+    cfg.attrs = attr;
+    cfg.numAttrs = CL > 1 ? 1 : 0;
+    cudaError_t e = cudaLaunchKernelEx(&cfg, strsv_tma_kernel<CL>, map, n, lower_op, op, unit, x, (long)incx,
+                                       h->ws.pub, ticket, epoch_word, h->ws.dev_status);
+    return e != cudaSuccess ? e : cudaGetLastError();
+}
+
 cudaError_t strsv_tma(iclblasHandle_t h, int uplo, int trans, int diag, int n, const float* A, int lda, float* x,
                       int incx, bool& used)
 {
     used = false;
+    const int op = trans == ICLBLAS_OP_N ? 0 : 1;
     CUtensorMap map;
-    if (lda < n || !tma::map_f32_colmajor(&map, A, n, n, lda, NB, NB)) return cudaSuccess;
+    // op N: boxes of 128 rows x 64 columns of A; op T: 64 rows x 128 columns
+    if (lda < n || !tma::map_f32_colmajor(&map, A, n, n, lda, op == 0 ? RB : HB, op == 0 ? HB : RB))
+        return cudaSuccess;
     if ((size_t)n > h->ws.pub_elems) {
         if (h->ws.pub) cudaFree(h->ws.pub);
         h->ws.pub = nullptr;
@@ -752,51 +936,43 @@ cudaError_t strsv_tma(iclblasHandle_t h, int uplo, int trans, int diag, int n, c
         h->ws.pub_elems = n;
     }
     const int smem = (int)sizeof(FastSmem) + 1024;
-    static int smem_set = 0;
-    if (!smem_set) {
+    // the attribute belongs to the current device's copy of each kernel
+    static std::atomic<unsigned long long> smem_set{0};
+    const unsigned long long bit = 1ull << (h->device & 63);
+    if (!(smem_set.load() & bit)) {
         cudaError_t e = cudaFuncSetAttribute(strsv_tma_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(strsv_tma_kernel<kMaxCluster>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+            e = cudaFuncSetAttribute(strsv_tma_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(strsv_tma_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(strsv_tma_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return e;
-        smem_set = 1;
+        smem_set.fetch_or(bit);
     }
-    const int op = trans == ICLBLAS_OP_N ? 0 : 1;
     const bool lower = uplo == ICLBLAS_FILL_MODE_LOWER;
     const int lower_op = (op == 0) ? lower : !lower;
-    const int nb = (n + NB - 1) / NB;
+    const int nb = (n + RB - 1) / RB;
     const int unit = diag == ICLBLAS_DIAG_UNIT;
     unsigned* ticket = h->ws.counters;
     unsigned* epoch_word = h->ws.counters + kCounterWords - 1;
-    // clusters of 8 consecutive blocks when the GPU can hold one (and there
-    // is more than one block); else one CTA per block
-    if (nb > 1) {
-        cudaLaunchConfig_t cfg = {};
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeClusterDimension;
-        attr[0].val.clusterDim.x = kMaxCluster;
-        attr[0].val.clusterDim.y = 1;
-        attr[0].val.clusterDim.z = 1;
-        cfg.gridDim = dim3((unsigned)((nb + kMaxCluster - 1) / kMaxCluster * kMaxCluster));
-        cfg.blockDim = dim3(kThreads);
-        cfg.dynamicSmemBytes = smem;
-        cfg.stream = h->stream;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        int clusters = 0;
-        if (cudaOccupancyMaxActiveClusters(&clusters, strsv_tma_kernel<kMaxCluster>, &cfg) == cudaSuccess &&
-            clusters > 0) {
-            cudaError_t e = cudaLaunchKernelEx(&cfg, strsv_tma_kernel<kMaxCluster>, map, n, lower_op, op, unit, x,
-                                               (long)incx, h->ws.pub, ticket, epoch_word, h->ws.dev_status);
-            if (e != cudaSuccess) return e;
-            used = true;
-            return cudaGetLastError();
-        }
-        cudaGetLastError();
-    }
-    strsv_tma_kernel<1><<<nb, kThreads, smem, h->stream>>>(map, n, lower_op, op, unit, x, incx, h->ws.pub, ticket,
-                                                           epoch_word, h->ws.dev_status);
     used = true;
-    return cudaGetLastError();
+    if (nb > 1) {
+        // the largest cluster size for which every cluster of the launch is
+        // resident at once; if none is, clusters of 8 (the most DSMEM
+        // hand-offs), else one CTA per block
+        const int c8 = strsv_cluster_capacity<8>(h->device, smem);
+        const int c4 = strsv_cluster_capacity<4>(h->device, smem);
+        const int c2 = strsv_cluster_capacity<2>(h->device, smem);
+        if (c8 > 0 && c8 * 8 >= nb)
+            return strsv_launch<8>(h, smem, nb, map, n, lower_op, op, unit, x, incx, ticket, epoch_word);
+        if (c4 > 0 && c4 * 4 >= nb)
+            return strsv_launch<4>(h, smem, nb, map, n, lower_op, op, unit, x, incx, ticket, epoch_word);
+        if (c2 > 0 && c2 * 2 >= nb)
+            return strsv_launch<2>(h, smem, nb, map, n, lower_op, op, unit, x, incx, ticket, epoch_word);
+        if (c8 > 0) return strsv_launch<8>(h, smem, nb, map, n, lower_op, op, unit, x, incx, ticket, epoch_word);
+    }
+    return strsv_launch<1>(h, smem, nb, map, n, lower_op, op, unit, x, incx, ticket, epoch_word);
 }
 
 template <class T>
