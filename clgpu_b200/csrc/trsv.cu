@@ -256,10 +256,10 @@ __global__ void __launch_bounds__(kThreads) trsv_kernel(int n, int lower_op, int
 //   - launched as clusters of CL consecutive blocks, a solved block also goes
 //     straight into the shared memory of the later CTAs of its cluster
 //     (st.async on a transaction barrier), so CL - 1 of every CL steps of the
-//     chain skip the global-memory round trip.  CL is the largest of 8, 4, 2
-//     for which the GPU holds every cluster of the launch at once (a cluster
-//     that can only start when another has finished starts its own setup
-//     late and then streams its tiles alone).
+//     chain skip the global-memory round trip.  CL is the largest size from
+//     8 down to 2 for which the GPU holds every cluster of the launch at once
+//     (a cluster that can only start when another has finished starts its
+//     own setup late and then streams its tiles alone).
 // Against 64-row blocks (two CTAs per SM, n = 16384 in 230 us) the chain has
 // half the steps and half the hand-offs between clusters.
 constexpr int RB = 128;  // rows (and columns) of a block
@@ -940,14 +940,14 @@ cudaError_t strsv_tma(iclblasHandle_t h, int uplo, int trans, int diag, int n, c
     static std::atomic<unsigned long long> smem_set{0};
     const unsigned long long bit = 1ull << (h->device & 63);
     if (!(smem_set.load() & bit)) {
-        cudaError_t e = cudaFuncSetAttribute(strsv_tma_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(strsv_tma_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(strsv_tma_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(strsv_tma_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e != cudaSuccess) return e;
+        const void* kernels[] = {(const void*)strsv_tma_kernel<1>, (const void*)strsv_tma_kernel<2>,
+                                 (const void*)strsv_tma_kernel<3>, (const void*)strsv_tma_kernel<4>,
+                                 (const void*)strsv_tma_kernel<5>, (const void*)strsv_tma_kernel<6>,
+                                 (const void*)strsv_tma_kernel<7>, (const void*)strsv_tma_kernel<8>};
+        for (const void* k : kernels) {
+            cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+            if (e != cudaSuccess) return e;
+        }
         smem_set.fetch_or(bit);
     }
     const bool lower = uplo == ICLBLAS_FILL_MODE_LOWER;
@@ -958,19 +958,33 @@ cudaError_t strsv_tma(iclblasHandle_t h, int uplo, int trans, int diag, int n, c
     unsigned* epoch_word = h->ws.counters + kCounterWords - 1;
     used = true;
     if (nb > 1) {
-        // the largest cluster size for which every cluster of the launch is
-        // resident at once; if none is, clusters of 8 (the most DSMEM
-        // hand-offs), else one CTA per block
-        const int c8 = strsv_cluster_capacity<8>(h->device, smem);
-        const int c4 = strsv_cluster_capacity<4>(h->device, smem);
-        const int c2 = strsv_cluster_capacity<2>(h->device, smem);
-        if (c8 > 0 && c8 * 8 >= nb)
-            return strsv_launch<8>(h, smem, nb, map, n, lower_op, op, unit, x, incx, ticket, epoch_word);
-        if (c4 > 0 && c4 * 4 >= nb)
-            return strsv_launch<4>(h, smem, nb, map, n, lower_op, op, unit, x, incx, ticket, epoch_word);
-        if (c2 > 0 && c2 * 2 >= nb)
-            return strsv_launch<2>(h, smem, nb, map, n, lower_op, op, unit, x, incx, ticket, epoch_word);
-        if (c8 > 0) return strsv_launch<8>(h, smem, nb, map, n, lower_op, op, unit, x, incx, ticket, epoch_word);
+        // the largest cluster size, 8 down to 2, for which every cluster of
+        // the launch is resident at once (sizes need not be powers of two: a
+        // GPC that holds two clusters of 8 may hold three of 6); if none is,
+        // clusters of 8 (the most DSMEM hand-offs), else one CTA per block
+        const int caps[9] = {0,
+                             0,
+                             strsv_cluster_capacity<2>(h->device, smem),
+                             strsv_cluster_capacity<3>(h->device, smem),
+                             strsv_cluster_capacity<4>(h->device, smem),
+                             strsv_cluster_capacity<5>(h->device, smem),
+                             strsv_cluster_capacity<6>(h->device, smem),
+                             strsv_cluster_capacity<7>(h->device, smem),
+                             strsv_cluster_capacity<8>(h->device, smem)};
+        int cl = 0;
+        for (int c = 8; c >= 2 && !cl; --c)
+            if (caps[c] > 0 && caps[c] * c >= nb) cl = c;
+        if (!cl && caps[8] > 0) cl = 8;
+        switch (cl) {
+        case 8: return strsv_launch<8>(h, smem, nb, map, n, lower_op, op, unit, x, incx, ticket, epoch_word);
+        case 7: return strsv_launch<7>(h, smem, nb, map, n, lower_op, op, unit, x, incx, ticket, epoch_word);
+        case 6: return strsv_launch<6>(h, smem, nb, map, n, lower_op, op, unit, x, incx, ticket, epoch_word);
+        case 5: return strsv_launch<5>(h, smem, nb, map, n, lower_op, op, unit, x, incx, ticket, epoch_word);
+        case 4: return strsv_launch<4>(h, smem, nb, map, n, lower_op, op, unit, x, incx, ticket, epoch_word);
+        case 3: return strsv_launch<3>(h, smem, nb, map, n, lower_op, op, unit, x, incx, ticket, epoch_word);
+        case 2: return strsv_launch<2>(h, smem, nb, map, n, lower_op, op, unit, x, incx, ticket, epoch_word);
+        default: break;
+        }
     }
     return strsv_launch<1>(h, smem, nb, map, n, lower_op, op, unit, x, incx, ticket, epoch_word);
 }
