@@ -54,6 +54,12 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
         if (global_ns() - t0 > limit_ns) return false;
     return true;
 }
+// Starts bringing a 2D box into L2 (no shared memory, no completion).
+__device__ __forceinline__ void prefetch_2d(const CUtensorMap* map, int x, int y)
+{
+    asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];" ::"l"((uint64_t)map), "r"(x), "r"(y)
+                 : "memory");
+}
 // 2D tiled load into this CTA's own shared memory; completion is
 // counted in bytes on `bar`.
 __device__ __forceinline__ void load_2d(void* smem_dst, const CUtensorMap* map, int x, int y, uint64_t* bar)

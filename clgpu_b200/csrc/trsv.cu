@@ -334,12 +334,13 @@ __device__ __forceinline__ void st_cluster_u32(uint32_t addr, unsigned v)
 {
     asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
 }
-// 4 bytes into another CTA's shared memory, counted as transaction bytes on
-// that CTA's barrier
-__device__ __forceinline__ void st_async_f32(uint32_t addr, float v, uint32_t bar)
+// 16 bytes into another CTA's shared memory (16-byte aligned), counted as
+// transaction bytes on that CTA's barrier
+__device__ __forceinline__ void st_async_f32x4(uint32_t addr, float a, float b, float c, float d, uint32_t bar)
 {
-    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.f32 [%0], %1, [%2];" ::"r"(addr), "f"(v),
-                 "r"(bar)
+    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v4.f32 [%0], {%1, %2, %3, %4}, [%5];" ::"r"(
+                     addr),
+                 "f"(a), "f"(b), "f"(c), "f"(d), "r"(bar)
                  : "memory");
 }
 __device__ __forceinline__ void cluster_sync_all()
@@ -488,6 +489,14 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (t == 0) {
         issue(0);
         issue(1);
+        // the tiles needed first after the inverse (block s-1's, then block
+        // 0's) start towards L2 now, while the inverse is formed
+        for (int L = 2; L < min(6, nloads); ++L) {
+            const int cb = L < 4 ? blk(s - 1) : blk(0);
+            const int c = cb * RB + (L & 1) * HB;
+            if (op == 0) tma::prefetch_2d(&amap, r0, c);
+            else tma::prefetch_2d(&amap, c, r0);
+        }
     }
     const float b = (t < nr) ? x[(long)(r0 + t) * incx] : 0.f;  // (threads t < RB)
     // on a failed wait: record it, let this CTA's copies still in flight land
@@ -678,19 +687,36 @@ __global__ void __launch_bounds__(kThreads, 1)
                 for (int j = 0; j < 4; ++j) Yc[tr + 16 * i][tcl + 16 * j] = -acc[i][j];
         }
         __syncthreads();
-        // this thread's entries of the inverse, in FP32; rows and columns
-        // past nr are cut off
+        // the inverse in FP32, row-major through stages 0 and 1 (16-byte word
+        // f of row R at f ^ ((f >> 2) & 7)), then each thread's 4 x 16 block
+        // from it: neither pass has bank conflicts (reading the FP64 pieces
+        // straight into the register layout had 8-way conflicts and took 3 us).
+        // Rows and columns past nr are cut off.
+        {
+            float4* Iv = reinterpret_cast<float4*>(&S.stage[0][0]);
+            for (int idx = t; idx < RB * 32; idx += kThreads) {
+                const int R = idx >> 5, f = idx & 31, C = 4 * f, rr = R & (HB - 1);
+                const bool right = C >= HB;  // columns 64 .. 127
+                const double* src;           // row R of the 64 x 64 piece holding the columns
+                if (lower_op) src = R < HB ? (right ? nullptr : Y[0][rr]) : (right ? Y[1][rr] : Yc[rr]);
+                else src = R < HB ? (right ? Yc[rr] : Y[0][rr]) : (right ? Y[1][rr] : nullptr);
+                float v[4];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const int R = R0 + k, rr = R & (HB - 1);
-            const bool right = cg >= 4;  // columns 64 .. 127
-            const double* src;           // row R of the 64 x 64 piece holding the columns
-            if (lower_op) src = R < HB ? (right ? nullptr : Y[0][rr]) : (right ? Y[1][rr] : Yc[rr]);
-            else src = R < HB ? (right ? Yc[rr] : Y[0][rr]) : (right ? Y[1][rr] : nullptr);
-            const bool keep = src != nullptr && R < nr;
-            const int c0 = (cg & 3) * 16;
+                for (int e = 0; e < 4; ++e)
+                    v[e] = (src != nullptr && R < nr && C + e < nr) ? (float)src[(C + e) & (HB - 1)] : 0.f;
+                Iv[R * 32 + (f ^ (f >> 2 & 7))] = make_float4(v[0], v[1], v[2], v[3]);
+            }
+            __syncthreads();
 #pragma unroll
-            for (int j = 0; j < 16; ++j) iv[k][j] = (keep && cg * 16 + j < nr) ? (float)src[c0 + j] : 0.f;
+            for (int k = 0; k < 4; ++k)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const float4 v = Iv[(R0 + k) * 32 + ((cg * 4 + q) ^ cg)];
+                    iv[k][4 * q] = v.x;
+                    iv[k][4 * q + 1] = v.y;
+                    iv[k][4 * q + 2] = v.z;
+                    iv[k][4 * q + 3] = v.w;
+                }
         }
         // D (stages 0, 1) and the FP64 workspace (stages 2 on) are free; the
         // stores to them come before the copies that reuse the stages
@@ -812,6 +838,26 @@ __global__ void __launch_bounds__(kThreads, 1)
     bool ok = true;
     float o[4];
     const int own = cg & 3, row = R0 + own;  // the row this lane publishes
+    // hand-off: lane 4 + d sends rows R0 .. R0+3 to the later CTAs rank + 1 + d
+    // and rank + 5 + d of the cluster (those that have blocks), 16 bytes
+    // each; the remote addresses are formed here, off the critical path
+    int ndst = 0;
+    uint32_t dx0 = 0, db0 = 0, dx1 = 0, db1 = 0;
+    if constexpr (CL > 1) {
+        if (cg >= 4) {
+            const unsigned d0 = rank + 1u + (unsigned)(cg - 4), d1 = d0 + 4u;
+            if (d0 < (unsigned)CL && cfirst + (int)d0 < nb) {
+                dx0 = map_to(&S.xin[rank][qidx(R0)], d0);
+                db0 = map_to(&S.xbar[rank], d0);
+                ndst = 1;
+                if (d1 < (unsigned)CL && cfirst + (int)d1 < nb) {
+                    dx1 = map_to(&S.xin[rank][qidx(R0)], d1);
+                    db1 = map_to(&S.xbar[rank], d1);
+                    ndst = 2;
+                }
+            }
+        }
+    }
     if (s >= 1) {
         const int p = s - 1;
         const float* xpv;
@@ -837,17 +883,16 @@ __global__ void __launch_bounds__(kThreads, 1)
     mv(iv, S.y2, o);
     const float xf = pick(o, own);
     if (ok) {
-        if (cg < 4) {
-            if (row < nr) {
-                x[(long)(r0 + row) * incx] = xf;
-                st_relaxed_u64(pub + r0 + row, ((unsigned long long)epoch << 32) | __float_as_uint(xf));
-            }
-        } else if constexpr (CL > 1) {
-            // hand the block to the later CTAs of the cluster that have blocks
-            const float v = row < nr ? xf : 0.f;
-            for (unsigned dd = rank + 1u; dd < (unsigned)CL && cfirst + (int)dd < nb; ++dd)
-                st_async_f32(map_to(&S.xin[rank][qidx(row)], dd), v, map_to(&S.xbar[rank], dd));
+        // the hand-offs first, then the published words; the output x last
+        if (ndst > 0) {
+            float v[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) v[k] = R0 + k < nr ? o[k] : 0.f;
+            st_async_f32x4(dx0, v[0], v[1], v[2], v[3], db0);
+            if (ndst > 1) st_async_f32x4(dx1, v[0], v[1], v[2], v[3], db1);
         }
+        if (cg < 4 && row < nr) st_relaxed_u64(pub + r0 + row, ((unsigned long long)epoch << 32) | __float_as_uint(xf));
+        if (cg < 4 && row < nr) x[(long)(r0 + row) * incx] = xf;
     } else {
         atomicOr(status, (int)kDevWaitTimeout);
         S.failed = 1;
