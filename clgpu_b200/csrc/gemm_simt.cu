@@ -14,6 +14,7 @@
 // the global loads are arranged so consecutive threads read consecutive
 // addresses for each operand layout (op N vs T/C).
 #include <algorithm>
+#include <type_traits>
 
 #include "common.cuh"
 
@@ -32,6 +33,26 @@ __device__ __forceinline__ void mac(cfloat& acc, cfloat a, cfloat b)
     acc.re = fmaf(-a.im, b.im, acc.re);
     acc.im = fmaf(a.re, b.im, acc.im);
     acc.im = fmaf(a.im, b.re, acc.im);
+}
+
+// Two FP32 fused multiply-adds in one instruction (fma.rn.f32x2): each lane
+// of the pair is rounded exactly as fmaf, so a result keeps its bits; the
+// float kernel issues half as many FMA instructions (it is issue-bound)
+__device__ __forceinline__ unsigned long long pack2(float lo, float hi)
+{
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ float half2f(unsigned long long v, int hi)
+{
+    float lo_v, hi_v;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo_v), "=f"(hi_v) : "l"(v));
+    return hi ? hi_v : lo_v;
+}
+__device__ __forceinline__ void mac2(unsigned long long& acc, unsigned long long a, unsigned long long b)
+{
+    asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(acc) : "l"(a), "l"(b));
 }
 
 __host__ __device__ __forceinline__ bool is_zero(float v) { return v == 0.f; }
@@ -157,11 +178,22 @@ __global__ void __launch_bounds__(Cfg<T, BM, BN, BK, TM, TN>::NT)
         }
     };
 
-    T acc[TM][TN];
+    // float: accumulators in pairs along j (acc[i][2j], acc[i][2j+1])
+    constexpr bool kPair = std::is_same<T, float>::value && TN % 2 == 0;
+    using AccT = std::conditional_t<kPair, unsigned long long, T>;
+    constexpr int TNA = kPair ? TN / 2 : TN;
+    AccT acc[TM][TNA];
 #pragma unroll
     for (int i = 0; i < TM; ++i)
 #pragma unroll
-        for (int j = 0; j < TN; ++j) acc[i][j] = zero_v(T());
+        for (int j = 0; j < TNA; ++j) {
+            if constexpr (kPair) acc[i][j] = 0ull;  // (+0.f, +0.f)
+            else acc[i][j] = zero_v(T());
+        }
+    auto acc_at = [&](int i, int j) -> T {
+        if constexpr (kPair) return half2f(acc[i][j >> 1], j & 1);
+        else return acc[i][j];
+    };
 
     const int ktiles = (k + BK - 1) / BK;
     if (ktiles > 0) {
@@ -184,10 +216,22 @@ __global__ void __launch_bounds__(Cfg<T, BM, BN, BK, TM, TN>::NT)
             lds_vec<T, TM / 2>(a + TM / 2, &As[buf][kk][BM / 2 + ty * (TM / 2)]);
             lds_vec<T, TN / 2>(b, &Bs[buf][kk][tx * (TN / 2)]);
             lds_vec<T, TN / 2>(b + TN / 2, &Bs[buf][kk][BN / 2 + tx * (TN / 2)]);
+            if constexpr (kPair) {
+                unsigned long long bp[TN / 2];
 #pragma unroll
-            for (int i = 0; i < TM; ++i)
+                for (int j = 0; j < TN / 2; ++j) bp[j] = pack2(b[2 * j], b[2 * j + 1]);
 #pragma unroll
-                for (int j = 0; j < TN; ++j) mac(acc[i][j], a[i], b[j]);
+                for (int i = 0; i < TM; ++i) {
+                    const unsigned long long ap = pack2(a[i], a[i]);
+#pragma unroll
+                    for (int j = 0; j < TN / 2; ++j) mac2(acc[i][j], ap, bp[j]);
+                }
+            } else {
+#pragma unroll
+                for (int i = 0; i < TM; ++i)
+#pragma unroll
+                    for (int j = 0; j < TN; ++j) mac(acc[i][j], a[i], b[j]);
+            }
         }
         if (t + 1 < ktiles) {
             store_a(buf ^ 1);
@@ -215,7 +259,7 @@ __global__ void __launch_bounds__(Cfg<T, BM, BN, BK, TM, TN>::NT)
             const int gj = n0 + (j < TN / 2 ? tx * (TN / 2) + j : BN / 2 + tx * (TN / 2) + (j - TN / 2));
             if (gj >= n) continue;
             if (tri != 0 && (tri == 1 ? gi < gj : gi > gj)) continue;
-            C[(long)gj * ldc + gi] = epilogue(alpha, acc[i][j], beta, &cv[j]);
+            C[(long)gj * ldc + gi] = epilogue(alpha, acc_at(i, j), beta, &cv[j]);
         }
     }
 }
