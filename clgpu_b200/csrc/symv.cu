@@ -32,7 +32,6 @@
 namespace iclb {
 namespace {
 
-constexpr int kThreads = 256;  // finish kernel
 
 bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 
@@ -130,6 +129,10 @@ __global__ void __launch_bounds__(Tile<T>::THREADS) symv_tile_kernel(int n, int 
     // rows of the same columns: DRAM pages stay open): for upper storage the
     // row-major lower enumeration transposed, for lower storage the same
     // enumeration mirrored through the anti-diagonal.
+    // the finishing kernel (launched as a programmatic dependent) may be
+    // scheduled once every tile CTA has started; it waits for this grid's
+    // completion before reading Q
+    asm volatile("griddepcontrol.launch_dependents;");
     int I, J;
     tile_of(blockIdx.x, I, J);
     if (LOWER) {
@@ -254,26 +257,60 @@ __device__ __forceinline__ void acc_d(double& re, double& im, cfloat v)
 
 // y_i = alpha * sum_t Q[t][i] + beta * y_i, the reference's final expressions
 // (Ssymv_naive_lower.cl:34-37, Chemv_naive.cl:45-46) on the FP64 sum rounded
-// to T.
-__global__ void __launch_bounds__(kThreads) symv_finish_kernel(int n, int nb, const float* __restrict__ Q, long qld,
-                                                               float alpha, float beta, float* y, long incy)
+// to T.  The sum runs in a fixed order: kFinChunks contiguous runs of t, each
+// summed in order by one thread, then the runs in order.  A CTA takes 32
+// rows (a warp per run, consecutive rows in its lanes); one thread per row
+// summing all nb partials in sequence left 32 CTAs waiting on their loads
+// (10-15 us of a 65-100 us call).
+constexpr int kFinChunks = 8;
+constexpr int kFinThreads = 32 * kFinChunks;
+
+template <class T>
+__device__ __forceinline__ void finish_sums(int n, int nb, const T* __restrict__ Q, long qld, long i, double& re,
+                                            double& im)
 {
-    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    double s = 0.0, unused = 0.0;
-    for (int t = 0; t < nb; ++t) acc_d(s, unused, Q[(long)t * qld + i]);
+    __shared__ double sre[kFinChunks][32], sim[kFinChunks][32];
+    // the tile kernel's partials are complete and visible after this wait
+    // (a no-op when the launch was not a programmatic dependent)
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    const int lane = threadIdx.x & 31, c = threadIdx.x >> 5;
+    const int t0 = (int)((long)nb * c / kFinChunks), t1 = (int)((long)nb * (c + 1) / kFinChunks);
+    double r = 0.0, m = 0.0;
+    if (i < n)
+        for (int t = t0; t < t1; ++t) acc_d(r, m, Q[(long)t * qld + i]);
+    sre[c][lane] = r;
+    sim[c][lane] = m;
+    __syncthreads();
+    re = 0.0;
+    im = 0.0;
+#pragma unroll
+    for (int cc = 0; cc < kFinChunks; ++cc) {
+        re += sre[cc][lane];
+        im += sim[cc][lane];
+    }
+}
+
+__global__ void __launch_bounds__(kFinThreads) symv_finish_kernel(int n, int nb, const float* __restrict__ Q,
+                                                                  long qld, float alpha, float beta, float* y,
+                                                                  long incy)
+{
+    const long i = (long)blockIdx.x * 32 + (threadIdx.x & 31);
+    double s, unused;
+    finish_sums(n, nb, Q, qld, i, s, unused);
+    if (threadIdx.x >= 32 || i >= n) return;
     const float r = (float)s;
     float* yp = y + i * incy;
     *yp = (beta != 0.f) ? fmaf(alpha, r, __fmul_rn(beta, *yp)) : __fmul_rn(alpha, r);
 }
 
-__global__ void __launch_bounds__(kThreads) hemv_finish_kernel(int n, int nb, const cfloat* __restrict__ Q, long qld,
-                                                               cfloat alpha, cfloat beta, cfloat* y, long incy)
+__global__ void __launch_bounds__(kFinThreads) hemv_finish_kernel(int n, int nb, const cfloat* __restrict__ Q,
+                                                                  long qld, cfloat alpha, cfloat beta, cfloat* y,
+                                                                  long incy)
 {
-    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    double re = 0.0, im = 0.0;
-    for (int t = 0; t < nb; ++t) acc_d(re, im, Q[(long)t * qld + i]);
+    const long i = (long)blockIdx.x * 32 + (threadIdx.x & 31);
+    double re, im;
+    finish_sums(n, nb, Q, qld, i, re, im);
+    if (threadIdx.x >= 32 || i >= n) return;
     const cfloat r = cmul_fma(cfloat{(float)re, (float)im}, alpha);
     cfloat* yp = y + i * incy;
     if (beta.re != 0.f || beta.im != 0.f) {
@@ -282,6 +319,23 @@ __global__ void __launch_bounds__(kThreads) hemv_finish_kernel(int n, int nb, co
     } else {
         *yp = r;
     }
+}
+
+// launches `kernel` on the handle's stream as a programmatic dependent of the
+// kernel before it (its CTAs may be scheduled during that kernel's last wave)
+template <class K, class... Args>
+cudaError_t launch_dependent(iclblasHandle_t h, K kernel, unsigned grid, unsigned threads, Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(threads);
+    cfg.stream = h->stream;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
 template <class T, bool HERM>
@@ -314,9 +368,9 @@ cudaError_t ssymv(iclblasHandle_t h, int uplo, int n, float alpha, const float* 
     if (!Q) return cudaErrorMemoryAllocation;
     cudaError_t e = symv_tiles<float, false>(h, uplo == ICLBLAS_FILL_MODE_LOWER, n, A, lda, x, incx, Q, qld, nb);
     if (e != cudaSuccess) return e;
-    symv_finish_kernel<<<(n + kThreads - 1) / kThreads, kThreads, 0, h->stream>>>(n, nb, Q, qld, alpha, beta, y,
-                                                                                  incy);
-    return cudaGetLastError();
+    e = launch_dependent(h, symv_finish_kernel, (unsigned)((n + 31) / 32), (unsigned)kFinThreads, n, nb,
+                         (const float*)Q, qld, alpha, beta, y, (long)incy);
+    return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 cudaError_t chemv(iclblasHandle_t h, int uplo, int n, cfloat alpha, const cfloat* A, int lda, const cfloat* x,
@@ -329,9 +383,9 @@ cudaError_t chemv(iclblasHandle_t h, int uplo, int n, cfloat alpha, const cfloat
     if (!Q) return cudaErrorMemoryAllocation;
     cudaError_t e = symv_tiles<cfloat, true>(h, uplo == ICLBLAS_FILL_MODE_LOWER, n, A, lda, x, incx, Q, qld, nb);
     if (e != cudaSuccess) return e;
-    hemv_finish_kernel<<<(n + kThreads - 1) / kThreads, kThreads, 0, h->stream>>>(n, nb, Q, qld, alpha, beta, y,
-                                                                                  incy);
-    return cudaGetLastError();
+    e = launch_dependent(h, hemv_finish_kernel, (unsigned)((n + 31) / 32), (unsigned)kFinThreads, n, nb,
+                         (const cfloat*)Q, qld, alpha, beta, y, (long)incy);
+    return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 }  // namespace iclb
