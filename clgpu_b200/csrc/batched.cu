@@ -23,6 +23,7 @@
 // and, when ICLBLAS_TUNE_CACHE names a file, on disk (one "key rc ctas" line
 // each).  All arithmetic is FP32 FMA on the CUDA cores, whatever the handle's
 // math mode.
+#include <atomic>
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
@@ -552,12 +553,15 @@ cudaError_t launch_inv(iclblasHandle_t h, const int2* inv_items, int n_inv, cons
                        int lower_op, int op, int unit, const float* const* A, float* inv)
 {
     if (n_inv == 0) return cudaSuccess;
-    static bool attr = false;
-    if (!attr) {
+    // the attribute belongs to each device's copy of the kernel (the calls
+    // run with the handle's device current)
+    static std::atomic<unsigned long long> attr_set{0};
+    const unsigned long long bit = 1ull << (h->device & 63);
+    if (!(attr_set.load() & bit)) {
         cudaError_t e = cudaFuncSetAttribute(batched_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              kInvSmem);
         if (e != cudaSuccess) return e;
-        attr = true;
+        attr_set.fetch_or(bit);
     }
     batched_inv_kernel<<<n_inv, kInvThreads, kInvSmem, h->stream>>>(inv_items, dims, inv_off, lower_op, op, unit, A,
                                                                     inv);
