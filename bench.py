@@ -1209,9 +1209,9 @@ def run_batched_study(args, torch):
 def kernel_cases(torch, dev, B, h):
     """Named single-routine cases (name -> thunk) at sizes larger than L2 and
     a few GB on the device at most, for ncu captures of one kernel each:
-    complex level-1 at n = 2^25 (256 MiB per vector), CTRSV 8192 and STRSV
-    8192 with lda = n + 1 (the kernel for a leading dimension TMA cannot
-    address), plain SGEMM and TF32 SGEMM at 4096^3 (the CUDA-core kernel; the
+    complex level-1 at n = 2^25 (256 MiB per vector), CTRSV 8192, STRSV
+    8192 with lda = n (the TMA kernel) and with lda = n + 1 (the kernel for a
+    leading dimension TMA cannot address), plain SGEMM and TF32 SGEMM at 4096^3 (the CUDA-core kernel; the
     split pre-pass), STRSM 3xBF16 8192 x 4096 (the FP64 inverse kernels and
     the update GEMMs on operand planes) and the batched TRSM forward + adjoint
     at 128 instances of the batched config's size distribution."""
@@ -1237,6 +1237,8 @@ def kernel_cases(torch, dev, B, h):
     Ls = torch.zeros(nt * (nt + 1), device=dev)
     Ls.view(nt, nt + 1)[:, :nt] = tri(nt, False).t()   # column-major, lda = n + 1
     xs = rnd(nt)
+    Lt = tri(nt, False).t().contiguous().reshape(-1)    # column-major, lda = n (the TMA path)
+    xt = rnd(nt)
     ng = 4096
     Ag, Bg, Cg = rnd(ng * ng), rnd(ng * ng), torch.zeros(ng * ng, device=dev)
     mt, nr = 8192, 4096
@@ -1276,6 +1278,7 @@ def kernel_cases(torch, dev, B, h):
         "icamax": lambda: B.check(B.iclblasIcamax(h, nc, cx, 1, ri), "icamax"),
         "ctrsv": lambda: B.check(B.iclblasCtrsv(h, 1, 0, 0, nt, Lc, nt, xc, 1), "ctrsv"),
         "strsv_lda": lambda: B.check(B.iclblasStrsv(h, 1, 0, 0, nt, Ls, nt + 1, xs, 1), "strsv"),
+        "strsv_tma": lambda: B.check(B.iclblasStrsv(h, 1, 0, 0, nt, Lt, nt, xt, 1), "strsv"),
         "sgemm_plain": lambda: B.check(B.iclblasSgemm(h, 0, 0, ng, ng, ng, 1.0, Ag, ng, Bg, ng, 0.0, Cg, ng), "sgemm"),
         "sgemm_tf32": mode_call(B.MATH_TF32, lambda: B.check(
             B.iclblasSgemm(h, 0, 0, ng, ng, ng, 1.0, Ag, ng, Bg, ng, 0.0, Cg, ng), "sgemm")),
