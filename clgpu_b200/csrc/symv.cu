@@ -68,6 +68,7 @@ struct Tile {
     static constexpr int THREADS = sizeof(T) == 4 ? 512 : 256;
     static constexpr int WARPS = THREADS / 32;
     static constexpr int PASSES = TS / WARPS;          // columns per warp
+    static constexpr int MIN_CTAS = sizeof(T) == 4 ? 2 : 5;  // resident CTAs per SM the registers allow
 };
 
 // Stored tile number t -> (I, J) with I >= J (row-major over the lower block
@@ -114,7 +115,7 @@ __device__ __forceinline__ void tile_products(const T (&a)[Tile<T>::PASSES][Tile
 }
 
 template <class T, bool LOWER, bool HERM, bool VEC>
-__global__ void __launch_bounds__(Tile<T>::THREADS) symv_tile_kernel(int n, int nb, const T* __restrict__ A, long lda,
+__global__ void __launch_bounds__(Tile<T>::THREADS, Tile<T>::MIN_CTAS) symv_tile_kernel(int n, int nb, const T* __restrict__ A, long lda,
                                                                  const T* __restrict__ x, long incx,
                                                                  T* __restrict__ Q, long qld)
 {
