@@ -149,6 +149,26 @@ __global__ void __launch_bounds__(kInvThreads) batched_inv_kernel(const int2* __
 // op(A)^T X^T = alpha B^T.  Loads and stores then run along the rows.
 constexpr int KC = 16;
 
+// Two FP32 fused multiply-adds in one instruction (fma.rn.f32x2): each lane
+// rounded as fmaf, so results keep their bits; the accumulators are held in
+// pairs along the columns
+__device__ __forceinline__ unsigned long long pack2(float lo, float hi)
+{
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ float2 unpack2(unsigned long long v)
+{
+    float2 r;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
+    return r;
+}
+__device__ __forceinline__ void mac2(unsigned long long& acc, unsigned long long a, unsigned long long b)
+{
+    asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(acc) : "l"(a), "l"(b));
+}
+
 template <int RC, bool BT>
 __global__ void __launch_bounds__(256, 4) batched_trsm_kernel(int nitems, const int2* __restrict__ items,
                                                            const int* __restrict__ dims,
@@ -190,11 +210,12 @@ __global__ void __launch_bounds__(256, 4) batched_trsm_kernel(int nitems, const 
                 Ys[r][c] = (r < nr && c < nc) ? alpha * B[bi] : 0.f;
             }
             __syncthreads();
-            float acc[4][CPT];
+            unsigned long long acc[4][CPT / 2];  // column pairs
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
-                for (int j = 0; j < CPT; ++j) acc[i][j] = Ys[ty * 4 + i][tx * CPT + j];
+                for (int j = 0; j < CPT / 2; ++j)
+                    acc[i][j] = pack2(Ys[ty * 4 + i][tx * CPT + 2 * j], Ys[ty * 4 + i][tx * CPT + 2 * j + 1]);
 
             // ---- update by the earlier blocks: K = 64 p in slices of 16
             const int nslices = p * (TB / KC);
@@ -255,10 +276,15 @@ __global__ void __launch_bounds__(256, 4) batched_trsm_kernel(int nitems, const 
                             b[0] = bv.x; b[1] = bv.y;
                         }
                         const float av[4] = {a.x, a.y, a.z, a.w};
+                        unsigned long long bp[CPT / 2];
 #pragma unroll
-                        for (int i = 0; i < 4; ++i)
+                        for (int j = 0; j < CPT / 2; ++j) bp[j] = pack2(b[2 * j], b[2 * j + 1]);
 #pragma unroll
-                            for (int j = 0; j < CPT; ++j) acc[i][j] = fmaf(-av[i], b[j], acc[i][j]);
+                        for (int i = 0; i < 4; ++i) {
+                            const unsigned long long ap = pack2(-av[i], -av[i]);
+#pragma unroll
+                            for (int j = 0; j < CPT / 2; ++j) mac2(acc[i][j], ap, bp[j]);
+                        }
                     }
                     if (sl + 1 < nslices) store(buf ^ 1);
                     __syncthreads();
@@ -270,12 +296,16 @@ __global__ void __launch_bounds__(256, 4) batched_trsm_kernel(int nitems, const 
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
-                for (int j = 0; j < CPT; ++j) Ys[ty * 4 + i][tx * CPT + j] = acc[i][j];
-            float out[4][CPT];
+                for (int j = 0; j < CPT / 2; ++j) {
+                    const float2 v = unpack2(acc[i][j]);
+                    Ys[ty * 4 + i][tx * CPT + 2 * j] = v.x;
+                    Ys[ty * 4 + i][tx * CPT + 2 * j + 1] = v.y;
+                }
+            unsigned long long out[4][CPT / 2];
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
-                for (int j = 0; j < CPT; ++j) out[i][j] = 0.f;
+                for (int j = 0; j < CPT / 2; ++j) out[i][j] = 0ull;  // (+0.f, +0.f)
             const float* IB = IV + (long)kb * TB * TB;
             for (int kk0 = 0; kk0 < TB; kk0 += KC) {
                 __syncthreads();
@@ -300,17 +330,26 @@ __global__ void __launch_bounds__(256, 4) batched_trsm_kernel(int nitems, const 
                         b[0] = bv.x; b[1] = bv.y;
                     }
                     const float av[4] = {a.x, a.y, a.z, a.w};
+                    unsigned long long bp[CPT / 2];
 #pragma unroll
-                    for (int i = 0; i < 4; ++i)
+                    for (int j = 0; j < CPT / 2; ++j) bp[j] = pack2(b[2 * j], b[2 * j + 1]);
 #pragma unroll
-                        for (int j = 0; j < CPT; ++j) out[i][j] = fmaf(av[i], b[j], out[i][j]);
+                    for (int i = 0; i < 4; ++i) {
+                        const unsigned long long ap = pack2(av[i], av[i]);
+#pragma unroll
+                        for (int j = 0; j < CPT / 2; ++j) mac2(out[i][j], ap, bp[j]);
+                    }
                 }
             }
             __syncthreads();
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
-                for (int j = 0; j < CPT; ++j) Ys[ty * 4 + i][tx * CPT + j] = out[i][j];
+                for (int j = 0; j < CPT / 2; ++j) {
+                    const float2 v = unpack2(out[i][j]);
+                    Ys[ty * 4 + i][tx * CPT + 2 * j] = v.x;
+                    Ys[ty * 4 + i][tx * CPT + 2 * j + 1] = v.y;
+                }
             __syncthreads();
             for (int idx = t; idx < TB * RC; idx += 256) {
                 const int r = BT ? idx / RC : idx % TB, cc = BT ? idx % RC : idx / TB;
@@ -362,11 +401,11 @@ __global__ void __launch_bounds__(256, 4) batched_gemm_kernel(int nitems, const 
         // adjoint tiles entirely off the kept triangle are only zeroed
         bool skip = false;
         if (MODE == 1) skip = tri_lower ? (j0 > i0 + TB - 1) : (i0 > j0 + RC - 1);
-        float acc[4][CPT];
+        unsigned long long acc[4][CPT / 2];  // column pairs
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
-            for (int j = 0; j < CPT; ++j) acc[i][j] = 0.f;
+            for (int j = 0; j < CPT / 2; ++j) acc[i][j] = 0ull;  // (+0.f, +0.f)
         const int nslices = skip ? 0 : (k + KC - 1) / KC;
         float ra[4], rb[BPT];
         auto load = [&](int sl) {
@@ -427,10 +466,15 @@ __global__ void __launch_bounds__(256, 4) batched_gemm_kernel(int nitems, const 
                         b[0] = bv.x; b[1] = bv.y;
                     }
                     const float av[4] = {a.x, a.y, a.z, a.w};
+                    unsigned long long bp[CPT / 2];
 #pragma unroll
-                    for (int i = 0; i < 4; ++i)
+                    for (int j = 0; j < CPT / 2; ++j) bp[j] = pack2(b[2 * j], b[2 * j + 1]);
 #pragma unroll
-                        for (int j = 0; j < CPT; ++j) acc[i][j] = fmaf(av[i], b[j], acc[i][j]);
+                    for (int i = 0; i < 4; ++i) {
+                        const unsigned long long ap = pack2(av[i], av[i]);
+#pragma unroll
+                        for (int j = 0; j < CPT / 2; ++j) mac2(acc[i][j], ap, bp[j]);
+                    }
                 }
                 if (sl + 1 < nslices) store(buf ^ 1);
                 __syncthreads();
@@ -442,13 +486,15 @@ __global__ void __launch_bounds__(256, 4) batched_gemm_kernel(int nitems, const 
             for (int j = 0; j < CPT; ++j) {
                 const int r = i0 + ty * 4 + i, c = j0 + tx * CPT + j;
                 if (r >= m || c >= n) continue;
+                const float2 v2 = unpack2(acc[i][j / 2]);
+                const float v = (j & 1) ? v2.y : v2.x;
                 float* cp = C + (long)c * ldc + r;
                 if (MODE == 1) {
                     const bool keep = tri_lower ? (r > c || (r == c && !tri_strict))
                                                 : (r < c || (r == c && !tri_strict));
-                    *cp = keep ? alpha * acc[i][j] : 0.f;
+                    *cp = keep ? alpha * v : 0.f;
                 } else {
-                    *cp = beta == 0.f ? alpha * acc[i][j] : fmaf(alpha, acc[i][j], __fmul_rn(beta, *cp));
+                    *cp = beta == 0.f ? alpha * v : fmaf(alpha, v, __fmul_rn(beta, *cp));
                 }
             }
     }
