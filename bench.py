@@ -1146,42 +1146,56 @@ def run_batched_study(args, torch):
         return worst
 
     out = []
+    ms_copy = None
     with B.Handle() as h, torch.cuda.stream(stream):
         h.set_stream(stream)
-        plan = B.BatchPlan(h, "trsm", side=0, uplo=1, trans=0, diag=0, m=[int(v) for v in ns],
-                           n=[int(v) for v in rs], lda=[int(v) for v in ns], ldb=[int(v) for v in ns])
-        # the adjoint uses the forward call's diagonal-block inverses (same A)
-        B.check(plan.set_inverse_reuse(True), "set_inverse_reuse")
-        _, width, ctas = plan.info()
+        modes = [("plain_fp32", B.MATH_PLAIN_FP32), ("bf16x3", B.MATH_BF16X3), ("bf16x6", B.MATH_BF16X6),
+                 ("tf32", B.MATH_TF32)]
+        for mname, mode in modes:
+            if args.math != "all" and mname not in ("plain_fp32", args.math):
+                continue
+            # a plan takes the handle's math mode at creation
+            h.set_math_mode(mode)
+            plan = B.BatchPlan(h, "trsm", side=0, uplo=1, trans=0, diag=0, m=[int(v) for v in ns],
+                               n=[int(v) for v in rs], lda=[int(v) for v in ns], ldb=[int(v) for v in ns])
+            # the adjoint uses the forward call's diagonal-block inverses (same A)
+            B.check(plan.set_inverse_reuse(True), "set_inverse_reuse")
+            _, width, ctas = plan.info()
 
-        def step():
-            B.check(B.iclblasStrsmBatchedUneven(h, plan, 1.0, pA, pX), "batched trsm")
-            B.check(B.iclblasStrsmBatchedUnevenBackward(h, plan, 1.0, pA, pX, pG, pdA), "batched adjoint")
+            def step():
+                B.check(B.iclblasStrsmBatchedUneven(h, plan, 1.0, pA, pX), "batched trsm")
+                B.check(B.iclblasStrsmBatchedUnevenBackward(h, plan, 1.0, pA, pX, pG, pdA), "batched adjoint")
 
-        # the restore copies are captured too; their own graph's time is subtracted
-        restore()
-        torch.cuda.synchronize()
-        graph = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(graph, stream=stream):
+            # the restore copies are captured too; their own graph's time is subtracted
             restore()
-            step()
-        rgraph = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(rgraph, stream=stream):
-            restore()
-        for _ in range(args.warmup):
+            torch.cuda.synchronize()
+            graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(graph, stream=stream):
+                restore()
+                step()
+            rgraph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(rgraph, stream=stream):
+                restore()
+            for _ in range(args.warmup):
+                graph.replay()
+            reps = max(args.steps, 3)
+            ms_all = timed(graph.replay, reps)
+            ms_copy = timed(rgraph.replay, reps)
+            ms = max(ms_all - ms_copy, 1e-6)
             graph.replay()
-        reps = max(args.steps, 3)
-        ms_all = timed(graph.replay, reps)
-        ms_copy = timed(rgraph.replay, reps)
-        ms = max(ms_all - ms_copy, 1e-6)
-        graph.replay()
-        torch.cuda.synchronize()
-        ex, eg, ea = errors()
-        r = {"routine": "batched strsm fwd+adjoint", "batch": batch, "form": "persistent launches in a CUDA graph",
-             "tile_width": width, "ctas_per_sm": ctas, "tflops": round(flops / (ms / 1e3) / 1e12, 3),
-             "ms": round(ms, 3), "err_X": ex, "err_dB": eg, "err_dA": ea}
-        print(json.dumps(r), flush=True)
-        out.append(r)
+            torch.cuda.synchronize()
+            ex, eg, ea = errors()
+            r = {"routine": "batched strsm fwd+adjoint", "batch": batch, "math": mname,
+                 "form": "persistent launches in a CUDA graph" if mode == B.MATH_PLAIN_FP32
+                 else "tensor-core launches per block step in a CUDA graph",
+                 "tile_width": width, "ctas_per_sm": ctas, "tflops": round(flops / (ms / 1e3) / 1e12, 3),
+                 "ms": round(ms, 3), "err_X": ex, "err_dB": eg, "err_dA": ea}
+            print(json.dumps(r), flush=True)
+            out.append(r)
+            del graph, rgraph
+            plan.destroy()
+        if args.math != "all" and not args.batched_loop:
+            return out
 
         # plain form: per-instance calls (PLAIN_FP32)
         h.set_math_mode(B.MATH_PLAIN_FP32)
@@ -1200,8 +1214,6 @@ def run_batched_study(args, torch):
              "err_dA": ea}
         print(json.dumps(r), flush=True)
         out.append(r)
-        del graph, rgraph
-        plan.destroy()
     return out
 
 
@@ -1452,6 +1464,10 @@ def main():
     ap.add_argument("--skip-cgemm", action="store_true")
     ap.add_argument("--quick", action="store_true")
     ap.add_argument("--batch", type=int, default=512)
+    ap.add_argument("--math", default="all", choices=["all", "bf16x3", "bf16x6", "tf32"],
+                    help="batched study: the tensor-core modes to time beside plain FP32")
+    ap.add_argument("--batched-loop", action="store_true",
+                    help="batched study with --math: also time the per-instance plain calls")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

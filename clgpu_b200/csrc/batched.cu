@@ -21,8 +21,9 @@
 // by timing the candidates on synthetic operands of the plan's shapes when
 // the plan is created; the choice is cached per (kind, shapes, GPU) in memory
 // and, when ICLBLAS_TUNE_CACHE names a file, on disk (one "key rc ctas" line
-// each).  All arithmetic is FP32 FMA on the CUDA cores, whatever the handle's
-// math mode.
+// each).  This is the plain-FP32 path (FP32 FMA on the CUDA cores); a plan
+// created while the handle is in the TF32, 3xBF16 or 6xBF16 mode runs the
+// tensor-core path of batched_tc.cu instead (no tuning, no work queue).
 #include <atomic>
 #include <algorithm>
 #include <cstdio>
@@ -37,6 +38,22 @@
 #include "common.cuh"
 
 namespace iclb {
+
+// The tensor-core path of plans created in the TF32 / 3xBF16 / 6xBF16 math
+// modes (batched_tc.cu).
+bool batch_tc_mode(iclblasMathMode_t mode);
+void batch_tc_free(BatchTc* t);
+cudaError_t batch_tc_create_trsm(iclblasHandle_t h, iclblasBatchPlan* plan, const std::vector<int>& dims, int right,
+                                 int lower_f, int op_f, int tri_lower, int unit);
+cudaError_t batch_tc_create_gemm(iclblasHandle_t h, iclblasBatchPlan* plan, const std::vector<int>& dims, int ta,
+                                 int tb);
+cudaError_t batch_tc_inverses(iclblasHandle_t h, const iclblasBatchPlan* plan, const float* const* A);
+cudaError_t batch_tc_solve(iclblasHandle_t h, const iclblasBatchPlan* plan, int adjoint, float alpha,
+                           const float* const* A, float* const* B);
+cudaError_t batch_tc_dA(iclblasHandle_t h, const iclblasBatchPlan* plan, float scale, const float* const* P,
+                        const float* const* Q, float* const* dA);
+cudaError_t batch_tc_gemm(iclblasHandle_t h, const iclblasBatchPlan* plan, float alpha, const float* const* A,
+                          const float* const* B, float beta, float* const* C);
 
 namespace {
 
@@ -905,6 +922,8 @@ void batch_plan_free(iclblasBatchPlan* p)
     if (!p) return;
     batch_list_free(p->main);
     batch_list_free(p->adj);
+    batch_tc_free(p->tc);
+    p->tc = nullptr;
     if (p->counter) cudaFree(p->counter);
     if (p->inv) cudaFree(p->inv);
     if (p->inv_off) cudaFree(p->inv_off);
@@ -971,11 +990,19 @@ cudaError_t batch_plan_create_trsm(iclblasHandle_t h, int side, int uplo, int tr
     // the right side solves op(A)^T X^T = alpha B^T: flipped operator, B's rows
     const int s_lower = right ? !lower_op_of(uplo, trans) : lower_op_of(uplo, trans);
     const int s_op = right ? !op : op;
-    if (e == cudaSuccess) e = tune_trsm(h, batch, dims, s_lower, s_op, unit, right, p->main);
-    // dA: left -(1/alpha) dB X^T (op N) or X dB^T; right -(1/alpha) X^T dB (op N) or dB^T X
-    if (e == cudaSuccess)
-        e = tune_gemm(h, batch, adims, right ? 1 : 0, right ? 0 : 1, true, uplo == ICLBLAS_FILL_MODE_LOWER, unit,
-                      p->adj);
+    if (batch_tc_mode(h->math)) {
+        // tensor-core path: 128-row tiles, one persistent CTA per SM
+        p->main.rc = 128;
+        p->main.ctas_per_sm = 1;
+        if (e == cudaSuccess)
+            e = batch_tc_create_trsm(h, p, dims, right ? 1 : 0, s_lower, s_op, uplo == ICLBLAS_FILL_MODE_LOWER, unit);
+    } else {
+        if (e == cudaSuccess) e = tune_trsm(h, batch, dims, s_lower, s_op, unit, right, p->main);
+        // dA: left -(1/alpha) dB X^T (op N) or X dB^T; right -(1/alpha) X^T dB (op N) or dB^T X
+        if (e == cudaSuccess)
+            e = tune_gemm(h, batch, adims, right ? 1 : 0, right ? 0 : 1, true, uplo == ICLBLAS_FILL_MODE_LOWER,
+                          unit, p->adj);
+    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) {
         batch_plan_free(p);
@@ -1009,7 +1036,13 @@ cudaError_t batch_plan_create_gemm(iclblasHandle_t h, int transa, int transb, in
     const int ta = transa != ICLBLAS_OP_N, tb = transb != ICLBLAS_OP_N;
     cudaError_t e = cudaMalloc(&p->counter, sizeof(unsigned));
     if (e == cudaSuccess) e = upload_dims(dims, p->main);
-    if (e == cudaSuccess) e = tune_gemm(h, batch, dims, ta, tb, false, 0, 0, p->main);
+    if (batch_tc_mode(h->math)) {
+        p->main.rc = 128;
+        p->main.ctas_per_sm = 1;
+        if (e == cudaSuccess) e = batch_tc_create_gemm(h, p, dims, ta, tb);
+    } else if (e == cudaSuccess) {
+        e = tune_gemm(h, batch, dims, ta, tb, false, 0, 0, p->main);
+    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) {
         batch_plan_free(p);
@@ -1030,6 +1063,11 @@ cudaError_t batch_trsm(iclblasHandle_t h, const iclblasBatchPlan* p, float alpha
     cudaError_t e = launch_inv(h, p->inv_items, p->n_inv, p->main.dims, p->inv_off, lower_op, op,
                                p->diag == ICLBLAS_DIAG_UNIT, A, p->inv);
     if (e != cudaSuccess) return e;
+    if (p->tc) {
+        if ((e = batch_tc_inverses(h, p, A)) != cudaSuccess) return e;
+        p->inv_formed = true;
+        return batch_tc_solve(h, p, 0, alpha, A, B);
+    }
     p->inv_formed = true;
     return launch_trsm(h, p->main, p->counter, p->inv_off, p->inv, lower_op, op, 0, right, alpha, A, B);
 }
@@ -1037,6 +1075,7 @@ cudaError_t batch_trsm(iclblasHandle_t h, const iclblasBatchPlan* p, float alpha
 cudaError_t batch_gemm(iclblasHandle_t h, const iclblasBatchPlan* p, float alpha, const float* const* A,
                        const float* const* B, float beta, float* const* C)
 {
+    if (p->tc) return batch_tc_gemm(h, p, alpha, A, B, beta, C);
     return launch_gemm(h, p->main, p->counter, false, p->transa != ICLBLAS_OP_N, p->transb != ICLBLAS_OP_N, alpha,
                        beta, A, B, C, 0, 0);
 }
@@ -1057,16 +1096,20 @@ cudaError_t batch_trsm_backward(iclblasHandle_t h, const iclblasBatchPlan* p, fl
     const int f_lower = lower_op_of(p->uplo, p->trans) ^ (right ? 1 : 0);
     const int f_op = op ^ (right ? 1 : 0);
     cudaError_t e = cudaSuccess;
-    if (!(p->reuse_inv && p->inv_formed))
+    if (!(p->reuse_inv && p->inv_formed)) {
         e = launch_inv(h, p->inv_items, p->n_inv, p->main.dims, p->inv_off, f_lower, f_op, unit, A, p->inv);
+        if (e == cudaSuccess && p->tc) e = batch_tc_inverses(h, p, A);
+    }
     if (e == cudaSuccess)
-        e = launch_trsm(h, p->main, p->counter, p->inv_off, p->inv, !f_lower, !f_op, 1, right, alpha, A, G);
+        e = p->tc ? batch_tc_solve(h, p, 1, alpha, A, G)
+                  : launch_trsm(h, p->main, p->counter, p->inv_off, p->inv, !f_lower, !f_op, 1, right, alpha, A, G);
     if (e != cudaSuccess || !dA) return e;
     const float s = alpha != 0.f ? -1.f / alpha : 0.f;
     const float* const* Gc = const_cast<const float* const*>(G);
     // left: dM = -W X^T; right: dM = -X^T W; dA = dM (op N) or dM^T (op T/C)
     const float* const* P = right ? (op ? Gc : X) : (op ? X : Gc);
     const float* const* Q = right ? (op ? X : Gc) : (op ? Gc : X);
+    if (p->tc) return batch_tc_dA(h, p, s, P, Q, dA);
     return launch_gemm(h, p->adj, p->counter, true, right ? 1 : 0, right ? 0 : 1, s, 0.f, P, Q, dA,
                        p->uplo == ICLBLAS_FILL_MODE_LOWER, unit);
 }

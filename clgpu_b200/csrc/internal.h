@@ -284,6 +284,7 @@ struct BatchList {
     int ctas_per_sm = 1;
 };
 cudaError_t batch_list_free(BatchList& l);
+struct BatchTc;  // a plan's tensor-core path (batched_tc.cu)
 
 }  // namespace iclb
 
@@ -310,6 +311,9 @@ struct iclblasBatchPlan {
     // (iclblasBatchPlanSetInverseReuse); inv_formed: a forward call formed them
     bool reuse_inv = false;
     mutable bool inv_formed = false;
+    // plans created in a tensor-core math mode (TF32, 3xBF16, 6xBF16): the
+    // tiled operand planes and launch lists of that path; null in PLAIN_FP32
+    iclb::BatchTc* tc = nullptr;
 };
 
 namespace iclb {
