@@ -83,7 +83,10 @@ __global__ void __launch_bounds__(kInvThreads) batched_inv_kernel(const int2* __
     extern __shared__ double ysm[];
     double(*Y)[TB + 1] = (double(*)[TB + 1])ysm;              // the inverse being built
     double(*Tm)[TB / 2 + 1] = (double(*)[TB / 2 + 1])(ysm + TB * (TB + 1));  // doubling temporary
-    float(*D)[TB + 1] = (float(*)[TB + 1])(ysm + TB * (TB + 1) + (TB / 2) * (TB / 2 + 1));
+    // the block itself, held in FP64 so that the products below convert
+    // nothing in their inner loops (FP32 -> FP64 conversions run at a
+    // quarter of the FP64 FMA rate)
+    double(*D)[TB + 1] = (double(*)[TB + 1])(ysm + TB * (TB + 1) + (TB / 2) * (TB / 2 + 1));
     const int t = threadIdx.x;
     const int2 w = inv_items[blockIdx.x];
     const int* d = dims + 4 * w.x;
@@ -93,7 +96,7 @@ __global__ void __launch_bounds__(kInvThreads) batched_inv_kernel(const int2* __
     const int r0 = w.y * TB, nr = min(TB, m - r0);
     for (int idx = t; idx < TB * TB; idx += kInvThreads) {
         const int r = idx % TB, c = idx / TB;  // A-local (r, c): coalesced down A's columns
-        float v = (r == c && (r >= nr || unit)) ? 1.f : 0.f;
+        double v = (r == c && (r >= nr || unit)) ? 1.0 : 0.0;
         if (r < nr && c < nr && !(r == c && unit)) v = A[(long)(r0 + c) * lda + r0 + r];
         if (op == 0) D[r][c] = v;
         else D[c][r] = v;
@@ -106,14 +109,14 @@ __global__ void __launch_bounds__(kInvThreads) batched_inv_kernel(const int2* __
         if (lower_op) {
             for (int i = 0; i < 16; ++i) {
                 double y = (i == j) ? 1.0 : 0.0;
-                for (int k = j; k < i; ++k) y = fma(-(double)D[b + i][b + k], Y[b + k][b + j], y);
-                Y[b + i][b + j] = (i >= j) ? y / (double)D[b + i][b + i] : 0.0;
+                for (int k = j; k < i; ++k) y = fma(-D[b + i][b + k], Y[b + k][b + j], y);
+                Y[b + i][b + j] = (i >= j) ? y / D[b + i][b + i] : 0.0;
             }
         } else {
             for (int i = 15; i >= 0; --i) {
                 double y = (i == j) ? 1.0 : 0.0;
-                for (int k = i + 1; k <= j; ++k) y = fma(-(double)D[b + i][b + k], Y[b + k][b + j], y);
-                Y[b + i][b + j] = (i <= j) ? y / (double)D[b + i][b + i] : 0.0;
+                for (int k = i + 1; k <= j; ++k) y = fma(-D[b + i][b + k], Y[b + k][b + j], y);
+                Y[b + i][b + j] = (i <= j) ? y / D[b + i][b + i] : 0.0;
             }
         }
     }
@@ -127,9 +130,9 @@ __global__ void __launch_bounds__(kInvThreads) batched_inv_kernel(const int2* __
             const int o = pr * 2 * h;
             double acc = 0.0;
             if (lower_op) {
-                for (int k = 0; k < h; ++k) acc = fma((double)D[o + h + r][o + k], Y[o + k][o + c], acc);
+                for (int k = 0; k < h; ++k) acc = fma(D[o + h + r][o + k], Y[o + k][o + c], acc);
             } else {
-                for (int k = 0; k < h; ++k) acc = fma((double)D[o + r][o + h + k], Y[o + h + k][o + h + c], acc);
+                for (int k = 0; k < h; ++k) acc = fma(D[o + r][o + h + k], Y[o + h + k][o + h + c], acc);
             }
             Tm[pr * h + r][c] = acc;
         }
@@ -608,8 +611,7 @@ int grid_of(iclblasHandle_t h, const BatchList& l)
 }
 
 // ---------------------------------------------------------------- host: launches
-constexpr int kInvSmem = TB * (TB + 1) * (int)(sizeof(double) + sizeof(float)) +
-                         (TB / 2) * (TB / 2 + 1) * (int)sizeof(double);
+constexpr int kInvSmem = TB * (TB + 1) * (int)(2 * sizeof(double)) + (TB / 2) * (TB / 2 + 1) * (int)sizeof(double);
 
 // The pass forming the diagonal-block inverses of M = op(A).
 cudaError_t launch_inv(iclblasHandle_t h, const int2* inv_items, int n_inv, const int* dims, const long* inv_off,

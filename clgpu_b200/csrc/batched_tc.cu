@@ -258,7 +258,7 @@ enum EpiKind { kEpiInv = 0, kEpiUpd = 1, kEpiGemm = 2, kEpiMask = 3 };
 // planes, when written, get (row j = column within the column tile, K =
 // row) in tile (column tile, row / KT).
 template <bool TF32, int EK>
-__device__ __forceinline__ void epilogue_group(const MmaLaunch& p, const float (&v)[32], int inst, int row, int ct,
+__device__ __forceinline__ void epilogue_group(const MmaLaunch& p, float (&v)[32], int inst, int row, int ct,
                                                int c0, const int4 ci)
 {
     constexpr int KT = TF32 ? 32 : 64;
@@ -269,47 +269,54 @@ __device__ __forceinline__ void epilogue_group(const MmaLaunch& p, const float (
     const int ncv = rv ? min(32, cols - col0) : 0;  // columns of this thread inside C
     float* const cp = p.C[inst] + (p.ct ? (long)row * ld + col0 : (long)col0 * ld + row);
     const long cs = p.ct ? 1 : ld;
-    float x[32];
+    // v becomes the value stored (C) or split (planes)
     if constexpr (EK == kEpiUpd || EK == kEpiGemm) {
         const bool load = EK == kEpiUpd || p.c_beta != 0.f;
 #pragma unroll
-        for (int j = 0; j < 32; ++j) x[j] = (load && j < ncv) ? cp[j * cs] : 0.f;
-    }
-    if constexpr (EK == kEpiUpd) {
+        for (int h = 0; h < 32; h += 16) {  // two halves: 16 loads in flight, fewer live registers
+            float x[16];
 #pragma unroll
-        for (int j = 0; j < 32; ++j) x[j] = x[j] - v[j];
-    } else if constexpr (EK == kEpiGemm) {
-        const bool beta = p.c_beta != 0.f;
+            for (int j = 0; j < 16; ++j) x[j] = (load && h + j < ncv) ? cp[(h + j) * cs] : 0.f;
 #pragma unroll
-        for (int j = 0; j < 32; ++j) x[j] = beta ? fmaf(p.c_alpha, v[j], p.c_beta * x[j]) : p.c_alpha * v[j];
+            for (int j = 0; j < 16; ++j) {
+                if constexpr (EK == kEpiUpd) {
+                    v[h + j] = x[j] - v[h + j];
+                } else {  // stored at once: v is not needed after
+                    const float y = load ? fmaf(p.c_alpha, v[h + j], p.c_beta * x[j]) : p.c_alpha * v[h + j];
+                    if (h + j < ncv) cp[(h + j) * cs] = y;
+                }
+            }
+        }
     } else if constexpr (EK == kEpiMask) {
         const bool strict = (p.mask & 4) != 0, lower = (p.mask & 3) == 1;
 #pragma unroll
         for (int j = 0; j < 32; ++j) {
             const int col = col0 + j;
             const bool keep = lower ? (strict ? row > col : row >= col) : (strict ? row < col : row <= col);
-            x[j] = keep ? p.c_alpha * v[j] : 0.f;
+            v[j] = keep ? p.c_alpha * v[j] : 0.f;
         }
-    } else {
-#pragma unroll
-        for (int j = 0; j < 32; ++j) x[j] = p.c_alpha * v[j];
     }
-    if constexpr (EK != kEpiUpd) {
+    if constexpr (EK == kEpiInv) {
 #pragma unroll
         for (int j = 0; j < 32; ++j)
-            if (j < ncv) cp[j * cs] = x[j];
+            if (j < ncv) cp[j * cs] = p.c_alpha * v[j];
+    } else if constexpr (EK == kEpiMask) {
+#pragma unroll
+        for (int j = 0; j < 32; ++j)
+            if (j < ncv) cp[j * cs] = v[j];
     }
     if constexpr (EK == kEpiInv || EK == kEpiUpd) {
-        // plane value: acc (X_s) or C - acc (Y_s); zero outside C
-        // K index = this thread's C row; tile row = c0 + j, whose swizzle
-        // phase is j % 8 (c0 is a multiple of 32)
+        // planes of acc (X_s) or C - acc (Y_s), zero outside C: row j = C
+        // column c0 + j of this column tile, K = this thread's row (a warp
+        // writes 32 consecutive K values of one tile row per store); the
+        // tile row's swizzle phase is j % 8 (c0 is a multiple of 8)
         char* const tile = p.w.base + tile_index(p.w, inst, ct, row / KT) * TILE_BYTES;
         const int b = (row % KT) * ESIZE;
         char* const base = tile + (long)c0 * ROWB + (b & 15);
         const int chunk = (b >> 4) << 4;
 #pragma unroll
         for (int j = 0; j < 32; ++j) {
-            const float pv = j < ncv ? (EK == kEpiInv ? v[j] : x[j]) : 0.f;
+            const float pv = j < ncv ? v[j] : 0.f;
             char* const a = base + j * ROWB + (chunk ^ ((j & 7) << 4));
             if (TF32) {
                 *(float*)a = to_tf32(pv);
@@ -449,22 +456,22 @@ __global__ void __launch_bounds__(THREADS, 1) btc_mma_kernel(const __grid_consta
             }
             const int4 ci = p.cinfo[inst];
             const int c0 = cg * 32;
-            if (c0 < b_rows(ci.y, ct)) {
-                float v[32];
-                if (nk > 0) {
-                    tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * TR + c0), v);
-                } else {
+            const bool active = c0 < b_rows(ci.y, ct);
+            float v[32];
+            if (nk > 0 && active) {
+                tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * TR + c0), v);
+            } else {
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) v[j] = 0.f;
-                }
-                epilogue_group<TF32, EK>(p, v, inst, rt * TR + r, ct, c0, ci);
+                for (int j = 0; j < 32; ++j) v[j] = 0.f;
             }
             if (nk > 0) {
+                // the values are in registers: the accumulator is free
                 tc_fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&tempty[acc]);
                 if (++acc == 2) { acc = 0; acc_ph ^= 1; }
             }
+            if (active) epilogue_group<TF32, EK>(p, v, inst, rt * TR + r, ct, c0, ci);
         }
     }
 
@@ -506,17 +513,32 @@ __global__ void __launch_bounds__(256) btc_split_kernel(const __grid_constant__ 
     const long ld = in.z;
     const float* S = k.src[inst];
     const int r0 = rt * TR, k0 = kt * KT, t = threadIdx.x;
+    // every load of the thread is issued before the first shared-memory store
+    constexpr int PER = TR * KT / 256;
+    float v[PER];
     if (k.rmajor) {
-        for (int idx = t; idx < TR * KT; idx += 256) {
-            const int rr = idx / KT, kk = idx % KT;
+#pragma unroll
+        for (int u = 0; u < PER; ++u) {
+            const int idx = t + u * 256, rr = idx / KT, kk = idx % KT;
             const int r = r0 + rr, c = k0 + kk;
-            tile[rr][kk] = (r < R && c < K) ? S[(long)r * ld + c] : 0.f;
+            v[u] = (r < R && c < K) ? S[(long)r * ld + c] : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < PER; ++u) {
+            const int idx = t + u * 256;
+            tile[idx / KT][idx % KT] = v[u];
         }
     } else {
-        for (int idx = t; idx < TR * KT; idx += 256) {
-            const int rr = idx % TR, kk = idx / TR;
+#pragma unroll
+        for (int u = 0; u < PER; ++u) {
+            const int idx = t + u * 256, rr = idx % TR, kk = idx / TR;
             const int r = r0 + rr, c = k0 + kk;
-            tile[rr][kk] = (r < R && c < K) ? S[r + (long)c * ld] : 0.f;
+            v[u] = (r < R && c < K) ? S[r + (long)c * ld] : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < PER; ++u) {
+            const int idx = t + u * 256;
+            tile[idx % TR][idx / TR] = v[u];
         }
     }
     __syncthreads();
@@ -552,8 +574,10 @@ __global__ void __launch_bounds__(256) btc_split_kernel(const __grid_constant__ 
 // missing second block) and the off-diagonal block C of M,
 //   lower: inv = [[P^-1, 0], [-Q^-1 (C P^-1), Q^-1]]
 //   upper: inv = [[P^-1, -P^-1 (C Q^-1)], [0, Q^-1]]
-// with both products accumulated in FP64 (4 x 4 outputs per thread); the
-// block is written as tiled planes of inv (row r, K c) and of inv^T.
+// with both products in FP64 (operands held in FP64 in shared memory, so
+// that the inner loops convert nothing; 4 x 4 outputs per thread).  The
+// block is then staged in FP32 and written as tiled planes of inv (row r,
+// K c) and of inv^T.
 struct InvLaunch {
     const int2* items;       // (instance, 128-row block)
     const int* dims;         // per instance: na, nr, lda, ldb
@@ -564,7 +588,8 @@ struct InvLaunch {
     Opnd w, wt;
     int nlev;
 };
-constexpr int kInvSmemBytes = 3 * 64 * 65 * (int)sizeof(float) + 64 * 65 * (int)sizeof(double);
+constexpr int kInvLd = 65;                                        // FP64 64 x 64 row stride
+constexpr int kInvSmemBytes = 4 * 64 * kInvLd * (int)sizeof(double);  // P, Q, C, T
 
 template <bool TF32>
 __global__ void __launch_bounds__(256) btc_inv_kernel(const __grid_constant__ InvLaunch p)
@@ -572,11 +597,14 @@ __global__ void __launch_bounds__(256) btc_inv_kernel(const __grid_constant__ In
     constexpr int KT = TF32 ? 32 : 64;
     constexpr int ESIZE = TF32 ? 4 : 2;
     constexpr int EPC = 16 / ESIZE;  // elements per 16-byte chunk
+    constexpr int CPR = TR / EPC;    // chunks per 128-element row
+    constexpr int FLD = TR + 1;      // FP32 staging row stride
     extern __shared__ double inv_smem[];
-    double(*T)[65] = (double(*)[65])inv_smem;
-    float(*P)[65] = (float(*)[65])(inv_smem + 64 * 65);
-    float(*Q)[65] = P + 64;
-    float(*Cm)[65] = Q + 64;
+    double(*P)[kInvLd] = (double(*)[kInvLd])inv_smem;
+    double(*Q)[kInvLd] = P + 64;
+    double(*Cm)[kInvLd] = Q + 64;
+    double(*T)[kInvLd] = Cm + 64;
+    float(*F)[FLD] = (float(*)[FLD])(Cm);  // the finished block (over C and T)
     const int t = threadIdx.x;
     const int2 it = p.items[blockIdx.x];
     const int inst = it.x, b = it.y;
@@ -591,10 +619,10 @@ __global__ void __launch_bounds__(256) btc_inv_kernel(const __grid_constant__ In
     for (int idx = t; idx < 64 * 64; idx += 256) {
         const int rr = idx % 64, cc = idx / 64;  // column-major: coalesced
         P[rr][cc] = inv[(long)(2 * b) * 4096 + idx];
-        Q[rr][cc] = has_q ? inv[(long)(2 * b + 1) * 4096 + idx] : (rr == cc ? 1.f : 0.f);
+        Q[rr][cc] = has_q ? inv[(long)(2 * b + 1) * 4096 + idx] : (rr == cc ? 1.0 : 0.0);
         // off-diagonal block of M (local rows i, columns j of the 128 block)
         const int i = p.lower ? 64 + rr : rr, j = p.lower ? cc : 64 + cc;
-        float v = 0.f;
+        double v = 0.0;
         if (r0 + i < na && r0 + j < na)
             v = p.op ? A[(long)(r0 + j) + (long)(r0 + i) * lda] : A[(long)(r0 + i) + (long)(r0 + j) * lda];
         Cm[rr][cc] = v;
@@ -603,7 +631,7 @@ __global__ void __launch_bounds__(256) btc_inv_kernel(const __grid_constant__ In
     const int tr = (t >> 4) * 4, tc = (t & 15) * 4;
     {
         // T = C P^-1 (lower) or C Q^-1 (upper)
-        float(*R)[65] = p.lower ? P : Q;
+        double(*R)[kInvLd] = p.lower ? P : Q;
         double acc[4][4] = {};
         for (int k = 0; k < 64; ++k) {
             double a[4], bb[4];
@@ -622,10 +650,10 @@ __global__ void __launch_bounds__(256) btc_inv_kernel(const __grid_constant__ In
             for (int j = 0; j < 4; ++j) T[tr + i][tc + j] = acc[i][j];
     }
     __syncthreads();
+    // off-diagonal block of the inverse: -Q^-1 T (lower) or -P^-1 T (upper)
+    double off[4][4] = {};
     {
-        // off-diagonal block of the inverse: -Q^-1 T (lower) or -P^-1 T (upper), into Cm
-        float(*L)[65] = p.lower ? Q : P;
-        double acc[4][4] = {};
+        double(*L)[kInvLd] = p.lower ? Q : P;
         for (int k = 0; k < 64; ++k) {
             double a[4], bb[4];
 #pragma unroll
@@ -635,34 +663,41 @@ __global__ void __launch_bounds__(256) btc_inv_kernel(const __grid_constant__ In
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], bb[j], acc[i][j]);
+                for (int j = 0; j < 4; ++j) off[i][j] = fma(a[i], bb[j], off[i][j]);
         }
+    }
+    __syncthreads();  // C and T are read no more: F overlays them
+    {
+        const int oi = p.lower ? 64 : 0, oj = p.lower ? 0 : 64;  // the off-diagonal quadrant
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) Cm[tr + i][tc + j] = (float)(-acc[i][j]);
+            for (int j = 0; j < 4; ++j) {
+                F[oi + tr + i][oj + tc + j] = (float)(-off[i][j]);
+                F[oj + tr + i][oi + tc + j] = 0.f;  // the zero quadrant
+            }
+        for (int idx = t; idx < 64 * 64; idx += 256) {
+            const int rr = idx / 64, cc = idx % 64;
+            F[rr][cc] = (float)P[rr][cc];
+            F[64 + rr][64 + cc] = (float)Q[rr][cc];
+        }
     }
     __syncthreads();
-    // element (r, c) of the 128 x 128 inverse
-    auto val = [&](int r, int c) -> float {
-        const int hr = r >> 6, hc = c >> 6, lr = r & 63, lc = c & 63;
-        if (hr == hc) return hr ? Q[lr][lc] : P[lr][lc];
-        if (p.lower) return hr ? Cm[lr][lc] : 0.f;
-        return hr ? 0.f : Cm[lr][lc];
-    };
-    constexpr int CPR = TR / EPC;  // chunks per 128-element row
+    // planes: pass 0 inv (a thread per 16-byte chunk, along the rows); pass 1
+    // inv^T (consecutive threads take consecutive rows, reading F down a
+    // column without bank conflicts)
     for (int pass = 0; pass < 2; ++pass) {
         const Opnd& o = pass ? p.wt : p.w;
         for (int idx = t; idx < TR * CPR; idx += 256) {
-            const int r = idx / CPR, ch = idx % CPR;
-            const int c0 = ch * EPC, kt = c0 / KT;
-            char* tile = o.base + tile_index(o, inst, b, kt) * TILE_BYTES;
-            const int off = swz(r, c0 % KT, ESIZE);
+            const int r = pass ? idx % TR : idx / CPR, ch = pass ? idx / TR : idx % CPR;
+            const int c0 = ch * EPC;
+            char* tile = o.base + tile_index(o, inst, b, c0 / KT) * TILE_BYTES;
+            const int off16 = swz(r, c0 % KT, ESIZE);
             float x[EPC];
 #pragma unroll
-            for (int e = 0; e < EPC; ++e) x[e] = pass ? val(c0 + e, r) : val(r, c0 + e);
+            for (int e = 0; e < EPC; ++e) x[e] = pass ? F[c0 + e][r] : F[r][c0 + e];
             if (TF32) {
-                *(float4*)(tile + off) = make_float4(to_tf32(x[0]), to_tf32(x[1]), to_tf32(x[2]), to_tf32(x[3]));
+                *(float4*)(tile + off16) = make_float4(to_tf32(x[0]), to_tf32(x[1]), to_tf32(x[2]), to_tf32(x[3]));
             } else {
                 uint32_t hv[EPC / 2], mv[EPC / 2], lv[EPC / 2];
 #pragma unroll
@@ -674,9 +709,9 @@ __global__ void __launch_bounds__(256) btc_inv_kernel(const __grid_constant__ In
                     mv[e] = (uint32_t)__bfloat16_as_ushort(m0) | ((uint32_t)__bfloat16_as_ushort(m1) << 16);
                     lv[e] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
                 }
-                *(uint4*)(tile + off) = make_uint4(hv[0], hv[1], hv[2], hv[3]);
-                if (p.nlev > 1) *(uint4*)(tile + o.lstride + off) = make_uint4(mv[0], mv[1], mv[2], mv[3]);
-                if (p.nlev > 2) *(uint4*)(tile + 2 * o.lstride + off) = make_uint4(lv[0], lv[1], lv[2], lv[3]);
+                *(uint4*)(tile + off16) = make_uint4(hv[0], hv[1], hv[2], hv[3]);
+                if (p.nlev > 1) *(uint4*)(tile + o.lstride + off16) = make_uint4(mv[0], mv[1], mv[2], mv[3]);
+                if (p.nlev > 2) *(uint4*)(tile + 2 * o.lstride + off16) = make_uint4(lv[0], lv[1], lv[2], lv[3]);
             }
         }
     }
