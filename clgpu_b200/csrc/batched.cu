@@ -73,6 +73,50 @@ constexpr int TB = 64;  // row block / tile height
 //      products spread over all threads.
 constexpr int kInvThreads = 256;
 
+// One doubling step for every pair of h x h diagonal blocks of the 64 x 64
+// block: with ar / ac the first row of the pair's second / first block
+// (lower; the other way round for upper),
+//   T = D[ar.., ac..] Y[ac.., ac..]   (C P^-1, resp. C Q^-1)
+//   Y[ar.., ac..] = -Y[ar.., ar..] T   (-Q^-1 T, resp. -P^-1 T)
+// each output an FP64 sum in increasing k; RT x CT outputs per thread.
+template <int H, int RT, int CT>
+__device__ __forceinline__ void inv_double(double (*Y)[TB + 1], double (*Tm)[TB / 2 + 1], double (*D)[TB + 1],
+                                           int lower_op, int t)
+{
+    constexpr int CTILES = H / CT, TILES = H / RT * CTILES;  // per pair
+    static_assert((TB / (2 * H)) * TILES == kInvThreads, "one tile per thread");
+    const int pr = t / TILES, e = t % TILES, r0 = (e / CTILES) * RT, c0 = (e % CTILES) * CT;
+    const int o = pr * 2 * H;
+    const int ar = lower_op ? o + H : o, ac = lower_op ? o : o + H;
+    double acc[RT][CT] = {};
+    for (int k = 0; k < H; ++k) {
+#pragma unroll
+        for (int i = 0; i < RT; ++i)
+#pragma unroll
+            for (int j = 0; j < CT; ++j) acc[i][j] = fma(D[ar + r0 + i][ac + k], Y[ac + k][ac + c0 + j], acc[i][j]);
+    }
+#pragma unroll
+    for (int i = 0; i < RT; ++i)
+#pragma unroll
+        for (int j = 0; j < CT; ++j) Tm[pr * H + r0 + i][c0 + j] = acc[i][j];
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < RT; ++i)
+#pragma unroll
+        for (int j = 0; j < CT; ++j) acc[i][j] = 0.0;
+    for (int k = 0; k < H; ++k) {
+#pragma unroll
+        for (int i = 0; i < RT; ++i)
+#pragma unroll
+            for (int j = 0; j < CT; ++j) acc[i][j] = fma(Y[ar + r0 + i][ar + k], Tm[pr * H + k][c0 + j], acc[i][j]);
+    }
+#pragma unroll
+    for (int i = 0; i < RT; ++i)
+#pragma unroll
+        for (int j = 0; j < CT; ++j) Y[ar + r0 + i][ac + c0 + j] = -acc[i][j];
+    __syncthreads();
+}
+
 __global__ void __launch_bounds__(kInvThreads) batched_inv_kernel(const int2* __restrict__ inv_items,
                                                                   const int* __restrict__ dims,
                                                                   const long* __restrict__ inv_off, int lower_op,
@@ -94,12 +138,22 @@ __global__ void __launch_bounds__(kInvThreads) batched_inv_kernel(const int2* __
     const long lda = d[2];
     const float* A = Aptr[w.x];
     const int r0 = w.y * TB, nr = min(TB, m - r0);
-    for (int idx = t; idx < TB * TB; idx += kInvThreads) {
-        const int r = idx % TB, c = idx / TB;  // A-local (r, c): coalesced down A's columns
-        double v = (r == c && (r >= nr || unit)) ? 1.0 : 0.0;
-        if (r < nr && c < nr && !(r == c && unit)) v = A[(long)(r0 + c) * lda + r0 + r];
-        if (op == 0) D[r][c] = v;
-        else D[c][r] = v;
+    {
+        // all 16 loads of the thread in flight before the first store
+        constexpr int PER = TB * TB / kInvThreads;
+        float a[PER];
+#pragma unroll
+        for (int u = 0; u < PER; ++u) {
+            const int idx = t + u * kInvThreads, r = idx % TB, c = idx / TB;  // coalesced down A's columns
+            a[u] = (r < nr && c < nr && !(r == c && unit)) ? A[(long)(r0 + c) * lda + r0 + r] : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < PER; ++u) {
+            const int idx = t + u * kInvThreads, r = idx % TB, c = idx / TB;
+            const double v = (r == c && (r >= nr || unit)) ? 1.0 : (double)a[u];
+            if (op == 0) D[r][c] = v;
+            else D[c][r] = v;
+        }
     }
     for (int idx = t; idx < TB * TB; idx += kInvThreads) Y[idx % TB][idx / TB] = 0.0;
     __syncthreads();
@@ -121,37 +175,10 @@ __global__ void __launch_bounds__(kInvThreads) batched_inv_kernel(const int2* __
         }
     }
     __syncthreads();
-    // 2. doubling: blocks of size h combine into 2h
-    for (int h = 16; h < TB; h *= 2) {
-        const int npairs = TB / (2 * h), nout = npairs * h * h;
-        // T = C P^-1 (lower) or C Q^-1 (upper), C the off-diagonal block of D
-        for (int idx = t; idx < nout; idx += kInvThreads) {
-            const int pr = idx / (h * h), e = idx % (h * h), r = e % h, c = e / h;
-            const int o = pr * 2 * h;
-            double acc = 0.0;
-            if (lower_op) {
-                for (int k = 0; k < h; ++k) acc = fma(D[o + h + r][o + k], Y[o + k][o + c], acc);
-            } else {
-                for (int k = 0; k < h; ++k) acc = fma(D[o + r][o + h + k], Y[o + h + k][o + h + c], acc);
-            }
-            Tm[pr * h + r][c] = acc;
-        }
-        __syncthreads();
-        // off-diagonal block of the inverse: -Q^-1 T (lower) or -P^-1 T (upper)
-        for (int idx = t; idx < nout; idx += kInvThreads) {
-            const int pr = idx / (h * h), e = idx % (h * h), r = e % h, c = e / h;
-            const int o = pr * 2 * h;
-            double acc = 0.0;
-            if (lower_op) {
-                for (int k = 0; k < h; ++k) acc = fma(Y[o + h + r][o + h + k], Tm[pr * h + k][c], acc);
-                Y[o + h + r][o + c] = -acc;
-            } else {
-                for (int k = 0; k < h; ++k) acc = fma(Y[o + r][o + k], Tm[pr * h + k][c], acc);
-                Y[o + r][o + h + c] = -acc;
-            }
-        }
-        __syncthreads();
-    }
+    // 2. doubling: blocks of size h combine into 2h (h = 16: two pairs, one
+    // row x two columns per thread; h = 32: one pair, 2 x 2 per thread)
+    inv_double<16, 1, 2>(Y, Tm, D, lower_op, t);
+    inv_double<32, 2, 2>(Y, Tm, D, lower_op, t);
     float* out = inv + inv_off[w.x] + (long)w.y * TB * TB;
     for (int idx = t; idx < TB * TB; idx += kInvThreads) out[idx] = (float)Y[idx % TB][idx / TB];
 }

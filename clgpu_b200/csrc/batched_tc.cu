@@ -574,10 +574,9 @@ __global__ void __launch_bounds__(256) btc_split_kernel(const __grid_constant__ 
 // missing second block) and the off-diagonal block C of M,
 //   lower: inv = [[P^-1, 0], [-Q^-1 (C P^-1), Q^-1]]
 //   upper: inv = [[P^-1, -P^-1 (C Q^-1)], [0, Q^-1]]
-// with both products in FP64 (operands held in FP64 in shared memory, so
-// that the inner loops convert nothing; 4 x 4 outputs per thread).  The
-// block is then staged in FP32 and written as tiled planes of inv (row r,
-// K c) and of inv^T.
+// with both products accumulated in FP64 (4 x 4 outputs per thread; T held
+// in FP64); the block is written as tiled planes of inv (row r, K c) and of
+// inv^T straight from its quadrants (a 16-byte chunk never crosses one).
 struct InvLaunch {
     const int2* items;       // (instance, 128-row block)
     const int* dims;         // per instance: na, nr, lda, ldb
@@ -588,8 +587,8 @@ struct InvLaunch {
     Opnd w, wt;
     int nlev;
 };
-constexpr int kInvLd = 65;                                        // FP64 64 x 64 row stride
-constexpr int kInvSmemBytes = 4 * 64 * kInvLd * (int)sizeof(double);  // P, Q, C, T
+constexpr int kInvLd = 65;
+constexpr int kInvSmemBytes = 3 * 64 * kInvLd * (int)sizeof(float) + 64 * kInvLd * (int)sizeof(double);
 
 template <bool TF32>
 __global__ void __launch_bounds__(256) btc_inv_kernel(const __grid_constant__ InvLaunch p)
@@ -598,13 +597,11 @@ __global__ void __launch_bounds__(256) btc_inv_kernel(const __grid_constant__ In
     constexpr int ESIZE = TF32 ? 4 : 2;
     constexpr int EPC = 16 / ESIZE;  // elements per 16-byte chunk
     constexpr int CPR = TR / EPC;    // chunks per 128-element row
-    constexpr int FLD = TR + 1;      // FP32 staging row stride
     extern __shared__ double inv_smem[];
-    double(*P)[kInvLd] = (double(*)[kInvLd])inv_smem;
-    double(*Q)[kInvLd] = P + 64;
-    double(*Cm)[kInvLd] = Q + 64;
-    double(*T)[kInvLd] = Cm + 64;
-    float(*F)[FLD] = (float(*)[FLD])(Cm);  // the finished block (over C and T)
+    double(*T)[kInvLd] = (double(*)[kInvLd])inv_smem;
+    float(*P)[kInvLd] = (float(*)[kInvLd])(inv_smem + 64 * kInvLd);
+    float(*Q)[kInvLd] = P + 64;
+    float(*Cm)[kInvLd] = Q + 64;  // C, then the off-diagonal block of the inverse
     const int t = threadIdx.x;
     const int2 it = p.items[blockIdx.x];
     const int inst = it.x, b = it.y;
@@ -616,22 +613,33 @@ __global__ void __launch_bounds__(256) btc_inv_kernel(const __grid_constant__ In
     const float* inv = p.inv64 + p.inv64_off[inst];
     const int r0 = b * TR;
     const bool has_q = 2 * b + 1 < nb64;
-    for (int idx = t; idx < 64 * 64; idx += 256) {
-        const int rr = idx % 64, cc = idx / 64;  // column-major: coalesced
-        P[rr][cc] = inv[(long)(2 * b) * 4096 + idx];
-        Q[rr][cc] = has_q ? inv[(long)(2 * b + 1) * 4096 + idx] : (rr == cc ? 1.0 : 0.0);
-        // off-diagonal block of M (local rows i, columns j of the 128 block)
-        const int i = p.lower ? 64 + rr : rr, j = p.lower ? cc : 64 + cc;
-        double v = 0.0;
-        if (r0 + i < na && r0 + j < na)
-            v = p.op ? A[(long)(r0 + j) + (long)(r0 + i) * lda] : A[(long)(r0 + i) + (long)(r0 + j) * lda];
-        Cm[rr][cc] = v;
+    {
+        // every load of the thread in flight before the first store
+        float vp[16], vq[16], vc[16];
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+            const int idx = t + u * 256, rr = idx % 64, cc = idx / 64;  // column-major: coalesced
+            vp[u] = inv[(long)(2 * b) * 4096 + idx];
+            vq[u] = has_q ? inv[(long)(2 * b + 1) * 4096 + idx] : (rr == cc ? 1.f : 0.f);
+            // off-diagonal block of M (local rows i, columns j of the 128 block)
+            const int i = p.lower ? 64 + rr : rr, j = p.lower ? cc : 64 + cc;
+            vc[u] = (r0 + i < na && r0 + j < na)
+                        ? (p.op ? A[(long)(r0 + j) + (long)(r0 + i) * lda] : A[(long)(r0 + i) + (long)(r0 + j) * lda])
+                        : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+            const int idx = t + u * 256, rr = idx % 64, cc = idx / 64;
+            P[rr][cc] = vp[u];
+            Q[rr][cc] = vq[u];
+            Cm[rr][cc] = vc[u];
+        }
     }
     __syncthreads();
     const int tr = (t >> 4) * 4, tc = (t & 15) * 4;
     {
         // T = C P^-1 (lower) or C Q^-1 (upper)
-        double(*R)[kInvLd] = p.lower ? P : Q;
+        float(*R)[kInvLd] = p.lower ? P : Q;
         double acc[4][4] = {};
         for (int k = 0; k < 64; ++k) {
             double a[4], bb[4];
@@ -650,10 +658,10 @@ __global__ void __launch_bounds__(256) btc_inv_kernel(const __grid_constant__ In
             for (int j = 0; j < 4; ++j) T[tr + i][tc + j] = acc[i][j];
     }
     __syncthreads();
-    // off-diagonal block of the inverse: -Q^-1 T (lower) or -P^-1 T (upper)
-    double off[4][4] = {};
     {
-        double(*L)[kInvLd] = p.lower ? Q : P;
+        // off-diagonal block of the inverse: -Q^-1 T (lower) or -P^-1 T (upper), into Cm
+        float(*L)[kInvLd] = p.lower ? Q : P;
+        double acc[4][4] = {};
         for (int k = 0; k < 64; ++k) {
             double a[4], bb[4];
 #pragma unroll
@@ -663,39 +671,34 @@ __global__ void __launch_bounds__(256) btc_inv_kernel(const __grid_constant__ In
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
-                for (int j = 0; j < 4; ++j) off[i][j] = fma(a[i], bb[j], off[i][j]);
+                for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], bb[j], acc[i][j]);
         }
-    }
-    __syncthreads();  // C and T are read no more: F overlays them
-    {
-        const int oi = p.lower ? 64 : 0, oj = p.lower ? 0 : 64;  // the off-diagonal quadrant
+        // Cm is read only by the first product, which every thread has finished
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                F[oi + tr + i][oj + tc + j] = (float)(-off[i][j]);
-                F[oj + tr + i][oi + tc + j] = 0.f;  // the zero quadrant
-            }
-        for (int idx = t; idx < 64 * 64; idx += 256) {
-            const int rr = idx / 64, cc = idx % 64;
-            F[rr][cc] = (float)P[rr][cc];
-            F[64 + rr][64 + cc] = (float)Q[rr][cc];
-        }
+            for (int j = 0; j < 4; ++j) Cm[tr + i][tc + j] = (float)(-acc[i][j]);
     }
     __syncthreads();
-    // planes: pass 0 inv (a thread per 16-byte chunk, along the rows); pass 1
-    // inv^T (consecutive threads take consecutive rows, reading F down a
-    // column without bank conflicts)
+    // planes: pass 0 inv (threads along a row's chunks), pass 1 inv^T
+    // (consecutive threads take consecutive rows: reading down a column of
+    // the quadrant without bank conflicts)
     for (int pass = 0; pass < 2; ++pass) {
         const Opnd& o = pass ? p.wt : p.w;
         for (int idx = t; idx < TR * CPR; idx += 256) {
             const int r = pass ? idx % TR : idx / CPR, ch = pass ? idx / TR : idx % CPR;
             const int c0 = ch * EPC;
-            char* tile = o.base + tile_index(o, inst, b, c0 / KT) * TILE_BYTES;
-            const int off16 = swz(r, c0 % KT, ESIZE);
+            // element (r, c0 + e) of inv (pass 0) or inv^T (pass 1)
+            const int gr = pass ? c0 : r, gc = pass ? r : c0;  // quadrant of inv holding it
+            const int hr = gr >> 6, hc = gc >> 6;
+            const float(*S)[kInvLd] = hr == hc ? (hr ? Q : P) : Cm;
+            const bool zero = hr != hc && (p.lower ? hr == 0 : hr == 1);
             float x[EPC];
 #pragma unroll
-            for (int e = 0; e < EPC; ++e) x[e] = pass ? F[c0 + e][r] : F[r][c0 + e];
+            for (int e = 0; e < EPC; ++e)
+                x[e] = zero ? 0.f : (pass ? S[(c0 + e) & 63][r & 63] : S[r & 63][(c0 + e) & 63]);
+            char* tile = o.base + tile_index(o, inst, b, c0 / KT) * TILE_BYTES;
+            const int off16 = swz(r, c0 % KT, ESIZE);
             if (TF32) {
                 *(float4*)(tile + off16) = make_float4(to_tf32(x[0]), to_tf32(x[1]), to_tf32(x[2]), to_tf32(x[3]));
             } else {
