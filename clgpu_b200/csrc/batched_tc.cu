@@ -407,15 +407,23 @@ __global__ void __launch_bounds__(THREADS, 1) btc_mma_kernel(const __grid_consta
             int acc = 0;
             uint32_t acc_ph = 0;
             bool ok = true;
+            // TMEM chunk: 6xBF16 one K tile (drained and summed in FP32 by
+            // the epilogue: the tensor core's accumulation loses a fraction
+            // of an ulp per step), the other modes the whole K range
+            const bool per_tile = p.nprod == 6;
             for (int it = blockIdx.x; it < p.nitems && ok; it += gridDim.x) {
                 const int4 w = p.items[it];
                 const int inst = w.x, ct = w.y & 0xffff, nk = w.w >> 16;
                 if (nk == 0) continue;
                 const uint32_t idesc = idesc_of(TF32 ? 2u : 1u, b_rows(p.cinfo[inst].y, ct));
-                if (!mbar_wait(&tempty[acc], acc_ph ^ 1, abort_flag)) break;
-                tc_fence_after();
-                const uint32_t d = tmem_base + (uint32_t)(acc * TR);
+                uint32_t d = 0;
+                bool open = false;  // MMAs issued into the current chunk, not yet committed
                 for (int kt = 0; kt < nk; ++kt) {
+                    if (kt == 0 || per_tile) {
+                        if (!mbar_wait(&tempty[acc], acc_ph ^ 1, abort_flag)) { ok = false; break; }
+                        tc_fence_after();
+                        d = tmem_base + (uint32_t)(acc * TR);
+                    }
                     if (!mbar_wait(&full[s], ph, abort_flag)) { ok = false; break; }
                     tc_fence_after();
                     const uint32_t st = smem_u32(ring + s * stage_bytes);
@@ -424,18 +432,23 @@ __global__ void __launch_bounds__(THREADS, 1) btc_mma_kernel(const __grid_consta
                         const uint64_t db = desc_sw128(st + (p.nlev + p.pb[pr]) * TILE_BYTES);
 #pragma unroll
                         for (int kk = 0; kk < 4; ++kk)  // 4 x 32 bytes of K per tile row
-                            umma<TF32>(d, da + 2 * kk, db + 2 * kk, idesc, (kt > 0 || pr > 0 || kk > 0) ? 1u : 0u);
+                            umma<TF32>(d, da + 2 * kk, db + 2 * kk, idesc,
+                                       ((kt > 0 && !per_tile) || pr > 0 || kk > 0) ? 1u : 0u);
                     }
+                    open = true;
                     umma_commit(&empty[s]);
                     if (++s == nstages) { s = 0; ph ^= 1; }
+                    if (per_tile || kt == nk - 1) {
+                        // chunk done: the epilogue may read this accumulator
+                        umma_commit(&tfull[acc]);
+                        open = false;
+                        if (++acc == 2) { acc = 0; acc_ph ^= 1; }
+                    }
                 }
-                // item done (or aborted): the epilogue may read this accumulator
-                umma_commit(&tfull[acc]);
-                if (!ok) {
+                if (!ok && open) {
+                    umma_commit(&tfull[acc]);
                     mbar_drain(&tfull[acc], acc_ph);  // every issued MMA done before TMEM is freed
-                    break;
                 }
-                if (++acc == 2) { acc = 0; acc_ph ^= 1; }
             }
         }
     } else {
@@ -448,29 +461,33 @@ __global__ void __launch_bounds__(THREADS, 1) btc_mma_kernel(const __grid_consta
         for (int it = blockIdx.x; it < p.nitems; it += gridDim.x) {
             const int4 w = p.items[it];
             const int inst = w.x, rt = w.y >> 16, ct = w.y & 0xffff, nk = w.w >> 16;
-            if (nk > 0) {
-                int okw = 1;
-                if (lane == 0) okw = mbar_wait(&tfull[acc], acc_ph, abort_flag) ? 1 : 0;
-                if (!__shfl_sync(0xffffffffu, okw, 0)) break;
-                tc_fence_after();
-            }
             const int4 ci = p.cinfo[inst];
             const int c0 = cg * 32;
             const bool active = c0 < b_rows(ci.y, ct);
             float v[32];
-            if (nk > 0 && active) {
-                tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * TR + c0), v);
-            } else {
 #pragma unroll
-                for (int j = 0; j < 32; ++j) v[j] = 0.f;
-            }
-            if (nk > 0) {
+            for (int j = 0; j < 32; ++j) v[j] = 0.f;
+            // the item's chunks (one per K tile in 6xBF16), summed in FP32 in K order
+            const int nchunks = nk == 0 ? 0 : (p.nprod == 6 ? nk : 1);
+            bool ok = true;
+            for (int c = 0; c < nchunks; ++c) {
+                int okw = 1;
+                if (lane == 0) okw = mbar_wait(&tfull[acc], acc_ph, abort_flag) ? 1 : 0;
+                if (!__shfl_sync(0xffffffffu, okw, 0)) { ok = false; break; }
+                tc_fence_after();
+                if (active) {
+                    float u[32];
+                    tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * TR + c0), u);
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) v[j] += u[j];
+                }
                 // the values are in registers: the accumulator is free
                 tc_fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&tempty[acc]);
                 if (++acc == 2) { acc = 0; acc_ph ^= 1; }
             }
+            if (!ok) break;
             if (active) epilogue_group<TF32, EK>(p, v, inst, rt * TR + r, ct, c0, ci);
         }
     }
