@@ -341,22 +341,27 @@ ICLBLAS_API iclblasStatus_t iclblasSgemm_backward(iclblasHandle_t handle, iclbla
                                                   float* dC, int lddc);
 
 /* Uneven batched TRSM and GEMM, no reference counterpart.  A plan is built
- * once for a list of instance sizes (host arrays of `batch` ints); each call
- * then runs every instance in one persistent launch (a memset of the plan's
- * work-queue head plus one kernel on the handle's stream), which can be
- * captured in a CUDA graph.  Plan creation is synchronous, allocates device
- * memory and times the launch-shape candidates on synthetic operands (the
+ * once for a list of instance sizes (host arrays of `batch` ints) and takes
+ * the handle's math mode at creation.  PLAIN_FP32 plans: each call runs
+ * every instance in one persistent launch per stage (a memset of the plan's
+ * work-queue head plus one kernel) with FP32 FMA on the CUDA cores; plan
+ * creation times the launch-shape candidates on synthetic operands (the
  * choice is cached per shapes and GPU, and in the file named by the
- * environment variable ICLBLAS_TUNE_CACHE when set); do not create a plan
- * during stream capture.  The calls take device arrays of `batch` device
- * pointers, one per instance; a plan serves one stream at a time.  All
- * arithmetic is FP32 FMA on the CUDA cores, whatever the math mode.
+ * environment variable ICLBLAS_TUNE_CACHE when set).  TF32 / 3xBF16 / 6xBF16
+ * plans: the products run on the tensor cores over operands split into
+ * planes once per call, TRSM by 128-row block steps (two launches per step
+ * of the largest instance); the plan holds the planes (about 2.8 GB for
+ * 512 instances of order up to 1024 in 6xBF16).  Either way the calls only
+ * launch kernels on the handle's stream and can be captured in a CUDA graph;
+ * plan creation is synchronous and allocates device memory: do not create a
+ * plan during stream capture.  The calls take device arrays of `batch`
+ * device pointers, one per instance; a plan serves one stream at a time.
  * TRSM: instance i solves op(A_i) X_i = alpha B_i (left side, A_i m_i x m_i,
  * lda_i >= max(1, m_i)) or X_i op(A_i) = alpha B_i (right side, A_i n_i x n_i,
  * lda_i >= max(1, n_i)); B_i is m_i x n_i with ldb_i >= max(1, m_i).
  * GEMM: C_i = alpha op(A_i) op(B_i) + beta C_i, leading dimensions at least
- * the stored row counts; each element is bit-identical to iclblasSgemm in
- * PLAIN_FP32 mode. */
+ * the stored row counts; in a PLAIN_FP32 plan each element is bit-identical
+ * to iclblasSgemm in PLAIN_FP32 mode. */
 typedef struct iclblasBatchPlan* iclblasBatchPlan_t;
 ICLBLAS_API iclblasStatus_t iclblasStrsmBatchedPlanCreate(iclblasHandle_t handle, iclblasSideMode_t side,
                                                           iclblasFillMode_t uplo, iclblasOperation_t trans,
