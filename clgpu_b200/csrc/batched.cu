@@ -49,7 +49,7 @@ cudaError_t batch_tc_create_gemm(iclblasHandle_t h, iclblasBatchPlan* plan, cons
                                  int tb);
 cudaError_t batch_tc_inverses(iclblasHandle_t h, const iclblasBatchPlan* plan, const float* const* A);
 cudaError_t batch_tc_solve(iclblasHandle_t h, const iclblasBatchPlan* plan, int adjoint, float alpha,
-                           const float* const* A, float* const* B);
+                           const float* const* A, float* const* B, int operator_ready);
 cudaError_t batch_tc_dA(iclblasHandle_t h, const iclblasBatchPlan* plan, float scale, const float* const* P,
                         const float* const* Q, float* const* dA);
 cudaError_t batch_tc_gemm(iclblasHandle_t h, const iclblasBatchPlan* plan, float alpha, const float* const* A,
@@ -1095,7 +1095,7 @@ cudaError_t batch_trsm(iclblasHandle_t h, const iclblasBatchPlan* p, float alpha
     if (p->tc) {
         if ((e = batch_tc_inverses(h, p, A)) != cudaSuccess) return e;
         p->inv_formed = true;
-        return batch_tc_solve(h, p, 0, alpha, A, B);
+        return batch_tc_solve(h, p, 0, alpha, A, B, 0);
     }
     p->inv_formed = true;
     return launch_trsm(h, p->main, p->counter, p->inv_off, p->inv, lower_op, op, 0, right, alpha, A, B);
@@ -1125,12 +1125,13 @@ cudaError_t batch_trsm_backward(iclblasHandle_t h, const iclblasBatchPlan* p, fl
     const int f_lower = lower_op_of(p->uplo, p->trans) ^ (right ? 1 : 0);
     const int f_op = op ^ (right ? 1 : 0);
     cudaError_t e = cudaSuccess;
-    if (!(p->reuse_inv && p->inv_formed)) {
+    const bool reuse = p->reuse_inv && p->inv_formed;
+    if (!reuse) {
         e = launch_inv(h, p->inv_items, p->n_inv, p->main.dims, p->inv_off, f_lower, f_op, unit, A, p->inv);
         if (e == cudaSuccess && p->tc) e = batch_tc_inverses(h, p, A);
     }
     if (e == cudaSuccess)
-        e = p->tc ? batch_tc_solve(h, p, 1, alpha, A, G)
+        e = p->tc ? batch_tc_solve(h, p, 1, alpha, A, G, reuse ? 1 : 0)
                   : launch_trsm(h, p->main, p->counter, p->inv_off, p->inv, !f_lower, !f_op, 1, right, alpha, A, G);
     if (e != cudaSuccess || !dA) return e;
     const float s = alpha != 0.f ? -1.f / alpha : 0.f;

@@ -101,6 +101,8 @@ struct MmaLaunch {
     float c_alpha, c_beta;
     Opnd w;             // planes of the result: row = C column, K = C row
     int mask;           // kEpiMask: 1 keep row >= col, 2 keep row <= col; +4 strict
+    int a_mn;           // A read MN-major from the tiles of its transpose (BF16 only)
+    int kpb;            // K tiles per 128-row block
     int* status;
 };
 
@@ -207,11 +209,27 @@ __device__ __forceinline__ uint64_t desc_sw128(uint32_t saddr)
     return d;
 }
 
-// Instruction descriptor: FP32 accumulator, A/B format (1 BF16, 2 TF32),
-// both K-major, N = n, M = 128.
-__device__ __forceinline__ uint32_t idesc_of(uint32_t fmt, int n)
+// Shared-memory matrix descriptor, MN-major, 128-byte swizzle: rows of 128 B
+// hold 64 consecutive M indices of one K index; 8-K groups 1024 B apart
+// (SBO); the next 64 M indices 8 KiB further (LBO).  One MMA (K = 16) spans
+// two 8-K groups: the start address advances by 2048 B per MMA.
+__device__ __forceinline__ uint64_t desc_mn_sw128(uint32_t saddr)
 {
-    return (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(TR >> 4) << 24);
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)(8192u >> 4) << 16;
+    d |= (uint64_t)(1024u >> 4) << 32;
+    d |= (uint64_t)1u << 46;
+    d |= (uint64_t)2u << 61;
+    return d;
+}
+
+// Instruction descriptor: FP32 accumulator, A/B format (1 BF16, 2 TF32),
+// A K-major or MN-major (bit 15), B K-major, N = n, M = 128.
+__device__ __forceinline__ uint32_t idesc_of(uint32_t fmt, int n, int a_mn)
+{
+    return (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)a_mn << 15) | ((uint32_t)(n >> 3) << 17) |
+           ((uint32_t)(TR >> 4) << 24);
 }
 
 __device__ __forceinline__ float to_tf32(float x)
@@ -380,14 +398,25 @@ __global__ void __launch_bounds__(THREADS, 1) btc_mma_kernel(const __grid_consta
                 const int inst = w.x, rt = w.y >> 16, ct = w.y & 0xffff, nk = w.w >> 16;
                 if (nk == 0) continue;
                 const uint32_t bbytes = (uint32_t)b_rows(p.cinfo[inst].y, ct) * ROWB;
-                const long ta = tile_index(p.a, inst, rt, w.z >> 16), tb = tile_index(p.b, inst, ct, w.z & 0xffff);
+                const int akt = w.z >> 16;
+                const long ta = p.a_mn ? 0 : tile_index(p.a, inst, rt, akt), tb = tile_index(p.b, inst, ct, w.z & 0xffff);
                 for (int kt = 0; kt < nk; ++kt) {
                     if (!mbar_wait(&empty[s], ph ^ 1, abort_flag)) { ok = false; break; }
                     uint8_t* st = ring + s * stage_bytes;
                     mbar_expect_tx(&full[s], (uint32_t)p.nlev * (TILE_BYTES + bbytes));
+                    // MN-major A: K tile k of the transpose = rows (k % kpb) * 64.. of
+                    // its row block k / kpb, the two 64-column tiles of block rt
+                    const int kg = akt + kt, sb = kg / p.kpb, half = (kg % p.kpb) * (TILE_BYTES / 2);
+                    const long tm = p.a_mn ? tile_index(p.a, inst, sb, 2 * rt) : 0;
                     for (int l = 0; l < p.nlev; ++l) {
-                        bulk_load(st + l * TILE_BYTES, p.a.base + l * p.a.lstride + (ta + kt) * TILE_BYTES, TILE_BYTES,
-                                  &full[s]);
+                        const char* const a = p.a.base + l * p.a.lstride;
+                        if (p.a_mn) {
+                            bulk_load(st + l * TILE_BYTES, a + tm * TILE_BYTES + half, TILE_BYTES / 2, &full[s]);
+                            bulk_load(st + l * TILE_BYTES + TILE_BYTES / 2, a + (tm + 1) * TILE_BYTES + half,
+                                      TILE_BYTES / 2, &full[s]);
+                        } else {
+                            bulk_load(st + l * TILE_BYTES, a + (ta + kt) * TILE_BYTES, TILE_BYTES, &full[s]);
+                        }
                         bulk_load(st + (p.nlev + l) * TILE_BYTES, p.b.base + l * p.b.lstride + (tb + kt) * TILE_BYTES,
                                   bbytes, &full[s]);
                     }
@@ -415,7 +444,8 @@ __global__ void __launch_bounds__(THREADS, 1) btc_mma_kernel(const __grid_consta
                 const int4 w = p.items[it];
                 const int inst = w.x, ct = w.y & 0xffff, nk = w.w >> 16;
                 if (nk == 0) continue;
-                const uint32_t idesc = idesc_of(TF32 ? 2u : 1u, b_rows(p.cinfo[inst].y, ct));
+                const uint32_t idesc = idesc_of(TF32 ? 2u : 1u, b_rows(p.cinfo[inst].y, ct), p.a_mn);
+                const uint64_t a_step = p.a_mn ? 128 : 2;  // per MMA, 16-byte units
                 uint32_t d = 0;
                 bool open = false;  // MMAs issued into the current chunk, not yet committed
                 for (int kt = 0; kt < nk; ++kt) {
@@ -428,11 +458,12 @@ __global__ void __launch_bounds__(THREADS, 1) btc_mma_kernel(const __grid_consta
                     tc_fence_after();
                     const uint32_t st = smem_u32(ring + s * stage_bytes);
                     for (int pr = 0; pr < p.nprod; ++pr) {
-                        const uint64_t da = desc_sw128(st + p.pa[pr] * TILE_BYTES);
+                        const uint32_t sa = st + p.pa[pr] * TILE_BYTES;
+                        const uint64_t da = p.a_mn ? desc_mn_sw128(sa) : desc_sw128(sa);
                         const uint64_t db = desc_sw128(st + (p.nlev + p.pb[pr]) * TILE_BYTES);
 #pragma unroll
                         for (int kk = 0; kk < 4; ++kk)  // 4 x 32 bytes of K per tile row
-                            umma<TF32>(d, da + 2 * kk, db + 2 * kk, idesc,
+                            umma<TF32>(d, da + a_step * kk, db + 2 * kk, idesc,
                                        ((kt > 0 && !per_tile) || pr > 0 || kk > 0) ? 1u : 0u);
                     }
                     open = true;
@@ -591,9 +622,12 @@ __global__ void __launch_bounds__(256) btc_split_kernel(const __grid_constant__ 
 // missing second block) and the off-diagonal block C of M,
 //   lower: inv = [[P^-1, 0], [-Q^-1 (C P^-1), Q^-1]]
 //   upper: inv = [[P^-1, -P^-1 (C Q^-1)], [0, Q^-1]]
-// with both products accumulated in FP64 (4 x 4 outputs per thread; T held
-// in FP64); the block is written as tiled planes of inv (row r, K c) and of
-// inv^T straight from its quadrants (a 16-byte chunk never crosses one).
+// with both products in FP64 (4 x 4 outputs per thread).  P^-1, Q^-1 and C
+// are held in FP64 in shared memory (converted once, on load: conversions
+// run at a quarter of the FP64 FMA rate), T = C P^-1 then overlays C and
+// the off-diagonal block overlays T, so that two CTAs fit on an SM.  The
+// block is written as tiled planes of inv (row r, K c) and of inv^T straight
+// from its quadrants (a 16-byte chunk never crosses one).
 struct InvLaunch {
     const int2* items;       // (instance, 128-row block)
     const int* dims;         // per instance: na, nr, lda, ldb
@@ -605,7 +639,7 @@ struct InvLaunch {
     int nlev;
 };
 constexpr int kInvLd = 65;
-constexpr int kInvSmemBytes = 3 * 64 * kInvLd * (int)sizeof(float) + 64 * kInvLd * (int)sizeof(double);
+constexpr int kInvSmemBytes = 3 * 64 * kInvLd * (int)sizeof(double);
 
 template <bool TF32>
 __global__ void __launch_bounds__(256) btc_inv_kernel(const __grid_constant__ InvLaunch p)
@@ -615,10 +649,9 @@ __global__ void __launch_bounds__(256) btc_inv_kernel(const __grid_constant__ In
     constexpr int EPC = 16 / ESIZE;  // elements per 16-byte chunk
     constexpr int CPR = TR / EPC;    // chunks per 128-element row
     extern __shared__ double inv_smem[];
-    double(*T)[kInvLd] = (double(*)[kInvLd])inv_smem;
-    float(*P)[kInvLd] = (float(*)[kInvLd])(inv_smem + 64 * kInvLd);
-    float(*Q)[kInvLd] = P + 64;
-    float(*Cm)[kInvLd] = Q + 64;  // C, then the off-diagonal block of the inverse
+    double(*P)[kInvLd] = (double(*)[kInvLd])inv_smem;
+    double(*Q)[kInvLd] = P + 64;
+    double(*Cm)[kInvLd] = Q + 64;  // C, then T, then the off-diagonal block of the inverse
     const int t = threadIdx.x;
     const int2 it = p.items[blockIdx.x];
     const int inst = it.x, b = it.y;
@@ -655,8 +688,8 @@ __global__ void __launch_bounds__(256) btc_inv_kernel(const __grid_constant__ In
     __syncthreads();
     const int tr = (t >> 4) * 4, tc = (t & 15) * 4;
     {
-        // T = C P^-1 (lower) or C Q^-1 (upper)
-        float(*R)[kInvLd] = p.lower ? P : Q;
+        // T = C P^-1 (lower) or C Q^-1 (upper), into Cm once every thread has read C
+        double(*R)[kInvLd] = p.lower ? P : Q;
         double acc[4][4] = {};
         for (int k = 0; k < 64; ++k) {
             double a[4], bb[4];
@@ -669,15 +702,17 @@ __global__ void __launch_bounds__(256) btc_inv_kernel(const __grid_constant__ In
 #pragma unroll
                 for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], bb[j], acc[i][j]);
         }
+        __syncthreads();
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) T[tr + i][tc + j] = acc[i][j];
+            for (int j = 0; j < 4; ++j) Cm[tr + i][tc + j] = acc[i][j];
     }
     __syncthreads();
     {
         // off-diagonal block of the inverse: -Q^-1 T (lower) or -P^-1 T (upper), into Cm
-        float(*L)[kInvLd] = p.lower ? Q : P;
+        double(*L)[kInvLd] = p.lower ? Q : P;
+        double(*T)[kInvLd] = Cm;
         double acc[4][4] = {};
         for (int k = 0; k < 64; ++k) {
             double a[4], bb[4];
@@ -690,11 +725,11 @@ __global__ void __launch_bounds__(256) btc_inv_kernel(const __grid_constant__ In
 #pragma unroll
                 for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], bb[j], acc[i][j]);
         }
-        // Cm is read only by the first product, which every thread has finished
+        __syncthreads();  // every thread has read T
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) Cm[tr + i][tc + j] = (float)(-acc[i][j]);
+            for (int j = 0; j < 4; ++j) Cm[tr + i][tc + j] = -acc[i][j];
     }
     __syncthreads();
     // planes: pass 0 inv (threads along a row's chunks), pass 1 inv^T
@@ -708,12 +743,12 @@ __global__ void __launch_bounds__(256) btc_inv_kernel(const __grid_constant__ In
             // element (r, c0 + e) of inv (pass 0) or inv^T (pass 1)
             const int gr = pass ? c0 : r, gc = pass ? r : c0;  // quadrant of inv holding it
             const int hr = gr >> 6, hc = gc >> 6;
-            const float(*S)[kInvLd] = hr == hc ? (hr ? Q : P) : Cm;
+            const double(*S)[kInvLd] = hr == hc ? (hr ? Q : P) : Cm;
             const bool zero = hr != hc && (p.lower ? hr == 0 : hr == 1);
             float x[EPC];
 #pragma unroll
             for (int e = 0; e < EPC; ++e)
-                x[e] = zero ? 0.f : (pass ? S[(c0 + e) & 63][r & 63] : S[r & 63][(c0 + e) & 63]);
+                x[e] = zero ? 0.f : (float)(pass ? S[(c0 + e) & 63][r & 63] : S[r & 63][(c0 + e) & 63]);
             char* tile = o.base + tile_index(o, inst, b, c0 / KT) * TILE_BYTES;
             const int off16 = swz(r, c0 % KT, ESIZE);
             if (TF32) {
@@ -830,7 +865,12 @@ struct BatchTc {
     int2* inv_items = nullptr;
     int n_inv = 0;
     int right = 0, lower_f = 0, op_f = 0, tri_lower = 0, unit = 0;
-    TcRange split_f, split_b, split_d, gemm_d;
+    // split launches: forward (first block + operator tiles); adjoint with
+    // the operator tiles (the forward's, read MN-major, in the BF16 modes;
+    // the transpose's in TF32) or, when the forward call's are reused, the
+    // first block only
+    TcRange split_f, split_b, split_b_first, split_d, gemm_d;
+    int a_mn_b = 0;  // the adjoint's updates read the forward's operator tiles MN-major
     std::vector<TcRange> inv_f, upd_f, inv_b, upd_b;
     // GEMM plans
     char *ap = nullptr, *bp = nullptr;
@@ -871,6 +911,7 @@ struct MmaArgs {
     float c_alpha = 1.f, c_beta = 0.f;
     Opnd w{};
     int mask = 0;
+    int a_mn = 0;
 };
 
 template <bool TF32>
@@ -905,6 +946,8 @@ cudaError_t run_mma(iclblasHandle_t h, const BatchTc& t, TcRange r, const MmaArg
     p.c_beta = m.c_beta;
     p.w = m.w;
     p.mask = m.mask;
+    p.a_mn = m.a_mn;
+    p.kpb = t.kpb;
     p.status = h->ws.dev_status;
     const int grid = std::min(r.count, h->sm_count);
     if (t.tf32) launch_mma<true>(p, m.kind, grid, h->stream);
@@ -950,27 +993,32 @@ void solve_items(const std::vector<int>& dims, int batch, int lower, int kpb, st
     }
 }
 
-// Split items of a solve: the operator's tiles strictly off the diagonal
-// blocks on its triangle (kind 0) and the first block of the right-hand
-// sides (kind 1).
-TcRange split_items(const std::vector<int>& dims, int batch, int lower, int kpb, std::vector<int4>& all)
+// Split items: the operator's tiles strictly off the diagonal blocks on
+// the side `lower` names (kind 0), and the first block, in the solve order
+// of `lower`, of the right-hand sides (kind 1).
+void operator_items(const std::vector<int>& dims, int batch, int lower, int kpb, std::vector<int4>& all)
 {
-    TcRange r;
-    r.off = (int)all.size();
     for (int i = 0; i < batch; ++i) {
         const int na = dims[4 * i], nr = dims[4 * i + 1];
         if (na == 0 || nr == 0) continue;
-        const int nblk = (na + TR - 1) / TR, nct = (nr + TR - 1) / TR;
+        const int nblk = (na + TR - 1) / TR;
         for (int tt = 0; tt < nblk; ++tt) {
             const int k0 = lower ? 0 : (tt + 1) * kpb, k1 = lower ? tt * kpb : nblk * kpb;
             for (int kt = k0; kt < k1; ++kt) all.push_back(make_int4(0, i, tt, kt));
         }
+    }
+}
+
+void first_block_items(const std::vector<int>& dims, int batch, int lower, int kpb, std::vector<int4>& all)
+{
+    for (int i = 0; i < batch; ++i) {
+        const int na = dims[4 * i], nr = dims[4 * i + 1];
+        if (na == 0 || nr == 0) continue;
+        const int nblk = (na + TR - 1) / TR, nct = (nr + TR - 1) / TR;
         const int s0 = lower ? 0 : nblk - 1;
         for (int c = 0; c < nct; ++c)
             for (int kt = s0 * kpb; kt < (s0 + 1) * kpb; ++kt) all.push_back(make_int4(1, i, c, kt));
     }
-    r.count = (int)all.size() - r.off;
-    return r;
 }
 
 template <class T>
@@ -1045,10 +1093,22 @@ cudaError_t batch_tc_create_trsm(iclblasHandle_t h, iclblasBatchPlan* plan, cons
     }
     t->n_inv = (int)inv_items.size();
     std::vector<int4> all;
-    // forward: operator M (lower_f); adjoint: M^T (!lower_f)
-    t->split_f = split_items(dims, batch, lower_f, t->kpb, all);
+    // forward: operator M (lower_f); adjoint: M^T (!lower_f).  Item order
+    // [first block fwd][M's tiles][M^T's tiles, TF32 only][first block adj]
+    // keeps every split launch one contiguous range.
+    t->a_mn_b = t->tf32 ? 0 : 1;
+    t->split_f.off = (int)all.size();
+    first_block_items(dims, batch, lower_f, t->kpb, all);
+    const int op_off = (int)all.size();
+    operator_items(dims, batch, lower_f, t->kpb, all);
+    t->split_f.count = (int)all.size() - t->split_f.off;
+    t->split_b.off = t->a_mn_b ? op_off : (int)all.size();
+    if (!t->a_mn_b) operator_items(dims, batch, !lower_f, t->kpb, all);
+    t->split_b_first.off = (int)all.size();
+    first_block_items(dims, batch, !lower_f, t->kpb, all);
+    t->split_b_first.count = (int)all.size() - t->split_b_first.off;
+    t->split_b.count = (int)all.size() - t->split_b.off;
     solve_items(dims, batch, lower_f, t->kpb, all, t->inv_f, t->upd_f);
-    t->split_b = split_items(dims, batch, !lower_f, t->kpb, all);
     solve_items(dims, batch, !lower_f, t->kpb, all, t->inv_b, t->upd_b);
     // dA: operands P (kind 0, rows na, K nr) and Q (kind 1), then the masked product
     t->split_d.off = (int)all.size();
@@ -1121,20 +1181,24 @@ cudaError_t batch_tc_inverses(iclblasHandle_t h, const iclblasBatchPlan* plan, c
 }
 
 // One blocked solve, in place on B: the forward operator (adjoint = 0) or
-// its transpose, with the inverse planes already formed.
+// its transpose, with the inverse planes already formed; operator_ready:
+// the operator tiles of the plan's last forward call are still valid
+// (same A), so the adjoint (BF16 modes) splits only its first block.
 cudaError_t batch_tc_solve(iclblasHandle_t h, const iclblasBatchPlan* plan, int adjoint, float alpha,
-                           const float* const* A, float* const* B)
+                           const float* const* A, float* const* B, int operator_ready)
 {
     const BatchTc& t = *plan->tc;
-    // operator tiles: L[r][k] = S[r][k], S = M = op(A) (forward) or M^T;
-    // M[i][j] = A[i + j*lda] (op N) or A[j + i*lda]
-    const int s_rmajor = adjoint ? !t.op_f : t.op_f;
+    // operator tiles: L[r][k] = S[r][k], S = M = op(A) (forward, and the
+    // adjoint in the BF16 modes, which reads them MN-major) or M^T (TF32
+    // adjoint); M[i][j] = A[i + j*lda] (op N) or A[j + i*lda]
+    const int s_rmajor = (adjoint && !t.a_mn_b) ? !t.op_f : t.op_f;
     const SplitKind ks{A, t.info_a, s_rmajor, opnd(t.sp, t.sp_l, t.off_s, t.nkt_s)};
     // right-hand sides: row j = right-hand side j, K = solve row (left: B's
     // columns, L[j][k] = B[k + j*ldb]; right: B's rows, L[j][k] = B[j + k*ldb])
     const Opnd xp = opnd(t.xp, t.xp_l, t.off_x, t.nkt_x);
     const SplitKind ky{const_cast<const float* const*>(B), t.info_y, t.right ? 0 : 1, xp};
-    cudaError_t e = run_split(h, t, adjoint ? t.split_b : t.split_f, ks, ky);
+    const TcRange sr = !adjoint ? t.split_f : ((operator_ready && t.a_mn_b) ? t.split_b_first : t.split_b);
+    cudaError_t e = run_split(h, t, sr, ks, ky);
     if (e != cudaSuccess) return e;
     const std::vector<TcRange>& invs = adjoint ? t.inv_b : t.inv_f;
     const std::vector<TcRange>& upds = adjoint ? t.upd_b : t.upd_f;
@@ -1150,6 +1214,7 @@ cudaError_t batch_tc_solve(iclblasHandle_t h, const iclblasBatchPlan* plan, int 
     MmaArgs mu = mi;
     mu.kind = kEpiUpd;  // planes of Y_s = B_s - acc; B_s is only read
     mu.a = opnd(t.sp, t.sp_l, t.off_s, t.nkt_s);
+    mu.a_mn = adjoint ? t.a_mn_b : 0;
     for (size_t q = 0; q < invs.size(); ++q) {
         if ((e = run_mma(h, t, upds[q], mu)) != cudaSuccess) return e;
         if ((e = run_mma(h, t, invs[q], mi)) != cudaSuccess) return e;

@@ -233,3 +233,39 @@ def test_batched_tc_trsm_under_cuda_graph(handle, cuda):
             assert torch.equal(w, e)
     del g
     plan.destroy()
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("uplo", [1, 0])
+def test_batched_tc_adjoint_reuses_forward(handle, cuda, mode, uplo):
+    """With inverse reuse the tensor-core adjoint takes the forward call's
+    inverse planes and (BF16 modes) its operator tiles, read MN-major:
+    results bit-identical to a plan that forms and splits them again."""
+    handle.set_stream(torch.cuda.current_stream())
+    rng = np.random.default_rng(400 + uplo)
+    batch = 9
+    ms, ns = rng.integers(1, 450, batch), rng.integers(1, 200, batch)
+    ms[0], ns[0] = 384, 128
+    As = [tri_np(int(m), uplo == 1, rng) for m in ms]
+    Bs = [rng.standard_normal(int(m) * int(n)).astype(np.float32) for m, n in zip(ms, ns)]
+    Gs = [rng.standard_normal(int(m) * int(n)).astype(np.float32) for m, n in zip(ms, ns)]
+    handle.set_math_mode(mode)
+    outs = []
+    for reuse in (False, True):
+        plan = B.BatchPlan(handle, "trsm", side=0, uplo=uplo, trans=0, diag=0, m=list(ms), n=list(ns),
+                           lda=list(ms), ldb=list(ms))
+        assert plan.set_inverse_reuse(reuse) == B.SUCCESS
+        dA = [torch.from_numpy(a).to(cuda) for a in As]
+        dX = [torch.from_numpy(b).to(cuda) for b in Bs]
+        dG = [torch.from_numpy(g).to(cuda) for g in Gs]
+        ddA = [torch.empty(int(m) * int(m), device=cuda) for m in ms]
+        pa, px, pg, pda = ptrs(dA, cuda), ptrs(dX, cuda), ptrs(dG, cuda), ptrs(ddA, cuda)
+        assert B.iclblasStrsmBatchedUneven(handle, plan, 0.5, pa, px) == B.SUCCESS
+        assert B.iclblasStrsmBatchedUnevenBackward(handle, plan, 0.5, pa, px, pg, pda) == B.SUCCESS
+        torch.cuda.synchronize()
+        outs.append(([g.clone() for g in dG], [d.clone() for d in ddA]))
+        plan.destroy()
+    for g0, g1 in zip(outs[0][0], outs[1][0]):
+        assert torch.equal(g0, g1)
+    for d0, d1 in zip(outs[0][1], outs[1][1]):
+        assert torch.equal(d0, d1)
