@@ -622,12 +622,12 @@ __global__ void __launch_bounds__(256) btc_split_kernel(const __grid_constant__ 
 // missing second block) and the off-diagonal block C of M,
 //   lower: inv = [[P^-1, 0], [-Q^-1 (C P^-1), Q^-1]]
 //   upper: inv = [[P^-1, -P^-1 (C Q^-1)], [0, Q^-1]]
-// with both products in FP64 (4 x 4 outputs per thread).  P^-1, Q^-1 and C
-// are held in FP64 in shared memory (converted once, on load: conversions
-// run at a quarter of the FP64 FMA rate), T = C P^-1 then overlays C and
-// the off-diagonal block overlays T, so that two CTAs fit on an SM.  The
-// block is written as tiled planes of inv (row r, K c) and of inv^T straight
-// from its quadrants (a 16-byte chunk never crosses one).
+// with both products accumulated in FP64 for 6xBF16, whose three planes
+// keep every bit of the FP32 inverse, and in FP32 for 3xBF16 and TF32, whose
+// planes keep about 16 and 11 bits of it (4 x 4 outputs per thread; T held
+// in the accumulation type); the block is written as tiled planes of inv
+// (row r, K c) and of inv^T straight from its quadrants (a 16-byte chunk
+// never crosses one).
 struct InvLaunch {
     const int2* items;       // (instance, 128-row block)
     const int* dims;         // per instance: na, nr, lda, ldb
@@ -639,9 +639,13 @@ struct InvLaunch {
     int nlev;
 };
 constexpr int kInvLd = 65;
-constexpr int kInvSmemBytes = 3 * 64 * kInvLd * (int)sizeof(double);
+template <class Acc>
+constexpr int inv_smem_bytes()
+{
+    return 3 * 64 * kInvLd * (int)sizeof(float) + 64 * kInvLd * (int)sizeof(Acc);
+}
 
-template <bool TF32>
+template <bool TF32, class Acc>
 __global__ void __launch_bounds__(256) btc_inv_kernel(const __grid_constant__ InvLaunch p)
 {
     constexpr int KT = TF32 ? 32 : 64;
@@ -649,9 +653,10 @@ __global__ void __launch_bounds__(256) btc_inv_kernel(const __grid_constant__ In
     constexpr int EPC = 16 / ESIZE;  // elements per 16-byte chunk
     constexpr int CPR = TR / EPC;    // chunks per 128-element row
     extern __shared__ double inv_smem[];
-    double(*P)[kInvLd] = (double(*)[kInvLd])inv_smem;
-    double(*Q)[kInvLd] = P + 64;
-    double(*Cm)[kInvLd] = Q + 64;  // C, then T, then the off-diagonal block of the inverse
+    Acc(*T)[kInvLd] = (Acc(*)[kInvLd])inv_smem;
+    float(*P)[kInvLd] = (float(*)[kInvLd])((Acc*)inv_smem + 64 * kInvLd);
+    float(*Q)[kInvLd] = P + 64;
+    float(*Cm)[kInvLd] = Q + 64;  // C, then the off-diagonal block of the inverse
     const int t = threadIdx.x;
     const int2 it = p.items[blockIdx.x];
     const int inst = it.x, b = it.y;
@@ -688,11 +693,11 @@ __global__ void __launch_bounds__(256) btc_inv_kernel(const __grid_constant__ In
     __syncthreads();
     const int tr = (t >> 4) * 4, tc = (t & 15) * 4;
     {
-        // T = C P^-1 (lower) or C Q^-1 (upper), into Cm once every thread has read C
-        double(*R)[kInvLd] = p.lower ? P : Q;
-        double acc[4][4] = {};
+        // T = C P^-1 (lower) or C Q^-1 (upper)
+        float(*R)[kInvLd] = p.lower ? P : Q;
+        Acc acc[4][4] = {};
         for (int k = 0; k < 64; ++k) {
-            double a[4], bb[4];
+            Acc a[4], bb[4];
 #pragma unroll
             for (int i = 0; i < 4; ++i) a[i] = Cm[tr + i][k];
 #pragma unroll
@@ -702,20 +707,18 @@ __global__ void __launch_bounds__(256) btc_inv_kernel(const __grid_constant__ In
 #pragma unroll
                 for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], bb[j], acc[i][j]);
         }
-        __syncthreads();
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) Cm[tr + i][tc + j] = acc[i][j];
+            for (int j = 0; j < 4; ++j) T[tr + i][tc + j] = acc[i][j];
     }
     __syncthreads();
     {
         // off-diagonal block of the inverse: -Q^-1 T (lower) or -P^-1 T (upper), into Cm
-        double(*L)[kInvLd] = p.lower ? Q : P;
-        double(*T)[kInvLd] = Cm;
-        double acc[4][4] = {};
+        float(*L)[kInvLd] = p.lower ? Q : P;
+        Acc acc[4][4] = {};
         for (int k = 0; k < 64; ++k) {
-            double a[4], bb[4];
+            Acc a[4], bb[4];
 #pragma unroll
             for (int i = 0; i < 4; ++i) a[i] = L[tr + i][k];
 #pragma unroll
@@ -725,11 +728,11 @@ __global__ void __launch_bounds__(256) btc_inv_kernel(const __grid_constant__ In
 #pragma unroll
                 for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], bb[j], acc[i][j]);
         }
-        __syncthreads();  // every thread has read T
+        // Cm is read only by the first product, which every thread has finished
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) Cm[tr + i][tc + j] = -acc[i][j];
+            for (int j = 0; j < 4; ++j) Cm[tr + i][tc + j] = (float)(-acc[i][j]);
     }
     __syncthreads();
     // planes: pass 0 inv (threads along a row's chunks), pass 1 inv^T
@@ -743,12 +746,12 @@ __global__ void __launch_bounds__(256) btc_inv_kernel(const __grid_constant__ In
             // element (r, c0 + e) of inv (pass 0) or inv^T (pass 1)
             const int gr = pass ? c0 : r, gc = pass ? r : c0;  // quadrant of inv holding it
             const int hr = gr >> 6, hc = gc >> 6;
-            const double(*S)[kInvLd] = hr == hc ? (hr ? Q : P) : Cm;
+            const float(*S)[kInvLd] = hr == hc ? (hr ? Q : P) : Cm;
             const bool zero = hr != hc && (p.lower ? hr == 0 : hr == 1);
             float x[EPC];
 #pragma unroll
             for (int e = 0; e < EPC; ++e)
-                x[e] = zero ? 0.f : (float)(pass ? S[(c0 + e) & 63][r & 63] : S[r & 63][(c0 + e) & 63]);
+                x[e] = zero ? 0.f : (pass ? S[(c0 + e) & 63][r & 63] : S[r & 63][(c0 + e) & 63]);
             char* tile = o.base + tile_index(o, inst, b, c0 / KT) * TILE_BYTES;
             const int off16 = swz(r, c0 % KT, ESIZE);
             if (TF32) {
@@ -832,11 +835,14 @@ cudaError_t set_attrs(int device)
     for (const void* k : kernels)
         if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES)) != cudaSuccess)
             return e;
-    if ((e = cudaFuncSetAttribute(btc_inv_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  kInvSmemBytes)) != cudaSuccess)
+    if ((e = cudaFuncSetAttribute(btc_inv_kernel<true, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  inv_smem_bytes<float>())) != cudaSuccess)
         return e;
-    if ((e = cudaFuncSetAttribute(btc_inv_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  kInvSmemBytes)) != cudaSuccess)
+    if ((e = cudaFuncSetAttribute(btc_inv_kernel<false, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  inv_smem_bytes<float>())) != cudaSuccess)
+        return e;
+    if ((e = cudaFuncSetAttribute(btc_inv_kernel<false, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  inv_smem_bytes<double>())) != cudaSuccess)
         return e;
     done.fetch_or(bit);
     return cudaSuccess;
@@ -1175,8 +1181,9 @@ cudaError_t batch_tc_inverses(iclblasHandle_t h, const iclblasBatchPlan* plan, c
     p.w = opnd(t.inv, t.inv_l, t.off_inv, nullptr, t.kpb);
     p.wt = opnd(t.invt, t.inv_l, t.off_inv, nullptr, t.kpb);
     p.nlev = t.nlev;
-    if (t.tf32) btc_inv_kernel<true><<<t.n_inv, 256, kInvSmemBytes, h->stream>>>(p);
-    else btc_inv_kernel<false><<<t.n_inv, 256, kInvSmemBytes, h->stream>>>(p);
+    if (t.tf32) btc_inv_kernel<true, float><<<t.n_inv, 256, inv_smem_bytes<float>(), h->stream>>>(p);
+    else if (t.nlev == 3) btc_inv_kernel<false, double><<<t.n_inv, 256, inv_smem_bytes<double>(), h->stream>>>(p);
+    else btc_inv_kernel<false, float><<<t.n_inv, 256, inv_smem_bytes<float>(), h->stream>>>(p);
     return cudaGetLastError();
 }
 
