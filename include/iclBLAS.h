@@ -374,13 +374,15 @@ ICLBLAS_API iclblasStatus_t iclblasSgemmBatchedPlanCreate(iclblasHandle_t handle
                                                           const int* ldc, iclblasBatchPlan_t* plan);
 ICLBLAS_API iclblasStatus_t iclblasBatchPlanDestroy(iclblasBatchPlan_t plan);
 /* Algorithmic flops of one call (TRSM sum m^2 n, GEMM sum 2mnk) and the
- * tuned launch shape (tile width, CTAs per SM); any output may be NULL. */
+ * launch shape (tile width, CTAs per SM: the tuner's choice in a PLAIN_FP32
+ * plan, 128 and 1 in a tensor-core plan); any output may be NULL. */
 ICLBLAS_API iclblasStatus_t iclblasBatchPlanGetInfo(iclblasBatchPlan_t plan, double* flops, int* tile_width,
                                                     int* ctas_per_sm);
 /* TRSM plans: with reuse = 1, iclblasStrsmBatchedUnevenBackward uses the
  * diagonal-block inverses formed by the plan's most recent
  * iclblasStrsmBatchedUneven call instead of forming them again (it forms
- * them when no forward call has run yet).  The caller promises that the
+ * them when no forward call has run yet); a tensor-core plan in the BF16
+ * modes also reuses that call's split operator tiles.  The caller promises that the
  * triangles A_i are unchanged since that forward call and that the two
  * calls run in order on one stream.  0 (the default) forms them in every
  * call.  INVALID_VALUE for a GEMM plan or another value. */
