@@ -23,7 +23,11 @@ its own clock record: SGEMM 8192^3 and STRSM 8192x4096 in plain FP32 and the
 tensor-core split modes (3xBF16, 6xBF16, TF32; STRSM also 3xBF16 + one
 refinement step) with their errors against FP64 (`sgemm_8192`,
 `strsm_8192x4096`), and config 1, plain SGEMM 512^3, beside the reference's
-cpu_gemm on one and on all host cores (`sgemm_512_config`).
+cpu_gemm on one and on all host cores (`sgemm_512_config`), and the batched
+config (`batched_512`: 512 uneven STRSM instances, forward + adjoint, in
+plain FP32 on the CUDA cores and in each tensor-core mode, beside the same
+work as per-instance plain calls, with errors against FP64 and its own
+clock record).
 
 `--impl reference` times the reference's CPU implementation with every host
 thread on the full sweep config.  Multi-GPU (torchrun): each rank runs an
@@ -1073,7 +1077,7 @@ def run_conv1x1_study(args, torch):
             torch.cuda.empty_cache()
 
 
-def run_batched_study(args, torch):
+def run_batched_study(args, torch, quiet=False):
     """Batched uneven TRSM + adjoint config: 512 instances, n ~ UniformInt[32,1024],
     nrhs ~ UniformInt[1,256], L built as in the STRSM config (diagonal U(1,2),
     strictly lower N(0,1)/sqrt(n)), B and upstream gradients N(0,1), seed 4.
@@ -1190,7 +1194,8 @@ def run_batched_study(args, torch):
                  else "tensor-core launches per block step in a CUDA graph",
                  "tile_width": width, "ctas_per_sm": ctas, "tflops": round(flops / (ms / 1e3) / 1e12, 3),
                  "ms": round(ms, 3), "err_X": ex, "err_dB": eg, "err_dA": ea}
-            print(json.dumps(r), flush=True)
+            if not quiet:
+                print(json.dumps(r), flush=True)
             out.append(r)
             del graph, rgraph
             plan.destroy()
@@ -1212,9 +1217,37 @@ def run_batched_study(args, torch):
         r = {"routine": "batched strsm fwd+adjoint", "batch": batch, "form": "per-instance calls, plain FP32",
              "tflops": round(flops / (ms_loop / 1e3) / 1e12, 3), "ms": round(ms_loop, 3), "err_X": ex, "err_dB": eg,
              "err_dA": ea}
-        print(json.dumps(r), flush=True)
+        if not quiet:
+            print(json.dumps(r), flush=True)
         out.append(r)
     return out
+
+
+def run_batched_leg(torch):
+    """The batched config in the default run: the study above (512
+    instances, forward + adjoint per step, one CUDA graph per math mode,
+    and the same work as per-instance plain calls) without its own output
+    lines, under one clock record; returns {form: {tflops, ms, errors,
+    x_plain_fp32}, "clocks": ...}."""
+    import types
+    ns = types.SimpleNamespace(batch=512, steps=5, warmup=3, math="all", batched_loop=True)
+    with Clocks(0) as clk:
+        t_wait = time.time()
+        while not clk.started() and time.time() - t_wait < 5.0:
+            time.sleep(0.05)
+        clk.mark_start()
+        rows = run_batched_study(ns, torch, quiet=True)
+        clk.mark_end()
+    res = {"config": "batched uneven STRSM forward + adjoint, 512 instances, n ~ UniformInt[32,1024], "
+                     "nrhs ~ UniformInt[1,256], seed 4; TFLOP/s = 3 sum n^2 nrhs / step time"}
+    plain = next((r["tflops"] for r in rows if r.get("math") == "plain_fp32"), None)
+    for r in rows:
+        key = r.get("math", "per_instance_plain_fp32")
+        res[key] = {k: r[k] for k in ("tflops", "ms", "err_X", "err_dB", "err_dA") if k in r}
+        if plain:
+            res[key]["x_plain_fp32"] = round(r["tflops"] / plain, 2)
+    res["clocks"] = clk.summary()
+    return res
 
 
 # ---------------------------------------------------------------- single-routine cases for profiles
@@ -1522,6 +1555,10 @@ def main():
     if world == 1 and not args.only and not args.no_precision:
         from clgpu_b200 import iclblas as B
         out.update(run_precision_legs(torch, torch.device("cuda", 0), B))
+        try:
+            out["batched_512"] = run_batched_leg(torch)
+        except Exception as e:  # reported in the line, never fatal to it
+            out["batched_512"] = {"error": repr(e)[:300]}
     if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.only:
         out["cpu_baseline"] = {k: v for k, v in cpu_sweep(1, reps=2).items() if k != "seconds_per_step"}
     if rank == 0:
