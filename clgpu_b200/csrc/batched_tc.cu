@@ -799,9 +799,9 @@ void mode_products(iclblasMathMode_t mode, int& tf32, int& nlev, int& nprod, int
     }
 }
 
-int4 mk_item(int inst, int rt, int ct, int akt, int bkt, int nk, int flags)
+int4 mk_item(int inst, int rt, int ct, int akt, int bkt, int nk)
 {
-    return make_int4(inst, (rt << 16) | ct, (akt << 16) | bkt, (nk << 16) | flags);
+    return make_int4(inst, (rt << 16) | ct, (akt << 16) | bkt, nk << 16);
 }
 
 template <class T>
@@ -984,7 +984,7 @@ void solve_items(const std::vector<int>& dims, int batch, int lower, int kpb, st
             if (na == 0 || nr == 0 || nblk <= q) continue;
             const int s = lower ? q : nblk - 1 - q;
             const int k0 = lower ? 0 : (s + 1) * kpb;
-            for (int c = 0; c < nct; ++c) all.push_back(mk_item(i, s, c, k0, k0, q * kpb, 1));
+            for (int c = 0; c < nct; ++c) all.push_back(mk_item(i, s, c, k0, k0, q * kpb));
         }
         upds[q].count = (int)all.size() - upds[q].off;
         invs[q].off = (int)all.size();
@@ -993,7 +993,7 @@ void solve_items(const std::vector<int>& dims, int batch, int lower, int kpb, st
             const int nblk = (na + TR - 1) / TR, nct = (nr + TR - 1) / TR;
             if (na == 0 || nr == 0 || nblk <= q) continue;
             const int s = lower ? q : nblk - 1 - q;
-            for (int c = 0; c < nct; ++c) all.push_back(mk_item(i, s, c, 0, s * kpb, kpb, 1));
+            for (int c = 0; c < nct; ++c) all.push_back(mk_item(i, s, c, 0, s * kpb, kpb));
         }
         invs[q].count = (int)all.size() - invs[q].off;
     }
@@ -1135,7 +1135,7 @@ cudaError_t batch_tc_create_trsm(iclblasHandle_t h, iclblasBatchPlan* plan, cons
                 for (int c = 0; c < nblk; ++c) {
                     const bool on = tri_lower ? rt >= c : rt <= c;
                     const int nk = on ? nkt_d[i] : 0;
-                    g.push_back({nk, mk_item(i, rt, c, 0, 0, nk, 0)});
+                    g.push_back({nk, mk_item(i, rt, c, 0, 0, nk)});
                 }
         }
         std::stable_sort(g.begin(), g.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
@@ -1292,7 +1292,7 @@ cudaError_t batch_tc_create_gemm(iclblasHandle_t h, iclblasBatchPlan* plan, cons
         for (int rt = 0; rt < nnt; ++rt)
             for (int kt = 0; kt < nk; ++kt) all.push_back(make_int4(1, i, rt, kt));
         for (int rt = 0; rt < nmt; ++rt)
-            for (int c = 0; c < nnt; ++c) g.push_back({(long)nk, mk_item(i, rt, c, 0, 0, nk, 0)});
+            for (int c = 0; c < nnt; ++c) g.push_back({(long)nk, mk_item(i, rt, c, 0, 0, nk)});
     }
     t->split_g.count = (int)all.size();
     std::stable_sort(g.begin(), g.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
