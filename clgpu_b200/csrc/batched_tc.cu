@@ -22,10 +22,13 @@
 // levels of one A and one B K tile per stage), one thread of warp 1 issues
 // tcgen05.mma (M = 128, N, K = 32 bytes per instruction; products
 // smallest first, as in the single-instance engine) into one of two TMEM
-// accumulators, and 8 epilogue warps drain the other: C (column- or
-// row-major, per-instance leading dimension), an optional triangle mask,
-// and optionally the result split straight into tiled planes again, so that
-// the next launch reads it as an operand.
+// accumulators, and 16 epilogue warps (a 32-column group of one TMEM lane
+// quarter each) drain the other: C (column- or row-major, per-instance
+// leading dimension), an optional triangle mask, and optionally the result
+// split straight into tiled planes again, so that the next launch reads it
+// as an operand.  6xBF16 drains the accumulator after every K tile and sums
+// the parts in FP32 (the tensor core's FP32 accumulation loses a fraction
+// of an ulp per step); the other modes accumulate the item's K range.
 //
 // TRSM, op(A) X = alpha B per instance, is solved by blocks of 128 rows in
 // the operator's order, level-synchronously over the batch:
@@ -36,11 +39,13 @@
 //            X_s = inv(M_ss) Y_s          (one launch; C = B block s gets
 //                                          alpha X_s, the planes get X_s)
 // with M's off-diagonal tiles split once per call and the 128 x 128
-// diagonal-block inverses formed in FP64 from the 64 x 64 FP64-formed FP32
+// diagonal-block inverses formed from the 64 x 64 FP64-formed FP32
 // inverses of batched.cu (one doubling step: off-diagonal block
-// -Q^-1 C P^-1 for lower, -P^-1 C Q^-1 for upper), written as planes of
-// inv and of inv^T (the adjoint's operator).  The adjoint solves with M^T
-// the same way and forms dA = -(1/alpha) dB X^T on the stored triangle with
+// -Q^-1 C P^-1 for lower, -P^-1 C Q^-1 for upper; FP64 accumulation for
+// 6xBF16, FP32 for the modes whose planes keep fewer bits), written as
+// planes of inv and of inv^T (the adjoint's operator).  The adjoint solves
+// with M^T the same way, reading M's tiles MN-major in the BF16 modes (TF32
+// splits M^T), and forms dA = -(1/alpha) dB X^T on the stored triangle with
 // one masked product launch (tiles off the triangle store zeros).
 //
 // Every wait is bounded (2 s); on timeout the kernel records
